@@ -1,0 +1,233 @@
+"""Seeded synthetic workloads with the shapes, sizes and value distributions of the benchmark
+configurations (the reference publishes no dataset; every input here is generated from a seed).
+
+Each builder returns a `Scene`: plain NumPy arrays plus the facade calls that configure a
+`Simulation` (the reference API, src/dem_bindings.cpp:72-432). Unit convention: metres, with
+`set_global_scale(r_ref)` and a canonical shape radius of 1, so the narrowphase finite-difference
+step (1e-4 canonical, src/narrowphase.hpp:235) is relative to the grain size.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+SPHERE, HOLLOW_CYLINDER, BOX = 1, 2, 3
+
+
+@dataclass
+class Scene:
+    name: str
+    pos: np.ndarray                      # (N,3)
+    vel: np.ndarray                      # (N,3)
+    inv_mass: np.ndarray                 # (N,)
+    inv_inertia: np.ndarray              # (N,3)
+    quat: np.ndarray | None = None       # (N,4) x,y,z,w
+    scales: np.ndarray | None = None     # (N,)
+    shape: tuple = (SPHERE, 1.0, 0.0, 0.0)
+    global_scale: float = 1.0
+    domain: tuple | None = None          # (min3, max3, periodic3)
+    planes: list = field(default_factory=list)
+    gravity: tuple = (0.0, 0.0, -9.81)
+    material: tuple = (0.5, 0.0, 0.5)    # (e_n, e_t, mu)
+    iterations: tuple = (10, 10)         # (position, velocity)
+    dt: float = 1e-5                     # one demStep call (= one substep)
+    substeps: int = 10                   # demStep calls per outer step
+    shell: np.ndarray | None = None      # optional explicit point shell
+    hertz: tuple | None = None           # (E, nu) for the Hertz engine
+
+    @property
+    def n(self) -> int:
+        return int(self.pos.shape[0])
+
+    def apply(self, sim):
+        """Configure `sim` (any object with the reference facade methods) with this scene."""
+        sim.initialize_shape(*self.shape)
+        if self.shell is not None:
+            sim.set_shell_points(self.shell)
+        sim.set_global_scale(self.global_scale)
+        if self.domain is not None:
+            mn, mx, per = self.domain
+            sim.set_domain(tuple(mn), tuple(mx))
+            sim.enable_periodicity(*per)
+        sim.set_gravity(*self.gravity)
+        sim.set_material_params(*self.material)
+        sim.set_solver_iterations(*self.iterations)
+        if self.hertz is not None:
+            sim.set_hertz_material(0, *self.hertz)
+        for p in self.planes:
+            sim.add_plane(*p)
+        sim.set_positions(self.pos)
+        if self.quat is not None:
+            sim.set_quaternions(self.quat)
+        if self.scales is not None:
+            sim.set_scales(self.scales)
+        sim.set_velocities(self.vel)
+        sim.set_inv_mass(self.inv_mass)
+        sim.set_inv_inertia(self.inv_inertia)
+        sim.set_dt(self.dt)
+        return sim
+
+
+def box_planes(mn, mx):
+    """Six inward-facing planes of a closed box (point, normal)."""
+    (x0, y0, z0), (x1, y1, z1) = mn, mx
+    return [(x0, 0, 0, 1, 0, 0), (x1, 0, 0, -1, 0, 0), (0, y0, 0, 0, 1, 0), (0, y1, 0, 0, -1, 0),
+            (0, 0, z0, 0, 0, 1), (0, 0, z1, 0, 0, -1)]
+
+
+def sphere_props(radius, density):
+    m = density * 4.0 / 3.0 * np.pi * radius ** 3
+    inv_i = 1.0 / (0.4 * m * radius ** 2)
+    return 1.0 / m, inv_i
+
+
+def plain_settling(seed=1, nx=16, ny=16, nz=16, cells_z=64, radius=1e-3, spacing_r=2.2,
+                   jitter_r=0.05, vmax=0.1, density=2500.0, e=0.5, mu=0.5, dt_outer=1e-4,
+                   substeps=10, iterations=(10, 10)) -> Scene:
+    """Plain XPBD settling: monodisperse spheres on a jittered simple-cubic lattice at the bottom of
+    a closed box of nx x ny x cells_z lattice cells (6 analytic planes), uniform random velocities.
+    Defaults are the 4,096-sphere configuration (16x16x16 in a 16x16x64-cell box)."""
+    rng = np.random.default_rng(seed)
+    a = spacing_r * radius
+    ii, jj, kk = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    base = np.stack([ii.ravel(), jj.ravel(), kk.ravel()], axis=1).astype(np.float64)
+    # particle index runs x-fastest (i + nx*(j + ny*k)) like a poured lattice
+    order = np.lexsort((base[:, 0], base[:, 1], base[:, 2]))
+    base = base[order]
+    pos = (base + 0.5) * a + rng.uniform(-jitter_r * radius, jitter_r * radius, base.shape)
+    vel = rng.uniform(-vmax, vmax, base.shape)
+    n = pos.shape[0]
+    im, iI = sphere_props(radius, density)
+    mn = (0.0, 0.0, 0.0)
+    mx = (nx * a, ny * a, cells_z * a)
+    return Scene(name=f"plain_settling_{n}", pos=pos, vel=vel, inv_mass=np.full(n, im),
+                 inv_inertia=np.full((n, 3), iI), shape=(SPHERE, 1.0, 0.0, 0.0),
+                 global_scale=radius, domain=(mn, mx, (False, False, False)),
+                 planes=box_planes(mn, mx), gravity=(0.0, 0.0, -9.81), material=(e, 0.0, mu),
+                 iterations=iterations, dt=dt_outer / substeps, substeps=substeps)
+
+
+def random_unit_quats(rng, n):
+    q = rng.normal(size=(n, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    return q
+
+
+def hollow_cylinders(seed=3, n=65536, r_out=1e-3, r_in=0.6e-3, length=3e-3, box=(60e-3, 60e-3, 120e-3),
+                     density=1200.0, e=0.4, mu=0.3, dt_outer=5e-5, substeps=8, iterations=(20, 10),
+                     shell_points=None, max_tries=200) -> Scene:
+    """Point-shell hollow cylinders (body axis y), uniform random orientations, centres by random
+    sequential addition with bounding-sphere exclusion in a closed box (6 planes)."""
+    rng = np.random.default_rng(seed)
+    rb = float(np.hypot(r_out, 0.5 * length))  # bounding-sphere radius
+    lo = np.array([rb, rb, rb])
+    hi = np.array(box) - rb
+    cell = 2 * rb
+    dims = np.maximum(1, np.floor((hi - lo) / cell).astype(int) + 1)
+    grid = {}
+    pts = []
+    tries = 0
+    while len(pts) < n and tries < n * max_tries:
+        tries += 1
+        p = lo + rng.uniform(0, 1, 3) * (hi - lo)
+        c = tuple(np.minimum(((p - lo) / cell).astype(int), dims - 1))
+        ok = True
+        for dx in (-1, 0, 1):
+            for dy in (-1, 0, 1):
+                for dz in (-1, 0, 1):
+                    for q in grid.get((c[0] + dx, c[1] + dy, c[2] + dz), ()):
+                        if np.sum((pts[q] - p) ** 2) < (2 * rb) ** 2:
+                            ok = False
+                            break
+                    if not ok:
+                        break
+                if not ok:
+                    break
+            if not ok:
+                break
+        if ok:
+            grid.setdefault(c, []).append(len(pts))
+            pts.append(p)
+    pos = np.array(pts)
+    n = pos.shape[0]
+    vol = np.pi * (r_out ** 2 - r_in ** 2) * length
+    m = density * vol
+    term = r_out ** 2 + r_in ** 2
+    ixx = m * (3 * term + length ** 2) / 12.0
+    iyy = 0.5 * m * term  # body axis y
+    inv_i = np.tile([1.0 / ixx, 1.0 / iyy, 1.0 / ixx], (n, 1))
+    mn, mx = (0.0, 0.0, 0.0), tuple(box)
+    s = r_out  # global scale: canonical outer radius 1
+    return Scene(name=f"hollow_cylinders_{n}", pos=pos, vel=np.zeros((n, 3)),
+                 inv_mass=np.full(n, 1.0 / m), inv_inertia=inv_i, quat=random_unit_quats(rng, n),
+                 shape=(HOLLOW_CYLINDER, 1.0, length / s, (r_out - r_in) / s), global_scale=s,
+                 domain=(mn, mx, (False, False, False)), planes=box_planes(mn, mx),
+                 material=(e, 0.0, mu), iterations=iterations, dt=dt_outer / substeps,
+                 substeps=substeps, shell=shell_points)
+
+
+def polydisperse(seed=2, n=262144, median=1e-3, sigma=0.25, rmin=0.5e-3, rmax=2e-3, phi=0.35,
+                 density=2500.0, E=1e7, nu=0.3, mu=0.4, e=0.6, dt_outer=2e-5, substeps=10,
+                 periodic=True) -> Scene:
+    """Polydisperse lognormal spheres placed without overlap by random sequential addition in a box
+    periodic in x and y (L_x = L_y, height 2 L_x, solids fraction phi) with a floor at z = 0."""
+    rng = np.random.default_rng(seed)
+    r = np.clip(rng.lognormal(np.log(median), sigma, n), rmin, rmax)
+    vs = np.sum(4.0 / 3.0 * np.pi * r ** 3)
+    L = (vs / (2.0 * phi)) ** (1.0 / 3.0)
+    H = 2.0 * L
+    order = np.argsort(-r)  # place large first
+    cell = 2 * rmax
+    dims = np.maximum(1, np.floor(np.array([L, L, H]) / cell).astype(int))
+    head = -np.ones(int(np.prod(dims)), dtype=np.int64)
+    nxt = -np.ones(n, dtype=np.int64)
+    pos = np.zeros((n, 3))
+    placed = np.zeros(n, bool)
+    for idx in order:
+        ri = r[idx]
+        for _ in range(1000):
+            p = np.array([rng.uniform(0, L), rng.uniform(0, L), rng.uniform(ri, H - ri)])
+            c = np.minimum((p / (np.array([L, L, H]) / dims)).astype(int), dims - 1)
+            ok = True
+            for dx in (-1, 0, 1):
+                for dy in (-1, 0, 1):
+                    for dz in (-1, 0, 1):
+                        cc = c + (dx, dy, dz)
+                        if cc[2] < 0 or cc[2] >= dims[2]:
+                            continue
+                        cc[0] %= dims[0]
+                        cc[1] %= dims[1]
+                        q = head[(cc[2] * dims[1] + cc[1]) * dims[0] + cc[0]]
+                        while q >= 0:
+                            d = pos[q] - p
+                            d[:2] -= L * np.round(d[:2] / L)
+                            if d @ d < (ri + r[q]) ** 2:
+                                ok = False
+                                break
+                            q = nxt[q]
+                        if not ok:
+                            break
+                    if not ok:
+                        break
+                if not ok:
+                    break
+            if ok:
+                pos[idx] = p
+                placed[idx] = True
+                k = (c[2] * dims[1] + c[1]) * dims[0] + c[0]
+                nxt[idx] = head[k]
+                head[k] = idx
+                break
+    keep = np.nonzero(placed)[0]
+    pos, r = pos[keep], r[keep]
+    n = pos.shape[0]
+    m = density * 4.0 / 3.0 * np.pi * r ** 3
+    inv_i = 1.0 / (0.4 * m * r ** 2)
+    mn, mx = (0.0, 0.0, 0.0), (L, L, H)
+    return Scene(name=f"polydisperse_{n}", pos=pos, vel=np.zeros((n, 3)), inv_mass=1.0 / m,
+                 inv_inertia=np.repeat(inv_i[:, None], 3, axis=1), scales=r / median,
+                 shape=(SPHERE, 1.0, 0.0, 0.0), global_scale=median,
+                 domain=(mn, mx, (periodic, periodic, False)),
+                 planes=[(0.0, 0.0, 0.0, 0.0, 0.0, 1.0)], material=(e, 0.0, mu),
+                 dt=dt_outer / substeps, substeps=substeps, hertz=(E, nu))

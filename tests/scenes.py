@@ -1,0 +1,106 @@
+"""Small seeded scenes that drive every branch of the substep for the parity tests.
+
+Each builder returns a `workloads.Scene` (positions, velocities, masses, shape, domain, planes and
+material settings) plus optional extra configuration applied after the scene (walls, materials,
+thermostat, growth). Sizes are chosen so the oracle finishes a few dozen substeps in well under a
+second.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from peclet.dem import workloads as W
+
+
+def _cluster(rng, n, box, radius):
+    lo, hi = np.array(box[0]) + radius, np.array(box[1]) - radius
+    return lo + rng.uniform(0, 1, (n, 3)) * (hi - lo)
+
+
+def dense_spheres(seed=11, n=300, box=((0, 0, 0), (8e-3, 8e-3, 8e-3)), radius=1e-3, vmax=0.3,
+                  e=0.5, mu=0.5, gravity=(0, 0, -9.81), iters=(10, 10), dt=1e-5):
+    """Overlapping random spheres in a closed box: many contacts, deep overlaps, all planes."""
+    rng = np.random.default_rng(seed)
+    pos = _cluster(rng, n, box, radius)
+    im, iI = W.sphere_props(radius, 2500.0)
+    return W.Scene(name="dense_spheres", pos=pos, vel=rng.uniform(-vmax, vmax, (n, 3)),
+                   inv_mass=np.full(n, im), inv_inertia=np.full((n, 3), iI),
+                   global_scale=radius, domain=(box[0], box[1], (False, False, False)),
+                   planes=W.box_planes(box[0], box[1]), gravity=gravity, material=(e, 0.0, mu),
+                   iterations=iters, dt=dt)
+
+
+def settled_column(seed=12, nx=5, ny=5, nz=12, iters=(10, 10)):
+    """A lattice column dropped onto the floor: persistent contacts, warm start, stabilization."""
+    sc = W.plain_settling(seed=seed, nx=nx, ny=ny, nz=nz, cells_z=nz + 2, spacing_r=1.98,
+                          jitter_r=0.02, vmax=0.05, iterations=iters)
+    sc.name = "settled_column"
+    return sc
+
+
+def polydisperse_periodic(seed=13, n=250, L=8e-3, H=6e-3, radius=1e-3):
+    """Polydisperse spheres in a box periodic in x and y with a floor plane (ghost images)."""
+    rng = np.random.default_rng(seed)
+    r = np.clip(rng.lognormal(np.log(radius), 0.25, n), 0.5 * radius, 2 * radius)
+    pos = np.stack([rng.uniform(0, L, n), rng.uniform(0, L, n), rng.uniform(r, H)], axis=1)
+    m = 2500.0 * 4 / 3 * np.pi * r ** 3
+    iI = 1.0 / (0.4 * m * r ** 2)
+    return W.Scene(name="poly_periodic", pos=pos, vel=rng.uniform(-0.2, 0.2, (n, 3)),
+                   inv_mass=1.0 / m, inv_inertia=np.repeat(iI[:, None], 3, 1), scales=r / radius,
+                   global_scale=radius, domain=((0, 0, 0), (L, L, H), (True, True, False)),
+                   planes=[(0, 0, 0, 0, 0, 1)], material=(0.6, 0.0, 0.4), dt=1e-5)
+
+
+def cylinders(seed=14, n=24, L=8e-3, shape_type=W.HOLLOW_CYLINDER, shell=None):
+    """A few hollow cylinders (or cubes) with random orientations: point-shell narrowphase."""
+    rng = np.random.default_rng(seed)
+    s = 1e-3
+    pos = _cluster(rng, n, ((0, 0, 0), (L, L, L)), 1.6 * s)
+    q = W.random_unit_quats(rng, n)
+    m = 1200.0 * np.pi * (1.0 - 0.36) * 3.0 * s ** 3
+    if shape_type == W.HOLLOW_CYLINDER:
+        shape = (W.HOLLOW_CYLINDER, 1.0, 3.0, 0.4)
+        iI = np.tile([12 / (m * (3 * 1.36 + 9) * s * s), 2 / (m * 1.36 * s * s),
+                      12 / (m * (3 * 1.36 + 9) * s * s)], (n, 1))
+    else:
+        shape = (W.BOX, 1.0, 0.0, 0.0)
+        iI = np.full((n, 3), 6.0 / (m * 4 * s * s))
+    return W.Scene(name=f"shells_{shape_type}", pos=pos, vel=rng.uniform(-0.3, 0.3, (n, 3)),
+                   inv_mass=np.full(n, 1.0 / m), inv_inertia=iI, quat=q, shape=shape,
+                   global_scale=s, domain=((0, 0, 0), (L, L, L), (False, False, False)),
+                   planes=W.box_planes((0, 0, 0), (L, L, L)), material=(0.4, 0.0, 0.3),
+                   iterations=(20, 10), dt=6.25e-6, shell=shell)
+
+
+def drum_wall_grid(R=6e-3, length=4e-3, h=0.5e-3):
+    """Hollow-cylinder container (axis z) as a world-space SDF grid, positive in the void."""
+    nx = ny = int(np.ceil(2.4 * R / h)) + 1
+    nz = int(np.ceil((length + 4 * h) / h)) + 1
+    origin = np.array([-1.2 * R, -1.2 * R, -2 * h])
+    x = origin[0] + h * np.arange(nx)
+    y = origin[1] + h * np.arange(ny)
+    z = origin[2] + h * np.arange(nz)
+    Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
+    radial = R - np.sqrt(X ** 2 + Y ** 2)
+    axial = np.minimum(Z, length - Z)
+    grid = np.minimum(radial, axial)  # x-fastest after ravel of (z, y, x)
+    return grid.ravel(), nx, ny, nz, origin, (h, h, h)
+
+
+def spheres_in_drum(seed=15, n=120, R=6e-3, length=4e-3, omega=2.0, e=0.5, mu=0.4):
+    rng = np.random.default_rng(seed)
+    r = 0.5e-3
+    ang = rng.uniform(0, 2 * np.pi, n)
+    rad = np.sqrt(rng.uniform(0, 1, n)) * (R - 1.5 * r)
+    pos = np.stack([rad * np.cos(ang), -np.abs(rad * np.sin(ang)), rng.uniform(1.5 * r, length - 1.5 * r, n)], 1)
+    im, iI = W.sphere_props(r, 2500.0)
+    sc = W.Scene(name="drum", pos=pos, vel=rng.uniform(-0.1, 0.1, (n, 3)), inv_mass=np.full(n, im),
+                 inv_inertia=np.full((n, 3), iI), global_scale=r,
+                 domain=((-R, -R, 0), (R, R, length), (False, False, False)),
+                 gravity=(0, -9.81, 0), material=(e, 0.0, mu), dt=1e-5)
+    grid, nx, ny, nz, origin, spacing = drum_wall_grid(R, length)
+
+    def extra(sim):
+        wid = sim.add_sdf_wall(grid, nx, ny, nz, origin, spacing, 0.5, 0.6)
+        sim.set_wall_velocity(wid, (0, 0, 0), (0, 0, omega), (0, 0, 0))
+    return sc, extra
