@@ -1,0 +1,155 @@
+/* peclet-dem B200 substep: C ABI.
+ *
+ * Drop-in boundary for the reference's `peclet.dem.Simulation` (nanobind module `_dem`,
+ * src/dem_bindings.cpp:51-464, facade src/sim.hpp:909-1670). Every entry point takes a handle, plain
+ * host pointers and sizes, returns an int status (PDEM_OK or an error code, message from
+ * pdem_last_error()) and never throws across the ABI. Host arrays are double precision; the handle's
+ * precision (64: FP64 step, 32: the reference's float arithmetic) decides what the device computes.
+ * Getters return the number of values available (which may exceed `cap`; only `cap` are written).
+ *
+ * Each declaration cites the reference interface it replaces (file:line).
+ */
+#ifndef PDEM_H
+#define PDEM_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PDEM_OK 0
+#define PDEM_ERR_RUNTIME 1     /* std::runtime_error in the reference  -> RuntimeError */
+#define PDEM_ERR_INVALID 2     /* std::invalid_argument in the reference -> ValueError  */
+#define PDEM_ERR_UNSUPPORTED 3 /* a mode this build does not provide                     */
+#define PDEM_ERR_CUDA 4        /* CUDA runtime failure (no device, out of memory, ...)   */
+
+typedef void* pdem_handle;
+
+/* last error message of this thread */
+const char* pdem_last_error(void);
+/* "CUDA sm_100a" and the device name; for diagnostics */
+const char* pdem_execution_space(void);
+
+/* Simulation(capacity)                         src/dem_bindings.cpp:72, src/sim.hpp:911-916 */
+int pdem_create(int capacity, int precision, pdem_handle* out);
+void pdem_destroy(pdem_handle h);
+
+/* initialize_shape / initialize / set_sphere_shape   src/dem_bindings.cpp:73-80, src/sim.hpp:949-1021 */
+int pdem_initialize_shape(pdem_handle h, int shape_type, double radius, double height, double thickness);
+/* set_sdf_shape                                 src/dem_bindings.cpp:86-103, src/sim.hpp:1034-1084 */
+int pdem_set_sdf_shape(pdem_handle h, const double* grid, int nx, int ny, int nz, const double* origin,
+                       const double* spacing, const double* shell, int nshell, const double* inv_inertia,
+                       double bounding_radius);
+/* extension: replace the active shape's surface point shell (keeps its analytic SDF)          */
+int pdem_set_shell_points(pdem_handle h, const double* pts, int n);
+/* set_domain(lx,ly,lz,px,py,pz)                 src/dem_bindings.cpp:104-106, src/sim.hpp:1086-1089 */
+int pdem_set_domain(pdem_handle h, double lx, double ly, double lz, int px, int py, int pz);
+/* set_domain(min, max)                          src/dem_bindings.cpp:109-118, src/sim.hpp:1091-1099 */
+int pdem_set_domain_minmax(pdem_handle h, const double* mn, const double* mx);
+/* enable_periodicity                            src/dem_bindings.cpp:119, src/sim.hpp:1100-1104 */
+int pdem_enable_periodicity(pdem_handle h, int x, int y, int z);
+/* set_gravity                                   src/dem_bindings.cpp:125, src/sim.hpp:1111 */
+int pdem_set_gravity(pdem_handle h, double gx, double gy, double gz);
+/* set_thermostat                                src/dem_bindings.cpp:127, src/sim.hpp:1112-1116 */
+int pdem_set_thermostat(pdem_handle h, double temperature, double tau, double kB);
+/* set_solver_iterations                         src/dem_bindings.cpp:130, src/sim.hpp:1117-1120 */
+int pdem_set_solver_iterations(pdem_handle h, int pos, int vel);
+/* set_velocity_use_gs                           src/dem_bindings.cpp:154, src/sim.hpp:1123 */
+int pdem_set_velocity_use_gs(pdem_handle h, int use_gs);
+/* set_stabilization / set_stabilization_mode    src/dem_bindings.cpp:142-153, src/sim.hpp:1128-1150 */
+int pdem_set_stabilization_mode(pdem_handle h, const char* mode);
+/* set_hertz_material                            src/dem_bindings.cpp:132, src/sim.hpp:1153-1164 */
+int pdem_set_hertz_material(pdem_handle h, int mat, double youngs, double poisson);
+/* set_global_scale                              src/dem_bindings.cpp:157, src/sim.hpp:1171-1174 */
+int pdem_set_global_scale(pdem_handle h, double s);
+/* set_dt                                        src/dem_bindings.cpp:159, src/sim.hpp:1175 */
+int pdem_set_dt(pdem_handle h, double dt);
+/* set_material_params                           src/dem_bindings.cpp:160, src/sim.hpp:1179-1183 */
+int pdem_set_material_params(pdem_handle h, double restitution_normal, double restitution_tangent,
+                             double friction);
+/* set_material_ids                              src/dem_bindings.cpp:163, src/sim.hpp:1187-1193 */
+int pdem_set_material_ids(pdem_handle h, const int* ids, int n);
+/* set_pair_material                             src/dem_bindings.cpp:166, src/sim.hpp:1196-1216 */
+int pdem_set_pair_material(pdem_handle h, int a, int b, double restitution, double friction);
+/* set_wall_material_id                          src/dem_bindings.cpp:170, src/sim.hpp:1218-1225 */
+int pdem_set_wall_material_id(pdem_handle h, int wid, int mat);
+/* add_plane (both overloads)                    src/dem_bindings.cpp:173-183, src/sim.hpp:1226-1232 */
+int pdem_add_plane(pdem_handle h, double px, double py, double pz, double nx, double ny, double nz);
+/* add_sdf_wall                                  src/dem_bindings.cpp:190-205, src/sim.hpp:1242-1274 */
+int pdem_add_sdf_wall(pdem_handle h, const double* grid, int nx, int ny, int nz, const double* origin,
+                      const double* spacing, double restitution, double friction, int* out_index);
+/* set_wall_velocity                             src/dem_bindings.cpp:208-223, src/sim.hpp:1280-1287 */
+int pdem_set_wall_velocity(pdem_handle h, int index, const double* lin_vel, const double* ang_vel,
+                           const double* center);
+/* set_positions (N,3)                           src/dem_bindings.cpp:225-251, src/sim.hpp:1290-1330 */
+int pdem_set_positions(pdem_handle h, const double* xyz, int n);
+/* set_velocities / set_external_forces / clear_external_forces / set_quaternions /
+ * set_angular_velocities / set_inv_inertia / set_inv_mass     src/dem_bindings.cpp:252-288,
+ *                                                             src/sim.hpp:1347-1405 */
+int pdem_set_velocities(pdem_handle h, const double* v, int n);
+int pdem_set_external_forces(pdem_handle h, const double* f, int n);
+int pdem_clear_external_forces(pdem_handle h);
+int pdem_set_quaternions(pdem_handle h, const double* q, int n);
+int pdem_set_angular_velocities(pdem_handle h, const double* w, int n);
+int pdem_set_inv_inertia(pdem_handle h, const double* ii, int n);
+int pdem_set_inv_mass(pdem_handle h, const double* im, int n);
+/* set_scales / set_scales_uniform / set_growth_params / get_growth_factor / get_growth_rate
+ *                                               src/dem_bindings.cpp:291-305, src/sim.hpp:1331-1426 */
+int pdem_set_scales(pdem_handle h, const double* s, int n);
+int pdem_set_scales_uniform(pdem_handle h, double s);
+int pdem_set_growth_params(pdem_handle h, double rate, double new_factor);
+double pdem_get_growth_factor(pdem_handle h);
+double pdem_get_growth_rate(pdem_handle h);
+/* get_positions / velocities / quaternions / angular_velocities / inv_inertia / scales / masses
+ *                                               src/dem_bindings.cpp:289-346, src/sim.hpp:1406-1452 */
+long pdem_get_positions(pdem_handle h, double* out, long cap);
+long pdem_get_velocities(pdem_handle h, double* out, long cap);
+long pdem_get_quaternions(pdem_handle h, double* out, long cap);
+long pdem_get_angular_velocities(pdem_handle h, double* out, long cap);
+long pdem_get_inv_inertia(pdem_handle h, double* out, long cap);
+long pdem_get_scales(pdem_handle h, double* out, long cap);
+long pdem_get_masses(pdem_handle h, double* out, long cap);
+/* step(dt): ONE XPBD substep                    src/dem_bindings.cpp:342, src/sim.hpp:1456-1459,97-488 */
+int pdem_step(pdem_handle h, double dt);
+/* step_hertz(dt, substeps, skin_frac)           src/dem_bindings.cpp:139, src/sim.hpp:1167-1170,628-750 */
+int pdem_step_hertz(pdem_handle h, double dt, int substeps, double skin_frac);
+/* compute_overlaps                              src/dem_bindings.cpp:368, src/sim.hpp:1462,494-541 */
+int pdem_compute_overlaps(pdem_handle h, double* out);
+/* num_particles / num_contacts / num_manifolds / max_overlap (+ get_* aliases)
+ *                                               src/dem_bindings.cpp:357-366, src/sim.hpp:1544-1556 */
+int pdem_num_particles(pdem_handle h);
+int pdem_num_contacts(pdem_handle h);
+int pdem_num_manifolds(pdem_handle h);
+double pdem_max_overlap(pdem_handle h);
+/* export_lammps / write_vtp                     src/dem_bindings.cpp:355,369-371, src/sim.hpp:1466-1475,1560-1601 */
+int pdem_export_lammps(pdem_handle h, const char* filename, int step);
+int pdem_write_vtp(pdem_handle h, const char* filename);
+
+/* ---- diagnostics: intermediate products of the last substep, canonical order ----
+ * (the reference keeps them in its Particles SoA, src/particles.hpp:49-151, without a getter)
+ * counts: pairs, contacts, manifolds, bodies incl. ghosts, ledger size, capacity, contact capacity,
+ *         pair capacity
+ * contacts: 17 doubles each (bodyA bodyB n[3] rA[3] rB[3] dist lambdaN wallVel[3] restitution);
+ *           contact_mu: the per-contact friction
+ * manifolds: 23 doubles each (bodyA bodyB Nsum[3] TauA[3] TauB[3] rA[3] rB[3] points wallVel[3] e mu)
+ * lambda: 4 doubles per manifold (normal accumulator, tangential accumulator[3])
+ * ledger: committed sorted keys + 5 doubles (lambda, lambdaT[3], position impulse) */
+int pdem_debug_counts(pdem_handle h, long* out8);
+long pdem_debug_pairs(pdem_handle h, int* out, long cap);
+long pdem_debug_contacts(pdem_handle h, double* out, long cap);
+long pdem_debug_contact_mu(pdem_handle h, double* out, long cap);
+long pdem_debug_manifolds(pdem_handle h, double* out, long cap);
+long pdem_debug_manifold_colors(pdem_handle h, int* out, long cap);
+long pdem_debug_contact_colors(pdem_handle h, int* out, long cap);
+long pdem_debug_lambda(pdem_handle h, double* out, long cap);
+long pdem_debug_pair_keys(pdem_handle h, unsigned long long* out, long cap);
+long pdem_debug_ledger(pdem_handle h, unsigned long long* keys, double* vals, long cap);
+long pdem_debug_grounded(pdem_handle h, int* out, long cap);
+long pdem_debug_pos_lambda(pdem_handle h, double* out, long cap);
+long pdem_debug_hertz(pdem_handle h, unsigned long long* keys, double* xi, long cap);
+/* test hook: set the contact buffer capacity (overflow / clamp behaviour) */
+int pdem_debug_set_max_contacts(pdem_handle h, int max_contacts);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PDEM_H */

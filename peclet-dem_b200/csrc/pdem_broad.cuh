@@ -1,0 +1,298 @@
+// LBVH broadphase (replaces src/broadphase_arborx.hpp:36-107, the ArborX BVH query).
+//
+// Candidate predicate (identical to the reference): box_i = [x_i - b_i, x_i + b_i] per axis with
+// b_i = rad_i + margin (non-finite or oversized boxes parked at -1e30 with b = 0, SANE_BOX), and
+// (i, j) is a candidate iff i is real, j > i and the two closed boxes overlap on every axis.
+// Build: 63-bit Morton codes of the box centres (21 bits per axis, quantised in double), a stable
+// radix sort of (code, index), a Karras binary radix tree (duplicate codes split by index), a
+// bottom-up refit with arrival counters (no waiting), and escape ("rope") links for a stackless
+// depth-first traversal. Emission: per-query count, exclusive scan, write, then each query's list
+// is sorted by j, so the pair list is sorted by (i, j) — the canonical order.
+#pragma once
+#include "pdem_common.cuh"
+
+namespace pdem {
+
+template <class R>
+struct Box {
+  R lo[3], hi[3];
+};
+
+template <class R>
+__device__ __forceinline__ Box<R> saneBox(const Dev<R>& d, int i, const Q4<R>* P, R margin, R boxCap) {
+  const Q4<R> p = P[i];
+  R x = p.x, y = p.y, z = p.z, b = d.rad[i] + margin;
+  if (!(b == b) || !(x == x) || !(y == y) || !(z == z) || (boxCap > R(0) && b > boxCap)) {
+    x = y = z = R(-1.0e30);
+    b = R(0);
+  }
+  Box<R> bx;
+  bx.lo[0] = x - b;
+  bx.lo[1] = y - b;
+  bx.lo[2] = z - b;
+  bx.hi[0] = x + b;
+  bx.hi[1] = y + b;
+  bx.hi[2] = z + b;
+  return bx;
+}
+template <class R>
+__device__ __forceinline__ bool boxOverlap(const Box<R>& a, const Box<R>& b) {
+  return !(a.lo[0] > b.hi[0] || a.hi[0] < b.lo[0] || a.lo[1] > b.hi[1] || a.hi[1] < b.lo[1] ||
+           a.lo[2] > b.hi[2] || a.hi[2] < b.lo[2]);
+}
+
+// order-preserving encoding of a double for atomic min/max of signed values
+__device__ __forceinline__ u64 orderedBits(double v) {
+  const u64 b = (u64)__double_as_longlong(v);
+  return (b & 0x8000000000000000ull) ? ~b : (b | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double fromOrderedBits(u64 o) {
+  const u64 b = (o & 0x8000000000000000ull) ? (o & 0x7fffffffffffffffull) : ~o;
+  return __longlong_as_double((long long)b);
+}
+
+struct BvhBuffers {
+  int n = 0;             // primitives (all particles incl. ghosts)
+  u64* codes = nullptr;  // [n] then sorted in place via the alt buffers
+  u64* codesAlt = nullptr;
+  int* idx = nullptr;    // [n] sorted primitive index
+  int* idxAlt = nullptr;
+  int *left = nullptr, *right = nullptr, *parent = nullptr, *rope = nullptr, *flag = nullptr;
+  u64* bounds = nullptr;  // [6] ordered bits: min xyz, max xyz
+  int* err = nullptr;     // error flags (Counters::err)
+};
+
+template <class R>
+struct BvhNodes {
+  Box<R>* prim = nullptr;  // [n] primitive boxes in ORIGINAL index order
+  Box<R>* node = nullptr;  // [n-1] internal node boxes
+};
+
+template <class R>
+__global__ void kBoxes(Dev<R> d, int n, R margin, R boxCap, BvhNodes<R> bn, BvhBuffers bb) {
+  GRID_STRIDE(i, n) {
+    const Box<R> b = saneBox(d, (int)i, d.posPred, margin, boxCap);
+    bn.prim[i] = b;
+    bool ok = true;
+    double c[3];
+    for (int a = 0; a < 3; ++a) {
+      c[a] = 0.5 * ((double)b.lo[a] + (double)b.hi[a]);
+      ok = ok && isfinite(c[a]) && fabs(c[a]) < 1e29;
+    }
+    if (ok)
+      for (int a = 0; a < 3; ++a) {
+        atomicMin(&bb.bounds[a], orderedBits(c[a]));
+        atomicMax(&bb.bounds[3 + a], orderedBits(c[a]));
+      }
+  }
+}
+
+__device__ __forceinline__ u64 spread21(u64 v) {
+  v &= 0x1fffffull;
+  v = (v | (v << 32)) & 0x1f00000000ffffull;
+  v = (v | (v << 16)) & 0x1f0000ff0000ffull;
+  v = (v | (v << 8)) & 0x100f00f00f00f00full;
+  v = (v | (v << 4)) & 0x10c30c30c30c30c3ull;
+  v = (v | (v << 2)) & 0x1249249249249249ull;
+  return v;
+}
+
+template <class R>
+__global__ void kMorton(int n, BvhNodes<R> bn, BvhBuffers bb) {
+  GRID_STRIDE(i, n) {
+    const Box<R> b = bn.prim[i];
+    double lo[3], ext[3];
+    for (int a = 0; a < 3; ++a) {
+      lo[a] = fromOrderedBits(bb.bounds[a]);
+      ext[a] = fromOrderedBits(bb.bounds[3 + a]) - lo[a];
+    }
+    u64 code = 0x7fffffffffffffffull;
+    bool ok = true;
+    u64 q[3];
+    for (int a = 0; a < 3; ++a) {
+      const double c = 0.5 * ((double)b.lo[a] + (double)b.hi[a]);
+      if (!(isfinite(c) && fabs(c) < 1e29)) {
+        ok = false;
+        break;
+      }
+      double t = ext[a] > 0.0 ? (c - lo[a]) / ext[a] : 0.0;
+      t = fmin(fmax(t, 0.0), 1.0);
+      q[a] = (u64)(t * 2097151.0);
+    }
+    if (ok)
+      code = (spread21(q[0]) << 2) | (spread21(q[1]) << 1) | spread21(q[2]);
+    bb.codes[i] = code;
+    bb.idx[i] = (int)i;
+  }
+}
+
+// common-prefix length of sorted keys i and j (duplicates split by position)
+__device__ __forceinline__ int deltaKey(const u64* k, int n, int i, int j) {
+  if (j < 0 || j >= n)
+    return -1;
+  const u64 a = k[i], b = k[j];
+  if (a == b)
+    return 64 + __clz(i ^ j);
+  return __clzll(a ^ b);
+}
+
+// Karras 2012: internal node i of n-1; leaves are nodes n-1 .. 2n-2
+__global__ void kKarras(BvhBuffers bb) {
+  const int n = bb.n;
+  GRID_STRIDE(ii, n - 1) {
+    const int i = (int)ii;
+    const u64* k = bb.codes;
+    const int dir = (deltaKey(k, n, i, i + 1) - deltaKey(k, n, i, i - 1)) >= 0 ? 1 : -1;
+    const int dmin = deltaKey(k, n, i, i - dir);
+    int lmax = 2;
+    while (deltaKey(k, n, i, i + lmax * dir) > dmin)
+      lmax <<= 1;
+    int l = 0;
+    for (int t = lmax >> 1; t >= 1; t >>= 1)
+      if (deltaKey(k, n, i, i + (l + t) * dir) > dmin)
+        l += t;
+    const int j = i + l * dir;
+    const int dnode = deltaKey(k, n, i, j);
+    int s = 0, t = l;
+    while (true) {
+      t = (t + 1) >> 1;
+      if (deltaKey(k, n, i, i + (s + t) * dir) > dnode)
+        s += t;
+      if (t <= 1)
+        break;
+    }
+    const int gamma = i + s * dir + (dir < 0 ? -1 : 0);
+    const int lo = i < j ? i : j, hi = i < j ? j : i;
+    const int L = (lo == gamma) ? (n - 1 + gamma) : gamma;
+    const int Rn = (hi == gamma + 1) ? (n - 1 + gamma + 1) : (gamma + 1);
+    bb.left[i] = L;
+    bb.right[i] = Rn;
+    bb.parent[L] = i;
+    bb.parent[Rn] = i;
+  }
+}
+
+template <class R>
+__device__ __forceinline__ Box<R> loadBoxCG(const Box<R>* p) {
+  Box<R> b;
+  const R* s = reinterpret_cast<const R*>(p);
+  R* o = reinterpret_cast<R*>(&b);
+#pragma unroll
+  for (int a = 0; a < 6; ++a)
+    o[a] = __ldcg(s + a);
+  return b;
+}
+
+// bottom-up box refit: the second child to arrive at a node computes its union
+template <class R>
+__global__ void kRefit(BvhBuffers bb, BvhNodes<R> bn) {
+  const int n = bb.n;
+  GRID_STRIDE(k, n) {
+    int node = bb.parent[n - 1 + (int)k];
+    for (int guard = 0;; ++guard) {
+      if (guard > n) {  // deeper than the number of primitives: corrupt tree, stop
+        atomicOr(&bb.err[0], 1);
+        break;
+      }
+      __threadfence();
+      if (atomicAdd(&bb.flag[node], 1) == 0)
+        break;
+      __threadfence();
+      Box<R> u;
+      const int c[2] = {bb.left[node], bb.right[node]};
+      for (int s = 0; s < 2; ++s) {
+        const Box<R> b = (c[s] >= n - 1) ? bn.prim[bb.idx[c[s] - (n - 1)]] : loadBoxCG(&bn.node[c[s]]);
+        for (int a = 0; a < 3; ++a) {
+          u.lo[a] = (s == 0) ? b.lo[a] : fmin(u.lo[a], b.lo[a]);
+          u.hi[a] = (s == 0) ? b.hi[a] : fmax(u.hi[a], b.hi[a]);
+        }
+      }
+      R* dst = reinterpret_cast<R*>(&bn.node[node]);
+      const R* src = reinterpret_cast<const R*>(&u);
+      for (int a = 0; a < 6; ++a)
+        __stcg(dst + a, src[a]);
+      if (node == 0)
+        break;
+      node = bb.parent[node];
+    }
+  }
+}
+
+// escape link of every node: the right sibling of the nearest ancestor-or-self that is a left
+// child (-1 past the last leaf)
+__global__ void kRopes(BvhBuffers bb) {
+  const int n = bb.n;
+  GRID_STRIDE(v, 2 * n - 1) {
+    int cur = (int)v, r = -1;
+    for (int guard = 0; cur != 0; ++guard) {
+      if (guard > n) {
+        atomicOr(&bb.err[0], 1);
+        break;
+      }
+      const int p = bb.parent[cur];
+      if (bb.left[p] == cur) {
+        r = bb.right[p];
+        break;
+      }
+      cur = p;
+    }
+    bb.rope[v] = r;
+  }
+}
+
+// stackless traversal for real particle i; mode 0 counts j > i, mode 1 writes them
+template <class R, int MODE>
+__global__ void kQuery(Dev<R> d, int numReal, BvhBuffers bb, BvhNodes<R> bn, int* cnt, const int* off,
+                       int2* out, int outCap) {
+  const int n = bb.n;
+  GRID_STRIDE(ii, numReal) {
+    const int i = (int)ii;
+    const Box<R> q = bn.prim[i];
+    int c = 0;
+    int base = MODE ? off[i] : 0;
+    int node = (n > 1) ? 0 : -1;
+    for (long guard = 0; node != -1; ++guard) {
+      if (guard > 4L * n + 8) {  // every node is visited at most once per query
+        atomicOr(&bb.err[0], 1);
+        break;
+      }
+      if (node >= n - 1) {
+        const int j = bb.idx[node - (n - 1)];
+        if (j > i && boxOverlap(q, bn.prim[j])) {
+          if (MODE) {
+            const int s = base + c;
+            if (s < outCap)
+              out[s] = make_int2(i, j);
+          }
+          ++c;
+        }
+        node = bb.rope[node];
+      } else {
+        if (boxOverlap(q, bn.node[node]))
+          node = bb.left[node];
+        else
+          node = bb.rope[node];
+      }
+    }
+    if (!MODE)
+      cnt[i] = c;
+  }
+}
+
+// sort each query's list by j (insertion sort; lists are short)
+__global__ void kSortPairLists(int numReal, const int* off, int2* pairs, int cap) {
+  GRID_STRIDE(ii, numReal) {
+    const int b = off[ii], e = min(off[ii + 1], cap);
+    for (int x = b + 1; x < e; ++x) {
+      const int2 v = pairs[x];
+      int y = x - 1;
+      while (y >= b && pairs[y].y > v.y) {
+        pairs[y + 1] = pairs[y];
+        --y;
+      }
+      pairs[y + 1] = v;
+    }
+  }
+}
+
+}  // namespace pdem

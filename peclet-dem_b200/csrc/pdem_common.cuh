@@ -1,0 +1,119 @@
+// Shared device-side definitions of the B200 substep: the device view of the simulation state
+// (`Dev<R>`), counters, launch geometry and order-preserving atomics.
+//
+// Layout in HBM (structure of arrays, one aligned 4-wide record per particle field so one field
+// of one body is one 16 B / 32 B load):
+//   particles [capacity]:   pos, vel, angVel, invI, posPred, velPred, angVelPred, quat, quatPred,
+//                           extForce, dVel, dAngVel, dPos (Q4<R>); invMass, scale, targetScale, rad
+//                           (R); shapeId, realIdx, counts (int); planeFric (2 R); grounded, matId (u8)
+//   pairs [maxPairs]:       int2 (i, j), sorted by (i, j)
+//   contacts [maxContacts]: cab int2 (bodyA, bodyB); cn = normal|dist, crA = rA|lambdaN,
+//                           crB = rB|restitution, cbv = wall velocity|friction (Q4<R>)
+//   manifolds [maxContacts]: mab int2; mnp int; mN = Nsum|restitution_sum, mTA = TauA|friction_sum,
+//                           mTB, mrA, mrB, mwv (Q4<R>)
+// Every cross-thread accumulation that the reference performs with atomics is done here in the
+// canonical order (ascending source index) with prefix sums and owner-computes gathers, so the
+// result is deterministic and matches the serial reference; only order-free reductions (max of
+// non-negative values, integer counts) use atomics.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "pdem_math.cuh"
+
+namespace pdem {
+
+using u64 = unsigned long long;
+
+constexpr int kMaxMaterials = 8;
+constexpr int kHertzMaxWalls = 4;
+constexpr int kMaxPlanes = 8;
+constexpr int kNumSMs = 148;
+constexpr int kBlock = 256;
+
+// device-resident counters and loop-control flags of one substep
+template <class R>
+struct Counters {
+  int pairCount;      // candidate pairs found (may exceed capacity: host grows and re-runs)
+  int contactTotal;   // contacts wanted (before the capacity clamp)
+  int contactCount;   // contacts stored
+  int manifoldCount;
+  int topGhost;       // numReal + ghosts stored
+  int ghostWanted;
+  int remaining;      // colouring: entries still uncoloured after the last round
+  int maxColor;       // colouring: max colour (INT_MIN identity)
+  int leftover;       // colouring: entries left uncoloured
+  int velDone;        // adaptive stop reached in the main velocity loop
+  int stabRun;        // stabilization pass triggered
+  int stabDone;       // adaptive stop reached in the stabilization loop
+  int posDone;        // adaptive stop reached in the position loop
+  int hzCand;         // Hertz wall candidates wanted
+  int hzRebuild;      // Hertz: displacement check asks for a pair-list rebuild
+  int err;            // bit flags: a bounded loop hit its iteration limit (1 = BVH traversal/build)
+  R maxOverlap;
+  R maxApproach;
+  R hzMaxDisp2;
+  R pad1;
+};
+
+template <class R>
+struct Dev {
+  int cap = 0, maxPairs = 0, maxContacts = 0;
+  Q4<R> *pos = nullptr, *vel = nullptr, *angVel = nullptr, *invI = nullptr, *posPred = nullptr,
+        *velPred = nullptr, *angVelPred = nullptr, *quat = nullptr, *quatPred = nullptr,
+        *extForce = nullptr, *dVel = nullptr, *dAngVel = nullptr, *dPos = nullptr;
+  R *invMass = nullptr, *scale = nullptr, *targetScale = nullptr, *rad = nullptr, *planeFric = nullptr;
+  int *shapeId = nullptr, *realIdx = nullptr, *counts = nullptr;
+  uint8_t *grounded = nullptr, *matId = nullptr;
+  long long* winner = nullptr;
+  u64* mask = nullptr;
+  int2* pairs = nullptr;
+  // contacts
+  int2* cab = nullptr;
+  Q4<R> *cn = nullptr, *crA = nullptr, *crB = nullptr, *cbv = nullptr;
+  int *cColor = nullptr, *cSlot = nullptr;
+  R* posLamC = nullptr;
+  // manifolds
+  int2* mab = nullptr;
+  int* mnp = nullptr;
+  Q4<R> *mN = nullptr, *mTA = nullptr, *mTB = nullptr, *mrA = nullptr, *mrB = nullptr, *mwv = nullptr;
+  int* mColor = nullptr;
+  u64 *pairKeys = nullptr, *prevKeys = nullptr;
+  uint8_t *persistent = nullptr, *sideFlags = nullptr;
+  R *lambda = nullptr, *prevLambda = nullptr, *vn0 = nullptr, *posImp = nullptr, *prevPosImp = nullptr;
+  Q4<R> *lambdaT = nullptr, *prevLambdaT = nullptr, *vt0 = nullptr;
+  // static geometry
+  const ShapeDesc<R>* shapes = nullptr;
+  const Q4<R>* shell = nullptr;
+  const R* sdfGrid = nullptr;
+  const PlaneDesc<R>* planes = nullptr;
+  const WallDesc<R>* walls = nullptr;
+  const R* wallGrid = nullptr;
+  const R* pairMat = nullptr;  // null = feature off
+  const R *hzE = nullptr, *hzNu = nullptr;
+  Counters<R>* ctr = nullptr;
+};
+
+// ---- launch geometry: grid-stride loops over a device-resident count ----
+inline int gridFor(long n, int block = kBlock) {
+  long b = (n + block - 1) / block;
+  if (b < 1)
+    b = 1;
+  if (b > kNumSMs * 32)
+    b = kNumSMs * 32;
+  return (int)b;
+}
+#define GRID_STRIDE(i, n) \
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < (long)(n); i += (long)gridDim.x * blockDim.x)
+
+// ---- max of non-negative values via ordered integer bits (order-free, NaN ignored) ----
+__device__ __forceinline__ void atomicMaxNonNeg(double* p, double v) {
+  if (v > 0.0)
+    atomicMax(reinterpret_cast<unsigned long long*>(p), (unsigned long long)__double_as_longlong(v));
+}
+__device__ __forceinline__ void atomicMaxNonNeg(float* p, float v) {
+  if (v > 0.0f)
+    atomicMax(reinterpret_cast<unsigned int*>(p), (unsigned int)__float_as_int(v));
+}
+
+}  // namespace pdem

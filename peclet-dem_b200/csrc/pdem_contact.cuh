@@ -1,0 +1,644 @@
+// Narrowphase, contact -> manifold reduction, warm-start ledger, support levels and colouring.
+//
+// Narrowphase (src/narrowphase.hpp:179-449): A's point shell (or, for a sphere, its centre with the
+// sphere radius) probes B's canonical-space SDF; plane and world-grid wall contacts per particle.
+// Analytic spheres run one thread per pair/particle; point shells run one warp per pair/particle
+// with the warp's points in shell order, the per-warp ballot prefix giving each contact its slot,
+// so contacts come out in (pair, k) / (particle, plane, k) / (particle, wall, k) order.
+#pragma once
+#include "pdem_common.cuh"
+
+namespace pdem {
+
+template <class R>
+struct NarrowP {
+  R margin, globalScale;
+  int numPlanes, numWalls;
+  int haveMat;
+};
+
+// ---------------------------------------------------------------------------------------------
+// body-body probe of point k of A against B (src/narrowphase.hpp:192-265)
+template <class R>
+struct Probe {
+  V3<R> pw, pc;
+  R prad, eff;
+};
+template <class R>
+__device__ __forceinline__ Probe<R> probeBody(const Dev<R>& d, int A, int B, int k, const ShapeDesc<R>& dA,
+                                             const ShapeDesc<R>& dB, R gs) {
+  const V3<R> pA = v3(d.posPred[A]), pB = v3(d.posPred[B]);
+  const Q4<R> qA = d.quatPred[A], qB = d.quatPred[B];
+  const R sA = d.scale[A] * gs, sB = d.scale[B] * gs;
+  V3<R> pl{0, 0, 0};
+  Probe<R> r;
+  r.prad = R(0);
+  if (dA.numPoints > 0)
+    pl = v3(d.shell[dA.shellOffset + k]);
+  else if (dA.type == SHAPE_SPHERE)
+    r.prad = dA.par[0] * sA;
+  r.pw = add(pA, rot(qA, mul(pl, sA)));
+  const V3<R> plB = invrot(qB, sub(r.pw, pB));
+  r.pc = mul(plB, R(1) / sB);
+  const R dist = sdfShape(r.pc, dB, d.sdfGrid) * sB;
+  r.eff = dist - r.prad;
+  return r;
+}
+template <class R>
+__device__ __forceinline__ void writeBodyContact(const Dev<R>& d, int slot, int A, int B, const Probe<R>& p,
+                                                 const ShapeDesc<R>& dB, const NarrowP<R>& np) {
+  const Q4<R> qB = d.quatPred[B];
+  const V3<R> pA = v3(d.posPred[A]), pB = v3(d.posPred[B]);
+  const V3<R> nl = sdfNormal(p.pc, dB, d.sdfGrid, R(1e-4));
+  const V3<R> nw = rot(qB, nl);
+  const V3<R> ps = sub(p.pw, mul(nw, p.prad));
+  const V3<R> rA = sub(ps, pA);
+  const V3<R> rB = sub(sub(ps, mul(nw, p.eff)), pB);
+  R e = R(-1), mu = R(-1);
+  if (np.haveMat) {
+    const int t = (int(d.matId[A]) * kMaxMaterials + int(d.matId[B])) * 2;
+    e = d.pairMat[t];
+    mu = d.pairMat[t + 1];
+  }
+  d.cab[slot] = make_int2(A, B);
+  d.cn[slot] = q4(nw, p.eff);
+  d.crA[slot] = q4(rA, R(0));
+  d.crB[slot] = q4(rB, e);
+  d.cbv[slot] = Q4<R>{0, 0, 0, mu};
+}
+
+// spheres (no shell): one thread per pair. MODE 0: count + max overlap; MODE 1: write
+template <class R, int MODE>
+__global__ void kNarrowSphere(Dev<R> d, int np, NarrowP<R> P, int* cnt, const int* off) {
+  const ShapeDesc<R> dA = d.shapes[0], dB = d.shapes[0];
+  GRID_STRIDE(idx, np) {
+    const int2 pr = d.pairs[idx];
+    const Probe<R> p = probeBody(d, pr.x, pr.y, 0, dA, dB, P.globalScale);
+    const bool hit = p.eff < P.margin;
+    if (MODE == 0) {
+      if (p.eff < R(0))
+        atomicMaxNonNeg(&d.ctr->maxOverlap, -p.eff);
+      cnt[idx] = hit ? 1 : 0;
+    } else if (hit) {
+      const int s = off[idx];
+      if (s < d.maxContacts)
+        writeBodyContact(d, s, pr.x, pr.y, p, dB, P);
+    }
+  }
+}
+
+// point shells: one warp per pair, lanes over shell points in order
+template <class R, int MODE>
+__global__ void kNarrowShell(Dev<R> d, int np, NarrowP<R> P, int* cnt, const int* off) {
+  const ShapeDesc<R> dA = d.shapes[0], dB = d.shapes[0];
+  const int lane = threadIdx.x & 31;
+  const long warp = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long nwarps = ((long)gridDim.x * blockDim.x) >> 5;
+  const int K = dA.numPoints > 0 ? dA.numPoints : 1;
+  for (long idx = warp; idx < np; idx += nwarps) {
+    const int2 pr = d.pairs[idx];
+    int running = MODE ? off[idx] : 0;
+    int total = 0;
+    for (int k0 = 0; k0 < K; k0 += 32) {
+      const int k = k0 + lane;
+      bool hit = false;
+      Probe<R> p;
+      if (k < K) {
+        p = probeBody(d, pr.x, pr.y, k, dA, dB, P.globalScale);
+        hit = p.eff < P.margin;
+        if (MODE == 0 && p.eff < R(0))
+          atomicMaxNonNeg(&d.ctr->maxOverlap, -p.eff);
+      }
+      const unsigned b = __ballot_sync(0xffffffffu, hit);
+      if (MODE == 1 && hit) {
+        const int s = running + __popc(b & ((1u << lane) - 1u));
+        if (s < d.maxContacts)
+          writeBodyContact(d, s, pr.x, pr.y, p, dB, P);
+      }
+      running += __popc(b);
+      total += __popc(b);
+    }
+    if (MODE == 0 && lane == 0)
+      cnt[idx] = total;
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// planes (src/narrowphase.hpp:371-449) and walls (:278-367), per real particle
+template <class R>
+struct BoundaryProbe {
+  V3<R> rA, n, pWall;
+  R dist;
+  bool hit;
+};
+
+template <class R>
+__device__ __forceinline__ BoundaryProbe<R> probePlane(const Dev<R>& d, int i, int pl, int k, const ShapeDesc<R>& sd,
+                                                      R s, R margin) {
+  const PlaneDesc<R> P = d.planes[pl];
+  const V3<R> pp{P.p[0], P.p[1], P.p[2]}, pn{P.n[0], P.n[1], P.n[2]};
+  const V3<R> pA = v3(d.posPred[i]);
+  BoundaryProbe<R> r;
+  if (sd.numPoints > 0) {
+    r.rA = rot(d.quatPred[i], mul(v3(d.shell[sd.shellOffset + k]), s));
+    const V3<R> pw = add(pA, r.rA);
+    r.dist = dot(sub(pw, pp), pn);
+  } else {
+    R bR = sd.par[0];
+    if (bR == R(0))
+      bR = R(1);
+    const R radius = bR * s;
+    r.dist = dot(sub(pA, pp), pn) - radius;
+    r.rA = mul(pn, -radius);
+  }
+  r.n = pn;
+  r.pWall = pp;
+  r.hit = r.dist < margin;
+  return r;
+}
+template <class R>
+__device__ __forceinline__ BoundaryProbe<R> probeWall(const Dev<R>& d, int i, int wi, int k, const ShapeDesc<R>& sd,
+                                                     R s, R margin, bool needNormal) {
+  const WallDesc<R>& w = d.walls[wi];
+  const V3<R> pA = v3(d.posPred[i]);
+  R bR = sd.par[0];
+  if (bR == R(0))
+    bR = R(1);
+  const R radius = bR * s;
+  BoundaryProbe<R> r;
+  V3<R> rA{0, 0, 0};
+  if (sd.numPoints > 0)
+    rA = rot(d.quatPred[i], mul(v3(d.shell[sd.shellOffset + k]), s));
+  const V3<R> pw = add(pA, rA);
+  const R sdf = sampleWall(pw, w, d.wallGrid);
+  r.dist = (sd.numPoints > 0) ? sdf : sdf - radius;
+  r.hit = r.dist < margin;
+  if (needNormal && r.hit) {
+    V3<R> n = wallGradient(pw, w, d.wallGrid, R(1e-4));
+    const R ln = vlen(n);
+    n = (ln > R(1e-9)) ? mul(n, R(1) / ln) : V3<R>{0, 1, 0};
+    r.n = n;
+    r.rA = (sd.numPoints > 0) ? rA : mul(n, -radius);
+    const V3<R> ps = add(pA, r.rA);
+    r.pWall = sub(ps, mul(n, r.dist));
+  }
+  return r;
+}
+template <class R>
+__device__ __forceinline__ void writeBoundaryContact(const Dev<R>& d, int slot, int i, const BoundaryProbe<R>& b,
+                                                     bool wall, int wi, int haveMat) {
+  d.cab[slot] = make_int2(i, -1);
+  d.cn[slot] = q4(b.n, b.dist);
+  d.crA[slot] = q4(b.rA, R(0));
+  if (!wall) {
+    d.crB[slot] = q4(b.pWall, R(-1));
+    d.cbv[slot] = Q4<R>{0, 0, 0, R(-1)};
+    return;
+  }
+  const WallDesc<R>& w = d.walls[wi];
+  const V3<R> r = sub(b.pWall, V3<R>{w.center[0], w.center[1], w.center[2]});
+  const V3<R> vW = add(V3<R>{w.linVel[0], w.linVel[1], w.linVel[2]}, cross(V3<R>{w.angVel[0], w.angVel[1], w.angVel[2]}, r));
+  R e, mu;
+  if (w.materialId >= 0 && haveMat) {
+    const int t = (int(d.matId[i]) * kMaxMaterials + w.materialId) * 2;
+    e = d.pairMat[t];
+    mu = d.pairMat[t + 1];
+  } else {
+    e = w.restitution;
+    mu = w.friction;
+  }
+  d.crB[slot] = q4(b.pWall, e);
+  d.cbv[slot] = q4(vW, mu);
+}
+
+// one warp per real particle, planes then walls, lanes over shell points (or lane 0 for a
+// sphere). MODE 0 counts (planes in cntP, walls in cntW) and records the max overlap; MODE 1 writes
+// at base + offsets.
+template <class R, int MODE>
+__global__ void kBoundary(Dev<R> d, int numReal, NarrowP<R> P, int* cntP, int* cntW, const int* offP,
+                          const int* offW, int basePlanes, int baseWalls) {
+  const ShapeDesc<R> sd = d.shapes[0];
+  const int lane = threadIdx.x & 31;
+  const long warp = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long nwarps = ((long)gridDim.x * blockDim.x) >> 5;
+  const int K = sd.numPoints > 0 ? sd.numPoints : 1;
+  for (long i = warp; i < numReal; i += nwarps) {
+    const R s = d.scale[i] * P.globalScale;
+    int run = MODE ? basePlanes + offP[i] : 0, tot = 0;
+    for (int pl = 0; pl < P.numPlanes; ++pl)
+      for (int k0 = 0; k0 < K; k0 += 32) {
+        const int k = k0 + lane;
+        BoundaryProbe<R> b;
+        b.hit = false;
+        if (k < K) {
+          b = probePlane(d, (int)i, pl, k, sd, s, P.margin);
+          if (MODE == 0 && b.dist < R(0))
+            atomicMaxNonNeg(&d.ctr->maxOverlap, -b.dist);
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, b.hit);
+        if (MODE == 1 && b.hit) {
+          const int slot = run + __popc(m & ((1u << lane) - 1u));
+          if (slot < d.maxContacts)
+            writeBoundaryContact(d, slot, (int)i, b, false, 0, 0);
+        }
+        run += __popc(m);
+        tot += __popc(m);
+      }
+    if (MODE == 0 && lane == 0)
+      cntP[i] = tot;
+    run = MODE ? baseWalls + offW[i] : 0;
+    tot = 0;
+    for (int wi = 0; wi < P.numWalls; ++wi)
+      for (int k0 = 0; k0 < K; k0 += 32) {
+        const int k = k0 + lane;
+        BoundaryProbe<R> b;
+        b.hit = false;
+        if (k < K) {
+          b = probeWall(d, (int)i, wi, k, sd, s, P.margin, MODE == 1);
+          if (MODE == 0 && b.dist < R(0))
+            atomicMaxNonNeg(&d.ctr->maxOverlap, -b.dist);
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, b.hit);
+        if (MODE == 1 && b.hit) {
+          const int slot = run + __popc(m & ((1u << lane) - 1u));
+          if (slot < d.maxContacts)
+            writeBoundaryContact(d, slot, (int)i, b, true, wi, P.haveMat);
+        }
+        run += __popc(m);
+        tot += __popc(m);
+      }
+    if (MODE == 0 && lane == 0)
+      cntW[i] = tot;
+  }
+}
+
+// =============================================================================================
+// contact -> manifold (src/contact_preprocessing.hpp:320-471)
+// =============================================================================================
+template <class R>
+__global__ void kContactKeys(Dev<R> d, int nc, u64* keys, int* vals) {
+  GRID_STRIDE(i, nc) {
+    const int2 ab = d.cab[i];
+    u64 k;
+    if (ab.y < 0)
+      k = ((u64)(unsigned)ab.x << 32) | 0xFFFFFFFFull;
+    else {
+      const unsigned u = ab.x < ab.y ? ab.x : ab.y, v = ab.x < ab.y ? ab.y : ab.x;
+      k = ((u64)u << 32) | v;
+    }
+    keys[i] = k;
+    vals[i] = (int)i;
+  }
+}
+__global__ void kSegHeads(int n, const u64* keys, int* head) {
+  GRID_STRIDE(p, n) head[p] = (p == 0 || keys[p] != keys[p - 1]) ? 1 : 0;
+}
+// segStart[s] = first sorted position of segment s (inclusive scan of heads gives s + 1)
+__global__ void kSegStarts(int n, const int* headScan, int* segStart) {
+  GRID_STRIDE(p, n) {
+    const int s = headScan[p] - 1;
+    if (p == 0 || headScan[p] != headScan[p - 1])
+      segStart[s] = (int)p;
+  }
+}
+// one thread per manifold: ordered sums over the segment's contacts (ascending contact index)
+template <class R>
+__global__ void kReduceManifolds(Dev<R> d, int nm, int nc, const int* segStart, const u64* keys, const int* perm) {
+  GRID_STRIDE(m, nm) {
+    const int b = segStart[m], e = (m + 1 < nm) ? segStart[m + 1] : nc;
+    const u64 k = keys[b];
+    const int A = (int)(k >> 32);
+    const unsigned v = (unsigned)(k & 0xFFFFFFFFull);
+    const int B = (v == 0xFFFFFFFFu) ? -1 : (int)v;
+    int npts = 0;
+    V3<R> N{0, 0, 0}, TA{0, 0, 0}, TB{0, 0, 0}, rA{0, 0, 0}, rB{0, 0, 0}, wv{0, 0, 0};
+    R es = 0, mus = 0;
+    for (int p = b; p < e; ++p) {
+      const int c = perm[p];
+      d.cSlot[c] = (int)m;
+      const Q4<R> cn = d.cn[c];
+      const R dist = cn.w;
+      if (dist > R(0))
+        continue;  // inactive contact: contributes an all-zero manifold (x + 0 = x)
+      const int2 ab = d.cab[c];
+      const bool flip = (ab.y >= 0 && ab.y < ab.x);
+      const V3<R> n = v3(cn);
+      const V3<R> na = flip ? n : neg(n);
+      const V3<R> sh{n.x * dist * R(0.5), n.y * dist * R(0.5), n.z * dist * R(0.5)};
+      const Q4<R> crA = d.crA[c], crB = d.crB[c], cbv = d.cbv[c];
+      const V3<R> ra = sub(v3(crA), sh);
+      const V3<R> rb = add(v3(crB), sh);
+      const V3<R> rc = flip ? rb : ra, ro = flip ? ra : rb;
+      npts += 1;
+      N = add(N, na);
+      TA = add(TA, cross(rc, na));
+      TB = add(TB, cross(ro, neg(na)));
+      rA = add(rA, rc);
+      rB = add(rB, ro);
+      wv = add(wv, v3(cbv));
+      es += crB.w;
+      mus += cbv.w;
+    }
+    d.mab[m] = make_int2(A, B);
+    d.mnp[m] = npts;
+    d.mN[m] = q4(N, es);
+    d.mTA[m] = q4(TA, mus);
+    d.mTB[m] = q4(TB);
+    d.mrA[m] = q4(rA);
+    d.mrB[m] = q4(rB);
+    d.mwv[m] = q4(wv);
+  }
+}
+
+// =============================================================================================
+// warm-start ledger (src/contact_preprocessing.hpp:70-192,501-538)
+// =============================================================================================
+__device__ __forceinline__ int lowerBound(const u64* keys, int n, u64 k) {
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (keys[mid] < k)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+template <class R>
+__device__ __forceinline__ u64 realPairKey(const Dev<R>& d, int2 ab) {
+  const unsigned a = (unsigned)d.realIdx[ab.x];
+  const unsigned b = ab.y >= 0 ? (unsigned)d.realIdx[ab.y] : 0xFFFFFFFFu;
+  const unsigned hi = a < b ? a : b, lo = a < b ? b : a;
+  return ((u64)hi << 32) | lo;
+}
+// gatherWarmLambda (:113-156) followed by markPersistentManifolds (:78-108): the second writes the
+// keys, so periodic-duplicate manifolds keep their real key but a zero warm start
+template <class R>
+__global__ void kGatherWarm(Dev<R> d, int nm, int prevCount) {
+  GRID_STRIDE(i, nm) {
+    const int2 ab = d.mab[i];
+    const int npts = d.mnp[i];
+    if (npts <= 0) {
+      d.pairKeys[i] = ~0ull;
+      d.persistent[i] = 0;
+      d.lambda[i] = R(0);
+      d.lambdaT[i] = Q4<R>{0, 0, 0, 0};
+      d.posImp[i] = R(0);
+      continue;
+    }
+    const u64 k = realPairKey(d, ab);
+    const int lo = lowerBound(d.prevKeys, prevCount, k);
+    const bool hit = lo < prevCount && d.prevKeys[lo] == k;
+    const bool dup = ab.y >= 0 && d.realIdx[ab.x] > d.realIdx[ab.y];
+    d.pairKeys[i] = k;
+    d.persistent[i] = hit ? 1 : 0;
+    const bool warm = hit && !dup;
+    d.lambda[i] = warm ? d.prevLambda[lo] : R(0);
+    d.lambdaT[i] = warm ? d.prevLambdaT[lo] : Q4<R>{0, 0, 0, 0};
+    d.posImp[i] = warm ? d.prevPosImp[lo] : R(0);
+  }
+}
+// commitPairKeysLambda (:160-192): keys/perm already stably sorted by key
+template <class R>
+__global__ void kCommitLedger(Dev<R> d, int nm, const u64* sortedKeys, const int* perm) {
+  GRID_STRIDE(i, nm) {
+    const int j = perm[i];
+    d.prevKeys[i] = sortedKeys[i];
+    d.prevLambda[i] = d.lambda[j];
+    d.prevLambdaT[i] = d.lambdaT[j];
+  }
+}
+// commitPosImpulse (:501-538). Per manifold: sum of l/dt over its contacts in ascending contact
+// index (the reference's scatter order); then the ledger slot of each key receives the value of the
+// LAST manifold (highest index) carrying that key, as the serial scatter leaves it.
+template <class R>
+__global__ void kPosLoad(Dev<R> d, int nm, int nc, const int* segStart, const int* cperm, R dt, R* scratch) {
+  GRID_STRIDE(m, nm) {
+    const int b = segStart[m], e = (m + 1 < nm) ? segStart[m + 1] : nc;
+    R acc = R(0);
+    for (int p = b; p < e; ++p) {
+      const R l = d.posLamC[cperm[p]];
+      if (l != R(0))
+        acc += l / dt;
+    }
+    scratch[m] = acc;
+  }
+}
+template <class R>
+__global__ void kPosLoadScatter(Dev<R> d, int nm, const int* perm, const R* scratch) {
+  GRID_STRIDE(s, nm) {
+    const u64 k = d.prevKeys[s];
+    if (k == ~0ull)
+      continue;
+    if (s > 0 && d.prevKeys[s - 1] == k)
+      continue;  // not the first of its key group
+    int e = (int)s;
+    while (e + 1 < nm && d.prevKeys[e + 1] == k)
+      ++e;
+    d.prevPosImp[s] = scratch[perm[e]];
+  }
+}
+
+// =============================================================================================
+// support levels (src/contact_preprocessing.hpp:213-253)
+// =============================================================================================
+template <class R>
+__global__ void kGroundDecay(Dev<R> d, int n, int decay) {
+  GRID_STRIDE(i, n) {
+    const int g = (int)d.grounded[i] - decay;
+    d.grounded[i] = (uint8_t)(g > 0 ? g : 0);
+  }
+}
+// Edge of the support graph: kind 0 = none, 1 = wall (dst := 255), 2 = src supports dst.
+// Directions depend only on positions, fixed for the substep's sweeps.
+template <class R>
+__global__ void kGroundEdges(Dev<R> d, int nm, V3<R> gHat, int4* edges) {
+  GRID_STRIDE(i, nm) {
+    int4 e = make_int4(0, 0, 0, 0);
+    if (d.mnp[i] > 0) {
+      const int2 ab = d.mab[i];
+      const int ra = d.realIdx[ab.x];
+      if (ab.y < 0) {
+        e = make_int4(1, ra, ra, 0);
+      } else {
+        const int rb = d.realIdx[ab.y];
+        const V3<R> dx = sub(v3(d.posPred[ab.x]), v3(d.posPred[ab.y]));
+        const R up = -(dx.x * gHat.x + dx.y * gHat.y + dx.z * gHat.z);
+        const R thr = R(0.3) * sqrt(dot(dx, dx));
+        if (up > thr)
+          e = make_int4(2, rb, ra, 0);
+        else if (up < -thr)
+          e = make_int4(2, ra, rb, 0);
+      }
+    }
+    edges[i] = e;
+  }
+}
+// Serial in-order sweeps (the reference's serial sweep reads levels updated earlier in the same
+// sweep). One warp walks the edges in windows of 32 (edges prefetched several windows ahead):
+//  fast path: every lane pushes (level_before_window[src] - 1) with an order-free max; if no
+//             source level changed inside the window, that is exactly the sequential result;
+//  exact path: otherwise each lane's source level is recomputed from the pre-window level and the
+//             pushes of EARLIER lanes whose destination is that source (fixed point over the
+//             window), and the exact pushes are applied. Fast-path pushes never exceed the exact
+//             ones (levels only grow), so applying both gives the sequential result.
+// A sweep that changes nothing ends the loop (later sweeps would repeat it unchanged).
+// Levels live in shared memory when they fit, else in a global scratch array.
+constexpr int kGroundPF = 8;
+__global__ void kGroundSweeps(int nm, int numReal, int sweeps, const int4* edges, uint8_t* grounded,
+                              int* gscratch, int useShared) {
+  extern __shared__ int slvl[];
+  int* L = useShared ? slvl : gscratch;
+  const int lane = threadIdx.x;
+  for (int i = lane; i < numReal; i += 32)
+    L[i] = grounded[i];
+  __threadfence_block();
+  __syncwarp();
+  const int nwin = (nm + 31) / 32;
+  for (int s = 0; s < sweeps; ++s) {
+    int sweepChanged = 0;
+    for (int w0 = 0; w0 < nwin; w0 += kGroundPF) {
+      int4 buf[kGroundPF];
+#pragma unroll
+      for (int q = 0; q < kGroundPF; ++q) {
+        const int ei = (w0 + q) * 32 + lane;
+        buf[q] = (ei < nm) ? edges[ei] : make_int4(0, 0, 0, 0);
+      }
+#pragma unroll
+      for (int q = 0; q < kGroundPF; ++q) {
+        if (w0 + q >= nwin)
+          break;
+        const int kind = buf[q].x, src = buf[q].y, dst = buf[q].z;
+        const int L0s = (kind == 2) ? L[src] : 0;
+        const int L0d = (kind != 0) ? L[dst] : 0;
+        int c = (kind == 1) ? 255 : (kind == 2 ? L0s - 1 : 0);
+        bool contrib = (kind == 1) || (kind == 2 && c > 0);
+        __syncwarp();
+        if (contrib && c > L0d)
+          atomicMax(&L[dst], c);
+        __threadfence_block();
+        __syncwarp();
+        const bool srcMoved = (kind == 2) && L[src] != L0s;
+        const bool dstMoved = (kind != 0) && L[dst] != L0d;
+        if (__any_sync(0xffffffffu, dstMoved))
+          sweepChanged = 1;
+        if (__any_sync(0xffffffffu, srcMoved)) {
+          for (int it = 0; it < 33; ++it) {
+            int best = L0s;
+            for (int t = 0; t < 32; ++t) {
+              const int dT = __shfl_sync(0xffffffffu, dst, t);
+              const int cT = __shfl_sync(0xffffffffu, c, t);
+              const int okT = __shfl_sync(0xffffffffu, contrib ? 1 : 0, t);
+              if (t < lane && kind == 2 && okT && dT == src && cT > best)
+                best = cT;
+            }
+            const int nc = (kind == 2) ? best - 1 : c;
+            const bool ch = nc != c;
+            c = nc;
+            contrib = (kind == 1) || (kind == 2 && c > 0);
+            if (!__any_sync(0xffffffffu, ch))
+              break;
+          }
+          if (contrib)
+            atomicMax(&L[dst], c);
+          __threadfence_block();
+          __syncwarp();
+        }
+      }
+    }
+    if (!__any_sync(0xffffffffu, sweepChanged))
+      break;
+  }
+  __syncwarp();
+  for (int i = lane; i < numReal; i += 32)
+    grounded[i] = (uint8_t)L[i];
+}
+
+// =============================================================================================
+// Jones-Plassmann colouring (src/solver_velocity.hpp:277-374, src/solver_position.hpp:155-241)
+// =============================================================================================
+// ends of edge i: manifolds use real body indices, contacts raw slots
+template <class R, bool MANIFOLD>
+__device__ __forceinline__ void colorEnds(const Dev<R>& d, int i, int& ea, int& eb) {
+  if (MANIFOLD) {
+    const int2 ab = d.mab[i];
+    ea = d.realIdx[ab.x];
+    eb = ab.y >= 0 ? d.realIdx[ab.y] : -1;
+  } else {
+    const int2 ab = d.cab[i];
+    ea = ab.x;
+    eb = ab.y;
+  }
+}
+template <class R>
+__global__ void kColorInitManifolds(Dev<R> d, int nm) {
+  GRID_STRIDE(i, nm) {
+    const int2 ab = d.mab[i];
+    if (d.mnp[i] <= 0 || (ab.y >= 0 && d.realIdx[ab.x] > d.realIdx[ab.y]))
+      d.mColor[i] = -2;
+    else
+      d.mColor[i] = -1;
+  }
+}
+__global__ void kFillInt(int* a, int n, int v) {
+  GRID_STRIDE(i, n) a[i] = v;
+}
+__global__ void kFillLL(long long* a, int n, long long v) {
+  GRID_STRIDE(i, n) a[i] = v;
+}
+__global__ void kFillU64(u64* a, int n, u64 v) {
+  GRID_STRIDE(i, n) a[i] = v;
+}
+template <class R, bool MANIFOLD>
+__global__ void kColorContend(Dev<R> d, int ne, const int* col) {
+  GRID_STRIDE(i, ne) {
+    if (col[i] != -1)
+      continue;
+    int ea, eb;
+    colorEnds<R, MANIFOLD>(d, (int)i, ea, eb);
+    const long long k = colorKey((int)i);
+    atomicMax(&d.winner[ea], k);
+    if (eb >= 0)
+      atomicMax(&d.winner[eb], k);
+  }
+}
+template <class R, bool MANIFOLD>
+__global__ void kColorCommit(Dev<R> d, int ne, int* col, int* remaining) {
+  GRID_STRIDE(i, ne) {
+    if (col[i] != -1)
+      continue;
+    int ea, eb;
+    colorEnds<R, MANIFOLD>(d, (int)i, ea, eb);
+    const long long k = colorKey((int)i);
+    if (d.winner[ea] != k || (eb >= 0 && d.winner[eb] != k)) {
+      atomicAdd(remaining, 1);
+      continue;
+    }
+    u64 forb = d.mask[ea];
+    if (eb >= 0)
+      forb |= d.mask[eb];
+    int c = 0;
+    while (c < 62 && (forb & (1ull << c)))
+      ++c;
+    col[i] = c;
+    d.mask[ea] |= 1ull << c;
+    if (eb >= 0)
+      d.mask[eb] |= 1ull << c;
+  }
+}
+__global__ void kColorStats(int ne, const int* col, int* maxColor, int* leftover) {
+  GRID_STRIDE(i, ne) {
+    atomicMax(maxColor, col[i]);
+    if (col[i] == -1)
+      atomicAdd(leftover, 1);
+  }
+}
+// colour keys for the stable colour-sorted execution order
+__global__ void kColorSortKeys(int ne, const int* col, unsigned* keys, int* vals) {
+  GRID_STRIDE(i, ne) {
+    const int c = col[i];
+    keys[i] = (c >= 0) ? (unsigned)c : 0xFFFFFFFFu;
+    vals[i] = (int)i;
+  }
+}
+}  // namespace pdem

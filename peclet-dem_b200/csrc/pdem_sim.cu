@@ -1,0 +1,1508 @@
+// Host orchestration of the B200 substep: facade setters/getters and the demStep stage sequence.
+// Each stage names the reference function (file:line) it reproduces. All device work runs on the
+// simulation's own stream; the host reads back only the counts that size the next stage (pair,
+// contact, manifold totals and colouring progress).
+#include <algorithm>
+#include <cstring>
+#include <numeric>
+
+#include <cub/cub.cuh>
+
+#include "pdem_broad.cuh"
+#include "pdem_contact.cuh"
+#include "pdem_hertz.cuh"
+#include "pdem_kernels.cuh"
+#include "pdem_shell.hpp"
+#include "pdem_sim.cuh"
+#include "pdem_solve.cuh"
+
+namespace pdem {
+
+void cudaCheck(cudaError_t e, const char* what) {
+  if (e != cudaSuccess)
+    throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
+}
+#define KCHECK(name) cudaCheck(cudaGetLastError(), name)
+
+template <class R>
+Sim<R>::Sim(int capacity) {
+  cudaCheck(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+  for (int i = 0; i < 8; ++i) {
+    hzE_[i] = R(1.0e9);
+    hzNu_[i] = R(0.25);
+  }
+  ctr_.ensure(1, false, stream_);
+  allocate(capacity, capacity * 64, capacity * 16);
+  initializeShape(SHAPE_SPHERE, R(1), R(0), R(0));
+}
+template <class R>
+Sim<R>::~Sim() {
+  if (stream_) {
+    cudaStreamSynchronize(stream_);
+    cudaStreamDestroy(stream_);
+  }
+}
+
+// src/particles.hpp:194-288
+template <class R>
+void Sim<R>::allocate(int cap, int mp, int mc) {
+  capacity_ = cap;
+  maxPairs_ = mp;
+  for (auto* b : {&pos_, &vel_, &angVel_, &invI_, &posPred_, &velPred_, &angVelPred_, &quat_, &quatPred_,
+                  &extF_, &dVel_, &dAngVel_, &dPos_})
+    b->ensure(cap, false, stream_);
+  for (auto* b : {&invMass_, &scale_, &target_, &rad_})
+    b->ensure(cap, false, stream_);
+  planeFric_.ensure(2 * (size_t)cap, false, stream_);
+  for (auto* b : {&shapeId_, &realIdx_, &counts_})
+    b->ensure(cap, false, stream_);
+  grounded_.ensure(cap, false, stream_);
+  matId_.ensure(cap, false, stream_);
+  winner_.ensure(cap, false, stream_);
+  mask_.ensure(cap, false, stream_);
+  pairs_.ensure(mp, false, stream_);
+  allocContactBuffers(mc);
+  hzXiWall_.ensure((size_t)cap * kHertzMaxWalls, false, stream_);
+  hzSnWall_.ensure((size_t)cap * kHertzMaxWalls, false, stream_);
+  hzWallCand_.ensure((size_t)cap * 2, false, stream_);
+  hzRefPos_.ensure(cap, false, stream_);
+  hzED_.ensure(8, false, stream_);
+  hzNuD_.ensure(8, false, stream_);
+  refreshDev();
+}
+template <class R>
+void Sim<R>::allocContactBuffers(int mc) {
+  maxContacts_ = mc;
+  cab_.ensure(mc, false, stream_);
+  for (auto* b : {&cn_, &crA_, &crB_, &cbv_})
+    b->ensure(mc, false, stream_);
+  for (auto* b : {&cColor_, &cSlot_, &mnp_, &mColor_})
+    b->ensure(mc, false, stream_);
+  posLamC_.ensure(mc, false, stream_);
+  mab_.ensure(mc, false, stream_);
+  for (auto* b : {&mN_, &mTA_, &mTB_, &mrA_, &mrB_, &mwv_, &lambdaT_, &prevLambdaT_, &vt0_})
+    b->ensure(mc, false, stream_);
+  pairKeys_.ensure(mc, false, stream_);
+  prevKeys_.ensure(mc, false, stream_);
+  persistent_.ensure(mc, false, stream_);
+  sideFlags_.ensure(mc, false, stream_);
+  for (auto* b : {&lambda_, &prevLambda_, &vn0_, &posImp_, &prevPosImp_})
+    b->ensure(mc, false, stream_);
+}
+// src/particles.hpp:297-327 (matId grown too; the reference keeps it at the construction size)
+template <class R>
+void Sim<R>::ensureCapacity(int nc) {
+  if (nc <= capacity_)
+    return;
+  for (auto* b : {&pos_, &vel_, &angVel_, &invI_, &posPred_, &velPred_, &angVelPred_, &quat_, &quatPred_,
+                  &extF_, &dVel_, &dAngVel_, &dPos_})
+    b->ensure(nc, true, stream_);
+  for (auto* b : {&invMass_, &scale_, &target_, &rad_})
+    b->ensure(nc, true, stream_);
+  planeFric_.ensure(2 * (size_t)nc, true, stream_);
+  for (auto* b : {&shapeId_, &realIdx_, &counts_})
+    b->ensure(nc, true, stream_);
+  grounded_.ensure(nc, true, stream_);
+  matId_.ensure(nc, true, stream_);
+  winner_.ensure(nc, true, stream_);
+  mask_.ensure(nc, true, stream_);
+  capacity_ = nc;
+  refreshDev();
+}
+// src/sim.hpp:1620-1654
+template <class R>
+void Sim<R>::ensureContactCapacity() {
+  const int perParticle = std::max(16, shellPoints_);
+  const long want = (long)capacity_ * perParticle + (long)capacity_ * std::max(1, shellPoints_) * (long)wallsHost_.size();
+  if (want > maxContacts_) {
+    allocContactBuffers((int)want);
+    prevPairCount_ = 0;
+    refreshDev();
+  }
+}
+template <class R>
+void Sim<R>::refreshDev() {
+  Dev<R>& d = d_;
+  d.cap = capacity_;
+  d.maxPairs = (int)pairs_.n;
+  d.maxContacts = maxContacts_;
+  d.pos = pos_.p, d.vel = vel_.p, d.angVel = angVel_.p, d.invI = invI_.p, d.posPred = posPred_.p;
+  d.velPred = velPred_.p, d.angVelPred = angVelPred_.p, d.quat = quat_.p, d.quatPred = quatPred_.p;
+  d.extForce = extF_.p, d.dVel = dVel_.p, d.dAngVel = dAngVel_.p, d.dPos = dPos_.p;
+  d.invMass = invMass_.p, d.scale = scale_.p, d.targetScale = target_.p, d.rad = rad_.p;
+  d.planeFric = planeFric_.p;
+  d.shapeId = shapeId_.p, d.realIdx = realIdx_.p, d.counts = counts_.p;
+  d.grounded = grounded_.p, d.matId = matId_.p, d.winner = winner_.p, d.mask = mask_.p;
+  d.pairs = pairs_.p;
+  d.cab = cab_.p, d.cn = cn_.p, d.crA = crA_.p, d.crB = crB_.p, d.cbv = cbv_.p;
+  d.cColor = cColor_.p, d.cSlot = cSlot_.p, d.posLamC = posLamC_.p;
+  d.mab = mab_.p, d.mnp = mnp_.p, d.mN = mN_.p, d.mTA = mTA_.p, d.mTB = mTB_.p, d.mrA = mrA_.p;
+  d.mrB = mrB_.p, d.mwv = mwv_.p, d.mColor = mColor_.p;
+  d.pairKeys = pairKeys_.p, d.prevKeys = prevKeys_.p, d.persistent = persistent_.p, d.sideFlags = sideFlags_.p;
+  d.lambda = lambda_.p, d.prevLambda = prevLambda_.p, d.vn0 = vn0_.p, d.posImp = posImp_.p;
+  d.prevPosImp = prevPosImp_.p, d.lambdaT = lambdaT_.p, d.prevLambdaT = prevLambdaT_.p, d.vt0 = vt0_.p;
+  d.shapes = shapeD_.p, d.shell = shellD_.p, d.sdfGrid = sdfGridD_.p, d.planes = planesD_.p;
+  d.walls = wallsD_.p, d.wallGrid = wallGridD_.p;
+  d.pairMat = pairMatHost_.empty() ? nullptr : pairMatD_.p;
+  d.hzE = hzED_.p, d.hzNu = hzNuD_.p;
+  d.ctr = ctr_.p;
+}
+template <class R>
+void Sim<R>::sync() {
+  cudaCheck(cudaStreamSynchronize(stream_), "cudaStreamSynchronize");
+}
+template <class R>
+Counters<R> Sim<R>::readCounters() {
+  Counters<R> c;
+  cudaCheck(cudaMemcpyAsync(&c, ctr_.p, sizeof c, cudaMemcpyDeviceToHost, stream_), "D2H counters");
+  sync();
+  return c;
+}
+
+// ---- CUB helpers ----
+template <class R>
+template <class T>
+void Sim<R>::sortPairs(const T* kin, T* kout, const int* vin, int* vout, int n, int endBit) {
+  if (n <= 0)
+    return;
+  size_t bytes = 0;
+  cudaCheck(cub::DeviceRadixSort::SortPairs(nullptr, bytes, kin, kout, vin, vout, n, 0, endBit, stream_), "cub sort");
+  cubTmp_.ensure(bytes, false, stream_);
+  cudaCheck(cub::DeviceRadixSort::SortPairs(cubTmp_.p, bytes, kin, kout, vin, vout, n, 0, endBit, stream_), "cub sort");
+}
+template <class R>
+template <class T>
+void Sim<R>::exclusiveSum(const T* in, T* out, int n) {
+  size_t bytes = 0;
+  cudaCheck(cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, n, stream_), "cub scan");
+  cubTmp_.ensure(bytes, false, stream_);
+  cudaCheck(cub::DeviceScan::ExclusiveSum(cubTmp_.p, bytes, in, out, n, stream_), "cub scan");
+}
+template <class R>
+template <class T>
+void Sim<R>::inclusiveSum(const T* in, T* out, int n) {
+  size_t bytes = 0;
+  cudaCheck(cub::DeviceScan::InclusiveSum(nullptr, bytes, in, out, n, stream_), "cub scan");
+  cubTmp_.ensure(bytes, false, stream_);
+  cudaCheck(cub::DeviceScan::InclusiveSum(cubTmp_.p, bytes, in, out, n, stream_), "cub scan");
+}
+static int bitsFor(long maxValue) {
+  int b = 1;
+  while (b < 64 && (1L << b) <= maxValue)
+    ++b;
+  return b;
+}
+
+// =============================================================================================
+// facade setters (src/sim.hpp:943-1424)
+// =============================================================================================
+// src/sim.hpp:949-1021
+template <class R>
+void Sim<R>::initializeShape(int type, R radius, R height, R thick) {
+  baseRadius_ = radius;
+  ShapeDesc<R> sd{};
+  std::vector<ShellPoint> sh;
+  if (type == SHAPE_HCYL) {
+    sd.par[0] = radius, sd.par[1] = height, sd.par[2] = thick, sd.par[3] = 0;
+    const float rf = (float)radius, tf = (float)thick;
+    float minDim = std::min(rf, tf);
+    if (minDim < 1e-4f)
+      minDim = rf;
+    float sp = std::min(rf * 0.3f, minDim * 0.5f);
+    if (sp < 1e-3f)
+      sp = 1e-3f;
+    sh = hollowCylinderShell(rf, (float)height, tf, sp);
+  } else if (type == SHAPE_BOX) {
+    sd.par[0] = sd.par[1] = sd.par[2] = radius;
+    const float sp = std::max((float)radius * 0.5f, 1e-3f);
+    sh = boxShell((float)radius, (float)radius, (float)radius, sp);
+  } else {
+    type = SHAPE_SPHERE;
+    sd.par[0] = radius;
+  }
+  const int n = (int)sh.size();
+  shellPoints_ = n;
+  if (n > 0) {
+    shellHost_.resize(n);
+    for (int i = 0; i < n; ++i)
+      shellHost_[i] = Q4<R>{R(sh[i].x), R(sh[i].y), R(sh[i].z), R(0)};
+  }
+  sd.type = type;
+  sd.numPoints = n;
+  sd.shellOffset = 0;
+  shape_ = sd;
+  uploadShape();
+  R ix = 1, iy = 1, iz = 1;
+  if (type == SHAPE_SPHERE) {
+    if (baseRadius_ > R(0)) {
+      const R v = R(2.5) / (baseRadius_ * baseRadius_);
+      ix = iy = iz = v;
+    }
+  } else if (type == SHAPE_HCYL) {
+    const R ro = baseRadius_;
+    R ri = baseRadius_ - thick;
+    if (ri < 0)
+      ri = 0;
+    const R tr = ro * ro + ri * ri;
+    const R Izz = R(0.5) * tr;
+    const R Ixx = (R(1.0) / R(12.0)) * (R(3.0) * tr + height * height);
+    if (Ixx > R(1e-6))
+      ix = iy = R(1.0) / Ixx;
+    if (Izz > R(1e-6))
+      iz = R(1.0) / Izz;
+  } else if (type == SHAPE_BOX) {
+    const R L = R(2.0) * baseRadius_;
+    const R I = (R(1.0) / R(6.0)) * L * L;
+    if (I > R(1e-6))
+      ix = iy = iz = R(1.0) / I;
+  }
+  defInvI_[0] = ix, defInvI_[1] = iy, defInvI_[2] = iz;
+}
+template <class R>
+void Sim<R>::uploadShape() {
+  shapeD_.ensure(1, false, stream_);
+  cudaCheck(cudaMemcpyAsync(shapeD_.p, &shape_, sizeof shape_, cudaMemcpyHostToDevice, stream_), "H2D shape");
+  const size_t ns = std::max<size_t>(1, shellHost_.size());
+  shellD_.ensure(ns, false, stream_);
+  if (!shellHost_.empty())
+    cudaCheck(cudaMemcpyAsync(shellD_.p, shellHost_.data(), shellHost_.size() * sizeof(Q4<R>),
+                              cudaMemcpyHostToDevice, stream_), "H2D shell");
+  sdfGridD_.ensure(std::max<size_t>(1, sdfGridHost_.size()), false, stream_);
+  if (!sdfGridHost_.empty())
+    cudaCheck(cudaMemcpyAsync(sdfGridD_.p, sdfGridHost_.data(), sdfGridHost_.size() * sizeof(R),
+                              cudaMemcpyHostToDevice, stream_), "H2D sdf grid");
+  sync();
+  refreshDev();
+}
+template <class R>
+void Sim<R>::setShellPoints(const std::vector<R>& p) {
+  const int n = (int)(p.size() / 3);
+  shellHost_.assign(std::max(n, 1), Q4<R>{0, 0, 0, 0});
+  for (int i = 0; i < n; ++i)
+    shellHost_[i] = Q4<R>{p[3 * i], p[3 * i + 1], p[3 * i + 2], R(0)};
+  if (n == 0)
+    shellHost_.clear();
+  shape_.numPoints = n;
+  shape_.shellOffset = 0;
+  shellPoints_ = n;
+  uploadShape();
+  ensureContactCapacity();
+}
+// src/sim.hpp:1034-1084
+template <class R>
+void Sim<R>::setSdfShape(const std::vector<R>& grid, int nx, int ny, int nz, const R* origin, const R* spacing,
+                         const std::vector<R>& shell, const R* invI, R bR) {
+  if (nx < 2 || ny < 2 || nz < 2)
+    throw std::runtime_error("setSdfShape: grid dims must be >= 2 on each axis");
+  if ((long)nx * ny * nz != (long)grid.size())
+    throw std::runtime_error("setSdfShape: grid.size() must equal nx*ny*nz");
+  const int n = (int)(shell.size() / 3);
+  if (n <= 0)
+    throw std::runtime_error("setSdfShape: empty surface point shell");
+  sdfGridHost_ = grid;
+  shellHost_.resize(n);
+  for (int i = 0; i < n; ++i)
+    shellHost_[i] = Q4<R>{shell[3 * i], shell[3 * i + 1], shell[3 * i + 2], R(0)};
+  ShapeDesc<R> sd{};
+  sd.type = SHAPE_GRID;
+  sd.par[0] = bR;
+  sd.numPoints = n;
+  sd.nx = nx, sd.ny = ny, sd.nz = nz;
+  for (int a = 0; a < 3; ++a) {
+    sd.gridOrigin[a] = origin[a];
+    sd.gridInvSpacing[a] = spacing[a] > 0 ? R(1) / spacing[a] : R(0);
+  }
+  shape_ = sd;
+  baseRadius_ = bR;
+  defInvI_[0] = invI[0], defInvI_[1] = invI[1], defInvI_[2] = invI[2];
+  shellPoints_ = n;
+  uploadShape();
+  ensureContactCapacity();
+}
+template <class R>
+void Sim<R>::setDomain(R lx, R ly, R lz, bool px, bool py, bool pz) {
+  dmin_[0] = dmin_[1] = dmin_[2] = 0;
+  dmax_[0] = dsize_[0] = lx;
+  dmax_[1] = dsize_[1] = ly;
+  dmax_[2] = dsize_[2] = lz;
+  per_[0] = px, per_[1] = py, per_[2] = pz;
+  skin_ = R(0.1) * gs_;
+}
+template <class R>
+void Sim<R>::setDomainMinMax(const R* mn, const R* mx) {
+  for (int a = 0; a < 3; ++a) {
+    dmin_[a] = mn[a];
+    dmax_[a] = mx[a];
+    dsize_[a] = mx[a] - mn[a];
+  }
+  skin_ = R(0.1) * gs_;
+}
+template <class R>
+void Sim<R>::enablePeriodicity(bool x, bool y, bool z) {
+  per_[0] = x, per_[1] = y, per_[2] = z;
+}
+template <class R>
+void Sim<R>::setStabilizationMode(const std::string& m) {
+  if (m == "off")
+    stabMode_ = 0;
+  else if (m == "onesided")
+    stabMode_ = 1;
+  else if (m == "multilevel")
+    stabMode_ = 2;
+  else if (m == "escalate")
+    stabMode_ = 3;
+  else if (m == "ordered")
+    stabMode_ = 4;
+  else
+    throw std::invalid_argument(
+        "set_stabilization_mode: expected 'off', 'onesided', 'multilevel', 'escalate' or 'ordered'");
+}
+template <class R>
+void Sim<R>::setHertzMaterial(int mat, R E, R nu) {
+  if (mat < 0 || mat >= 8)
+    throw std::invalid_argument("material id out of range");
+  hzE_[mat] = E;
+  hzNu_[mat] = nu;
+}
+template <class R>
+void Sim<R>::setMaterialIds(const int* ids, int n) {
+  const int m = std::min(numReal_, n);
+  if (m <= 0)
+    return;
+  std::vector<uint8_t> h(m);
+  for (int i = 0; i < m; ++i)
+    h[i] = (uint8_t)ids[i];
+  cudaCheck(cudaMemcpyAsync(matId_.p, h.data(), m, cudaMemcpyHostToDevice, stream_), "H2D matId");
+  sync();
+}
+// src/sim.hpp:1196-1216
+template <class R>
+void Sim<R>::setPairMaterial(int a, int b, R e, R f) {
+  if (a < 0 || b < 0 || a >= kMaxMaterials || b >= kMaxMaterials)
+    throw std::invalid_argument("material id out of range");
+  if (pairMatHost_.empty()) {
+    pairMatHost_.assign(kMaxMaterials * kMaxMaterials * 2, R(0));
+    for (int i = 0; i < kMaxMaterials * kMaxMaterials; ++i) {
+      pairMatHost_[2 * i] = eN_;
+      pairMatHost_[2 * i + 1] = mu_;
+    }
+  }
+  pairMatHost_[(a * kMaxMaterials + b) * 2] = e;
+  pairMatHost_[(a * kMaxMaterials + b) * 2 + 1] = f;
+  pairMatHost_[(b * kMaxMaterials + a) * 2] = e;
+  pairMatHost_[(b * kMaxMaterials + a) * 2 + 1] = f;
+  pairMatD_.ensure(pairMatHost_.size(), false, stream_);
+  cudaCheck(cudaMemcpyAsync(pairMatD_.p, pairMatHost_.data(), pairMatHost_.size() * sizeof(R),
+                            cudaMemcpyHostToDevice, stream_), "H2D pair table");
+  sync();
+  refreshDev();
+}
+template <class R>
+void Sim<R>::setWallMaterialId(int wid, int mat) {
+  if (wid < 0 || wid >= (int)wallsHost_.size())
+    throw std::invalid_argument("wall index out of range");
+  wallsHost_[wid].materialId = mat;
+  uploadWalls();
+}
+template <class R>
+void Sim<R>::addPlane(const R* p, const R* n) {
+  if ((int)planesHost_.size() < kMaxPlanes) {
+    PlaneDesc<R> pl;
+    for (int a = 0; a < 3; ++a) {
+      pl.p[a] = p[a];
+      pl.n[a] = n[a];
+    }
+    planesHost_.push_back(pl);
+  }
+  planesD_.ensure(kMaxPlanes, false, stream_);
+  cudaCheck(cudaMemcpyAsync(planesD_.p, planesHost_.data(), planesHost_.size() * sizeof(PlaneDesc<R>),
+                            cudaMemcpyHostToDevice, stream_), "H2D planes");
+  sync();
+  refreshDev();
+}
+// src/sim.hpp:1242-1274
+template <class R>
+int Sim<R>::addSdfWall(const std::vector<R>& grid, int nx, int ny, int nz, const R* origin, const R* spacing, R e,
+                       R f) {
+  if (nx < 2 || ny < 2 || nz < 2)
+    throw std::runtime_error("addSdfWall: grid dims must be >= 2 on each axis");
+  if ((long)nx * ny * nz != (long)grid.size())
+    throw std::runtime_error("addSdfWall: grid.size() must equal nx*ny*nz");
+  WallDesc<R> w{};
+  w.nx = nx, w.ny = ny, w.nz = nz;
+  w.gridOffset = (int)wallGridHost_.size();
+  for (int a = 0; a < 3; ++a) {
+    w.origin[a] = origin[a];
+    w.invSpacing[a] = spacing[a] > 0 ? R(1) / spacing[a] : R(0);
+  }
+  w.restitution = e;
+  w.friction = f;
+  w.materialId = -1;
+  wallsHost_.push_back(w);
+  wallGridHost_.insert(wallGridHost_.end(), grid.begin(), grid.end());
+  wallGridD_.ensure(wallGridHost_.size(), false, stream_);
+  cudaCheck(cudaMemcpyAsync(wallGridD_.p, wallGridHost_.data(), wallGridHost_.size() * sizeof(R),
+                            cudaMemcpyHostToDevice, stream_), "H2D wall grid");
+  uploadWalls();
+  if (f > wallFrictionMax_)
+    wallFrictionMax_ = f;
+  ensureContactCapacity();
+  return (int)wallsHost_.size() - 1;
+}
+template <class R>
+void Sim<R>::uploadWalls() {
+  wallsD_.ensure(std::max<size_t>(1, wallsHost_.size()), false, stream_);
+  if (!wallsHost_.empty())
+    cudaCheck(cudaMemcpyAsync(wallsD_.p, wallsHost_.data(), wallsHost_.size() * sizeof(WallDesc<R>),
+                              cudaMemcpyHostToDevice, stream_), "H2D walls");
+  sync();
+  refreshDev();
+}
+template <class R>
+void Sim<R>::setWallVelocity(int idx, const R* lin, const R* ang, const R* center) {
+  if (idx < 0 || idx >= (int)wallsHost_.size())
+    throw std::runtime_error("setWallVelocity: wall index out of range");
+  for (int a = 0; a < 3; ++a) {
+    wallsHost_[idx].linVel[a] = lin[a];
+    wallsHost_[idx].angVel[a] = ang[a];
+    wallsHost_[idx].center[a] = center[a];
+  }
+  uploadWalls();
+}
+// src/sim.hpp:1290-1330
+template <class R>
+void Sim<R>::setPositions(const R* xyz, int n) {
+  if (n > capacity_)
+    throw std::invalid_argument("set_positions: more particles than the simulation capacity");
+  numReal_ = n;
+  numParticles_ = n;
+  hzNumPairs_ = -1;
+  hzPrevCount_ = 0;
+  std::vector<Q4<R>> p(n), q(n, Q4<R>{0, 0, 0, 1}), ii(n, Q4<R>{defInvI_[0], defInvI_[1], defInvI_[2], 0}),
+      z(n, Q4<R>{0, 0, 0, 0});
+  std::vector<R> ones(n, R(1));
+  std::vector<int> zi(n, 0);
+  for (int i = 0; i < n; ++i)
+    p[i] = Q4<R>{xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], R(0)};
+  auto up = [&](void* dst, const void* src, size_t bytes) {
+    if (bytes)
+      cudaCheck(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream_), "H2D state");
+  };
+  up(pos_.p, p.data(), n * sizeof(Q4<R>));
+  up(quat_.p, q.data(), n * sizeof(Q4<R>));
+  up(invMass_.p, ones.data(), n * sizeof(R));
+  up(scale_.p, ones.data(), n * sizeof(R));
+  up(shapeId_.p, zi.data(), n * sizeof(int));
+  up(invI_.p, ii.data(), n * sizeof(Q4<R>));
+  up(vel_.p, z.data(), n * sizeof(Q4<R>));
+  up(angVel_.p, z.data(), n * sizeof(Q4<R>));
+  cudaCheck(cudaMemcpyAsync(target_.p, scale_.p, capacity_ * sizeof(R), cudaMemcpyDeviceToDevice, stream_), "D2D");
+  sync();
+}
+// field codes: 0 vel, 1 extForce, 2 quat, 3 angVel, 4 invI, 5 invMass
+template <class R>
+void Sim<R>::setRows(int field, const R* a, int n) {
+  const int m = std::min(numReal_, n);
+  if (m <= 0)
+    return;
+  if (field == 5) {
+    cudaCheck(cudaMemcpyAsync(invMass_.p, a, m * sizeof(R), cudaMemcpyHostToDevice, stream_), "H2D invMass");
+    sync();
+    return;
+  }
+  std::vector<Q4<R>> h(m);
+  const int cols = (field == 2) ? 4 : 3;
+  for (int i = 0; i < m; ++i)
+    h[i] = Q4<R>{a[cols * i], a[cols * i + 1], a[cols * i + 2], cols == 4 ? a[cols * i + 3] : R(0)};
+  Q4<R>* dst = field == 0 ? vel_.p : field == 1 ? extF_.p : field == 2 ? quat_.p : field == 3 ? angVel_.p : invI_.p;
+  cudaCheck(cudaMemcpyAsync(dst, h.data(), m * sizeof(Q4<R>), cudaMemcpyHostToDevice, stream_), "H2D rows");
+  sync();
+}
+template <class R>
+void Sim<R>::clearExternalForces() {
+  extF_.zero(stream_);
+  sync();
+}
+template <class R>
+void Sim<R>::setScales(const R* s, int n) {  // src/sim.hpp:1340-1346
+  const int m = std::min(numReal_, n);
+  if (m > 0)
+    cudaCheck(cudaMemcpyAsync(target_.p, s, m * sizeof(R), cudaMemcpyHostToDevice, stream_), "H2D scales");
+  cudaCheck(cudaMemcpyAsync(scale_.p, target_.p, capacity_ * sizeof(R), cudaMemcpyDeviceToDevice, stream_), "D2D");
+  sync();
+}
+template <class R>
+void Sim<R>::setScalesUniform(R s) {  // src/sim.hpp:1331-1337
+  if (numReal_ > 0) {
+    std::vector<R> h(numReal_, s);
+    cudaCheck(cudaMemcpyAsync(scale_.p, h.data(), numReal_ * sizeof(R), cudaMemcpyHostToDevice, stream_), "H2D");
+  }
+  cudaCheck(cudaMemcpyAsync(target_.p, scale_.p, capacity_ * sizeof(R), cudaMemcpyDeviceToDevice, stream_), "D2D");
+  sync();
+}
+template <class R>
+void Sim<R>::setGrowthParams(R rate, R nf) {  // src/sim.hpp:1416-1424
+  if (gf_ == R(-1))
+    gf_ = (nf > R(0)) ? nf : R(0.01);
+  else if (nf > R(0))
+    gf_ = nf;
+  gr_ = rate;
+  if (gf_ > R(0) && numReal_ > 0) {
+    kGrowthScales<<<gridFor(numReal_), kBlock, 0, stream_>>>(d_, numReal_, gf_);
+    KCHECK("growth");
+    sync();
+  }
+}
+// field codes: 0 pos, 1 vel, 2 quat, 3 angVel, 4 invI, 5 scale, 6 masses
+template <class R>
+void Sim<R>::getRows(int field, R* out, long cap) {
+  const int n = numReal_;
+  if (n <= 0)
+    return;
+  if (field >= 5) {
+    std::vector<R> h(n);
+    cudaCheck(cudaMemcpyAsync(h.data(), field == 5 ? scale_.p : invMass_.p, n * sizeof(R), cudaMemcpyDeviceToHost,
+                              stream_), "D2H");
+    sync();
+    for (int i = 0; i < n && i < cap; ++i)
+      out[i] = (field == 5) ? h[i] : ((h[i] > R(0)) ? R(1) / h[i] : R(0));
+    return;
+  }
+  std::vector<Q4<R>> h(n);
+  const Q4<R>* src = field == 0 ? pos_.p : field == 1 ? vel_.p : field == 2 ? quat_.p : field == 3 ? angVel_.p : invI_.p;
+  cudaCheck(cudaMemcpyAsync(h.data(), src, n * sizeof(Q4<R>), cudaMemcpyDeviceToHost, stream_), "D2H rows");
+  sync();
+  const int cols = (field == 2) ? 4 : 3;
+  for (int i = 0; i < n && (long)cols * i + cols - 1 < cap; ++i) {
+    out[cols * i] = h[i].x;
+    out[cols * i + 1] = h[i].y;
+    out[cols * i + 2] = h[i].z;
+    if (cols == 4)
+      out[cols * i + 3] = h[i].w;
+  }
+}
+
+// =============================================================================================
+// substep stages
+// =============================================================================================
+// src/periodicity.hpp:25-38
+template <class R>
+int Sim<R>::ghostCapacity(int nReal, R band) const {
+  const R sx = per_[0] ? band : R(0), sy = per_[1] ? band : R(0), sz = per_[2] ? band : R(0);
+  const double ix = (dsize_[0] - R(2) * sx > R(0)) ? (double)(dsize_[0] - R(2) * sx) : 0.0;
+  const double iy = (dsize_[1] - R(2) * sy > R(0)) ? (double)(dsize_[1] - R(2) * sy) : 0.0;
+  const double iz = (dsize_[2] - R(2) * sz > R(0)) ? (double)(dsize_[2] - R(2) * sz) : 0.0;
+  const double vt = (double)dsize_[0] * (double)dsize_[1] * (double)dsize_[2];
+  if (vt <= 0.0)
+    return nReal * 8;
+  const double gf = (vt - ix * iy * iz) / vt;
+  const double est = (gf > 0.5) ? nReal * 32.0 : nReal * gf * 4.0;
+  return nReal + (int)est + 4096;
+}
+// src/sim.hpp:61-70
+template <class R>
+R Sim<R>::maxOwnedRadius() {
+  if (numReal_ <= 0)
+    return gs_ * baseRadius_;
+  rA_.ensure(1, false, stream_);
+  rA_.zero(stream_, 1);
+  kMaxScale<<<gridFor(numReal_), kBlock, 0, stream_>>>(d_, numReal_, rA_.p);
+  KCHECK("maxScale");
+  R mx;
+  cudaCheck(cudaMemcpyAsync(&mx, rA_.p, sizeof(R), cudaMemcpyDeviceToHost, stream_), "D2H");
+  sync();
+  return mx * gs_ * baseRadius_;
+}
+// src/sim.hpp:119-145 (+ periodicity.hpp:43-94)
+template <class R>
+void Sim<R>::resetGhosts(R band) {
+  kIota<R><<<gridFor(numReal_), kBlock, 0, stream_>>>(realIdx_.p, numReal_);
+  KCHECK("iota");
+  ensureCapacity(ghostCapacity(numReal_, band));
+  numParticles_ = numReal_;
+  if ((per_[0] || per_[1] || per_[2]) && numReal_ > 0) {
+    DomainP<R> dom;
+    for (int a = 0; a < 3; ++a) {
+      dom.mn[a] = dmin_[a], dom.mx[a] = dmax_[a], dom.sz[a] = dsize_[a], dom.per[a] = per_[a];
+    }
+    iA_.ensure(numReal_ + 1, false, stream_);
+    iB_.ensure(numReal_ + 1, false, stream_);
+    iA_.zero(stream_, numReal_ + 1);
+    kGhostCount<<<gridFor(numReal_), kBlock, 0, stream_>>>(d_, numReal_, dom, band, iA_.p);
+    KCHECK("ghostCount");
+    exclusiveSum(iA_.p, iB_.p, numReal_ + 1);
+    int total = 0;
+    cudaCheck(cudaMemcpyAsync(&total, iB_.p + numReal_, sizeof(int), cudaMemcpyDeviceToHost, stream_), "D2H");
+    sync();
+    kGhostWrite<<<gridFor(numReal_), kBlock, 0, stream_>>>(d_, numReal_, dom, band, iB_.p);
+    KCHECK("ghostWrite");
+    numParticles_ = std::min(numReal_ + total, capacity_);
+  }
+}
+// broadphase over numParticles_ boxes of positions P with margin; pairs into pairs_ (cap entries)
+template <class R>
+int Sim<R>::findCollisions(R margin, int cap) {
+  const int n = numParticles_;
+  const R boxCap = std::max(std::max(dsize_[0], dsize_[1]), dsize_[2]);
+  if (n < 2 || numReal_ <= 0)
+    return 0;
+  bvhBoxes_.ensure(sizeof(Box<R>) * n, false, stream_);
+  bvhNodes_.ensure(sizeof(Box<R>) * n, false, stream_);
+  codes_.ensure(n, false, stream_);
+  codesAlt_.ensure(n, false, stream_);
+  bidx_.ensure(n, false, stream_);
+  bidxAlt_.ensure(n, false, stream_);
+  left_.ensure(n, false, stream_);
+  right_.ensure(n, false, stream_);
+  parent_.ensure(2 * n, false, stream_);
+  rope_.ensure(2 * n, false, stream_);
+  flag_.ensure(n, false, stream_);
+  bounds_.ensure(6, false, stream_);
+  qcnt_.ensure(numReal_ + 1, false, stream_);
+  qoff_.ensure(numReal_ + 1, false, stream_);
+  BvhNodes<R> bn{reinterpret_cast<Box<R>*>(bvhBoxes_.p), reinterpret_cast<Box<R>*>(bvhNodes_.p)};
+  BvhBuffers bb;
+  bb.n = n;
+  bb.codes = codes_.p, bb.codesAlt = codesAlt_.p, bb.idx = bidx_.p, bb.idxAlt = bidxAlt_.p;
+  bb.left = left_.p, bb.right = right_.p, bb.parent = parent_.p, bb.rope = rope_.p, bb.flag = flag_.p;
+  bb.bounds = bounds_.p;
+  bb.err = &ctr_.p->err;
+  const u64 init[6] = {~0ull, ~0ull, ~0ull, 0ull, 0ull, 0ull};
+  cudaCheck(cudaMemcpyAsync(bounds_.p, init, sizeof init, cudaMemcpyHostToDevice, stream_), "H2D bounds");
+  kBoxes<<<gridFor(n), kBlock, 0, stream_>>>(d_, n, margin, boxCap, bn, bb);
+  KCHECK("boxes");
+  kMorton<R><<<gridFor(n), kBlock, 0, stream_>>>(n, bn, bb);
+  KCHECK("morton");
+  sortPairs(codes_.p, codesAlt_.p, bidx_.p, bidxAlt_.p, n, 63);
+  std::swap(bb.codes, bb.codesAlt);
+  std::swap(bb.idx, bb.idxAlt);
+  cudaCheck(cudaMemsetAsync(flag_.p, 0, n * sizeof(int), stream_), "memset");
+  kKarras<<<gridFor(n - 1), kBlock, 0, stream_>>>(bb);
+  KCHECK("karras");
+  kRefit<R><<<gridFor(n), kBlock, 0, stream_>>>(bb, bn);
+  KCHECK("refit");
+  kRopes<<<gridFor(2 * n - 1), kBlock, 0, stream_>>>(bb);
+  KCHECK("ropes");
+  cudaCheck(cudaMemsetAsync(qcnt_.p, 0, (numReal_ + 1) * sizeof(int), stream_), "memset");
+  kQuery<R, 0><<<gridFor(numReal_, 128), 128, 0, stream_>>>(d_, numReal_, bb, bn, qcnt_.p, nullptr, nullptr, 0);
+  KCHECK("query count");
+  exclusiveSum(qcnt_.p, qoff_.p, numReal_ + 1);
+  int total = 0, err = 0;
+  cudaCheck(cudaMemcpyAsync(&total, qoff_.p + numReal_, sizeof(int), cudaMemcpyDeviceToHost, stream_), "D2H");
+  cudaCheck(cudaMemcpyAsync(&err, &ctr_.p->err, sizeof(int), cudaMemcpyDeviceToHost, stream_), "D2H");
+  sync();
+  if (err)
+    throw std::runtime_error("broadphase: BVH traversal exceeded its iteration bound (corrupt tree)");
+  if (total <= cap) {
+    kQuery<R, 1><<<gridFor(numReal_, 128), 128, 0, stream_>>>(d_, numReal_, bb, bn, nullptr, qoff_.p, pairs_.p, cap);
+    KCHECK("query write");
+    kSortPairLists<<<gridFor(numReal_), kBlock, 0, stream_>>>(numReal_, qoff_.p, pairs_.p, cap);
+    KCHECK("pair sort");
+  }
+  return total;
+}
+// src/sim.hpp:82-94: grow the pair buffer and re-run when the candidates exceed it
+template <class R>
+int Sim<R>::findCollisionsGrow(R margin, const Q4<R>*) {
+  int np = findCollisions(margin, (int)pairs_.n);
+  if (np > (int)pairs_.n) {
+    const int grown = np + np / 2 + 64;
+    pairs_.ensure(grown, false, stream_);
+    maxPairs_ = grown;
+    refreshDev();
+    np = findCollisions(margin, (int)pairs_.n);
+  }
+  return std::min(np, (int)pairs_.n);
+}
+template <class R>
+void Sim<R>::detectAll(R margin) {
+  const int np = findCollisionsGrow(margin, posPred_.p);
+  kResetCounters<<<1, 1, 0, stream_>>>(ctr_.p);
+  NarrowP<R> P{margin, gs_, (int)planesHost_.size(), (int)wallsHost_.size(), pairMatHost_.empty() ? 0 : 1};
+  const bool shell = shape_.numPoints > 0;
+  const int nr = numReal_;
+  iA_.ensure(std::max(np, 1) + 1, false, stream_);
+  iB_.ensure(std::max(np, 1) + 1, false, stream_);
+  iC_.ensure(nr + 1, false, stream_);
+  iD_.ensure(nr + 1, false, stream_);
+  iE_.ensure(2 * (size_t)nr + 2, false, stream_);
+  iA_.zero(stream_, np + 1);
+  iC_.zero(stream_, nr + 1);
+  iD_.zero(stream_, nr + 1);
+  int* cntW = iE_.p;
+  int* offP = iE_.p + (nr + 1);
+  // counts
+  if (np > 0) {
+    if (shell)
+      kNarrowShell<R, 0><<<gridFor((long)np * 32), kBlock, 0, stream_>>>(d_, np, P, iA_.p, nullptr);
+    else
+      kNarrowSphere<R, 0><<<gridFor(np), kBlock, 0, stream_>>>(d_, np, P, iA_.p, nullptr);
+    KCHECK("narrow count");
+  }
+  const bool boundary = nr > 0 && (P.numPlanes > 0 || P.numWalls > 0);
+  if (boundary) {
+    kBoundary<R, 0><<<gridFor((long)nr * 32), kBlock, 0, stream_>>>(d_, nr, P, iC_.p, iD_.p, nullptr, nullptr, 0, 0);
+    KCHECK("boundary count");
+  }
+  exclusiveSum(iA_.p, iB_.p, np + 1);
+  exclusiveSum(iC_.p, offP, nr + 1);
+  exclusiveSum(iD_.p, cntW, nr + 1);
+  int tot[3] = {0, 0, 0};
+  cudaCheck(cudaMemcpyAsync(&tot[0], iB_.p + np, sizeof(int), cudaMemcpyDeviceToHost, stream_), "D2H");
+  cudaCheck(cudaMemcpyAsync(&tot[1], offP + nr, sizeof(int), cudaMemcpyDeviceToHost, stream_), "D2H");
+  cudaCheck(cudaMemcpyAsync(&tot[2], cntW + nr, sizeof(int), cudaMemcpyDeviceToHost, stream_), "D2H");
+  sync();
+  if (np > 0 && tot[0] > 0) {
+    if (shell)
+      kNarrowShell<R, 1><<<gridFor((long)np * 32), kBlock, 0, stream_>>>(d_, np, P, nullptr, iB_.p);
+    else
+      kNarrowSphere<R, 1><<<gridFor(np), kBlock, 0, stream_>>>(d_, np, P, nullptr, iB_.p);
+    KCHECK("narrow write");
+  }
+  if (boundary && tot[1] + tot[2] > 0 && tot[0] < maxContacts_) {
+    kBoundary<R, 1><<<gridFor((long)nr * 32), kBlock, 0, stream_>>>(d_, nr, P, nullptr, nullptr, offP, cntW, tot[0],
+                                                                     tot[0] + tot[1]);
+    KCHECK("boundary write");
+  }
+  const long total = (long)tot[0] + tot[1] + tot[2];
+  Counters<R> c = readCounters();
+  c.pairCount = np;
+  c.contactTotal = (int)std::min<long>(total, 0x7fffffff);
+  c.contactCount = (int)std::min<long>(total, maxContacts_);
+  cudaCheck(cudaMemcpyAsync(ctr_.p, &c, sizeof c, cudaMemcpyHostToDevice, stream_), "H2D counters");
+}
+
+// src/contact_preprocessing.hpp:378-471
+template <class R>
+int Sim<R>::reduceManifolds(int nc) {
+  if (nc <= 0)
+    return 0;
+  ckeys_.ensure(nc, false, stream_);
+  ckeysS_.ensure(nc, false, stream_);
+  cpermIn_.ensure(nc, false, stream_);
+  cperm_.ensure(nc, false, stream_);
+  head_.ensure(nc, false, stream_);
+  headScan_.ensure(nc, false, stream_);
+  segStart_.ensure(nc + 1, false, stream_);
+  kContactKeys<<<gridFor(nc), kBlock, 0, stream_>>>(d_, nc, ckeys_.p, cpermIn_.p);
+  KCHECK("contact keys");
+  sortPairs(ckeys_.p, ckeysS_.p, cpermIn_.p, cperm_.p, nc, 64);
+  kSegHeads<<<gridFor(nc), kBlock, 0, stream_>>>(nc, ckeysS_.p, head_.p);
+  KCHECK("seg heads");
+  inclusiveSum(head_.p, headScan_.p, nc);
+  int nm = 0;
+  cudaCheck(cudaMemcpyAsync(&nm, headScan_.p + nc - 1, sizeof(int), cudaMemcpyDeviceToHost, stream_), "D2H");
+  sync();
+  kSegStarts<<<gridFor(nc), kBlock, 0, stream_>>>(nc, headScan_.p, segStart_.p);
+  KCHECK("seg starts");
+  kReduceManifolds<<<gridFor(nm), kBlock, 0, stream_>>>(d_, nm, nc, segStart_.p, ckeysS_.p, cperm_.p);
+  KCHECK("reduce manifolds");
+  return nm;
+}
+
+// Jones-Plassmann rounds (src/solver_velocity.hpp:277-374 / src/solver_position.hpp:155-241)
+template <class R>
+int Sim<R>::colorGraph(bool manifold, int ne, int nb, int& leftover) {
+  leftover = 0;
+  if (ne <= 0 || nb <= 0)
+    return 0;
+  int* col = manifold ? mColor_.p : cColor_.p;
+  kFillU64<<<gridFor(nb), kBlock, 0, stream_>>>(mask_.p, nb, 0ull);
+  if (manifold)
+    kColorInitManifolds<<<gridFor(ne), kBlock, 0, stream_>>>(d_, ne);
+  else
+    kFillInt<<<gridFor(ne), kBlock, 0, stream_>>>(col, ne, -1);
+  KCHECK("color init");
+  int remaining = 1, prevRem = -1;
+  const int maxRounds = nb + 2;
+  for (int round = 0; round < maxRounds && remaining > 0; ++round) {
+    kFillLL<<<gridFor(nb), kBlock, 0, stream_>>>(winner_.p, nb, -1ll);
+    if (manifold)
+      kColorContend<R, true><<<gridFor(ne), kBlock, 0, stream_>>>(d_, ne, col);
+    else
+      kColorContend<R, false><<<gridFor(ne), kBlock, 0, stream_>>>(d_, ne, col);
+    cudaCheck(cudaMemsetAsync(&ctr_.p->remaining, 0, sizeof(int), stream_), "memset");
+    if (manifold)
+      kColorCommit<R, true><<<gridFor(ne), kBlock, 0, stream_>>>(d_, ne, col, &ctr_.p->remaining);
+    else
+      kColorCommit<R, false><<<gridFor(ne), kBlock, 0, stream_>>>(d_, ne, col, &ctr_.p->remaining);
+    KCHECK("color round");
+    int rem = 0;
+    cudaCheck(cudaMemcpyAsync(&rem, &ctr_.p->remaining, sizeof(int), cudaMemcpyDeviceToHost, stream_), "D2H");
+    sync();
+    if (rem == prevRem)
+      break;
+    prevRem = rem;
+    remaining = rem;
+  }
+  const int st[2] = {std::numeric_limits<int>::min(), 0};
+  cudaCheck(cudaMemcpyAsync(&ctr_.p->maxColor, st, sizeof st, cudaMemcpyHostToDevice, stream_), "H2D");
+  kColorStats<<<gridFor(ne), kBlock, 0, stream_>>>(ne, col, &ctr_.p->maxColor, &ctr_.p->leftover);
+  KCHECK("color stats");
+  int res[2];
+  cudaCheck(cudaMemcpyAsync(res, &ctr_.p->maxColor, sizeof res, cudaMemcpyDeviceToHost, stream_), "D2H");
+  sync();
+  leftover = res[1];
+  return res[0] + 1;
+}
+// stable colour-sorted execution order: colour c occupies [off[c], off[c+1])
+template <class R>
+void Sim<R>::colorOrder(bool manifold, int ne, int ncol) {
+  DBuf<int>& order = manifold ? mOrder_ : cOrder_;
+  DBuf<int>& off = manifold ? mOff_ : cOff_;
+  order.ensure(ne, false, stream_);
+  off.ensure(std::max(ncol, 0) + 2, false, stream_);
+  uA_.ensure(ne, false, stream_);
+  uB_.ensure(ne, false, stream_);
+  iE_.ensure(ne, false, stream_);
+  kColorSortKeys<<<gridFor(ne), kBlock, 0, stream_>>>(ne, manifold ? mColor_.p : cColor_.p, uA_.p, iE_.p);
+  KCHECK("color keys");
+  sortPairs(uA_.p, uB_.p, iE_.p, order.p, ne, 32);
+  kLowerBoundOffsets<unsigned><<<gridFor(ncol + 1), kBlock, 0, stream_>>>(ne, uB_.p, ncol, off.p);
+  KCHECK("color offsets");
+}
+// per-body incidence lists in ascending source order. kind 0: manifolds x real bodies,
+// 1: contacts x real bodies, 2: contacts x raw body slots
+template <class R>
+void Sim<R>::buildIncidence(int kind, int ne, int nb) {
+  const int n2 = 2 * ne;
+  incKeys_.ensure(std::max(n2, 1), false, stream_);
+  incKeysS_.ensure(std::max(n2, 1), false, stream_);
+  incVals_.ensure(std::max(n2, 1), false, stream_);
+  incValsS_.ensure(std::max(n2, 1), false, stream_);
+  incOff_.ensure(nb + 2, false, stream_);
+  if (ne <= 0) {
+    incOff_.zero(stream_, nb + 1);
+    return;
+  }
+  if (kind == 0)
+    kIncidenceKeys<R, 0><<<gridFor(ne), kBlock, 0, stream_>>>(d_, ne, incKeys_.p, incVals_.p, nb);
+  else if (kind == 1)
+    kIncidenceKeys<R, 1><<<gridFor(ne), kBlock, 0, stream_>>>(d_, ne, incKeys_.p, incVals_.p, nb);
+  else if (kind == 2)
+    kIncidenceKeys<R, 2><<<gridFor(ne), kBlock, 0, stream_>>>(d_, ne, incKeys_.p, incVals_.p, nb);
+  else
+    kIncidenceKeys<R, 3><<<gridFor(ne), kBlock, 0, stream_>>>(d_, ne, incKeys_.p, incVals_.p, nb);
+  KCHECK("incidence keys");
+  sortPairs(incKeys_.p, incKeysS_.p, incVals_.p, incValsS_.p, n2, bitsFor(nb));
+  kLowerBoundOffsets<int><<<gridFor(nb + 1), kBlock, 0, stream_>>>(n2, incKeysS_.p, nb, incOff_.p);
+  KCHECK("incidence offsets");
+}
+
+// =============================================================================================
+// the substep: src/sim.hpp:97-488
+// =============================================================================================
+template <class R>
+void Sim<R>::step(R dt) {
+  dt_ = dt;
+  demStep();
+}
+
+template <class R>
+void Sim<R>::demStep() {
+  const int B = kBlock;
+  cudaStream_t s = stream_;
+  if (gf_ != R(-1) && gr_ != R(0)) {
+    gf_ *= std::exp(gr_ * dt_);
+    if (gf_ > R(1))
+      gf_ = R(1);
+  }
+  if (gf_ > R(0) && numReal_ > 0) {
+    kGrowthScales<<<gridFor(numReal_), B, 0, s>>>(d_, numReal_, gf_);
+    KCHECK("growth");
+  }
+  const R maxRad = maxOwnedRadius();
+  const R margin = R(0.1) * maxRad;
+  const V3<R> g{g_[0], g_[1], g_[2]};
+  if (numReal_ > 0) {
+    kPredict<<<gridFor(numReal_), B, 0, s>>>(d_, numReal_, g, dt_);
+    KCHECK("predict");
+  }
+  resetGhosts(maxRad);
+  if (numParticles_ > 0) {
+    kRadii<<<gridFor(numParticles_), B, 0, s>>>(d_, numParticles_, gs_, baseRadius_);
+    KCHECK("radii");
+  }
+  detectAll(margin);
+  Counters<R> c0 = readCounters();
+  const int nc = c0.contactCount;
+  const int nm = reduceManifolds(nc);
+  c0.manifoldCount = nm;
+  c0.velDone = c0.stabRun = c0.stabDone = c0.posDone = 0;
+  cudaCheck(cudaMemcpyAsync(ctr_.p, &c0, sizeof c0, cudaMemcpyHostToDevice, s), "H2D counters");
+
+  const bool friction = (mu_ > R(0) || wallFrictionMax_ > R(0));
+  const bool gNZ = (g_[0] != R(0) || g_[1] != R(0) || g_[2] != R(0));
+  const bool legacyFriction = friction && !(gNZ && useGS_);
+  if (legacyFriction) {
+    planeFric_.zero(s);
+    if (nc > 0)
+      kPlaneLoad<<<gridFor(nc), B, 0, s>>>(d_, nc);
+    KCHECK("plane load");
+  }
+  int velLeft = 0;
+  const int ncolV = useGS_ ? colorGraph(true, nm, numReal_, velLeft) : 0;
+  if (useGS_ && ncolV > 0)
+    colorOrder(true, nm, ncolV);
+  const bool usePGS = gNZ && useGS_;
+  const R gMag = std::sqrt(g_[0] * g_[0] + g_[1] * g_[1] + g_[2] * g_[2]);
+  const V3<R> gHat = gNZ ? V3<R>{g_[0] / gMag, g_[1] / gMag, g_[2] / gMag} : V3<R>{0, 0, 0};
+  const bool needInc = (usePGS && nm > 0) || ((velLeft > 0 || !useGS_) && nm > 0);
+  if (needInc)
+    buildIncidence(0, nm, numReal_);
+  Incidence incM{incOff_.p, incValsS_.p};
+  if (usePGS && nm > 0) {
+    kGatherWarm<<<gridFor(nm), B, 0, s>>>(d_, nm, prevPairCount_);
+    KCHECK("gather warm");
+    if (numReal_ > 0) {
+      kGroundDecay<<<gridFor(numReal_), B, 0, s>>>(d_, numReal_, 8);
+      edges_.ensure(nm, false, s);
+      kGroundEdges<<<gridFor(nm), B, 0, s>>>(d_, nm, gHat, edges_.p);
+      const bool smem = (size_t)numReal_ * sizeof(int) <= 200 * 1024;
+      if (!smem)
+        gscratch_.ensure(numReal_, false, s);
+      static bool attr = false;
+      if (!attr) {
+        cudaFuncSetAttribute(kGroundSweeps, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        attr = true;
+      }
+      kGroundSweeps<<<1, 32, smem ? numReal_ * sizeof(int) : 0, s>>>(nm, numReal_, 8, edges_.p, grounded_.p,
+                                                                     gscratch_.p, smem ? 1 : 0);
+      KCHECK("grounded");
+    }
+    sideFlags_.zero(s, nm);
+    kVn0<<<gridFor(nm), B, 0, s>>>(d_, nm, gr_);
+    kWarmApply<<<gridFor(numReal_), B, 0, s>>>(d_, numReal_, incM);
+    kWarmProject<<<gridFor(nm), B, 0, s>>>(d_, nm);
+    KCHECK("warm start");
+  } else if (usePGS) {
+    // no manifolds: the reference still decays the support levels
+    if (numReal_ > 0)
+      kGroundDecay<<<gridFor(numReal_), B, 0, s>>>(d_, numReal_, 8);
+  }
+  SolveP<R> sp{gr_, eN_, eT_, mu_, R(0), dt_, ncolV};
+  const R vRest = R(2) * dt_ * std::sqrt(g_[0] * g_[0] + g_[1] * g_[1] + g_[2] * g_[2]);
+  sp.vRest = vRest;
+  // Jacobi scratch
+  if (nm > 0 && (velLeft > 0 || !useGS_)) {
+    rA_.ensure(nm, false, s);
+    iC_.ensure(nm, false, s);
+  }
+  if (legacyFriction && nc > 0 && velIters_ > 0)
+    ;  // accumulate normal impulse runs each iteration below
+  for (int it = 0; it < velIters_; ++it) {
+    if (legacyFriction && nc > 0) {
+      // the reference accumulates every iteration, including after an adaptive stop would
+      // have ended the loop; it runs before the stop test, so gate it on the loop flag
+      kAccumNormal<<<gridFor(nc), B, 0, s>>>(d_, nc, gr_);
+      KCHECK("accum normal");
+    }
+    if (useGS_) {
+      kCtl<<<1, 1, 0, s>>>(ctr_.p, CTL_VEL_BEGIN, R(0), 0);
+      for (int col = 0; col < ncolV; ++col) {
+        if (usePGS)
+          kPGSColor<<<gridFor(nm), B, 0, s>>>(d_, mOrder_.p, mOff_.p, col, sp, 1);
+        else
+          kGSColor<<<gridFor(nm), B, 0, s>>>(d_, mOrder_.p, mOff_.p, col, sp, 1);
+      }
+      KCHECK("velocity sweep");
+      if (velLeft > 0) {
+        kJacobiImpulses<<<gridFor(nm), B, 0, s>>>(d_, nm, sp, 1, rA_.p, iC_.p, 1);
+        kJacobiGather<<<gridFor(numReal_), B, 0, s>>>(d_, numReal_, incM, rA_.p, iC_.p, 1);
+        kApplyVelAveraged<<<gridFor(numParticles_), B, 0, s>>>(d_, numParticles_, 1);
+        KCHECK("velocity jacobi fallback");
+      }
+      kCtl<<<1, 1, 0, s>>>(ctr_.p, CTL_VEL_END, usePGS ? R(0.02) * vRest : vRest, 0);
+    } else {
+      if (nm > 0) {
+        kJacobiImpulses<<<gridFor(nm), B, 0, s>>>(d_, nm, sp, 0, rA_.p, iC_.p, 0);
+        kJacobiGather<<<gridFor(numReal_), B, 0, s>>>(d_, numReal_, incM, rA_.p, iC_.p, 0);
+      }
+      kApplyVelAveraged<<<gridFor(numParticles_), B, 0, s>>>(d_, numParticles_, 0);
+      KCHECK("velocity jacobi");
+    }
+  }
+  if (usePGS) {
+    const R vRestS = R(2) * dt_ * gMag;
+    if (stabMode_ == 2 || stabMode_ == 4) {
+      throw std::runtime_error("stabilization modes 'multilevel' and 'ordered' are not supported by the B200 step");
+    }
+    kCtl<<<1, 1, 0, s>>>(ctr_.p, CTL_STAB_DECIDE, vRestS, stabMode_);
+    if (stabMode_ == 1 || stabMode_ == 3) {
+      if (stabMode_ == 1 && nm > 0)
+        kSideFlags<<<gridFor(nm), B, 0, s>>>(d_, nm, gHat, R(8) * dt_ * gMag, R(8) * dt_ * gMag);
+      SolveP<R> ss = sp;
+      ss.vRest = vRestS;
+      const int iters = stabMode_ == 1 ? 2 * velIters_ : 256;
+      for (int it = 0; it < iters; ++it) {
+        kCtl<<<1, 1, 0, s>>>(ctr_.p, CTL_STAB_BEGIN, R(0), 0);
+        for (int col = 0; col < ncolV; ++col)
+          kPGSColor<<<gridFor(nm), B, 0, s>>>(d_, mOrder_.p, mOff_.p, col, ss, 2);
+        kCtl<<<1, 1, 0, s>>>(ctr_.p, CTL_STAB_END, vRestS, 0);
+        if ((it & 15) == 15) {
+          const Counters<R> cc = readCounters();
+          if (cc.stabDone)
+            break;
+        }
+      }
+      KCHECK("stabilization");
+    }
+  }
+  if (usePGS) {  // src/contact_preprocessing.hpp:160-192
+    if (nm > 0) {
+      lkeysS_.ensure(nm, false, s);
+      lpermIn_.ensure(nm, false, s);
+      lperm_.ensure(nm, false, s);
+      kIota<R><<<gridFor(nm), B, 0, s>>>(lpermIn_.p, nm);
+      sortPairs(pairKeys_.p, lkeysS_.p, lpermIn_.p, lperm_.p, nm, 64);
+      kCommitLedger<<<gridFor(nm), B, 0, s>>>(d_, nm, lkeysS_.p, lperm_.p);
+      KCHECK("commit ledger");
+    }
+    prevPairCount_ = nm;
+  }
+  if (legacyFriction && nc > 0) {  // src/sim.hpp:423-429
+    kCountFriction<<<gridFor(nc), B, 0, s>>>(d_, nc);
+    qA_.ensure(nc, false, s);
+    qB_.ensure(nc, false, s);
+    qC_.ensure(nc, false, s);
+    iC_.ensure(nc, false, s);
+    kFrictionImpulses<<<gridFor(nc), B, 0, s>>>(d_, nc, mu_, qA_.p, qB_.p, qC_.p, iC_.p);
+    buildIncidence(1, nc, numReal_);
+    Incidence incF{incOff_.p, incValsS_.p};
+    dVel_.zero(s);
+    dAngVel_.zero(s);
+    kFrictionGather<<<gridFor(numReal_), B, 0, s>>>(d_, numReal_, incF, qA_.p, qB_.p, qC_.p, iC_.p);
+    kApplyVelocityDeltas<<<gridFor(numParticles_), B, 0, s>>>(d_, numParticles_);
+    KCHECK("legacy friction");
+  } else if (legacyFriction) {
+    dVel_.zero(s);
+    dAngVel_.zero(s);
+  }
+  if (numParticles_ > 0) {
+    kApplyVelPredictPos<<<gridFor(numParticles_), B, 0, s>>>(d_, numParticles_, dt_);
+    KCHECK("apply vel predict pos");
+  }
+  int posLeft = 0;
+  const int ncolP = useGS_ ? colorGraph(false, nc, numParticles_, posLeft) : 0;
+  if (useGS_ && ncolP > 0)
+    colorOrder(false, nc, ncolP);
+  const R posTol = R(1e-4) * baseRadius_ * gs_;
+  if (nc > 0)
+    posLamC_.zero(s, nc);
+  const bool posJacobi = (posLeft > 0 || !useGS_) && nc > 0;
+  if (posJacobi) {
+    buildIncidence(2, nc, numParticles_);
+    qA_.ensure(nc, false, s);
+    iC_.ensure(nc, false, s);
+  }
+  Incidence incP{incOff_.p, incValsS_.p};
+  for (int it = 0; it < posIters_; ++it) {
+    if (useGS_) {
+      kCtl<<<1, 1, 0, s>>>(ctr_.p, CTL_POS_BEGIN, R(0), 0);
+      for (int col = 0; col < ncolP; ++col)
+        kPosGSColor<<<gridFor(nc), B, 0, s>>>(d_, cOrder_.p, cOff_.p, col, 3);
+      if (posLeft > 0) {
+        kPosJacobiPre<<<gridFor(nc), B, 0, s>>>(d_, nc, 1, qA_.p, iC_.p, 3);
+        kPosJacobiGather<<<gridFor(numParticles_), B, 0, s>>>(d_, numParticles_, incP, qA_.p, iC_.p, 3);
+        kApplyUpdatesGated<<<gridFor(numParticles_), B, 0, s>>>(d_, numParticles_, 3);
+      }
+      kCtl<<<1, 1, 0, s>>>(ctr_.p, CTL_POS_END, posTol, 0);
+    } else {
+      if (nc > 0) {
+        kPosJacobiPre<<<gridFor(nc), B, 0, s>>>(d_, nc, 0, qA_.p, iC_.p, 0);
+        kPosJacobiGather<<<gridFor(numParticles_), B, 0, s>>>(d_, numParticles_, incP, qA_.p, iC_.p, 0);
+      }
+      kApplyUpdatesGated<<<gridFor(numParticles_), B, 0, s>>>(d_, numParticles_, 0);
+    }
+    KCHECK("position sweep");
+  }
+  if (usePGS && nm > 0) {  // src/contact_preprocessing.hpp:501-538 (scratch = vn0, as the reference)
+    kPosLoad<<<gridFor(nm), B, 0, s>>>(d_, nm, nc, segStart_.p, cperm_.p, dt_, vn0_.p);
+    kPosLoadScatter<<<gridFor(nm), B, 0, s>>>(d_, nm, lperm_.p, vn0_.p);
+    KCHECK("commit position impulse");
+  }
+  if (numReal_ > 0) {
+    DomainP<R> dom;
+    for (int a = 0; a < 3; ++a) {
+      dom.mn[a] = dmin_[a], dom.mx[a] = dmax_[a], dom.sz[a] = dsize_[a], dom.per[a] = per_[a];
+    }
+    kFinalCommit<<<gridFor(numReal_), B, 0, s>>>(d_, numReal_, dom);
+    KCHECK("final commit");
+  }
+  if (thTau_ > R(0) && dt_ > R(0) && numReal_ > 0) {  // src/integration.hpp:229-272
+    thermo_.ensure(2, false, s);
+    kThermoEnergy<<<1, 1, 0, s>>>(d_, numReal_, thermo_.p);
+    double ke[2];
+    cudaCheck(cudaMemcpyAsync(ke, thermo_.p, sizeof ke, cudaMemcpyDeviceToHost, s), "D2H");
+    sync();
+    const double ndof = 3.0 * numReal_, kB = (double)thKB_, tau = (double)thTau_, Tt = (double)thT_;
+    auto lam = [&](double kin) -> R {
+      if (ndof <= 0 || kB <= 0)
+        return R(1);
+      const double Tc = (2.0 * kin) / (ndof * kB);
+      if (Tc < 1e-6)
+        return R(1);
+      double f = 1.0 + ((double)dt_ / tau) * (Tt / Tc - 1.0);
+      if (f < 0.0)
+        f = 0.0;
+      return static_cast<R>(std::sqrt(f));
+    };
+    kThermoScale<<<gridFor(numReal_), B, 0, s>>>(d_, numReal_, lam(ke[0]), lam(ke[1]));
+    KCHECK("thermostat");
+  }
+  sync();
+}
+
+// src/sim.hpp:494-541
+template <class R>
+R Sim<R>::computeOverlaps() {
+  const R maxRad = maxOwnedRadius();
+  const R margin = R(0.1) * maxRad;
+  numParticles_ = numReal_;
+  cudaCheck(cudaMemcpyAsync(posPred_.p, pos_.p, capacity_ * sizeof(Q4<R>), cudaMemcpyDeviceToDevice, stream_), "D2D");
+  cudaCheck(cudaMemcpyAsync(quatPred_.p, quat_.p, capacity_ * sizeof(Q4<R>), cudaMemcpyDeviceToDevice, stream_), "D2D");
+  resetGhosts(maxRad);
+  if (numParticles_ > 0)
+    kRadii<<<gridFor(numParticles_), kBlock, 0, stream_>>>(d_, numParticles_, gs_, baseRadius_);
+  detectAll(margin);
+  numParticles_ = numReal_;
+  return readCounters().maxOverlap;
+}
+template <class R>
+int Sim<R>::numContacts() {
+  return readCounters().contactCount;
+}
+template <class R>
+int Sim<R>::numManifolds() {
+  return readCounters().manifoldCount;
+}
+template <class R>
+R Sim<R>::maxOverlap() {
+  return readCounters().maxOverlap;
+}
+
+// =============================================================================================
+// diagnostics
+// =============================================================================================
+template <class R>
+void Sim<R>::counts(long* out) {
+  const Counters<R> c = readCounters();
+  out[0] = c.pairCount;
+  out[1] = c.contactCount;
+  out[2] = c.manifoldCount;
+  out[3] = numParticles_;
+  out[4] = prevPairCount_;
+  out[5] = capacity_;
+  out[6] = maxContacts_;
+  out[7] = (long)pairs_.n;
+}
+template <class T>
+static std::vector<T> d2h(const T* p, long n, cudaStream_t s) {
+  std::vector<T> h(std::max(n, 0L));
+  if (n > 0) {
+    cudaCheck(cudaMemcpyAsync(h.data(), p, n * sizeof(T), cudaMemcpyDeviceToHost, s), "D2H");
+    cudaCheck(cudaStreamSynchronize(s), "sync");
+  }
+  return h;
+}
+template <class R>
+long Sim<R>::getPairs(int* out, long cap) {
+  const long n = std::min<long>(readCounters().pairCount, (long)pairs_.n);
+  const auto h = d2h(pairs_.p, n, stream_);
+  for (long i = 0; i < n && 2 * i + 1 < cap; ++i) {
+    out[2 * i] = h[i].x;
+    out[2 * i + 1] = h[i].y;
+  }
+  return n;
+}
+template <class R>
+long Sim<R>::getContacts(double* out, long cap, bool muOnly) {
+  const long n = readCounters().contactCount;
+  const auto ab = d2h(cab_.p, n, stream_);
+  const auto cn = d2h(cn_.p, n, stream_), ra = d2h(crA_.p, n, stream_), rb = d2h(crB_.p, n, stream_),
+             bv = d2h(cbv_.p, n, stream_);
+  for (long i = 0; i < n; ++i) {
+    if (muOnly) {
+      if (i < cap)
+        out[i] = bv[i].w;
+      continue;
+    }
+    if (17 * i + 16 >= cap)
+      break;
+    const double v[17] = {(double)ab[i].x, (double)ab[i].y, cn[i].x, cn[i].y, cn[i].z, ra[i].x, ra[i].y, ra[i].z,
+                          rb[i].x, rb[i].y, rb[i].z, cn[i].w, ra[i].w, bv[i].x, bv[i].y, bv[i].z, rb[i].w};
+    std::memcpy(out + 17 * i, v, sizeof v);
+  }
+  return n;
+}
+template <class R>
+long Sim<R>::getManifolds(double* out, long cap) {
+  const long n = readCounters().manifoldCount;
+  const auto ab = d2h(mab_.p, n, stream_);
+  const auto np = d2h(mnp_.p, n, stream_);
+  const auto N = d2h(mN_.p, n, stream_), TA = d2h(mTA_.p, n, stream_), TB = d2h(mTB_.p, n, stream_),
+             rA = d2h(mrA_.p, n, stream_), rB = d2h(mrB_.p, n, stream_), wv = d2h(mwv_.p, n, stream_);
+  for (long i = 0; i < n && 23 * i + 22 < cap; ++i) {
+    const double v[23] = {(double)ab[i].x, (double)ab[i].y, N[i].x,  N[i].y,  N[i].z,  TA[i].x,
+                          TA[i].y,         TA[i].z,         TB[i].x, TB[i].y, TB[i].z, rA[i].x,
+                          rA[i].y,         rA[i].z,         rB[i].x, rB[i].y, rB[i].z, (double)np[i],
+                          wv[i].x,         wv[i].y,         wv[i].z, N[i].w,  TA[i].w};
+    std::memcpy(out + 23 * i, v, sizeof v);
+  }
+  return n;
+}
+template <class R>
+long Sim<R>::getColors(bool manifold, int* out, long cap) {
+  const Counters<R> c = readCounters();
+  const long n = manifold ? c.manifoldCount : c.contactCount;
+  const auto h = d2h(manifold ? mColor_.p : cColor_.p, n, stream_);
+  for (long i = 0; i < n && i < cap; ++i)
+    out[i] = h[i];
+  return n;
+}
+template <class R>
+long Sim<R>::getLambda(double* out, long cap) {
+  const long n = readCounters().manifoldCount;
+  const auto l = d2h(lambda_.p, n, stream_);
+  const auto t = d2h(lambdaT_.p, n, stream_);
+  for (long i = 0; i < n && 4 * i + 3 < cap; ++i) {
+    out[4 * i] = l[i];
+    out[4 * i + 1] = t[i].x;
+    out[4 * i + 2] = t[i].y;
+    out[4 * i + 3] = t[i].z;
+  }
+  return n;
+}
+template <class R>
+long Sim<R>::getPairKeys(unsigned long long* out, long cap) {
+  const long n = readCounters().manifoldCount;
+  const auto h = d2h(pairKeys_.p, n, stream_);
+  for (long i = 0; i < n && i < cap; ++i)
+    out[i] = h[i];
+  return n;
+}
+template <class R>
+long Sim<R>::getLedger(unsigned long long* keys, double* vals, long cap) {
+  const long n = prevPairCount_;
+  const auto k = d2h(prevKeys_.p, n, stream_);
+  const auto l = d2h(prevLambda_.p, n, stream_);
+  const auto t = d2h(prevLambdaT_.p, n, stream_);
+  const auto p = d2h(prevPosImp_.p, n, stream_);
+  for (long i = 0; i < n && i < cap; ++i) {
+    keys[i] = k[i];
+    vals[5 * i] = l[i];
+    vals[5 * i + 1] = t[i].x;
+    vals[5 * i + 2] = t[i].y;
+    vals[5 * i + 3] = t[i].z;
+    vals[5 * i + 4] = p[i];
+  }
+  return n;
+}
+template <class R>
+long Sim<R>::getGrounded(int* out, long cap) {
+  const long n = numReal_;
+  const auto h = d2h(grounded_.p, n, stream_);
+  for (long i = 0; i < n && i < cap; ++i)
+    out[i] = h[i];
+  return n;
+}
+template <class R>
+long Sim<R>::getPosLambda(double* out, long cap) {
+  const long n = readCounters().contactCount;
+  const auto h = d2h(posLamC_.p, n, stream_);
+  for (long i = 0; i < n && i < cap; ++i)
+    out[i] = h[i];
+  return n;
+}
+// test hook: shrink (or grow) the contact capacity, as replacing the reference's contact View
+template <class R>
+void Sim<R>::setMaxContacts(int n) {
+  if ((size_t)n > cab_.n)
+    allocContactBuffers(n);
+  maxContacts_ = n;
+  refreshDev();
+}
+
+// =============================================================================================
+// Hertz-Mindlin engine: src/sim.hpp:545-750
+// =============================================================================================
+// src/sim.hpp:597-625
+template <class R>
+void Sim<R>::hertzCommitHistory() {
+  const int n = hzNumPairs_;
+  if (n <= 0) {
+    hzPrevCount_ = 0;
+    return;
+  }
+  lpermIn_.ensure(n, false, stream_);
+  lperm_.ensure(n, false, stream_);
+  kIota<R><<<gridFor(n), kBlock, 0, stream_>>>(lpermIn_.p, n);
+  sortPairs(hzKeys_.p, hzPrevKeys_.p, lpermIn_.p, lperm_.p, n, 64);
+  kHertzGatherPrev<<<gridFor(n), kBlock, 0, stream_>>>(n, lperm_.p, hzXi_.p, hzPrevXi_.p);
+  KCHECK("hertz commit history");
+  hzPrevCount_ = n;
+}
+// src/sim.hpp:545-594
+template <class R>
+void Sim<R>::hertzRebuildPairs(R skin) {
+  cudaCheck(cudaMemcpyAsync(posPred_.p, pos_.p, capacity_ * sizeof(Q4<R>), cudaMemcpyDeviceToDevice, stream_), "D2D");
+  const int np = findCollisionsGrow(skin, posPred_.p);
+  const size_t need = pairs_.n;
+  if (hzXi_.n < need) {
+    // fresh buffers, as the reference reallocates (the previous history was committed above)
+    DBuf<u64> pk;
+    DBuf<Q4<R>> px;
+    pk.ensure(need, false, stream_);
+    px.ensure(need, false, stream_);
+    if (hzPrevCount_ > 0) {
+      cudaCheck(cudaMemcpyAsync(pk.p, hzPrevKeys_.p, hzPrevCount_ * sizeof(u64), cudaMemcpyDeviceToDevice, stream_), "D2D");
+      cudaCheck(cudaMemcpyAsync(px.p, hzPrevXi_.p, hzPrevCount_ * sizeof(Q4<R>), cudaMemcpyDeviceToDevice, stream_), "D2D");
+    }
+    sync();
+    std::swap(pk.p, hzPrevKeys_.p);
+    std::swap(pk.n, hzPrevKeys_.n);
+    std::swap(px.p, hzPrevXi_.p);
+    std::swap(px.n, hzPrevXi_.n);
+    hzXi_.ensure(need, false, stream_);
+    hzSnPair_.ensure(need, false, stream_);
+    hzKeys_.ensure(need, false, stream_);
+  }
+  if (np > 0) {
+    kHertzCarry<<<gridFor(np), kBlock, 0, stream_>>>(d_, np, hzPrevCount_, hzPrevKeys_.p, hzPrevXi_.p, hzKeys_.p,
+                                                      hzXi_.p);
+    KCHECK("hertz carry");
+    hzSnPair_.zero(stream_, np);
+  }
+  hzNumPairs_ = np;
+  cudaCheck(cudaMemcpyAsync(hzRefPos_.p, pos_.p, numReal_ * sizeof(Q4<R>), cudaMemcpyDeviceToDevice, stream_), "D2D");
+  // pair incidence per body (pair order), reused until the next rebuild
+  buildIncidence(3, np, numReal_);
+}
+// src/solver_hertz.hpp:343-370
+template <class R>
+int Sim<R>::hertzWallCandidates(R skin) {
+  const int n = numReal_;
+  iC_.ensure(n + 1, false, stream_);
+  iD_.ensure(n + 1, false, stream_);
+  iC_.zero(stream_, n + 1);
+  kHertzWallCand<R, 0><<<gridFor(n), kBlock, 0, stream_>>>(d_, n, (int)wallsHost_.size(), skin, iC_.p, nullptr,
+                                                           nullptr, 0);
+  exclusiveSum(iC_.p, iD_.p, n + 1);
+  int total = 0;
+  cudaCheck(cudaMemcpyAsync(&total, iD_.p + n, sizeof(int), cudaMemcpyDeviceToHost, stream_), "D2H");
+  sync();
+  const int cap = (int)hzWallCand_.n;
+  kHertzWallCand<R, 1><<<gridFor(n), kBlock, 0, stream_>>>(d_, n, (int)wallsHost_.size(), skin, nullptr, iD_.p,
+                                                           hzWallCand_.p, cap);
+  KCHECK("hertz wall candidates");
+  hzCandOff_.ensure(n + 1, false, stream_);
+  cudaCheck(cudaMemcpyAsync(hzCandOff_.p, iD_.p, (n + 1) * sizeof(int), cudaMemcpyDeviceToDevice, stream_), "D2D");
+  return total < cap ? total : cap;
+}
+// src/sim.hpp:628-750
+template <class R>
+void Sim<R>::stepHertz(R dt, int nsteps, R skinFrac) {
+  dt_ = dt;
+  if (per_[0] || per_[1] || per_[2])
+    throw std::runtime_error("step_hertz: periodic domains not supported");
+  if (!planesHost_.empty())
+    throw std::runtime_error("step_hertz: analytic planes not supported (use an SDF wall)");
+  if ((int)wallsHost_.size() > kHertzMaxWalls)
+    throw std::runtime_error("step_hertz: too many SDF walls");
+  const int n = numReal_;
+  if (n > 0)
+    kRadii<<<gridFor(n), kBlock, 0, stream_>>>(d_, n, gs_, baseRadius_);
+  // min radius = min over scale * gs * bR: rounding is monotone, so it is minScale * gs * bR
+  R minRad = std::numeric_limits<R>::max();
+  if (n > 0) {
+    const auto sc = [&] {
+      std::vector<R> h(n);
+      cudaCheck(cudaMemcpyAsync(h.data(), rad_.p, n * sizeof(R), cudaMemcpyDeviceToHost, stream_), "D2H");
+      sync();
+      return h;
+    }();
+    for (R r : sc)
+      if (r < minRad)
+        minRad = r;
+  }
+  const R skin = skinFrac * minRad;
+  const R rebuildAt = R(0.25) * skin * skin;
+  bool rebuild = hzNumPairs_ < 0;
+  if (!rebuild)  // the incidence buffers are shared with the XPBD step: rebuild them for this call
+    buildIncidence(3, hzNumPairs_, numReal_);
+  const bool hasShapes = shape_.numPoints > 0;
+  const int nw = (int)wallsHost_.size();
+  HertzP<R> P{dt, eN_, mu_, gs_, hzContactFrac_, nw};
+  const V3<R> g{g_[0], g_[1], g_[2]};
+  for (int k = 0; k < nsteps; ++k) {
+    if (rebuild) {
+      hertzCommitHistory();
+      hertzRebuildPairs(skin);
+      if (nw > 0)
+        hzNumWallCand_ = hertzWallCandidates(skin);
+      rebuild = false;
+    }
+    const int np = hzNumPairs_;
+    qA_.ensure(std::max(np, 1), false, stream_);
+    qB_.ensure(std::max(np, 1), false, stream_);
+    qC_.ensure(std::max(np, 1), false, stream_);
+    iE_.ensure(std::max(np, 1), false, stream_);
+    if (np > 0) {
+      if (hasShapes)
+        kHertzShapePairs<<<gridFor(np), kBlock, 0, stream_>>>(d_, np, P, hzXi_.p, hzSnPair_.p, qA_.p, qB_.p, qC_.p,
+                                                               iE_.p);
+      else
+        kHertzPairs<<<gridFor(np), kBlock, 0, stream_>>>(d_, np, P, hzXi_.p, qA_.p, qB_.p, qC_.p, iE_.p);
+      KCHECK("hertz pairs");
+    }
+    const int nc = (nw > 0) ? hzNumWallCand_ : 0;
+    hzFW_.ensure(std::max(nc, 1), false, stream_);
+    hzTW_.ensure(std::max(nc, 1), false, stream_);
+    hzOnW_.ensure(std::max(nc, 1), false, stream_);
+    if (nc > 0) {
+      kHertzWalls<<<gridFor(nc), kBlock, 0, stream_>>>(d_, nc, P, hzWallCand_.p, hzXiWall_.p, hzSnWall_.p,
+                                                        hasShapes ? 1 : 0, hzFW_.p, hzTW_.p, hzOnW_.p);
+      KCHECK("hertz walls");
+    }
+    if (n > 0) {
+      kHertzGatherIntegrate<<<gridFor(n), kBlock, 0, stream_>>>(
+          d_, n, incOff_.p, incValsS_.p, qA_.p, qB_.p, qC_.p, iE_.p, nc > 0 ? hzCandOff_.p : nullptr, nc, hzFW_.p,
+          hzTW_.p, hzOnW_.p, g, dt, hasShapes ? 1 : 0);
+      KCHECK("hertz integrate");
+    }
+    if ((k & 15) == 15 || k == nsteps - 1) {
+      rA_.ensure(1, false, stream_);
+      rA_.zero(stream_, 1);
+      if (n > 0)
+        kHertzMaxDisp2<<<gridFor(n), kBlock, 0, stream_>>>(d_, n, hzRefPos_.p, rA_.p);
+      R m = 0;
+      cudaCheck(cudaMemcpyAsync(&m, rA_.p, sizeof(R), cudaMemcpyDeviceToHost, stream_), "D2H");
+      sync();
+      if (n <= 0)
+        m = std::numeric_limits<R>::lowest();
+      if (m > rebuildAt)
+        rebuild = true;
+    }
+  }
+  cudaCheck(cudaMemcpyAsync(posPred_.p, pos_.p, capacity_ * sizeof(Q4<R>), cudaMemcpyDeviceToDevice, stream_), "D2D");
+  cudaCheck(cudaMemcpyAsync(velPred_.p, vel_.p, capacity_ * sizeof(Q4<R>), cudaMemcpyDeviceToDevice, stream_), "D2D");
+  sync();
+}
+template <class R>
+long Sim<R>::getHertz(unsigned long long* keys, double* xi, long cap) {
+  const long n = std::max(hzNumPairs_, 0);
+  const auto k = d2h(hzKeys_.p, n, stream_);
+  const auto x = d2h(hzXi_.p, n, stream_);
+  for (long i = 0; i < n && i < cap; ++i) {
+    keys[i] = k[i];
+    xi[3 * i] = x[i].x;
+    xi[3 * i + 1] = x[i].y;
+    xi[3 * i + 2] = x[i].z;
+  }
+  return n;
+}
+
+template class Sim<float>;
+template class Sim<double>;
+
+}  // namespace pdem

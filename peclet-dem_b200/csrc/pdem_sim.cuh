@@ -1,0 +1,234 @@
+// Host side of the B200 substep: the Simulation facade state (src/sim.hpp:909-1670) and the step
+// orchestration (src/sim.hpp:97-488, 494-541, 628-750), owning all device memory.
+#pragma once
+#include <cmath>
+#include <cstdint>
+#include <limits>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "pdem_common.cuh"
+
+namespace pdem {
+
+struct CudaError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+void cudaCheck(cudaError_t e, const char* what);
+
+// growable device buffer (contents not preserved unless asked)
+template <class T>
+struct DBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DBuf() = default;
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+  ~DBuf() {
+    if (p)
+      cudaFree(p);
+  }
+  void ensure(size_t want, bool preserve = false, cudaStream_t s = 0) {
+    if (want <= n && p)
+      return;
+    size_t cap = want < 1 ? 1 : want;
+    T* q = nullptr;
+    cudaCheck(cudaMalloc(&q, cap * sizeof(T)), "cudaMalloc");
+    cudaCheck(cudaMemsetAsync(q, 0, cap * sizeof(T), s), "cudaMemset");
+    if (preserve && p && n)
+      cudaCheck(cudaMemcpyAsync(q, p, n * sizeof(T), cudaMemcpyDeviceToDevice, s), "cudaMemcpy");
+    if (p) {
+      cudaCheck(cudaStreamSynchronize(s), "sync");
+      cudaFree(p);
+    }
+    p = q;
+    n = cap;
+  }
+  void zero(cudaStream_t s, size_t count = 0) {
+    if (p)
+      cudaCheck(cudaMemsetAsync(p, 0, (count ? count : n) * sizeof(T), s), "cudaMemset");
+  }
+};
+
+template <class R>
+class Sim {
+ public:
+  explicit Sim(int capacity);
+  ~Sim();
+
+  // ---- facade (src/sim.hpp:943-1424) ----
+  void initializeShape(int type, R radius, R height, R thick);
+  void setShellPoints(const std::vector<R>& pts);
+  void setSdfShape(const std::vector<R>& grid, int nx, int ny, int nz, const R* origin, const R* spacing,
+                   const std::vector<R>& shell, const R* invI, R boundingRadius);
+  void setDomain(R lx, R ly, R lz, bool px, bool py, bool pz);
+  void setDomainMinMax(const R* mn, const R* mx);
+  void enablePeriodicity(bool x, bool y, bool z);
+  void setGravity(R gx, R gy, R gz) { g_[0] = gx, g_[1] = gy, g_[2] = gz; }
+  void setThermostat(R T, R tau, R kB) { thT_ = T, thTau_ = tau, thKB_ = kB; }
+  void setSolverIterations(int pos, int vel) { posIters_ = pos, velIters_ = vel; }
+  void setVelocityUseGS(bool b) { useGS_ = b; }
+  void setStabilizationMode(const std::string& m);
+  void setHertzMaterial(int mat, R E, R nu);
+  void setGlobalScale(R s) { gs_ = s, skin_ = R(0.1) * s; }
+  void setDt(R dt) { dt_ = dt; }
+  void setMaterialParams(R en, R et, R mu) { eN_ = en, eT_ = et, mu_ = mu; }
+  void setMaterialIds(const int* ids, int n);
+  void setPairMaterial(int a, int b, R e, R mu);
+  void setWallMaterialId(int wid, int mat);
+  void addPlane(const R* p, const R* n);
+  int addSdfWall(const std::vector<R>& grid, int nx, int ny, int nz, const R* origin, const R* spacing, R e,
+                 R mu);
+  void setWallVelocity(int idx, const R* lin, const R* ang, const R* center);
+  void setPositions(const R* xyz, int n);
+  void setRows(int field, const R* a, int n);  // velocities, forces, quats, angvel, invI, invMass
+  void clearExternalForces();
+  void setScales(const R* s, int n);
+  void setScalesUniform(R s);
+  void setGrowthParams(R rate, R nf);
+  R growthFactor() const { return gf_; }
+  R growthRate() const { return gr_; }
+  void getRows(int field, R* out, long cap);  // positions .. masses
+  void step(R dt);
+  void stepHertz(R dt, int substeps, R skinFrac);
+  R computeOverlaps();
+  int numParticles() const { return numReal_; }
+  int numContacts();
+  int numManifolds();
+  R maxOverlap();
+  void sync();
+
+  // ---- diagnostics (canonical order) ----
+  void counts(long* out);
+  long getPairs(int* out, long cap);
+  long getContacts(double* out, long cap, bool muOnly);
+  long getManifolds(double* out, long cap);
+  long getColors(bool manifold, int* out, long cap);
+  long getLambda(double* out, long cap);
+  long getPairKeys(unsigned long long* out, long cap);
+  long getLedger(unsigned long long* keys, double* vals, long cap);
+  long getGrounded(int* out, long cap);
+  long getPosLambda(double* out, long cap);
+  long getHertz(unsigned long long* keys, double* xi, long cap);
+  void setMaxContacts(int n);
+
+  // host-side facade state
+  int capacity_ = 0, numReal_ = 0, numParticles_ = 0, maxPairs_ = 0, maxContacts_ = 0;
+  int shellPoints_ = 0;
+  R baseRadius_ = 1, defInvI_[3] = {R(2.5), R(2.5), R(2.5)};
+  R dmin_[3] = {0, 0, 0}, dmax_[3] = {0, 0, 0}, dsize_[3] = {0, 0, 0};
+  bool per_[3] = {false, false, false};
+  R g_[3] = {0, 0, 0};
+  R dt_ = R(1e-3), gs_ = 1, gr_ = 0, gf_ = -1, thT_ = 0, thTau_ = 0, thKB_ = 1;
+  R eN_ = 0, eT_ = 0, mu_ = 0, skin_ = R(0.1), wallFrictionMax_ = 0;
+  int posIters_ = 10, velIters_ = 0, stabMode_ = 1;
+  bool useGS_ = true;
+  int prevPairCount_ = 0;
+  ShapeDesc<R> shape_{};
+  std::vector<Q4<R>> shellHost_;
+  std::vector<R> sdfGridHost_;
+  std::vector<PlaneDesc<R>> planesHost_;
+  std::vector<WallDesc<R>> wallsHost_;
+  std::vector<R> wallGridHost_;
+  std::vector<R> pairMatHost_;
+  R hzE_[8], hzNu_[8];
+  int hzNumPairs_ = -1, hzPrevCount_ = 0, hzNumWallCand_ = 0;
+  R hzContactFrac_ = R(0.5);
+
+  cudaStream_t stream_ = nullptr;
+  Dev<R> d_{};
+
+ private:
+  // device buffers
+  DBuf<Q4<R>> pos_, vel_, angVel_, invI_, posPred_, velPred_, angVelPred_, quat_, quatPred_, extF_, dVel_,
+      dAngVel_, dPos_;
+  DBuf<R> invMass_, scale_, target_, rad_, planeFric_;
+  DBuf<int> shapeId_, realIdx_, counts_;
+  DBuf<uint8_t> grounded_, matId_;
+  DBuf<long long> winner_;
+  DBuf<u64> mask_;
+  DBuf<int2> pairs_;
+  DBuf<int2> cab_;
+  DBuf<Q4<R>> cn_, crA_, crB_, cbv_;
+  DBuf<int> cColor_, cSlot_;
+  DBuf<R> posLamC_;
+  DBuf<int2> mab_;
+  DBuf<int> mnp_, mColor_;
+  DBuf<Q4<R>> mN_, mTA_, mTB_, mrA_, mrB_, mwv_;
+  DBuf<u64> pairKeys_, prevKeys_;
+  DBuf<uint8_t> persistent_, sideFlags_;
+  DBuf<R> lambda_, prevLambda_, vn0_, posImp_, prevPosImp_;
+  DBuf<Q4<R>> lambdaT_, prevLambdaT_, vt0_;
+  DBuf<ShapeDesc<R>> shapeD_;
+  DBuf<Q4<R>> shellD_;
+  DBuf<R> sdfGridD_;
+  DBuf<PlaneDesc<R>> planesD_;
+  DBuf<WallDesc<R>> wallsD_;
+  DBuf<R> wallGridD_, pairMatD_, hzED_, hzNuD_;
+  DBuf<Counters<R>> ctr_;
+  // scratch
+  DBuf<char> cubTmp_;
+  DBuf<int> iA_, iB_, iC_, iD_, iE_;
+  DBuf<u64> kA_, kB_;
+  DBuf<unsigned> uA_, uB_;
+  DBuf<R> rA_, rB2_;
+  DBuf<Q4<R>> qA_, qB_, qC_;
+  DBuf<int4> edges_;
+  DBuf<int> gscratch_;
+  DBuf<double> thermo_;
+  // broadphase scratch
+  DBuf<char> bvhBoxes_, bvhNodes_;
+  DBuf<u64> codes_, codesAlt_, bounds_;
+  DBuf<int> bidx_, bidxAlt_, left_, right_, parent_, rope_, flag_, qcnt_, qoff_;
+  // manifold reduction scratch (kept for the position-impulse commit)
+  DBuf<u64> ckeys_, ckeysS_;
+  DBuf<int> cperm_, cpermIn_, head_, headScan_, segStart_;
+  // colour orders
+  DBuf<int> mOrder_, mOff_, cOrder_, cOff_;
+  // ledger sort
+  DBuf<u64> lkeysS_;
+  DBuf<int> lperm_, lpermIn_;
+  // incidence lists
+  DBuf<int> incKeys_, incKeysS_, incVals_, incValsS_, incOff_;
+  // Hertz
+  DBuf<Q4<R>> hzXi_, hzPrevXi_, hzXiWall_, hzRefPos_;
+  DBuf<u64> hzKeys_, hzPrevKeys_;
+  DBuf<R> hzSnPair_, hzSnWall_;
+  DBuf<int> hzWallCand_, hzCandOff_, hzOnW_;
+  DBuf<Q4<R>> hzFW_, hzTW_;
+
+  void allocate(int cap, int maxPairs, int maxContacts);
+  void allocContactBuffers(int mc);
+  void ensureCapacity(int nc);
+  void ensureContactCapacity();
+  void refreshDev();
+  void uploadShape();
+  void uploadWalls();
+  int ghostCapacity(int nReal, R band) const;
+  R maxOwnedRadius();
+  void resetGhosts(R band);
+  int findCollisionsGrow(R margin, const Q4<R>* P);
+  int findCollisions(R margin, int cap);
+  void detectAll(R margin);
+  int reduceManifolds(int nc);
+  int colorGraph(bool manifold, int ne, int nb, int& leftover);
+  void colorOrder(bool manifold, int ne, int ncol);
+  void buildIncidence(int kind, int ne, int nb);
+  void demStep();
+  Counters<R> readCounters();
+  template <class T>
+  void sortPairs(const T* kin, T* kout, const int* vin, int* vout, int n, int endBit);
+  template <class T>
+  void exclusiveSum(const T* in, T* out, int n);
+  template <class T>
+  void inclusiveSum(const T* in, T* out, int n);
+  // Hertz engine
+  void hertzCommitHistory();
+  void hertzRebuildPairs(R skin);
+  int hertzWallCandidates(R skin);
+};
+
+}  // namespace pdem

@@ -1,0 +1,913 @@
+// Velocity and position solves of the substep (src/solver_velocity.hpp, src/solver_position.hpp,
+// src/solver_friction.hpp).
+//
+// Colour classes are body-disjoint, so each per-colour kernel updates velocities / positions in
+// place with no atomics (the reference's colored Gauss-Seidel). Accumulations the reference does
+// with atomics (warm-start impulses, Jacobi deltas, friction deltas) are owner-computes gathers over
+// per-body incidence lists sorted by source index — the serial reference's order. Loop control
+// (adaptive stops, the stabilization trigger) lives in device flags so the host never waits.
+#pragma once
+#include "pdem_common.cuh"
+
+namespace pdem {
+
+// incidence list entry: source index << 1 | side (0 = body A, 1 = body B)
+struct Incidence {
+  const int* off;  // [nbodies + 1]
+  const int* ent;  // entries sorted by (body, source index, side)
+};
+
+template <class R>
+struct ManifoldView {
+  int ra, rb;
+  R imA, imB;
+  V3<R> iIA, iIB;
+  Q4<R> qA, qB;
+  R invN;
+  V3<R> N, TA, TB, rAa, rBa, dc, wv;
+  R eSum, muSum;
+};
+template <class R>
+__device__ __forceinline__ ManifoldView<R> loadManifold(const Dev<R>& d, int idx) {
+  ManifoldView<R> v;
+  const int2 ab = d.mab[idx];
+  v.ra = d.realIdx[ab.x];
+  v.rb = ab.y >= 0 ? d.realIdx[ab.y] : ab.y;
+  v.imA = d.invMass[v.ra];
+  v.imB = ab.y >= 0 ? d.invMass[v.rb] : R(0);
+  v.iIA = v3(d.invI[v.ra]);
+  v.iIB = ab.y >= 0 ? v3(d.invI[v.rb]) : V3<R>{0, 0, 0};
+  v.qA = d.quat[v.ra];
+  v.qB = ab.y >= 0 ? d.quat[v.rb] : Q4<R>{0, 0, 0, 1};
+  v.invN = R(1) / static_cast<R>(d.mnp[idx]);
+  const Q4<R> N = d.mN[idx], TA = d.mTA[idx];
+  v.N = v3(N);
+  v.eSum = N.w;
+  v.TA = v3(TA);
+  v.muSum = TA.w;
+  v.TB = v3(d.mTB[idx]);
+  v.rAa = mul(v3(d.mrA[idx]), v.invN);
+  v.rBa = mul(v3(d.mrB[idx]), v.invN);
+  v.dc = (ab.y < 0) ? v.rAa : sub(v.rAa, v.rBa);
+  v.wv = v3(d.mwv[idx]);
+  return v;
+}
+
+template <class R>
+struct SolveP {
+  R growthRate, eN, eT, mu, vRest, dt;
+  int ncol;
+};
+
+// ---------------------------------------------------------------------------------------------
+// loop control
+enum CtlOp : int {
+  CTL_VEL_BEGIN = 0,   // main velocity sweep start: maxApproach = 0 unless done
+  CTL_VEL_END = 1,     // main velocity sweep end: done if maxApproach <= thr
+  CTL_STAB_DECIDE = 2, // stabilization runs iff mode != 0 && maxApproach > thr
+  CTL_STAB_BEGIN = 3,
+  CTL_STAB_END = 4,
+  CTL_POS_BEGIN = 5,   // position sweep start: maxOverlap = 0 unless done
+  CTL_POS_END = 6,     // position sweep end: done if maxOverlap < thr
+};
+template <class R>
+__global__ void kCtl(Counters<R>* c, int op, R thr, int mode) {
+  if (threadIdx.x | blockIdx.x)
+    return;
+  switch (op) {
+    case CTL_VEL_BEGIN:
+      if (!c->velDone)
+        c->maxApproach = R(0);
+      break;
+    case CTL_VEL_END:
+      if (!c->velDone && c->maxApproach <= thr)
+        c->velDone = 1;
+      break;
+    case CTL_STAB_DECIDE:
+      c->stabRun = (mode != 0 && c->maxApproach > thr) ? 1 : 0;
+      c->stabDone = c->stabRun ? 0 : 1;
+      break;
+    case CTL_STAB_BEGIN:
+      if (!c->stabDone)
+        c->maxApproach = R(0);
+      break;
+    case CTL_STAB_END:
+      if (!c->stabDone && c->maxApproach <= thr)
+        c->stabDone = 1;
+      break;
+    case CTL_POS_BEGIN:
+      if (!c->posDone)
+        c->maxOverlap = R(0);
+      break;
+    case CTL_POS_END:
+      if (!c->posDone && c->maxOverlap < thr)
+        c->posDone = 1;
+      break;
+  }
+}
+template <class R>
+__device__ __forceinline__ bool gateOpen(const Counters<R>* c, int gate) {
+  // gate: 0 always, 1 main velocity loop, 2 stabilization loop, 3 position loop
+  if (gate == 1)
+    return !c->velDone;
+  if (gate == 2)
+    return !c->stabDone;
+  if (gate == 3)
+    return !c->posDone;
+  return true;
+}
+
+// ---------------------------------------------------------------------------------------------
+// pre-solve approach velocity (src/solver_velocity.hpp:390-447)
+template <class R>
+__global__ void kVn0(Dev<R> d, int nm, R growthRate) {
+  GRID_STRIDE(idx, nm) {
+    if (d.mnp[idx] <= 0)
+      continue;
+    const int2 ab = d.mab[idx];
+    const int ra = d.realIdx[ab.x];
+    if (ab.y >= 0 && ra > d.realIdx[ab.y])
+      continue;
+    const ManifoldView<R> v = loadManifold(d, (int)idx);
+    const V3<R> vA = v3(d.velPred[ra]), wA = v3(d.angVelPred[ra]);
+    V3<R> vB{0, 0, 0}, wB{0, 0, 0};
+    if (ab.y >= 0) {
+      vB = v3(d.velPred[v.rb]);
+      wB = v3(d.angVelPred[v.rb]);
+    } else {
+      vB = mul(v.wv, v.invN);
+    }
+    const V3<R> vG = mul(v.dc, growthRate);
+    R vn = dot(vA, v.N) + dot(wA, v.TA) + dot(vB, neg(v.N)) + dot(wB, v.TB);
+    vn += dot(vG, v.N);
+    d.vn0[idx] = vn;
+    const R lenN = sqrt(dot(v.N, v.N));
+    V3<R> vt{0, 0, 0};
+    if (lenN > R(1e-9)) {
+      const V3<R> nh = mul(v.N, R(1) / lenN);
+      const V3<R> wBv = ab.y >= 0 ? v3(d.angVelPred[v.rb]) : V3<R>{0, 0, 0};
+      const V3<R> vr = sub(add(vA, cross(wA, v.rAa)), add(vB, cross(wBv, v.rBa)));
+      vt = sub(vr, mul(nh, dot(vr, nh)));
+    }
+    d.vt0[idx] = q4(vt);
+  }
+}
+
+// one-sided stabilization flags (src/solver_velocity.hpp:456-495)
+template <class R>
+__global__ void kSideFlags(Dev<R> d, int nm, V3<R> gHat, R riseThr, R approachThr) {
+  if (!d.ctr->stabRun)
+    return;
+  GRID_STRIDE(idx, nm) {
+    const uint8_t was = d.persistent[idx];
+    d.sideFlags[idx] = 0;
+    const int2 ab = d.mab[idx];
+    if (d.mnp[idx] <= 0 || ab.y < 0 || was == 0)
+      continue;
+    if (fabs(d.vn0[idx]) > approachThr)
+      continue;
+    const int ra = d.realIdx[ab.x], rb = d.realIdx[ab.y];
+    if (ra > rb)
+      continue;
+    const V3<R> dx = sub(v3(d.posPred[ab.x]), v3(d.posPred[ab.y]));
+    const R up = -(dx.x * gHat.x + dx.y * gHat.y + dx.z * gHat.z);
+    const R thr = R(0.3) * sqrt(dot(dx, dx));
+    if (up > thr && -dot(v3(d.velPred[rb]), gHat) <= riseThr && d.grounded[rb] > 0)
+      d.sideFlags[idx] = 1;
+    else if (up < -thr && -dot(v3(d.velPred[ra]), gHat) <= riseThr && d.grounded[ra] > 0)
+      d.sideFlags[idx] = 2;
+  }
+}
+
+// warm-start impulses (src/solver_velocity.hpp:498-605), gathered per real body in manifold order.
+// Per manifold the reference applies: normal on A, normal on B, tangential on A, tangential on B.
+template <class R>
+__device__ __forceinline__ bool warmParts(const Dev<R>& d, int idx, R& lam, V3<R>& lt, bool& hasT) {
+  const R p = d.lambda[idx];
+  lt = v3(d.lambdaT[idx]);
+  hasT = nonzero(lt);
+  if (p == R(0) && !hasT)
+    return false;
+  if (d.mnp[idx] <= 0)
+    return false;
+  const int2 ab = d.mab[idx];
+  if (ab.y >= 0 && d.realIdx[ab.x] > d.realIdx[ab.y])
+    return false;
+  const R invN = R(1) / static_cast<R>(d.mnp[idx]);
+  const V3<R> N = v3(d.mN[idx]);
+  const V3<R> rAa = mul(v3(d.mrA[idx]), invN), rBa = mul(v3(d.mrB[idx]), invN);
+  const V3<R> dc = (ab.y < 0) ? rAa : sub(rAa, rBa);
+  const R al = dot(N, dc);
+  const R sgn = (al > R(0)) ? R(1) : R(-1);
+  lam = -sgn * p;
+  if (hasT) {
+    const R l2 = sqrt(dot(N, N));
+    if (l2 > R(1e-9)) {
+      const V3<R> nh = mul(N, R(1) / l2);
+      lt = sub(lt, mul(nh, dot(lt, nh)));
+    }
+  }
+  return true;
+}
+// the projected tangential accumulator is written back once per manifold
+template <class R>
+__global__ void kWarmProject(Dev<R> d, int nm) {
+  GRID_STRIDE(idx, nm) {
+    R lam;
+    V3<R> lt;
+    bool hasT;
+    if (warmParts(d, (int)idx, lam, lt, hasT) && hasT)
+      d.lambdaT[idx] = q4(lt);
+  }
+}
+template <class R>
+__global__ void kWarmApply(Dev<R> d, int numReal, Incidence inc) {
+  GRID_STRIDE(b, numReal) {
+    const int s = inc.off[b], e = inc.off[b + 1];
+    if (s == e)
+      continue;
+    V3<R> v = v3(d.velPred[b]), w = v3(d.angVelPred[b]);
+    const R im = d.invMass[b];
+    const V3<R> iI = v3(d.invI[b]);
+    const Q4<R> q = d.quat[b];
+    for (int t = s; t < e; ++t) {
+      const int idx = inc.ent[t] >> 1, side = inc.ent[t] & 1;
+      const bool both = (side == 0 && t + 1 < e && (inc.ent[t + 1] >> 1) == idx);
+      R lam;
+      V3<R> lt;
+      bool hasT;
+      if (!warmParts(d, idx, lam, lt, hasT)) {
+        if (both)
+          ++t;
+        continue;
+      }
+      const V3<R> N = v3(d.mN[idx]);
+      const R invN = R(1) / static_cast<R>(d.mnp[idx]);
+      const V3<R> J = mul(N, lam);
+      // normal part(s)
+      for (int sd = side; sd <= (both ? 1 : side); ++sd) {
+        if (sd == 0) {
+          v = add(v, mul(J, im));
+          w = add(w, angResponse(q, mul(v3(d.mTA[idx]), lam), iI));
+        } else {
+          v = add(v, mul(neg(J), im));
+          w = add(w, angResponse(q, mul(v3(d.mTB[idx]), lam), iI));
+        }
+      }
+      if (hasT)
+        for (int sd = side; sd <= (both ? 1 : side); ++sd) {
+          if (sd == 0) {
+            v = add(v, mul(lt, im));
+            w = add(w, angResponse(q, cross(mul(v3(d.mrA[idx]), invN), lt), iI));
+          } else {
+            v = add(v, mul(neg(lt), im));
+            w = add(w, angResponse(q, cross(mul(v3(d.mrB[idx]), invN), mul(lt, R(-1))), iI));
+          }
+        }
+      if (both)
+        ++t;
+    }
+    d.velPred[b] = q4(v);
+    d.angVelPred[b] = q4(w);
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// projected Gauss-Seidel sweep of one colour (src/solver_velocity.hpp:641-858)
+template <class R>
+__global__ void kPGSColor(Dev<R> d, const int* order, const int* coff, int color, SolveP<R> P, int gate) {
+  if (!gateOpen(d.ctr, gate))
+    return;
+  const int b = coff[color], n = coff[color + 1] - b;
+  GRID_STRIDE(t, n) {
+    const int idx = order[b + t];
+    const ManifoldView<R> v = loadManifold(d, idx);
+    const int ra = v.ra, rb = v.rb;
+    const bool hasB = d.mab[idx].y >= 0;
+    const V3<R> vA = v3(d.velPred[ra]), wA = v3(d.angVelPred[ra]);
+    V3<R> vB{0, 0, 0}, wB{0, 0, 0};
+    R e = P.eN;
+    if (hasB) {
+      vB = v3(d.velPred[rb]);
+      wB = v3(d.angVelPred[rb]);
+    } else {
+      vB = mul(v.wv, v.invN);
+    }
+    {
+      const R ra2 = v.eSum * v.invN;
+      if (ra2 >= R(0))
+        e = ra2;
+    }
+    const R lenN = sqrt(dot(v.N, v.N));
+    if (lenN < R(1e-9))
+      continue;
+    const V3<R> vG = mul(v.dc, P.growthRate);
+    R vn = dot(vA, v.N) + dot(wA, v.TA) + dot(vB, neg(v.N)) + dot(wB, v.TB);
+    vn += dot(vG, v.N);
+    const R al = dot(v.N, v.dc);
+    const R sgn = (al > R(0)) ? R(1) : R(-1);
+    const R Nsq = dot(v.N, v.N);
+    R wAn = Nsq * v.imA + genInvMass(v.TA, v.iIA, v.qA);
+    R wBn = Nsq * v.imB + genInvMass(v.TB, v.iIB, v.qB);
+    bool applyA = true, applyB = true;
+    const uint8_t sf = d.sideFlags[idx];
+    if (sf == 1) {
+      wBn = R(0);
+      applyB = false;
+      e = R(0);
+    } else if (sf == 2) {
+      wAn = R(0);
+      applyA = false;
+      e = R(0);
+    }
+    const R wT = wAn + wBn;
+    if (wT <= R(0))
+      continue;
+    const R vn0 = d.vn0[idx];
+    const R v0 = sgn * vn0;
+    if (fabs(vn0) < P.vRest * lenN)
+      e = R(0);
+    const R target = (v0 > R(0)) ? -e * v0 : R(0);
+    const R vt = sgn * vn;
+    const R dp = (vt - target) / wT;
+    const R pOld = d.lambda[idx];
+    R pNew = pOld + dp;
+    if (pNew < R(0))
+      pNew = R(0);
+    const R dA = pNew - pOld;
+    V3<R> vA2 = vA, wA2 = wA, vB2 = vB, wB2 = wB;
+    if (dA != R(0)) {
+      d.lambda[idx] = pNew;
+      atomicMaxNonNeg(&d.ctr->maxApproach, fabs(dA) * wT / lenN);
+      const R lam = -sgn * dA;
+      const V3<R> J = mul(v.N, lam), JA = mul(v.TA, lam), JB = mul(v.TB, lam);
+      if (applyA) {
+        vA2 = add(vA2, mul(J, v.imA));
+        wA2 = add(wA2, angResponse(v.qA, JA, v.iIA));
+      }
+      if (hasB && applyB) {
+        vB2 = add(vB2, mul(neg(J), v.imB));
+        wB2 = add(wB2, angResponse(v.qB, JB, v.iIB));
+      }
+    }
+    // friction cone
+    R mu = P.mu;
+    const R fa = v.muSum * v.invN;
+    if (fa >= R(0))
+      mu = fa;
+    const V3<R> ltOld = v3(d.lambdaT[idx]);
+    const bool haveOld = nonzero(ltOld);
+    if (mu > R(0) || haveOld) {
+      const V3<R> nh = mul(v.N, R(1) / lenN);
+      const V3<R> vBf = hasB ? vB2 : mul(v.wv, v.invN);
+      const V3<R> wBf = hasB ? wB2 : V3<R>{0, 0, 0};
+      const V3<R> vr = sub(add(vA2, cross(wA2, v.rAa)), add(vBf, cross(wBf, v.rBa)));
+      const V3<R> vtv = sub(vr, mul(nh, dot(vr, nh)));
+      R beta = P.eT;
+      if (beta != R(0) && (sf != 0 || fabs(vn0) < P.vRest * lenN))
+        beta = R(0);
+      V3<R> err = vtv;
+      if (beta != R(0)) {
+        V3<R> w0 = v3(d.vt0[idx]);
+        w0 = sub(w0, mul(nh, dot(w0, nh)));
+        err = add(vtv, mul(w0, beta));
+      }
+      const R vl = sqrt(dot(err, err));
+      V3<R> ltNew = ltOld;
+      R wTt = v.imA + v.imB;
+      if (vl > R(1e-9)) {
+        const V3<R> th = mul(err, R(1) / vl);
+        const R wAt = (sf == 2) ? R(0) : v.imA + genInvMass(cross(v.rAa, th), v.iIA, v.qA);
+        const R wBt = (sf == 1 || !hasB) ? R(0) : v.imB + genInvMass(cross(v.rBa, th), v.iIB, v.qB);
+        wTt = wAt + wBt;
+        if (wTt > R(1e-9))
+          ltNew = add(ltOld, mul(th, -vl / wTt));
+      }
+      ltNew = sub(ltNew, mul(nh, dot(ltNew, nh)));
+      R nTot = fmax(d.lambda[idx], R(0)) * lenN;
+      if (fabs(vn0) < P.vRest * lenN)
+        nTot += fmax(d.posImp[idx], R(0));
+      const R bound = mu * nTot;
+      const R ll = sqrt(dot(ltNew, ltNew));
+      if (ll > bound)
+        ltNew = (bound > R(0)) ? mul(ltNew, bound / ll) : V3<R>{0, 0, 0};
+      const V3<R> dd = sub(ltNew, ltOld);
+      if (nonzero(dd)) {
+        d.lambdaT[idx] = q4(ltNew);
+        const R dl = sqrt(dot(dd, dd));
+        if (wTt > R(1e-9))
+          atomicMaxNonNeg(&d.ctr->maxApproach, dl * wTt);
+        if (applyA) {
+          vA2 = add(vA2, mul(dd, v.imA));
+          wA2 = add(wA2, angResponse(v.qA, cross(v.rAa, dd), v.iIA));
+        }
+        if (hasB && applyB) {
+          vB2 = add(vB2, mul(neg(dd), v.imB));
+          wB2 = add(wB2, angResponse(v.qB, cross(v.rBa, mul(dd, R(-1))), v.iIB));
+        }
+      }
+    }
+    d.velPred[ra] = q4(vA2);
+    d.angVelPred[ra] = q4(wA2);
+    if (hasB) {
+      d.velPred[rb] = q4(vB2);
+      d.angVelPred[rb] = q4(wB2);
+    }
+  }
+}
+
+// one-shot coloured GS of one colour, g = 0 path (src/solver_velocity.hpp:989-1137)
+template <class R>
+__global__ void kGSColor(Dev<R> d, const int* order, const int* coff, int color, SolveP<R> P, int gate) {
+  if (!gateOpen(d.ctr, gate))
+    return;
+  const int b = coff[color], n = coff[color + 1] - b;
+  GRID_STRIDE(t, n) {
+    const int idx = order[b + t];
+    const ManifoldView<R> v = loadManifold(d, idx);
+    const bool hasB = d.mab[idx].y >= 0;
+    const V3<R> vA = v3(d.velPred[v.ra]), wA = v3(d.angVelPred[v.ra]);
+    V3<R> vB{0, 0, 0}, wB{0, 0, 0};
+    if (hasB) {
+      vB = v3(d.velPred[v.rb]);
+      wB = v3(d.angVelPred[v.rb]);
+    }
+    R e = P.eN;
+    if (!hasB)
+      vB = mul(v.wv, v.invN);
+    {
+      const R ra2 = v.eSum * v.invN;
+      if (ra2 >= R(0))
+        e = ra2;
+    }
+    const R lenN = sqrt(dot(v.N, v.N));
+    if (lenN < R(1e-9))
+      continue;
+    const V3<R> vG = mul(v.dc, P.growthRate);
+    R vn = dot(vA, v.N) + dot(wA, v.TA) + dot(vB, neg(v.N)) + dot(wB, v.TB);
+    vn += dot(vG, v.N);
+    const R al = dot(v.N, v.dc);
+    if (al > R(0)) {
+      if (vn < R(0))
+        continue;
+    } else {
+      if (vn > R(0))
+        continue;
+    }
+    const R Nsq = dot(v.N, v.N);
+    const R wAn = Nsq * v.imA + genInvMass(v.TA, v.iIA, v.qA);
+    const R wBn = Nsq * v.imB + genInvMass(v.TB, v.iIB, v.qB);
+    const R wT = wAn + wBn;
+    if (wT <= R(0))
+      continue;
+    atomicMaxNonNeg(&d.ctr->maxApproach, fabs(vn) / lenN);
+    if (fabs(vn) < P.vRest * lenN)
+      e = R(0);
+    const R lam = (-e * vn - vn) / wT;
+    const V3<R> J = mul(v.N, lam), JA = mul(v.TA, lam), JB = mul(v.TB, lam);
+    d.velPred[v.ra] = q4(add(vA, mul(J, v.imA)));
+    d.angVelPred[v.ra] = q4(add(wA, angResponse(v.qA, JA, v.iIA)));
+    if (hasB) {
+      d.velPred[v.rb] = q4(add(vB, mul(neg(J), v.imB)));
+      d.angVelPred[v.rb] = q4(add(wB, angResponse(v.qB, JB, v.iIB)));
+    }
+  }
+}
+
+// Jacobi velocity solve (src/solver_velocity.hpp:38-226), gathered per real body; filt selects the
+// manifolds left uncoloured (-1) for the colouring-saturation fallback
+template <class R>
+__device__ __forceinline__ bool jacobiImpulse(const Dev<R>& d, int idx, const SolveP<R>& P, bool filt, R& lam) {
+  if (filt && d.mColor[idx] != -1)
+    return false;
+  if (d.mnp[idx] <= 0)
+    return false;
+  const int2 ab = d.mab[idx];
+  const int ra = d.realIdx[ab.x];
+  int rb = ab.y;
+  if (ab.y >= 0) {
+    rb = d.realIdx[ab.y];
+    if (ra > rb)
+      return false;
+  }
+  const ManifoldView<R> v = loadManifold(d, idx);
+  const V3<R> vA = v3(d.velPred[ra]), wA = v3(d.angVelPred[ra]);
+  V3<R> vB{0, 0, 0}, wB{0, 0, 0};
+  if (ab.y >= 0) {
+    vB = v3(d.velPred[rb]);
+    wB = v3(d.angVelPred[rb]);
+  }
+  R e = P.eN;
+  if (ab.y < 0)
+    vB = mul(v.wv, v.invN);
+  {
+    const R ra2 = v.eSum * v.invN;
+    if (ra2 >= R(0))
+      e = ra2;
+  }
+  const R lenN = sqrt(dot(v.N, v.N));
+  if (lenN < R(1e-9))
+    return false;
+  const V3<R> vG = mul(v.dc, P.growthRate);
+  R vn = dot(vA, v.N) + dot(wA, v.TA) + dot(vB, neg(v.N)) + dot(wB, v.TB);
+  vn += dot(vG, v.N);
+  const R al = dot(v.N, v.dc);
+  if (al > R(0)) {
+    if (vn < R(0))
+      return false;
+  } else {
+    if (vn > R(0))
+      return false;
+  }
+  const R Nsq = dot(v.N, v.N);
+  const R wT = (Nsq * v.imA + genInvMass(v.TA, v.iIA, v.qA)) + (Nsq * v.imB + genInvMass(v.TB, v.iIB, v.qB));
+  if (wT <= R(0))
+    return false;
+  if (fabs(vn) < P.vRest * lenN)
+    e = R(0);
+  lam = (-e * vn - vn) / wT;
+  return true;
+}
+// each manifold's impulse is computed once (pre-pass, reads the velocities before any delta)
+template <class R>
+__global__ void kJacobiImpulses(Dev<R> d, int nm, SolveP<R> P, int filt, R* lamOut, int* okOut, int gate) {
+  if (!gateOpen(d.ctr, gate))
+    return;
+  GRID_STRIDE(idx, nm) {
+    R lam = R(0);
+    okOut[idx] = jacobiImpulse(d, (int)idx, P, filt != 0, lam) ? 1 : 0;
+    lamOut[idx] = lam;
+  }
+}
+template <class R>
+__global__ void kJacobiGather(Dev<R> d, int numReal, Incidence inc, const R* lam, const int* ok, int gate) {
+  if (!gateOpen(d.ctr, gate))
+    return;
+  GRID_STRIDE(b, numReal) {
+    const int s = inc.off[b], e = inc.off[b + 1];
+    if (s == e)
+      continue;
+    V3<R> dv = v3(d.dVel[b]), dw = v3(d.dAngVel[b]);
+    int cnt = d.counts[b];
+    const R im = d.invMass[b];
+    const V3<R> iI = v3(d.invI[b]);
+    const Q4<R> q = d.quat[b];
+    for (int t = s; t < e; ++t) {
+      const int idx = inc.ent[t] >> 1, side = inc.ent[t] & 1;
+      if (!ok[idx])
+        continue;
+      const R l = lam[idx];
+      const V3<R> J = mul(v3(d.mN[idx]), l);
+      if (side == 0) {
+        dv = add(dv, mul(J, im));
+        dw = add(dw, angResponse(q, mul(v3(d.mTA[idx]), l), iI));
+      } else {
+        dv = add(dv, mul(neg(J), im));
+        dw = add(dw, angResponse(q, mul(v3(d.mTB[idx]), l), iI));
+      }
+      cnt += 1;
+    }
+    d.dVel[b] = q4(dv);
+    d.dAngVel[b] = q4(dw);
+    d.counts[b] = cnt;
+  }
+}
+// src/solver_velocity.hpp:234-255
+template <class R>
+__global__ void kApplyVelAveraged(Dev<R> d, int n, int gate) {
+  if (!gateOpen(d.ctr, gate))
+    return;
+  GRID_STRIDE(i, n) {
+    const int c = d.counts[i];
+    if (c <= 0)
+      continue;
+    const R f = fmin(R(1), R(2) / static_cast<R>(c));
+    d.velPred[i] = q4(add(v3(d.velPred[i]), mul(v3(d.dVel[i]), f)));
+    d.angVelPred[i] = q4(add(v3(d.angVelPred[i]), mul(v3(d.dAngVel[i]), f)));
+    d.dVel[i] = Q4<R>{0, 0, 0, 0};
+    d.dAngVel[i] = Q4<R>{0, 0, 0, 0};
+    d.counts[i] = 0;
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// legacy friction cluster (src/solver_friction.hpp)
+template <class R>
+__global__ void kPlaneLoad(Dev<R> d, int nc) {
+  GRID_STRIDE(idx, nc) {
+    const int2 ab = d.cab[idx];
+    if (ab.y >= 0)
+      continue;
+    const int A = ab.x;
+    const R im = d.invMass[A];
+    if (im <= R(0))
+      continue;
+    const V3<R> rA = v3(d.crA[idx]), n = v3(d.cn[idx]), bv = v3(d.cbv[idx]);
+    const V3<R> vAc = add(v3(d.velPred[A]), cross(v3(d.angVelPred[A]), rA));
+    const R ap = -dot(sub(vAc, bv), n);
+    if (ap <= R(0))
+      continue;
+    const R wn = computeW(rA, n, im, v3(d.invI[A]));
+    d.crA[idx].w = (wn > R(1e-6)) ? ap / wn : R(0);
+    atomicMaxNonNeg(&d.planeFric[2 * A], ap / im);
+  }
+}
+template <class R>
+__global__ void kAccumNormal(Dev<R> d, int nc, R growthRate) {
+  GRID_STRIDE(idx, nc) {
+    const int2 ab = d.cab[idx];
+    const V3<R> rA = v3(d.crA[idx]), rB = v3(d.crB[idx]), n = v3(d.cn[idx]);
+    if (ab.y < 0) {
+      const int A = ab.x;
+      const R im = d.invMass[A];
+      if (im <= R(0))
+        continue;
+      const V3<R> vAc = add(v3(d.velPred[A]), cross(v3(d.angVelPred[A]), rA));
+      const R ap = -dot(sub(vAc, v3(d.cbv[idx])), n);
+      if (ap <= R(0))
+        continue;
+      const R wn = computeW(rA, n, im, v3(d.invI[A]));
+      if (wn > R(1e-6))
+        d.crA[idx].w += ap / wn;
+      continue;
+    }
+    const int ra = d.realIdx[ab.x], rb = d.realIdx[ab.y];
+    if (ra > rb)
+      continue;
+    const R imA = d.invMass[ra], imB = d.invMass[rb];
+    const V3<R> vAc = add(v3(d.velPred[ra]), cross(v3(d.angVelPred[ra]), rA));
+    const V3<R> vBc = add(v3(d.velPred[rb]), cross(v3(d.angVelPred[rb]), rB));
+    const V3<R> vr = add(sub(vAc, vBc), mul(sub(rA, rB), growthRate));
+    const R ap = -dot(vr, n);
+    if (ap <= R(0))
+      continue;
+    const R wn = computeW(rA, n, imA, v3(d.invI[ra])) + computeW(rB, n, imB, v3(d.invI[rb]));
+    if (wn > R(1e-6))
+      d.crA[idx].w += ap / wn;
+  }
+}
+template <class R>
+__global__ void kCountFriction(Dev<R> d, int nc) {
+  GRID_STRIDE(idx, nc) {
+    if (d.crA[idx].w <= R(0))
+      continue;
+    const int2 ab = d.cab[idx];
+    atomicAdd(&d.planeFric[2 * d.realIdx[ab.x] + 1], R(1));
+    if (ab.y >= 0)
+      atomicAdd(&d.planeFric[2 * d.realIdx[ab.y] + 1], R(1));
+  }
+}
+// per contact tangential impulse (src/solver_friction.hpp:152-217), reading pre-sweep velocities
+template <class R>
+__device__ __forceinline__ bool frictionImpulse(const Dev<R>& d, int idx, R muG, V3<R>& t, R& lt, V3<R>& rnA,
+                                                V3<R>& rnB) {
+  const R ln = d.crA[idx].w;
+  if (ln <= R(0))
+    return false;
+  const int2 ab = d.cab[idx];
+  const int ra = d.realIdx[ab.x];
+  const int rb = ab.y >= 0 ? d.realIdx[ab.y] : -1;
+  const R imA = d.invMass[ra], imB = ab.y >= 0 ? d.invMass[rb] : R(0);
+  const V3<R> iA = v3(d.invI[ra]), iB = ab.y >= 0 ? v3(d.invI[rb]) : V3<R>{0, 0, 0};
+  const V3<R> rA = v3(d.crA[idx]), rB = v3(d.crB[idx]), n = v3(d.cn[idx]);
+  const V3<R> vAc = add(v3(d.velPred[ra]), cross(v3(d.angVelPred[ra]), rA));
+  V3<R> vBc{0, 0, 0};
+  if (ab.y >= 0)
+    vBc = add(v3(d.velPred[rb]), cross(v3(d.angVelPred[rb]), rB));
+  else
+    vBc = v3(d.cbv[idx]);
+  const V3<R> vr = sub(vAc, vBc);
+  const R vn = dot(vr, n);
+  const V3<R> vt = sub(vr, mul(n, vn));
+  const R vl = sqrt(dot(vt, vt));
+  if (vl < R(1e-7))
+    return false;
+  t = mul(vt, R(1) / vl);
+  rnA = cross(rA, t);
+  rnB = cross(rB, t);
+  const R wt = imA + imB + rnA.x * rnA.x * iA.x + rnA.y * rnA.y * iA.y + rnA.z * rnA.z * iA.z +
+               rnB.x * rnB.x * iB.x + rnB.y * rnB.y * iB.y + rnB.z * rnB.z * iB.z;
+  if (wt < R(1e-6))
+    return false;
+  const R bound = ln;
+  const R nA = d.planeFric[2 * ra + 1];
+  const R nB = ab.y >= 0 ? d.planeFric[2 * rb + 1] : R(0);
+  const R invn = R(1) / fmax(fmax(nA, nB), R(1));
+  lt = -vl / wt;
+  const R mu = (d.cbv[idx].w >= R(0)) ? d.cbv[idx].w : muG;
+  const R maxf = mu * bound;
+  if (lt < -maxf)
+    lt = -maxf;
+  lt *= invn;
+  return true;
+}
+template <class R>
+__global__ void kFrictionImpulses(Dev<R> d, int nc, R muG, Q4<R>* tl, Q4<R>* rnAo, Q4<R>* rnBo, int* ok) {
+  GRID_STRIDE(idx, nc) {
+    V3<R> t, rnA, rnB;
+    R lt = R(0);
+    ok[idx] = frictionImpulse(d, (int)idx, muG, t, lt, rnA, rnB) ? 1 : 0;
+    tl[idx] = q4(t, lt);
+    rnAo[idx] = q4(rnA);
+    rnBo[idx] = q4(rnB);
+  }
+}
+// deltas zeroed then gathered per real body in contact order (src/solver_friction.hpp:149-217)
+template <class R>
+__global__ void kFrictionGather(Dev<R> d, int n, Incidence inc, const Q4<R>* tl, const Q4<R>* rnA,
+                                const Q4<R>* rnB, const int* ok) {
+  GRID_STRIDE(b, n) {
+    V3<R> dv{0, 0, 0}, dw{0, 0, 0};
+    const int s = inc.off[b], e = inc.off[b + 1];
+    const R im = d.invMass[b];
+    const V3<R> iI = v3(d.invI[b]);
+    for (int q = s; q < e; ++q) {
+      const int idx = inc.ent[q] >> 1, side = inc.ent[q] & 1;
+      if (!ok[idx])
+        continue;
+      const Q4<R> T = tl[idx];
+      const R lt = T.w;
+      if (side == 0) {
+        const V3<R> r = v3(rnA[idx]);
+        dv = add(dv, V3<R>{T.x * lt * im, T.y * lt * im, T.z * lt * im});
+        dw = add(dw, V3<R>{r.x * iI.x * lt, r.y * iI.y * lt, r.z * iI.z * lt});
+      } else {
+        const V3<R> r = v3(rnB[idx]);
+        dv = add(dv, V3<R>{-T.x * lt * im, -T.y * lt * im, -T.z * lt * im});
+        dw = add(dw, V3<R>{-r.x * iI.x * lt, -r.y * iI.y * lt, -r.z * iI.z * lt});
+      }
+    }
+    d.dVel[b] = q4(dv);
+    d.dAngVel[b] = q4(dw);
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// position solve (src/solver_position.hpp)
+template <class R>
+__device__ __forceinline__ bool posConstraint(const Dev<R>& d, int idx, V3<R>& n, R& C, R& wT, int& A, int& B) {
+  const int2 ab = d.cab[idx];
+  A = ab.x;
+  B = ab.y;
+  const R imA = d.invMass[A], imB = B >= 0 ? d.invMass[B] : R(0);
+  const V3<R> pA = v3(d.posPred[A]);
+  const Q4<R> qA = d.quatPred[A];
+  V3<R> pB{0, 0, 0};
+  Q4<R> qB{0, 0, 0, 1};
+  if (B >= 0) {
+    pB = v3(d.posPred[B]);
+    qB = d.quatPred[B];
+  }
+  const Q4<R> cnq = d.cn[idx];
+  const V3<R> cn = v3(cnq), crA = v3(d.crA[idx]), crB = v3(d.crB[idx]);
+  const Q4<R> qAd = qmul(qA, qinv(d.quat[A]));
+  const V3<R> rA = rot(qAd, crA);
+  V3<R> rB = crB;
+  n = cn;
+  if (B >= 0) {
+    const Q4<R> qBd = qmul(qB, qinv(d.quat[B]));
+    rB = rot(qBd, rB);
+    n = rot(qBd, n);
+  }
+  if (B < 0) {
+    n = cn;
+    C = dot(sub(add(pA, rA), crB), n);
+  } else {
+    C = dot(sub(add(pA, rA), add(pB, rB)), n);
+  }
+  if (C >= R(0))
+    return false;
+  const V3<R> iA = v3(d.invI[A]), iB = B >= 0 ? v3(d.invI[B]) : V3<R>{0, 0, 0};
+  wT = computeW(rA, n, imA, iA) + computeW(rB, n, imB, iB);
+  return true;
+}
+template <class R>
+__global__ void kPosGSColor(Dev<R> d, const int* order, const int* coff, int color, int gate) {
+  if (!gateOpen(d.ctr, gate))
+    return;
+  const int b = coff[color], n = coff[color + 1] - b;
+  GRID_STRIDE(t, n) {
+    const int idx = order[b + t];
+    V3<R> nv;
+    R C = R(0), wT = R(0);
+    int A, B;
+    if (!posConstraint(d, idx, nv, C, wT, A, B))
+      continue;
+    if (wT < R(1e-6))
+      continue;
+    const R dl = -C / wT;
+    d.posLamC[idx] += dl;
+    const R imA = d.invMass[A];
+    const V3<R> pA = v3(d.posPred[A]);
+    d.posPred[A] = q4(add(pA, V3<R>{nv.x * dl * imA, nv.y * dl * imA, nv.z * dl * imA}));
+    if (B >= 0) {
+      const R imB = d.invMass[B];
+      const V3<R> pB = v3(d.posPred[B]);
+      d.posPred[B] = q4(add(pB, V3<R>{-nv.x * dl * imB, -nv.y * dl * imB, -nv.z * dl * imB}));
+    }
+    atomicMaxNonNeg(&d.ctr->maxOverlap, -C);
+  }
+}
+// Jacobi position solve (src/solver_position.hpp:34-134): per-contact correction pre-pass, then a
+// gather per body slot in contact order
+template <class R>
+__global__ void kPosJacobiPre(Dev<R> d, int nc, int filt, Q4<R>* corr, int* ok, int gate) {
+  if (!gateOpen(d.ctr, gate))
+    return;
+  GRID_STRIDE(idx, nc) {
+    ok[idx] = 0;
+    if (filt && d.cColor[idx] != -1)
+      continue;
+    V3<R> nv;
+    R C = R(0), wT = R(0);
+    int A, B;
+    if (!posConstraint(d, (int)idx, nv, C, wT, A, B))
+      continue;
+    if (wT < R(1e-6))
+      continue;
+    const R dl = -C / wT;
+    corr[idx] = q4(nv, dl);
+    ok[idx] = 1;
+    if (C < R(0))
+      atomicMaxNonNeg(&d.ctr->maxOverlap, -C);
+  }
+}
+template <class R>
+__global__ void kPosJacobiGather(Dev<R> d, int n, Incidence inc, const Q4<R>* corr, const int* ok, int gate) {
+  if (!gateOpen(d.ctr, gate))
+    return;
+  GRID_STRIDE(b, n) {
+    const int s = inc.off[b], e = inc.off[b + 1];
+    if (s == e)
+      continue;
+    V3<R> dp = v3(d.dPos[b]);
+    int cnt = d.counts[b];
+    const R im = d.invMass[b];
+    for (int q = s; q < e; ++q) {
+      const int idx = inc.ent[q] >> 1, side = inc.ent[q] & 1;
+      if (!ok[idx])
+        continue;
+      const Q4<R> c = corr[idx];
+      const R dl = c.w;
+      if (side == 0)
+        dp = add(dp, V3<R>{c.x * dl * im, c.y * dl * im, c.z * dl * im});
+      else
+        dp = add(dp, V3<R>{-c.x * dl * im, -c.y * dl * im, -c.z * dl * im});
+      cnt += 1;
+    }
+    d.dPos[b] = q4(dp);
+    d.counts[b] = cnt;
+  }
+}
+template <class R>
+__global__ void kApplyUpdatesGated(Dev<R> d, int n, int gate) {
+  if (!gateOpen(d.ctr, gate))
+    return;
+  GRID_STRIDE(i, n) {
+    const int c = d.counts[i];
+    if (c <= 0)
+      continue;
+    const R f = R(1) / static_cast<R>(c);
+    d.posPred[i] = q4(add(v3(d.posPred[i]), mul(v3(d.dPos[i]), f)));
+    d.velPred[i] = q4(add(v3(d.velPred[i]), mul(v3(d.dVel[i]), f)));
+    d.dPos[i] = Q4<R>{0, 0, 0, 0};
+    d.dVel[i] = Q4<R>{0, 0, 0, 0};
+    d.counts[i] = 0;
+  }
+}
+
+// incidence entries: entry 2i = (body of side A, i<<1), 2i+1 = (body of side B, i<<1|1) or none
+template <class R, int KIND>
+__global__ void kIncidenceKeys(Dev<R> d, int ne, int* keys, int* vals, int none) {
+  // KIND 0: manifolds by real body; 1: contacts by real body; 2: contacts by raw slot;
+  // 3: candidate pairs by raw slot
+  GRID_STRIDE(i, ne) {
+    int2 ab = (KIND == 0) ? d.mab[i] : (KIND == 3 ? d.pairs[i] : d.cab[i]);
+    int a = ab.x, b = ab.y;
+    if (KIND == 0 || KIND == 1) {
+      a = d.realIdx[a];
+      b = b >= 0 ? d.realIdx[b] : -1;
+    }
+    keys[2 * i] = a;
+    vals[2 * i] = (int)(i << 1);
+    keys[2 * i + 1] = b >= 0 ? b : none;
+    vals[2 * i + 1] = (int)((i << 1) | 1);
+  }
+}
+// off[c] = first sorted position whose key >= c, for c in [0, nb]
+template <class K>
+__global__ void kLowerBoundOffsets(int ne, const K* sortedKeys, int nb, int* off) {
+  GRID_STRIDE(c, nb + 1) {
+    int lo = 0, hi = ne;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (sortedKeys[mid] < (K)c)
+        lo = mid + 1;
+      else
+        hi = mid;
+    }
+    off[c] = lo;
+  }
+}
+
+}  // namespace pdem
