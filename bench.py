@@ -1,0 +1,301 @@
+"""Benchmark: particle-substeps/s of the plain FP64 XPBD substep on one B200.
+
+Workload (seeded synthetic, no dataset): 262,144 polydisperse spheres, radii lognormal (median
+1 mm, sigma 0.25, clipped to [0.5, 2] mm), placed without overlap by random sequential addition in a
+box periodic in x and y (L_x = L_y, height 2 L_x, solids fraction 0.35) with a floor plane at z = 0;
+density 2500 kg/m^3, e = 0.6, mu = 0.4, gravity -9.81 m/s^2, dt = 2e-5 s split into 10 substeps
+(one `step(2e-6)` call = one substep), 10 position and 10 velocity iterations. One benchmark step
+= one outer step = 10 substeps. Metric = N x substeps / second.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+`value` is device time (CUDA events on the library's stream, summed over the step's stages) with
+the state resident in HBM; `e2e` runs the same loop through the public API with host buffers
+(external forces copied in, positions and velocities copied out every outer step) timed by the
+host clock. `--impl reference` times the reference's own code (its headers built against the
+OpenMP flavour of the Kokkos shim) on this machine's host cores. More than one GPU runs replicas
+(the single-scene step has no shard-parallel decomposition).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "peclet-dem_b200"))
+
+import numpy as np  # noqa: E402
+
+METRIC = "particle-substeps/s"
+SUBSTEPS = 10
+REF_OMP = os.path.join(ROOT, "oracle", "_ref", "libref_omp.so")
+
+
+def workload_desc(n):
+    return {"workload": f"polydisperse_{n}_periodic_xy_floor_xpbd",
+            "particles": n, "substeps_per_step": SUBSTEPS, "dt_substep": 2e-6,
+            "radii": "lognormal median 1 mm sigma 0.25 clipped [0.5,2] mm", "solids_fraction": 0.35,
+            "iterations": {"position": 10, "velocity": 10}, "precision": "fp64",
+            "l2": "state larger than L2 (no flush needed)"}
+
+
+def make_scene(n):
+    from peclet.dem import workloads as W
+    return W.polydisperse(n=n)
+
+
+# ---------------------------------------------------------------------------------------------
+# GPU clocks during the timed region
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index=0):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                                       "-lms", "200", "-i", str(self.index)], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            self.p.wait(timeout=10)
+
+    def summary(self):
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.strip().split(", ") for r in self.f.read().splitlines() if r.strip()]
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = max(mx, float(r[2]))
+                for k, name in enumerate(names):
+                    if r[5 + k].strip().lower() == "active":
+                        reasons.add(name)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------------------------
+# algorithmic bytes of one substep (FP64: D = 8 bytes per real) — byte model of the substep:
+# particles 81 D N, pairs 16 P, contacts 2 C (8 + 16 D), manifolds M (12 + 20 D), colouring
+# 12 (M + C), ledger M (16 + 8 D), velocity sweeps I_v M (12 + 20 D + 53 D), position sweeps
+# I_p C (8 + 48 D)
+def substep_bytes(n, P, C, M, iv, ip, D=8):
+    Sm = 12 + 20 * D
+    return (81 * D * n + 16 * P + 2 * C * (8 + 16 * D) + M * Sm + 12 * (M + C) + M * (16 + 8 * D)
+            + iv * M * (Sm + 53 * D) + ip * C * (8 + 48 * D))
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            pk = json.load(f)
+        return float(pk["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------------------------
+def cpu_reference(scene, substeps, threads):
+    """Time the reference's own substep (OpenMP shim build) for `substeps` calls; returns
+    particle-substeps/s. State set exactly as on the GPU (the reference computes in float)."""
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    os.environ.setdefault("OMP_PROC_BIND", "close")
+    from peclet.dem._capi import CApi, CApiSimulation
+    api = CApi(REF_OMP, "ref")
+    sim = scene.apply(CApiSimulation(api, scene.n + 8, "fp32"))
+    sim.step(scene.dt)  # warm-up: first-touch allocations and ghost capacity
+    t = time.perf_counter()
+    for _ in range(substeps):
+        sim.step(scene.dt)
+    dt = time.perf_counter() - t
+    sim.close()
+    return scene.n * substeps / dt, dt
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    if not os.path.exists(REF_OMP):
+        print(json.dumps({"impl": "reference", "unavailable": "reference build oracle/_ref/libref_omp.so missing"}))
+        return 0
+    threads = os.cpu_count() or 1
+    scene = make_scene(args.particles)
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    from peclet.dem._capi import CApi, CApiSimulation
+    api = CApi(REF_OMP, "ref")
+    sim = scene.apply(CApiSimulation(api, scene.n + 8, "fp32"))
+    # one reference "step" = one substep of the workload (a bounded sample: an outer step of 10
+    # substeps at this size takes tens of seconds on the host)
+    for _ in range(args.warmup):
+        sim.step(scene.dt)
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        sim.step(scene.dt)
+    el = time.perf_counter() - t
+    value = scene.n * args.steps / el
+    cfg = workload_desc(scene.n)
+    cfg["precision"] = "fp32 (the reference computes in float)"
+    print(json.dumps({
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+        "config": cfg, "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": METRIC, "cores": threads, "kind": "reference",
+                         "sample": f"{args.steps} substeps of the {scene.n}-sphere workload after "
+                                   f"{args.warmup} warm-up substeps; OpenMP, {threads} threads"},
+        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+    return 0
+
+
+def run_ours(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    import peclet.dem as dem
+    from peclet.dem._capi import STAGES
+    dem._API.check(dem._API.fn["set_device"](local), "set_device")
+
+    scene = make_scene(args.particles)
+    n = scene.n
+    sim = scene.apply(dem.Simulation(n + 8, "fp64"))
+    for _ in range(args.warmup):
+        for _ in range(SUBSTEPS):
+            sim.step(scene.dt)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    # ---- device-timed region ----
+    barrier()
+    sim.profile_enable(True)
+    clocks = ClockSampler(local)
+    t0 = time.perf_counter()
+    with clocks:
+        for _ in range(args.steps):
+            for _ in range(SUBSTEPS):
+                sim.step(scene.dt)
+    wall = time.perf_counter() - t0
+    stages, launches = sim.profile_read()
+    barrier()
+    dev_ms = sum(ms for ms, _ in stages.values())
+    counts = sim.debug_counts()
+    sweeps = sim.debug_sweeps() if hasattr(sim, "debug_sweeps") else None
+    sim.profile_enable(False)
+    # max over ranks of the device time; value = all ranks' particle-substeps / that time
+    t_max = dev_ms / 1e3
+    if dist is not None:
+        import torch
+        tt = torch.tensor([t_max], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_max = float(tt.item())
+    value = world * n * SUBSTEPS * args.steps / t_max
+
+    # ---- end to end through the public API with host buffers ----
+    force = np.zeros((n, 3))
+    barrier()
+    te = time.perf_counter()
+    for _ in range(args.steps):
+        sim.set_external_forces(force)
+        for _ in range(SUBSTEPS):
+            sim.step(scene.dt)
+        pos = sim.get_positions()
+        vel = sim.get_velocities()
+    e2e_s = time.perf_counter() - te
+    assert np.all(np.isfinite(pos)) and np.all(np.isfinite(vel))
+    e2e = {"value": world * n * SUBSTEPS * args.steps / e2e_s, "unit": METRIC,
+           "h2d_bytes_per_step": int(force.nbytes), "d2h_bytes_per_step": int(pos.nbytes + vel.nbytes)}
+
+    # ---- roofline of the dominant stage ----
+    per_step = {k: (ms / args.steps, c / args.steps) for k, (ms, c) in stages.items() if c}
+    dominant = max(per_step, key=lambda k: per_step[k][0])
+    peak, peak_kind = measured_peaks()
+    P, C, M = counts["pairs"], counts["contacts"], counts["manifolds"]
+    iv = sweeps["velocity"] / args.steps / SUBSTEPS if sweeps else 10
+    ip = sweeps["position"] / args.steps / SUBSTEPS if sweeps else 10
+    stage_bytes = {
+        "velocity": iv * M * (12 + 20 * 8 + 53 * 8),
+        "position": ip * C * (8 + 48 * 8),
+        "broadphase": n * 4 * 8 + 8 * P,
+        "narrowphase": 8 * P + C * (8 + 16 * 8),
+        "manifolds": 2 * C * (8 + 16 * 8) + M * (12 + 20 * 8),
+    }
+    step_bytes = substep_bytes(n, P, C, M, iv, ip) * SUBSTEPS
+    roof_stage = dominant if dominant in stage_bytes else "velocity"
+    st_ms = per_step[roof_stage][0] / SUBSTEPS
+    achieved = stage_bytes[roof_stage] / (st_ms / 1e3) / 1e9 if st_ms > 0 else 0.0
+    roofline = {"bound": "hbm", "kernel": f"{roof_stage} stage (per substep)", "achieved": achieved,
+                "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                "traffic": None, "algorithmic_bytes": stage_bytes[roof_stage],
+                "step_algorithmic_GBps": step_bytes / (dev_ms / 1e3 / args.steps) / 1e9}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu and os.path.exists(REF_OMP):
+        threads = os.cpu_count() or 1
+        v, el = cpu_reference(scene, args.cpu_substeps, threads)
+        cpu = {"value": v, "unit": METRIC, "cores": threads, "kind": "reference",
+               "sample": f"{args.cpu_substeps} substeps of the same {n}-sphere workload (reference code, "
+                         f"OpenMP Kokkos-shim build, float), {el:.1f} s"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": dict(workload_desc(n), parallelism="replicas" if world > 1 else "single"),
+            "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu,
+            "clocks": clocks.summary(), "wall_ms_per_step": 1e3 * wall / args.steps,
+            "stages_ms_per_step": {k: round(v[0], 4) for k, v in per_step.items()},
+            "counts_last_substep": counts, "sweeps": sweeps,
+        }
+        print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--particles", type=int, default=262144)
+    ap.add_argument("--cpu-substeps", type=int, default=3)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

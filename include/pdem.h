@@ -29,6 +29,10 @@ const char* pdem_last_error(void);
 /* "CUDA sm_100a" and the device name; for diagnostics */
 const char* pdem_execution_space(void);
 
+/* select the CUDA device later pdem_create calls of this thread use (one process per GPU); the
+ * reference runs on Kokkos' default device, src/dem_bindings.cpp:54-55 */
+int pdem_set_device(int device);
+
 /* Simulation(capacity)                         src/dem_bindings.cpp:72, src/sim.hpp:911-916 */
 int pdem_create(int capacity, int precision, pdem_handle* out);
 void pdem_destroy(pdem_handle h);
@@ -148,6 +152,18 @@ long pdem_debug_pos_lambda(pdem_handle h, double* out, long cap);
 long pdem_debug_hertz(pdem_handle h, unsigned long long* keys, double* xi, long cap);
 /* test hook: set the contact buffer capacity (overflow / clamp behaviour) */
 int pdem_debug_set_max_contacts(pdem_handle h, int max_contacts);
+
+/* ---- instrumentation (no reference counterpart; the reference's Kokkos labels serve Kokkos Tools) ----
+ * profile_enable(1) resets and starts per-stage device timing (CUDA events between stage
+ * boundaries of every step) and the count of this library's kernel launches; profile_read returns
+ * the number of stages and fills per-stage milliseconds and call counts, in this order:
+ * predict, ghosts, broadphase, narrowphase, manifolds, colour_velocity, warm_start, velocity,
+ * stabilization, ledger, friction, integrate, colour_position, position, commit, hertz_pairs,
+ * hertz_rebuild, hertz_integrate */
+int pdem_profile_enable(pdem_handle h, int on);
+int pdem_profile_read(pdem_handle h, double* ms, long* calls, int cap, long* launches);
+/* sweeps executed since profile_enable: velocity, stabilization, position; and substeps */
+int pdem_debug_sweeps(pdem_handle h, long* out4);
 
 #ifdef __cplusplus
 }

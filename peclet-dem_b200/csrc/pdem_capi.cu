@@ -143,6 +143,15 @@ const char* pdem_execution_space(void) {
   return g_space.c_str();
 }
 
+int pdem_set_device(int device) {
+  const cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) {
+    g_err = std::string("cudaSetDevice: ") + cudaGetErrorString(e);
+    return PDEM_ERR_CUDA;
+  }
+  return PDEM_OK;
+}
+
 int pdem_create(int capacity, int precision, pdem_handle* out) {
   if (!out) {
     g_err = "null output handle";
@@ -438,5 +447,27 @@ long pdem_debug_hertz(pdem_handle h, unsigned long long* keys, double* xi, long 
   return n;
 }
 int pdem_debug_set_max_contacts(pdem_handle h, int n) { BODY(S.setMaxContacts(n)); }
+
+// ---- instrumentation ----
+int pdem_debug_sweeps(pdem_handle h, long* out4) {
+  BODY(for (int i = 0; i < 4; ++i) out4[i] = S.sweeps_[i]);
+}
+int pdem_profile_enable(pdem_handle h, int on) { BODY(S.profileEnable(on != 0)); }
+int pdem_profile_read(pdem_handle h, double* ms, long* calls, int cap, long* launches) {
+  int n = -1;
+  with(h, [&](auto& S) {
+    using T = std::remove_reference_t<decltype(S)>;
+    n = T::ST_COUNT;
+    for (int i = 0; i < n && i < cap; ++i) {
+      if (ms)
+        ms[i] = S.stageMs_[i];
+      if (calls)
+        calls[i] = S.stageCalls_[i];
+    }
+    if (launches)
+      *launches = S.launches_;
+  });
+  return n;
+}
 
 }  // extern "C"

@@ -50,6 +50,10 @@ struct Counters {
   int hzCand;         // Hertz wall candidates wanted
   int hzRebuild;      // Hertz: displacement check asks for a pair-list rebuild
   int err;            // bit flags: a bounded loop hit its iteration limit (1 = BVH traversal/build)
+  int velSweeps;      // sweeps executed this substep (main velocity loop)
+  int stabSweeps;     // sweeps executed this substep (stabilization loop)
+  int posSweeps;      // sweeps executed this substep (position loop)
+  int pad2;
   R maxOverlap;
   R maxApproach;
   R hzMaxDisp2;

@@ -548,7 +548,7 @@ void Sim<R>::setGrowthParams(R rate, R nf) {  // src/sim.hpp:1416-1424
     gf_ = nf;
   gr_ = rate;
   if (gf_ > R(0) && numReal_ > 0) {
-    kGrowthScales<<<gridFor(numReal_), kBlock, 0, stream_>>>(d_, numReal_, gf_);
+    ++launches_, kGrowthScales<<<gridFor(numReal_), kBlock, 0, stream_>>>(d_, numReal_, gf_);
     KCHECK("growth");
     sync();
   }
@@ -606,7 +606,7 @@ R Sim<R>::maxOwnedRadius() {
     return gs_ * baseRadius_;
   rA_.ensure(1, false, stream_);
   rA_.zero(stream_, 1);
-  kMaxScale<<<gridFor(numReal_), kBlock, 0, stream_>>>(d_, numReal_, rA_.p);
+  ++launches_, kMaxScale<<<gridFor(numReal_), kBlock, 0, stream_>>>(d_, numReal_, rA_.p);
   KCHECK("maxScale");
   R mx;
   cudaCheck(cudaMemcpyAsync(&mx, rA_.p, sizeof(R), cudaMemcpyDeviceToHost, stream_), "D2H");
@@ -616,7 +616,7 @@ R Sim<R>::maxOwnedRadius() {
 // src/sim.hpp:119-145 (+ periodicity.hpp:43-94)
 template <class R>
 void Sim<R>::resetGhosts(R band) {
-  kIota<R><<<gridFor(numReal_), kBlock, 0, stream_>>>(realIdx_.p, numReal_);
+  ++launches_, kIota<R><<<gridFor(numReal_), kBlock, 0, stream_>>>(realIdx_.p, numReal_);
   KCHECK("iota");
   ensureCapacity(ghostCapacity(numReal_, band));
   numParticles_ = numReal_;
@@ -628,13 +628,13 @@ void Sim<R>::resetGhosts(R band) {
     iA_.ensure(numReal_ + 1, false, stream_);
     iB_.ensure(numReal_ + 1, false, stream_);
     iA_.zero(stream_, numReal_ + 1);
-    kGhostCount<<<gridFor(numReal_), kBlock, 0, stream_>>>(d_, numReal_, dom, band, iA_.p);
+    ++launches_, kGhostCount<<<gridFor(numReal_), kBlock, 0, stream_>>>(d_, numReal_, dom, band, iA_.p);
     KCHECK("ghostCount");
     exclusiveSum(iA_.p, iB_.p, numReal_ + 1);
     int total = 0;
     cudaCheck(cudaMemcpyAsync(&total, iB_.p + numReal_, sizeof(int), cudaMemcpyDeviceToHost, stream_), "D2H");
     sync();
-    kGhostWrite<<<gridFor(numReal_), kBlock, 0, stream_>>>(d_, numReal_, dom, band, iB_.p);
+    ++launches_, kGhostWrite<<<gridFor(numReal_), kBlock, 0, stream_>>>(d_, numReal_, dom, band, iB_.p);
     KCHECK("ghostWrite");
     numParticles_ = std::min(numReal_ + total, capacity_);
   }
@@ -669,22 +669,22 @@ int Sim<R>::findCollisions(R margin, int cap) {
   bb.err = &ctr_.p->err;
   const u64 init[6] = {~0ull, ~0ull, ~0ull, 0ull, 0ull, 0ull};
   cudaCheck(cudaMemcpyAsync(bounds_.p, init, sizeof init, cudaMemcpyHostToDevice, stream_), "H2D bounds");
-  kBoxes<<<gridFor(n), kBlock, 0, stream_>>>(d_, n, margin, boxCap, bn, bb);
+  ++launches_, kBoxes<<<gridFor(n), kBlock, 0, stream_>>>(d_, n, margin, boxCap, bn, bb);
   KCHECK("boxes");
-  kMorton<R><<<gridFor(n), kBlock, 0, stream_>>>(n, bn, bb);
+  ++launches_, kMorton<R><<<gridFor(n), kBlock, 0, stream_>>>(n, bn, bb);
   KCHECK("morton");
   sortPairs(codes_.p, codesAlt_.p, bidx_.p, bidxAlt_.p, n, 63);
   std::swap(bb.codes, bb.codesAlt);
   std::swap(bb.idx, bb.idxAlt);
   cudaCheck(cudaMemsetAsync(flag_.p, 0, n * sizeof(int), stream_), "memset");
-  kKarras<<<gridFor(n - 1), kBlock, 0, stream_>>>(bb);
+  ++launches_, kKarras<<<gridFor(n - 1), kBlock, 0, stream_>>>(bb);
   KCHECK("karras");
-  kRefit<R><<<gridFor(n), kBlock, 0, stream_>>>(bb, bn);
+  ++launches_, kRefit<R><<<gridFor(n), kBlock, 0, stream_>>>(bb, bn);
   KCHECK("refit");
-  kRopes<<<gridFor(2 * n - 1), kBlock, 0, stream_>>>(bb);
+  ++launches_, kRopes<<<gridFor(2 * n - 1), kBlock, 0, stream_>>>(bb);
   KCHECK("ropes");
   cudaCheck(cudaMemsetAsync(qcnt_.p, 0, (numReal_ + 1) * sizeof(int), stream_), "memset");
-  kQuery<R, 0><<<gridFor(numReal_, 128), 128, 0, stream_>>>(d_, numReal_, bb, bn, qcnt_.p, nullptr, nullptr, 0);
+  ++launches_, kQuery<R, 0><<<gridFor(numReal_, 128), 128, 0, stream_>>>(d_, numReal_, bb, bn, qcnt_.p, nullptr, nullptr, 0);
   KCHECK("query count");
   exclusiveSum(qcnt_.p, qoff_.p, numReal_ + 1);
   int total = 0, err = 0;
@@ -694,9 +694,9 @@ int Sim<R>::findCollisions(R margin, int cap) {
   if (err)
     throw std::runtime_error("broadphase: BVH traversal exceeded its iteration bound (corrupt tree)");
   if (total <= cap) {
-    kQuery<R, 1><<<gridFor(numReal_, 128), 128, 0, stream_>>>(d_, numReal_, bb, bn, nullptr, qoff_.p, pairs_.p, cap);
+    ++launches_, kQuery<R, 1><<<gridFor(numReal_, 128), 128, 0, stream_>>>(d_, numReal_, bb, bn, nullptr, qoff_.p, pairs_.p, cap);
     KCHECK("query write");
-    kSortPairLists<<<gridFor(numReal_), kBlock, 0, stream_>>>(numReal_, qoff_.p, pairs_.p, cap);
+    ++launches_, kSortPairLists<<<gridFor(numReal_), kBlock, 0, stream_>>>(numReal_, qoff_.p, pairs_.p, cap);
     KCHECK("pair sort");
   }
   return total;
@@ -717,7 +717,8 @@ int Sim<R>::findCollisionsGrow(R margin, const Q4<R>*) {
 template <class R>
 void Sim<R>::detectAll(R margin) {
   const int np = findCollisionsGrow(margin, posPred_.p);
-  kResetCounters<<<1, 1, 0, stream_>>>(ctr_.p);
+  mark(ST_NARROW);
+  ++launches_, kResetCounters<<<1, 1, 0, stream_>>>(ctr_.p);
   NarrowP<R> P{margin, gs_, (int)planesHost_.size(), (int)wallsHost_.size(), pairMatHost_.empty() ? 0 : 1};
   const bool shell = shape_.numPoints > 0;
   const int nr = numReal_;
@@ -734,14 +735,14 @@ void Sim<R>::detectAll(R margin) {
   // counts
   if (np > 0) {
     if (shell)
-      kNarrowShell<R, 0><<<gridFor((long)np * 32), kBlock, 0, stream_>>>(d_, np, P, iA_.p, nullptr);
+      ++launches_, kNarrowShell<R, 0><<<gridFor((long)np * 32), kBlock, 0, stream_>>>(d_, np, P, iA_.p, nullptr);
     else
-      kNarrowSphere<R, 0><<<gridFor(np), kBlock, 0, stream_>>>(d_, np, P, iA_.p, nullptr);
+      ++launches_, kNarrowSphere<R, 0><<<gridFor(np), kBlock, 0, stream_>>>(d_, np, P, iA_.p, nullptr);
     KCHECK("narrow count");
   }
   const bool boundary = nr > 0 && (P.numPlanes > 0 || P.numWalls > 0);
   if (boundary) {
-    kBoundary<R, 0><<<gridFor((long)nr * 32), kBlock, 0, stream_>>>(d_, nr, P, iC_.p, iD_.p, nullptr, nullptr, 0, 0);
+    ++launches_, kBoundary<R, 0><<<gridFor((long)nr * 32), kBlock, 0, stream_>>>(d_, nr, P, iC_.p, iD_.p, nullptr, nullptr, 0, 0);
     KCHECK("boundary count");
   }
   exclusiveSum(iA_.p, iB_.p, np + 1);
@@ -754,13 +755,13 @@ void Sim<R>::detectAll(R margin) {
   sync();
   if (np > 0 && tot[0] > 0) {
     if (shell)
-      kNarrowShell<R, 1><<<gridFor((long)np * 32), kBlock, 0, stream_>>>(d_, np, P, nullptr, iB_.p);
+      ++launches_, kNarrowShell<R, 1><<<gridFor((long)np * 32), kBlock, 0, stream_>>>(d_, np, P, nullptr, iB_.p);
     else
-      kNarrowSphere<R, 1><<<gridFor(np), kBlock, 0, stream_>>>(d_, np, P, nullptr, iB_.p);
+      ++launches_, kNarrowSphere<R, 1><<<gridFor(np), kBlock, 0, stream_>>>(d_, np, P, nullptr, iB_.p);
     KCHECK("narrow write");
   }
   if (boundary && tot[1] + tot[2] > 0 && tot[0] < maxContacts_) {
-    kBoundary<R, 1><<<gridFor((long)nr * 32), kBlock, 0, stream_>>>(d_, nr, P, nullptr, nullptr, offP, cntW, tot[0],
+    ++launches_, kBoundary<R, 1><<<gridFor((long)nr * 32), kBlock, 0, stream_>>>(d_, nr, P, nullptr, nullptr, offP, cntW, tot[0],
                                                                      tot[0] + tot[1]);
     KCHECK("boundary write");
   }
@@ -784,18 +785,18 @@ int Sim<R>::reduceManifolds(int nc) {
   head_.ensure(nc, false, stream_);
   headScan_.ensure(nc, false, stream_);
   segStart_.ensure(nc + 1, false, stream_);
-  kContactKeys<<<gridFor(nc), kBlock, 0, stream_>>>(d_, nc, ckeys_.p, cpermIn_.p);
+  ++launches_, kContactKeys<<<gridFor(nc), kBlock, 0, stream_>>>(d_, nc, ckeys_.p, cpermIn_.p);
   KCHECK("contact keys");
   sortPairs(ckeys_.p, ckeysS_.p, cpermIn_.p, cperm_.p, nc, 64);
-  kSegHeads<<<gridFor(nc), kBlock, 0, stream_>>>(nc, ckeysS_.p, head_.p);
+  ++launches_, kSegHeads<<<gridFor(nc), kBlock, 0, stream_>>>(nc, ckeysS_.p, head_.p);
   KCHECK("seg heads");
   inclusiveSum(head_.p, headScan_.p, nc);
   int nm = 0;
   cudaCheck(cudaMemcpyAsync(&nm, headScan_.p + nc - 1, sizeof(int), cudaMemcpyDeviceToHost, stream_), "D2H");
   sync();
-  kSegStarts<<<gridFor(nc), kBlock, 0, stream_>>>(nc, headScan_.p, segStart_.p);
+  ++launches_, kSegStarts<<<gridFor(nc), kBlock, 0, stream_>>>(nc, headScan_.p, segStart_.p);
   KCHECK("seg starts");
-  kReduceManifolds<<<gridFor(nm), kBlock, 0, stream_>>>(d_, nm, nc, segStart_.p, ckeysS_.p, cperm_.p);
+  ++launches_, kReduceManifolds<<<gridFor(nm), kBlock, 0, stream_>>>(d_, nm, nc, segStart_.p, ckeysS_.p, cperm_.p);
   KCHECK("reduce manifolds");
   return nm;
 }
@@ -807,25 +808,25 @@ int Sim<R>::colorGraph(bool manifold, int ne, int nb, int& leftover) {
   if (ne <= 0 || nb <= 0)
     return 0;
   int* col = manifold ? mColor_.p : cColor_.p;
-  kFillU64<<<gridFor(nb), kBlock, 0, stream_>>>(mask_.p, nb, 0ull);
+  ++launches_, kFillU64<<<gridFor(nb), kBlock, 0, stream_>>>(mask_.p, nb, 0ull);
   if (manifold)
-    kColorInitManifolds<<<gridFor(ne), kBlock, 0, stream_>>>(d_, ne);
+    ++launches_, kColorInitManifolds<<<gridFor(ne), kBlock, 0, stream_>>>(d_, ne);
   else
-    kFillInt<<<gridFor(ne), kBlock, 0, stream_>>>(col, ne, -1);
+    ++launches_, kFillInt<<<gridFor(ne), kBlock, 0, stream_>>>(col, ne, -1);
   KCHECK("color init");
   int remaining = 1, prevRem = -1;
   const int maxRounds = nb + 2;
   for (int round = 0; round < maxRounds && remaining > 0; ++round) {
-    kFillLL<<<gridFor(nb), kBlock, 0, stream_>>>(winner_.p, nb, -1ll);
+    ++launches_, kFillLL<<<gridFor(nb), kBlock, 0, stream_>>>(winner_.p, nb, -1ll);
     if (manifold)
-      kColorContend<R, true><<<gridFor(ne), kBlock, 0, stream_>>>(d_, ne, col);
+      ++launches_, kColorContend<R, true><<<gridFor(ne), kBlock, 0, stream_>>>(d_, ne, col);
     else
-      kColorContend<R, false><<<gridFor(ne), kBlock, 0, stream_>>>(d_, ne, col);
+      ++launches_, kColorContend<R, false><<<gridFor(ne), kBlock, 0, stream_>>>(d_, ne, col);
     cudaCheck(cudaMemsetAsync(&ctr_.p->remaining, 0, sizeof(int), stream_), "memset");
     if (manifold)
-      kColorCommit<R, true><<<gridFor(ne), kBlock, 0, stream_>>>(d_, ne, col, &ctr_.p->remaining);
+      ++launches_, kColorCommit<R, true><<<gridFor(ne), kBlock, 0, stream_>>>(d_, ne, col, &ctr_.p->remaining);
     else
-      kColorCommit<R, false><<<gridFor(ne), kBlock, 0, stream_>>>(d_, ne, col, &ctr_.p->remaining);
+      ++launches_, kColorCommit<R, false><<<gridFor(ne), kBlock, 0, stream_>>>(d_, ne, col, &ctr_.p->remaining);
     KCHECK("color round");
     int rem = 0;
     cudaCheck(cudaMemcpyAsync(&rem, &ctr_.p->remaining, sizeof(int), cudaMemcpyDeviceToHost, stream_), "D2H");
@@ -837,7 +838,7 @@ int Sim<R>::colorGraph(bool manifold, int ne, int nb, int& leftover) {
   }
   const int st[2] = {std::numeric_limits<int>::min(), 0};
   cudaCheck(cudaMemcpyAsync(&ctr_.p->maxColor, st, sizeof st, cudaMemcpyHostToDevice, stream_), "H2D");
-  kColorStats<<<gridFor(ne), kBlock, 0, stream_>>>(ne, col, &ctr_.p->maxColor, &ctr_.p->leftover);
+  ++launches_, kColorStats<<<gridFor(ne), kBlock, 0, stream_>>>(ne, col, &ctr_.p->maxColor, &ctr_.p->leftover);
   KCHECK("color stats");
   int res[2];
   cudaCheck(cudaMemcpyAsync(res, &ctr_.p->maxColor, sizeof res, cudaMemcpyDeviceToHost, stream_), "D2H");
@@ -855,10 +856,10 @@ void Sim<R>::colorOrder(bool manifold, int ne, int ncol) {
   uA_.ensure(ne, false, stream_);
   uB_.ensure(ne, false, stream_);
   iE_.ensure(ne, false, stream_);
-  kColorSortKeys<<<gridFor(ne), kBlock, 0, stream_>>>(ne, manifold ? mColor_.p : cColor_.p, uA_.p, iE_.p);
+  ++launches_, kColorSortKeys<<<gridFor(ne), kBlock, 0, stream_>>>(ne, manifold ? mColor_.p : cColor_.p, uA_.p, iE_.p);
   KCHECK("color keys");
   sortPairs(uA_.p, uB_.p, iE_.p, order.p, ne, 32);
-  kLowerBoundOffsets<unsigned><<<gridFor(ncol + 1), kBlock, 0, stream_>>>(ne, uB_.p, ncol, off.p);
+  ++launches_, kLowerBoundOffsets<unsigned><<<gridFor(ncol + 1), kBlock, 0, stream_>>>(ne, uB_.p, ncol, off.p);
   KCHECK("color offsets");
 }
 // per-body incidence lists in ascending source order. kind 0: manifolds x real bodies,
@@ -876,16 +877,16 @@ void Sim<R>::buildIncidence(int kind, int ne, int nb) {
     return;
   }
   if (kind == 0)
-    kIncidenceKeys<R, 0><<<gridFor(ne), kBlock, 0, stream_>>>(d_, ne, incKeys_.p, incVals_.p, nb);
+    ++launches_, kIncidenceKeys<R, 0><<<gridFor(ne), kBlock, 0, stream_>>>(d_, ne, incKeys_.p, incVals_.p, nb);
   else if (kind == 1)
-    kIncidenceKeys<R, 1><<<gridFor(ne), kBlock, 0, stream_>>>(d_, ne, incKeys_.p, incVals_.p, nb);
+    ++launches_, kIncidenceKeys<R, 1><<<gridFor(ne), kBlock, 0, stream_>>>(d_, ne, incKeys_.p, incVals_.p, nb);
   else if (kind == 2)
-    kIncidenceKeys<R, 2><<<gridFor(ne), kBlock, 0, stream_>>>(d_, ne, incKeys_.p, incVals_.p, nb);
+    ++launches_, kIncidenceKeys<R, 2><<<gridFor(ne), kBlock, 0, stream_>>>(d_, ne, incKeys_.p, incVals_.p, nb);
   else
-    kIncidenceKeys<R, 3><<<gridFor(ne), kBlock, 0, stream_>>>(d_, ne, incKeys_.p, incVals_.p, nb);
+    ++launches_, kIncidenceKeys<R, 3><<<gridFor(ne), kBlock, 0, stream_>>>(d_, ne, incKeys_.p, incVals_.p, nb);
   KCHECK("incidence keys");
   sortPairs(incKeys_.p, incKeysS_.p, incVals_.p, incValsS_.p, n2, bitsFor(nb));
-  kLowerBoundOffsets<int><<<gridFor(nb + 1), kBlock, 0, stream_>>>(n2, incKeysS_.p, nb, incOff_.p);
+  ++launches_, kLowerBoundOffsets<int><<<gridFor(nb + 1), kBlock, 0, stream_>>>(n2, incKeysS_.p, nb, incOff_.p);
   KCHECK("incidence offsets");
 }
 
@@ -902,30 +903,34 @@ template <class R>
 void Sim<R>::demStep() {
   const int B = kBlock;
   cudaStream_t s = stream_;
+  mark(ST_PREDICT);
   if (gf_ != R(-1) && gr_ != R(0)) {
     gf_ *= std::exp(gr_ * dt_);
     if (gf_ > R(1))
       gf_ = R(1);
   }
   if (gf_ > R(0) && numReal_ > 0) {
-    kGrowthScales<<<gridFor(numReal_), B, 0, s>>>(d_, numReal_, gf_);
+    ++launches_, kGrowthScales<<<gridFor(numReal_), B, 0, s>>>(d_, numReal_, gf_);
     KCHECK("growth");
   }
   const R maxRad = maxOwnedRadius();
   const R margin = R(0.1) * maxRad;
   const V3<R> g{g_[0], g_[1], g_[2]};
   if (numReal_ > 0) {
-    kPredict<<<gridFor(numReal_), B, 0, s>>>(d_, numReal_, g, dt_);
+    ++launches_, kPredict<<<gridFor(numReal_), B, 0, s>>>(d_, numReal_, g, dt_);
     KCHECK("predict");
   }
+  mark(ST_GHOSTS);
   resetGhosts(maxRad);
   if (numParticles_ > 0) {
-    kRadii<<<gridFor(numParticles_), B, 0, s>>>(d_, numParticles_, gs_, baseRadius_);
+    ++launches_, kRadii<<<gridFor(numParticles_), B, 0, s>>>(d_, numParticles_, gs_, baseRadius_);
     KCHECK("radii");
   }
+  mark(ST_BROAD);
   detectAll(margin);
   Counters<R> c0 = readCounters();
   const int nc = c0.contactCount;
+  mark(ST_MANIFOLD);
   const int nm = reduceManifolds(nc);
   c0.manifoldCount = nm;
   c0.velDone = c0.stabRun = c0.stabDone = c0.posDone = 0;
@@ -937,9 +942,10 @@ void Sim<R>::demStep() {
   if (legacyFriction) {
     planeFric_.zero(s);
     if (nc > 0)
-      kPlaneLoad<<<gridFor(nc), B, 0, s>>>(d_, nc);
+      ++launches_, kPlaneLoad<<<gridFor(nc), B, 0, s>>>(d_, nc);
     KCHECK("plane load");
   }
+  mark(ST_COLOR_V);
   int velLeft = 0;
   const int ncolV = useGS_ ? colorGraph(true, nm, numReal_, velLeft) : 0;
   if (useGS_ && ncolV > 0)
@@ -951,13 +957,14 @@ void Sim<R>::demStep() {
   if (needInc)
     buildIncidence(0, nm, numReal_);
   Incidence incM{incOff_.p, incValsS_.p};
+  mark(ST_WARM);
   if (usePGS && nm > 0) {
-    kGatherWarm<<<gridFor(nm), B, 0, s>>>(d_, nm, prevPairCount_);
+    ++launches_, kGatherWarm<<<gridFor(nm), B, 0, s>>>(d_, nm, prevPairCount_);
     KCHECK("gather warm");
     if (numReal_ > 0) {
-      kGroundDecay<<<gridFor(numReal_), B, 0, s>>>(d_, numReal_, 8);
+      ++launches_, kGroundDecay<<<gridFor(numReal_), B, 0, s>>>(d_, numReal_, 8);
       edges_.ensure(nm, false, s);
-      kGroundEdges<<<gridFor(nm), B, 0, s>>>(d_, nm, gHat, edges_.p);
+      ++launches_, kGroundEdges<<<gridFor(nm), B, 0, s>>>(d_, nm, gHat, edges_.p);
       const bool smem = (size_t)numReal_ * sizeof(int) <= 200 * 1024;
       if (!smem)
         gscratch_.ensure(numReal_, false, s);
@@ -966,20 +973,21 @@ void Sim<R>::demStep() {
         cudaFuncSetAttribute(kGroundSweeps, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
         attr = true;
       }
-      kGroundSweeps<<<1, 32, smem ? numReal_ * sizeof(int) : 0, s>>>(nm, numReal_, 8, edges_.p, grounded_.p,
+      ++launches_, kGroundSweeps<<<1, 32, smem ? numReal_ * sizeof(int) : 0, s>>>(nm, numReal_, 8, edges_.p, grounded_.p,
                                                                      gscratch_.p, smem ? 1 : 0);
       KCHECK("grounded");
     }
     sideFlags_.zero(s, nm);
-    kVn0<<<gridFor(nm), B, 0, s>>>(d_, nm, gr_);
-    kWarmApply<<<gridFor(numReal_), B, 0, s>>>(d_, numReal_, incM);
-    kWarmProject<<<gridFor(nm), B, 0, s>>>(d_, nm);
+    ++launches_, kVn0<<<gridFor(nm), B, 0, s>>>(d_, nm, gr_);
+    ++launches_, kWarmApply<<<gridFor(numReal_), B, 0, s>>>(d_, numReal_, incM);
+    ++launches_, kWarmProject<<<gridFor(nm), B, 0, s>>>(d_, nm);
     KCHECK("warm start");
   } else if (usePGS) {
     // no manifolds: the reference still decays the support levels
     if (numReal_ > 0)
-      kGroundDecay<<<gridFor(numReal_), B, 0, s>>>(d_, numReal_, 8);
+      ++launches_, kGroundDecay<<<gridFor(numReal_), B, 0, s>>>(d_, numReal_, 8);
   }
+  mark(ST_VELOCITY);
   SolveP<R> sp{gr_, eN_, eT_, mu_, R(0), dt_, ncolV};
   const R vRest = R(2) * dt_ * std::sqrt(g_[0] * g_[0] + g_[1] * g_[1] + g_[2] * g_[2]);
   sp.vRest = vRest;
@@ -988,57 +996,56 @@ void Sim<R>::demStep() {
     rA_.ensure(nm, false, s);
     iC_.ensure(nm, false, s);
   }
-  if (legacyFriction && nc > 0 && velIters_ > 0)
-    ;  // accumulate normal impulse runs each iteration below
   for (int it = 0; it < velIters_; ++it) {
     if (legacyFriction && nc > 0) {
-      // the reference accumulates every iteration, including after an adaptive stop would
-      // have ended the loop; it runs before the stop test, so gate it on the loop flag
-      kAccumNormal<<<gridFor(nc), B, 0, s>>>(d_, nc, gr_);
+      // runs at the top of every iteration the loop reaches (src/sim.hpp:224-226): with the
+      // coloured solve the adaptive stop ends the loop, so it is gated on the loop flag
+      ++launches_, kAccumNormal<<<gridFor(nc), B, 0, s>>>(d_, nc, gr_, useGS_ ? 1 : 0);
       KCHECK("accum normal");
     }
     if (useGS_) {
-      kCtl<<<1, 1, 0, s>>>(ctr_.p, CTL_VEL_BEGIN, R(0), 0);
+      ++launches_, kCtl<<<1, 1, 0, s>>>(ctr_.p, CTL_VEL_BEGIN, R(0), 0);
       for (int col = 0; col < ncolV; ++col) {
         if (usePGS)
-          kPGSColor<<<gridFor(nm), B, 0, s>>>(d_, mOrder_.p, mOff_.p, col, sp, 1);
+          ++launches_, kPGSColor<<<gridFor(nm), B, 0, s>>>(d_, mOrder_.p, mOff_.p, col, sp, 1);
         else
-          kGSColor<<<gridFor(nm), B, 0, s>>>(d_, mOrder_.p, mOff_.p, col, sp, 1);
+          ++launches_, kGSColor<<<gridFor(nm), B, 0, s>>>(d_, mOrder_.p, mOff_.p, col, sp, 1);
       }
       KCHECK("velocity sweep");
       if (velLeft > 0) {
-        kJacobiImpulses<<<gridFor(nm), B, 0, s>>>(d_, nm, sp, 1, rA_.p, iC_.p, 1);
-        kJacobiGather<<<gridFor(numReal_), B, 0, s>>>(d_, numReal_, incM, rA_.p, iC_.p, 1);
-        kApplyVelAveraged<<<gridFor(numParticles_), B, 0, s>>>(d_, numParticles_, 1);
+        ++launches_, kJacobiImpulses<<<gridFor(nm), B, 0, s>>>(d_, nm, sp, 1, rA_.p, iC_.p, 1);
+        ++launches_, kJacobiGather<<<gridFor(numReal_), B, 0, s>>>(d_, numReal_, incM, rA_.p, iC_.p, 1);
+        ++launches_, kApplyVelAveraged<<<gridFor(numParticles_), B, 0, s>>>(d_, numParticles_, 1);
         KCHECK("velocity jacobi fallback");
       }
-      kCtl<<<1, 1, 0, s>>>(ctr_.p, CTL_VEL_END, usePGS ? R(0.02) * vRest : vRest, 0);
+      ++launches_, kCtl<<<1, 1, 0, s>>>(ctr_.p, CTL_VEL_END, usePGS ? R(0.02) * vRest : vRest, 0);
     } else {
       if (nm > 0) {
-        kJacobiImpulses<<<gridFor(nm), B, 0, s>>>(d_, nm, sp, 0, rA_.p, iC_.p, 0);
-        kJacobiGather<<<gridFor(numReal_), B, 0, s>>>(d_, numReal_, incM, rA_.p, iC_.p, 0);
+        ++launches_, kJacobiImpulses<<<gridFor(nm), B, 0, s>>>(d_, nm, sp, 0, rA_.p, iC_.p, 0);
+        ++launches_, kJacobiGather<<<gridFor(numReal_), B, 0, s>>>(d_, numReal_, incM, rA_.p, iC_.p, 0);
       }
-      kApplyVelAveraged<<<gridFor(numParticles_), B, 0, s>>>(d_, numParticles_, 0);
+      ++launches_, kApplyVelAveraged<<<gridFor(numParticles_), B, 0, s>>>(d_, numParticles_, 0);
       KCHECK("velocity jacobi");
     }
   }
+  mark(ST_STAB);
   if (usePGS) {
     const R vRestS = R(2) * dt_ * gMag;
     if (stabMode_ == 2 || stabMode_ == 4) {
       throw std::runtime_error("stabilization modes 'multilevel' and 'ordered' are not supported by the B200 step");
     }
-    kCtl<<<1, 1, 0, s>>>(ctr_.p, CTL_STAB_DECIDE, vRestS, stabMode_);
+    ++launches_, kCtl<<<1, 1, 0, s>>>(ctr_.p, CTL_STAB_DECIDE, vRestS, stabMode_);
     if (stabMode_ == 1 || stabMode_ == 3) {
       if (stabMode_ == 1 && nm > 0)
-        kSideFlags<<<gridFor(nm), B, 0, s>>>(d_, nm, gHat, R(8) * dt_ * gMag, R(8) * dt_ * gMag);
+        ++launches_, kSideFlags<<<gridFor(nm), B, 0, s>>>(d_, nm, gHat, R(8) * dt_ * gMag, R(8) * dt_ * gMag);
       SolveP<R> ss = sp;
       ss.vRest = vRestS;
       const int iters = stabMode_ == 1 ? 2 * velIters_ : 256;
       for (int it = 0; it < iters; ++it) {
-        kCtl<<<1, 1, 0, s>>>(ctr_.p, CTL_STAB_BEGIN, R(0), 0);
+        ++launches_, kCtl<<<1, 1, 0, s>>>(ctr_.p, CTL_STAB_BEGIN, R(0), 0);
         for (int col = 0; col < ncolV; ++col)
-          kPGSColor<<<gridFor(nm), B, 0, s>>>(d_, mOrder_.p, mOff_.p, col, ss, 2);
-        kCtl<<<1, 1, 0, s>>>(ctr_.p, CTL_STAB_END, vRestS, 0);
+          ++launches_, kPGSColor<<<gridFor(nm), B, 0, s>>>(d_, mOrder_.p, mOff_.p, col, ss, 2);
+        ++launches_, kCtl<<<1, 1, 0, s>>>(ctr_.p, CTL_STAB_END, vRestS, 0);
         if ((it & 15) == 15) {
           const Counters<R> cc = readCounters();
           if (cc.stabDone)
@@ -1048,44 +1055,49 @@ void Sim<R>::demStep() {
       KCHECK("stabilization");
     }
   }
+  mark(ST_LEDGER);
   if (usePGS) {  // src/contact_preprocessing.hpp:160-192
     if (nm > 0) {
       lkeysS_.ensure(nm, false, s);
       lpermIn_.ensure(nm, false, s);
       lperm_.ensure(nm, false, s);
-      kIota<R><<<gridFor(nm), B, 0, s>>>(lpermIn_.p, nm);
+      ++launches_, kIota<R><<<gridFor(nm), B, 0, s>>>(lpermIn_.p, nm);
       sortPairs(pairKeys_.p, lkeysS_.p, lpermIn_.p, lperm_.p, nm, 64);
-      kCommitLedger<<<gridFor(nm), B, 0, s>>>(d_, nm, lkeysS_.p, lperm_.p);
+      ++launches_, kCommitLedger<<<gridFor(nm), B, 0, s>>>(d_, nm, lkeysS_.p, lperm_.p);
       KCHECK("commit ledger");
     }
     prevPairCount_ = nm;
   }
+  mark(ST_FRICTION);
   if (legacyFriction && nc > 0) {  // src/sim.hpp:423-429
-    kCountFriction<<<gridFor(nc), B, 0, s>>>(d_, nc);
+    ++launches_, kCountFriction<<<gridFor(nc), B, 0, s>>>(d_, nc);
     qA_.ensure(nc, false, s);
     qB_.ensure(nc, false, s);
     qC_.ensure(nc, false, s);
     iC_.ensure(nc, false, s);
-    kFrictionImpulses<<<gridFor(nc), B, 0, s>>>(d_, nc, mu_, qA_.p, qB_.p, qC_.p, iC_.p);
+    ++launches_, kFrictionImpulses<<<gridFor(nc), B, 0, s>>>(d_, nc, mu_, qA_.p, qB_.p, qC_.p, iC_.p);
     buildIncidence(1, nc, numReal_);
     Incidence incF{incOff_.p, incValsS_.p};
     dVel_.zero(s);
     dAngVel_.zero(s);
-    kFrictionGather<<<gridFor(numReal_), B, 0, s>>>(d_, numReal_, incF, qA_.p, qB_.p, qC_.p, iC_.p);
-    kApplyVelocityDeltas<<<gridFor(numParticles_), B, 0, s>>>(d_, numParticles_);
+    ++launches_, kFrictionGather<<<gridFor(numReal_), B, 0, s>>>(d_, numReal_, incF, qA_.p, qB_.p, qC_.p, iC_.p);
+    ++launches_, kApplyVelocityDeltas<<<gridFor(numParticles_), B, 0, s>>>(d_, numParticles_);
     KCHECK("legacy friction");
   } else if (legacyFriction) {
     dVel_.zero(s);
     dAngVel_.zero(s);
   }
+  mark(ST_INTEGRATE);
   if (numParticles_ > 0) {
-    kApplyVelPredictPos<<<gridFor(numParticles_), B, 0, s>>>(d_, numParticles_, dt_);
+    ++launches_, kApplyVelPredictPos<<<gridFor(numParticles_), B, 0, s>>>(d_, numParticles_, dt_);
     KCHECK("apply vel predict pos");
   }
+  mark(ST_COLOR_P);
   int posLeft = 0;
   const int ncolP = useGS_ ? colorGraph(false, nc, numParticles_, posLeft) : 0;
   if (useGS_ && ncolP > 0)
     colorOrder(false, nc, ncolP);
+  mark(ST_POSITION);
   const R posTol = R(1e-4) * baseRadius_ * gs_;
   if (nc > 0)
     posLamC_.zero(s, nc);
@@ -1098,27 +1110,28 @@ void Sim<R>::demStep() {
   Incidence incP{incOff_.p, incValsS_.p};
   for (int it = 0; it < posIters_; ++it) {
     if (useGS_) {
-      kCtl<<<1, 1, 0, s>>>(ctr_.p, CTL_POS_BEGIN, R(0), 0);
+      ++launches_, kCtl<<<1, 1, 0, s>>>(ctr_.p, CTL_POS_BEGIN, R(0), 0);
       for (int col = 0; col < ncolP; ++col)
-        kPosGSColor<<<gridFor(nc), B, 0, s>>>(d_, cOrder_.p, cOff_.p, col, 3);
+        ++launches_, kPosGSColor<<<gridFor(nc), B, 0, s>>>(d_, cOrder_.p, cOff_.p, col, 3);
       if (posLeft > 0) {
-        kPosJacobiPre<<<gridFor(nc), B, 0, s>>>(d_, nc, 1, qA_.p, iC_.p, 3);
-        kPosJacobiGather<<<gridFor(numParticles_), B, 0, s>>>(d_, numParticles_, incP, qA_.p, iC_.p, 3);
-        kApplyUpdatesGated<<<gridFor(numParticles_), B, 0, s>>>(d_, numParticles_, 3);
+        ++launches_, kPosJacobiPre<<<gridFor(nc), B, 0, s>>>(d_, nc, 1, qA_.p, iC_.p, 3);
+        ++launches_, kPosJacobiGather<<<gridFor(numParticles_), B, 0, s>>>(d_, numParticles_, incP, qA_.p, iC_.p, 3);
+        ++launches_, kApplyUpdatesGated<<<gridFor(numParticles_), B, 0, s>>>(d_, numParticles_, 3);
       }
-      kCtl<<<1, 1, 0, s>>>(ctr_.p, CTL_POS_END, posTol, 0);
+      ++launches_, kCtl<<<1, 1, 0, s>>>(ctr_.p, CTL_POS_END, posTol, 0);
     } else {
       if (nc > 0) {
-        kPosJacobiPre<<<gridFor(nc), B, 0, s>>>(d_, nc, 0, qA_.p, iC_.p, 0);
-        kPosJacobiGather<<<gridFor(numParticles_), B, 0, s>>>(d_, numParticles_, incP, qA_.p, iC_.p, 0);
+        ++launches_, kPosJacobiPre<<<gridFor(nc), B, 0, s>>>(d_, nc, 0, qA_.p, iC_.p, 0);
+        ++launches_, kPosJacobiGather<<<gridFor(numParticles_), B, 0, s>>>(d_, numParticles_, incP, qA_.p, iC_.p, 0);
       }
-      kApplyUpdatesGated<<<gridFor(numParticles_), B, 0, s>>>(d_, numParticles_, 0);
+      ++launches_, kApplyUpdatesGated<<<gridFor(numParticles_), B, 0, s>>>(d_, numParticles_, 0);
     }
     KCHECK("position sweep");
   }
+  mark(ST_COMMIT);
   if (usePGS && nm > 0) {  // src/contact_preprocessing.hpp:501-538 (scratch = vn0, as the reference)
-    kPosLoad<<<gridFor(nm), B, 0, s>>>(d_, nm, nc, segStart_.p, cperm_.p, dt_, vn0_.p);
-    kPosLoadScatter<<<gridFor(nm), B, 0, s>>>(d_, nm, lperm_.p, vn0_.p);
+    ++launches_, kPosLoad<<<gridFor(nm), B, 0, s>>>(d_, nm, nc, segStart_.p, cperm_.p, dt_, vn0_.p);
+    ++launches_, kPosLoadScatter<<<gridFor(nm), B, 0, s>>>(d_, nm, lperm_.p, vn0_.p);
     KCHECK("commit position impulse");
   }
   if (numReal_ > 0) {
@@ -1126,12 +1139,12 @@ void Sim<R>::demStep() {
     for (int a = 0; a < 3; ++a) {
       dom.mn[a] = dmin_[a], dom.mx[a] = dmax_[a], dom.sz[a] = dsize_[a], dom.per[a] = per_[a];
     }
-    kFinalCommit<<<gridFor(numReal_), B, 0, s>>>(d_, numReal_, dom);
+    ++launches_, kFinalCommit<<<gridFor(numReal_), B, 0, s>>>(d_, numReal_, dom);
     KCHECK("final commit");
   }
   if (thTau_ > R(0) && dt_ > R(0) && numReal_ > 0) {  // src/integration.hpp:229-272
     thermo_.ensure(2, false, s);
-    kThermoEnergy<<<1, 1, 0, s>>>(d_, numReal_, thermo_.p);
+    ++launches_, kThermoEnergy<<<1, 1, 0, s>>>(d_, numReal_, thermo_.p);
     double ke[2];
     cudaCheck(cudaMemcpyAsync(ke, thermo_.p, sizeof ke, cudaMemcpyDeviceToHost, s), "D2H");
     sync();
@@ -1147,8 +1160,17 @@ void Sim<R>::demStep() {
         f = 0.0;
       return static_cast<R>(std::sqrt(f));
     };
-    kThermoScale<<<gridFor(numReal_), B, 0, s>>>(d_, numReal_, lam(ke[0]), lam(ke[1]));
+    ++launches_, kThermoScale<<<gridFor(numReal_), B, 0, s>>>(d_, numReal_, lam(ke[0]), lam(ke[1]));
     KCHECK("thermostat");
+  }
+  mark(ST_END);
+  flushMarks();
+  if (prof_) {
+    const Counters<R> cc = readCounters();
+    sweeps_[0] += cc.velSweeps;
+    sweeps_[1] += cc.stabSweeps;
+    sweeps_[2] += cc.posSweeps;
+    sweeps_[3] += 1;
   }
   sync();
 }
@@ -1163,7 +1185,7 @@ R Sim<R>::computeOverlaps() {
   cudaCheck(cudaMemcpyAsync(quatPred_.p, quat_.p, capacity_ * sizeof(Q4<R>), cudaMemcpyDeviceToDevice, stream_), "D2D");
   resetGhosts(maxRad);
   if (numParticles_ > 0)
-    kRadii<<<gridFor(numParticles_), kBlock, 0, stream_>>>(d_, numParticles_, gs_, baseRadius_);
+    ++launches_, kRadii<<<gridFor(numParticles_), kBlock, 0, stream_>>>(d_, numParticles_, gs_, baseRadius_);
   detectAll(margin);
   numParticles_ = numReal_;
   return readCounters().maxOverlap;
@@ -1336,9 +1358,9 @@ void Sim<R>::hertzCommitHistory() {
   }
   lpermIn_.ensure(n, false, stream_);
   lperm_.ensure(n, false, stream_);
-  kIota<R><<<gridFor(n), kBlock, 0, stream_>>>(lpermIn_.p, n);
+  ++launches_, kIota<R><<<gridFor(n), kBlock, 0, stream_>>>(lpermIn_.p, n);
   sortPairs(hzKeys_.p, hzPrevKeys_.p, lpermIn_.p, lperm_.p, n, 64);
-  kHertzGatherPrev<<<gridFor(n), kBlock, 0, stream_>>>(n, lperm_.p, hzXi_.p, hzPrevXi_.p);
+  ++launches_, kHertzGatherPrev<<<gridFor(n), kBlock, 0, stream_>>>(n, lperm_.p, hzXi_.p, hzPrevXi_.p);
   KCHECK("hertz commit history");
   hzPrevCount_ = n;
 }
@@ -1368,7 +1390,7 @@ void Sim<R>::hertzRebuildPairs(R skin) {
     hzKeys_.ensure(need, false, stream_);
   }
   if (np > 0) {
-    kHertzCarry<<<gridFor(np), kBlock, 0, stream_>>>(d_, np, hzPrevCount_, hzPrevKeys_.p, hzPrevXi_.p, hzKeys_.p,
+    ++launches_, kHertzCarry<<<gridFor(np), kBlock, 0, stream_>>>(d_, np, hzPrevCount_, hzPrevKeys_.p, hzPrevXi_.p, hzKeys_.p,
                                                       hzXi_.p);
     KCHECK("hertz carry");
     hzSnPair_.zero(stream_, np);
@@ -1385,14 +1407,14 @@ int Sim<R>::hertzWallCandidates(R skin) {
   iC_.ensure(n + 1, false, stream_);
   iD_.ensure(n + 1, false, stream_);
   iC_.zero(stream_, n + 1);
-  kHertzWallCand<R, 0><<<gridFor(n), kBlock, 0, stream_>>>(d_, n, (int)wallsHost_.size(), skin, iC_.p, nullptr,
+  ++launches_, kHertzWallCand<R, 0><<<gridFor(n), kBlock, 0, stream_>>>(d_, n, (int)wallsHost_.size(), skin, iC_.p, nullptr,
                                                            nullptr, 0);
   exclusiveSum(iC_.p, iD_.p, n + 1);
   int total = 0;
   cudaCheck(cudaMemcpyAsync(&total, iD_.p + n, sizeof(int), cudaMemcpyDeviceToHost, stream_), "D2H");
   sync();
   const int cap = (int)hzWallCand_.n;
-  kHertzWallCand<R, 1><<<gridFor(n), kBlock, 0, stream_>>>(d_, n, (int)wallsHost_.size(), skin, nullptr, iD_.p,
+  ++launches_, kHertzWallCand<R, 1><<<gridFor(n), kBlock, 0, stream_>>>(d_, n, (int)wallsHost_.size(), skin, nullptr, iD_.p,
                                                            hzWallCand_.p, cap);
   KCHECK("hertz wall candidates");
   hzCandOff_.ensure(n + 1, false, stream_);
@@ -1411,7 +1433,7 @@ void Sim<R>::stepHertz(R dt, int nsteps, R skinFrac) {
     throw std::runtime_error("step_hertz: too many SDF walls");
   const int n = numReal_;
   if (n > 0)
-    kRadii<<<gridFor(n), kBlock, 0, stream_>>>(d_, n, gs_, baseRadius_);
+    ++launches_, kRadii<<<gridFor(n), kBlock, 0, stream_>>>(d_, n, gs_, baseRadius_);
   // min radius = min over scale * gs * bR: rounding is monotone, so it is minScale * gs * bR
   R minRad = std::numeric_limits<R>::max();
   if (n > 0) {
@@ -1436,12 +1458,14 @@ void Sim<R>::stepHertz(R dt, int nsteps, R skinFrac) {
   const V3<R> g{g_[0], g_[1], g_[2]};
   for (int k = 0; k < nsteps; ++k) {
     if (rebuild) {
+      mark(ST_HERTZ_REBUILD);
       hertzCommitHistory();
       hertzRebuildPairs(skin);
       if (nw > 0)
         hzNumWallCand_ = hertzWallCandidates(skin);
       rebuild = false;
     }
+    mark(ST_HERTZ_PAIRS);
     const int np = hzNumPairs_;
     qA_.ensure(std::max(np, 1), false, stream_);
     qB_.ensure(std::max(np, 1), false, stream_);
@@ -1449,10 +1473,10 @@ void Sim<R>::stepHertz(R dt, int nsteps, R skinFrac) {
     iE_.ensure(std::max(np, 1), false, stream_);
     if (np > 0) {
       if (hasShapes)
-        kHertzShapePairs<<<gridFor(np), kBlock, 0, stream_>>>(d_, np, P, hzXi_.p, hzSnPair_.p, qA_.p, qB_.p, qC_.p,
+        ++launches_, kHertzShapePairs<<<gridFor(np), kBlock, 0, stream_>>>(d_, np, P, hzXi_.p, hzSnPair_.p, qA_.p, qB_.p, qC_.p,
                                                                iE_.p);
       else
-        kHertzPairs<<<gridFor(np), kBlock, 0, stream_>>>(d_, np, P, hzXi_.p, qA_.p, qB_.p, qC_.p, iE_.p);
+        ++launches_, kHertzPairs<<<gridFor(np), kBlock, 0, stream_>>>(d_, np, P, hzXi_.p, qA_.p, qB_.p, qC_.p, iE_.p);
       KCHECK("hertz pairs");
     }
     const int nc = (nw > 0) ? hzNumWallCand_ : 0;
@@ -1460,12 +1484,13 @@ void Sim<R>::stepHertz(R dt, int nsteps, R skinFrac) {
     hzTW_.ensure(std::max(nc, 1), false, stream_);
     hzOnW_.ensure(std::max(nc, 1), false, stream_);
     if (nc > 0) {
-      kHertzWalls<<<gridFor(nc), kBlock, 0, stream_>>>(d_, nc, P, hzWallCand_.p, hzXiWall_.p, hzSnWall_.p,
+      ++launches_, kHertzWalls<<<gridFor(nc), kBlock, 0, stream_>>>(d_, nc, P, hzWallCand_.p, hzXiWall_.p, hzSnWall_.p,
                                                         hasShapes ? 1 : 0, hzFW_.p, hzTW_.p, hzOnW_.p);
       KCHECK("hertz walls");
     }
+    mark(ST_HERTZ_INTEGRATE);
     if (n > 0) {
-      kHertzGatherIntegrate<<<gridFor(n), kBlock, 0, stream_>>>(
+      ++launches_, kHertzGatherIntegrate<<<gridFor(n), kBlock, 0, stream_>>>(
           d_, n, incOff_.p, incValsS_.p, qA_.p, qB_.p, qC_.p, iE_.p, nc > 0 ? hzCandOff_.p : nullptr, nc, hzFW_.p,
           hzTW_.p, hzOnW_.p, g, dt, hasShapes ? 1 : 0);
       KCHECK("hertz integrate");
@@ -1474,7 +1499,7 @@ void Sim<R>::stepHertz(R dt, int nsteps, R skinFrac) {
       rA_.ensure(1, false, stream_);
       rA_.zero(stream_, 1);
       if (n > 0)
-        kHertzMaxDisp2<<<gridFor(n), kBlock, 0, stream_>>>(d_, n, hzRefPos_.p, rA_.p);
+        ++launches_, kHertzMaxDisp2<<<gridFor(n), kBlock, 0, stream_>>>(d_, n, hzRefPos_.p, rA_.p);
       R m = 0;
       cudaCheck(cudaMemcpyAsync(&m, rA_.p, sizeof(R), cudaMemcpyDeviceToHost, stream_), "D2H");
       sync();
@@ -1484,6 +1509,8 @@ void Sim<R>::stepHertz(R dt, int nsteps, R skinFrac) {
         rebuild = true;
     }
   }
+  mark(ST_END);
+  flushMarks();
   cudaCheck(cudaMemcpyAsync(posPred_.p, pos_.p, capacity_ * sizeof(Q4<R>), cudaMemcpyDeviceToDevice, stream_), "D2D");
   cudaCheck(cudaMemcpyAsync(velPred_.p, vel_.p, capacity_ * sizeof(Q4<R>), cudaMemcpyDeviceToDevice, stream_), "D2D");
   sync();
@@ -1500,6 +1527,48 @@ long Sim<R>::getHertz(unsigned long long* keys, double* xi, long cap) {
     xi[3 * i + 2] = x[i].z;
   }
   return n;
+}
+
+// ---- instrumentation ----
+template <class R>
+void Sim<R>::profileEnable(bool on) {
+  prof_ = on;
+  for (int i = 0; i < ST_COUNT; ++i) {
+    stageMs_[i] = 0;
+    stageCalls_[i] = 0;
+  }
+  launches_ = 0;
+  for (long& v : sweeps_)
+    v = 0;
+}
+template <class R>
+void Sim<R>::mark(int stage) {
+  if (!prof_)
+    return;
+  cudaEvent_t e;
+  if (evFree_.empty())
+    cudaCheck(cudaEventCreate(&e), "cudaEventCreate");
+  else {
+    e = evFree_.back();
+    evFree_.pop_back();
+  }
+  cudaCheck(cudaEventRecord(e, stream_), "cudaEventRecord");
+  marks_.push_back({stage, e});
+}
+template <class R>
+void Sim<R>::flushMarks() {
+  if (marks_.empty())
+    return;
+  sync();
+  for (size_t k = 0; k + 1 < marks_.size(); ++k) {
+    float ms = 0;
+    cudaCheck(cudaEventElapsedTime(&ms, marks_[k].ev, marks_[k + 1].ev), "cudaEventElapsedTime");
+    stageMs_[marks_[k].stage] += ms;
+    stageCalls_[marks_[k].stage] += 1;
+  }
+  for (auto& m : marks_)
+    evFree_.push_back(m.ev);
+  marks_.clear();
 }
 
 template class Sim<float>;

@@ -141,6 +141,21 @@ class Sim {
   cudaStream_t stream_ = nullptr;
   Dev<R> d_{};
 
+  // ---- instrumentation: kernel launch count and opt-in per-stage device time ----
+  enum Stage {
+    ST_PREDICT, ST_GHOSTS, ST_BROAD, ST_NARROW, ST_MANIFOLD, ST_COLOR_V, ST_WARM, ST_VELOCITY, ST_STAB,
+    ST_LEDGER, ST_FRICTION, ST_INTEGRATE, ST_COLOR_P, ST_POSITION, ST_COMMIT, ST_HERTZ_PAIRS, ST_HERTZ_REBUILD,
+    ST_HERTZ_INTEGRATE, ST_END, ST_COUNT
+  };
+  long launches_ = 0;
+  long sweeps_[4] = {0, 0, 0, 0};  // velocity, stabilization, position sweeps; substeps (profiled)
+  bool prof_ = false;
+  double stageMs_[ST_COUNT] = {};
+  long stageCalls_[ST_COUNT] = {};
+  void profileEnable(bool on);
+  void mark(int stage);
+  void flushMarks();
+
  private:
   // device buffers
   DBuf<Q4<R>> pos_, vel_, angVel_, invI_, posPred_, velPred_, angVelPred_, quat_, quatPred_, extF_, dVel_,
@@ -199,6 +214,12 @@ class Sim {
   DBuf<R> hzSnPair_, hzSnWall_;
   DBuf<int> hzWallCand_, hzCandOff_, hzOnW_;
   DBuf<Q4<R>> hzFW_, hzTW_;
+  struct Mark {
+    int stage;
+    cudaEvent_t ev;
+  };
+  std::vector<Mark> marks_;
+  std::vector<cudaEvent_t> evFree_;
 
   void allocate(int cap, int maxPairs, int maxContacts);
   void allocContactBuffers(int mc);

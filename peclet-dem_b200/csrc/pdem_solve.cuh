@@ -11,6 +11,10 @@
 
 namespace pdem {
 
+// colours are capped at 62 (src/solver_velocity.hpp:341-342): bodies of degree > 62 can leave
+// several manifolds sharing a body in colour 62
+constexpr int kSaturatedColor = 62;
+
 // incidence list entry: source index << 1 | side (0 = body A, 1 = body B)
 struct Incidence {
   const int* off;  // [nbodies + 1]
@@ -76,8 +80,10 @@ __global__ void kCtl(Counters<R>* c, int op, R thr, int mode) {
     return;
   switch (op) {
     case CTL_VEL_BEGIN:
-      if (!c->velDone)
+      if (!c->velDone) {
         c->maxApproach = R(0);
+        c->velSweeps += 1;
+      }
       break;
     case CTL_VEL_END:
       if (!c->velDone && c->maxApproach <= thr)
@@ -88,16 +94,20 @@ __global__ void kCtl(Counters<R>* c, int op, R thr, int mode) {
       c->stabDone = c->stabRun ? 0 : 1;
       break;
     case CTL_STAB_BEGIN:
-      if (!c->stabDone)
+      if (!c->stabDone) {
         c->maxApproach = R(0);
+        c->stabSweeps += 1;
+      }
       break;
     case CTL_STAB_END:
       if (!c->stabDone && c->maxApproach <= thr)
         c->stabDone = 1;
       break;
     case CTL_POS_BEGIN:
-      if (!c->posDone)
+      if (!c->posDone) {
         c->maxOverlap = R(0);
+        c->posSweeps += 1;
+      }
       break;
     case CTL_POS_END:
       if (!c->posDone && c->maxOverlap < thr)
@@ -279,7 +289,13 @@ __global__ void kPGSColor(Dev<R> d, const int* order, const int* coff, int color
   if (!gateOpen(d.ctr, gate))
     return;
   const int b = coff[color], n = coff[color + 1] - b;
-  GRID_STRIDE(t, n) {
+  // colour 62 is where the 62-colour mask saturates: it is not an independent set, so it
+  // runs serially in manifold order, as the reference's serial sweep does
+  const bool serial = color >= kSaturatedColor;
+  if (serial && (blockIdx.x | threadIdx.x))
+    return;
+  for (long t = serial ? 0 : (long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+       t += serial ? 1 : (long)gridDim.x * blockDim.x) {
     const int idx = order[b + t];
     const ManifoldView<R> v = loadManifold(d, idx);
     const int ra = v.ra, rb = v.rb;
@@ -422,7 +438,13 @@ __global__ void kGSColor(Dev<R> d, const int* order, const int* coff, int color,
   if (!gateOpen(d.ctr, gate))
     return;
   const int b = coff[color], n = coff[color + 1] - b;
-  GRID_STRIDE(t, n) {
+  // colour 62 is where the 62-colour mask saturates: it is not an independent set, so it
+  // runs serially in manifold order, as the reference's serial sweep does
+  const bool serial = color >= kSaturatedColor;
+  if (serial && (blockIdx.x | threadIdx.x))
+    return;
+  for (long t = serial ? 0 : (long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+       t += serial ? 1 : (long)gridDim.x * blockDim.x) {
     const int idx = order[b + t];
     const ManifoldView<R> v = loadManifold(d, idx);
     const bool hasB = d.mab[idx].y >= 0;
@@ -613,7 +635,9 @@ __global__ void kPlaneLoad(Dev<R> d, int nc) {
   }
 }
 template <class R>
-__global__ void kAccumNormal(Dev<R> d, int nc, R growthRate) {
+__global__ void kAccumNormal(Dev<R> d, int nc, R growthRate, int gate) {
+  if (!gateOpen(d.ctr, gate))
+    return;
   GRID_STRIDE(idx, nc) {
     const int2 ab = d.cab[idx];
     const V3<R> rA = v3(d.crA[idx]), rB = v3(d.crB[idx]), n = v3(d.cn[idx]);
@@ -786,7 +810,13 @@ __global__ void kPosGSColor(Dev<R> d, const int* order, const int* coff, int col
   if (!gateOpen(d.ctr, gate))
     return;
   const int b = coff[color], n = coff[color + 1] - b;
-  GRID_STRIDE(t, n) {
+  // colour 62 is where the 62-colour mask saturates: it is not an independent set, so it
+  // runs serially in manifold order, as the reference's serial sweep does
+  const bool serial = color >= kSaturatedColor;
+  if (serial && (blockIdx.x | threadIdx.x))
+    return;
+  for (long t = serial ? 0 : (long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+       t += serial ? 1 : (long)gridDim.x * blockDim.x) {
     const int idx = order[b + t];
     V3<R> nv;
     R C = R(0), wT = R(0);

@@ -28,6 +28,7 @@ OK, ERR_RUNTIME, ERR_INVALID, ERR_UNSUPPORTED, ERR_CUDA = 0, 1, 2, 3, 4
 # name -> (restype, argtypes) for the shared ABI (the prefix is prepended at load time)
 _SIGS = {
     "last_error": (C.c_char_p, []),
+    "set_device": (C.c_int, [C.c_int]),
     "create": (C.c_int, [C.c_int, C.c_int, C.POINTER(_vp)]),
     "destroy": (None, [_vp]),
     "initialize_shape": (C.c_int, [_vp, C.c_int, C.c_double, C.c_double, C.c_double]),
@@ -97,7 +98,15 @@ _SIGS = {
     "debug_pos_lambda": (C.c_long, [_vp, _dbl_p, C.c_long]),
     "debug_hertz": (C.c_long, [_vp, _u64_p, _dbl_p, C.c_long]),
     "debug_set_max_contacts": (C.c_int, [_vp, C.c_int]),
+    # instrumentation
+    "profile_enable": (C.c_int, [_vp, C.c_int]),
+    "profile_read": (C.c_int, [_vp, _dbl_p, _long_p, C.c_int, _long_p]),
+    "debug_sweeps": (C.c_int, [_vp, _long_p]),
 }
+
+STAGES = ("predict", "ghosts", "broadphase", "narrowphase", "manifolds", "colour_velocity", "warm_start",
+          "velocity", "stabilization", "ledger", "friction", "integrate", "colour_position", "position",
+          "commit", "hertz_pairs", "hertz_rebuild", "hertz_integrate")
 
 _STAB_MODES = ("off", "onesided", "multilevel", "escalate", "ordered")
 
@@ -480,3 +489,23 @@ class CApiSimulation:
 
     def debug_set_max_contacts(self, n):
         self._call("debug_set_max_contacts", int(n))
+
+    # ---- instrumentation -------------------------------------------------------------------------
+    def profile_enable(self, on=True):
+        """Start (reset) per-stage device timing and the kernel launch count."""
+        self._call("profile_enable", int(bool(on)))
+
+    def profile_read(self):
+        """(dict stage -> (milliseconds, calls), kernel launches) since profile_enable."""
+        ms = np.zeros(32, dtype=np.float64)
+        calls = np.zeros(32, dtype=np.int64)
+        launches = C.c_long(0)
+        n = self._f["profile_read"](self._h, _ptr(ms), calls.ctypes.data_as(_long_p), 32, C.byref(launches))
+        stages = {STAGES[i]: (float(ms[i]), int(calls[i])) for i in range(min(n, len(STAGES)))}
+        return stages, int(launches.value)
+
+    def debug_sweeps(self):
+        """Sweeps executed since profile_enable (velocity, stabilization, position) and substeps."""
+        out = np.zeros(4, dtype=np.int64)
+        self._call("debug_sweeps", out.ctypes.data_as(_long_p))
+        return dict(zip(("velocity", "stabilization", "position", "substeps"), (int(v) for v in out)))

@@ -8,6 +8,9 @@ step (1e-4 canonical, src/narrowphase.hpp:235) is relative to the grain size.
 """
 from __future__ import annotations
 
+import ctypes
+import os
+import subprocess
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -167,58 +170,57 @@ def hollow_cylinders(seed=3, n=65536, r_out=1e-3, r_in=0.6e-3, length=3e-3, box=
                  substeps=substeps, shell=shell_points)
 
 
+_RSA_SRC = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_gen", "rsa.c")
+_RSA_LIB = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_gen", "librsa.so")
+
+
+def _rsa_lib():
+    if not os.path.exists(_RSA_LIB) or os.path.getmtime(_RSA_LIB) < os.path.getmtime(_RSA_SRC):
+        subprocess.run(["gcc", "-O2", "-shared", "-fPIC", "-o", _RSA_LIB, _RSA_SRC, "-lm"], check=True)
+    lib = ctypes.CDLL(_RSA_LIB)
+    dp = ctypes.POINTER(ctypes.c_double)
+    lib.pdem_rsa_spheres.restype = ctypes.c_long
+    lib.pdem_rsa_spheres.argtypes = [ctypes.c_long, dp, dp, dp, ctypes.POINTER(ctypes.c_int),
+                                     ctypes.c_ulonglong, ctypes.c_int, dp,
+                                     ctypes.POINTER(ctypes.c_ubyte)]
+    return lib
+
+
+def rsa_spheres(seed, radii, lo, hi, periodic=(False, False, False), tries=1000):
+    """Random sequential addition (largest first, uniform proposals, rejection on overlap) by the
+    compiled helper _gen/rsa.c; returns (positions, placed mask)."""
+    lib = _rsa_lib()
+    r = np.ascontiguousarray(radii, dtype=np.float64)
+    order = np.argsort(-r, kind="stable")
+    rs = np.ascontiguousarray(r[order])
+    pos = np.zeros((r.size, 3))
+    placed = np.zeros(r.size, dtype=np.uint8)
+    lo = np.ascontiguousarray(lo, dtype=np.float64)
+    hi = np.ascontiguousarray(hi, dtype=np.float64)
+    per = np.ascontiguousarray(np.asarray(periodic, dtype=np.int32))
+    dp = ctypes.POINTER(ctypes.c_double)
+    lib.pdem_rsa_spheres(r.size, rs.ctypes.data_as(dp), lo.ctypes.data_as(dp), hi.ctypes.data_as(dp),
+                         per.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), int(seed), int(tries),
+                         pos.ctypes.data_as(dp), placed.ctypes.data_as(ctypes.POINTER(ctypes.c_ubyte)))
+    out = np.zeros_like(pos)
+    ok = np.zeros(r.size, dtype=bool)
+    out[order] = pos
+    ok[order] = placed.astype(bool)
+    return out, ok
+
+
 def polydisperse(seed=2, n=262144, median=1e-3, sigma=0.25, rmin=0.5e-3, rmax=2e-3, phi=0.35,
                  density=2500.0, E=1e7, nu=0.3, mu=0.4, e=0.6, dt_outer=2e-5, substeps=10,
                  periodic=True) -> Scene:
-    """Polydisperse lognormal spheres placed without overlap by random sequential addition in a box
-    periodic in x and y (L_x = L_y, height 2 L_x, solids fraction phi) with a floor at z = 0."""
+    """Polydisperse lognormal spheres (median 1 mm, sigma 0.25, clipped to [0.5, 2] mm) placed
+    without overlap by random sequential addition in a box periodic in x and y with a floor plane
+    at z = 0; L_x = L_y and the height 2 L_x are chosen for a solids fraction `phi`."""
     rng = np.random.default_rng(seed)
     r = np.clip(rng.lognormal(np.log(median), sigma, n), rmin, rmax)
     vs = np.sum(4.0 / 3.0 * np.pi * r ** 3)
     L = (vs / (2.0 * phi)) ** (1.0 / 3.0)
     H = 2.0 * L
-    order = np.argsort(-r)  # place large first
-    cell = 2 * rmax
-    dims = np.maximum(1, np.floor(np.array([L, L, H]) / cell).astype(int))
-    head = -np.ones(int(np.prod(dims)), dtype=np.int64)
-    nxt = -np.ones(n, dtype=np.int64)
-    pos = np.zeros((n, 3))
-    placed = np.zeros(n, bool)
-    for idx in order:
-        ri = r[idx]
-        for _ in range(1000):
-            p = np.array([rng.uniform(0, L), rng.uniform(0, L), rng.uniform(ri, H - ri)])
-            c = np.minimum((p / (np.array([L, L, H]) / dims)).astype(int), dims - 1)
-            ok = True
-            for dx in (-1, 0, 1):
-                for dy in (-1, 0, 1):
-                    for dz in (-1, 0, 1):
-                        cc = c + (dx, dy, dz)
-                        if cc[2] < 0 or cc[2] >= dims[2]:
-                            continue
-                        cc[0] %= dims[0]
-                        cc[1] %= dims[1]
-                        q = head[(cc[2] * dims[1] + cc[1]) * dims[0] + cc[0]]
-                        while q >= 0:
-                            d = pos[q] - p
-                            d[:2] -= L * np.round(d[:2] / L)
-                            if d @ d < (ri + r[q]) ** 2:
-                                ok = False
-                                break
-                            q = nxt[q]
-                        if not ok:
-                            break
-                    if not ok:
-                        break
-                if not ok:
-                    break
-            if ok:
-                pos[idx] = p
-                placed[idx] = True
-                k = (c[2] * dims[1] + c[1]) * dims[0] + c[0]
-                nxt[idx] = head[k]
-                head[k] = idx
-                break
+    pos, placed = rsa_spheres(seed, r, (0.0, 0.0, 0.0), (L, L, H), (periodic, periodic, False))
     keep = np.nonzero(placed)[0]
     pos, r = pos[keep], r[keep]
     n = pos.shape[0]
