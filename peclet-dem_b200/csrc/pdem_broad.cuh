@@ -70,6 +70,7 @@ struct BvhNodes {
 
 template <class R>
 __global__ void kBoxes(Dev<R> d, int n, R margin, R boxCap, BvhNodes<R> bn, BvhBuffers bb) {
+  u64 lo[3] = {~0ull, ~0ull, ~0ull}, hi[3] = {0ull, 0ull, 0ull};
   GRID_STRIDE(i, n) {
     const Box<R> b = saneBox(d, (int)i, d.posPred, margin, boxCap);
     bn.prim[i] = b;
@@ -81,9 +82,24 @@ __global__ void kBoxes(Dev<R> d, int n, R margin, R boxCap, BvhNodes<R> bn, BvhB
     }
     if (ok)
       for (int a = 0; a < 3; ++a) {
-        atomicMin(&bb.bounds[a], orderedBits(c[a]));
-        atomicMax(&bb.bounds[3 + a], orderedBits(c[a]));
+        const u64 o = orderedBits(c[a]);
+        lo[a] = o < lo[a] ? o : lo[a];
+        hi[a] = o > hi[a] ? o : hi[a];
       }
+  }
+  // scene bounds: warp reduction, one atomic per warp and axis
+  for (int a = 0; a < 3; ++a) {
+    for (int o = 16; o > 0; o >>= 1) {
+      const u64 l = __shfl_xor_sync(0xffffffffu, lo[a], o), h = __shfl_xor_sync(0xffffffffu, hi[a], o);
+      lo[a] = l < lo[a] ? l : lo[a];
+      hi[a] = h > hi[a] ? h : hi[a];
+    }
+    if ((threadIdx.x & 31) == 0) {
+      if (lo[a] != ~0ull)
+        atomicMin(&bb.bounds[a], lo[a]);
+      if (hi[a] != 0ull)
+        atomicMax(&bb.bounds[3 + a], hi[a]);
+    }
   }
 }
 
@@ -245,8 +261,12 @@ template <class R, int MODE>
 __global__ void kQuery(Dev<R> d, int numReal, BvhBuffers bb, BvhNodes<R> bn, int* cnt, const int* off,
                        int2* out, int outCap) {
   const int n = bb.n;
-  GRID_STRIDE(ii, numReal) {
-    const int i = (int)ii;
+  // threads take the primitives in Morton order, so a warp's queries are spatial neighbours and
+  // walk nearly the same nodes; each real particle's results go to its own (i-ordered) segment
+  GRID_STRIDE(kk, n) {
+    const int i = bb.idx[kk];
+    if (i >= numReal)
+      continue;
     const Box<R> q = bn.prim[i];
     int c = 0;
     int base = MODE ? off[i] : 0;

@@ -120,4 +120,23 @@ __device__ __forceinline__ void atomicMaxNonNeg(float* p, float v) {
     atomicMax(reinterpret_cast<unsigned int*>(p), (unsigned int)__float_as_int(v));
 }
 
+// Order-free max of non-negative values with one atomic per warp: every lane of the warp must
+// call it (after its grid-stride loop). Lanes carry their own running max (0 when nothing).
+template <class R>
+__device__ __forceinline__ void warpMaxAtomic(R* p, R v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const R w = __shfl_xor_sync(0xffffffffu, v, o);
+    v = w > v ? w : v;
+  }
+  if ((threadIdx.x & 31) == 0)
+    atomicMaxNonNeg(p, v);
+}
+// running max that ignores NaN (the reference's atomic max never stores NaN)
+template <class R>
+__device__ __forceinline__ void runMax(R& acc, R v) {
+  if (v > acc)
+    acc = v;
+}
+
 }  // namespace pdem

@@ -71,13 +71,14 @@ __device__ __forceinline__ void writeBodyContact(const Dev<R>& d, int slot, int 
 template <class R, int MODE>
 __global__ void kNarrowSphere(Dev<R> d, int np, NarrowP<R> P, int* cnt, const int* off) {
   const ShapeDesc<R> dA = d.shapes[0], dB = d.shapes[0];
+  R mo = R(0);
   GRID_STRIDE(idx, np) {
     const int2 pr = d.pairs[idx];
     const Probe<R> p = probeBody(d, pr.x, pr.y, 0, dA, dB, P.globalScale);
     const bool hit = p.eff < P.margin;
     if (MODE == 0) {
       if (p.eff < R(0))
-        atomicMaxNonNeg(&d.ctr->maxOverlap, -p.eff);
+        runMax(mo, -p.eff);
       cnt[idx] = hit ? 1 : 0;
     } else if (hit) {
       const int s = off[idx];
@@ -85,6 +86,8 @@ __global__ void kNarrowSphere(Dev<R> d, int np, NarrowP<R> P, int* cnt, const in
         writeBodyContact(d, s, pr.x, pr.y, p, dB, P);
     }
   }
+  if (MODE == 0)
+    warpMaxAtomic(&d.ctr->maxOverlap, mo);
 }
 
 // point shells: one warp per pair, lanes over shell points in order
@@ -95,6 +98,7 @@ __global__ void kNarrowShell(Dev<R> d, int np, NarrowP<R> P, int* cnt, const int
   const long warp = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const long nwarps = ((long)gridDim.x * blockDim.x) >> 5;
   const int K = dA.numPoints > 0 ? dA.numPoints : 1;
+  R mo = R(0);
   for (long idx = warp; idx < np; idx += nwarps) {
     const int2 pr = d.pairs[idx];
     int running = MODE ? off[idx] : 0;
@@ -107,7 +111,7 @@ __global__ void kNarrowShell(Dev<R> d, int np, NarrowP<R> P, int* cnt, const int
         p = probeBody(d, pr.x, pr.y, k, dA, dB, P.globalScale);
         hit = p.eff < P.margin;
         if (MODE == 0 && p.eff < R(0))
-          atomicMaxNonNeg(&d.ctr->maxOverlap, -p.eff);
+          runMax(mo, -p.eff);
       }
       const unsigned b = __ballot_sync(0xffffffffu, hit);
       if (MODE == 1 && hit) {
@@ -121,6 +125,8 @@ __global__ void kNarrowShell(Dev<R> d, int np, NarrowP<R> P, int* cnt, const int
     if (MODE == 0 && lane == 0)
       cnt[idx] = total;
   }
+  if (MODE == 0)
+    warpMaxAtomic(&d.ctr->maxOverlap, mo);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -222,6 +228,7 @@ __global__ void kBoundary(Dev<R> d, int numReal, NarrowP<R> P, int* cntP, int* c
   const long warp = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const long nwarps = ((long)gridDim.x * blockDim.x) >> 5;
   const int K = sd.numPoints > 0 ? sd.numPoints : 1;
+  R mo = R(0);
   for (long i = warp; i < numReal; i += nwarps) {
     const R s = d.scale[i] * P.globalScale;
     int run = MODE ? basePlanes + offP[i] : 0, tot = 0;
@@ -233,7 +240,7 @@ __global__ void kBoundary(Dev<R> d, int numReal, NarrowP<R> P, int* cntP, int* c
         if (k < K) {
           b = probePlane(d, (int)i, pl, k, sd, s, P.margin);
           if (MODE == 0 && b.dist < R(0))
-            atomicMaxNonNeg(&d.ctr->maxOverlap, -b.dist);
+            runMax(mo, -b.dist);
         }
         const unsigned m = __ballot_sync(0xffffffffu, b.hit);
         if (MODE == 1 && b.hit) {
@@ -256,7 +263,7 @@ __global__ void kBoundary(Dev<R> d, int numReal, NarrowP<R> P, int* cntP, int* c
         if (k < K) {
           b = probeWall(d, (int)i, wi, k, sd, s, P.margin, MODE == 1);
           if (MODE == 0 && b.dist < R(0))
-            atomicMaxNonNeg(&d.ctr->maxOverlap, -b.dist);
+            runMax(mo, -b.dist);
         }
         const unsigned m = __ballot_sync(0xffffffffu, b.hit);
         if (MODE == 1 && b.hit) {
@@ -270,6 +277,8 @@ __global__ void kBoundary(Dev<R> d, int numReal, NarrowP<R> P, int* cntP, int* c
     if (MODE == 0 && lane == 0)
       cntW[i] = tot;
   }
+  if (MODE == 0)
+    warpMaxAtomic(&d.ctr->maxOverlap, mo);
 }
 
 // =============================================================================================

@@ -185,10 +185,9 @@ __global__ void kGrowthScales(Dev<R> d, int n, R factor) {
 // sim.hpp:61-70 partial: max scale over [0, n) (non-negative scales; order-free max)
 template <class R>
 __global__ void kMaxScale(Dev<R> d, int n, R* out) {
-  GRID_STRIDE(i, n) {
-    const R s = d.scale[i];
-    atomicMaxNonNeg(out, s);
-  }
+  R m = R(0);
+  GRID_STRIDE(i, n) runMax(m, d.scale[i]);
+  warpMaxAtomic(out, m);
 }
 
 // per-detection counter reset; maxApproach persists across substeps like the reference's View

@@ -474,6 +474,7 @@ template <class R>
 void Sim<R>::setPositions(const R* xyz, int n) {
   if (n > capacity_)
     throw std::invalid_argument("set_positions: more particles than the simulation capacity");
+  ensureGrounded();  // the logged support graphs index the previous particle set
   numReal_ = n;
   numParticles_ = n;
   hzNumPairs_ = -1;
@@ -684,7 +685,7 @@ int Sim<R>::findCollisions(R margin, int cap) {
   ++launches_, kRopes<<<gridFor(2 * n - 1), kBlock, 0, stream_>>>(bb);
   KCHECK("ropes");
   cudaCheck(cudaMemsetAsync(qcnt_.p, 0, (numReal_ + 1) * sizeof(int), stream_), "memset");
-  ++launches_, kQuery<R, 0><<<gridFor(numReal_, 128), 128, 0, stream_>>>(d_, numReal_, bb, bn, qcnt_.p, nullptr, nullptr, 0);
+  ++launches_, kQuery<R, 0><<<gridFor(n, 128), 128, 0, stream_>>>(d_, numReal_, bb, bn, qcnt_.p, nullptr, nullptr, 0);
   KCHECK("query count");
   exclusiveSum(qcnt_.p, qoff_.p, numReal_ + 1);
   int total = 0, err = 0;
@@ -694,7 +695,7 @@ int Sim<R>::findCollisions(R margin, int cap) {
   if (err)
     throw std::runtime_error("broadphase: BVH traversal exceeded its iteration bound (corrupt tree)");
   if (total <= cap) {
-    ++launches_, kQuery<R, 1><<<gridFor(numReal_, 128), 128, 0, stream_>>>(d_, numReal_, bb, bn, nullptr, qoff_.p, pairs_.p, cap);
+    ++launches_, kQuery<R, 1><<<gridFor(n, 128), 128, 0, stream_>>>(d_, numReal_, bb, bn, nullptr, qoff_.p, pairs_.p, cap);
     KCHECK("query write");
     ++launches_, kSortPairLists<<<gridFor(numReal_), kBlock, 0, stream_>>>(numReal_, qoff_.p, pairs_.p, cap);
     KCHECK("pair sort");
@@ -961,31 +962,14 @@ void Sim<R>::demStep() {
   if (usePGS && nm > 0) {
     ++launches_, kGatherWarm<<<gridFor(nm), B, 0, s>>>(d_, nm, prevPairCount_);
     KCHECK("gather warm");
-    if (numReal_ > 0) {
-      ++launches_, kGroundDecay<<<gridFor(numReal_), B, 0, s>>>(d_, numReal_, 8);
-      edges_.ensure(nm, false, s);
-      ++launches_, kGroundEdges<<<gridFor(nm), B, 0, s>>>(d_, nm, gHat, edges_.p);
-      const bool smem = (size_t)numReal_ * sizeof(int) <= 200 * 1024;
-      if (!smem)
-        gscratch_.ensure(numReal_, false, s);
-      static bool attr = false;
-      if (!attr) {
-        cudaFuncSetAttribute(kGroundSweeps, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-        attr = true;
-      }
-      ++launches_, kGroundSweeps<<<1, 32, smem ? numReal_ * sizeof(int) : 0, s>>>(nm, numReal_, 8, edges_.p, grounded_.p,
-                                                                     gscratch_.p, smem ? 1 : 0);
-      KCHECK("grounded");
-    }
+    logSupportGraph(nm, gHat);
     sideFlags_.zero(s, nm);
     ++launches_, kVn0<<<gridFor(nm), B, 0, s>>>(d_, nm, gr_);
     ++launches_, kWarmApply<<<gridFor(numReal_), B, 0, s>>>(d_, numReal_, incM);
     ++launches_, kWarmProject<<<gridFor(nm), B, 0, s>>>(d_, nm);
     KCHECK("warm start");
   } else if (usePGS) {
-    // no manifolds: the reference still decays the support levels
-    if (numReal_ > 0)
-      ++launches_, kGroundDecay<<<gridFor(numReal_), B, 0, s>>>(d_, numReal_, 8);
+    logSupportGraph(0, gHat);  // no manifolds: the levels still decay this substep
   }
   mark(ST_VELOCITY);
   SolveP<R> sp{gr_, eN_, eT_, mu_, R(0), dt_, ncolV};
@@ -1035,9 +1019,14 @@ void Sim<R>::demStep() {
       throw std::runtime_error("stabilization modes 'multilevel' and 'ordered' are not supported by the B200 step");
     }
     ++launches_, kCtl<<<1, 1, 0, s>>>(ctr_.p, CTL_STAB_DECIDE, vRestS, stabMode_);
-    if (stabMode_ == 1 || stabMode_ == 3) {
-      if (stabMode_ == 1 && nm > 0)
+    // the pass runs only when the main sweeps left a residual (src/sim.hpp:282): read the
+    // decision so an untriggered pass costs nothing
+    const bool stabRun = (stabMode_ == 1 || stabMode_ == 3) && readCounters().stabRun;
+    if (stabRun) {
+      if (stabMode_ == 1 && nm > 0) {
+        ensureGrounded();
         ++launches_, kSideFlags<<<gridFor(nm), B, 0, s>>>(d_, nm, gHat, R(8) * dt_ * gMag, R(8) * dt_ * gMag);
+      }
       SolveP<R> ss = sp;
       ss.vRest = vRestS;
       const int iters = stabMode_ == 1 ? 2 * velIters_ : 256;
@@ -1322,6 +1311,7 @@ long Sim<R>::getLedger(unsigned long long* keys, double* vals, long cap) {
 }
 template <class R>
 long Sim<R>::getGrounded(int* out, long cap) {
+  ensureGrounded();
   const long n = numReal_;
   const auto h = d2h(grounded_.p, n, stream_);
   for (long i = 0; i < n && i < cap; ++i)
@@ -1527,6 +1517,60 @@ long Sim<R>::getHertz(unsigned long long* keys, double* xi, long cap) {
     xi[3 * i + 2] = x[i].z;
   }
   return n;
+}
+
+// ---- support levels (src/contact_preprocessing.hpp:213-253), evaluated lazily ----
+// Each substep of the PGS path decays every level by 8 and then runs 8 serial sweeps over that
+// substep's support graph. A level is at most 255, so anything older than 32 logged substeps has
+// decayed to 0: the levels are a function of the last 32 support graphs alone. They are read only
+// by the one-sided stabilization pass, so each substep just records its graph in a 32-slot ring and
+// the sweeps are replayed (from the last checkpoint, or from zero over the last 32 graphs) only when
+// the pass needs the levels. The result is identical to sweeping every substep.
+template <class R>
+void Sim<R>::logSupportGraph(int nm, V3<R> gHat) {
+  const int slot = (int)(gLog_ % kGroundRing);
+  gRingNm_[slot] = nm;
+  gRingReal_[slot] = numReal_;
+  if (nm > 0) {
+    gRing_[slot].ensure(nm, false, stream_);
+    ++launches_, kGroundEdges<<<gridFor(nm), kBlock, 0, stream_>>>(d_, nm, gHat, gRing_[slot].p);
+    KCHECK("support graph");
+  }
+  ++gLog_;
+}
+template <class R>
+void Sim<R>::ensureGrounded() {
+  long pending = gLog_ - gCheckpoint_;
+  if (pending <= 0)
+    return;
+  long start = gCheckpoint_;
+  if (pending > kGroundRing) {
+    start = gLog_ - kGroundRing;
+    const int nr = gRingReal_[start % kGroundRing];
+    if (nr > 0)
+      cudaCheck(cudaMemsetAsync(grounded_.p, 0, nr, stream_), "memset");
+  }
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(kGroundSweeps, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    attr = true;
+  }
+  for (long e = start; e < gLog_; ++e) {
+    const int slot = (int)(e % kGroundRing);
+    const int nr = gRingReal_[slot], nm = gRingNm_[slot];
+    if (nr <= 0)
+      continue;
+    ++launches_, kGroundDecay<<<gridFor(nr), kBlock, 0, stream_>>>(d_, nr, 8);
+    if (nm > 0) {
+      const bool smem = (size_t)nr * sizeof(int) <= 200 * 1024;
+      if (!smem)
+        gscratch_.ensure(nr, false, stream_);
+      ++launches_, kGroundSweeps<<<1, 32, smem ? nr * sizeof(int) : 0, stream_>>>(nm, nr, 8, gRing_[slot].p,
+                                                                                grounded_.p, gscratch_.p, smem);
+    }
+    KCHECK("support sweeps");
+  }
+  gCheckpoint_ = gLog_;
 }
 
 // ---- instrumentation ----

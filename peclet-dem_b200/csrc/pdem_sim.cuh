@@ -191,7 +191,10 @@ class Sim {
   DBuf<unsigned> uA_, uB_;
   DBuf<R> rA_, rB2_;
   DBuf<Q4<R>> qA_, qB_, qC_;
-  DBuf<int4> edges_;
+  static constexpr int kGroundRing = 32;  // 255 / 8 < 32 substeps of decay erase any level
+  DBuf<int4> gRing_[kGroundRing];
+  int gRingNm_[kGroundRing] = {}, gRingReal_[kGroundRing] = {};
+  long gLog_ = 0, gCheckpoint_ = 0;
   DBuf<int> gscratch_;
   DBuf<double> thermo_;
   // broadphase scratch
@@ -238,6 +241,8 @@ class Sim {
   int colorGraph(bool manifold, int ne, int nb, int& leftover);
   void colorOrder(bool manifold, int ne, int ncol);
   void buildIncidence(int kind, int ne, int nb);
+  void logSupportGraph(int nm, V3<R> gHat);
+  void ensureGrounded();
   void demStep();
   Counters<R> readCounters();
   template <class T>

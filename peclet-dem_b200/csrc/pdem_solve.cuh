@@ -294,6 +294,7 @@ __global__ void kPGSColor(Dev<R> d, const int* order, const int* coff, int color
   const bool serial = color >= kSaturatedColor;
   if (serial && (blockIdx.x | threadIdx.x))
     return;
+  R mx = R(0);
   for (long t = serial ? 0 : (long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
        t += serial ? 1 : (long)gridDim.x * blockDim.x) {
     const int idx = order[b + t];
@@ -354,7 +355,7 @@ __global__ void kPGSColor(Dev<R> d, const int* order, const int* coff, int color
     V3<R> vA2 = vA, wA2 = wA, vB2 = vB, wB2 = wB;
     if (dA != R(0)) {
       d.lambda[idx] = pNew;
-      atomicMaxNonNeg(&d.ctr->maxApproach, fabs(dA) * wT / lenN);
+      runMax(mx, fabs(dA) * wT / lenN);
       const R lam = -sgn * dA;
       const V3<R> J = mul(v.N, lam), JA = mul(v.TA, lam), JB = mul(v.TB, lam);
       if (applyA) {
@@ -412,7 +413,7 @@ __global__ void kPGSColor(Dev<R> d, const int* order, const int* coff, int color
         d.lambdaT[idx] = q4(ltNew);
         const R dl = sqrt(dot(dd, dd));
         if (wTt > R(1e-9))
-          atomicMaxNonNeg(&d.ctr->maxApproach, dl * wTt);
+          runMax(mx, dl * wTt);
         if (applyA) {
           vA2 = add(vA2, mul(dd, v.imA));
           wA2 = add(wA2, angResponse(v.qA, cross(v.rAa, dd), v.iIA));
@@ -430,6 +431,10 @@ __global__ void kPGSColor(Dev<R> d, const int* order, const int* coff, int color
       d.angVelPred[rb] = q4(wB2);
     }
   }
+  if (serial)
+    atomicMaxNonNeg(&d.ctr->maxApproach, mx);
+  else
+    warpMaxAtomic(&d.ctr->maxApproach, mx);
 }
 
 // one-shot coloured GS of one colour, g = 0 path (src/solver_velocity.hpp:989-1137)
@@ -443,6 +448,7 @@ __global__ void kGSColor(Dev<R> d, const int* order, const int* coff, int color,
   const bool serial = color >= kSaturatedColor;
   if (serial && (blockIdx.x | threadIdx.x))
     return;
+  R mx = R(0);
   for (long t = serial ? 0 : (long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
        t += serial ? 1 : (long)gridDim.x * blockDim.x) {
     const int idx = order[b + t];
@@ -482,7 +488,7 @@ __global__ void kGSColor(Dev<R> d, const int* order, const int* coff, int color,
     const R wT = wAn + wBn;
     if (wT <= R(0))
       continue;
-    atomicMaxNonNeg(&d.ctr->maxApproach, fabs(vn) / lenN);
+    runMax(mx, fabs(vn) / lenN);
     if (fabs(vn) < P.vRest * lenN)
       e = R(0);
     const R lam = (-e * vn - vn) / wT;
@@ -494,6 +500,10 @@ __global__ void kGSColor(Dev<R> d, const int* order, const int* coff, int color,
       d.angVelPred[v.rb] = q4(add(wB, angResponse(v.qB, JB, v.iIB)));
     }
   }
+  if (serial)
+    atomicMaxNonNeg(&d.ctr->maxApproach, mx);
+  else
+    warpMaxAtomic(&d.ctr->maxApproach, mx);
 }
 
 // Jacobi velocity solve (src/solver_velocity.hpp:38-226), gathered per real body; filt selects the
@@ -815,6 +825,7 @@ __global__ void kPosGSColor(Dev<R> d, const int* order, const int* coff, int col
   const bool serial = color >= kSaturatedColor;
   if (serial && (blockIdx.x | threadIdx.x))
     return;
+  R mx = R(0);
   for (long t = serial ? 0 : (long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
        t += serial ? 1 : (long)gridDim.x * blockDim.x) {
     const int idx = order[b + t];
@@ -835,8 +846,12 @@ __global__ void kPosGSColor(Dev<R> d, const int* order, const int* coff, int col
       const V3<R> pB = v3(d.posPred[B]);
       d.posPred[B] = q4(add(pB, V3<R>{-nv.x * dl * imB, -nv.y * dl * imB, -nv.z * dl * imB}));
     }
-    atomicMaxNonNeg(&d.ctr->maxOverlap, -C);
+    runMax(mx, -C);
   }
+  if (serial)
+    atomicMaxNonNeg(&d.ctr->maxOverlap, mx);
+  else
+    warpMaxAtomic(&d.ctr->maxOverlap, mx);
 }
 // Jacobi position solve (src/solver_position.hpp:34-134): per-contact correction pre-pass, then a
 // gather per body slot in contact order
