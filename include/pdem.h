@@ -165,6 +165,19 @@ int pdem_profile_read(pdem_handle h, double* ms, long* calls, int cap, long* lau
 /* sweeps executed since profile_enable: velocity, stabilization, position; and substeps */
 int pdem_debug_sweeps(pdem_handle h, long* out4);
 
+/* ---- candidate pairs without allocation (no counterpart in the reference) ----
+ * The broadphase of the step (same predicate and canonical (i, j) order as the pair list that
+ * pdem_compute_overlaps builds) over caller-owned DEVICE arrays: d_xyz (n x 3 doubles), d_radius (n
+ * doubles); pairs go to d_pairs (pair_cap x 2 ints), their number to *out_count (when it exceeds
+ * pair_cap nothing is written). All scratch is a fixed static device buffer: this call allocates
+ * no device or pinned memory, so callers that own the whole device memory budget can use it.
+ * n is at most 16384 (PDEM_ERR_INVALID above). The first call on a device does a one-time set-up
+ * and should come before any stream capture; calls that overlap in time share the scratch and
+ * race. Work is ordered on `stream` (a cudaStream_t, NULL = default stream); the call returns
+ * after synchronising it. */
+int pdem_find_pairs_static(const double* d_xyz, const double* d_radius, int n, double margin, double box_cap,
+                           int* d_pairs, long pair_cap, long* out_count, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

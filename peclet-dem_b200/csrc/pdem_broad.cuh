@@ -153,7 +153,7 @@ __device__ __forceinline__ int deltaKey(const u64* k, int n, int i, int j) {
 }
 
 // Karras 2012: internal node i of n-1; leaves are nodes n-1 .. 2n-2
-__global__ void kKarras(BvhBuffers bb) {
+static __global__ void kKarras(BvhBuffers bb) {
   const int n = bb.n;
   GRID_STRIDE(ii, n - 1) {
     const int i = (int)ii;
@@ -236,7 +236,7 @@ __global__ void kRefit(BvhBuffers bb, BvhNodes<R> bn) {
 
 // escape link of every node: the right sibling of the nearest ancestor-or-self that is a left
 // child (-1 past the last leaf)
-__global__ void kRopes(BvhBuffers bb) {
+static __global__ void kRopes(BvhBuffers bb) {
   const int n = bb.n;
   GRID_STRIDE(v, 2 * n - 1) {
     int cur = (int)v, r = -1;
@@ -300,7 +300,7 @@ __global__ void kQuery(Dev<R> d, int numReal, BvhBuffers bb, BvhNodes<R> bn, int
 }
 
 // sort each query's list by j (insertion sort; lists are short)
-__global__ void kSortPairLists(int numReal, const int* off, int2* pairs, int cap) {
+static __global__ void kSortPairLists(int numReal, const int* off, int2* pairs, int cap) {
   GRID_STRIDE(ii, numReal) {
     const int b = off[ii], e = min(off[ii + 1], cap);
     for (int x = b + 1; x < e; ++x) {

@@ -130,6 +130,11 @@ void fetch(S& s, int field, int cols, std::vector<double>& out) {
 }
 }  // namespace
 
+namespace pdem {
+// message of the last failing entry point, for entry points defined in other translation units
+void setLastError(const std::string& msg) { g_err = msg; }
+}  // namespace pdem
+
 extern "C" {
 
 const char* pdem_last_error(void) { return g_err.c_str(); }

@@ -102,6 +102,8 @@ _SIGS = {
     "profile_enable": (C.c_int, [_vp, C.c_int]),
     "profile_read": (C.c_int, [_vp, _dbl_p, _long_p, C.c_int, _long_p]),
     "debug_sweeps": (C.c_int, [_vp, _long_p]),
+    # candidate pairs over caller-owned device arrays, with no allocation (pdem_static.cu)
+    "find_pairs_static": (C.c_int, [_vp, _vp, C.c_int, C.c_double, C.c_double, _vp, C.c_long, _long_p, _vp]),
 }
 
 STAGES = ("predict", "ghosts", "broadphase", "narrowphase", "manifolds", "colour_velocity", "warm_start",
