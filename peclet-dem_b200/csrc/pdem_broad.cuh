@@ -316,3 +316,231 @@ static __global__ void kSortPairLists(int numReal, const int* off, int2* pairs, 
 }
 
 }  // namespace pdem
+
+namespace pdem {
+
+// =============================================================================================
+// Packed tree for the single-pass query. Every node (internal 0..n-2, leaf n-1+k for sorted
+// position k) is one 32-byte record: a float box rounded outward (it contains the exact box, so a
+// miss on it is a miss on the exact box), the first child (internal) or -(j + 1) for the primitive
+// j (leaf), and the escape link. The traversal tests the float box; a leaf hit is confirmed on the
+// primitive's exact box in R, so the candidate set is exactly the reference predicate.
+// =============================================================================================
+struct __align__(16) PNode {
+  float lo[3], hi[3];
+  int a;     // internal: left child; leaf: -(primitive + 1)
+  int rope;  // escape link (-1 past the last leaf)
+};
+
+__device__ __forceinline__ float roundDown(double v) { return __double2float_rd(v); }
+__device__ __forceinline__ float roundUp(double v) { return __double2float_ru(v); }
+__device__ __forceinline__ float roundDown(float v) { return v; }
+__device__ __forceinline__ float roundUp(float v) { return v; }
+
+template <class R>
+__device__ __forceinline__ void outwardBox(const Box<R>& b, float lo[3], float hi[3]) {
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    lo[a] = roundDown(b.lo[a]);
+    hi[a] = roundUp(b.hi[a]);
+  }
+}
+__device__ __forceinline__ bool overlapF(const float qlo[3], const float qhi[3], const PNode& n) {
+  return !(qlo[0] > n.hi[0] || qhi[0] < n.lo[0] || qlo[1] > n.hi[1] || qhi[1] < n.lo[1] || qlo[2] > n.hi[2] ||
+           qhi[2] < n.lo[2]);
+}
+__device__ __forceinline__ PNode loadNode(const PNode* p) {
+  const float4* s = reinterpret_cast<const float4*>(p);
+  const float4 u = __ldg(s), v = __ldg(s + 1);
+  PNode n;
+  n.lo[0] = u.x, n.lo[1] = u.y, n.lo[2] = u.z, n.hi[0] = u.w;
+  n.hi[1] = v.x, n.hi[2] = v.y;
+  n.a = __float_as_int(v.z);
+  n.rope = __float_as_int(v.w);
+  return n;
+}
+
+// leaves in sorted order: outward float box of the primitive and its index
+template <class R>
+__global__ void kPackLeaves(BvhBuffers bb, const Box<R>* prim, PNode* nodes) {
+  const int n = bb.n;
+  GRID_STRIDE(k, n) {
+    const int j = bb.idx[k];
+    PNode p;
+    outwardBox(prim[j], p.lo, p.hi);
+    p.a = -(j + 1);
+    p.rope = -1;
+    nodes[n - 1 + k] = p;
+  }
+}
+
+// bottom-up union of the float boxes; the second child to arrive at a node computes it
+static __global__ void kRefitPacked(BvhBuffers bb, PNode* nodes) {
+  const int n = bb.n;
+  GRID_STRIDE(k, n) {
+    int node = bb.parent[n - 1 + (int)k];
+    for (int guard = 0;; ++guard) {
+      if (guard > n) {  // deeper than the number of primitives: corrupt tree, stop
+        atomicOr(&bb.err[0], 1);
+        break;
+      }
+      __threadfence();
+      if (atomicAdd(&bb.flag[node], 1) == 0)
+        break;
+      __threadfence();
+      const int c0 = bb.left[node], c1 = bb.right[node];
+      float lo[3], hi[3];
+      const float* b0 = reinterpret_cast<const float*>(&nodes[c0]);
+      const float* b1 = reinterpret_cast<const float*>(&nodes[c1]);
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        lo[a] = fminf(__ldcg(b0 + a), __ldcg(b1 + a));
+        hi[a] = fmaxf(__ldcg(b0 + 3 + a), __ldcg(b1 + 3 + a));
+      }
+      float* dst = reinterpret_cast<float*>(&nodes[node]);
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        __stcg(dst + a, lo[a]);
+        __stcg(dst + 3 + a, hi[a]);
+      }
+      if (node == 0)
+        break;
+      node = bb.parent[node];
+    }
+  }
+}
+
+// escape links of all nodes, and the first child of internal nodes
+static __global__ void kRopesPacked(BvhBuffers bb, PNode* nodes) {
+  const int n = bb.n;
+  GRID_STRIDE(v, 2 * n - 1) {
+    int cur = (int)v, r = -1;
+    for (int guard = 0; cur != 0; ++guard) {
+      if (guard > n) {
+        atomicOr(&bb.err[0], 1);
+        break;
+      }
+      const int p = bb.parent[cur];
+      if (bb.left[p] == cur) {
+        r = bb.right[p];
+        break;
+      }
+      cur = p;
+    }
+    nodes[v].rope = r;
+    if (v < n - 1)
+      nodes[v].a = bb.left[v];
+  }
+}
+
+// Half traversal: the query at sorted position kk starts at its own leaf's escape link, so it
+// visits only subtrees of sorted positions > kk and every overlapping unordered pair is found
+// exactly once, by its lower sorted position. A found pair {i, j} belongs to row a = min(i, j)
+// (kept when a is real); its rank in the row is taken with an atomic on the row count and kept,
+// with the partner, in the query's own slots. The scatter pass places each pair at row offset +
+// rank and the per-row sort by j restores the canonical (i, j) order, so the result does not
+// depend on the order of the atomics. A query with more than kSlots pairs raises `overflow`; the
+// host then runs the full two-pass traversal instead.
+constexpr int kSlots = 32;
+
+template <class R>
+__global__ void kQueryHalf(BvhBuffers bb, const Box<R>* prim, const PNode* nodes, int numReal, int* rowCnt,
+                           int* qcnt, int2* slots, int* overflow) {
+  const int n = bb.n;
+  GRID_STRIDE(kk, n) {
+    const PNode self = loadNode(&nodes[n - 1 + kk]);
+    const int i = -self.a - 1;
+    const Box<R> q = prim[i];
+    float qlo[3], qhi[3];
+    outwardBox(q, qlo, qhi);
+    int c = 0;
+    int node = self.rope;
+    for (long guard = 0; node != -1; ++guard) {
+      if (guard > 2L * n + 8) {  // each node is visited at most once
+        atomicOr(&bb.err[0], 1);
+        break;
+      }
+      const PNode nd = loadNode(&nodes[node]);
+      if (overlapF(qlo, qhi, nd)) {
+        if (nd.a >= 0) {
+          node = nd.a;
+          continue;
+        }
+        const int j = -nd.a - 1;
+        if (boxOverlap(q, prim[j])) {
+          const int lo = i < j ? i : j;
+          if (lo < numReal) {
+            if (c < kSlots)
+              slots[(long)kk * kSlots + c] = make_int2(j, atomicAdd(&rowCnt[lo], 1));
+            ++c;
+          }
+        }
+      }
+      node = nd.rope;
+    }
+    qcnt[kk] = c;
+    if (c > kSlots)
+      *overflow = 1;
+  }
+}
+
+// place every found pair at its row offset + rank
+static __global__ void kScatterHalf(BvhBuffers bb, const int* qcnt, const int2* slots, const int* rowOff, int2* out,
+                             int outCap) {
+  GRID_STRIDE(kk, bb.n) {
+    const int c = min(qcnt[kk], kSlots);
+    if (c == 0)
+      continue;
+    const int i = bb.idx[kk];
+    for (int t = 0; t < c; ++t) {
+      const int2 s = slots[(long)kk * kSlots + t];
+      const int lo = i < s.x ? i : s.x, hi = i < s.x ? s.x : i;
+      const int p = rowOff[lo] + s.y;
+      if (p < outCap)
+        out[p] = make_int2(lo, hi);
+    }
+  }
+}
+
+// Full traversal from the root for real particle i = idx[kk] (used when a half-traversal query
+// overflowed its slots): MODE 0 counts the partners j > i, MODE 1 writes them at off[i].
+template <class R, int MODE>
+__global__ void kQueryFull(BvhBuffers bb, const Box<R>* prim, const PNode* nodes, int numReal, int* cnt,
+                           const int* off, int2* out, int outCap) {
+  const int n = bb.n;
+  GRID_STRIDE(kk, n) {
+    const int i = bb.idx[kk];
+    if (i >= numReal)
+      continue;
+    const Box<R> q = prim[i];
+    float qlo[3], qhi[3];
+    outwardBox(q, qlo, qhi);
+    int c = 0;
+    const int base = MODE ? off[i] : 0;
+    int node = 0;
+    for (long guard = 0; node != -1; ++guard) {
+      if (guard > 2L * n + 8) {
+        atomicOr(&bb.err[0], 1);
+        break;
+      }
+      const PNode nd = loadNode(&nodes[node]);
+      if (overlapF(qlo, qhi, nd)) {
+        if (nd.a >= 0) {
+          node = nd.a;
+          continue;
+        }
+        const int j = -nd.a - 1;
+        if (j > i && boxOverlap(q, prim[j])) {
+          if (MODE && base + c < outCap)
+            out[base + c] = make_int2(i, j);
+          ++c;
+        }
+      }
+      node = nd.rope;
+    }
+    if (!MODE)
+      cnt[i] = c;
+  }
+}
+
+}  // namespace pdem

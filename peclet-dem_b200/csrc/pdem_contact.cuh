@@ -73,6 +73,10 @@ __global__ void kNarrowSphere(Dev<R> d, int np, NarrowP<R> P, int* cnt, const in
   const ShapeDesc<R> dA = d.shapes[0], dB = d.shapes[0];
   R mo = R(0);
   GRID_STRIDE(idx, np) {
+    // the write pass revisits only the pairs the count pass found in contact (off[idx + 1] is
+    // the exclusive scan of the 0/1 counts)
+    if (MODE == 1 && off[idx + 1] == off[idx])
+      continue;
     const int2 pr = d.pairs[idx];
     const Probe<R> p = probeBody(d, pr.x, pr.y, 0, dA, dB, P.globalScale);
     const bool hit = p.eff < P.margin;
@@ -275,6 +279,48 @@ __global__ void kBoundary(Dev<R> d, int numReal, NarrowP<R> P, int* cntP, int* c
         tot += __popc(m);
       }
     if (MODE == 0 && lane == 0)
+      cntW[i] = tot;
+  }
+  if (MODE == 0)
+    warpMaxAtomic(&d.ctr->maxOverlap, mo);
+}
+
+// single-point shapes (spheres): one thread per particle, same slots as kBoundary
+template <class R, int MODE>
+__global__ void kBoundarySphere(Dev<R> d, int numReal, NarrowP<R> P, int* cntP, int* cntW, const int* offP,
+                                const int* offW, int basePlanes, int baseWalls) {
+  const ShapeDesc<R> sd = d.shapes[0];
+  R mo = R(0);
+  GRID_STRIDE(i, numReal) {
+    const R s = d.scale[i] * P.globalScale;
+    int run = MODE ? basePlanes + offP[i] : 0, tot = 0;
+    for (int pl = 0; pl < P.numPlanes; ++pl) {
+      const BoundaryProbe<R> b = probePlane(d, (int)i, pl, 0, sd, s, P.margin);
+      if (MODE == 0 && b.dist < R(0))
+        runMax(mo, -b.dist);
+      if (b.hit) {
+        if (MODE == 1 && run < d.maxContacts)
+          writeBoundaryContact(d, run, (int)i, b, false, 0, 0);
+        ++run;
+        ++tot;
+      }
+    }
+    if (MODE == 0)
+      cntP[i] = tot;
+    run = MODE ? baseWalls + offW[i] : 0;
+    tot = 0;
+    for (int wi = 0; wi < P.numWalls; ++wi) {
+      const BoundaryProbe<R> b = probeWall(d, (int)i, wi, 0, sd, s, P.margin, MODE == 1);
+      if (MODE == 0 && b.dist < R(0))
+        runMax(mo, -b.dist);
+      if (b.hit) {
+        if (MODE == 1 && run < d.maxContacts)
+          writeBoundaryContact(d, run, (int)i, b, true, wi, P.haveMat);
+        ++run;
+        ++tot;
+      }
+    }
+    if (MODE == 0)
       cntW[i] = tot;
   }
   if (MODE == 0)
@@ -646,7 +692,7 @@ __global__ void kColorStats(int ne, const int* col, int* maxColor, int* leftover
 __global__ void kColorSortKeys(int ne, const int* col, unsigned* keys, int* vals) {
   GRID_STRIDE(i, ne) {
     const int c = col[i];
-    keys[i] = (c >= 0) ? (unsigned)c : 0xFFFFFFFFu;
+    keys[i] = (c >= 0) ? (unsigned)c : 63u;  // colours are 0..62; 63 sorts the uncoloured last
     vals[i] = (int)i;
   }
 }

@@ -12,6 +12,7 @@
 #include "pdem_contact.cuh"
 #include "pdem_hertz.cuh"
 #include "pdem_kernels.cuh"
+#include "pdem_persist.cuh"
 #include "pdem_shell.hpp"
 #include "pdem_sim.cuh"
 #include "pdem_solve.cuh"
@@ -27,6 +28,15 @@ void cudaCheck(cudaError_t e, const char* what) {
 template <class R>
 Sim<R>::Sim(int capacity) {
   cudaCheck(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+  {
+    int dev = 0;
+    cudaCheck(cudaGetDevice(&dev), "cudaGetDevice");
+    cudaCheck(cudaDeviceGetAttribute(&numSMs_, cudaDevAttrMultiProcessorCount, dev), "SM count");
+    int coop = 0;
+    cudaCheck(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev), "cooperative launch attribute");
+    if (!coop)
+      throw CudaError("device does not support cooperative launches");
+  }
   for (int i = 0; i < 8; ++i) {
     hzE_[i] = R(1.0e9);
     hzNu_[i] = R(0.25);
@@ -156,7 +166,31 @@ Counters<R> Sim<R>::readCounters() {
   Counters<R> c;
   cudaCheck(cudaMemcpyAsync(&c, ctr_.p, sizeof c, cudaMemcpyDeviceToHost, stream_), "D2H counters");
   sync();
+  if (c.err & kErrBarrier)
+    throw CudaError("a grid-wide barrier of a persistent loop timed out (blocks not co-resident)");
   return c;
+}
+
+// blocks of a cooperative launch of `kernel`: resident blocks per SM (at most 4) x SMs
+template <class R>
+template <class K>
+int Sim<R>::coopGrid(K kernel) {
+  int per = 0;
+  cudaCheck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kBlock, 0), "occupancy");
+  if (per < 1)
+    throw CudaError("persistent loop kernel cannot be resident");
+  return std::min(per, 4) * numSMs_;
+}
+template <class R>
+template <class K, class... A>
+void Sim<R>::launchCoop(K kernel, A... args) {
+  gbar_.ensure(2, false, stream_);
+  cudaCheck(cudaMemsetAsync(gbar_.p, 0, 2 * sizeof(unsigned), stream_), "memset barrier");
+  void* argv[] = {static_cast<void*>(&args)...};
+  ++launches_;
+  cudaCheck(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(kernel), dim3(coopGrid(kernel)), dim3(kBlock),
+                                        argv, 0, stream_),
+            "cooperative launch");
 }
 
 // ---- CUB helpers ----
@@ -640,7 +674,8 @@ void Sim<R>::resetGhosts(R band) {
     numParticles_ = std::min(numReal_ + total, capacity_);
   }
 }
-// broadphase over numParticles_ boxes of positions P with margin; pairs into pairs_ (cap entries)
+// broadphase over numParticles_ boxes of the predicted positions with margin; pairs into pairs_
+// (cap entries). Returns the number of candidates, which may exceed cap (nothing written then).
 template <class R>
 int Sim<R>::findCollisions(R margin, int cap) {
   const int n = numParticles_;
@@ -648,7 +683,7 @@ int Sim<R>::findCollisions(R margin, int cap) {
   if (n < 2 || numReal_ <= 0)
     return 0;
   bvhBoxes_.ensure(sizeof(Box<R>) * n, false, stream_);
-  bvhNodes_.ensure(sizeof(Box<R>) * n, false, stream_);
+  bvhNodes_.ensure(sizeof(PNode) * (2 * (size_t)n - 1), false, stream_);
   codes_.ensure(n, false, stream_);
   codesAlt_.ensure(n, false, stream_);
   bidx_.ensure(n, false, stream_);
@@ -656,16 +691,19 @@ int Sim<R>::findCollisions(R margin, int cap) {
   left_.ensure(n, false, stream_);
   right_.ensure(n, false, stream_);
   parent_.ensure(2 * n, false, stream_);
-  rope_.ensure(2 * n, false, stream_);
   flag_.ensure(n, false, stream_);
   bounds_.ensure(6, false, stream_);
-  qcnt_.ensure(numReal_ + 1, false, stream_);
+  qcnt_.ensure(n, false, stream_);
   qoff_.ensure(numReal_ + 1, false, stream_);
-  BvhNodes<R> bn{reinterpret_cast<Box<R>*>(bvhBoxes_.p), reinterpret_cast<Box<R>*>(bvhNodes_.p)};
+  rowCnt_.ensure(numReal_ + 1, false, stream_);
+  slots_.ensure((size_t)n * kSlots, false, stream_);
+  Box<R>* prim = reinterpret_cast<Box<R>*>(bvhBoxes_.p);
+  PNode* nodes = reinterpret_cast<PNode*>(bvhNodes_.p);
+  BvhNodes<R> bn{prim, nullptr};
   BvhBuffers bb;
   bb.n = n;
   bb.codes = codes_.p, bb.codesAlt = codesAlt_.p, bb.idx = bidx_.p, bb.idxAlt = bidxAlt_.p;
-  bb.left = left_.p, bb.right = right_.p, bb.parent = parent_.p, bb.rope = rope_.p, bb.flag = flag_.p;
+  bb.left = left_.p, bb.right = right_.p, bb.parent = parent_.p, bb.rope = nullptr, bb.flag = flag_.p;
   bb.bounds = bounds_.p;
   bb.err = &ctr_.p->err;
   const u64 init[6] = {~0ull, ~0ull, ~0ull, 0ull, 0ull, 0ull};
@@ -678,25 +716,50 @@ int Sim<R>::findCollisions(R margin, int cap) {
   std::swap(bb.codes, bb.codesAlt);
   std::swap(bb.idx, bb.idxAlt);
   cudaCheck(cudaMemsetAsync(flag_.p, 0, n * sizeof(int), stream_), "memset");
+  cudaCheck(cudaMemsetAsync(rowCnt_.p, 0, (numReal_ + 1) * sizeof(int), stream_), "memset");
+  bflag_.ensure(1, false, stream_);
+  cudaCheck(cudaMemsetAsync(bflag_.p, 0, sizeof(int), stream_), "memset");
   ++launches_, kKarras<<<gridFor(n - 1), kBlock, 0, stream_>>>(bb);
   KCHECK("karras");
-  ++launches_, kRefit<R><<<gridFor(n), kBlock, 0, stream_>>>(bb, bn);
+  ++launches_, kPackLeaves<R><<<gridFor(n), kBlock, 0, stream_>>>(bb, prim, nodes);
+  KCHECK("leaves");
+  ++launches_, kRefitPacked<<<gridFor(n), kBlock, 0, stream_>>>(bb, nodes);
   KCHECK("refit");
-  ++launches_, kRopes<<<gridFor(2 * n - 1), kBlock, 0, stream_>>>(bb);
+  ++launches_, kRopesPacked<<<gridFor(2 * n - 1), kBlock, 0, stream_>>>(bb, nodes);
   KCHECK("ropes");
-  cudaCheck(cudaMemsetAsync(qcnt_.p, 0, (numReal_ + 1) * sizeof(int), stream_), "memset");
-  ++launches_, kQuery<R, 0><<<gridFor(n, 128), 128, 0, stream_>>>(d_, numReal_, bb, bn, qcnt_.p, nullptr, nullptr, 0);
-  KCHECK("query count");
-  exclusiveSum(qcnt_.p, qoff_.p, numReal_ + 1);
-  int total = 0, err = 0;
+  ++launches_, kQueryHalf<R><<<gridFor(n, 128), 128, 0, stream_>>>(bb, prim, nodes, numReal_, rowCnt_.p, qcnt_.p,
+                                                                     slots_.p, bflag_.p);
+  KCHECK("query");
+  exclusiveSum(rowCnt_.p, qoff_.p, numReal_ + 1);
+  int total = 0, err = 0, overflow = 0;
   cudaCheck(cudaMemcpyAsync(&total, qoff_.p + numReal_, sizeof(int), cudaMemcpyDeviceToHost, stream_), "D2H");
   cudaCheck(cudaMemcpyAsync(&err, &ctr_.p->err, sizeof(int), cudaMemcpyDeviceToHost, stream_), "D2H");
+  cudaCheck(cudaMemcpyAsync(&overflow, bflag_.p, sizeof(int), cudaMemcpyDeviceToHost, stream_), "D2H");
   sync();
-  if (err)
+  if (err & 1)
     throw std::runtime_error("broadphase: BVH traversal exceeded its iteration bound (corrupt tree)");
+  if (overflow) {
+    // some query had more partners than its slots: count and write with full traversals
+    cudaCheck(cudaMemsetAsync(rowCnt_.p, 0, (numReal_ + 1) * sizeof(int), stream_), "memset");
+    ++launches_, kQueryFull<R, 0><<<gridFor(n, 128), 128, 0, stream_>>>(bb, prim, nodes, numReal_, rowCnt_.p,
+                                                                          nullptr, nullptr, 0);
+    KCHECK("query count");
+    exclusiveSum(rowCnt_.p, qoff_.p, numReal_ + 1);
+    cudaCheck(cudaMemcpyAsync(&total, qoff_.p + numReal_, sizeof(int), cudaMemcpyDeviceToHost, stream_), "D2H");
+    cudaCheck(cudaMemcpyAsync(&err, &ctr_.p->err, sizeof(int), cudaMemcpyDeviceToHost, stream_), "D2H");
+    sync();
+    if (err & 1)
+      throw std::runtime_error("broadphase: BVH traversal exceeded its iteration bound (corrupt tree)");
+    if (total <= cap) {
+      ++launches_, kQueryFull<R, 1><<<gridFor(n, 128), 128, 0, stream_>>>(bb, prim, nodes, numReal_, nullptr,
+                                                                            qoff_.p, pairs_.p, cap);
+      KCHECK("query write");
+    }
+  } else if (total <= cap) {
+    ++launches_, kScatterHalf<<<gridFor(n), kBlock, 0, stream_>>>(bb, qcnt_.p, slots_.p, qoff_.p, pairs_.p, cap);
+    KCHECK("pair scatter");
+  }
   if (total <= cap) {
-    ++launches_, kQuery<R, 1><<<gridFor(n, 128), 128, 0, stream_>>>(d_, numReal_, bb, bn, nullptr, qoff_.p, pairs_.p, cap);
-    KCHECK("query write");
     ++launches_, kSortPairLists<<<gridFor(numReal_), kBlock, 0, stream_>>>(numReal_, qoff_.p, pairs_.p, cap);
     KCHECK("pair sort");
   }
@@ -743,7 +806,10 @@ void Sim<R>::detectAll(R margin) {
   }
   const bool boundary = nr > 0 && (P.numPlanes > 0 || P.numWalls > 0);
   if (boundary) {
-    ++launches_, kBoundary<R, 0><<<gridFor((long)nr * 32), kBlock, 0, stream_>>>(d_, nr, P, iC_.p, iD_.p, nullptr, nullptr, 0, 0);
+    if (shell)
+      ++launches_, kBoundary<R, 0><<<gridFor((long)nr * 32), kBlock, 0, stream_>>>(d_, nr, P, iC_.p, iD_.p, nullptr, nullptr, 0, 0);
+    else
+      ++launches_, kBoundarySphere<R, 0><<<gridFor(nr), kBlock, 0, stream_>>>(d_, nr, P, iC_.p, iD_.p, nullptr, nullptr, 0, 0);
     KCHECK("boundary count");
   }
   exclusiveSum(iA_.p, iB_.p, np + 1);
@@ -762,8 +828,12 @@ void Sim<R>::detectAll(R margin) {
     KCHECK("narrow write");
   }
   if (boundary && tot[1] + tot[2] > 0 && tot[0] < maxContacts_) {
-    ++launches_, kBoundary<R, 1><<<gridFor((long)nr * 32), kBlock, 0, stream_>>>(d_, nr, P, nullptr, nullptr, offP, cntW, tot[0],
-                                                                     tot[0] + tot[1]);
+    if (shell)
+      ++launches_, kBoundary<R, 1><<<gridFor((long)nr * 32), kBlock, 0, stream_>>>(d_, nr, P, nullptr, nullptr, offP, cntW,
+                                                                                 tot[0], tot[0] + tot[1]);
+    else
+      ++launches_, kBoundarySphere<R, 1><<<gridFor(nr), kBlock, 0, stream_>>>(d_, nr, P, nullptr, nullptr, offP, cntW,
+                                                                              tot[0], tot[0] + tot[1]);
     KCHECK("boundary write");
   }
   const long total = (long)tot[0] + tot[1] + tot[2];
@@ -815,35 +885,25 @@ int Sim<R>::colorGraph(bool manifold, int ne, int nb, int& leftover) {
   else
     ++launches_, kFillInt<<<gridFor(ne), kBlock, 0, stream_>>>(col, ne, -1);
   KCHECK("color init");
-  int remaining = 1, prevRem = -1;
-  const int maxRounds = nb + 2;
-  for (int round = 0; round < maxRounds && remaining > 0; ++round) {
-    ++launches_, kFillLL<<<gridFor(nb), kBlock, 0, stream_>>>(winner_.p, nb, -1ll);
-    if (manifold)
-      ++launches_, kColorContend<R, true><<<gridFor(ne), kBlock, 0, stream_>>>(d_, ne, col);
-    else
-      ++launches_, kColorContend<R, false><<<gridFor(ne), kBlock, 0, stream_>>>(d_, ne, col);
-    cudaCheck(cudaMemsetAsync(&ctr_.p->remaining, 0, sizeof(int), stream_), "memset");
-    if (manifold)
-      ++launches_, kColorCommit<R, true><<<gridFor(ne), kBlock, 0, stream_>>>(d_, ne, col, &ctr_.p->remaining);
-    else
-      ++launches_, kColorCommit<R, false><<<gridFor(ne), kBlock, 0, stream_>>>(d_, ne, col, &ctr_.p->remaining);
-    KCHECK("color round");
-    int rem = 0;
-    cudaCheck(cudaMemcpyAsync(&rem, &ctr_.p->remaining, sizeof(int), cudaMemcpyDeviceToHost, stream_), "D2H");
-    sync();
-    if (rem == prevRem)
-      break;
-    prevRem = rem;
-    remaining = rem;
-  }
-  const int st[2] = {std::numeric_limits<int>::min(), 0};
-  cudaCheck(cudaMemcpyAsync(&ctr_.p->maxColor, st, sizeof st, cudaMemcpyHostToDevice, stream_), "H2D");
-  ++launches_, kColorStats<<<gridFor(ne), kBlock, 0, stream_>>>(ne, col, &ctr_.p->maxColor, &ctr_.p->leftover);
-  KCHECK("color stats");
+  winner2_.ensure(nb, false, stream_);
+  colorAux_.ensure(8, false, stream_);
+  ++launches_, kFillLL<<<gridFor(nb), kBlock, 0, stream_>>>(winner_.p, nb, -1ll);
+  const int aux[5] = {0, 0, 0, std::numeric_limits<int>::min(), 0};  // remCnt[3], stats[2]
+  cudaCheck(cudaMemcpyAsync(colorAux_.p, aux, sizeof aux, cudaMemcpyHostToDevice, stream_), "H2D colour aux");
+  gbar_.ensure(2, false, stream_);
+  const GridBar gb{gbar_.p, &ctr_.p->err};
+  if (manifold)
+    launchCoop(kColorLoop<R, true>, d_, ne, nb + 2, col, winner_.p, winner2_.p, colorAux_.p, colorAux_.p + 3, gb);
+  else
+    launchCoop(kColorLoop<R, false>, d_, ne, nb + 2, col, winner_.p, winner2_.p, colorAux_.p, colorAux_.p + 3, gb);
+  KCHECK("colour loop");
   int res[2];
-  cudaCheck(cudaMemcpyAsync(res, &ctr_.p->maxColor, sizeof res, cudaMemcpyDeviceToHost, stream_), "D2H");
+  cudaCheck(cudaMemcpyAsync(res, colorAux_.p + 3, sizeof res, cudaMemcpyDeviceToHost, stream_), "D2H");
+  int err = 0;
+  cudaCheck(cudaMemcpyAsync(&err, &ctr_.p->err, sizeof err, cudaMemcpyDeviceToHost, stream_), "D2H");
   sync();
+  if (err & kErrBarrier)
+    throw CudaError("colouring: a grid-wide barrier timed out");
   leftover = res[1];
   return res[0] + 1;
 }
@@ -859,7 +919,7 @@ void Sim<R>::colorOrder(bool manifold, int ne, int ncol) {
   iE_.ensure(ne, false, stream_);
   ++launches_, kColorSortKeys<<<gridFor(ne), kBlock, 0, stream_>>>(ne, manifold ? mColor_.p : cColor_.p, uA_.p, iE_.p);
   KCHECK("color keys");
-  sortPairs(uA_.p, uB_.p, iE_.p, order.p, ne, 32);
+  sortPairs(uA_.p, uB_.p, iE_.p, order.p, ne, 6);
   ++launches_, kLowerBoundOffsets<unsigned><<<gridFor(ncol + 1), kBlock, 0, stream_>>>(ne, uB_.p, ncol, off.p);
   KCHECK("color offsets");
 }
@@ -980,7 +1040,20 @@ void Sim<R>::demStep() {
     rA_.ensure(nm, false, s);
     iC_.ensure(nm, false, s);
   }
-  for (int it = 0; it < velIters_; ++it) {
+  // the whole loop as one persistent launch when every sweep is colours only
+  const bool velPersistent = useGS_ && !legacyFriction && velLeft == 0 && ncolV > 0 && velIters_ > 0;
+  if (velPersistent) {
+    gbar_.ensure(2, false, s);
+    const GridBar gb{gbar_.p, &ctr_.p->err};
+    const R thr = usePGS ? R(0.02) * vRest : vRest;
+    ++launches_, kCtl<<<1, 1, 0, s>>>(ctr_.p, CTL_VEL_BEGIN, R(0), 0);
+    if (usePGS)
+      launchCoop(kSweepLoop<R, 0, 1>, d_, (const int*)mOrder_.p, (const int*)mOff_.p, ncolV, velIters_, sp, thr, gb);
+    else
+      launchCoop(kSweepLoop<R, 1, 1>, d_, (const int*)mOrder_.p, (const int*)mOff_.p, ncolV, velIters_, sp, thr, gb);
+    KCHECK("velocity loop");
+  }
+  for (int it = 0; it < (velPersistent ? 0 : velIters_); ++it) {
     if (legacyFriction && nc > 0) {
       // runs at the top of every iteration the loop reaches (src/sim.hpp:224-226): with the
       // coloured solve the adaptive stop ends the loop, so it is gated on the loop flag
@@ -1030,7 +1103,14 @@ void Sim<R>::demStep() {
       SolveP<R> ss = sp;
       ss.vRest = vRestS;
       const int iters = stabMode_ == 1 ? 2 * velIters_ : 256;
-      for (int it = 0; it < iters; ++it) {
+      const bool stabPersistent = ncolV > 0;
+      if (stabPersistent) {
+        gbar_.ensure(2, false, s);
+        const GridBar gb{gbar_.p, &ctr_.p->err};
+        ++launches_, kCtl<<<1, 1, 0, s>>>(ctr_.p, CTL_STAB_BEGIN, R(0), 0);
+        launchCoop(kSweepLoop<R, 0, 2>, d_, (const int*)mOrder_.p, (const int*)mOff_.p, ncolV, iters, ss, vRestS, gb);
+      }
+      for (int it = 0; it < (stabPersistent ? 0 : iters); ++it) {
         ++launches_, kCtl<<<1, 1, 0, s>>>(ctr_.p, CTL_STAB_BEGIN, R(0), 0);
         for (int col = 0; col < ncolV; ++col)
           ++launches_, kPGSColor<<<gridFor(nm), B, 0, s>>>(d_, mOrder_.p, mOff_.p, col, ss, 2);
@@ -1097,7 +1177,15 @@ void Sim<R>::demStep() {
     iC_.ensure(nc, false, s);
   }
   Incidence incP{incOff_.p, incValsS_.p};
-  for (int it = 0; it < posIters_; ++it) {
+  const bool posPersistent = useGS_ && posLeft == 0 && ncolP > 0 && posIters_ > 0;
+  if (posPersistent) {
+    gbar_.ensure(2, false, s);
+    const GridBar gb{gbar_.p, &ctr_.p->err};
+    ++launches_, kCtl<<<1, 1, 0, s>>>(ctr_.p, CTL_POS_BEGIN, R(0), 0);
+    launchCoop(kSweepLoop<R, 2, 3>, d_, (const int*)cOrder_.p, (const int*)cOff_.p, ncolP, posIters_, sp, posTol, gb);
+    KCHECK("position loop");
+  }
+  for (int it = 0; it < (posPersistent ? 0 : posIters_); ++it) {
     if (useGS_) {
       ++launches_, kCtl<<<1, 1, 0, s>>>(ctr_.p, CTL_POS_BEGIN, R(0), 0);
       for (int col = 0; col < ncolP; ++col)

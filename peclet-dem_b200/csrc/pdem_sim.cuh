@@ -184,6 +184,10 @@ class Sim {
   DBuf<WallDesc<R>> wallsD_;
   DBuf<R> wallGridD_, pairMatD_, hzED_, hzNuD_;
   DBuf<Counters<R>> ctr_;
+  int numSMs_ = 148;
+  DBuf<unsigned> gbar_;        // grid barrier of the persistent loops
+  DBuf<long long> winner2_;    // second winner array of the colouring rounds
+  DBuf<int> colorAux_;         // colouring: per-round remaining counts [3], statistics [2]
   // scratch
   DBuf<char> cubTmp_;
   DBuf<int> iA_, iB_, iC_, iD_, iE_;
@@ -200,7 +204,8 @@ class Sim {
   // broadphase scratch
   DBuf<char> bvhBoxes_, bvhNodes_;
   DBuf<u64> codes_, codesAlt_, bounds_;
-  DBuf<int> bidx_, bidxAlt_, left_, right_, parent_, rope_, flag_, qcnt_, qoff_;
+  DBuf<int> bidx_, bidxAlt_, left_, right_, parent_, flag_, qcnt_, qoff_, rowCnt_, bflag_;
+  DBuf<int2> slots_;
   // manifold reduction scratch (kept for the position-impulse commit)
   DBuf<u64> ckeys_, ckeysS_;
   DBuf<int> cperm_, cpermIn_, head_, headScan_, segStart_;
@@ -245,6 +250,10 @@ class Sim {
   void ensureGrounded();
   void demStep();
   Counters<R> readCounters();
+  template <class K>
+  int coopGrid(K kernel);
+  template <class K, class... A>
+  void launchCoop(K kernel, A... args);
   template <class T>
   void sortPairs(const T* kin, T* kout, const int* vin, int* vout, int n, int endBit);
   template <class T>

@@ -285,6 +285,141 @@ __global__ void kWarmApply(Dev<R> d, int numReal, Incidence inc) {
 // ---------------------------------------------------------------------------------------------
 // projected Gauss-Seidel sweep of one colour (src/solver_velocity.hpp:641-858)
 template <class R>
+__device__ __forceinline__ void pgsOne(const Dev<R>& d, int idx, const SolveP<R>& P, R& mx) {
+  const ManifoldView<R> v = loadManifold(d, idx);
+  const int ra = v.ra, rb = v.rb;
+  const bool hasB = d.mab[idx].y >= 0;
+  const V3<R> vA = v3(d.velPred[ra]), wA = v3(d.angVelPred[ra]);
+  V3<R> vB{0, 0, 0}, wB{0, 0, 0};
+  R e = P.eN;
+  if (hasB) {
+    vB = v3(d.velPred[rb]);
+    wB = v3(d.angVelPred[rb]);
+  } else {
+    vB = mul(v.wv, v.invN);
+  }
+  {
+    const R ra2 = v.eSum * v.invN;
+    if (ra2 >= R(0))
+      e = ra2;
+  }
+  const R lenN = sqrt(dot(v.N, v.N));
+  if (lenN < R(1e-9))
+    return;
+  const V3<R> vG = mul(v.dc, P.growthRate);
+  R vn = dot(vA, v.N) + dot(wA, v.TA) + dot(vB, neg(v.N)) + dot(wB, v.TB);
+  vn += dot(vG, v.N);
+  const R al = dot(v.N, v.dc);
+  const R sgn = (al > R(0)) ? R(1) : R(-1);
+  const R Nsq = dot(v.N, v.N);
+  R wAn = Nsq * v.imA + genInvMass(v.TA, v.iIA, v.qA);
+  R wBn = Nsq * v.imB + genInvMass(v.TB, v.iIB, v.qB);
+  bool applyA = true, applyB = true;
+  const uint8_t sf = d.sideFlags[idx];
+  if (sf == 1) {
+    wBn = R(0);
+    applyB = false;
+    e = R(0);
+  } else if (sf == 2) {
+    wAn = R(0);
+    applyA = false;
+    e = R(0);
+  }
+  const R wT = wAn + wBn;
+  if (wT <= R(0))
+    return;
+  const R vn0 = d.vn0[idx];
+  const R v0 = sgn * vn0;
+  if (fabs(vn0) < P.vRest * lenN)
+    e = R(0);
+  const R target = (v0 > R(0)) ? -e * v0 : R(0);
+  const R vt = sgn * vn;
+  const R dp = (vt - target) / wT;
+  const R pOld = d.lambda[idx];
+  R pNew = pOld + dp;
+  if (pNew < R(0))
+    pNew = R(0);
+  const R dA = pNew - pOld;
+  V3<R> vA2 = vA, wA2 = wA, vB2 = vB, wB2 = wB;
+  if (dA != R(0)) {
+    d.lambda[idx] = pNew;
+    runMax(mx, fabs(dA) * wT / lenN);
+    const R lam = -sgn * dA;
+    const V3<R> J = mul(v.N, lam), JA = mul(v.TA, lam), JB = mul(v.TB, lam);
+    if (applyA) {
+      vA2 = add(vA2, mul(J, v.imA));
+      wA2 = add(wA2, angResponse(v.qA, JA, v.iIA));
+    }
+    if (hasB && applyB) {
+      vB2 = add(vB2, mul(neg(J), v.imB));
+      wB2 = add(wB2, angResponse(v.qB, JB, v.iIB));
+    }
+  }
+  // friction cone
+  R mu = P.mu;
+  const R fa = v.muSum * v.invN;
+  if (fa >= R(0))
+    mu = fa;
+  const V3<R> ltOld = v3(d.lambdaT[idx]);
+  const bool haveOld = nonzero(ltOld);
+  if (mu > R(0) || haveOld) {
+    const V3<R> nh = mul(v.N, R(1) / lenN);
+    const V3<R> vBf = hasB ? vB2 : mul(v.wv, v.invN);
+    const V3<R> wBf = hasB ? wB2 : V3<R>{0, 0, 0};
+    const V3<R> vr = sub(add(vA2, cross(wA2, v.rAa)), add(vBf, cross(wBf, v.rBa)));
+    const V3<R> vtv = sub(vr, mul(nh, dot(vr, nh)));
+    R beta = P.eT;
+    if (beta != R(0) && (sf != 0 || fabs(vn0) < P.vRest * lenN))
+      beta = R(0);
+    V3<R> err = vtv;
+    if (beta != R(0)) {
+      V3<R> w0 = v3(d.vt0[idx]);
+      w0 = sub(w0, mul(nh, dot(w0, nh)));
+      err = add(vtv, mul(w0, beta));
+    }
+    const R vl = sqrt(dot(err, err));
+    V3<R> ltNew = ltOld;
+    R wTt = v.imA + v.imB;
+    if (vl > R(1e-9)) {
+      const V3<R> th = mul(err, R(1) / vl);
+      const R wAt = (sf == 2) ? R(0) : v.imA + genInvMass(cross(v.rAa, th), v.iIA, v.qA);
+      const R wBt = (sf == 1 || !hasB) ? R(0) : v.imB + genInvMass(cross(v.rBa, th), v.iIB, v.qB);
+      wTt = wAt + wBt;
+      if (wTt > R(1e-9))
+        ltNew = add(ltOld, mul(th, -vl / wTt));
+    }
+    ltNew = sub(ltNew, mul(nh, dot(ltNew, nh)));
+    R nTot = fmax(d.lambda[idx], R(0)) * lenN;
+    if (fabs(vn0) < P.vRest * lenN)
+      nTot += fmax(d.posImp[idx], R(0));
+    const R bound = mu * nTot;
+    const R ll = sqrt(dot(ltNew, ltNew));
+    if (ll > bound)
+      ltNew = (bound > R(0)) ? mul(ltNew, bound / ll) : V3<R>{0, 0, 0};
+    const V3<R> dd = sub(ltNew, ltOld);
+    if (nonzero(dd)) {
+      d.lambdaT[idx] = q4(ltNew);
+      const R dl = sqrt(dot(dd, dd));
+      if (wTt > R(1e-9))
+        runMax(mx, dl * wTt);
+      if (applyA) {
+        vA2 = add(vA2, mul(dd, v.imA));
+        wA2 = add(wA2, angResponse(v.qA, cross(v.rAa, dd), v.iIA));
+      }
+      if (hasB && applyB) {
+        vB2 = add(vB2, mul(neg(dd), v.imB));
+        wB2 = add(wB2, angResponse(v.qB, cross(v.rBa, mul(dd, R(-1))), v.iIB));
+      }
+    }
+  }
+  d.velPred[ra] = q4(vA2);
+  d.angVelPred[ra] = q4(wA2);
+  if (hasB) {
+    d.velPred[rb] = q4(vB2);
+    d.angVelPred[rb] = q4(wB2);
+  }
+}
+template <class R>
 __global__ void kPGSColor(Dev<R> d, const int* order, const int* coff, int color, SolveP<R> P, int gate) {
   if (!gateOpen(d.ctr, gate))
     return;
@@ -297,139 +432,7 @@ __global__ void kPGSColor(Dev<R> d, const int* order, const int* coff, int color
   R mx = R(0);
   for (long t = serial ? 0 : (long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
        t += serial ? 1 : (long)gridDim.x * blockDim.x) {
-    const int idx = order[b + t];
-    const ManifoldView<R> v = loadManifold(d, idx);
-    const int ra = v.ra, rb = v.rb;
-    const bool hasB = d.mab[idx].y >= 0;
-    const V3<R> vA = v3(d.velPred[ra]), wA = v3(d.angVelPred[ra]);
-    V3<R> vB{0, 0, 0}, wB{0, 0, 0};
-    R e = P.eN;
-    if (hasB) {
-      vB = v3(d.velPred[rb]);
-      wB = v3(d.angVelPred[rb]);
-    } else {
-      vB = mul(v.wv, v.invN);
-    }
-    {
-      const R ra2 = v.eSum * v.invN;
-      if (ra2 >= R(0))
-        e = ra2;
-    }
-    const R lenN = sqrt(dot(v.N, v.N));
-    if (lenN < R(1e-9))
-      continue;
-    const V3<R> vG = mul(v.dc, P.growthRate);
-    R vn = dot(vA, v.N) + dot(wA, v.TA) + dot(vB, neg(v.N)) + dot(wB, v.TB);
-    vn += dot(vG, v.N);
-    const R al = dot(v.N, v.dc);
-    const R sgn = (al > R(0)) ? R(1) : R(-1);
-    const R Nsq = dot(v.N, v.N);
-    R wAn = Nsq * v.imA + genInvMass(v.TA, v.iIA, v.qA);
-    R wBn = Nsq * v.imB + genInvMass(v.TB, v.iIB, v.qB);
-    bool applyA = true, applyB = true;
-    const uint8_t sf = d.sideFlags[idx];
-    if (sf == 1) {
-      wBn = R(0);
-      applyB = false;
-      e = R(0);
-    } else if (sf == 2) {
-      wAn = R(0);
-      applyA = false;
-      e = R(0);
-    }
-    const R wT = wAn + wBn;
-    if (wT <= R(0))
-      continue;
-    const R vn0 = d.vn0[idx];
-    const R v0 = sgn * vn0;
-    if (fabs(vn0) < P.vRest * lenN)
-      e = R(0);
-    const R target = (v0 > R(0)) ? -e * v0 : R(0);
-    const R vt = sgn * vn;
-    const R dp = (vt - target) / wT;
-    const R pOld = d.lambda[idx];
-    R pNew = pOld + dp;
-    if (pNew < R(0))
-      pNew = R(0);
-    const R dA = pNew - pOld;
-    V3<R> vA2 = vA, wA2 = wA, vB2 = vB, wB2 = wB;
-    if (dA != R(0)) {
-      d.lambda[idx] = pNew;
-      runMax(mx, fabs(dA) * wT / lenN);
-      const R lam = -sgn * dA;
-      const V3<R> J = mul(v.N, lam), JA = mul(v.TA, lam), JB = mul(v.TB, lam);
-      if (applyA) {
-        vA2 = add(vA2, mul(J, v.imA));
-        wA2 = add(wA2, angResponse(v.qA, JA, v.iIA));
-      }
-      if (hasB && applyB) {
-        vB2 = add(vB2, mul(neg(J), v.imB));
-        wB2 = add(wB2, angResponse(v.qB, JB, v.iIB));
-      }
-    }
-    // friction cone
-    R mu = P.mu;
-    const R fa = v.muSum * v.invN;
-    if (fa >= R(0))
-      mu = fa;
-    const V3<R> ltOld = v3(d.lambdaT[idx]);
-    const bool haveOld = nonzero(ltOld);
-    if (mu > R(0) || haveOld) {
-      const V3<R> nh = mul(v.N, R(1) / lenN);
-      const V3<R> vBf = hasB ? vB2 : mul(v.wv, v.invN);
-      const V3<R> wBf = hasB ? wB2 : V3<R>{0, 0, 0};
-      const V3<R> vr = sub(add(vA2, cross(wA2, v.rAa)), add(vBf, cross(wBf, v.rBa)));
-      const V3<R> vtv = sub(vr, mul(nh, dot(vr, nh)));
-      R beta = P.eT;
-      if (beta != R(0) && (sf != 0 || fabs(vn0) < P.vRest * lenN))
-        beta = R(0);
-      V3<R> err = vtv;
-      if (beta != R(0)) {
-        V3<R> w0 = v3(d.vt0[idx]);
-        w0 = sub(w0, mul(nh, dot(w0, nh)));
-        err = add(vtv, mul(w0, beta));
-      }
-      const R vl = sqrt(dot(err, err));
-      V3<R> ltNew = ltOld;
-      R wTt = v.imA + v.imB;
-      if (vl > R(1e-9)) {
-        const V3<R> th = mul(err, R(1) / vl);
-        const R wAt = (sf == 2) ? R(0) : v.imA + genInvMass(cross(v.rAa, th), v.iIA, v.qA);
-        const R wBt = (sf == 1 || !hasB) ? R(0) : v.imB + genInvMass(cross(v.rBa, th), v.iIB, v.qB);
-        wTt = wAt + wBt;
-        if (wTt > R(1e-9))
-          ltNew = add(ltOld, mul(th, -vl / wTt));
-      }
-      ltNew = sub(ltNew, mul(nh, dot(ltNew, nh)));
-      R nTot = fmax(d.lambda[idx], R(0)) * lenN;
-      if (fabs(vn0) < P.vRest * lenN)
-        nTot += fmax(d.posImp[idx], R(0));
-      const R bound = mu * nTot;
-      const R ll = sqrt(dot(ltNew, ltNew));
-      if (ll > bound)
-        ltNew = (bound > R(0)) ? mul(ltNew, bound / ll) : V3<R>{0, 0, 0};
-      const V3<R> dd = sub(ltNew, ltOld);
-      if (nonzero(dd)) {
-        d.lambdaT[idx] = q4(ltNew);
-        const R dl = sqrt(dot(dd, dd));
-        if (wTt > R(1e-9))
-          runMax(mx, dl * wTt);
-        if (applyA) {
-          vA2 = add(vA2, mul(dd, v.imA));
-          wA2 = add(wA2, angResponse(v.qA, cross(v.rAa, dd), v.iIA));
-        }
-        if (hasB && applyB) {
-          vB2 = add(vB2, mul(neg(dd), v.imB));
-          wB2 = add(wB2, angResponse(v.qB, cross(v.rBa, mul(dd, R(-1))), v.iIB));
-        }
-      }
-    }
-    d.velPred[ra] = q4(vA2);
-    d.angVelPred[ra] = q4(wA2);
-    if (hasB) {
-      d.velPred[rb] = q4(vB2);
-      d.angVelPred[rb] = q4(wB2);
-    }
+    pgsOne(d, order[b + t], P, mx);
   }
   if (serial)
     atomicMaxNonNeg(&d.ctr->maxApproach, mx);
@@ -438,6 +441,56 @@ __global__ void kPGSColor(Dev<R> d, const int* order, const int* coff, int color
 }
 
 // one-shot coloured GS of one colour, g = 0 path (src/solver_velocity.hpp:989-1137)
+template <class R>
+__device__ __forceinline__ void gsOne(const Dev<R>& d, int idx, const SolveP<R>& P, R& mx) {
+  const ManifoldView<R> v = loadManifold(d, idx);
+  const bool hasB = d.mab[idx].y >= 0;
+  const V3<R> vA = v3(d.velPred[v.ra]), wA = v3(d.angVelPred[v.ra]);
+  V3<R> vB{0, 0, 0}, wB{0, 0, 0};
+  if (hasB) {
+    vB = v3(d.velPred[v.rb]);
+    wB = v3(d.angVelPred[v.rb]);
+  }
+  R e = P.eN;
+  if (!hasB)
+    vB = mul(v.wv, v.invN);
+  {
+    const R ra2 = v.eSum * v.invN;
+    if (ra2 >= R(0))
+      e = ra2;
+  }
+  const R lenN = sqrt(dot(v.N, v.N));
+  if (lenN < R(1e-9))
+    return;
+  const V3<R> vG = mul(v.dc, P.growthRate);
+  R vn = dot(vA, v.N) + dot(wA, v.TA) + dot(vB, neg(v.N)) + dot(wB, v.TB);
+  vn += dot(vG, v.N);
+  const R al = dot(v.N, v.dc);
+  if (al > R(0)) {
+    if (vn < R(0))
+      return;
+  } else {
+    if (vn > R(0))
+      return;
+  }
+  const R Nsq = dot(v.N, v.N);
+  const R wAn = Nsq * v.imA + genInvMass(v.TA, v.iIA, v.qA);
+  const R wBn = Nsq * v.imB + genInvMass(v.TB, v.iIB, v.qB);
+  const R wT = wAn + wBn;
+  if (wT <= R(0))
+    return;
+  runMax(mx, fabs(vn) / lenN);
+  if (fabs(vn) < P.vRest * lenN)
+    e = R(0);
+  const R lam = (-e * vn - vn) / wT;
+  const V3<R> J = mul(v.N, lam), JA = mul(v.TA, lam), JB = mul(v.TB, lam);
+  d.velPred[v.ra] = q4(add(vA, mul(J, v.imA)));
+  d.angVelPred[v.ra] = q4(add(wA, angResponse(v.qA, JA, v.iIA)));
+  if (hasB) {
+    d.velPred[v.rb] = q4(add(vB, mul(neg(J), v.imB)));
+    d.angVelPred[v.rb] = q4(add(wB, angResponse(v.qB, JB, v.iIB)));
+  }
+}
 template <class R>
 __global__ void kGSColor(Dev<R> d, const int* order, const int* coff, int color, SolveP<R> P, int gate) {
   if (!gateOpen(d.ctr, gate))
@@ -451,54 +504,7 @@ __global__ void kGSColor(Dev<R> d, const int* order, const int* coff, int color,
   R mx = R(0);
   for (long t = serial ? 0 : (long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
        t += serial ? 1 : (long)gridDim.x * blockDim.x) {
-    const int idx = order[b + t];
-    const ManifoldView<R> v = loadManifold(d, idx);
-    const bool hasB = d.mab[idx].y >= 0;
-    const V3<R> vA = v3(d.velPred[v.ra]), wA = v3(d.angVelPred[v.ra]);
-    V3<R> vB{0, 0, 0}, wB{0, 0, 0};
-    if (hasB) {
-      vB = v3(d.velPred[v.rb]);
-      wB = v3(d.angVelPred[v.rb]);
-    }
-    R e = P.eN;
-    if (!hasB)
-      vB = mul(v.wv, v.invN);
-    {
-      const R ra2 = v.eSum * v.invN;
-      if (ra2 >= R(0))
-        e = ra2;
-    }
-    const R lenN = sqrt(dot(v.N, v.N));
-    if (lenN < R(1e-9))
-      continue;
-    const V3<R> vG = mul(v.dc, P.growthRate);
-    R vn = dot(vA, v.N) + dot(wA, v.TA) + dot(vB, neg(v.N)) + dot(wB, v.TB);
-    vn += dot(vG, v.N);
-    const R al = dot(v.N, v.dc);
-    if (al > R(0)) {
-      if (vn < R(0))
-        continue;
-    } else {
-      if (vn > R(0))
-        continue;
-    }
-    const R Nsq = dot(v.N, v.N);
-    const R wAn = Nsq * v.imA + genInvMass(v.TA, v.iIA, v.qA);
-    const R wBn = Nsq * v.imB + genInvMass(v.TB, v.iIB, v.qB);
-    const R wT = wAn + wBn;
-    if (wT <= R(0))
-      continue;
-    runMax(mx, fabs(vn) / lenN);
-    if (fabs(vn) < P.vRest * lenN)
-      e = R(0);
-    const R lam = (-e * vn - vn) / wT;
-    const V3<R> J = mul(v.N, lam), JA = mul(v.TA, lam), JB = mul(v.TB, lam);
-    d.velPred[v.ra] = q4(add(vA, mul(J, v.imA)));
-    d.angVelPred[v.ra] = q4(add(wA, angResponse(v.qA, JA, v.iIA)));
-    if (hasB) {
-      d.velPred[v.rb] = q4(add(vB, mul(neg(J), v.imB)));
-      d.angVelPred[v.rb] = q4(add(wB, angResponse(v.qB, JB, v.iIB)));
-    }
+    gsOne(d, order[b + t], P, mx);
   }
   if (serial)
     atomicMaxNonNeg(&d.ctr->maxApproach, mx);
@@ -816,6 +822,27 @@ __device__ __forceinline__ bool posConstraint(const Dev<R>& d, int idx, V3<R>& n
   return true;
 }
 template <class R>
+__device__ __forceinline__ void posGSOne(const Dev<R>& d, int idx, R& mx) {
+  V3<R> nv;
+  R C = R(0), wT = R(0);
+  int A, B;
+  if (!posConstraint(d, idx, nv, C, wT, A, B))
+    return;
+  if (wT < R(1e-6))
+    return;
+  const R dl = -C / wT;
+  d.posLamC[idx] += dl;
+  const R imA = d.invMass[A];
+  const V3<R> pA = v3(d.posPred[A]);
+  d.posPred[A] = q4(add(pA, V3<R>{nv.x * dl * imA, nv.y * dl * imA, nv.z * dl * imA}));
+  if (B >= 0) {
+    const R imB = d.invMass[B];
+    const V3<R> pB = v3(d.posPred[B]);
+    d.posPred[B] = q4(add(pB, V3<R>{-nv.x * dl * imB, -nv.y * dl * imB, -nv.z * dl * imB}));
+  }
+  runMax(mx, -C);
+}
+template <class R>
 __global__ void kPosGSColor(Dev<R> d, const int* order, const int* coff, int color, int gate) {
   if (!gateOpen(d.ctr, gate))
     return;
@@ -828,25 +855,7 @@ __global__ void kPosGSColor(Dev<R> d, const int* order, const int* coff, int col
   R mx = R(0);
   for (long t = serial ? 0 : (long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
        t += serial ? 1 : (long)gridDim.x * blockDim.x) {
-    const int idx = order[b + t];
-    V3<R> nv;
-    R C = R(0), wT = R(0);
-    int A, B;
-    if (!posConstraint(d, idx, nv, C, wT, A, B))
-      continue;
-    if (wT < R(1e-6))
-      continue;
-    const R dl = -C / wT;
-    d.posLamC[idx] += dl;
-    const R imA = d.invMass[A];
-    const V3<R> pA = v3(d.posPred[A]);
-    d.posPred[A] = q4(add(pA, V3<R>{nv.x * dl * imA, nv.y * dl * imA, nv.z * dl * imA}));
-    if (B >= 0) {
-      const R imB = d.invMass[B];
-      const V3<R> pB = v3(d.posPred[B]);
-      d.posPred[B] = q4(add(pB, V3<R>{-nv.x * dl * imB, -nv.y * dl * imB, -nv.z * dl * imB}));
-    }
-    runMax(mx, -C);
+    posGSOne(d, order[b + t], mx);
   }
   if (serial)
     atomicMaxNonNeg(&d.ctr->maxOverlap, mx);
