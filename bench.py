@@ -115,6 +115,22 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
+def max_over_ranks(value, dist=None, device="cpu"):
+    """Largest per-rank value over the process group (the device time of the slowest replica).
+    NCCL on GPUs; the multi-rank tests run it over gloo on CPU."""
+    if dist is None:
+        return float(value)
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_rate(world, n, substeps, steps, t_max):
+    """Whole-job particle-substeps/s: every replica's work over the slowest replica's time."""
+    return world * n * substeps * steps / t_max
+
+
 # ---------------------------------------------------------------------------------------------
 def cpu_reference(scene, substeps, threads):
     """Time the reference's own substep (OpenMP shim build) for `substeps` calls; returns
@@ -212,13 +228,8 @@ def run_ours(args):
     sweeps = sim.debug_sweeps() if hasattr(sim, "debug_sweeps") else None
     sim.profile_enable(False)
     # max over ranks of the device time; value = all ranks' particle-substeps / that time
-    t_max = dev_ms / 1e3
-    if dist is not None:
-        import torch
-        tt = torch.tensor([t_max], dtype=torch.float64, device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_max = float(tt.item())
-    value = world * n * SUBSTEPS * args.steps / t_max
+    t_max = max_over_ranks(dev_ms / 1e3, dist, "cuda")
+    value = aggregate_rate(world, n, SUBSTEPS, args.steps, t_max)
 
     # ---- end to end through the public API with host buffers ----
     force = np.zeros((n, 3))

@@ -60,7 +60,21 @@ struct BvhBuffers {
   int *left = nullptr, *right = nullptr, *parent = nullptr, *rope = nullptr, *flag = nullptr;
   u64* bounds = nullptr;  // [6] ordered bits: min xyz, max xyz
   int* err = nullptr;     // error flags (Counters::err)
+  // batched form: each scene's leaves are one contiguous sorted range (its id leads the key), so
+  // each scene is one subtree; first/last leaf of every internal node bound a query to its scene
+  const int* sceneOf = nullptr;    // [n] scene of each primitive (null: one scene)
+  const int* leafFirst = nullptr;  // [scenes + 1] first sorted position of each scene
+  int *first = nullptr, *last = nullptr;  // [n - 1] leaf range of each internal node
 };
+constexpr int kSceneShift = 54;  // batched Morton key: scene << 54 | the top 54 bits of the 63-bit code
+
+// first / last sorted leaf under node v
+__device__ __forceinline__ int nodeFirst(const BvhBuffers& bb, int v) {
+  return v >= bb.n - 1 ? v - (bb.n - 1) : bb.first[v];
+}
+__device__ __forceinline__ int nodeLast(const BvhBuffers& bb, int v) {
+  return v >= bb.n - 1 ? v - (bb.n - 1) : bb.last[v];
+}
 
 template <class R>
 struct BvhNodes {
@@ -72,7 +86,8 @@ template <class R>
 __global__ void kBoxes(Dev<R> d, int n, R margin, R boxCap, BvhNodes<R> bn, BvhBuffers bb) {
   u64 lo[3] = {~0ull, ~0ull, ~0ull}, hi[3] = {0ull, 0ull, 0ull};
   GRID_STRIDE(i, n) {
-    const Box<R> b = saneBox(d, (int)i, d.posPred, margin, boxCap);
+    const R mg = d.scn ? d.scn[d.sceneOf[i]].margin : margin;
+    const Box<R> b = saneBox(d, (int)i, d.posPred, mg, boxCap);
     bn.prim[i] = b;
     bool ok = true;
     double c[3];
@@ -137,6 +152,8 @@ __global__ void kMorton(int n, BvhNodes<R> bn, BvhBuffers bb) {
     }
     if (ok)
       code = (spread21(q[0]) << 2) | (spread21(q[1]) << 1) | spread21(q[2]);
+    if (bb.sceneOf)
+      code = ((u64)bb.sceneOf[i] << kSceneShift) | (code >> (63 - kSceneShift));
     bb.codes[i] = code;
     bb.idx[i] = (int)i;
   }
@@ -181,6 +198,10 @@ static __global__ void kKarras(BvhBuffers bb) {
     const int lo = i < j ? i : j, hi = i < j ? j : i;
     const int L = (lo == gamma) ? (n - 1 + gamma) : gamma;
     const int Rn = (hi == gamma + 1) ? (n - 1 + gamma + 1) : (gamma + 1);
+    if (bb.first) {
+      bb.first[i] = lo;
+      bb.last[i] = hi;
+    }
     bb.left[i] = L;
     bb.right[i] = Rn;
     bb.parent[L] = i;
@@ -374,6 +395,14 @@ __global__ void kPackLeaves(BvhBuffers bb, const Box<R>* prim, PNode* nodes) {
   }
 }
 
+// arrival counter with acquire-release ordering at device scope: the child's box stores before it
+// are visible to the thread that sees the count, and that thread's loads come after it
+__device__ __forceinline__ int arriveAcqRel(int* p) {
+  int old;
+  asm volatile("atom.acq_rel.gpu.global.add.s32 %0, [%1], 1;" : "=r"(old) : "l"(p) : "memory");
+  return old;
+}
+
 // bottom-up union of the float boxes; the second child to arrive at a node computes it
 static __global__ void kRefitPacked(BvhBuffers bb, PNode* nodes) {
   const int n = bb.n;
@@ -384,10 +413,8 @@ static __global__ void kRefitPacked(BvhBuffers bb, PNode* nodes) {
         atomicOr(&bb.err[0], 1);
         break;
       }
-      __threadfence();
-      if (atomicAdd(&bb.flag[node], 1) == 0)
+      if (arriveAcqRel(&bb.flag[node]) == 0)
         break;
-      __threadfence();
       const int c0 = bb.left[node], c1 = bb.right[node];
       float lo[3], hi[3];
       const float* b0 = reinterpret_cast<const float*>(&nodes[c0]);
@@ -443,6 +470,22 @@ static __global__ void kRopesPacked(BvhBuffers bb, PNode* nodes) {
 // host then runs the full two-pass traversal instead.
 constexpr int kSlots = 32;
 
+// first sorted leaf of every scene (the scene id leads each sorted key): leafFirst[s] = number of
+// keys whose scene is below s
+static __global__ void kSceneLeafFirst(int n, int scenes, const u64* sortedCodes, int* leafFirst) {
+  GRID_STRIDE(s, scenes + 1) {
+    int lo = 0, hi = n;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if ((long)(sortedCodes[mid] >> kSceneShift) < (long)s)
+        lo = mid + 1;
+      else
+        hi = mid;
+    }
+    leafFirst[s] = lo;
+  }
+}
+
 template <class R>
 __global__ void kQueryHalf(BvhBuffers bb, const Box<R>* prim, const PNode* nodes, int numReal, int* rowCnt,
                            int* qcnt, int2* slots, int* overflow) {
@@ -455,11 +498,15 @@ __global__ void kQueryHalf(BvhBuffers bb, const Box<R>* prim, const PNode* nodes
     outwardBox(q, qlo, qhi);
     int c = 0;
     int node = self.rope;
+    // batched form: the walk leaves this scene's subtree at the first node past its last leaf
+    const int sceneEnd = bb.sceneOf ? bb.leafFirst[bb.sceneOf[i] + 1] : n;
     for (long guard = 0; node != -1; ++guard) {
       if (guard > 2L * n + 8) {  // each node is visited at most once
         atomicOr(&bb.err[0], 1);
         break;
       }
+      if (bb.sceneOf && nodeFirst(bb, node) >= sceneEnd)
+        break;
       const PNode nd = loadNode(&nodes[node]);
       if (overlapF(qlo, qhi, nd)) {
         if (nd.a >= 0) {
@@ -518,12 +565,18 @@ __global__ void kQueryFull(BvhBuffers bb, const Box<R>* prim, const PNode* nodes
     int c = 0;
     const int base = MODE ? off[i] : 0;
     int node = 0;
+    const int s0 = bb.sceneOf ? bb.leafFirst[bb.sceneOf[i]] : 0;
+    const int s1 = bb.sceneOf ? bb.leafFirst[bb.sceneOf[i] + 1] : n;
     for (long guard = 0; node != -1; ++guard) {
       if (guard > 2L * n + 8) {
         atomicOr(&bb.err[0], 1);
         break;
       }
       const PNode nd = loadNode(&nodes[node]);
+      if (bb.sceneOf && (nodeLast(bb, node) < s0 || nodeFirst(bb, node) >= s1)) {  // other scenes only
+        node = nd.rope;
+        continue;
+      }
       if (overlapF(qlo, qhi, nd)) {
         if (nd.a >= 0) {
           node = nd.a;

@@ -60,6 +60,17 @@ struct Counters {
   R pad1;
 };
 
+// Batched form: several independent scenes in one body array (scene s = bodies
+// [sceneFirst[s], sceneFirst[s + 1])). Each scene keeps the reference's own loop state and
+// parameters, so it steps exactly as it would alone; this record holds them per scene.
+template <class R>
+struct SceneCtl {
+  R maxOverlap, maxApproach;  // as the Counters fields, per scene
+  R margin, eN, mu, pad;      // contact margin (0.1 x the scene's largest radius), restitution, friction
+  int velDone, stabRun, stabDone, posDone;
+  int velSweeps, stabSweeps, posSweeps, pad2;
+};
+
 template <class R>
 struct Dev {
   int cap = 0, maxPairs = 0, maxContacts = 0;
@@ -96,7 +107,42 @@ struct Dev {
   const R* pairMat = nullptr;  // null = feature off
   const R *hzE = nullptr, *hzNu = nullptr;
   Counters<R>* ctr = nullptr;
+  // batched form (all null / 1 for a single scene)
+  int numScenes = 1;
+  const int* sceneOf = nullptr;        // [real bodies] scene of each body
+  SceneCtl<R>* scn = nullptr;          // [numScenes]
+  const int* sceneWallOff = nullptr;   // [numScenes + 1] walls of scene s: sceneWallIdx[off[s] .. off[s + 1])
+  const int* sceneWallIdx = nullptr;
+  const int* sceneManFirst = nullptr;  // [numScenes + 1] first manifold of each scene
+  const int* sceneConFirst = nullptr;  // [3 (numScenes + 1)] first pair / plane / wall contact of each scene
+  const int* sceneLeafFirst = nullptr; // [numScenes + 1] first BVH leaf (sorted position) of each scene
 };
+
+// scene of body i (0 for a single scene)
+template <class R>
+__device__ __forceinline__ int sceneOfBody(const Dev<R>& d, int i) {
+  return d.sceneOf ? d.sceneOf[i] : 0;
+}
+// scene-local index of manifold m / contact c (the index the scene would have alone): the colour
+// priorities of the batched form are those of each scene stepped alone
+template <class R>
+__device__ __forceinline__ int localManifold(const Dev<R>& d, int m, int s) {
+  return d.sceneManFirst ? m - d.sceneManFirst[s] : m;
+}
+template <class R>
+__device__ __forceinline__ int localContact(const Dev<R>& d, int c, int s) {
+  if (!d.sceneConFirst)
+    return c;
+  const int S = d.numScenes;
+  const int* P = d.sceneConFirst;               // pair contacts: P[0..S], region end P[S]
+  const int* Q = d.sceneConFirst + (S + 1);     // plane contacts: Q[0..S]
+  const int* W = d.sceneConFirst + 2 * (S + 1); // wall contacts: W[0..S]
+  if (c < P[S])
+    return c - P[s];
+  if (c < Q[S])
+    return (P[s + 1] - P[s]) + (c - Q[s]);
+  return (P[s + 1] - P[s]) + (Q[s + 1] - Q[s]) + (c - W[s]);
+}
 
 // ---- launch geometry: grid-stride loops over a device-resident count ----
 inline int gridFor(long n, int block = kBlock) {

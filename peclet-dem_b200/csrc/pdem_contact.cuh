@@ -17,6 +17,32 @@ struct NarrowP {
   int haveMat;
 };
 
+// walls that body i meets: all of them, or (batched form) those of its scene, in wall order
+template <class R>
+__device__ __forceinline__ int wallBegin(const Dev<R>& d, int i) {
+  return d.sceneWallOff ? d.sceneWallOff[d.sceneOf[i]] : 0;
+}
+template <class R>
+__device__ __forceinline__ int wallEnd(const Dev<R>& d, const NarrowP<R>& P, int i) {
+  return d.sceneWallOff ? d.sceneWallOff[d.sceneOf[i] + 1] : P.numWalls;
+}
+template <class R>
+__device__ __forceinline__ int wallAt(const Dev<R>& d, int q) {
+  return d.sceneWallIdx ? d.sceneWallIdx[q] : q;
+}
+// contact margin of body i's scene, and the running max of the overlap (per scene when batched)
+template <class R>
+__device__ __forceinline__ R marginOf(const Dev<R>& d, const NarrowP<R>& P, int i) {
+  return d.scn ? d.scn[d.sceneOf[i]].margin : P.margin;
+}
+template <class R>
+__device__ __forceinline__ void overlapMax(const Dev<R>& d, int i, R v, R& mo) {
+  if (d.scn)
+    atomicMaxNonNeg(&d.scn[d.sceneOf[i]].maxOverlap, v);
+  else
+    runMax(mo, v);
+}
+
 // ---------------------------------------------------------------------------------------------
 // body-body probe of point k of A against B (src/narrowphase.hpp:192-265)
 template <class R>
@@ -79,10 +105,10 @@ __global__ void kNarrowSphere(Dev<R> d, int np, NarrowP<R> P, int* cnt, const in
       continue;
     const int2 pr = d.pairs[idx];
     const Probe<R> p = probeBody(d, pr.x, pr.y, 0, dA, dB, P.globalScale);
-    const bool hit = p.eff < P.margin;
+    const bool hit = p.eff < marginOf(d, P, pr.x);
     if (MODE == 0) {
       if (p.eff < R(0))
-        runMax(mo, -p.eff);
+        overlapMax(d, pr.x, -p.eff, mo);
       cnt[idx] = hit ? 1 : 0;
     } else if (hit) {
       const int s = off[idx];
@@ -92,6 +118,27 @@ __global__ void kNarrowSphere(Dev<R> d, int np, NarrowP<R> P, int* cnt, const in
   }
   if (MODE == 0)
     warpMaxAtomic(&d.ctr->maxOverlap, mo);
+}
+
+// spheres, write pass: one thread per contact slot s, whose pair is hitIdx[s] (the pairs the count
+// pass found in contact, in pair order), so every lane of a warp writes a contact
+__global__ void kHitIndex(int np, const int* off, int* hitIdx) {
+  GRID_STRIDE(idx, np) {
+    const int o = off[idx];
+    if (off[idx + 1] != o)
+      hitIdx[o] = (int)idx;
+  }
+}
+template <class R>
+__global__ void kNarrowSphereWrite(Dev<R> d, int nhit, NarrowP<R> P, const int* hitIdx) {
+  const ShapeDesc<R> dA = d.shapes[0], dB = d.shapes[0];
+  GRID_STRIDE(s, nhit) {
+    if (s >= d.maxContacts)
+      break;
+    const int2 pr = d.pairs[hitIdx[s]];
+    const Probe<R> p = probeBody(d, pr.x, pr.y, 0, dA, dB, P.globalScale);
+    writeBodyContact(d, (int)s, pr.x, pr.y, p, dB, P);
+  }
 }
 
 // point shells: one warp per pair, lanes over shell points in order
@@ -113,9 +160,9 @@ __global__ void kNarrowShell(Dev<R> d, int np, NarrowP<R> P, int* cnt, const int
       Probe<R> p;
       if (k < K) {
         p = probeBody(d, pr.x, pr.y, k, dA, dB, P.globalScale);
-        hit = p.eff < P.margin;
+        hit = p.eff < marginOf(d, P, pr.x);
         if (MODE == 0 && p.eff < R(0))
-          runMax(mo, -p.eff);
+          overlapMax(d, pr.x, -p.eff, mo);
       }
       const unsigned b = __ballot_sync(0xffffffffu, hit);
       if (MODE == 1 && hit) {
@@ -242,9 +289,9 @@ __global__ void kBoundary(Dev<R> d, int numReal, NarrowP<R> P, int* cntP, int* c
         BoundaryProbe<R> b;
         b.hit = false;
         if (k < K) {
-          b = probePlane(d, (int)i, pl, k, sd, s, P.margin);
+          b = probePlane(d, (int)i, pl, k, sd, s, marginOf(d, P, (int)i));
           if (MODE == 0 && b.dist < R(0))
-            runMax(mo, -b.dist);
+            overlapMax(d, (int)i, -b.dist, mo);
         }
         const unsigned m = __ballot_sync(0xffffffffu, b.hit);
         if (MODE == 1 && b.hit) {
@@ -259,15 +306,16 @@ __global__ void kBoundary(Dev<R> d, int numReal, NarrowP<R> P, int* cntP, int* c
       cntP[i] = tot;
     run = MODE ? baseWalls + offW[i] : 0;
     tot = 0;
-    for (int wi = 0; wi < P.numWalls; ++wi)
+    for (int q = wallBegin(d, (int)i); q < wallEnd(d, P, (int)i); ++q) {
+      const int wi = wallAt(d, q);
       for (int k0 = 0; k0 < K; k0 += 32) {
         const int k = k0 + lane;
         BoundaryProbe<R> b;
         b.hit = false;
         if (k < K) {
-          b = probeWall(d, (int)i, wi, k, sd, s, P.margin, MODE == 1);
+          b = probeWall(d, (int)i, wi, k, sd, s, marginOf(d, P, (int)i), MODE == 1);
           if (MODE == 0 && b.dist < R(0))
-            runMax(mo, -b.dist);
+            overlapMax(d, (int)i, -b.dist, mo);
         }
         const unsigned m = __ballot_sync(0xffffffffu, b.hit);
         if (MODE == 1 && b.hit) {
@@ -278,6 +326,7 @@ __global__ void kBoundary(Dev<R> d, int numReal, NarrowP<R> P, int* cntP, int* c
         run += __popc(m);
         tot += __popc(m);
       }
+    }
     if (MODE == 0 && lane == 0)
       cntW[i] = tot;
   }
@@ -295,9 +344,9 @@ __global__ void kBoundarySphere(Dev<R> d, int numReal, NarrowP<R> P, int* cntP, 
     const R s = d.scale[i] * P.globalScale;
     int run = MODE ? basePlanes + offP[i] : 0, tot = 0;
     for (int pl = 0; pl < P.numPlanes; ++pl) {
-      const BoundaryProbe<R> b = probePlane(d, (int)i, pl, 0, sd, s, P.margin);
+      const BoundaryProbe<R> b = probePlane(d, (int)i, pl, 0, sd, s, marginOf(d, P, (int)i));
       if (MODE == 0 && b.dist < R(0))
-        runMax(mo, -b.dist);
+        overlapMax(d, (int)i, -b.dist, mo);
       if (b.hit) {
         if (MODE == 1 && run < d.maxContacts)
           writeBoundaryContact(d, run, (int)i, b, false, 0, 0);
@@ -309,10 +358,11 @@ __global__ void kBoundarySphere(Dev<R> d, int numReal, NarrowP<R> P, int* cntP, 
       cntP[i] = tot;
     run = MODE ? baseWalls + offW[i] : 0;
     tot = 0;
-    for (int wi = 0; wi < P.numWalls; ++wi) {
-      const BoundaryProbe<R> b = probeWall(d, (int)i, wi, 0, sd, s, P.margin, MODE == 1);
+    for (int q = wallBegin(d, (int)i); q < wallEnd(d, P, (int)i); ++q) {
+      const int wi = wallAt(d, q);
+      const BoundaryProbe<R> b = probeWall(d, (int)i, wi, 0, sd, s, marginOf(d, P, (int)i), MODE == 1);
       if (MODE == 0 && b.dist < R(0))
-        runMax(mo, -b.dist);
+        overlapMax(d, (int)i, -b.dist, mo);
       if (b.hit) {
         if (MODE == 1 && run < d.maxContacts)
           writeBoundaryContact(d, run, (int)i, b, true, wi, P.haveMat);
@@ -330,16 +380,21 @@ __global__ void kBoundarySphere(Dev<R> d, int numReal, NarrowP<R> P, int* cntP, 
 // =============================================================================================
 // contact -> manifold (src/contact_preprocessing.hpp:320-471)
 // =============================================================================================
+// Key of a contact's body pair, (smaller index, larger index or "none" for a boundary contact),
+// packed as u << bits | v with the all-ones v for "none": the same order as the reference's
+// (u << 32 | v) pair key with 0xFFFFFFFF for a boundary, in 2 * bits bits (fewer sort passes).
+// bits is chosen so that every body index is below 2^bits - 1.
 template <class R>
-__global__ void kContactKeys(Dev<R> d, int nc, u64* keys, int* vals) {
+__global__ void kContactKeys(Dev<R> d, int nc, int bits, u64* keys, int* vals) {
+  const u64 none = (1ull << bits) - 1ull;
   GRID_STRIDE(i, nc) {
     const int2 ab = d.cab[i];
     u64 k;
     if (ab.y < 0)
-      k = ((u64)(unsigned)ab.x << 32) | 0xFFFFFFFFull;
+      k = ((u64)(unsigned)ab.x << bits) | none;
     else {
       const unsigned u = ab.x < ab.y ? ab.x : ab.y, v = ab.x < ab.y ? ab.y : ab.x;
-      k = ((u64)u << 32) | v;
+      k = ((u64)u << bits) | v;
     }
     keys[i] = k;
     vals[i] = (int)i;
@@ -358,13 +413,15 @@ __global__ void kSegStarts(int n, const int* headScan, int* segStart) {
 }
 // one thread per manifold: ordered sums over the segment's contacts (ascending contact index)
 template <class R>
-__global__ void kReduceManifolds(Dev<R> d, int nm, int nc, const int* segStart, const u64* keys, const int* perm) {
+__global__ void kReduceManifolds(Dev<R> d, int nm, int nc, int bits, const int* segStart, const u64* keys,
+                                 const int* perm) {
+  const u64 none = (1ull << bits) - 1ull;
   GRID_STRIDE(m, nm) {
     const int b = segStart[m], e = (m + 1 < nm) ? segStart[m + 1] : nc;
     const u64 k = keys[b];
-    const int A = (int)(k >> 32);
-    const unsigned v = (unsigned)(k & 0xFFFFFFFFull);
-    const int B = (v == 0xFFFFFFFFu) ? -1 : (int)v;
+    const int A = (int)(k >> bits);
+    const u64 v = k & none;
+    const int B = (v == none) ? -1 : (int)v;
     int npts = 0;
     V3<R> N{0, 0, 0}, TA{0, 0, 0}, TB{0, 0, 0}, rA{0, 0, 0}, rB{0, 0, 0}, wv{0, 0, 0};
     R es = 0, mus = 0;
@@ -453,12 +510,23 @@ __global__ void kGatherWarm(Dev<R> d, int nm, int prevCount) {
     d.posImp[i] = warm ? d.prevPosImp[lo] : R(0);
   }
 }
+// ledger sort keys: the 64-bit pair key (u << 32 | v, v = 0xFFFFFFFF for a boundary, all ones for
+// an empty manifold) packed order-preservingly into 2 * bits bits, with the manifold index as value
+__global__ void kLedgerKeys(int nm, int bits, const u64* pairKeys, u64* packed, int* vals) {
+  const u64 none = (1ull << bits) - 1ull;
+  GRID_STRIDE(i, nm) {
+    const u64 k = pairKeys[i];
+    const u64 u = k >> 32, v = k & 0xFFFFFFFFull;
+    packed[i] = ((u == 0xFFFFFFFFull ? none : u) << bits) | (v == 0xFFFFFFFFull ? none : v);
+    vals[i] = (int)i;
+  }
+}
 // commitPairKeysLambda (:160-192): keys/perm already stably sorted by key
 template <class R>
-__global__ void kCommitLedger(Dev<R> d, int nm, const u64* sortedKeys, const int* perm) {
+__global__ void kCommitLedger(Dev<R> d, int nm, const int* perm) {
   GRID_STRIDE(i, nm) {
     const int j = perm[i];
-    d.prevKeys[i] = sortedKeys[i];
+    d.prevKeys[i] = d.pairKeys[j];
     d.prevLambda[i] = d.lambda[j];
     d.prevLambdaT[i] = d.lambdaT[j];
   }
@@ -625,6 +693,14 @@ __device__ __forceinline__ void colorEnds(const Dev<R>& d, int i, int& ea, int& 
     eb = ab.y;
   }
 }
+// colour priority of entry i with first body ea: the key of its scene-local index (batched form)
+template <class R, bool MANIFOLD>
+__device__ __forceinline__ long long entryKey(const Dev<R>& d, int i, int ea) {
+  if (!d.sceneOf)
+    return colorKey(i);
+  const int s = d.sceneOf[ea];
+  return colorKey(MANIFOLD ? localManifold(d, i, s) : localContact(d, i, s));
+}
 template <class R>
 __global__ void kColorInitManifolds(Dev<R> d, int nm) {
   GRID_STRIDE(i, nm) {
@@ -651,7 +727,7 @@ __global__ void kColorContend(Dev<R> d, int ne, const int* col) {
       continue;
     int ea, eb;
     colorEnds<R, MANIFOLD>(d, (int)i, ea, eb);
-    const long long k = colorKey((int)i);
+    const long long k = entryKey<R, MANIFOLD>(d, (int)i, ea);
     atomicMax(&d.winner[ea], k);
     if (eb >= 0)
       atomicMax(&d.winner[eb], k);
@@ -664,7 +740,7 @@ __global__ void kColorCommit(Dev<R> d, int ne, int* col, int* remaining) {
       continue;
     int ea, eb;
     colorEnds<R, MANIFOLD>(d, (int)i, ea, eb);
-    const long long k = colorKey((int)i);
+    const long long k = entryKey<R, MANIFOLD>(d, (int)i, ea);
     if (d.winner[ea] != k || (eb >= 0 && d.winner[eb] != k)) {
       atomicAdd(remaining, 1);
       continue;

@@ -81,7 +81,7 @@ __global__ void __launch_bounds__(kBlock) kSweepLoop(Dev<R> d, const int* order,
       if (!serial || lead)
         for (long t = serial ? 0 : gtid; t < n; t += serial ? 1 : gstride) {
           if (KIND == 0)
-            pgsOne(d, order[b + t], P, mx);
+            pgsOne(d, order[b + t], P, mx, LOOP);
           else if (KIND == 1)
             gsOne(d, order[b + t], P, mx);
           else
@@ -93,7 +93,29 @@ __global__ void __launch_bounds__(kBlock) kSweepLoop(Dev<R> d, const int* order,
         return;
     }
     // END of this sweep, then BEGIN of the next one
-    if (lead) {
+    if (d.scn) {  // batched form: every scene's own END/BEGIN; done when all scenes are
+      if (blockIdx.x == 0) {
+        int notDone = 0;
+        for (int s = threadIdx.x; s < d.numScenes; s += blockDim.x) {
+          SceneCtl<R>& q = d.scn[s];
+          volatile int* dn = LOOP == 1 ? &q.velDone : LOOP == 2 ? &q.stabDone : &q.posDone;
+          volatile R* m = KIND == 2 ? &q.maxOverlap : &q.maxApproach;
+          if (!*dn) {
+            const R mv = *m;
+            if (KIND == 2 ? (mv < thr) : (mv <= thr)) {
+              *dn = 1;
+            } else if (it + 1 < iters) {
+              *m = R(0);
+              (LOOP == 1 ? q.velSweeps : LOOP == 2 ? q.stabSweeps : q.posSweeps) += 1;
+            }
+          }
+          notDone |= !*dn;
+        }
+        notDone = __syncthreads_or(notDone);
+        if (threadIdx.x == 0 && !notDone)
+          *done = 1;
+      }
+    } else if (lead) {
       const R m = *reinterpret_cast<volatile R*>(mxp);
       const bool stop = KIND == 2 ? (m < thr) : (m <= thr);
       if (stop) {
@@ -119,8 +141,10 @@ __global__ void __launch_bounds__(kBlock) kSweepLoop(Dev<R> d, const int* order,
 // of round r lives in remCnt[r % 3]; the lead zeroes the slot of round r + 1 during round r.
 // At the end the colour statistics (largest colour, entries left uncoloured) are accumulated into
 // stats[0] (atomic max, preset to INT_MIN) and stats[1] (preset to 0).
+constexpr int kColorBlock = 1024;  // one large block per SM: fewer arrivals per grid barrier
+
 template <class R, bool MANIFOLD>
-__global__ void __launch_bounds__(kBlock) kColorLoop(Dev<R> d, int ne, int maxRounds, int* col, long long* winA,
+__global__ void __launch_bounds__(kColorBlock) kColorLoop(Dev<R> d, int ne, int maxRounds, int* col, long long* winA,
                                                      long long* winB, int* remCnt, int* stats, GridBar gb) {
   const bool lead = (blockIdx.x | threadIdx.x) == 0;
   const long gtid = (long)blockIdx.x * blockDim.x + threadIdx.x, gstride = (long)gridDim.x * blockDim.x;
@@ -135,7 +159,7 @@ __global__ void __launch_bounds__(kBlock) kColorLoop(Dev<R> d, int ne, int maxRo
         continue;
       int ea, eb;
       colorEnds<R, MANIFOLD>(d, (int)i, ea, eb);
-      const long long k = colorKey((int)i);
+      const long long k = entryKey<R, MANIFOLD>(d, (int)i, ea);
       atomicMax(&win[ea], k);
       if (eb >= 0)
         atomicMax(&win[eb], k);
@@ -148,7 +172,7 @@ __global__ void __launch_bounds__(kBlock) kColorLoop(Dev<R> d, int ne, int maxRo
         continue;
       int ea, eb;
       colorEnds<R, MANIFOLD>(d, (int)i, ea, eb);
-      const long long k = colorKey((int)i);
+      const long long k = entryKey<R, MANIFOLD>(d, (int)i, ea);
       if (win[ea] != k || (eb >= 0 && win[eb] != k)) {
         ++lost;
         nxt[ea] = -1;

@@ -43,6 +43,7 @@ Sim<R>::Sim(int capacity) {
   }
   ctr_.ensure(1, false, stream_);
   allocate(capacity, capacity * 64, capacity * 16);
+  uploadHertzMaterials();
   initializeShape(SHAPE_SPHERE, R(1), R(0), R(0));
 }
 template <class R>
@@ -174,23 +175,28 @@ Counters<R> Sim<R>::readCounters() {
 // blocks of a cooperative launch of `kernel`: resident blocks per SM (at most 4) x SMs
 template <class R>
 template <class K>
-int Sim<R>::coopGrid(K kernel) {
+int Sim<R>::coopGrid(K kernel, int block) {
   int per = 0;
-  cudaCheck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kBlock, 0), "occupancy");
+  cudaCheck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, block, 0), "occupancy");
   if (per < 1)
     throw CudaError("persistent loop kernel cannot be resident");
   return std::min(per, 4) * numSMs_;
 }
 template <class R>
 template <class K, class... A>
-void Sim<R>::launchCoop(K kernel, A... args) {
+void Sim<R>::launchCoopB(K kernel, int block, A... args) {
   gbar_.ensure(2, false, stream_);
   cudaCheck(cudaMemsetAsync(gbar_.p, 0, 2 * sizeof(unsigned), stream_), "memset barrier");
   void* argv[] = {static_cast<void*>(&args)...};
   ++launches_;
-  cudaCheck(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(kernel), dim3(coopGrid(kernel)), dim3(kBlock),
-                                        argv, 0, stream_),
+  cudaCheck(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(kernel), dim3(coopGrid(kernel, block)),
+                                        dim3(block), argv, 0, stream_),
             "cooperative launch");
+}
+template <class R>
+template <class K, class... A>
+void Sim<R>::launchCoop(K kernel, A... args) {
+  launchCoopB(kernel, kBlock, args...);
 }
 
 // ---- CUB helpers ----
@@ -397,6 +403,13 @@ void Sim<R>::setHertzMaterial(int mat, R E, R nu) {
     throw std::invalid_argument("material id out of range");
   hzE_[mat] = E;
   hzNu_[mat] = nu;
+  uploadHertzMaterials();
+}
+template <class R>
+void Sim<R>::uploadHertzMaterials() {
+  cudaCheck(cudaMemcpyAsync(hzED_.p, hzE_, sizeof hzE_, cudaMemcpyHostToDevice, stream_), "H2D hertz E");
+  cudaCheck(cudaMemcpyAsync(hzNuD_.p, hzNu_, sizeof hzNu_, cudaMemcpyHostToDevice, stream_), "H2D hertz nu");
+  sync();
 }
 template <class R>
 void Sim<R>::setMaterialIds(const int* ids, int n) {
@@ -823,8 +836,11 @@ void Sim<R>::detectAll(R margin) {
   if (np > 0 && tot[0] > 0) {
     if (shell)
       ++launches_, kNarrowShell<R, 1><<<gridFor((long)np * 32), kBlock, 0, stream_>>>(d_, np, P, nullptr, iB_.p);
-    else
-      ++launches_, kNarrowSphere<R, 1><<<gridFor(np), kBlock, 0, stream_>>>(d_, np, P, nullptr, iB_.p);
+    else {
+      // iA_ (the 0/1 counts) is free after the scan: it receives the hit pair of every slot
+      ++launches_, kHitIndex<<<gridFor(np), kBlock, 0, stream_>>>(np, iB_.p, iA_.p);
+      ++launches_, kNarrowSphereWrite<R><<<gridFor(tot[0]), kBlock, 0, stream_>>>(d_, tot[0], P, iA_.p);
+    }
     KCHECK("narrow write");
   }
   if (boundary && tot[1] + tot[2] > 0 && tot[0] < maxContacts_) {
@@ -856,9 +872,10 @@ int Sim<R>::reduceManifolds(int nc) {
   head_.ensure(nc, false, stream_);
   headScan_.ensure(nc, false, stream_);
   segStart_.ensure(nc + 1, false, stream_);
-  ++launches_, kContactKeys<<<gridFor(nc), kBlock, 0, stream_>>>(d_, nc, ckeys_.p, cpermIn_.p);
+  const int kb = bitsFor((long)numParticles_ + 1);
+  ++launches_, kContactKeys<R><<<gridFor(nc), kBlock, 0, stream_>>>(d_, nc, kb, ckeys_.p, cpermIn_.p);
   KCHECK("contact keys");
-  sortPairs(ckeys_.p, ckeysS_.p, cpermIn_.p, cperm_.p, nc, 64);
+  sortPairs(ckeys_.p, ckeysS_.p, cpermIn_.p, cperm_.p, nc, 2 * kb);
   ++launches_, kSegHeads<<<gridFor(nc), kBlock, 0, stream_>>>(nc, ckeysS_.p, head_.p);
   KCHECK("seg heads");
   inclusiveSum(head_.p, headScan_.p, nc);
@@ -867,7 +884,7 @@ int Sim<R>::reduceManifolds(int nc) {
   sync();
   ++launches_, kSegStarts<<<gridFor(nc), kBlock, 0, stream_>>>(nc, headScan_.p, segStart_.p);
   KCHECK("seg starts");
-  ++launches_, kReduceManifolds<<<gridFor(nm), kBlock, 0, stream_>>>(d_, nm, nc, segStart_.p, ckeysS_.p, cperm_.p);
+  ++launches_, kReduceManifolds<<<gridFor(nm), kBlock, 0, stream_>>>(d_, nm, nc, kb, segStart_.p, ckeysS_.p, cperm_.p);
   KCHECK("reduce manifolds");
   return nm;
 }
@@ -893,9 +910,9 @@ int Sim<R>::colorGraph(bool manifold, int ne, int nb, int& leftover) {
   gbar_.ensure(2, false, stream_);
   const GridBar gb{gbar_.p, &ctr_.p->err};
   if (manifold)
-    launchCoop(kColorLoop<R, true>, d_, ne, nb + 2, col, winner_.p, winner2_.p, colorAux_.p, colorAux_.p + 3, gb);
+    launchCoopB(kColorLoop<R, true>, kColorBlock, d_, ne, nb + 2, col, winner_.p, winner2_.p, colorAux_.p, colorAux_.p + 3, gb);
   else
-    launchCoop(kColorLoop<R, false>, d_, ne, nb + 2, col, winner_.p, winner2_.p, colorAux_.p, colorAux_.p + 3, gb);
+    launchCoopB(kColorLoop<R, false>, kColorBlock, d_, ne, nb + 2, col, winner_.p, winner2_.p, colorAux_.p, colorAux_.p + 3, gb);
   KCHECK("colour loop");
   int res[2];
   cudaCheck(cudaMemcpyAsync(res, colorAux_.p + 3, sizeof res, cudaMemcpyDeviceToHost, stream_), "D2H");
@@ -1053,7 +1070,14 @@ void Sim<R>::demStep() {
       launchCoop(kSweepLoop<R, 1, 1>, d_, (const int*)mOrder_.p, (const int*)mOff_.p, ncolV, velIters_, sp, thr, gb);
     KCHECK("velocity loop");
   }
-  for (int it = 0; it < (velPersistent ? 0 : velIters_); ++it) {
+  // no colours and no fallback: the first sweep is empty, its END finds maxApproach = 0 <= thr
+  // and the loop is done, so one BEGIN/END pair stands for the whole loop
+  const bool velEmpty = useGS_ && !legacyFriction && velLeft == 0 && ncolV <= 0 && velIters_ > 0;
+  if (velEmpty) {
+    ++launches_, kCtl<<<1, 1, 0, s>>>(ctr_.p, CTL_VEL_BEGIN, R(0), 0);
+    ++launches_, kCtl<<<1, 1, 0, s>>>(ctr_.p, CTL_VEL_END, usePGS ? R(0.02) * vRest : vRest, 0);
+  }
+  for (int it = 0; it < (velPersistent || velEmpty ? 0 : velIters_); ++it) {
     if (legacyFriction && nc > 0) {
       // runs at the top of every iteration the loop reaches (src/sim.hpp:224-226): with the
       // coloured solve the adaptive stop ends the loop, so it is gated on the loop flag
@@ -1130,9 +1154,11 @@ void Sim<R>::demStep() {
       lkeysS_.ensure(nm, false, s);
       lpermIn_.ensure(nm, false, s);
       lperm_.ensure(nm, false, s);
-      ++launches_, kIota<R><<<gridFor(nm), B, 0, s>>>(lpermIn_.p, nm);
-      sortPairs(pairKeys_.p, lkeysS_.p, lpermIn_.p, lperm_.p, nm, 64);
-      ++launches_, kCommitLedger<<<gridFor(nm), B, 0, s>>>(d_, nm, lkeysS_.p, lperm_.p);
+      const int kb = bitsFor((long)numParticles_ + 1);
+      lkeysIn_.ensure(nm, false, s);
+      ++launches_, kLedgerKeys<<<gridFor(nm), B, 0, s>>>(nm, kb, pairKeys_.p, lkeysIn_.p, lpermIn_.p);
+      sortPairs(lkeysIn_.p, lkeysS_.p, lpermIn_.p, lperm_.p, nm, 2 * kb);
+      ++launches_, kCommitLedger<<<gridFor(nm), B, 0, s>>>(d_, nm, lperm_.p);
       KCHECK("commit ledger");
     }
     prevPairCount_ = nm;
@@ -1185,7 +1211,12 @@ void Sim<R>::demStep() {
     launchCoop(kSweepLoop<R, 2, 3>, d_, (const int*)cOrder_.p, (const int*)cOff_.p, ncolP, posIters_, sp, posTol, gb);
     KCHECK("position loop");
   }
-  for (int it = 0; it < (posPersistent ? 0 : posIters_); ++it) {
+  const bool posEmpty = useGS_ && posLeft == 0 && ncolP <= 0 && posIters_ > 0 && posTol > R(0);
+  if (posEmpty) {  // as velEmpty: maxOverlap = 0 < posTol ends the loop after its first sweep
+    ++launches_, kCtl<<<1, 1, 0, s>>>(ctr_.p, CTL_POS_BEGIN, R(0), 0);
+    ++launches_, kCtl<<<1, 1, 0, s>>>(ctr_.p, CTL_POS_END, posTol, 0);
+  }
+  for (int it = 0; it < (posPersistent || posEmpty ? 0 : posIters_); ++it) {
     if (useGS_) {
       ++launches_, kCtl<<<1, 1, 0, s>>>(ctr_.p, CTL_POS_BEGIN, R(0), 0);
       for (int col = 0; col < ncolP; ++col)

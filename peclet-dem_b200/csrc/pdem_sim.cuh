@@ -212,7 +212,7 @@ class Sim {
   // colour orders
   DBuf<int> mOrder_, mOff_, cOrder_, cOff_;
   // ledger sort
-  DBuf<u64> lkeysS_;
+  DBuf<u64> lkeysS_, lkeysIn_;
   DBuf<int> lperm_, lpermIn_;
   // incidence lists
   DBuf<int> incKeys_, incKeysS_, incVals_, incValsS_, incOff_;
@@ -236,6 +236,7 @@ class Sim {
   void refreshDev();
   void uploadShape();
   void uploadWalls();
+  void uploadHertzMaterials();
   int ghostCapacity(int nReal, R band) const;
   R maxOwnedRadius();
   void resetGhosts(R band);
@@ -251,7 +252,9 @@ class Sim {
   void demStep();
   Counters<R> readCounters();
   template <class K>
-  int coopGrid(K kernel);
+  int coopGrid(K kernel, int block);
+  template <class K, class... A>
+  void launchCoopB(K kernel, int block, A... args);
   template <class K, class... A>
   void launchCoop(K kernel, A... args);
   template <class T>

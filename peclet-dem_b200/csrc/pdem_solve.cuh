@@ -115,6 +115,67 @@ __global__ void kCtl(Counters<R>* c, int op, R thr, int mode) {
       break;
   }
 }
+// batched form: the same control for every scene (one block); the global flags become "every
+// scene done" and "some scene runs the stabilization pass", so whole launches still skip
+template <class R>
+__global__ void kCtlScenes(Counters<R>* c, SceneCtl<R>* scn, int S, int op, R thr, int mode) {
+  int notDone = 0, anyStab = 0;
+  for (int s = threadIdx.x; s < S; s += blockDim.x) {
+    SceneCtl<R>& q = scn[s];
+    switch (op) {
+      case CTL_VEL_BEGIN:
+        if (!q.velDone) {
+          q.maxApproach = R(0);
+          q.velSweeps += 1;
+        }
+        break;
+      case CTL_VEL_END:
+        if (!q.velDone && q.maxApproach <= thr)
+          q.velDone = 1;
+        break;
+      case CTL_STAB_DECIDE:
+        q.stabRun = (mode != 0 && q.maxApproach > thr) ? 1 : 0;
+        q.stabDone = q.stabRun ? 0 : 1;
+        break;
+      case CTL_STAB_BEGIN:
+        if (!q.stabDone) {
+          q.maxApproach = R(0);
+          q.stabSweeps += 1;
+        }
+        break;
+      case CTL_STAB_END:
+        if (!q.stabDone && q.maxApproach <= thr)
+          q.stabDone = 1;
+        break;
+      case CTL_POS_BEGIN:
+        if (!q.posDone) {
+          q.maxOverlap = R(0);
+          q.posSweeps += 1;
+        }
+        break;
+      case CTL_POS_END:
+        if (!q.posDone && q.maxOverlap < thr)
+          q.posDone = 1;
+        break;
+    }
+    notDone |= (op <= CTL_VEL_END) ? !q.velDone : (op <= CTL_STAB_END) ? !q.stabDone : !q.posDone;
+    anyStab |= q.stabRun;
+  }
+  notDone = __syncthreads_or(notDone);
+  anyStab = __syncthreads_or(anyStab);
+  if (threadIdx.x == 0) {
+    if (op <= CTL_VEL_END) {
+      c->velDone = !notDone;
+    } else if (op == CTL_STAB_DECIDE) {
+      c->stabRun = anyStab;
+      c->stabDone = !anyStab;
+    } else if (op <= CTL_STAB_END) {
+      c->stabDone = !notDone;
+    } else {
+      c->posDone = !notDone;
+    }
+  }
+}
 template <class R>
 __device__ __forceinline__ bool gateOpen(const Counters<R>* c, int gate) {
   // gate: 0 always, 1 main velocity loop, 2 stabilization loop, 3 position loop
@@ -284,14 +345,38 @@ __global__ void kWarmApply(Dev<R> d, int numReal, Incidence inc) {
 
 // ---------------------------------------------------------------------------------------------
 // projected Gauss-Seidel sweep of one colour (src/solver_velocity.hpp:641-858)
+// batched form: the scene of a solve entry, its done flag for the loop (1 main velocity,
+// 2 stabilization, 3 position) and the per-scene running maximum
 template <class R>
-__device__ __forceinline__ void pgsOne(const Dev<R>& d, int idx, const SolveP<R>& P, R& mx) {
+__device__ __forceinline__ bool sceneDone(const Dev<R>& d, int s, int loop) {
+  const SceneCtl<R>& S = d.scn[s];
+  return loop == 1 ? S.velDone != 0 : loop == 2 ? S.stabDone != 0 : S.posDone != 0;
+}
+template <class R>
+__device__ __forceinline__ void loopMax(const Dev<R>& d, int s, bool position, R v, R& mx) {
+  if (d.scn)
+    atomicMaxNonNeg(position ? &d.scn[s].maxOverlap : &d.scn[s].maxApproach, v);
+  else
+    runMax(mx, v);
+}
+
+template <class R>
+__device__ __forceinline__ void pgsOne(const Dev<R>& d, int idx, const SolveP<R>& P, R& mx, int loop) {
+  int sc = 0;
+  R eG = P.eN, muG = P.mu;
+  if (d.scn) {
+    sc = d.sceneOf[d.mab[idx].x];
+    if (sceneDone(d, sc, loop))
+      return;
+    eG = d.scn[sc].eN;
+    muG = d.scn[sc].mu;
+  }
   const ManifoldView<R> v = loadManifold(d, idx);
   const int ra = v.ra, rb = v.rb;
   const bool hasB = d.mab[idx].y >= 0;
   const V3<R> vA = v3(d.velPred[ra]), wA = v3(d.angVelPred[ra]);
   V3<R> vB{0, 0, 0}, wB{0, 0, 0};
-  R e = P.eN;
+  R e = eG;
   if (hasB) {
     vB = v3(d.velPred[rb]);
     wB = v3(d.angVelPred[rb]);
@@ -343,7 +428,7 @@ __device__ __forceinline__ void pgsOne(const Dev<R>& d, int idx, const SolveP<R>
   V3<R> vA2 = vA, wA2 = wA, vB2 = vB, wB2 = wB;
   if (dA != R(0)) {
     d.lambda[idx] = pNew;
-    runMax(mx, fabs(dA) * wT / lenN);
+    loopMax(d, sc, false, fabs(dA) * wT / lenN, mx);
     const R lam = -sgn * dA;
     const V3<R> J = mul(v.N, lam), JA = mul(v.TA, lam), JB = mul(v.TB, lam);
     if (applyA) {
@@ -356,7 +441,7 @@ __device__ __forceinline__ void pgsOne(const Dev<R>& d, int idx, const SolveP<R>
     }
   }
   // friction cone
-  R mu = P.mu;
+  R mu = muG;
   const R fa = v.muSum * v.invN;
   if (fa >= R(0))
     mu = fa;
@@ -401,7 +486,7 @@ __device__ __forceinline__ void pgsOne(const Dev<R>& d, int idx, const SolveP<R>
       d.lambdaT[idx] = q4(ltNew);
       const R dl = sqrt(dot(dd, dd));
       if (wTt > R(1e-9))
-        runMax(mx, dl * wTt);
+        loopMax(d, sc, false, dl * wTt, mx);
       if (applyA) {
         vA2 = add(vA2, mul(dd, v.imA));
         wA2 = add(wA2, angResponse(v.qA, cross(v.rAa, dd), v.iIA));
@@ -432,7 +517,7 @@ __global__ void kPGSColor(Dev<R> d, const int* order, const int* coff, int color
   R mx = R(0);
   for (long t = serial ? 0 : (long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
        t += serial ? 1 : (long)gridDim.x * blockDim.x) {
-    pgsOne(d, order[b + t], P, mx);
+    pgsOne(d, order[b + t], P, mx, gate);
   }
   if (serial)
     atomicMaxNonNeg(&d.ctr->maxApproach, mx);
@@ -443,6 +528,14 @@ __global__ void kPGSColor(Dev<R> d, const int* order, const int* coff, int color
 // one-shot coloured GS of one colour, g = 0 path (src/solver_velocity.hpp:989-1137)
 template <class R>
 __device__ __forceinline__ void gsOne(const Dev<R>& d, int idx, const SolveP<R>& P, R& mx) {
+  int sc = 0;
+  R eG = P.eN;
+  if (d.scn) {
+    sc = d.sceneOf[d.mab[idx].x];
+    if (sceneDone(d, sc, 1))
+      return;
+    eG = d.scn[sc].eN;
+  }
   const ManifoldView<R> v = loadManifold(d, idx);
   const bool hasB = d.mab[idx].y >= 0;
   const V3<R> vA = v3(d.velPred[v.ra]), wA = v3(d.angVelPred[v.ra]);
@@ -451,7 +544,7 @@ __device__ __forceinline__ void gsOne(const Dev<R>& d, int idx, const SolveP<R>&
     vB = v3(d.velPred[v.rb]);
     wB = v3(d.angVelPred[v.rb]);
   }
-  R e = P.eN;
+  R e = eG;
   if (!hasB)
     vB = mul(v.wv, v.invN);
   {
@@ -479,7 +572,7 @@ __device__ __forceinline__ void gsOne(const Dev<R>& d, int idx, const SolveP<R>&
   const R wT = wAn + wBn;
   if (wT <= R(0))
     return;
-  runMax(mx, fabs(vn) / lenN);
+  loopMax(d, sc, false, fabs(vn) / lenN, mx);
   if (fabs(vn) < P.vRest * lenN)
     e = R(0);
   const R lam = (-e * vn - vn) / wT;
@@ -823,6 +916,12 @@ __device__ __forceinline__ bool posConstraint(const Dev<R>& d, int idx, V3<R>& n
 }
 template <class R>
 __device__ __forceinline__ void posGSOne(const Dev<R>& d, int idx, R& mx) {
+  int sc = 0;
+  if (d.scn) {
+    sc = d.sceneOf[d.cab[idx].x];
+    if (sceneDone(d, sc, 3))
+      return;
+  }
   V3<R> nv;
   R C = R(0), wT = R(0);
   int A, B;
@@ -840,7 +939,7 @@ __device__ __forceinline__ void posGSOne(const Dev<R>& d, int idx, R& mx) {
     const V3<R> pB = v3(d.posPred[B]);
     d.posPred[B] = q4(add(pB, V3<R>{-nv.x * dl * imB, -nv.y * dl * imB, -nv.z * dl * imB}));
   }
-  runMax(mx, -C);
+  loopMax(d, sc, true, -C, mx);
 }
 template <class R>
 __global__ void kPosGSColor(Dev<R> d, const int* order, const int* coff, int color, int gate) {
