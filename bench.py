@@ -131,6 +131,52 @@ def aggregate_rate(world, n, substeps, steps, t_max):
     return world * n * substeps * steps / t_max
 
 
+def split_scenes(sizes, world):
+    """Scenes of the batched form per rank: largest first to the rank with the fewest bodies."""
+    loads = [0] * world
+    owner = [0] * len(sizes)
+    for s in sorted(range(len(sizes)), key=lambda k: -sizes[k]):
+        r = min(range(world), key=lambda k: loads[k])
+        owner[s] = r
+        loads[r] += sizes[s]
+    return [[s for s in range(len(sizes)) if owner[s] == r] for r in range(world)]
+
+
+def run_batched(args, rank, world, dist, dem):
+    """Batched rotating drums (512 scenes) in one simulation per GPU, FP64; scenes are split over
+    the ranks with no exchange while stepping. Returns the sub-object of the JSON line."""
+    from peclet.dem import workloads as W
+    from peclet.dem.batch import apply_batch
+    scenes, extras = W.rotating_drums(scenes=args.drums)
+    mine = split_scenes([sc.n for sc in scenes], world)[rank]
+    sc_m = [scenes[s] for s in mine]
+    n_all = sum(sc.n for sc in scenes)
+    n_mine = sum(sc.n for sc in sc_m)
+    sim = dem.Simulation(n_mine + 8, "fp64")
+    apply_batch(sim, sc_m, [extras[s] for s in mine])
+    dt = sc_m[0].dt
+    for _ in range(args.warmup * SUBSTEPS):
+        sim.step(dt)
+    if dist is not None:
+        dist.barrier()
+    sim.profile_enable(True)
+    for _ in range(args.steps * SUBSTEPS):
+        sim.step(dt)
+    stages, launches = sim.profile_read()
+    sim.profile_enable(False)
+    t_max = max_over_ranks(sum(ms for ms, _ in stages.values()) / 1e3, dist, "cuda")
+    per_step = {k: round(ms / args.steps, 3) for k, (ms, c) in stages.items() if c}
+    sweeps = sim.scene_counters()
+    sim.close()
+    return {"workload": f"rotating_drums_{len(scenes)}_scenes", "scenes": len(scenes), "particles": n_all,
+            "value": n_all * SUBSTEPS * args.steps / t_max, "unit": METRIC, "precision": "fp64",
+            "ms_per_step": 1e3 * t_max / args.steps, "gpu_launches": launches, "stages_ms_per_step": per_step,
+            "err_vs_fp64": 0.0, "scaling": "weak (scenes split over ranks)",
+            "mean_sweeps_last_substep": {"velocity": float(sweeps[:, 2].mean()), "position": float(sweeps[:, 4].mean())},
+            "config": "R 50 mm, L 20 mm drums, omega U[0.5,3] rad/s, N_s U{256..8192} capped at 30% fill of the "
+                      "lower half, radii U[0.8,1.2] mm, mu U[0.2,0.8], e U[0.3,0.9], dt 5e-5 s / 10 substeps"}
+
+
 # ---------------------------------------------------------------------------------------------
 def cpu_reference(scene, substeps, threads):
     """Time the reference's own substep (OpenMP shim build) for `substeps` calls; returns
@@ -235,16 +281,20 @@ def run_ours(args):
     force = np.zeros((n, 3))
     barrier()
     te = time.perf_counter()
+    laps = []
     for _ in range(args.steps):
+        tl = time.perf_counter()
         sim.set_external_forces(force)
         for _ in range(SUBSTEPS):
             sim.step(scene.dt)
         pos = sim.get_positions()
         vel = sim.get_velocities()
+        laps.append(round(1e3 * (time.perf_counter() - tl), 2))
     e2e_s = time.perf_counter() - te
     assert np.all(np.isfinite(pos)) and np.all(np.isfinite(vel))
     e2e = {"value": world * n * SUBSTEPS * args.steps / e2e_s, "unit": METRIC,
-           "h2d_bytes_per_step": int(force.nbytes), "d2h_bytes_per_step": int(pos.nbytes + vel.nbytes)}
+           "h2d_bytes_per_step": int(force.nbytes), "d2h_bytes_per_step": int(pos.nbytes + vel.nbytes),
+           "ms_per_step_each": laps}
 
     # ---- roofline of the dominant stage ----
     per_step = {k: (ms / args.steps, c / args.steps) for k, (ms, c) in stages.items() if c}
@@ -277,6 +327,8 @@ def run_ours(args):
                "sample": f"{args.cpu_substeps} substeps of the same {n}-sphere workload (reference code, "
                          f"OpenMP Kokkos-shim build, float), {el:.1f} s"}
 
+    batched = run_batched(args, rank, world, dist, dem) if args.drums > 0 else None
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
@@ -286,7 +338,7 @@ def run_ours(args):
             "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu,
             "clocks": clocks.summary(), "wall_ms_per_step": 1e3 * wall / args.steps,
             "stages_ms_per_step": {k: round(v[0], 4) for k, v in per_step.items()},
-            "counts_last_substep": counts, "sweeps": sweeps,
+            "counts_last_substep": counts, "sweeps": sweeps, "batched": batched,
         }
         print(json.dumps(line))
     if dist is not None:
@@ -303,6 +355,7 @@ def main():
     ap.add_argument("--particles", type=int, default=262144)
     ap.add_argument("--cpu-substeps", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--drums", type=int, default=512, help="scenes of the batched line (0: skip it)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)

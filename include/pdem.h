@@ -153,6 +153,24 @@ long pdem_debug_hertz(pdem_handle h, unsigned long long* keys, double* xi, long 
 /* test hook: set the contact buffer capacity (overflow / clamp behaviour) */
 int pdem_debug_set_max_contacts(pdem_handle h, int max_contacts);
 
+/* ---- batched form (no reference counterpart: the reference steps one scene per Simulation) ----
+ * Several independent scenes share one simulation: scene s owns the bodies
+ * [first_body[s], first_body[s+1]) of the arrays given to set_positions (call set_scenes after it;
+ * first_body[0] = 0, first_body[nscenes] = particle count, at most 1023 scenes). Every scene is
+ * stepped exactly as a simulation of that scene alone would step it: candidate pairs only inside
+ * a scene, its own contact margin (0.1 x its largest radius), restitution and friction, walls and
+ * adaptive iteration stops, and the colour priorities of its own indices. Scenes may overlap in
+ * space. Shared: shape, global scale, gravity, iterations, dt, stabilization mode, planes (walls
+ * with scene -1). Not supported: periodic domains, growth, thermostat, zero-gravity friction,
+ * the Hertz engine. */
+int pdem_set_scenes(pdem_handle h, int nscenes, const int* first_body);
+int pdem_set_scene_material(pdem_handle h, int scene, double e_n, double mu);
+/* the wall (index from add_sdf_wall) is met only by the bodies of `scene` (-1: by every scene) */
+int pdem_set_wall_scene(pdem_handle h, int wall, int scene);
+/* per scene, 5 values: max overlap, max approach, velocity / stabilization / position sweeps of
+ * the last substep; returns the number of scenes (0 when not batched, -1 on error) */
+long pdem_scene_counters(pdem_handle h, double* out, long cap);
+
 /* ---- instrumentation (no reference counterpart; the reference's Kokkos labels serve Kokkos Tools) ----
  * profile_enable(1) resets and starts per-stage device timing (CUDA events between stage
  * boundaries of every step) and the count of this library's kernel launches; profile_read returns

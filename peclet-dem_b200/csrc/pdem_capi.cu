@@ -453,6 +453,25 @@ long pdem_debug_hertz(pdem_handle h, unsigned long long* keys, double* xi, long 
 }
 int pdem_debug_set_max_contacts(pdem_handle h, int n) { BODY(S.setMaxContacts(n)); }
 
+// ---- batched form ----
+int pdem_set_scenes(pdem_handle h, int nscenes, const int* first_body) {
+  if (!first_body) {
+    g_err = "set_scenes: null scene table";
+    return PDEM_ERR_INVALID;
+  }
+  BODY(S.setScenes(nscenes, first_body));
+}
+int pdem_set_scene_material(pdem_handle h, int scene, double e_n, double mu) {
+  BODY(S.setSceneMaterial(scene, (R)e_n, (R)mu));
+}
+int pdem_set_wall_scene(pdem_handle h, int wall, int scene) { BODY(S.setWallScene(wall, scene)); }
+long pdem_scene_counters(pdem_handle h, double* out, long cap) {
+  long n = -1;
+  if (with(h, [&](auto& S) { n = S.sceneCounters(out, cap); }) != PDEM_OK)
+    return -1;
+  return n;
+}
+
 // ---- instrumentation ----
 int pdem_debug_sweeps(pdem_handle h, long* out4) {
   BODY(for (int i = 0; i < 4; ++i) out4[i] = S.sweeps_[i]);

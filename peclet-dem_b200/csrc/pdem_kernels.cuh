@@ -190,6 +190,43 @@ __global__ void kMaxScale(Dev<R> d, int n, R* out) {
   warpMaxAtomic(out, m);
 }
 
+// batched form: largest scale of every scene (out[s] zeroed by the host)
+template <class R>
+__global__ void kSceneMaxScale(Dev<R> d, int n, R* out) {
+  GRID_STRIDE(i, n) atomicMaxNonNeg(&out[d.sceneOf[i]], d.scale[i]);
+}
+// batched form, start of a substep: per-scene parameters (margin, restitution, friction; params =
+// 3 values per scene) and loop state reset as the single-scene Counters are; maxApproach persists
+template <class R>
+__global__ void kSceneBegin(SceneCtl<R>* scn, int S, const R* params) {
+  GRID_STRIDE(s, S) {
+    SceneCtl<R> q = scn[s];
+    const R keep = q.maxApproach;
+    q = SceneCtl<R>{};
+    q.maxApproach = keep;
+    q.margin = params[3 * s];
+    q.eN = params[3 * s + 1];
+    q.mu = params[3 * s + 2];
+    scn[s] = q;
+  }
+}
+// batched form: first entry of every scene in the body-sorted range [b, e) of an entry array whose
+// first body is ab[].x (pair / plane / wall contacts, manifolds); out[S] = e
+__global__ void kSceneBounds(const int2* ab, int b, int e, int S, const int* sceneFirst, int* out) {
+  GRID_STRIDE(s, S + 1) {
+    const int body = sceneFirst[s];
+    int lo = b, hi = e;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (ab[mid].x < body)
+        lo = mid + 1;
+      else
+        hi = mid;
+    }
+    out[s] = lo;
+  }
+}
+
 // per-detection counter reset; maxApproach persists across substeps like the reference's View
 // (a step with no velocity sweep reads the previous one's residual)
 template <class R>

@@ -124,12 +124,28 @@ void Sim<R>::ensureCapacity(int nc) {
 template <class R>
 void Sim<R>::ensureContactCapacity() {
   const int perParticle = std::max(16, shellPoints_);
-  const long want = (long)capacity_ * perParticle + (long)capacity_ * std::max(1, shellPoints_) * (long)wallsHost_.size();
+  const long want = (long)capacity_ * perParticle + (long)capacity_ * std::max(1, shellPoints_) * wallsPerBody();
   if (want > maxContacts_) {
     allocContactBuffers((int)want);
     prevPairCount_ = 0;
     refreshDev();
   }
+}
+// walls a body can touch: all of them, or (batched form) the most that any one scene meets
+template <class R>
+long Sim<R>::wallsPerBody() const {
+  if (!batch_)
+    return (long)wallsHost_.size();
+  long global = 0;
+  std::vector<long> own(numScenes_, 0);
+  for (size_t w = 0; w < wallsHost_.size(); ++w) {
+    const int sc = w < wallScene_.size() ? wallScene_[w] : -1;
+    if (sc < 0)
+      ++global;
+    else if (sc < numScenes_)
+      ++own[sc];
+  }
+  return global + (own.empty() ? 0 : *std::max_element(own.begin(), own.end()));
 }
 template <class R>
 void Sim<R>::refreshDev() {
@@ -157,6 +173,14 @@ void Sim<R>::refreshDev() {
   d.pairMat = pairMatHost_.empty() ? nullptr : pairMatD_.p;
   d.hzE = hzED_.p, d.hzNu = hzNuD_.p;
   d.ctr = ctr_.p;
+  d.numScenes = batch_ ? numScenes_ : 1;
+  d.sceneOf = batch_ ? sceneOf_.p : nullptr;
+  d.scn = batch_ ? scn_.p : nullptr;
+  d.sceneWallOff = batch_ ? sceneWallOffD_.p : nullptr;
+  d.sceneWallIdx = batch_ ? sceneWallIdxD_.p : nullptr;
+  d.sceneManFirst = batch_ ? sceneManFirstD_.p : nullptr;
+  d.sceneConFirst = batch_ ? sceneConFirstD_.p : nullptr;
+  d.sceneLeafFirst = batch_ ? sceneLeafFirstD_.p : nullptr;
 }
 template <class R>
 void Sim<R>::sync() {
@@ -477,7 +501,15 @@ int Sim<R>::addSdfWall(const std::vector<R>& grid, int nx, int ny, int nz, const
     throw std::runtime_error("addSdfWall: grid.size() must equal nx*ny*nz");
   WallDesc<R> w{};
   w.nx = nx, w.ny = ny, w.nz = nz;
-  w.gridOffset = (int)wallGridHost_.size();
+  // a grid identical to one already held (the same container in many batched scenes) is shared
+  int shared = -1;
+  for (const WallDesc<R>& o : wallsHost_)
+    if (o.nx == nx && o.ny == ny && o.nz == nz &&
+        std::equal(grid.begin(), grid.end(), wallGridHost_.begin() + o.gridOffset)) {
+      shared = o.gridOffset;
+      break;
+    }
+  w.gridOffset = shared >= 0 ? shared : (int)wallGridHost_.size();
   for (int a = 0; a < 3; ++a) {
     w.origin[a] = origin[a];
     w.invSpacing[a] = spacing[a] > 0 ? R(1) / spacing[a] : R(0);
@@ -486,10 +518,14 @@ int Sim<R>::addSdfWall(const std::vector<R>& grid, int nx, int ny, int nz, const
   w.friction = f;
   w.materialId = -1;
   wallsHost_.push_back(w);
-  wallGridHost_.insert(wallGridHost_.end(), grid.begin(), grid.end());
-  wallGridD_.ensure(wallGridHost_.size(), false, stream_);
-  cudaCheck(cudaMemcpyAsync(wallGridD_.p, wallGridHost_.data(), wallGridHost_.size() * sizeof(R),
-                            cudaMemcpyHostToDevice, stream_), "H2D wall grid");
+  if (shared < 0) {
+    wallGridHost_.insert(wallGridHost_.end(), grid.begin(), grid.end());
+    wallGridD_.ensure(wallGridHost_.size(), false, stream_);
+    cudaCheck(cudaMemcpyAsync(wallGridD_.p, wallGridHost_.data(), wallGridHost_.size() * sizeof(R),
+                              cudaMemcpyHostToDevice, stream_), "H2D wall grid");
+  }
+  wallScene_.resize(wallsHost_.size(), -1);
+  sceneWallsDirty_ = true;
   uploadWalls();
   if (f > wallFrictionMax_)
     wallFrictionMax_ = f;
@@ -522,6 +558,9 @@ void Sim<R>::setPositions(const R* xyz, int n) {
   if (n > capacity_)
     throw std::invalid_argument("set_positions: more particles than the simulation capacity");
   ensureGrounded();  // the logged support graphs index the previous particle set
+  if (batch_ && n != numReal_)
+    batch_ = false;  // the scene layout described the previous particle set
+  sceneParamsDirty_ = true;
   numReal_ = n;
   numParticles_ = n;
   hzNumPairs_ = -1;
@@ -573,6 +612,7 @@ void Sim<R>::clearExternalForces() {
 }
 template <class R>
 void Sim<R>::setScales(const R* s, int n) {  // src/sim.hpp:1340-1346
+  sceneParamsDirty_ = true;
   const int m = std::min(numReal_, n);
   if (m > 0)
     cudaCheck(cudaMemcpyAsync(target_.p, s, m * sizeof(R), cudaMemcpyHostToDevice, stream_), "H2D scales");
@@ -581,6 +621,7 @@ void Sim<R>::setScales(const R* s, int n) {  // src/sim.hpp:1340-1346
 }
 template <class R>
 void Sim<R>::setScalesUniform(R s) {  // src/sim.hpp:1331-1337
+  sceneParamsDirty_ = true;
   if (numReal_ > 0) {
     std::vector<R> h(numReal_, s);
     cudaCheck(cudaMemcpyAsync(scale_.p, h.data(), numReal_ * sizeof(R), cudaMemcpyHostToDevice, stream_), "H2D");
@@ -719,15 +760,28 @@ int Sim<R>::findCollisions(R margin, int cap) {
   bb.left = left_.p, bb.right = right_.p, bb.parent = parent_.p, bb.rope = nullptr, bb.flag = flag_.p;
   bb.bounds = bounds_.p;
   bb.err = &ctr_.p->err;
+  int codeBits = 63;
+  if (batch_) {  // scene id leads the key: every scene is one subtree, queries stay inside it
+    bvhFirst_.ensure(n, false, stream_);
+    bvhLast_.ensure(n, false, stream_);
+    bb.sceneOf = sceneOf_.p;
+    bb.leafFirst = sceneLeafFirstD_.p;
+    bb.first = bvhFirst_.p;
+    bb.last = bvhLast_.p;
+    codeBits = std::min(64, kSceneShift + bitsFor(numScenes_));
+  }
   const u64 init[6] = {~0ull, ~0ull, ~0ull, 0ull, 0ull, 0ull};
   cudaCheck(cudaMemcpyAsync(bounds_.p, init, sizeof init, cudaMemcpyHostToDevice, stream_), "H2D bounds");
   ++launches_, kBoxes<<<gridFor(n), kBlock, 0, stream_>>>(d_, n, margin, boxCap, bn, bb);
   KCHECK("boxes");
   ++launches_, kMorton<R><<<gridFor(n), kBlock, 0, stream_>>>(n, bn, bb);
   KCHECK("morton");
-  sortPairs(codes_.p, codesAlt_.p, bidx_.p, bidxAlt_.p, n, 63);
+  sortPairs(codes_.p, codesAlt_.p, bidx_.p, bidxAlt_.p, n, codeBits);
   std::swap(bb.codes, bb.codesAlt);
   std::swap(bb.idx, bb.idxAlt);
+  if (batch_)
+    ++launches_, kSceneLeafFirst<<<gridFor(numScenes_ + 1), kBlock, 0, stream_>>>(n, numScenes_, bb.codes,
+                                                                                  sceneLeafFirstD_.p);
   cudaCheck(cudaMemsetAsync(flag_.p, 0, n * sizeof(int), stream_), "memset");
   cudaCheck(cudaMemsetAsync(rowCnt_.p, 0, (numReal_ + 1) * sizeof(int), stream_), "memset");
   bflag_.ensure(1, false, stream_);
@@ -853,6 +907,9 @@ void Sim<R>::detectAll(R margin) {
     KCHECK("boundary write");
   }
   const long total = (long)tot[0] + tot[1] + tot[2];
+  lastTot_[0] = tot[0], lastTot_[1] = tot[1], lastTot_[2] = tot[2];
+  if (batch_ && total > maxContacts_)
+    throw std::runtime_error("batched scenes: the contact buffer overflowed (raise the capacity)");
   Counters<R> c = readCounters();
   c.pairCount = np;
   c.contactTotal = (int)std::min<long>(total, 0x7fffffff);
@@ -982,6 +1039,8 @@ void Sim<R>::demStep() {
   const int B = kBlock;
   cudaStream_t s = stream_;
   mark(ST_PREDICT);
+  if (batch_)
+    batchBegin();
   if (gf_ != R(-1) && gr_ != R(0)) {
     gf_ *= std::exp(gr_ * dt_);
     if (gf_ > R(1))
@@ -1010,6 +1069,8 @@ void Sim<R>::demStep() {
   const int nc = c0.contactCount;
   mark(ST_MANIFOLD);
   const int nm = reduceManifolds(nc);
+  if (batch_)
+    batchBounds(nm);
   c0.manifoldCount = nm;
   c0.velDone = c0.stabRun = c0.stabDone = c0.posDone = 0;
   cudaCheck(cudaMemcpyAsync(ctr_.p, &c0, sizeof c0, cudaMemcpyHostToDevice, s), "H2D counters");
@@ -1017,6 +1078,8 @@ void Sim<R>::demStep() {
   const bool friction = (mu_ > R(0) || wallFrictionMax_ > R(0));
   const bool gNZ = (g_[0] != R(0) || g_[1] != R(0) || g_[2] != R(0));
   const bool legacyFriction = friction && !(gNZ && useGS_);
+  if (batch_ && legacyFriction)
+    throw std::runtime_error("batched scenes: the Jacobi friction path (zero gravity) is not supported");
   if (legacyFriction) {
     planeFric_.zero(s);
     if (nc > 0)
@@ -1026,6 +1089,8 @@ void Sim<R>::demStep() {
   mark(ST_COLOR_V);
   int velLeft = 0;
   const int ncolV = useGS_ ? colorGraph(true, nm, numReal_, velLeft) : 0;
+  if (batch_ && velLeft > 0)
+    throw std::runtime_error("batched scenes: uncoloured manifolds (Jacobi fallback) are not supported");
   if (useGS_ && ncolV > 0)
     colorOrder(true, nm, ncolV);
   const bool usePGS = gNZ && useGS_;
@@ -1063,7 +1128,7 @@ void Sim<R>::demStep() {
     gbar_.ensure(2, false, s);
     const GridBar gb{gbar_.p, &ctr_.p->err};
     const R thr = usePGS ? R(0.02) * vRest : vRest;
-    ++launches_, kCtl<<<1, 1, 0, s>>>(ctr_.p, CTL_VEL_BEGIN, R(0), 0);
+    ctl(CTL_VEL_BEGIN, R(0), 0);
     if (usePGS)
       launchCoop(kSweepLoop<R, 0, 1>, d_, (const int*)mOrder_.p, (const int*)mOff_.p, ncolV, velIters_, sp, thr, gb);
     else
@@ -1074,8 +1139,8 @@ void Sim<R>::demStep() {
   // and the loop is done, so one BEGIN/END pair stands for the whole loop
   const bool velEmpty = useGS_ && !legacyFriction && velLeft == 0 && ncolV <= 0 && velIters_ > 0;
   if (velEmpty) {
-    ++launches_, kCtl<<<1, 1, 0, s>>>(ctr_.p, CTL_VEL_BEGIN, R(0), 0);
-    ++launches_, kCtl<<<1, 1, 0, s>>>(ctr_.p, CTL_VEL_END, usePGS ? R(0.02) * vRest : vRest, 0);
+    ctl(CTL_VEL_BEGIN, R(0), 0);
+    ctl(CTL_VEL_END, usePGS ? R(0.02) * vRest : vRest, 0);
   }
   for (int it = 0; it < (velPersistent || velEmpty ? 0 : velIters_); ++it) {
     if (legacyFriction && nc > 0) {
@@ -1085,7 +1150,7 @@ void Sim<R>::demStep() {
       KCHECK("accum normal");
     }
     if (useGS_) {
-      ++launches_, kCtl<<<1, 1, 0, s>>>(ctr_.p, CTL_VEL_BEGIN, R(0), 0);
+      ctl(CTL_VEL_BEGIN, R(0), 0);
       for (int col = 0; col < ncolV; ++col) {
         if (usePGS)
           ++launches_, kPGSColor<<<gridFor(nm), B, 0, s>>>(d_, mOrder_.p, mOff_.p, col, sp, 1);
@@ -1099,7 +1164,7 @@ void Sim<R>::demStep() {
         ++launches_, kApplyVelAveraged<<<gridFor(numParticles_), B, 0, s>>>(d_, numParticles_, 1);
         KCHECK("velocity jacobi fallback");
       }
-      ++launches_, kCtl<<<1, 1, 0, s>>>(ctr_.p, CTL_VEL_END, usePGS ? R(0.02) * vRest : vRest, 0);
+      ctl(CTL_VEL_END, usePGS ? R(0.02) * vRest : vRest, 0);
     } else {
       if (nm > 0) {
         ++launches_, kJacobiImpulses<<<gridFor(nm), B, 0, s>>>(d_, nm, sp, 0, rA_.p, iC_.p, 0);
@@ -1115,7 +1180,7 @@ void Sim<R>::demStep() {
     if (stabMode_ == 2 || stabMode_ == 4) {
       throw std::runtime_error("stabilization modes 'multilevel' and 'ordered' are not supported by the B200 step");
     }
-    ++launches_, kCtl<<<1, 1, 0, s>>>(ctr_.p, CTL_STAB_DECIDE, vRestS, stabMode_);
+    ctl(CTL_STAB_DECIDE, vRestS, stabMode_);
     // the pass runs only when the main sweeps left a residual (src/sim.hpp:282): read the
     // decision so an untriggered pass costs nothing
     const bool stabRun = (stabMode_ == 1 || stabMode_ == 3) && readCounters().stabRun;
@@ -1131,14 +1196,14 @@ void Sim<R>::demStep() {
       if (stabPersistent) {
         gbar_.ensure(2, false, s);
         const GridBar gb{gbar_.p, &ctr_.p->err};
-        ++launches_, kCtl<<<1, 1, 0, s>>>(ctr_.p, CTL_STAB_BEGIN, R(0), 0);
+        ctl(CTL_STAB_BEGIN, R(0), 0);
         launchCoop(kSweepLoop<R, 0, 2>, d_, (const int*)mOrder_.p, (const int*)mOff_.p, ncolV, iters, ss, vRestS, gb);
       }
       for (int it = 0; it < (stabPersistent ? 0 : iters); ++it) {
-        ++launches_, kCtl<<<1, 1, 0, s>>>(ctr_.p, CTL_STAB_BEGIN, R(0), 0);
+        ctl(CTL_STAB_BEGIN, R(0), 0);
         for (int col = 0; col < ncolV; ++col)
           ++launches_, kPGSColor<<<gridFor(nm), B, 0, s>>>(d_, mOrder_.p, mOff_.p, col, ss, 2);
-        ++launches_, kCtl<<<1, 1, 0, s>>>(ctr_.p, CTL_STAB_END, vRestS, 0);
+        ctl(CTL_STAB_END, vRestS, 0);
         if ((it & 15) == 15) {
           const Counters<R> cc = readCounters();
           if (cc.stabDone)
@@ -1190,6 +1255,8 @@ void Sim<R>::demStep() {
   mark(ST_COLOR_P);
   int posLeft = 0;
   const int ncolP = useGS_ ? colorGraph(false, nc, numParticles_, posLeft) : 0;
+  if (batch_ && posLeft > 0)
+    throw std::runtime_error("batched scenes: uncoloured contacts (Jacobi fallback) are not supported");
   if (useGS_ && ncolP > 0)
     colorOrder(false, nc, ncolP);
   mark(ST_POSITION);
@@ -1207,18 +1274,18 @@ void Sim<R>::demStep() {
   if (posPersistent) {
     gbar_.ensure(2, false, s);
     const GridBar gb{gbar_.p, &ctr_.p->err};
-    ++launches_, kCtl<<<1, 1, 0, s>>>(ctr_.p, CTL_POS_BEGIN, R(0), 0);
+    ctl(CTL_POS_BEGIN, R(0), 0);
     launchCoop(kSweepLoop<R, 2, 3>, d_, (const int*)cOrder_.p, (const int*)cOff_.p, ncolP, posIters_, sp, posTol, gb);
     KCHECK("position loop");
   }
   const bool posEmpty = useGS_ && posLeft == 0 && ncolP <= 0 && posIters_ > 0 && posTol > R(0);
   if (posEmpty) {  // as velEmpty: maxOverlap = 0 < posTol ends the loop after its first sweep
-    ++launches_, kCtl<<<1, 1, 0, s>>>(ctr_.p, CTL_POS_BEGIN, R(0), 0);
-    ++launches_, kCtl<<<1, 1, 0, s>>>(ctr_.p, CTL_POS_END, posTol, 0);
+    ctl(CTL_POS_BEGIN, R(0), 0);
+    ctl(CTL_POS_END, posTol, 0);
   }
   for (int it = 0; it < (posPersistent || posEmpty ? 0 : posIters_); ++it) {
     if (useGS_) {
-      ++launches_, kCtl<<<1, 1, 0, s>>>(ctr_.p, CTL_POS_BEGIN, R(0), 0);
+      ctl(CTL_POS_BEGIN, R(0), 0);
       for (int col = 0; col < ncolP; ++col)
         ++launches_, kPosGSColor<<<gridFor(nc), B, 0, s>>>(d_, cOrder_.p, cOff_.p, col, 3);
       if (posLeft > 0) {
@@ -1226,7 +1293,7 @@ void Sim<R>::demStep() {
         ++launches_, kPosJacobiGather<<<gridFor(numParticles_), B, 0, s>>>(d_, numParticles_, incP, qA_.p, iC_.p, 3);
         ++launches_, kApplyUpdatesGated<<<gridFor(numParticles_), B, 0, s>>>(d_, numParticles_, 3);
       }
-      ++launches_, kCtl<<<1, 1, 0, s>>>(ctr_.p, CTL_POS_END, posTol, 0);
+      ctl(CTL_POS_END, posTol, 0);
     } else {
       if (nc > 0) {
         ++launches_, kPosJacobiPre<<<gridFor(nc), B, 0, s>>>(d_, nc, 0, qA_.p, iC_.p, 0);
@@ -1286,6 +1353,8 @@ void Sim<R>::demStep() {
 // src/sim.hpp:494-541
 template <class R>
 R Sim<R>::computeOverlaps() {
+  if (batch_)
+    batchBegin();
   const R maxRad = maxOwnedRadius();
   const R margin = R(0.1) * maxRad;
   numParticles_ = numReal_;
@@ -1534,6 +1603,8 @@ int Sim<R>::hertzWallCandidates(R skin) {
 template <class R>
 void Sim<R>::stepHertz(R dt, int nsteps, R skinFrac) {
   dt_ = dt;
+  if (batch_)
+    throw std::runtime_error("step_hertz: not supported for batched scenes");
   if (per_[0] || per_[1] || per_[2])
     throw std::runtime_error("step_hertz: periodic domains not supported");
   if (!planesHost_.empty())
@@ -1732,6 +1803,151 @@ void Sim<R>::flushMarks() {
   for (auto& m : marks_)
     evFree_.push_back(m.ev);
   marks_.clear();
+}
+
+// =============================================================================================
+// batched form
+// =============================================================================================
+template <class R>
+void Sim<R>::ctl(int op, R thr, int mode) {
+  if (batch_)
+    ++launches_, kCtlScenes<<<1, 1024, 0, stream_>>>(ctr_.p, scn_.p, numScenes_, op, thr, mode);
+  else
+    ++launches_, kCtl<<<1, 1, 0, stream_>>>(ctr_.p, op, thr, mode);
+}
+template <class R>
+void Sim<R>::setScenes(int S, const int* first) {
+  if (S < 1 || S > 1023)
+    throw std::invalid_argument("set_scenes: between 1 and 1023 scenes");
+  if (first[0] != 0 || first[S] != numReal_)
+    throw std::invalid_argument("set_scenes: scene ranges must start at 0 and end at the particle count");
+  for (int s = 0; s < S; ++s)
+    if (first[s + 1] < first[s])
+      throw std::invalid_argument("set_scenes: scene ranges must be non-decreasing");
+  numScenes_ = S;
+  sceneFirstHost_.assign(first, first + S + 1);
+  std::vector<int> of(std::max(numReal_, 1), 0);
+  for (int s = 0; s < S; ++s)
+    for (int i = first[s]; i < first[s + 1]; ++i)
+      of[i] = s;
+  sceneOf_.ensure(capacity_, false, stream_);
+  cudaCheck(cudaMemcpyAsync(sceneOf_.p, of.data(), numReal_ * sizeof(int), cudaMemcpyHostToDevice, stream_), "H2D");
+  sceneFirstD_.ensure(S + 1, false, stream_);
+  cudaCheck(cudaMemcpyAsync(sceneFirstD_.p, first, (S + 1) * sizeof(int), cudaMemcpyHostToDevice, stream_), "H2D");
+  scn_.ensure(S, false, stream_);
+  scn_.zero(stream_, S);
+  sceneParams_.ensure(3 * (size_t)S, false, stream_);
+  sceneMaxScale_.ensure(S, false, stream_);
+  sceneManFirstD_.ensure(S + 1, false, stream_);
+  sceneConFirstD_.ensure(3 * ((size_t)S + 1), false, stream_);
+  sceneLeafFirstD_.ensure(S + 1, false, stream_);
+  sceneWallOffD_.ensure(S + 1, false, stream_);
+  sceneE_.assign(S, eN_);
+  sceneMu_.assign(S, mu_);
+  batch_ = true;
+  sceneParamsDirty_ = sceneWallsDirty_ = true;
+  refreshDev();
+  sync();
+}
+template <class R>
+void Sim<R>::setSceneMaterial(int scene, R e, R mu) {
+  if (!batch_ || scene < 0 || scene >= numScenes_)
+    throw std::invalid_argument("set_scene_material: scene index out of range");
+  sceneE_[scene] = e;
+  sceneMu_[scene] = mu;
+  sceneParamsDirty_ = true;
+}
+template <class R>
+void Sim<R>::setWallScene(int wall, int scene) {
+  if (wall < 0 || wall >= (int)wallsHost_.size())
+    throw std::invalid_argument("set_wall_scene: wall index out of range");
+  if (scene < -1)
+    throw std::invalid_argument("set_wall_scene: scene index out of range");
+  wallScene_.resize(wallsHost_.size(), -1);
+  wallScene_[wall] = scene;
+  sceneWallsDirty_ = true;
+}
+// per scene: max overlap, max approach, velocity / stabilization / position sweeps of the last substep
+template <class R>
+long Sim<R>::sceneCounters(double* out, long cap) {
+  if (!batch_)
+    return 0;
+  std::vector<SceneCtl<R>> h(numScenes_);
+  cudaCheck(cudaMemcpyAsync(h.data(), scn_.p, numScenes_ * sizeof(SceneCtl<R>), cudaMemcpyDeviceToHost, stream_), "D2H");
+  sync();
+  long k = 0;
+  for (int s = 0; s < numScenes_ && k + 5 <= cap; ++s) {
+    out[k++] = h[s].maxOverlap;
+    out[k++] = h[s].maxApproach;
+    out[k++] = h[s].velSweeps;
+    out[k++] = h[s].stabSweeps;
+    out[k++] = h[s].posSweeps;
+  }
+  return numScenes_;
+}
+// start of a batched substep: per-scene margins (0.1 x the scene's largest radius, as
+// src/sim.hpp:61-70 computes for a scene alone), materials, wall lists and loop state
+template <class R>
+void Sim<R>::batchBegin() {
+  if (per_[0] || per_[1] || per_[2])
+    throw std::runtime_error("batched scenes: periodic domains are not supported");
+  if (gf_ > R(0) || (thTau_ > R(0)))
+    throw std::runtime_error("batched scenes: growth and the thermostat are not supported");
+  if (!useGS_)
+    throw std::runtime_error("batched scenes: the Jacobi velocity solve is not supported");
+  const int S = numScenes_;
+  if (sceneWallsDirty_) {
+    wallScene_.resize(wallsHost_.size(), -1);
+    std::vector<int> off(S + 1, 0), idx;
+    for (int s = 0; s < S; ++s) {
+      off[s] = (int)idx.size();
+      for (int w = 0; w < (int)wallsHost_.size(); ++w)
+        if (wallScene_[w] < 0 || wallScene_[w] == s)
+          idx.push_back(w);
+    }
+    off[S] = (int)idx.size();
+    sceneWallIdxD_.ensure(std::max<size_t>(idx.size(), 1), false, stream_);
+    if (!idx.empty())
+      cudaCheck(cudaMemcpyAsync(sceneWallIdxD_.p, idx.data(), idx.size() * sizeof(int), cudaMemcpyHostToDevice, stream_), "H2D");
+    cudaCheck(cudaMemcpyAsync(sceneWallOffD_.p, off.data(), off.size() * sizeof(int), cudaMemcpyHostToDevice, stream_), "H2D");
+    ensureContactCapacity();
+    refreshDev();
+    sync();
+    sceneWallsDirty_ = false;
+  }
+  if (sceneParamsDirty_) {
+    sceneMaxScale_.zero(stream_, S);
+    if (numReal_ > 0)
+      ++launches_, kSceneMaxScale<<<gridFor(numReal_), kBlock, 0, stream_>>>(d_, numReal_, sceneMaxScale_.p);
+    KCHECK("scene max scale");
+    std::vector<R> mx(S), par(3 * (size_t)S);
+    cudaCheck(cudaMemcpyAsync(mx.data(), sceneMaxScale_.p, S * sizeof(R), cudaMemcpyDeviceToHost, stream_), "D2H");
+    sync();
+    for (int s = 0; s < S; ++s) {
+      const bool empty = sceneFirstHost_[s + 1] == sceneFirstHost_[s];
+      const R maxRad = empty ? gs_ * baseRadius_ : mx[s] * gs_ * baseRadius_;
+      par[3 * s] = R(0.1) * maxRad;
+      par[3 * s + 1] = sceneE_[s];
+      par[3 * s + 2] = sceneMu_[s];
+    }
+    cudaCheck(cudaMemcpyAsync(sceneParams_.p, par.data(), par.size() * sizeof(R), cudaMemcpyHostToDevice, stream_), "H2D");
+    sync();
+    sceneParamsDirty_ = false;
+  }
+  ++launches_, kSceneBegin<<<gridFor(S), kBlock, 0, stream_>>>(scn_.p, S, sceneParams_.p);
+  KCHECK("scene begin");
+}
+// after the manifold reduction: first pair / plane / wall contact and first manifold of every scene
+template <class R>
+void Sim<R>::batchBounds(int nm) {
+  const int S = numScenes_;
+  const int t0 = lastTot_[0], t1 = t0 + lastTot_[1], t2 = t1 + lastTot_[2];
+  int* cf = sceneConFirstD_.p;
+  ++launches_, kSceneBounds<<<gridFor(S + 1), kBlock, 0, stream_>>>(cab_.p, 0, t0, S, sceneFirstD_.p, cf);
+  ++launches_, kSceneBounds<<<gridFor(S + 1), kBlock, 0, stream_>>>(cab_.p, t0, t1, S, sceneFirstD_.p, cf + (S + 1));
+  ++launches_, kSceneBounds<<<gridFor(S + 1), kBlock, 0, stream_>>>(cab_.p, t1, t2, S, sceneFirstD_.p, cf + 2 * (S + 1));
+  ++launches_, kSceneBounds<<<gridFor(S + 1), kBlock, 0, stream_>>>(mab_.p, 0, nm, S, sceneFirstD_.p, sceneManFirstD_.p);
+  KCHECK("scene bounds");
 }
 
 template class Sim<float>;

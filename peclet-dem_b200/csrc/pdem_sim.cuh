@@ -138,6 +138,13 @@ class Sim {
   int hzNumPairs_ = -1, hzPrevCount_ = 0, hzNumWallCand_ = 0;
   R hzContactFrac_ = R(0.5);
 
+  // ---- batched form: independent scenes in one body array, each stepped as it would be alone ----
+  void setScenes(int S, const int* firstBody);
+  void setSceneMaterial(int scene, R e, R mu);
+  void setWallScene(int wall, int scene);
+  long sceneCounters(double* out, long cap);
+  int numScenes() const { return batch_ ? numScenes_ : 1; }
+
   cudaStream_t stream_ = nullptr;
   Dev<R> d_{};
 
@@ -185,6 +192,21 @@ class Sim {
   DBuf<R> wallGridD_, pairMatD_, hzED_, hzNuD_;
   DBuf<Counters<R>> ctr_;
   int numSMs_ = 148;
+  // batched form
+  bool batch_ = false, sceneParamsDirty_ = true, sceneWallsDirty_ = true;
+  int numScenes_ = 1;
+  std::vector<int> sceneFirstHost_;   // [S + 1] first body of each scene
+  std::vector<R> sceneE_, sceneMu_;   // per-scene restitution and friction
+  std::vector<int> wallScene_;        // per wall: its scene, or -1 for every scene
+  DBuf<int> sceneOf_, sceneFirstD_, sceneWallOffD_, sceneWallIdxD_, sceneManFirstD_, sceneConFirstD_,
+      sceneLeafFirstD_, bvhFirst_, bvhLast_;
+  DBuf<SceneCtl<R>> scn_;
+  DBuf<R> sceneParams_, sceneMaxScale_;
+  int lastTot_[3] = {0, 0, 0};
+  void batchBegin();
+  long wallsPerBody() const;
+  void batchBounds(int nm);
+  void ctl(int op, R thr, int mode);
   DBuf<unsigned> gbar_;        // grid barrier of the persistent loops
   DBuf<long long> winner2_;    // second winner array of the colouring rounds
   DBuf<int> colorAux_;         // colouring: per-round remaining counts [3], statistics [2]

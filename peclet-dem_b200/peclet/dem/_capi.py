@@ -102,6 +102,11 @@ _SIGS = {
     "profile_enable": (C.c_int, [_vp, C.c_int]),
     "profile_read": (C.c_int, [_vp, _dbl_p, _long_p, C.c_int, _long_p]),
     "debug_sweeps": (C.c_int, [_vp, _long_p]),
+    # batched form
+    "set_scenes": (C.c_int, [_vp, C.c_int, _int_p]),
+    "set_scene_material": (C.c_int, [_vp, C.c_int, C.c_double, C.c_double]),
+    "set_wall_scene": (C.c_int, [_vp, C.c_int, C.c_int]),
+    "scene_counters": (C.c_long, [_vp, _dbl_p, C.c_long]),
     # candidate pairs over caller-owned device arrays, with no allocation (pdem_static.cu)
     "find_pairs_static": (C.c_int, [_vp, _vp, C.c_int, C.c_double, C.c_double, _vp, C.c_long, _long_p, _vp]),
 }
@@ -302,6 +307,27 @@ class CApiSimulation:
                           center=(0.0, 0.0, 0.0)):
         a, b, c = _vec3(lin_vel), _vec3(ang_vel), _vec3(center)
         self._call("set_wall_velocity", int(wall_index), _ptr(a), _ptr(b), _ptr(c))
+
+    # ---- batched form (no reference counterpart) -------------------------------------------------
+    def set_scenes(self, first_body):
+        """Declare scene s = bodies [first_body[s], first_body[s+1]) (call after set_positions)."""
+        f = np.ascontiguousarray(first_body, dtype=np.int32)
+        self._call("set_scenes", int(f.size - 1), f.ctypes.data_as(_int_p))
+
+    def set_scene_material(self, scene, restitution, friction):
+        self._call("set_scene_material", int(scene), float(restitution), float(friction))
+
+    def set_wall_scene(self, wall, scene):
+        self._call("set_wall_scene", int(wall), int(scene))
+
+    def scene_counters(self):
+        """(S, 5): max overlap, max approach, velocity / stabilization / position sweeps."""
+        cap = 5 * 4096
+        out = np.zeros(cap)
+        n = int(self._f["scene_counters"](self._h, out.ctypes.data_as(_dbl_p), cap))
+        if n < 0:
+            raise RuntimeError(f"scene_counters: {self._api.error()}")
+        return out[: 5 * n].reshape(n, 5)
 
     # ---- particle state ------------------------------------------------------------------------
     def set_positions(self, a):

@@ -19,8 +19,32 @@ static uint64_t sm64(uint64_t* s) {
 }
 static double unit(uint64_t* s) { return (double)(sm64(s) >> 11) * (1.0 / 9007199254740992.0); }
 
+/* region 0: the whole box; region 1: the part of a cylinder (axis z, radius rg[0], centre x = rg[1],
+ * y = rg[2]) with y <= rg[3], each sphere lying entirely inside it */
+static int inRegion(int region, const double* rg, const double* p, double r) {
+  if (region == 0)
+    return 1;
+  const double dx = p[0] - rg[1], dy = p[1] - rg[2];
+  return sqrt(dx * dx + dy * dy) + r <= rg[0] && p[1] + r <= rg[3];
+}
+
+static long rsa(long n, const double* r, const double* lo, const double* hi, const int* periodic,
+                unsigned long long seed, int tries, int region, const double* rg, double* pos,
+                unsigned char* placed);
+
 long pdem_rsa_spheres(long n, const double* r, const double* lo, const double* hi, const int* periodic,
                       unsigned long long seed, int tries, double* pos, unsigned char* placed) {
+  return rsa(n, r, lo, hi, periodic, seed, tries, 0, NULL, pos, placed);
+}
+long pdem_rsa_spheres_region(long n, const double* r, const double* lo, const double* hi, unsigned long long seed,
+                             int tries, int region, const double* rg, double* pos, unsigned char* placed) {
+  const int closed[3] = {0, 0, 0};
+  return rsa(n, r, lo, hi, closed, seed, tries, region, rg, pos, placed);
+}
+
+static long rsa(long n, const double* r, const double* lo, const double* hi, const int* periodic,
+                unsigned long long seed, int tries, int region, const double* rg, double* pos,
+                unsigned char* placed) {
   double rmax = 0.0, ext[3];
   for (long i = 0; i < n; ++i)
     if (r[i] > rmax)
@@ -56,7 +80,7 @@ long pdem_rsa_spheres(long n, const double* r, const double* lo, const double* h
         if (c[a] < 0)
           c[a] = 0;
       }
-      int ok = 1;
+      int ok = inRegion(region, rg, p, r[i]);
       for (int dz = -1; dz <= 1 && ok; ++dz)
         for (int dy = -1; dy <= 1 && ok; ++dy)
           for (int dx = -1; dx <= 1 && ok; ++dx) {

@@ -183,6 +183,9 @@ def _rsa_lib():
     lib.pdem_rsa_spheres.argtypes = [ctypes.c_long, dp, dp, dp, ctypes.POINTER(ctypes.c_int),
                                      ctypes.c_ulonglong, ctypes.c_int, dp,
                                      ctypes.POINTER(ctypes.c_ubyte)]
+    lib.pdem_rsa_spheres_region.restype = ctypes.c_long
+    lib.pdem_rsa_spheres_region.argtypes = [ctypes.c_long, dp, dp, dp, ctypes.c_ulonglong, ctypes.c_int,
+                                            ctypes.c_int, dp, dp, ctypes.POINTER(ctypes.c_ubyte)]
     return lib
 
 
@@ -233,3 +236,79 @@ def polydisperse(seed=2, n=262144, median=1e-3, sigma=0.25, rmin=0.5e-3, rmax=2e
                  domain=(mn, mx, (periodic, periodic, False)),
                  planes=[(0.0, 0.0, 0.0, 0.0, 0.0, 1.0)], material=(e, 0.0, mu),
                  dt=dt_outer / substeps, substeps=substeps, hertz=(E, nu))
+
+
+# ---------------------------------------------------------------------------------------------
+# batched rotating drums
+def drum_wall_grid(R=6e-3, length=4e-3, h=0.5e-3):
+    """Hollow-cylinder container (axis z) as a world-space SDF grid, positive in the void."""
+    nx = ny = int(np.ceil(2.4 * R / h)) + 1
+    nz = int(np.ceil((length + 4 * h) / h)) + 1
+    origin = np.array([-1.2 * R, -1.2 * R, -2 * h])
+    x = origin[0] + h * np.arange(nx)
+    y = origin[1] + h * np.arange(ny)
+    z = origin[2] + h * np.arange(nz)
+    Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
+    radial = R - np.sqrt(X ** 2 + Y ** 2)
+    axial = np.minimum(Z, length - Z)
+    grid = np.minimum(radial, axial)  # x-fastest after ravel of (z, y, x)
+    return grid.ravel(), nx, ny, nz, origin, (h, h, h)
+
+
+def drum_deposit(seed, radii, R, length, tries=200):
+    """Random sequential addition of the spheres into the lower half (y <= 0) of a drum of radius R
+    and length `length` (axis z); returns (positions, placed mask)."""
+    lib = _rsa_lib()
+    r = np.ascontiguousarray(radii, dtype=np.float64)
+    order = np.argsort(-r, kind="stable")
+    rs = np.ascontiguousarray(r[order])
+    pos = np.zeros((r.size, 3))
+    placed = np.zeros(r.size, dtype=np.uint8)
+    lo = np.array([-R, -R, 0.0])
+    hi = np.array([R, 0.0, length])
+    rg = np.array([R, 0.0, 0.0, 0.0])
+    dp = ctypes.POINTER(ctypes.c_double)
+    lib.pdem_rsa_spheres_region(r.size, rs.ctypes.data_as(dp), lo.ctypes.data_as(dp), hi.ctypes.data_as(dp),
+                                int(seed), int(tries), 1, rg.ctypes.data_as(dp), pos.ctypes.data_as(dp),
+                                placed.ctypes.data_as(ctypes.POINTER(ctypes.c_ubyte)))
+    out = np.zeros_like(pos)
+    ok = np.zeros(r.size, dtype=bool)
+    out[order] = pos
+    ok[order] = placed.astype(bool)
+    return out, ok
+
+
+def rotating_drums(seed=4, scenes=512, R=50e-3, length=20e-3, nmin=256, nmax=8192, rlo=0.8e-3, rhi=1.2e-3,
+                   fill=0.30, density=2500.0, dt_outer=5e-5, substeps=10, grid_h=1e-3):
+    """Batched rotating drums (one scene per drum): omega ~ U[0.5, 3] rad/s about the drum axis (z),
+    N_s ~ U{nmin..nmax} spheres with radii ~ U[rlo, rhi], mu ~ U[0.2, 0.8], e ~ U[0.3, 0.9], placed by
+    seeded random deposition in the lower half of the drum up to `fill` of the half volume (capped
+    at N_s). Gravity -9.81 m/s^2 along y. Returns (scenes, extras) for batch.apply_batch; every
+    drum is the same container grid (shared on the device), turning at its own rate."""
+    rng = np.random.default_rng(seed)
+    grid = drum_wall_grid(R, length, grid_h)
+    half_volume = 0.5 * np.pi * R * R * length
+    out, extras = [], []
+    for s in range(scenes):
+        omega = rng.uniform(0.5, 3.0)
+        ns = int(rng.integers(nmin, nmax + 1))
+        mu = rng.uniform(0.2, 0.8)
+        e = rng.uniform(0.3, 0.9)
+        r = rng.uniform(rlo, rhi, ns)
+        vol = np.cumsum(4.0 / 3.0 * np.pi * r ** 3)
+        r = r[: max(1, int(np.searchsorted(vol, fill * half_volume)))]
+        pos, ok = drum_deposit(int(rng.integers(1 << 62)), r, R, length)
+        r, pos = r[ok], pos[ok]
+        m = density * 4.0 / 3.0 * np.pi * r ** 3
+        iI = 1.0 / (0.4 * m * r ** 2)
+        out.append(Scene(name=f"drum{s}", pos=pos, vel=np.zeros_like(pos), inv_mass=1.0 / m,
+                         inv_inertia=np.repeat(iI[:, None], 3, 1), scales=r / 1e-3, global_scale=1e-3,
+                         domain=((-R, -R, 0.0), (R, R, length), (False, False, False)),
+                         gravity=(0.0, -9.81, 0.0), material=(e, 0.0, mu), iterations=(10, 10),
+                         dt=dt_outer / substeps, substeps=substeps))
+
+        def extra(sim, w=omega):
+            wid = sim.add_sdf_wall(*grid, 0.5, 0.5)
+            sim.set_wall_velocity(wid, (0.0, 0.0, 0.0), (0.0, 0.0, w), (0.0, 0.0, 0.0))
+        extras.append(extra)
+    return out, extras

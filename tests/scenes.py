@@ -72,19 +72,7 @@ def cylinders(seed=14, n=24, L=8e-3, shape_type=W.HOLLOW_CYLINDER, shell=None):
                    iterations=(20, 10), dt=6.25e-6, shell=shell)
 
 
-def drum_wall_grid(R=6e-3, length=4e-3, h=0.5e-3):
-    """Hollow-cylinder container (axis z) as a world-space SDF grid, positive in the void."""
-    nx = ny = int(np.ceil(2.4 * R / h)) + 1
-    nz = int(np.ceil((length + 4 * h) / h)) + 1
-    origin = np.array([-1.2 * R, -1.2 * R, -2 * h])
-    x = origin[0] + h * np.arange(nx)
-    y = origin[1] + h * np.arange(ny)
-    z = origin[2] + h * np.arange(nz)
-    Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
-    radial = R - np.sqrt(X ** 2 + Y ** 2)
-    axial = np.minimum(Z, length - Z)
-    grid = np.minimum(radial, axial)  # x-fastest after ravel of (z, y, x)
-    return grid.ravel(), nx, ny, nz, origin, (h, h, h)
+drum_wall_grid = W.drum_wall_grid
 
 
 def spheres_in_drum(seed=15, n=120, R=6e-3, length=4e-3, omega=2.0, e=0.5, mu=0.4):
