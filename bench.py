@@ -143,8 +143,10 @@ def split_scenes(sizes, world):
 
 
 def run_batched(args, rank, world, dist, dem):
-    """Batched rotating drums (512 scenes) in one simulation per GPU, FP64; scenes are split over
-    the ranks with no exchange while stepping. Returns the sub-object of the JSON line."""
+    """Batched rotating drums (512 scenes) in one simulation per GPU, in FP64 and in the FP32-mixed
+    form; scenes are split over the ranks with no exchange while stepping. The mixed form's error
+    is its largest position difference from the FP64 run after the same substeps, in radii.
+    Returns the sub-object of the JSON line."""
     from peclet.dem import workloads as W
     from peclet.dem.batch import apply_batch
     scenes, extras = W.rotating_drums(scenes=args.drums)
@@ -152,27 +154,43 @@ def run_batched(args, rank, world, dist, dem):
     sc_m = [scenes[s] for s in mine]
     n_all = sum(sc.n for sc in scenes)
     n_mine = sum(sc.n for sc in sc_m)
-    sim = dem.Simulation(n_mine + 8, "fp64")
-    apply_batch(sim, sc_m, [extras[s] for s in mine])
+    radius = np.concatenate([sc.scales * sc.global_scale for sc in sc_m])
     dt = sc_m[0].dt
-    for _ in range(args.warmup * SUBSTEPS):
-        sim.step(dt)
-    if dist is not None:
-        dist.barrier()
-    sim.profile_enable(True)
-    for _ in range(args.steps * SUBSTEPS):
-        sim.step(dt)
-    stages, launches = sim.profile_read()
-    sim.profile_enable(False)
-    t_max = max_over_ranks(sum(ms for ms, _ in stages.values()) / 1e3, dist, "cuda")
-    per_step = {k: round(ms / args.steps, 3) for k, (ms, c) in stages.items() if c}
-    sweeps = sim.scene_counters()
-    sim.close()
+
+    def one(precision):
+        sim = dem.Simulation(n_mine + 8, precision)
+        apply_batch(sim, sc_m, [extras[s] for s in mine])
+        for _ in range(args.warmup * SUBSTEPS):
+            sim.step(dt)
+        if dist is not None:
+            dist.barrier()
+        sim.profile_enable(True)
+        for _ in range(args.steps * SUBSTEPS):
+            sim.step(dt)
+        stages, launches = sim.profile_read()
+        sim.profile_enable(False)
+        t = max_over_ranks(sum(ms for ms, _ in stages.values()) / 1e3, dist, "cuda")
+        sweeps = sim.scene_counters()
+        x = sim.get_positions()
+        sim.close()
+        per_step = {k: round(ms / args.steps, 3) for k, (ms, c) in stages.items() if c}
+        return t, per_step, launches, sweeps, x
+
+    t64, st64, l64, sw64, x64 = one("fp64")
+    tmx, stmx, lmx, _, xmx = one("mixed")
+    err = np.linalg.norm(xmx - x64, axis=1) / radius
+    err_max = max_over_ranks(float(err.max()) if err.size else 0.0, dist, "cuda")
+    rate = lambda t: n_all * SUBSTEPS * args.steps / t
     return {"workload": f"rotating_drums_{len(scenes)}_scenes", "scenes": len(scenes), "particles": n_all,
-            "value": n_all * SUBSTEPS * args.steps / t_max, "unit": METRIC, "precision": "fp64",
-            "ms_per_step": 1e3 * t_max / args.steps, "gpu_launches": launches, "stages_ms_per_step": per_step,
-            "err_vs_fp64": 0.0, "scaling": "weak (scenes split over ranks)",
-            "mean_sweeps_last_substep": {"velocity": float(sweeps[:, 2].mean()), "position": float(sweeps[:, 4].mean())},
+            "unit": METRIC, "scaling": "weak (scenes split over ranks)",
+            "fp64": {"value": rate(t64), "ms_per_step": 1e3 * t64 / args.steps, "gpu_launches": l64,
+                     "stages_ms_per_step": st64, "err_vs_fp64": 0.0},
+            "mixed": {"value": rate(tmx), "ms_per_step": 1e3 * tmx / args.steps, "gpu_launches": lmx,
+                      "stages_ms_per_step": stmx,
+                      "err_vs_fp64": {"max_position_error_radii": err_max,
+                                      "median_position_error_radii": float(np.median(err)) if err.size else 0.0,
+                                      "after_substeps": (args.warmup + args.steps) * SUBSTEPS}},
+            "mean_sweeps_last_substep": {"velocity": float(sw64[:, 2].mean()), "position": float(sw64[:, 4].mean())},
             "config": "R 50 mm, L 20 mm drums, omega U[0.5,3] rad/s, N_s U{256..8192} capped at 30% fill of the "
                       "lower half, radii U[0.8,1.2] mm, mu U[0.2,0.8], e U[0.3,0.9], dt 5e-5 s / 10 substeps"}
 
@@ -262,11 +280,13 @@ def run_ours(args):
         time.sleep(0.5)  # sampler running before the timed region starts
         barrier()
         sim.profile_enable(True)
+        timed_allocs = dem._API.fn["debug_allocs"]()
         t0 = time.perf_counter()
         for _ in range(args.steps):
             for _ in range(SUBSTEPS):
                 sim.step(scene.dt)
         wall = time.perf_counter() - t0
+        timed_allocs = dem._API.fn["debug_allocs"]() - timed_allocs
     stages, launches = sim.profile_read()
     barrier()
     dev_ms = sum(ms for ms, _ in stages.values())
@@ -281,6 +301,8 @@ def run_ours(args):
     force = np.zeros((n, 3))
     barrier()
     te = time.perf_counter()
+    allocs = dem._API.fn["debug_allocs"]
+    a0 = allocs()
     laps = []
     for _ in range(args.steps):
         tl = time.perf_counter()
@@ -294,7 +316,7 @@ def run_ours(args):
     assert np.all(np.isfinite(pos)) and np.all(np.isfinite(vel))
     e2e = {"value": world * n * SUBSTEPS * args.steps / e2e_s, "unit": METRIC,
            "h2d_bytes_per_step": int(force.nbytes), "d2h_bytes_per_step": int(pos.nbytes + vel.nbytes),
-           "ms_per_step_each": laps}
+           "ms_per_step_each": laps, "device_allocations": int(allocs() - a0)}
 
     # ---- roofline of the dominant stage ----
     per_step = {k: (ms / args.steps, c / args.steps) for k, (ms, c) in stages.items() if c}
@@ -339,6 +361,7 @@ def run_ours(args):
             "clocks": clocks.summary(), "wall_ms_per_step": 1e3 * wall / args.steps,
             "stages_ms_per_step": {k: round(v[0], 4) for k, v in per_step.items()},
             "counts_last_substep": counts, "sweeps": sweeps, "batched": batched,
+            "device_allocations_timed": int(timed_allocs),
         }
         print(json.dumps(line))
     if dist is not None:

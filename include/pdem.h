@@ -16,6 +16,7 @@
 extern "C" {
 #endif
 
+#define PDEM_MIXED 3264 /* pdem_create precision: FP32 step with FP64 master positions/orientations */
 #define PDEM_OK 0
 #define PDEM_ERR_RUNTIME 1     /* std::runtime_error in the reference  -> RuntimeError */
 #define PDEM_ERR_INVALID 2     /* std::invalid_argument in the reference -> ValueError  */
@@ -33,7 +34,9 @@ const char* pdem_execution_space(void);
  * reference runs on Kokkos' default device, src/dem_bindings.cpp:54-55 */
 int pdem_set_device(int device);
 
-/* Simulation(capacity)                         src/dem_bindings.cpp:72, src/sim.hpp:911-916 */
+/* Simulation(capacity)                         src/dem_bindings.cpp:72, src/sim.hpp:911-916
+ * precision: 64 = FP64 step (the drop-in), 32 = the reference's float arithmetic,
+ * PDEM_MIXED = float step whose positions and orientations are kept and returned in FP64 */
 int pdem_create(int capacity, int precision, pdem_handle* out);
 void pdem_destroy(pdem_handle h);
 
@@ -180,6 +183,8 @@ long pdem_scene_counters(pdem_handle h, double* out, long cap);
  * hertz_rebuild, hertz_integrate */
 int pdem_profile_enable(pdem_handle h, int on);
 int pdem_profile_read(pdem_handle h, double* ms, long* calls, int cap, long* launches);
+/* device allocations made by this library's growable buffers since it was loaded */
+long pdem_debug_allocs(void);
 /* sweeps executed since profile_enable: velocity, stabilization, position; and substeps */
 int pdem_debug_sweeps(pdem_handle h, long* out4);
 

@@ -167,8 +167,8 @@ int pdem_create(int capacity, int precision, pdem_handle* out) {
     g_err = "capacity must be >= 0";
     return PDEM_ERR_INVALID;
   }
-  if (precision != 32 && precision != 64) {
-    g_err = "precision must be 32 or 64";
+  if (precision != 32 && precision != 64 && precision != PDEM_MIXED) {
+    g_err = "precision must be 32, 64 or PDEM_MIXED";
     return PDEM_ERR_INVALID;
   }
   int ndev = 0;
@@ -179,9 +179,10 @@ int pdem_create(int capacity, int precision, pdem_handle* out) {
   }
   Handle* H = new Handle;
   try {
-    if (precision == 32)
+    if (precision == 32 || precision == PDEM_MIXED) {
       H->f = new Sim<float>(capacity);
-    else
+      H->f->setMixed(precision == PDEM_MIXED);
+    } else
       H->d = new Sim<double>(capacity);
   } catch (const std::exception& ex) {
     g_err = ex.what();
@@ -276,6 +277,7 @@ int pdem_set_positions(pdem_handle h, const double* xyz, int n) {
   BODY({
     const auto v = conv<R>(xyz, (long)n * 3);
     S.setPositions(v.data(), n);
+    S.setMaster(0, xyz, n);
   });
 }
 #define SETROWS(NAME, FIELD, COLS)                                  \
@@ -287,7 +289,13 @@ int pdem_set_positions(pdem_handle h, const double* xyz, int n) {
   }
 SETROWS(pdem_set_velocities, 0, 3)
 SETROWS(pdem_set_external_forces, 1, 3)
-SETROWS(pdem_set_quaternions, 2, 4)
+int pdem_set_quaternions(pdem_handle h, const double* a, int n) {
+  BODY({
+    const auto v = conv<R>(a, (long)n * 4);
+    S.setRows(2, v.data(), n);
+    S.setMaster(2, a, n);
+  });
+}
 SETROWS(pdem_set_angular_velocities, 3, 3)
 SETROWS(pdem_set_inv_inertia, 4, 3)
 SETROWS(pdem_set_inv_mass, 5, 1)
@@ -316,6 +324,8 @@ double pdem_get_growth_rate(pdem_handle h) {
     with(h, [&](auto& S) {                                                \
       using R = RealOf<decltype(S)>;                                      \
       n = (long)S.numReal_ * COLS;                                        \
+      if (S.getMaster(FIELD, out, cap))                                   \
+        return;                                                           \
       std::vector<R> tmp((size_t)std::max(n, 0L));                        \
       S.getRows(FIELD, tmp.data(), (long)tmp.size());                     \
       for (long i = 0; i < n && i < cap; ++i)                             \
@@ -473,6 +483,7 @@ long pdem_scene_counters(pdem_handle h, double* out, long cap) {
 }
 
 // ---- instrumentation ----
+long pdem_debug_allocs(void) { return pdem::gDeviceAllocs; }
 int pdem_debug_sweeps(pdem_handle h, long* out4) {
   BODY(for (int i = 0; i < 4; ++i) out4[i] = S.sweeps_[i]);
 }

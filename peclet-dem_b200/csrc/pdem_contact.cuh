@@ -608,13 +608,12 @@ __global__ void kGroundEdges(Dev<R> d, int nm, V3<R> gHat, int4* edges) {
 // A sweep that changes nothing ends the loop (later sweeps would repeat it unchanged).
 // Levels live in shared memory when they fit, else in a global scratch array.
 constexpr int kGroundPF = 8;
-__global__ void kGroundSweeps(int nm, int numReal, int sweeps, const int4* edges, uint8_t* grounded,
-                              int* gscratch, int useShared) {
-  extern __shared__ int slvl[];
-  int* L = useShared ? slvl : gscratch;
-  const int lane = threadIdx.x;
-  for (int i = lane; i < numReal; i += 32)
-    L[i] = grounded[i];
+// one warp: the sweeps over edges[0, nm) whose bodies are [b0, b0 + nb) with levels in L[i - b0]
+__device__ __forceinline__ void groundSweepsWarp(int nm, int b0, int nb, int sweeps, const int4* edges,
+                                                 uint8_t* grounded, int* L) {
+  const int lane = threadIdx.x & 31;
+  for (int i = lane; i < nb; i += 32)
+    L[i] = grounded[b0 + i];
   __threadfence_block();
   __syncwarp();
   const int nwin = (nm + 31) / 32;
@@ -631,7 +630,7 @@ __global__ void kGroundSweeps(int nm, int numReal, int sweeps, const int4* edges
       for (int q = 0; q < kGroundPF; ++q) {
         if (w0 + q >= nwin)
           break;
-        const int kind = buf[q].x, src = buf[q].y, dst = buf[q].z;
+        const int kind = buf[q].x, src = buf[q].y - b0, dst = buf[q].z - b0;
         const int L0s = (kind == 2) ? L[src] : 0;
         const int L0d = (kind != 0) ? L[dst] : 0;
         int c = (kind == 1) ? 255 : (kind == 2 ? L0s - 1 : 0);
@@ -673,8 +672,23 @@ __global__ void kGroundSweeps(int nm, int numReal, int sweeps, const int4* edges
       break;
   }
   __syncwarp();
-  for (int i = lane; i < numReal; i += 32)
-    grounded[i] = (uint8_t)L[i];
+  for (int i = lane; i < nb; i += 32)
+    grounded[b0 + i] = (uint8_t)L[i];
+}
+__global__ void kGroundSweeps(int nm, int numReal, int sweeps, const int4* edges, uint8_t* grounded,
+                              int* gscratch, int useShared) {
+  extern __shared__ int slvl[];
+  groundSweepsWarp(nm, 0, numReal, sweeps, edges, grounded, useShared ? slvl : gscratch);
+}
+// batched form: one warp (block) per scene over its own edge range manFirst[s..s+1) and bodies
+// bodyFirst[s..s+1): the sweeps of independent scenes are independent, and each stops on its own
+__global__ void kGroundSweepsScenes(const int* manFirst, const int* bodyFirst, int sweeps, const int4* edges,
+                                    uint8_t* grounded, int* gscratch, int useShared) {
+  extern __shared__ int slvl[];
+  const int s = blockIdx.x;
+  const int b0 = bodyFirst[s], nb = bodyFirst[s + 1] - b0;
+  const int e0 = manFirst[s], ne = manFirst[s + 1] - e0;
+  groundSweepsWarp(ne, b0, nb, sweeps, edges + e0, grounded, useShared ? slvl : gscratch + b0);
 }
 
 // =============================================================================================
@@ -700,69 +714,6 @@ __device__ __forceinline__ long long entryKey(const Dev<R>& d, int i, int ea) {
     return colorKey(i);
   const int s = d.sceneOf[ea];
   return colorKey(MANIFOLD ? localManifold(d, i, s) : localContact(d, i, s));
-}
-template <class R>
-__global__ void kColorInitManifolds(Dev<R> d, int nm) {
-  GRID_STRIDE(i, nm) {
-    const int2 ab = d.mab[i];
-    if (d.mnp[i] <= 0 || (ab.y >= 0 && d.realIdx[ab.x] > d.realIdx[ab.y]))
-      d.mColor[i] = -2;
-    else
-      d.mColor[i] = -1;
-  }
-}
-__global__ void kFillInt(int* a, int n, int v) {
-  GRID_STRIDE(i, n) a[i] = v;
-}
-__global__ void kFillLL(long long* a, int n, long long v) {
-  GRID_STRIDE(i, n) a[i] = v;
-}
-__global__ void kFillU64(u64* a, int n, u64 v) {
-  GRID_STRIDE(i, n) a[i] = v;
-}
-template <class R, bool MANIFOLD>
-__global__ void kColorContend(Dev<R> d, int ne, const int* col) {
-  GRID_STRIDE(i, ne) {
-    if (col[i] != -1)
-      continue;
-    int ea, eb;
-    colorEnds<R, MANIFOLD>(d, (int)i, ea, eb);
-    const long long k = entryKey<R, MANIFOLD>(d, (int)i, ea);
-    atomicMax(&d.winner[ea], k);
-    if (eb >= 0)
-      atomicMax(&d.winner[eb], k);
-  }
-}
-template <class R, bool MANIFOLD>
-__global__ void kColorCommit(Dev<R> d, int ne, int* col, int* remaining) {
-  GRID_STRIDE(i, ne) {
-    if (col[i] != -1)
-      continue;
-    int ea, eb;
-    colorEnds<R, MANIFOLD>(d, (int)i, ea, eb);
-    const long long k = entryKey<R, MANIFOLD>(d, (int)i, ea);
-    if (d.winner[ea] != k || (eb >= 0 && d.winner[eb] != k)) {
-      atomicAdd(remaining, 1);
-      continue;
-    }
-    u64 forb = d.mask[ea];
-    if (eb >= 0)
-      forb |= d.mask[eb];
-    int c = 0;
-    while (c < 62 && (forb & (1ull << c)))
-      ++c;
-    col[i] = c;
-    d.mask[ea] |= 1ull << c;
-    if (eb >= 0)
-      d.mask[eb] |= 1ull << c;
-  }
-}
-__global__ void kColorStats(int ne, const int* col, int* maxColor, int* leftover) {
-  GRID_STRIDE(i, ne) {
-    atomicMax(maxColor, col[i]);
-    if (col[i] == -1)
-      atomicAdd(leftover, 1);
-  }
 }
 // colour keys for the stable colour-sorted execution order
 __global__ void kColorSortKeys(int ne, const int* col, unsigned* keys, int* vals) {

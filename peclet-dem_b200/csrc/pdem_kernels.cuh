@@ -143,6 +143,43 @@ __global__ void kFinalCommit(Dev<R> d, int n, DomainP<R> dom) {
   }
 }
 
+// FP32-mixed form, end of a substep: the FP64 master positions and orientations advance by the
+// substep's single-precision increment (the difference of two nearby floats, exact), periodic
+// wrapping is applied in double, and the single-precision state is re-derived from the master,
+// so rounding does not accumulate in the stored state across substeps.
+template <class R>
+__global__ void kMixedCommit(Dev<R> d, int n, DomainP<R> dom, Q4<double>* posD, Q4<double>* quatD) {
+  GRID_STRIDE(i, n) {
+    const Q4<R> pp = d.posPred[i], p0 = d.pos[i], qp = d.quatPred[i], q0 = d.quat[i];
+    Q4<double> x = posD[i];
+    x.x += (double)(pp.x - p0.x);
+    x.y += (double)(pp.y - p0.y);
+    x.z += (double)(pp.z - p0.z);
+    double* c = &x.x;
+    for (int a = 0; a < 3; ++a)
+      if (dom.per[a]) {
+        if (c[a] < (double)dom.mn[a])
+          c[a] += (double)dom.sz[a];
+        else if (c[a] >= (double)dom.mx[a])
+          c[a] -= (double)dom.sz[a];
+      }
+    x.w = 0.0;
+    Q4<double> q = quatD[i];
+    q.x += (double)(qp.x - q0.x);
+    q.y += (double)(qp.y - q0.y);
+    q.z += (double)(qp.z - q0.z);
+    q.w += (double)(qp.w - q0.w);
+    const double qn = sqrt(q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w);
+    if (qn > 1e-12) {
+      q.x /= qn, q.y /= qn, q.z /= qn, q.w /= qn;
+    }
+    posD[i] = x;
+    quatD[i] = q;
+    d.pos[i] = Q4<R>{(R)x.x, (R)x.y, (R)x.z, R(0)};
+    d.quat[i] = Q4<R>{(R)q.x, (R)q.y, (R)q.z, (R)q.w};
+  }
+}
+
 // integration.hpp:229-249 — kinetic energies summed in double in ascending index (one thread:
 // the thermostat is an opt-in diagnostic path and must reproduce the serial sum bit for bit)
 template <class R>

@@ -132,80 +132,99 @@ __global__ void __launch_bounds__(kBlock) kSweepLoop(Dev<R> d, const int* order,
   }
 }
 
-// ---------------------------------------------------------------------------------------------
-// Jones-Plassmann colouring rounds (src/solver_velocity.hpp:277-374, src/solver_position.hpp:
-// 155-241) until no entry is left or a round colours nothing. Preconditions set by the host:
-// mask[0..nb) = 0, col initialised (-1 = to colour, -2 = skipped), winA[0..nb) = -1,
-// remCnt[0..3) = 0. Two winner arrays alternate by round: the losers of round r, the only entries
-// of round r + 1, reset their bodies in the other array during round r. The remaining-entry count
-// of round r lives in remCnt[r % 3]; the lead zeroes the slot of round r + 1 during round r.
-// At the end the colour statistics (largest colour, entries left uncoloured) are accumulated into
-// stats[0] (atomic max, preset to INT_MIN) and stats[1] (preset to 0).
 constexpr int kColorBlock = 1024;  // one large block per SM: fewer arrivals per grid barrier
 
+// ---------------------------------------------------------------------------------------------
+// Both colourings of a substep in ONE cooperative launch: the manifold graph (velocity solve) and
+// the contact graph (position solve) are independent, so their Jones-Plassmann rounds run in
+// lockstep behind the same grid barriers, each graph stopping on its own. The initialisation
+// (masks, colours, first winner array, counters) is the kernel's first phase. Per graph the
+// rounds, the winners and the statistics are exactly those of kColorLoop.
+struct ColorJob {
+  int ne, nb;          // entries, bodies
+  int* col;            // [ne] colours out
+  long long *winA, *winB;
+  u64* mask;           // [nb]
+  int* aux;            // [0..2] remaining counts by round % 3, [3] max colour, [4] left uncoloured
+};
+
 template <class R, bool MANIFOLD>
-__global__ void __launch_bounds__(kColorBlock) kColorLoop(Dev<R> d, int ne, int maxRounds, int* col, long long* winA,
-                                                     long long* winB, int* remCnt, int* stats, GridBar gb) {
-  const bool lead = (blockIdx.x | threadIdx.x) == 0;
-  const long gtid = (long)blockIdx.x * blockDim.x + threadIdx.x, gstride = (long)gridDim.x * blockDim.x;
-  int prev = -1;
-  for (int round = 0; round < maxRounds; ++round) {
-    long long* win = (round & 1) ? winB : winA;
-    long long* nxt = (round & 1) ? winA : winB;
-    if (lead)
-      remCnt[(round + 1) % 3] = 0;
-    for (long i = gtid; i < ne; i += gstride) {
-      if (col[i] != -1)
-        continue;
-      int ea, eb;
-      colorEnds<R, MANIFOLD>(d, (int)i, ea, eb);
-      const long long k = entryKey<R, MANIFOLD>(d, (int)i, ea);
-      atomicMax(&win[ea], k);
-      if (eb >= 0)
-        atomicMax(&win[eb], k);
-    }
-    if (!gridBarrier(gb))
-      return;
-    int lost = 0;
-    for (long i = gtid; i < ne; i += gstride) {
-      if (col[i] != -1)
-        continue;
-      int ea, eb;
-      colorEnds<R, MANIFOLD>(d, (int)i, ea, eb);
-      const long long k = entryKey<R, MANIFOLD>(d, (int)i, ea);
-      if (win[ea] != k || (eb >= 0 && win[eb] != k)) {
-        ++lost;
-        nxt[ea] = -1;
-        if (eb >= 0)
-          nxt[eb] = -1;
-        continue;
-      }
-      u64 forb = d.mask[ea];
-      if (eb >= 0)
-        forb |= d.mask[eb];
-      int cc = 0;
-      while (cc < 62 && (forb & (1ull << cc)))
-        ++cc;
-      col[i] = cc;
-      d.mask[ea] |= 1ull << cc;
-      if (eb >= 0)
-        d.mask[eb] |= 1ull << cc;
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1)
-      lost += __shfl_xor_sync(0xffffffffu, lost, o);
-    if ((threadIdx.x & 31) == 0 && lost)
-      atomicAdd(&remCnt[round % 3], lost);
-    if (!gridBarrier(gb))
-      return;
-    const int rem = *reinterpret_cast<volatile int*>(&remCnt[round % 3]);
-    if (rem == 0 || rem == prev)
-      break;
-    prev = rem;
+__device__ __forceinline__ void colorInit(const Dev<R>& d, const ColorJob& J, long gtid, long gstride) {
+  for (long b = gtid; b < J.nb; b += gstride) {
+    J.mask[b] = 0ull;
+    J.winA[b] = -1ll;
   }
+  for (long i = gtid; i < J.ne; i += gstride) {
+    if (MANIFOLD) {
+      const int2 ab = d.mab[i];
+      J.col[i] = (d.mnp[i] <= 0 || (ab.y >= 0 && d.realIdx[ab.x] > d.realIdx[ab.y])) ? -2 : -1;
+    } else {
+      J.col[i] = -1;
+    }
+  }
+  if (gtid == 0) {
+    J.aux[0] = J.aux[1] = J.aux[2] = 0;
+    J.aux[3] = INT_MIN;
+    J.aux[4] = 0;
+  }
+}
+template <class R, bool MANIFOLD>
+__device__ __forceinline__ void colorContend(const Dev<R>& d, const ColorJob& J, int round, long gtid,
+                                             long gstride) {
+  long long* win = (round & 1) ? J.winB : J.winA;
+  if (gtid == 0)
+    J.aux[(round + 1) % 3] = 0;
+  for (long i = gtid; i < J.ne; i += gstride) {
+    if (J.col[i] != -1)
+      continue;
+    int ea, eb;
+    colorEnds<R, MANIFOLD>(d, (int)i, ea, eb);
+    const long long k = entryKey<R, MANIFOLD>(d, (int)i, ea);
+    atomicMax(&win[ea], k);
+    if (eb >= 0)
+      atomicMax(&win[eb], k);
+  }
+}
+template <class R, bool MANIFOLD>
+__device__ __forceinline__ void colorCommit(const Dev<R>& d, const ColorJob& J, int round, long gtid,
+                                            long gstride) {
+  long long* win = (round & 1) ? J.winB : J.winA;
+  long long* nxt = (round & 1) ? J.winA : J.winB;
+  int lost = 0;
+  for (long i = gtid; i < J.ne; i += gstride) {
+    if (J.col[i] != -1)
+      continue;
+    int ea, eb;
+    colorEnds<R, MANIFOLD>(d, (int)i, ea, eb);
+    const long long k = entryKey<R, MANIFOLD>(d, (int)i, ea);
+    if (win[ea] != k || (eb >= 0 && win[eb] != k)) {
+      ++lost;
+      nxt[ea] = -1;
+      if (eb >= 0)
+        nxt[eb] = -1;
+      continue;
+    }
+    u64 forb = J.mask[ea];
+    if (eb >= 0)
+      forb |= J.mask[eb];
+    int cc = 0;
+    while (cc < 62 && (forb & (1ull << cc)))
+      ++cc;
+    J.col[i] = cc;
+    J.mask[ea] |= 1ull << cc;
+    if (eb >= 0)
+      J.mask[eb] |= 1ull << cc;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
+    lost += __shfl_xor_sync(0xffffffffu, lost, o);
+  if ((threadIdx.x & 31) == 0 && lost)
+    atomicAdd(&J.aux[round % 3], lost);
+}
+__device__ __forceinline__ void colorStats(const ColorJob& J, long gtid, long gstride) {
   int mxc = INT_MIN, left = 0;
-  for (long i = gtid; i < ne; i += gstride) {
-    const int v = col[i];
+  for (long i = gtid; i < J.ne; i += gstride) {
+    const int v = J.col[i];
     mxc = v > mxc ? v : mxc;
     left += (v == -1) ? 1 : 0;
   }
@@ -217,10 +236,49 @@ __global__ void __launch_bounds__(kColorBlock) kColorLoop(Dev<R> d, int ne, int 
   }
   if ((threadIdx.x & 31) == 0) {
     if (mxc != INT_MIN)
-      atomicMax(&stats[0], mxc);
+      atomicMax(&J.aux[3], mxc);
     if (left)
-      atomicAdd(&stats[1], left);
+      atomicAdd(&J.aux[4], left);
   }
+}
+
+// job 0: manifolds over real bodies (skipped when ne = 0), job 1: contacts over body slots
+template <class R>
+__global__ void __launch_bounds__(kColorBlock) kColorBoth(Dev<R> d, ColorJob jm, ColorJob jc, int maxRounds,
+                                                          GridBar gb) {
+  const long gtid = (long)blockIdx.x * blockDim.x + threadIdx.x, gstride = (long)gridDim.x * blockDim.x;
+  colorInit<R, true>(d, jm, gtid, gstride);
+  colorInit<R, false>(d, jc, gtid, gstride);
+  if (!gridBarrier(gb))
+    return;
+  int prevM = -1, prevC = -1;
+  bool doneM = jm.ne <= 0, doneC = jc.ne <= 0;
+  for (int round = 0; round < maxRounds && !(doneM && doneC); ++round) {
+    if (!doneM)
+      colorContend<R, true>(d, jm, round, gtid, gstride);
+    if (!doneC)
+      colorContend<R, false>(d, jc, round, gtid, gstride);
+    if (!gridBarrier(gb))
+      return;
+    if (!doneM)
+      colorCommit<R, true>(d, jm, round, gtid, gstride);
+    if (!doneC)
+      colorCommit<R, false>(d, jc, round, gtid, gstride);
+    if (!gridBarrier(gb))
+      return;
+    if (!doneM) {
+      const int rem = *reinterpret_cast<volatile int*>(&jm.aux[round % 3]);
+      doneM = rem == 0 || rem == prevM;
+      prevM = rem;
+    }
+    if (!doneC) {
+      const int rem = *reinterpret_cast<volatile int*>(&jc.aux[round % 3]);
+      doneC = rem == 0 || rem == prevC;
+      prevC = rem;
+    }
+  }
+  colorStats(jm, gtid, gstride);
+  colorStats(jc, gtid, gstride);
 }
 
 }  // namespace pdem

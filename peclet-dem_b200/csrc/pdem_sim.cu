@@ -19,6 +19,8 @@
 
 namespace pdem {
 
+long gDeviceAllocs = 0;
+
 void cudaCheck(cudaError_t e, const char* what) {
   if (e != cudaSuccess)
     throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
@@ -561,6 +563,7 @@ void Sim<R>::setPositions(const R* xyz, int n) {
   if (batch_ && n != numReal_)
     batch_ = false;  // the scene layout described the previous particle set
   sceneParamsDirty_ = true;
+  maxScaleValid_ = false;
   numReal_ = n;
   numParticles_ = n;
   hzNumPairs_ = -1;
@@ -613,6 +616,7 @@ void Sim<R>::clearExternalForces() {
 template <class R>
 void Sim<R>::setScales(const R* s, int n) {  // src/sim.hpp:1340-1346
   sceneParamsDirty_ = true;
+  maxScaleValid_ = false;
   const int m = std::min(numReal_, n);
   if (m > 0)
     cudaCheck(cudaMemcpyAsync(target_.p, s, m * sizeof(R), cudaMemcpyHostToDevice, stream_), "H2D scales");
@@ -622,6 +626,7 @@ void Sim<R>::setScales(const R* s, int n) {  // src/sim.hpp:1340-1346
 template <class R>
 void Sim<R>::setScalesUniform(R s) {  // src/sim.hpp:1331-1337
   sceneParamsDirty_ = true;
+  maxScaleValid_ = false;
   if (numReal_ > 0) {
     std::vector<R> h(numReal_, s);
     cudaCheck(cudaMemcpyAsync(scale_.p, h.data(), numReal_ * sizeof(R), cudaMemcpyHostToDevice, stream_), "H2D");
@@ -636,6 +641,7 @@ void Sim<R>::setGrowthParams(R rate, R nf) {  // src/sim.hpp:1416-1424
   else if (nf > R(0))
     gf_ = nf;
   gr_ = rate;
+  maxScaleValid_ = false;
   if (gf_ > R(0) && numReal_ > 0) {
     ++launches_, kGrowthScales<<<gridFor(numReal_), kBlock, 0, stream_>>>(d_, numReal_, gf_);
     KCHECK("growth");
@@ -693,14 +699,18 @@ template <class R>
 R Sim<R>::maxOwnedRadius() {
   if (numReal_ <= 0)
     return gs_ * baseRadius_;
-  rA_.ensure(1, false, stream_);
-  rA_.zero(stream_, 1);
-  ++launches_, kMaxScale<<<gridFor(numReal_), kBlock, 0, stream_>>>(d_, numReal_, rA_.p);
-  KCHECK("maxScale");
-  R mx;
-  cudaCheck(cudaMemcpyAsync(&mx, rA_.p, sizeof(R), cudaMemcpyDeviceToHost, stream_), "D2H");
-  sync();
-  return mx * gs_ * baseRadius_;
+  // the largest scale changes only through the scale setters, set_positions and growth: it is
+  // read back once and kept until one of them runs
+  if (!maxScaleValid_ || gf_ > R(0)) {
+    rA_.ensure(1, false, stream_);
+    rA_.zero(stream_, 1);
+    ++launches_, kMaxScale<<<gridFor(numReal_), kBlock, 0, stream_>>>(d_, numReal_, rA_.p);
+    KCHECK("maxScale");
+    cudaCheck(cudaMemcpyAsync(&maxScaleHost_, rA_.p, sizeof(R), cudaMemcpyDeviceToHost, stream_), "D2H");
+    sync();
+    maxScaleValid_ = true;
+  }
+  return maxScaleHost_ * gs_ * baseRadius_;
 }
 // src/sim.hpp:119-145 (+ periodicity.hpp:43-94)
 template <class R>
@@ -882,11 +892,16 @@ void Sim<R>::detectAll(R margin) {
   exclusiveSum(iA_.p, iB_.p, np + 1);
   exclusiveSum(iC_.p, offP, nr + 1);
   exclusiveSum(iD_.p, cntW, nr + 1);
+  // one read-back: the three totals and the counters the count passes updated (max overlap, errors)
   int tot[3] = {0, 0, 0};
+  Counters<R> c;
   cudaCheck(cudaMemcpyAsync(&tot[0], iB_.p + np, sizeof(int), cudaMemcpyDeviceToHost, stream_), "D2H");
   cudaCheck(cudaMemcpyAsync(&tot[1], offP + nr, sizeof(int), cudaMemcpyDeviceToHost, stream_), "D2H");
   cudaCheck(cudaMemcpyAsync(&tot[2], cntW + nr, sizeof(int), cudaMemcpyDeviceToHost, stream_), "D2H");
+  cudaCheck(cudaMemcpyAsync(&c, ctr_.p, sizeof c, cudaMemcpyDeviceToHost, stream_), "D2H counters");
   sync();
+  if (c.err & kErrBarrier)
+    throw CudaError("a grid-wide barrier of a persistent loop timed out (blocks not co-resident)");
   if (np > 0 && tot[0] > 0) {
     if (shell)
       ++launches_, kNarrowShell<R, 1><<<gridFor((long)np * 32), kBlock, 0, stream_>>>(d_, np, P, nullptr, iB_.p);
@@ -910,11 +925,13 @@ void Sim<R>::detectAll(R margin) {
   lastTot_[0] = tot[0], lastTot_[1] = tot[1], lastTot_[2] = tot[2];
   if (batch_ && total > maxContacts_)
     throw std::runtime_error("batched scenes: the contact buffer overflowed (raise the capacity)");
-  Counters<R> c = readCounters();
+  // the write passes leave the counters unchanged: the snapshot above is current
   c.pairCount = np;
   c.contactTotal = (int)std::min<long>(total, 0x7fffffff);
   c.contactCount = (int)std::min<long>(total, maxContacts_);
-  cudaCheck(cudaMemcpyAsync(ctr_.p, &c, sizeof c, cudaMemcpyHostToDevice, stream_), "H2D counters");
+  detectCounters_ = c;
+  cudaCheck(cudaMemcpyAsync(ctr_.p, &detectCounters_, sizeof(Counters<R>), cudaMemcpyHostToDevice, stream_),
+            "H2D counters");
 }
 
 // src/contact_preprocessing.hpp:378-471
@@ -946,40 +963,43 @@ int Sim<R>::reduceManifolds(int nc) {
   return nm;
 }
 
-// Jones-Plassmann rounds (src/solver_velocity.hpp:277-374 / src/solver_position.hpp:155-241)
+// Both Jones-Plassmann colourings of the substep in one cooperative launch
+// (src/solver_velocity.hpp:277-374 for the manifolds, src/solver_position.hpp:155-241 for the
+// contacts); one read-back gives each graph's colour count and uncoloured entries.
 template <class R>
-int Sim<R>::colorGraph(bool manifold, int ne, int nb, int& leftover) {
-  leftover = 0;
-  if (ne <= 0 || nb <= 0)
-    return 0;
-  int* col = manifold ? mColor_.p : cColor_.p;
-  ++launches_, kFillU64<<<gridFor(nb), kBlock, 0, stream_>>>(mask_.p, nb, 0ull);
-  if (manifold)
-    ++launches_, kColorInitManifolds<<<gridFor(ne), kBlock, 0, stream_>>>(d_, ne);
-  else
-    ++launches_, kFillInt<<<gridFor(ne), kBlock, 0, stream_>>>(col, ne, -1);
-  KCHECK("color init");
-  winner2_.ensure(nb, false, stream_);
-  colorAux_.ensure(8, false, stream_);
-  ++launches_, kFillLL<<<gridFor(nb), kBlock, 0, stream_>>>(winner_.p, nb, -1ll);
-  const int aux[5] = {0, 0, 0, std::numeric_limits<int>::min(), 0};  // remCnt[3], stats[2]
-  cudaCheck(cudaMemcpyAsync(colorAux_.p, aux, sizeof aux, cudaMemcpyHostToDevice, stream_), "H2D colour aux");
+void Sim<R>::colorBoth(int nm, int nc, int& ncolV, int& velLeft, int& ncolP, int& posLeft) {
+  ncolV = ncolP = velLeft = posLeft = 0;
+  const int nbM = numReal_, nbC = numParticles_;
+  const int neM = (nm > 0 && nbM > 0) ? nm : 0, neC = (nc > 0 && nbC > 0) ? nc : 0;
+  if (neM == 0 && neC == 0)
+    return;
+  mask_.ensure(std::max(nbM, 1), false, stream_);
+  maskP_.ensure(std::max(nbC, 1), false, stream_);
+  winner_.ensure(std::max(nbM, 1), false, stream_);
+  winner2_.ensure(std::max(nbM, 1), false, stream_);
+  winnerP_.ensure(std::max(nbC, 1), false, stream_);
+  winnerP2_.ensure(std::max(nbC, 1), false, stream_);
+  colorAux_.ensure(10, false, stream_);
+  const ColorJob jm{neM, nbM, mColor_.p, winner_.p, winner2_.p, mask_.p, colorAux_.p};
+  const ColorJob jc{neC, nbC, cColor_.p, winnerP_.p, winnerP2_.p, maskP_.p, colorAux_.p + 5};
   gbar_.ensure(2, false, stream_);
   const GridBar gb{gbar_.p, &ctr_.p->err};
-  if (manifold)
-    launchCoopB(kColorLoop<R, true>, kColorBlock, d_, ne, nb + 2, col, winner_.p, winner2_.p, colorAux_.p, colorAux_.p + 3, gb);
-  else
-    launchCoopB(kColorLoop<R, false>, kColorBlock, d_, ne, nb + 2, col, winner_.p, winner2_.p, colorAux_.p, colorAux_.p + 3, gb);
+  launchCoopB(kColorBoth<R>, kColorBlock, d_, jm, jc, std::max(nbM, nbC) + 2, gb);
   KCHECK("colour loop");
-  int res[2];
-  cudaCheck(cudaMemcpyAsync(res, colorAux_.p + 3, sizeof res, cudaMemcpyDeviceToHost, stream_), "D2H");
-  int err = 0;
+  int res[10], err = 0;
+  cudaCheck(cudaMemcpyAsync(res, colorAux_.p, sizeof res, cudaMemcpyDeviceToHost, stream_), "D2H");
   cudaCheck(cudaMemcpyAsync(&err, &ctr_.p->err, sizeof err, cudaMemcpyDeviceToHost, stream_), "D2H");
   sync();
   if (err & kErrBarrier)
     throw CudaError("colouring: a grid-wide barrier timed out");
-  leftover = res[1];
-  return res[0] + 1;
+  if (neM > 0) {
+    ncolV = res[3] + 1;
+    velLeft = res[4];
+  }
+  if (neC > 0) {
+    ncolP = res[8] + 1;
+    posLeft = res[9];
+  }
 }
 // stable colour-sorted execution order: colour c occupies [off[c], off[c+1])
 template <class R>
@@ -1065,7 +1085,7 @@ void Sim<R>::demStep() {
   }
   mark(ST_BROAD);
   detectAll(margin);
-  Counters<R> c0 = readCounters();
+  Counters<R> c0 = detectCounters_;  // the device counters as detectAll left them
   const int nc = c0.contactCount;
   mark(ST_MANIFOLD);
   const int nm = reduceManifolds(nc);
@@ -1087,12 +1107,16 @@ void Sim<R>::demStep() {
     KCHECK("plane load");
   }
   mark(ST_COLOR_V);
-  int velLeft = 0;
-  const int ncolV = useGS_ ? colorGraph(true, nm, numReal_, velLeft) : 0;
-  if (batch_ && velLeft > 0)
-    throw std::runtime_error("batched scenes: uncoloured manifolds (Jacobi fallback) are not supported");
+  // both colourings now: the contact graph is fixed since the narrowphase
+  int velLeft = 0, posLeft = 0, ncolV = 0, ncolP = 0;
+  if (useGS_)
+    colorBoth(nm, nc, ncolV, velLeft, ncolP, posLeft);
+  if (batch_ && (velLeft > 0 || posLeft > 0))
+    throw std::runtime_error("batched scenes: uncoloured entries (Jacobi fallback) are not supported");
   if (useGS_ && ncolV > 0)
     colorOrder(true, nm, ncolV);
+  if (useGS_ && ncolP > 0)
+    colorOrder(false, nc, ncolP);
   const bool usePGS = gNZ && useGS_;
   const R gMag = std::sqrt(g_[0] * g_[0] + g_[1] * g_[1] + g_[2] * g_[2]);
   const V3<R> gHat = gNZ ? V3<R>{g_[0] / gMag, g_[1] / gMag, g_[2] / gMag} : V3<R>{0, 0, 0};
@@ -1253,12 +1277,6 @@ void Sim<R>::demStep() {
     KCHECK("apply vel predict pos");
   }
   mark(ST_COLOR_P);
-  int posLeft = 0;
-  const int ncolP = useGS_ ? colorGraph(false, nc, numParticles_, posLeft) : 0;
-  if (batch_ && posLeft > 0)
-    throw std::runtime_error("batched scenes: uncoloured contacts (Jacobi fallback) are not supported");
-  if (useGS_ && ncolP > 0)
-    colorOrder(false, nc, ncolP);
   mark(ST_POSITION);
   const R posTol = R(1e-4) * baseRadius_ * gs_;
   if (nc > 0)
@@ -1314,7 +1332,10 @@ void Sim<R>::demStep() {
     for (int a = 0; a < 3; ++a) {
       dom.mn[a] = dmin_[a], dom.mx[a] = dmax_[a], dom.sz[a] = dsize_[a], dom.per[a] = per_[a];
     }
-    ++launches_, kFinalCommit<<<gridFor(numReal_), B, 0, s>>>(d_, numReal_, dom);
+    if (mixed_)
+      ++launches_, kMixedCommit<<<gridFor(numReal_), B, 0, s>>>(d_, numReal_, dom, posD_.p, quatD_.p);
+    else
+      ++launches_, kFinalCommit<<<gridFor(numReal_), B, 0, s>>>(d_, numReal_, dom);
     KCHECK("final commit");
   }
   if (thTau_ > R(0) && dt_ > R(0) && numReal_ > 0) {  // src/integration.hpp:229-272
@@ -1605,6 +1626,8 @@ void Sim<R>::stepHertz(R dt, int nsteps, R skinFrac) {
   dt_ = dt;
   if (batch_)
     throw std::runtime_error("step_hertz: not supported for batched scenes");
+  if (mixed_)
+    throw std::runtime_error("step_hertz: not supported in the FP32-mixed precision");
   if (per_[0] || per_[1] || per_[2])
     throw std::runtime_error("step_hertz: periodic domains not supported");
   if (!planesHost_.empty())
@@ -1721,6 +1744,12 @@ void Sim<R>::logSupportGraph(int nm, V3<R> gHat) {
   const int slot = (int)(gLog_ % kGroundRing);
   gRingNm_[slot] = nm;
   gRingReal_[slot] = numReal_;
+  gRingScenes_[slot] = batch_ ? numScenes_ : 0;
+  if (batch_) {  // the scenes' edge ranges of this substep, for one warp per scene at replay
+    gRingScn_[slot].ensure(numScenes_ + 1, false, stream_);
+    cudaCheck(cudaMemcpyAsync(gRingScn_[slot].p, sceneManFirstD_.p, (numScenes_ + 1) * sizeof(int),
+                              cudaMemcpyDeviceToDevice, stream_), "D2D scene ranges");
+  }
   if (nm > 0) {
     gRing_[slot].ensure(nm, false, stream_);
     ++launches_, kGroundEdges<<<gridFor(nm), kBlock, 0, stream_>>>(d_, nm, gHat, gRing_[slot].p);
@@ -1743,6 +1772,7 @@ void Sim<R>::ensureGrounded() {
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(kGroundSweeps, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(kGroundSweepsScenes, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     attr = true;
   }
   for (long e = start; e < gLog_; ++e) {
@@ -1751,7 +1781,14 @@ void Sim<R>::ensureGrounded() {
     if (nr <= 0)
       continue;
     ++launches_, kGroundDecay<<<gridFor(nr), kBlock, 0, stream_>>>(d_, nr, 8);
-    if (nm > 0) {
+    if (nm > 0 && gRingScenes_[slot] > 0) {
+      const int S = gRingScenes_[slot];
+      const bool smem = (size_t)maxSceneBodies_ * sizeof(int) <= 200 * 1024;
+      if (!smem)
+        gscratch_.ensure(nr, false, stream_);
+      ++launches_, kGroundSweepsScenes<<<S, 32, smem ? maxSceneBodies_ * sizeof(int) : 0, stream_>>>(
+          gRingScn_[slot].p, sceneFirstD_.p, 8, gRing_[slot].p, grounded_.p, gscratch_.p, smem);
+    } else if (nm > 0) {
       const bool smem = (size_t)nr * sizeof(int) <= 200 * 1024;
       if (!smem)
         gscratch_.ensure(nr, false, stream_);
@@ -1806,6 +1843,60 @@ void Sim<R>::flushMarks() {
 }
 
 // =============================================================================================
+// FP32-mixed form: single-precision step, FP64 master positions and orientations
+// =============================================================================================
+template <class R>
+void Sim<R>::setMixed(bool on) {
+  mixed_ = on;
+  if (on) {
+    posD_.ensure(capacity_, false, stream_);
+    quatD_.ensure(capacity_, false, stream_);
+  }
+}
+// field 0: positions (n x 3), 2: quaternions (n x 4, x y z w); also resets the orientations to
+// identity when the positions are set (set_positions resets every other field)
+template <class R>
+void Sim<R>::setMaster(int field, const double* a, int n) {
+  if (!mixed_)
+    return;
+  const int m = std::min(numReal_, n);
+  if (m <= 0)
+    return;
+  const int cols = field == 2 ? 4 : 3;
+  std::vector<Q4<double>> h(m);
+  for (int i = 0; i < m; ++i)
+    h[i] = Q4<double>{a[cols * i], a[cols * i + 1], a[cols * i + 2], cols == 4 ? a[cols * i + 3] : 0.0};
+  cudaCheck(cudaMemcpyAsync(field == 2 ? quatD_.p : posD_.p, h.data(), m * sizeof(Q4<double>),
+                            cudaMemcpyHostToDevice, stream_), "H2D master");
+  if (field == 0) {
+    std::vector<Q4<double>> q(m, Q4<double>{0, 0, 0, 1});
+    cudaCheck(cudaMemcpyAsync(quatD_.p, q.data(), m * sizeof(Q4<double>), cudaMemcpyHostToDevice, stream_), "H2D");
+  }
+  sync();
+}
+template <class R>
+bool Sim<R>::getMaster(int field, double* out, long cap) {
+  if (!mixed_ || (field != 0 && field != 2))
+    return false;
+  const int n = numReal_;
+  std::vector<Q4<double>> h(std::max(n, 0));
+  if (n > 0) {
+    cudaCheck(cudaMemcpyAsync(h.data(), field == 2 ? quatD_.p : posD_.p, n * sizeof(Q4<double>),
+                              cudaMemcpyDeviceToHost, stream_), "D2H master");
+    sync();
+  }
+  const int cols = field == 2 ? 4 : 3;
+  for (int i = 0; i < n && (long)cols * i + cols - 1 < cap; ++i) {
+    out[cols * i] = h[i].x;
+    out[cols * i + 1] = h[i].y;
+    out[cols * i + 2] = h[i].z;
+    if (cols == 4)
+      out[cols * i + 3] = h[i].w;
+  }
+  return true;
+}
+
+// =============================================================================================
 // batched form
 // =============================================================================================
 template <class R>
@@ -1824,8 +1915,12 @@ void Sim<R>::setScenes(int S, const int* first) {
   for (int s = 0; s < S; ++s)
     if (first[s + 1] < first[s])
       throw std::invalid_argument("set_scenes: scene ranges must be non-decreasing");
+  ensureGrounded();  // the logged support graphs index the previous scene layout
   numScenes_ = S;
   sceneFirstHost_.assign(first, first + S + 1);
+  maxSceneBodies_ = 0;
+  for (int s = 0; s < S; ++s)
+    maxSceneBodies_ = std::max(maxSceneBodies_, first[s + 1] - first[s]);
   std::vector<int> of(std::max(numReal_, 1), 0);
   for (int s = 0; s < S; ++s)
     for (int i = first[s]; i < first[s + 1]; ++i)
@@ -1856,6 +1951,7 @@ void Sim<R>::setSceneMaterial(int scene, R e, R mu) {
   sceneE_[scene] = e;
   sceneMu_[scene] = mu;
   sceneParamsDirty_ = true;
+  maxScaleValid_ = false;
 }
 template <class R>
 void Sim<R>::setWallScene(int wall, int scene) {

@@ -19,6 +19,10 @@ struct CudaError : std::runtime_error {
 };
 void cudaCheck(cudaError_t e, const char* what);
 
+// device allocations made by growable buffers since load (instrumentation: a step that reallocates
+// stalls on cudaMalloc / cudaFree)
+extern long gDeviceAllocs;
+
 // growable device buffer (contents not preserved unless asked)
 template <class T>
 struct DBuf {
@@ -35,7 +39,10 @@ struct DBuf {
     if (want <= n && p)
       return;
     size_t cap = want < 1 ? 1 : want;
+    if (p && cap < n + n / 2)
+      cap = n + n / 2;  // grow geometrically: counts that creep up each substep reallocate rarely
     T* q = nullptr;
+    ++gDeviceAllocs;
     cudaCheck(cudaMalloc(&q, cap * sizeof(T)), "cudaMalloc");
     cudaCheck(cudaMemsetAsync(q, 0, cap * sizeof(T), s), "cudaMemset");
     if (preserve && p && n)
@@ -138,6 +145,12 @@ class Sim {
   int hzNumPairs_ = -1, hzPrevCount_ = 0, hzNumWallCand_ = 0;
   R hzContactFrac_ = R(0.5);
 
+  // ---- FP32-mixed form (meaningful for R = float): FP64 master positions / orientations ----
+  void setMixed(bool on);
+  void setMaster(int field, const double* a, int n);
+  bool getMaster(int field, double* out, long cap);
+  bool mixed_ = false;
+
   // ---- batched form: independent scenes in one body array, each stepped as it would be alone ----
   void setScenes(int S, const int* firstBody);
   void setSceneMaterial(int scene, R e, R mu);
@@ -194,22 +207,28 @@ class Sim {
   int numSMs_ = 148;
   // batched form
   bool batch_ = false, sceneParamsDirty_ = true, sceneWallsDirty_ = true;
-  int numScenes_ = 1;
+  bool maxScaleValid_ = false;  // maxScaleHost_ holds the largest scale of the real bodies
+  R maxScaleHost_ = R(0);
+  int numScenes_ = 1, maxSceneBodies_ = 0;
   std::vector<int> sceneFirstHost_;   // [S + 1] first body of each scene
   std::vector<R> sceneE_, sceneMu_;   // per-scene restitution and friction
   std::vector<int> wallScene_;        // per wall: its scene, or -1 for every scene
   DBuf<int> sceneOf_, sceneFirstD_, sceneWallOffD_, sceneWallIdxD_, sceneManFirstD_, sceneConFirstD_,
       sceneLeafFirstD_, bvhFirst_, bvhLast_;
   DBuf<SceneCtl<R>> scn_;
+  DBuf<Q4<double>> posD_, quatD_;  // FP32-mixed form: master positions and orientations
   DBuf<R> sceneParams_, sceneMaxScale_;
   int lastTot_[3] = {0, 0, 0};
+  Counters<R> detectCounters_{};  // host copy of the counters after the narrowphase (H2D source)
   void batchBegin();
   long wallsPerBody() const;
   void batchBounds(int nm);
   void ctl(int op, R thr, int mode);
   DBuf<unsigned> gbar_;        // grid barrier of the persistent loops
   DBuf<long long> winner2_;    // second winner array of the colouring rounds
-  DBuf<int> colorAux_;         // colouring: per-round remaining counts [3], statistics [2]
+  DBuf<long long> winnerP_, winnerP2_;  // winner arrays of the contact colouring
+  DBuf<u64> maskP_;                     // colour masks of the contact colouring
+  DBuf<int> colorAux_;         // colouring, per graph (5 each): remaining counts [3], statistics [2]
   // scratch
   DBuf<char> cubTmp_;
   DBuf<int> iA_, iB_, iC_, iD_, iE_;
@@ -220,6 +239,8 @@ class Sim {
   static constexpr int kGroundRing = 32;  // 255 / 8 < 32 substeps of decay erase any level
   DBuf<int4> gRing_[kGroundRing];
   int gRingNm_[kGroundRing] = {}, gRingReal_[kGroundRing] = {};
+  int gRingScenes_[kGroundRing] = {};   // batched form: scenes of the slot (0: one scene)
+  DBuf<int> gRingScn_[kGroundRing];     // batched form: first manifold of each scene in the slot
   long gLog_ = 0, gCheckpoint_ = 0;
   DBuf<int> gscratch_;
   DBuf<double> thermo_;
@@ -266,7 +287,7 @@ class Sim {
   int findCollisions(R margin, int cap);
   void detectAll(R margin);
   int reduceManifolds(int nc);
-  int colorGraph(bool manifold, int ne, int nb, int& leftover);
+  void colorBoth(int nm, int nc, int& ncolV, int& velLeft, int& ncolP, int& posLeft);
   void colorOrder(bool manifold, int ne, int ncol);
   void buildIncidence(int kind, int ne, int nb);
   void logSupportGraph(int nm, V3<R> gHat);

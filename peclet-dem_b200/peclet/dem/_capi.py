@@ -22,6 +22,9 @@ _long_p = C.POINTER(C.c_long)
 _u64_p = C.POINTER(C.c_ulonglong)
 _vp = C.c_void_p
 
+# precision code of the FP32-mixed form (include/pdem.h PDEM_MIXED)
+PRECISION_MIXED = 3264
+
 # status codes (include/pdem.h)
 OK, ERR_RUNTIME, ERR_INVALID, ERR_UNSUPPORTED, ERR_CUDA = 0, 1, 2, 3, 4
 
@@ -102,6 +105,7 @@ _SIGS = {
     "profile_enable": (C.c_int, [_vp, C.c_int]),
     "profile_read": (C.c_int, [_vp, _dbl_p, _long_p, C.c_int, _long_p]),
     "debug_sweeps": (C.c_int, [_vp, _long_p]),
+    "debug_allocs": (C.c_long, []),
     # batched form
     "set_scenes": (C.c_int, [_vp, C.c_int, _int_p]),
     "set_scene_material": (C.c_int, [_vp, C.c_int, C.c_double, C.c_double]),
@@ -178,15 +182,15 @@ class CApiSimulation:
     """
 
     def __init__(self, api: CApi, capacity: int, precision: str = "fp64"):
-        if precision not in ("fp64", "fp32"):
-            raise ValueError("precision must be 'fp64' or 'fp32'")
+        if precision not in ("fp64", "fp32", "mixed"):
+            raise ValueError("precision must be 'fp64', 'fp32' or 'mixed'")
         self._api = api
         self._f = api.fn
         self.precision = precision
-        self._out_dtype = np.float64 if precision == "fp64" else np.float32
+        self._out_dtype = np.float32 if precision == "fp32" else np.float64
+        code = {"fp64": 64, "fp32": 32, "mixed": PRECISION_MIXED}[precision]
         h = _vp()
-        api.check(self._f["create"](int(capacity), 64 if precision == "fp64" else 32, C.byref(h)),
-                  "Simulation(capacity)")
+        api.check(self._f["create"](int(capacity), code, C.byref(h)), "Simulation(capacity)")
         self._h = h
 
     # ---- lifetime -------------------------------------------------------------------------------

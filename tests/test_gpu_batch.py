@@ -21,25 +21,48 @@ def _drums():
     return [S.spheres_in_drum(seed=seed, n=n, omega=om, e=e, mu=mu) for seed, n, om, e, mu in SPECS]
 
 
+def _columns():
+    """Settling lattice columns: resting contacts under gravity fire the stabilization pass (support
+    levels, side flags) in every scene."""
+    out = []
+    for seed, (e, mu) in zip((41, 42, 43), ((0.5, 0.5), (0.3, 0.8), (0.8, 0.2))):
+        sc = S.settled_column(seed=seed)
+        sc.material = (e, 0.0, mu)
+        out.append((sc, None))
+    return out
+
+
+CASES = [("drums", _drums, 12), ("columns", _columns, 25)]
+
+
 @pytest.mark.parametrize("precision,rtol", [("fp32", 0.0), ("fp64", 1e-12)])
-def test_batch_matches_each_scene_alone(gpu_api, orc_api, precision, rtol):
-    drums = _drums()
-    scenes = [d[0] for d in drums]
+@pytest.mark.parametrize("name,mk,steps", CASES, ids=[c[0] for c in CASES])
+def test_batch_matches_each_scene_alone(gpu_api, orc_api, name, mk, steps, precision, rtol):
+    cases = mk()
+    scenes = [c[0] for c in cases]
     batch = CApiSimulation(gpu_api, sum(sc.n for sc in scenes) + 8, precision)
-    first = apply_batch(batch, scenes, [d[1] for d in drums])
-    alone = [P.build(orc_api, sc, ex, precision) for sc, ex in drums]
+    first = apply_batch(batch, scenes, [c[1] for c in cases])
+    alone = [P.build(orc_api, sc, ex, precision) for sc, ex in cases]
     dt = scenes[0].dt
-    for k in range(12):
+    stab = np.zeros(len(scenes))
+    for k in range(steps):
         batch.step(dt)
         for a in alone:
             a.step(dt)
+        counters = batch.scene_counters()
+        assert counters.shape == (len(scenes), 5)
+        stab += counters[:, 3]
         got = P.snapshot(batch, products=False)
+        got["grounded"] = batch.debug_grounded()  # support levels (stabilization), per body
         for s, a in enumerate(alone):
             sl = slice(int(first[s]), int(first[s + 1]))
             mine = {key: v[sl] for key, v in got.items()}
-            bad = P.diff(mine, P.snapshot(a, products=False), rtol=rtol)
-            assert not bad, f"{precision}: substep {k}, scene {s}: {bad[:4]}"
-    assert batch.scene_counters().shape == (len(scenes), 5)
+            want = P.snapshot(a, products=False)
+            want["grounded"] = a.debug_grounded()
+            bad = P.diff(mine, want, rtol=rtol)
+            assert not bad, f"{name} {precision}: substep {k}, scene {s}: {bad[:4]}"
+    if name == "columns":
+        assert stab.min() > 0, "the stabilization pass (support levels) did not run in every scene"
 
 
 def test_batch_overlap_per_scene(gpu_api, orc_api):
