@@ -403,6 +403,23 @@ __device__ __forceinline__ int arriveAcqRel(int* p) {
   return old;
 }
 
+// refit-only substeps: the leaves keep their place in the last build's order (and their links);
+// only their boxes are refreshed from the current primitive boxes
+template <class R>
+__global__ void kRefreshLeaves(BvhBuffers bb, const Box<R>* prim, PNode* nodes) {
+  const int n = bb.n;
+  GRID_STRIDE(k, n) {
+    float lo[3], hi[3];
+    outwardBox(prim[bb.idx[k]], lo, hi);
+    float* dst = reinterpret_cast<float*>(&nodes[n - 1 + k]);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      dst[a] = lo[a];
+      dst[3 + a] = hi[a];
+    }
+  }
+}
+
 // bottom-up union of the float boxes; the second child to arrive at a node computes it
 static __global__ void kRefitPacked(BvhBuffers bb, PNode* nodes) {
   const int n = bb.n;

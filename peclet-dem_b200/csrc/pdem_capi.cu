@@ -283,16 +283,19 @@ int pdem_set_positions(pdem_handle h, const double* xyz, int n) {
 #define SETROWS(NAME, FIELD, COLS)                                  \
   int NAME(pdem_handle h, const double* a, int n) {                 \
     BODY({                                                          \
-      const auto v = conv<R>(a, (long)n * COLS);                    \
-      S.setRows(FIELD, v.data(), n);                                \
+      if (FIELD == 5) {                                             \
+        const auto v = conv<R>(a, (long)n * COLS);                  \
+        S.setRows(FIELD, v.data(), n);                              \
+      } else {                                                      \
+        S.setRowsD(FIELD, a, n);                                    \
+      }                                                             \
     });                                                             \
   }
 SETROWS(pdem_set_velocities, 0, 3)
 SETROWS(pdem_set_external_forces, 1, 3)
 int pdem_set_quaternions(pdem_handle h, const double* a, int n) {
   BODY({
-    const auto v = conv<R>(a, (long)n * 4);
-    S.setRows(2, v.data(), n);
+    S.setRowsD(2, a, n);
     S.setMaster(2, a, n);
   });
 }
@@ -326,6 +329,10 @@ double pdem_get_growth_rate(pdem_handle h) {
       n = (long)S.numReal_ * COLS;                                        \
       if (S.getMaster(FIELD, out, cap))                                   \
         return;                                                           \
+      if (FIELD <= 4) {                                                   \
+        S.getRowsD(FIELD, out, cap);                                      \
+        return;                                                           \
+      }                                                                   \
       std::vector<R> tmp((size_t)std::max(n, 0L));                        \
       S.getRows(FIELD, tmp.data(), (long)tmp.size());                     \
       for (long i = 0; i < n && i < cap; ++i)                             \

@@ -715,6 +715,17 @@ __device__ __forceinline__ long long entryKey(const Dev<R>& d, int i, int ea) {
   const int s = d.sceneOf[ea];
   return colorKey(MANIFOLD ? localManifold(d, i, s) : localContact(d, i, s));
 }
+// batched form: (scene, colour) keys, so each scene's colour classes are contiguous and in colour
+// order (scene << 6 | colour, 63 = uncoloured)
+template <class R, bool MANIFOLD>
+__global__ void kColorSortKeysScenes(Dev<R> d, int ne, const int* col, unsigned* keys, int* vals) {
+  GRID_STRIDE(i, ne) {
+    const int c = col[i];
+    const int body = MANIFOLD ? d.mab[i].x : d.cab[i].x;
+    keys[i] = ((unsigned)d.sceneOf[body] << 6) | ((c >= 0) ? (unsigned)c : 63u);
+    vals[i] = (int)i;
+  }
+}
 // colour keys for the stable colour-sorted execution order
 __global__ void kColorSortKeys(int ne, const int* col, unsigned* keys, int* vals) {
   GRID_STRIDE(i, ne) {

@@ -143,6 +143,27 @@ __global__ void kFinalCommit(Dev<R> d, int n, DomainP<R> dom) {
   }
 }
 
+// host rows (n x cols doubles, uploaded as they are) <-> the aligned 4-wide records of a field
+template <class R>
+__global__ void kPackRows(const double* src, int n, int cols, Q4<R>* dst) {
+  GRID_STRIDE(i, n) {
+    const double* r = src + (long)cols * i;
+    dst[i] = Q4<R>{(R)r[0], (R)r[1], (R)r[2], cols == 4 ? (R)r[3] : R(0)};
+  }
+}
+template <class R>
+__global__ void kUnpackRows(const Q4<R>* src, int n, int cols, double* dst) {
+  GRID_STRIDE(i, n) {
+    const Q4<R> q = src[i];
+    double* r = dst + (long)cols * i;
+    r[0] = q.x;
+    r[1] = q.y;
+    r[2] = q.z;
+    if (cols == 4)
+      r[3] = q.w;
+  }
+}
+
 // FP32-mixed form, end of a substep: the FP64 master positions and orientations advance by the
 // substep's single-precision increment (the difference of two nearby floats, exact), periodic
 // wrapping is applied in double, and the single-precision state is re-derived from the master,

@@ -564,6 +564,7 @@ void Sim<R>::setPositions(const R* xyz, int n) {
     batch_ = false;  // the scene layout described the previous particle set
   sceneParamsDirty_ = true;
   maxScaleValid_ = false;
+  bvhValid_ = false;
   numReal_ = n;
   numParticles_ = n;
   hzNumPairs_ = -1;
@@ -607,6 +608,47 @@ void Sim<R>::setRows(int field, const R* a, int n) {
   Q4<R>* dst = field == 0 ? vel_.p : field == 1 ? extF_.p : field == 2 ? quat_.p : field == 3 ? angVel_.p : invI_.p;
   cudaCheck(cudaMemcpyAsync(dst, h.data(), m * sizeof(Q4<R>), cudaMemcpyHostToDevice, stream_), "H2D rows");
   sync();
+}
+// rows of a 4-wide field straight from the caller's doubles: one copy to the device, packed
+// there (fields as setRows: 0 velocities, 1 external forces, 2 quaternions, 3 angular
+// velocities, 4 inverse inertia)
+template <class R>
+void Sim<R>::setRowsD(int field, const double* a, int n) {
+  const int m = std::min(numReal_, n);
+  if (m <= 0)
+    return;
+  const int cols = (field == 2) ? 4 : 3;
+  rowStage_.ensure((size_t)m * cols, false, stream_);
+  cudaCheck(cudaMemcpyAsync(rowStage_.p, a, (size_t)m * cols * sizeof(double), cudaMemcpyHostToDevice, stream_),
+            "H2D rows");
+  Q4<R>* dst = field == 0 ? vel_.p : field == 1 ? extF_.p : field == 2 ? quat_.p : field == 3 ? angVel_.p : invI_.p;
+  ++launches_, kPackRows<R><<<gridFor(m), kBlock, 0, stream_>>>(rowStage_.p, m, cols, dst);
+  KCHECK("pack rows");
+  sync();
+}
+// rows of a 4-wide field to the caller's doubles (fields as getRows: 0 positions, 1 velocities,
+// 2 quaternions, 3 angular velocities, 4 inverse inertia): unpacked on the device, one copy back
+template <class R>
+void Sim<R>::getRowsD(int field, double* out, long cap) {
+  const int n = numReal_;
+  if (n <= 0)
+    return;
+  const int cols = (field == 2) ? 4 : 3;
+  const long need = (long)n * cols;
+  rowStage_.ensure(need, false, stream_);
+  const Q4<R>* src = field == 0 ? pos_.p : field == 1 ? vel_.p : field == 2 ? quat_.p : field == 3 ? angVel_.p : invI_.p;
+  ++launches_, kUnpackRows<R><<<gridFor(n), kBlock, 0, stream_>>>(src, n, cols, rowStage_.p);
+  KCHECK("unpack rows");
+  if (cap >= need) {
+    cudaCheck(cudaMemcpyAsync(out, rowStage_.p, need * sizeof(double), cudaMemcpyDeviceToHost, stream_), "D2H rows");
+    sync();
+  } else {
+    std::vector<double> h(need);
+    cudaCheck(cudaMemcpyAsync(h.data(), rowStage_.p, need * sizeof(double), cudaMemcpyDeviceToHost, stream_),
+              "D2H rows");
+    sync();
+    std::copy(h.begin(), h.begin() + std::max(cap, 0L), out);
+  }
 }
 template <class R>
 void Sim<R>::clearExternalForces() {
@@ -780,30 +822,49 @@ int Sim<R>::findCollisions(R margin, int cap) {
     bb.last = bvhLast_.p;
     codeBits = std::min(64, kSceneShift + bitsFor(numScenes_));
   }
+  // The tree's topology (leaf order, links) is rebuilt when the body set changed or every
+  // kBvhRebuild substeps; in between only the boxes are refitted. Any tree whose boxes contain
+  // the current boxes gives the exact candidate set, so both paths give the same pairs.
+  const bool rebuild = !bvhValid_ || bvhN_ != n || bvhReal_ != numReal_ || bvhAge_ >= kBvhRebuild;
   const u64 init[6] = {~0ull, ~0ull, ~0ull, 0ull, 0ull, 0ull};
   cudaCheck(cudaMemcpyAsync(bounds_.p, init, sizeof init, cudaMemcpyHostToDevice, stream_), "H2D bounds");
   ++launches_, kBoxes<<<gridFor(n), kBlock, 0, stream_>>>(d_, n, margin, boxCap, bn, bb);
   KCHECK("boxes");
-  ++launches_, kMorton<R><<<gridFor(n), kBlock, 0, stream_>>>(n, bn, bb);
-  KCHECK("morton");
-  sortPairs(codes_.p, codesAlt_.p, bidx_.p, bidxAlt_.p, n, codeBits);
-  std::swap(bb.codes, bb.codesAlt);
-  std::swap(bb.idx, bb.idxAlt);
-  if (batch_)
+  if (rebuild) {
+    ++launches_, kMorton<R><<<gridFor(n), kBlock, 0, stream_>>>(n, bn, bb);  // into codes_ / bidx_
+    KCHECK("morton");
+    sortPairs(codes_.p, codesAlt_.p, bidx_.p, bidxAlt_.p, n, codeBits);
+  }
+  // the sorted order (this build's, or the last build's on a refit-only substep) is the sort's
+  // output, in the *Alt buffers
+  bb.codes = codesAlt_.p, bb.codesAlt = codes_.p, bb.idx = bidxAlt_.p, bb.idxAlt = bidx_.p;
+  if (rebuild && batch_)
     ++launches_, kSceneLeafFirst<<<gridFor(numScenes_ + 1), kBlock, 0, stream_>>>(n, numScenes_, bb.codes,
                                                                                   sceneLeafFirstD_.p);
   cudaCheck(cudaMemsetAsync(flag_.p, 0, n * sizeof(int), stream_), "memset");
   cudaCheck(cudaMemsetAsync(rowCnt_.p, 0, (numReal_ + 1) * sizeof(int), stream_), "memset");
   bflag_.ensure(1, false, stream_);
   cudaCheck(cudaMemsetAsync(bflag_.p, 0, sizeof(int), stream_), "memset");
-  ++launches_, kKarras<<<gridFor(n - 1), kBlock, 0, stream_>>>(bb);
-  KCHECK("karras");
-  ++launches_, kPackLeaves<R><<<gridFor(n), kBlock, 0, stream_>>>(bb, prim, nodes);
-  KCHECK("leaves");
-  ++launches_, kRefitPacked<<<gridFor(n), kBlock, 0, stream_>>>(bb, nodes);
-  KCHECK("refit");
-  ++launches_, kRopesPacked<<<gridFor(2 * n - 1), kBlock, 0, stream_>>>(bb, nodes);
-  KCHECK("ropes");
+  if (rebuild) {
+    ++launches_, kKarras<<<gridFor(n - 1), kBlock, 0, stream_>>>(bb);
+    KCHECK("karras");
+    ++launches_, kPackLeaves<R><<<gridFor(n), kBlock, 0, stream_>>>(bb, prim, nodes);
+    KCHECK("leaves");
+    ++launches_, kRefitPacked<<<gridFor(n), kBlock, 0, stream_>>>(bb, nodes);
+    KCHECK("refit");
+    ++launches_, kRopesPacked<<<gridFor(2 * n - 1), kBlock, 0, stream_>>>(bb, nodes);
+    KCHECK("ropes");
+    bvhValid_ = true;
+    bvhN_ = n;
+    bvhReal_ = numReal_;
+    bvhAge_ = 0;
+  } else {
+    ++launches_, kRefreshLeaves<R><<<gridFor(n), kBlock, 0, stream_>>>(bb, prim, nodes);
+    KCHECK("leaves");
+    ++launches_, kRefitPacked<<<gridFor(n), kBlock, 0, stream_>>>(bb, nodes);
+    KCHECK("refit");
+  }
+  ++bvhAge_;
   ++launches_, kQueryHalf<R><<<gridFor(n, 128), 128, 0, stream_>>>(bb, prim, nodes, numReal_, rowCnt_.p, qcnt_.p,
                                                                      slots_.p, bflag_.p);
   KCHECK("query");
@@ -984,7 +1045,14 @@ void Sim<R>::colorBoth(int nm, int nc, int& ncolV, int& velLeft, int& ncolP, int
   const ColorJob jc{neC, nbC, cColor_.p, winnerP_.p, winnerP2_.p, maskP_.p, colorAux_.p + 5};
   gbar_.ensure(2, false, stream_);
   const GridBar gb{gbar_.p, &ctr_.p->err};
-  launchCoopB(kColorBoth<R>, kColorBlock, d_, jm, jc, std::max(nbM, nbC) + 2, gb);
+  if (batch_) {  // one block per scene; the statistics slots start cleared
+    const int aux[10] = {0, 0, 0, std::numeric_limits<int>::min(), 0, 0, 0, 0, std::numeric_limits<int>::min(), 0};
+    cudaCheck(cudaMemcpyAsync(colorAux_.p, aux, sizeof aux, cudaMemcpyHostToDevice, stream_), "H2D colour aux");
+    ++launches_, kColorScenes<R><<<numScenes_, kSceneBlock, 0, stream_>>>(d_, jm, jc, sceneFirstD_.p,
+                                                                         std::max(nbM, nbC) + 2);
+  } else {
+    launchCoopB(kColorBoth<R>, kColorBlock, d_, jm, jc, std::max(nbM, nbC) + 2, gb);
+  }
   KCHECK("colour loop");
   int res[10], err = 0;
   cudaCheck(cudaMemcpyAsync(res, colorAux_.p, sizeof res, cudaMemcpyDeviceToHost, stream_), "D2H");
@@ -1011,6 +1079,19 @@ void Sim<R>::colorOrder(bool manifold, int ne, int ncol) {
   uA_.ensure(ne, false, stream_);
   uB_.ensure(ne, false, stream_);
   iE_.ensure(ne, false, stream_);
+  if (batch_) {  // (scene, colour) order: each scene's classes contiguous, for one block per scene
+    const int nk = numScenes_ * 64;
+    off.ensure(nk + 2, false, stream_);
+    if (manifold)
+      ++launches_, kColorSortKeysScenes<R, true><<<gridFor(ne), kBlock, 0, stream_>>>(d_, ne, mColor_.p, uA_.p, iE_.p);
+    else
+      ++launches_, kColorSortKeysScenes<R, false><<<gridFor(ne), kBlock, 0, stream_>>>(d_, ne, cColor_.p, uA_.p, iE_.p);
+    KCHECK("color keys");
+    sortPairs(uA_.p, uB_.p, iE_.p, order.p, ne, 6 + bitsFor(numScenes_));
+    ++launches_, kLowerBoundOffsets<unsigned><<<gridFor(nk + 1), kBlock, 0, stream_>>>(ne, uB_.p, nk, off.p);
+    KCHECK("color offsets");
+    return;
+  }
   ++launches_, kColorSortKeys<<<gridFor(ne), kBlock, 0, stream_>>>(ne, manifold ? mColor_.p : cColor_.p, uA_.p, iE_.p);
   KCHECK("color keys");
   sortPairs(uA_.p, uB_.p, iE_.p, order.p, ne, 6);
@@ -1153,7 +1234,11 @@ void Sim<R>::demStep() {
     const GridBar gb{gbar_.p, &ctr_.p->err};
     const R thr = usePGS ? R(0.02) * vRest : vRest;
     ctl(CTL_VEL_BEGIN, R(0), 0);
-    if (usePGS)
+    if (batch_ && usePGS)
+      ++launches_, kSweepScenes<R, 0, 1><<<numScenes_, kSceneBlock, 0, s>>>(d_, mOrder_.p, mOff_.p, velIters_, sp, thr);
+    else if (batch_)
+      ++launches_, kSweepScenes<R, 1, 1><<<numScenes_, kSceneBlock, 0, s>>>(d_, mOrder_.p, mOff_.p, velIters_, sp, thr);
+    else if (usePGS)
       launchCoop(kSweepLoop<R, 0, 1>, d_, (const int*)mOrder_.p, (const int*)mOff_.p, ncolV, velIters_, sp, thr, gb);
     else
       launchCoop(kSweepLoop<R, 1, 1>, d_, (const int*)mOrder_.p, (const int*)mOff_.p, ncolV, velIters_, sp, thr, gb);
@@ -1221,7 +1306,10 @@ void Sim<R>::demStep() {
         gbar_.ensure(2, false, s);
         const GridBar gb{gbar_.p, &ctr_.p->err};
         ctl(CTL_STAB_BEGIN, R(0), 0);
-        launchCoop(kSweepLoop<R, 0, 2>, d_, (const int*)mOrder_.p, (const int*)mOff_.p, ncolV, iters, ss, vRestS, gb);
+        if (batch_)
+          ++launches_, kSweepScenes<R, 0, 2><<<numScenes_, kSceneBlock, 0, s>>>(d_, mOrder_.p, mOff_.p, iters, ss, vRestS);
+        else
+          launchCoop(kSweepLoop<R, 0, 2>, d_, (const int*)mOrder_.p, (const int*)mOff_.p, ncolV, iters, ss, vRestS, gb);
       }
       for (int it = 0; it < (stabPersistent ? 0 : iters); ++it) {
         ctl(CTL_STAB_BEGIN, R(0), 0);
@@ -1293,7 +1381,10 @@ void Sim<R>::demStep() {
     gbar_.ensure(2, false, s);
     const GridBar gb{gbar_.p, &ctr_.p->err};
     ctl(CTL_POS_BEGIN, R(0), 0);
-    launchCoop(kSweepLoop<R, 2, 3>, d_, (const int*)cOrder_.p, (const int*)cOff_.p, ncolP, posIters_, sp, posTol, gb);
+    if (batch_)
+      ++launches_, kSweepScenes<R, 2, 3><<<numScenes_, kSceneBlock, 0, s>>>(d_, cOrder_.p, cOff_.p, posIters_, sp, posTol);
+    else
+      launchCoop(kSweepLoop<R, 2, 3>, d_, (const int*)cOrder_.p, (const int*)cOff_.p, ncolP, posIters_, sp, posTol, gb);
     KCHECK("position loop");
   }
   const bool posEmpty = useGS_ && posLeft == 0 && ncolP <= 0 && posIters_ > 0 && posTol > R(0);
@@ -1746,12 +1837,20 @@ void Sim<R>::logSupportGraph(int nm, V3<R> gHat) {
   gRingReal_[slot] = numReal_;
   gRingScenes_[slot] = batch_ ? numScenes_ : 0;
   if (batch_) {  // the scenes' edge ranges of this substep, for one warp per scene at replay
-    gRingScn_[slot].ensure(numScenes_ + 1, false, stream_);
+    if (gRingScn_[slot].n < (size_t)numScenes_ + 1)
+      for (auto& b : gRingScn_)
+        b.ensure(numScenes_ + 1, false, stream_);
     cudaCheck(cudaMemcpyAsync(gRingScn_[slot].p, sceneManFirstD_.p, (numScenes_ + 1) * sizeof(int),
                               cudaMemcpyDeviceToDevice, stream_), "D2D scene ranges");
   }
   if (nm > 0) {
-    gRing_[slot].ensure(nm, false, stream_);
+    // all slots grow together (and with headroom): a slot first used, or outgrown, later in a
+    // run would otherwise stall a substep on cudaMalloc / cudaFree
+    if (gRing_[slot].n < (size_t)nm) {
+      const size_t cap = (size_t)nm + (size_t)nm / 4;
+      for (auto& b : gRing_)
+        b.ensure(cap, false, stream_);
+    }
     ++launches_, kGroundEdges<<<gridFor(nm), kBlock, 0, stream_>>>(d_, nm, gHat, gRing_[slot].p);
     KCHECK("support graph");
   }
@@ -1916,6 +2015,7 @@ void Sim<R>::setScenes(int S, const int* first) {
     if (first[s + 1] < first[s])
       throw std::invalid_argument("set_scenes: scene ranges must be non-decreasing");
   ensureGrounded();  // the logged support graphs index the previous scene layout
+  bvhValid_ = false;  // the tree's leaf order must put every scene in one subtree
   numScenes_ = S;
   sceneFirstHost_.assign(first, first + S + 1);
   maxSceneBodies_ = 0;

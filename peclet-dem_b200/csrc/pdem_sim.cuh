@@ -99,6 +99,8 @@ class Sim {
   R growthFactor() const { return gf_; }
   R growthRate() const { return gr_; }
   void getRows(int field, R* out, long cap);  // positions .. masses
+  void setRowsD(int field, const double* a, int n);  // fields 0-4 of setRows, packed on the device
+  void getRowsD(int field, double* out, long cap);   // fields 0-4 of getRows, unpacked on the device
   void step(R dt);
   void stepHertz(R dt, int substeps, R skinFrac);
   R computeOverlaps();
@@ -208,6 +210,10 @@ class Sim {
   // batched form
   bool batch_ = false, sceneParamsDirty_ = true, sceneWallsDirty_ = true;
   bool maxScaleValid_ = false;  // maxScaleHost_ holds the largest scale of the real bodies
+  // broadphase tree reuse: topology rebuilt when the body set changes or every kBvhRebuild substeps
+  static constexpr int kBvhRebuild = 16;
+  bool bvhValid_ = false;
+  int bvhN_ = 0, bvhReal_ = 0, bvhAge_ = 0;
   R maxScaleHost_ = R(0);
   int numScenes_ = 1, maxSceneBodies_ = 0;
   std::vector<int> sceneFirstHost_;   // [S + 1] first body of each scene
@@ -217,6 +223,7 @@ class Sim {
       sceneLeafFirstD_, bvhFirst_, bvhLast_;
   DBuf<SceneCtl<R>> scn_;
   DBuf<Q4<double>> posD_, quatD_;  // FP32-mixed form: master positions and orientations
+  DBuf<double> rowStage_;           // host rows staged on the device (set/get of 4-wide fields)
   DBuf<R> sceneParams_, sceneMaxScale_;
   int lastTot_[3] = {0, 0, 0};
   Counters<R> detectCounters_{};  // host copy of the counters after the narrowphase (H2D source)
