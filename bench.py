@@ -15,6 +15,11 @@ the state resident in HBM; `e2e` runs the same loop through the public API with 
 host clock. `--impl reference` times the reference's own code (its headers built against the
 OpenMP flavour of the Kokkos shim) on this machine's host cores. More than one GPU runs replicas
 (the single-scene step has no shard-parallel decomposition).
+
+The `batched` object of the line measures the batched form on 512 rotating drums
+(`workloads.rotating_drums`, about 1.9 M bodies, one simulation per GPU; scenes split over the
+ranks) in FP64 and in the FP32-mixed form, with the mixed form's position error against the FP64
+run after the same substeps. `--drums 0` skips it.
 """
 from __future__ import annotations
 
@@ -104,6 +109,12 @@ def substep_bytes(n, P, C, M, iv, ip, D=8):
     Sm = 12 + 20 * D
     return (81 * D * n + 16 * P + 2 * C * (8 + 16 * D) + M * Sm + 12 * (M + C) + M * (16 + 8 * D)
             + iv * M * (Sm + 53 * D) + ip * C * (8 + 48 * D))
+
+
+# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum over the stage's kernels, one ncu
+# capture of a refit-only substep) of the broadphase stage at the default workload of 262,144
+# spheres, in bytes per substep; other sizes report none
+BROADPHASE_DRAM_BYTES = {262144: 140.7e6}
 
 
 def measured_peaks():
@@ -336,9 +347,11 @@ def run_ours(args):
     roof_stage = dominant if dominant in stage_bytes else "velocity"
     st_ms = per_step[roof_stage][0] / SUBSTEPS
     achieved = stage_bytes[roof_stage] / (st_ms / 1e3) / 1e9 if st_ms > 0 else 0.0
+    traffic = BROADPHASE_DRAM_BYTES.get(n) if roof_stage == "broadphase" else None
     roofline = {"bound": "hbm", "kernel": f"{roof_stage} stage (per substep)", "achieved": achieved,
                 "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
-                "traffic": None, "algorithmic_bytes": stage_bytes[roof_stage],
+                "traffic": traffic, "traffic_unit": "bytes per substep (ncu)",
+                "algorithmic_bytes": stage_bytes[roof_stage],
                 "step_algorithmic_GBps": step_bytes / (dev_ms / 1e3 / args.steps) / 1e9}
 
     cpu = None

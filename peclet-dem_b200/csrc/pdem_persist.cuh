@@ -333,149 +333,4 @@ __global__ void __launch_bounds__(kColorBlock) kColorBoth(Dev<R> d, ColorJob jm,
   colorStats(jc, gtid, gstride);
 }
 
-// ---------------------------------------------------------------------------------------------
-// Batched form: both colourings with ONE BLOCK PER SCENE (block barriers only). Scene s colours
-// its manifolds [manFirst[s], manFirst[s+1]) and its contacts (pair, plane and wall ranges of
-// sceneConFirst) over its own bodies [bodyFirst[s], bodyFirst[s+1]); rounds, winners, colours and
-// the stall rule are those of kColorBoth for each scene alone. Statistics go to the same aux slots.
-template <class R, bool MANIFOLD>
-__device__ __forceinline__ int sceneEntryRange(const Dev<R>& d, int s, int r, int& b, int& e) {
-  if (MANIFOLD) {
-    b = d.sceneManFirst[s], e = d.sceneManFirst[s + 1];
-    return r == 0 ? 1 : 0;
-  }
-  const int* F = d.sceneConFirst + r * (d.numScenes + 1);
-  b = F[s], e = F[s + 1];
-  return r < 3 ? 1 : 0;
-}
-template <class R, bool MANIFOLD>
-__device__ __forceinline__ int colorSceneRound(const Dev<R>& d, const ColorJob& J, int s, int round, int phase) {
-  long long* win = (round & 1) ? J.winB : J.winA;
-  long long* nxt = (round & 1) ? J.winA : J.winB;
-  int lost = 0;
-  for (int r = 0;; ++r) {
-    int b, e;
-    if (!sceneEntryRange<R, MANIFOLD>(d, s, r, b, e))
-      break;
-    for (int i = b + threadIdx.x; i < e; i += blockDim.x) {
-      if (J.col[i] != -1)
-        continue;
-      int ea, eb;
-      colorEnds<R, MANIFOLD>(d, i, ea, eb);
-      const long long k = entryKey<R, MANIFOLD>(d, i, ea);
-      if (phase == 0) {
-        atomicMax(&win[ea], k);
-        if (eb >= 0)
-          atomicMax(&win[eb], k);
-        continue;
-      }
-      if (win[ea] != k || (eb >= 0 && win[eb] != k)) {
-        ++lost;
-        nxt[ea] = -1;
-        if (eb >= 0)
-          nxt[eb] = -1;
-        continue;
-      }
-      u64 forb = J.mask[ea];
-      if (eb >= 0)
-        forb |= J.mask[eb];
-      int cc = 0;
-      while (cc < 62 && (forb & (1ull << cc)))
-        ++cc;
-      J.col[i] = cc;
-      J.mask[ea] |= 1ull << cc;
-      if (eb >= 0)
-        J.mask[eb] |= 1ull << cc;
-    }
-  }
-  return lost;
-}
-template <class R, bool MANIFOLD>
-__device__ __forceinline__ void colorSceneInit(const Dev<R>& d, const ColorJob& J, int s, int b0, int b1) {
-  for (int b = b0 + threadIdx.x; b < b1; b += blockDim.x) {
-    J.mask[b] = 0ull;
-    J.winA[b] = -1ll;
-  }
-  for (int r = 0;; ++r) {
-    int b, e;
-    if (!sceneEntryRange<R, MANIFOLD>(d, s, r, b, e))
-      break;
-    for (int i = b + threadIdx.x; i < e; i += blockDim.x) {
-      if (MANIFOLD) {
-        const int2 ab = d.mab[i];
-        J.col[i] = (d.mnp[i] <= 0 || (ab.y >= 0 && d.realIdx[ab.x] > d.realIdx[ab.y])) ? -2 : -1;
-      } else {
-        J.col[i] = -1;
-      }
-    }
-  }
-}
-template <class R, bool MANIFOLD>
-__device__ __forceinline__ void colorSceneStats(const Dev<R>& d, const ColorJob& J, int s) {
-  int mxc = INT_MIN, left = 0;
-  for (int r = 0;; ++r) {
-    int b, e;
-    if (!sceneEntryRange<R, MANIFOLD>(d, s, r, b, e))
-      break;
-    for (int i = b + threadIdx.x; i < e; i += blockDim.x) {
-      const int v = J.col[i];
-      mxc = v > mxc ? v : mxc;
-      left += (v == -1) ? 1 : 0;
-    }
-  }
-  if (mxc != INT_MIN)
-    atomicMax(&J.aux[3], mxc);
-  if (left)
-    atomicAdd(&J.aux[4], left);
-}
-
-template <class R>
-__global__ void __launch_bounds__(kSceneBlock) kColorScenes(Dev<R> d, ColorJob jm, ColorJob jc, const int* bodyFirst,
-                                                            int maxRounds) {
-  __shared__ int lost[2];
-  const int s = blockIdx.x;
-  const int b0 = bodyFirst[s], b1 = bodyFirst[s + 1];
-  if (jm.ne > 0)
-    colorSceneInit<R, true>(d, jm, s, b0, b1);
-  if (jc.ne > 0)
-    colorSceneInit<R, false>(d, jc, s, b0, b1);
-  __syncthreads();
-  int prevM = -1, prevC = -1;
-  bool doneM = jm.ne <= 0, doneC = jc.ne <= 0;
-  for (int round = 0; round < maxRounds && !(doneM && doneC); ++round) {
-    if (threadIdx.x == 0)
-      lost[0] = lost[1] = 0;
-    if (!doneM)
-      colorSceneRound<R, true>(d, jm, s, round, 0);
-    if (!doneC)
-      colorSceneRound<R, false>(d, jc, s, round, 0);
-    __syncthreads();
-    if (!doneM) {
-      const int l = colorSceneRound<R, true>(d, jm, s, round, 1);
-      if (l)
-        atomicAdd(&lost[0], l);
-    }
-    if (!doneC) {
-      const int l = colorSceneRound<R, false>(d, jc, s, round, 1);
-      if (l)
-        atomicAdd(&lost[1], l);
-    }
-    __syncthreads();
-    const int remM = lost[0], remC = lost[1];
-    if (!doneM) {
-      doneM = remM == 0 || remM == prevM;
-      prevM = remM;
-    }
-    if (!doneC) {
-      doneC = remC == 0 || remC == prevC;
-      prevC = remC;
-    }
-    __syncthreads();
-  }
-  if (jm.ne > 0)
-    colorSceneStats<R, true>(d, jm, s);
-  if (jc.ne > 0)
-    colorSceneStats<R, false>(d, jc, s);
-}
-
 }  // namespace pdem

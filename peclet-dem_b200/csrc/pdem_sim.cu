@@ -1045,14 +1045,7 @@ void Sim<R>::colorBoth(int nm, int nc, int& ncolV, int& velLeft, int& ncolP, int
   const ColorJob jc{neC, nbC, cColor_.p, winnerP_.p, winnerP2_.p, maskP_.p, colorAux_.p + 5};
   gbar_.ensure(2, false, stream_);
   const GridBar gb{gbar_.p, &ctr_.p->err};
-  if (batch_) {  // one block per scene; the statistics slots start cleared
-    const int aux[10] = {0, 0, 0, std::numeric_limits<int>::min(), 0, 0, 0, 0, std::numeric_limits<int>::min(), 0};
-    cudaCheck(cudaMemcpyAsync(colorAux_.p, aux, sizeof aux, cudaMemcpyHostToDevice, stream_), "H2D colour aux");
-    ++launches_, kColorScenes<R><<<numScenes_, kSceneBlock, 0, stream_>>>(d_, jm, jc, sceneFirstD_.p,
-                                                                         std::max(nbM, nbC) + 2);
-  } else {
-    launchCoopB(kColorBoth<R>, kColorBlock, d_, jm, jc, std::max(nbM, nbC) + 2, gb);
-  }
+  launchCoopB(kColorBoth<R>, kColorBlock, d_, jm, jc, std::max(nbM, nbC) + 2, gb);
   KCHECK("colour loop");
   int res[10], err = 0;
   cudaCheck(cudaMemcpyAsync(res, colorAux_.p, sizeof res, cudaMemcpyDeviceToHost, stream_), "D2H");
