@@ -111,10 +111,11 @@ def substep_bytes(n, P, C, M, iv, ip, D=8):
             + iv * M * (Sm + 53 * D) + ip * C * (8 + 48 * D))
 
 
-# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum over the stage's kernels, one ncu
-# capture of a refit-only substep) of the broadphase stage at the default workload of 262,144
-# spheres, in bytes per substep; other sizes report none
-BROADPHASE_DRAM_BYTES = {262144: 140.7e6}
+# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum summed over a stage's kernels in one
+# ncu capture of one substep) at the default workload of 262,144 spheres, in bytes per substep;
+# stages and sizes not captured report none. The colouring stage covers both colourings, the
+# contact colour order and the manifold incidence lists.
+STAGE_DRAM_BYTES = {(262144, "colour_velocity"): 26.7e6}
 
 
 def measured_peaks():
@@ -331,7 +332,6 @@ def run_ours(args):
 
     # ---- roofline of the dominant stage ----
     per_step = {k: (ms / args.steps, c / args.steps) for k, (ms, c) in stages.items() if c}
-    dominant = max(per_step, key=lambda k: per_step[k][0])
     peak, peak_kind = measured_peaks()
     P, C, M = counts["pairs"], counts["contacts"], counts["manifolds"]
     iv = sweeps["velocity"] / args.steps / SUBSTEPS if sweeps else 10
@@ -342,12 +342,15 @@ def run_ours(args):
         "broadphase": n * 4 * 8 + 8 * P,
         "narrowphase": 8 * P + C * (8 + 16 * 8),
         "manifolds": 2 * C * (8 + 16 * 8) + M * (12 + 20 * 8),
+        "colour_velocity": 12 * (M + C),
+        "ledger": M * (16 + 8 * 8),
     }
     step_bytes = substep_bytes(n, P, C, M, iv, ip) * SUBSTEPS
-    roof_stage = dominant if dominant in stage_bytes else "velocity"
+    # the dominant stage among those with a byte model (all the heavy ones)
+    roof_stage = max((k for k in per_step if k in stage_bytes), key=lambda k: per_step[k][0])
     st_ms = per_step[roof_stage][0] / SUBSTEPS
     achieved = stage_bytes[roof_stage] / (st_ms / 1e3) / 1e9 if st_ms > 0 else 0.0
-    traffic = BROADPHASE_DRAM_BYTES.get(n) if roof_stage == "broadphase" else None
+    traffic = STAGE_DRAM_BYTES.get((n, roof_stage))
     roofline = {"bound": "hbm", "kernel": f"{roof_stage} stage (per substep)", "achieved": achieved,
                 "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
                 "traffic": traffic, "traffic_unit": "bytes per substep (ncu)",

@@ -83,10 +83,10 @@ struct BvhNodes {
 };
 
 template <class R>
-__global__ void kBoxes(Dev<R> d, int n, R margin, R boxCap, BvhNodes<R> bn, BvhBuffers bb) {
+__global__ void kBoxes(Dev<R> d, int n, R margin, R boxCap, BvhNodes<R> bn, BvhBuffers bb, R extra = R(0)) {
   u64 lo[3] = {~0ull, ~0ull, ~0ull}, hi[3] = {0ull, 0ull, 0ull};
   GRID_STRIDE(i, n) {
-    const R mg = d.scn ? d.scn[d.sceneOf[i]].margin : margin;
+    const R mg = (d.scn ? d.scn[d.sceneOf[i]].margin : margin) + extra;
     const Box<R> b = saneBox(d, (int)i, d.posPred, mg, boxCap);
     bn.prim[i] = b;
     bool ok = true;
@@ -610,6 +610,40 @@ __global__ void kQueryFull(BvhBuffers bb, const Box<R>* prim, const PNode* nodes
     }
     if (!MODE)
       cnt[i] = c;
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Verlet superset. A candidate list built with every box widened by half a skin contains every
+// pair whose exact boxes overlap later, as long as no body moved more than half the skin (per
+// axis) since the build and no box size changed. Between rebuilds each substep filters that list
+// by the exact predicate on the current boxes; the filter keeps the list's canonical (i, j) order.
+
+// largest per-axis displacement since the build over all primitives; a primitive whose slot now
+// holds another body's image (or whose position is not finite) counts as infinitely far
+template <class R>
+__global__ void kVerletDisplacement(Dev<R> d, int n, const Q4<R>* ref, const int* refReal, R* out) {
+  R m = R(0);
+  GRID_STRIDE(i, n) {
+    const Q4<R> a = d.posPred[i], b = ref[i];
+    R v = fmax(fmax(fabs(a.x - b.x), fabs(a.y - b.y)), fabs(a.z - b.z));
+    if (!(v <= R(1e30)) || d.realIdx[i] != refReal[i])
+      v = R(1e30);
+    runMax(m, v);
+  }
+  warpMaxAtomic(out, m);
+}
+template <class R>
+__global__ void kFilterPairs(const int2* cand, int nc, const Box<R>* prim, int* keep) {
+  GRID_STRIDE(k, nc) {
+    const int2 p = cand[k];
+    keep[k] = boxOverlap(prim[p.x], prim[p.y]) ? 1 : 0;
+  }
+}
+static __global__ void kCompactPairs(const int2* cand, int nc, const int* keep, const int* off, int2* out, int cap) {
+  GRID_STRIDE(k, nc) {
+    if (keep[k] && off[k] < cap)
+      out[off[k]] = cand[k];
   }
 }
 

@@ -265,6 +265,7 @@ static int bitsFor(long maxValue) {
 // src/sim.hpp:949-1021
 template <class R>
 void Sim<R>::initializeShape(int type, R radius, R height, R thick) {
+  vValid_ = false;  // box sizes, parking or images may change
   baseRadius_ = radius;
   ShapeDesc<R> sd{};
   std::vector<ShellPoint> sh;
@@ -342,6 +343,7 @@ void Sim<R>::uploadShape() {
 }
 template <class R>
 void Sim<R>::setShellPoints(const std::vector<R>& p) {
+  vValid_ = false;  // box sizes, parking or images may change
   const int n = (int)(p.size() / 3);
   shellHost_.assign(std::max(n, 1), Q4<R>{0, 0, 0, 0});
   for (int i = 0; i < n; ++i)
@@ -358,6 +360,7 @@ void Sim<R>::setShellPoints(const std::vector<R>& p) {
 template <class R>
 void Sim<R>::setSdfShape(const std::vector<R>& grid, int nx, int ny, int nz, const R* origin, const R* spacing,
                          const std::vector<R>& shell, const R* invI, R bR) {
+  vValid_ = false;  // box sizes, parking or images may change
   if (nx < 2 || ny < 2 || nz < 2)
     throw std::runtime_error("setSdfShape: grid dims must be >= 2 on each axis");
   if ((long)nx * ny * nz != (long)grid.size())
@@ -387,6 +390,7 @@ void Sim<R>::setSdfShape(const std::vector<R>& grid, int nx, int ny, int nz, con
 }
 template <class R>
 void Sim<R>::setDomain(R lx, R ly, R lz, bool px, bool py, bool pz) {
+  vValid_ = false;  // box sizes, parking or images may change
   dmin_[0] = dmin_[1] = dmin_[2] = 0;
   dmax_[0] = dsize_[0] = lx;
   dmax_[1] = dsize_[1] = ly;
@@ -396,6 +400,7 @@ void Sim<R>::setDomain(R lx, R ly, R lz, bool px, bool py, bool pz) {
 }
 template <class R>
 void Sim<R>::setDomainMinMax(const R* mn, const R* mx) {
+  vValid_ = false;  // box sizes, parking or images may change
   for (int a = 0; a < 3; ++a) {
     dmin_[a] = mn[a];
     dmax_[a] = mx[a];
@@ -405,6 +410,7 @@ void Sim<R>::setDomainMinMax(const R* mn, const R* mx) {
 }
 template <class R>
 void Sim<R>::enablePeriodicity(bool x, bool y, bool z) {
+  vValid_ = false;  // box sizes, parking or images may change
   per_[0] = x, per_[1] = y, per_[2] = z;
 }
 template <class R>
@@ -564,6 +570,7 @@ void Sim<R>::setPositions(const R* xyz, int n) {
     batch_ = false;  // the scene layout described the previous particle set
   sceneParamsDirty_ = true;
   maxScaleValid_ = false;
+  vValid_ = false;
   bvhValid_ = false;
   numReal_ = n;
   numParticles_ = n;
@@ -659,6 +666,7 @@ template <class R>
 void Sim<R>::setScales(const R* s, int n) {  // src/sim.hpp:1340-1346
   sceneParamsDirty_ = true;
   maxScaleValid_ = false;
+  vValid_ = false;
   const int m = std::min(numReal_, n);
   if (m > 0)
     cudaCheck(cudaMemcpyAsync(target_.p, s, m * sizeof(R), cudaMemcpyHostToDevice, stream_), "H2D scales");
@@ -669,6 +677,7 @@ template <class R>
 void Sim<R>::setScalesUniform(R s) {  // src/sim.hpp:1331-1337
   sceneParamsDirty_ = true;
   maxScaleValid_ = false;
+  vValid_ = false;
   if (numReal_ > 0) {
     std::vector<R> h(numReal_, s);
     cudaCheck(cudaMemcpyAsync(scale_.p, h.data(), numReal_ * sizeof(R), cudaMemcpyHostToDevice, stream_), "H2D");
@@ -684,6 +693,7 @@ void Sim<R>::setGrowthParams(R rate, R nf) {  // src/sim.hpp:1416-1424
     gf_ = nf;
   gr_ = rate;
   maxScaleValid_ = false;
+  vValid_ = false;
   if (gf_ > R(0) && numReal_ > 0) {
     ++launches_, kGrowthScales<<<gridFor(numReal_), kBlock, 0, stream_>>>(d_, numReal_, gf_);
     KCHECK("growth");
@@ -783,7 +793,7 @@ void Sim<R>::resetGhosts(R band) {
 // broadphase over numParticles_ boxes of the predicted positions with margin; pairs into pairs_
 // (cap entries). Returns the number of candidates, which may exceed cap (nothing written then).
 template <class R>
-int Sim<R>::findCollisions(R margin, int cap) {
+int Sim<R>::findCollisions(R margin, int cap, int2* out, R extra) {
   const int n = numParticles_;
   const R boxCap = std::max(std::max(dsize_[0], dsize_[1]), dsize_[2]);
   if (n < 2 || numReal_ <= 0)
@@ -828,7 +838,7 @@ int Sim<R>::findCollisions(R margin, int cap) {
   const bool rebuild = !bvhValid_ || bvhN_ != n || bvhReal_ != numReal_ || bvhAge_ >= kBvhRebuild;
   const u64 init[6] = {~0ull, ~0ull, ~0ull, 0ull, 0ull, 0ull};
   cudaCheck(cudaMemcpyAsync(bounds_.p, init, sizeof init, cudaMemcpyHostToDevice, stream_), "H2D bounds");
-  ++launches_, kBoxes<<<gridFor(n), kBlock, 0, stream_>>>(d_, n, margin, boxCap, bn, bb);
+  ++launches_, kBoxes<<<gridFor(n), kBlock, 0, stream_>>>(d_, n, margin, boxCap, bn, bb, extra);
   KCHECK("boxes");
   if (rebuild) {
     ++launches_, kMorton<R><<<gridFor(n), kBlock, 0, stream_>>>(n, bn, bb);  // into codes_ / bidx_
@@ -890,15 +900,15 @@ int Sim<R>::findCollisions(R margin, int cap) {
       throw std::runtime_error("broadphase: BVH traversal exceeded its iteration bound (corrupt tree)");
     if (total <= cap) {
       ++launches_, kQueryFull<R, 1><<<gridFor(n, 128), 128, 0, stream_>>>(bb, prim, nodes, numReal_, nullptr,
-                                                                            qoff_.p, pairs_.p, cap);
+                                                                            qoff_.p, out, cap);
       KCHECK("query write");
     }
   } else if (total <= cap) {
-    ++launches_, kScatterHalf<<<gridFor(n), kBlock, 0, stream_>>>(bb, qcnt_.p, slots_.p, qoff_.p, pairs_.p, cap);
+    ++launches_, kScatterHalf<<<gridFor(n), kBlock, 0, stream_>>>(bb, qcnt_.p, slots_.p, qoff_.p, out, cap);
     KCHECK("pair scatter");
   }
   if (total <= cap) {
-    ++launches_, kSortPairLists<<<gridFor(numReal_), kBlock, 0, stream_>>>(numReal_, qoff_.p, pairs_.p, cap);
+    ++launches_, kSortPairLists<<<gridFor(numReal_), kBlock, 0, stream_>>>(numReal_, qoff_.p, out, cap);
     KCHECK("pair sort");
   }
   return total;
@@ -906,19 +916,93 @@ int Sim<R>::findCollisions(R margin, int cap) {
 // src/sim.hpp:82-94: grow the pair buffer and re-run when the candidates exceed it
 template <class R>
 int Sim<R>::findCollisionsGrow(R margin, const Q4<R>*) {
-  int np = findCollisions(margin, (int)pairs_.n);
+  int np = findCollisions(margin, (int)pairs_.n, pairs_.p);
   if (np > (int)pairs_.n) {
     const int grown = np + np / 2 + 64;
     pairs_.ensure(grown, false, stream_);
     maxPairs_ = grown;
     refreshDev();
-    np = findCollisions(margin, (int)pairs_.n);
+    np = findCollisions(margin, (int)pairs_.n, pairs_.p);
   }
   return std::min(np, (int)pairs_.n);
 }
+// The step's candidate pairs through a Verlet superset (see kVerletDisplacement): the exact list,
+// in canonical order, identical to findCollisionsGrow's. The superset is rebuilt (BVH query with
+// every box widened by half the skin) when the body set, the margin or a scale changed, or when
+// some body moved more than half the skin since the last build.
+template <class R>
+int Sim<R>::findCollisionsVerlet(R margin) {
+  const int n = numParticles_;
+  if (n < 2 || numReal_ <= 0)
+    return 0;
+  const R skin = R(0.5) * margin;
+  const R boxCap = std::max(std::max(dsize_[0], dsize_[1]), dsize_[2]);
+  // a widened box that the exact predicate would not park must not be parked either
+  if (boxCap > R(0) && maxOwnedRadius() + margin + R(0.5) * skin > boxCap)
+    return findCollisionsGrow(margin, posPred_.p);
+  bvhBoxes_.ensure(sizeof(Box<R>) * n, false, stream_);
+  bounds_.ensure(6, false, stream_);
+  rA_.ensure(1, false, stream_);
+  Box<R>* prim = reinterpret_cast<Box<R>*>(bvhBoxes_.p);
+  BvhNodes<R> bn{prim, nullptr};
+  BvhBuffers bb;
+  bb.n = n;
+  bb.bounds = bounds_.p;
+  bb.err = &ctr_.p->err;
+  const bool fresh = vValid_ && vN_ == n && vReal_ == numReal_ && vMargin_ == margin;
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    const bool useOld = fresh && attempt == 0;
+    if (!useOld) {
+      // (re)build the superset: BVH query with the widened boxes, into vpairs_ (grown on demand)
+      int nv = findCollisions(margin, (int)vpairs_.n, vpairs_.p, R(0.5) * skin);
+      if (nv > (int)vpairs_.n) {
+        vpairs_.ensure((size_t)nv + nv / 2 + 64, false, stream_);
+        nv = findCollisions(margin, (int)vpairs_.n, vpairs_.p, R(0.5) * skin);
+      }
+      vCount_ = nv;
+      vRef_.ensure(n, false, stream_);
+      vRefReal_.ensure(n, false, stream_);
+      cudaCheck(cudaMemcpyAsync(vRef_.p, posPred_.p, n * sizeof(Q4<R>), cudaMemcpyDeviceToDevice, stream_), "D2D");
+      cudaCheck(cudaMemcpyAsync(vRefReal_.p, realIdx_.p, n * sizeof(int), cudaMemcpyDeviceToDevice, stream_), "D2D");
+      vValid_ = true, vN_ = n, vReal_ = numReal_, vMargin_ = margin;
+    }
+    // exact boxes of this substep, displacement since the build, and the filter
+    const u64 init[6] = {~0ull, ~0ull, ~0ull, 0ull, 0ull, 0ull};
+    cudaCheck(cudaMemcpyAsync(bounds_.p, init, sizeof init, cudaMemcpyHostToDevice, stream_), "H2D bounds");
+    ++launches_, kBoxes<<<gridFor(n), kBlock, 0, stream_>>>(d_, n, margin, boxCap, bn, bb);
+    rA_.zero(stream_, 1);
+    ++launches_, kVerletDisplacement<<<gridFor(n), kBlock, 0, stream_>>>(d_, n, vRef_.p, vRefReal_.p, rA_.p);
+    const int nc = vCount_;
+    vKeep_.ensure((size_t)nc + 1, false, stream_);
+    vOff_.ensure((size_t)nc + 1, false, stream_);
+    if (nc > 0)
+      ++launches_, kFilterPairs<<<gridFor(nc), kBlock, 0, stream_>>>(vpairs_.p, nc, prim, vKeep_.p);
+    cudaCheck(cudaMemsetAsync(vKeep_.p + nc, 0, sizeof(int), stream_), "memset");
+    exclusiveSum(vKeep_.p, vOff_.p, nc + 1);
+    KCHECK("verlet filter");
+    int total = 0;
+    R disp = 0;
+    cudaCheck(cudaMemcpyAsync(&total, vOff_.p + nc, sizeof(int), cudaMemcpyDeviceToHost, stream_), "D2H");
+    cudaCheck(cudaMemcpyAsync(&disp, rA_.p, sizeof(R), cudaMemcpyDeviceToHost, stream_), "D2H");
+    sync();
+    if (useOld && !(disp <= R(0.5) * skin))
+      continue;  // some body left its widened box: rebuild and filter again
+    if (total > (int)pairs_.n) {
+      pairs_.ensure((size_t)total + total / 2 + 64, false, stream_);
+      maxPairs_ = (int)pairs_.n;
+      refreshDev();
+    }
+    if (nc > 0)
+      ++launches_, kCompactPairs<<<gridFor(nc), kBlock, 0, stream_>>>(vpairs_.p, nc, vKeep_.p, vOff_.p, pairs_.p,
+                                                                      (int)pairs_.n);
+    KCHECK("verlet compact");
+    return total;
+  }
+  throw std::runtime_error("broadphase: a freshly built candidate superset failed its own displacement check");
+}
 template <class R>
 void Sim<R>::detectAll(R margin) {
-  const int np = findCollisionsGrow(margin, posPred_.p);
+  const int np = verlet_ ? findCollisionsVerlet(margin) : findCollisionsGrow(margin, posPred_.p);
   mark(ST_NARROW);
   ++launches_, kResetCounters<<<1, 1, 0, stream_>>>(ctr_.p);
   NarrowP<R> P{margin, gs_, (int)planesHost_.size(), (int)wallsHost_.size(), pairMatHost_.empty() ? 0 : 1};
@@ -1141,6 +1225,7 @@ void Sim<R>::demStep() {
       gf_ = R(1);
   }
   if (gf_ > R(0) && numReal_ > 0) {
+    vValid_ = false;  // the radii change this substep
     ++launches_, kGrowthScales<<<gridFor(numReal_), B, 0, s>>>(d_, numReal_, gf_);
     KCHECK("growth");
   }
@@ -2009,6 +2094,7 @@ void Sim<R>::setScenes(int S, const int* first) {
       throw std::invalid_argument("set_scenes: scene ranges must be non-decreasing");
   ensureGrounded();  // the logged support graphs index the previous scene layout
   bvhValid_ = false;  // the tree's leaf order must put every scene in one subtree
+  vValid_ = false;
   numScenes_ = S;
   sceneFirstHost_.assign(first, first + S + 1);
   maxSceneBodies_ = 0;
@@ -2045,6 +2131,7 @@ void Sim<R>::setSceneMaterial(int scene, R e, R mu) {
   sceneMu_[scene] = mu;
   sceneParamsDirty_ = true;
   maxScaleValid_ = false;
+  vValid_ = false;
 }
 template <class R>
 void Sim<R>::setWallScene(int wall, int scene) {

@@ -80,7 +80,7 @@ class Sim {
   void setVelocityUseGS(bool b) { useGS_ = b; }
   void setStabilizationMode(const std::string& m);
   void setHertzMaterial(int mat, R E, R nu);
-  void setGlobalScale(R s) { gs_ = s, skin_ = R(0.1) * s; }
+  void setGlobalScale(R s) { gs_ = s, skin_ = R(0.1) * s, vValid_ = false; }
   void setDt(R dt) { dt_ = dt; }
   void setMaterialParams(R en, R et, R mu) { eN_ = en, eT_ = et, mu_ = mu; }
   void setMaterialIds(const int* ids, int n);
@@ -214,6 +214,13 @@ class Sim {
   static constexpr int kBvhRebuild = 16;
   bool bvhValid_ = false;
   int bvhN_ = 0, bvhReal_ = 0, bvhAge_ = 0;
+  // Verlet candidate superset (skin = half the contact margin): the step's pairs are filtered from it
+  bool verlet_ = true, vValid_ = false;
+  int vN_ = 0, vReal_ = 0, vCount_ = 0;
+  R vMargin_ = R(0);
+  DBuf<int2> vpairs_;
+  DBuf<Q4<R>> vRef_;
+  DBuf<int> vRefReal_, vKeep_, vOff_;
   R maxScaleHost_ = R(0);
   int numScenes_ = 1, maxSceneBodies_ = 0;
   std::vector<int> sceneFirstHost_;   // [S + 1] first body of each scene
@@ -291,7 +298,8 @@ class Sim {
   R maxOwnedRadius();
   void resetGhosts(R band);
   int findCollisionsGrow(R margin, const Q4<R>* P);
-  int findCollisions(R margin, int cap);
+  int findCollisions(R margin, int cap, int2* out, R extra = R(0));
+  int findCollisionsVerlet(R margin);
   void detectAll(R margin);
   int reduceManifolds(int nc);
   void colorBoth(int nm, int nc, int& ncolV, int& velLeft, int& ncolP, int& posLeft);
