@@ -9,8 +9,9 @@ density 2500 kg/m^3, e = 0.6, mu = 0.4, gravity -9.81 m/s^2, dt = 2e-5 s split i
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-`value` is device time (CUDA events on the library's stream, summed over the step's stages) with
-the state resident in HBM; `e2e` runs the same loop through the public API with host buffers
+`value` is device time (two CUDA events on the library's stream around all timed substeps, idle
+gaps included; a second pass with per-stage events gives the stage breakdown) with the state
+resident in HBM; `e2e` runs the same loop through the public API with host buffers
 (external forces copied in, positions and velocities copied out every outer step) timed by the
 host clock. `--impl reference` times the reference's own code (its headers built against the
 OpenMP flavour of the Kokkos shim) on this machine's host cores. More than one GPU runs replicas
@@ -176,14 +177,17 @@ def run_batched(args, rank, world, dist, dem):
             sim.step(dt)
         if dist is not None:
             dist.barrier()
+        sim.timer_start()
+        for _ in range(args.steps * SUBSTEPS):
+            sim.step(dt)
+        t = max_over_ranks(sim.timer_stop() / 1e3, dist, "cuda")
+        sweeps = sim.scene_counters()
+        x = sim.get_positions()  # the error is measured at the end of the timed substeps
         sim.profile_enable(True)
         for _ in range(args.steps * SUBSTEPS):
             sim.step(dt)
         stages, launches = sim.profile_read()
         sim.profile_enable(False)
-        t = max_over_ranks(sum(ms for ms, _ in stages.values()) / 1e3, dist, "cuda")
-        sweeps = sim.scene_counters()
-        x = sim.get_positions()
         sim.close()
         per_step = {k: round(ms / args.steps, 3) for k, (ms, c) in stages.items() if c}
         return t, per_step, launches, sweeps, x
@@ -291,19 +295,26 @@ def run_ours(args):
     with clocks:
         time.sleep(0.5)  # sampler running before the timed region starts
         barrier()
-        sim.profile_enable(True)
         timed_allocs = dem._API.fn["debug_allocs"]()
         t0 = time.perf_counter()
+        sim.timer_start()  # events on the library's stream around the whole timed region
         for _ in range(args.steps):
             for _ in range(SUBSTEPS):
                 sim.step(scene.dt)
+        dev_ms = sim.timer_stop()
         wall = time.perf_counter() - t0
         timed_allocs = dem._API.fn["debug_allocs"]() - timed_allocs
-    stages, launches = sim.profile_read()
     barrier()
-    dev_ms = sum(ms for ms, _ in stages.values())
+    # the same number of steps again with per-stage events (their synchronisation per substep
+    # slows the step; these figures explain the timed value, they are not it)
+    sim.profile_enable(True)
+    for _ in range(args.steps):
+        for _ in range(SUBSTEPS):
+            sim.step(scene.dt)
+    stages, launches = sim.profile_read()
     counts = sim.debug_counts()
     sweeps = sim.debug_sweeps() if hasattr(sim, "debug_sweeps") else None
+    reuse = sim.debug_reuse()
     sim.profile_enable(False)
     # max over ranks of the device time; value = all ranks' particle-substeps / that time
     t_max = max_over_ranks(dev_ms / 1e3, dist, "cuda")
@@ -376,7 +387,7 @@ def run_ours(args):
             "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu,
             "clocks": clocks.summary(), "wall_ms_per_step": 1e3 * wall / args.steps,
             "stages_ms_per_step": {k: round(v[0], 4) for k, v in per_step.items()},
-            "counts_last_substep": counts, "sweeps": sweeps, "batched": batched,
+            "counts_last_substep": counts, "sweeps": sweeps, "topology_kept": reuse, "batched": batched,
             "device_allocations_timed": int(timed_allocs),
         }
         print(json.dumps(line))

@@ -183,6 +183,14 @@ long pdem_scene_counters(pdem_handle h, double* out, long cap);
  * hertz_rebuild, hertz_integrate */
 int pdem_profile_enable(pdem_handle h, int on);
 int pdem_profile_read(pdem_handle h, double* ms, long* calls, int cap, long* launches);
+/* device-timeline interval: timer_start records an event on the simulation's stream, timer_stop
+ * records another, waits for it and returns the milliseconds between them (everything the stream
+ * ran, and any idle time, in between) */
+int pdem_timer_start(pdem_handle h);
+int pdem_timer_stop(pdem_handle h, double* ms);
+/* substeps since profile_enable that kept the previous substep's manifold grouping, contact
+ * colours and manifold colours (their lists were unchanged) */
+int pdem_debug_reuse(pdem_handle h, long* out3);
 /* device allocations made by this library's growable buffers since it was loaded */
 long pdem_debug_allocs(void);
 /* sweeps executed since profile_enable: velocity, stabilization, position; and substeps */

@@ -490,6 +490,9 @@ long pdem_scene_counters(pdem_handle h, double* out, long cap) {
 }
 
 // ---- instrumentation ----
+int pdem_timer_start(pdem_handle h) { BODY(S.timerStart()); }
+int pdem_debug_reuse(pdem_handle h, long* out3) { BODY(for (int i = 0; i < 3; ++i) out3[i] = S.reuse_[i]); }
+int pdem_timer_stop(pdem_handle h, double* ms) { BODY(*ms = S.timerStop()); }
 long pdem_debug_allocs(void) { return pdem::gDeviceAllocs; }
 int pdem_debug_sweeps(pdem_handle h, long* out4) {
   BODY(for (int i = 0; i < 4; ++i) out4[i] = S.sweeps_[i]);

@@ -726,6 +726,30 @@ __global__ void kColorSortKeysScenes(Dev<R> d, int ne, const int* col, unsigned*
     vals[i] = (int)i;
   }
 }
+// Topology reuse. The colourings, colour orders, manifold grouping, incidence lists and ledger
+// order are functions of the contact list's body pairs (and, for the manifold side, of each
+// manifold's real ends and whether it is active). When those equal the previous substep's, the
+// products of that substep are still exact and are kept. These kernels compare and record.
+__global__ void kSameInt2(const int2* cur, int2* prev, int n, int* differ) {
+  GRID_STRIDE(i, n) {
+    const int2 a = cur[i], b = prev[i];
+    if (a.x != b.x || a.y != b.y)
+      *differ = 1;
+    prev[i] = a;
+  }
+}
+template <class R>
+__global__ void kSameManifolds(Dev<R> d, int nm, int4* prev, int* differ) {
+  GRID_STRIDE(i, nm) {
+    const int2 ab = d.mab[i];
+    const int ra = d.realIdx[ab.x], rb = ab.y >= 0 ? d.realIdx[ab.y] : -1;
+    const int init = (d.mnp[i] <= 0 || (ab.y >= 0 && ra > rb)) ? -2 : -1;
+    const int4 sig = make_int4(ra, rb, init, 0), old = prev[i];
+    if (sig.x != old.x || sig.y != old.y || sig.z != old.z)
+      *differ = 1;
+    prev[i] = sig;
+  }
+}
 // colour keys for the stable colour-sorted execution order
 __global__ void kColorSortKeys(int ne, const int* col, unsigned* keys, int* vals) {
   GRID_STRIDE(i, ne) {

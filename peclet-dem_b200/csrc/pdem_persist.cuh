@@ -202,6 +202,8 @@ struct ColorJob {
 
 template <class R, bool MANIFOLD>
 __device__ __forceinline__ void colorInit(const Dev<R>& d, const ColorJob& J, long gtid, long gstride) {
+  if (J.ne <= 0)
+    return;  // a kept (or empty) graph: its colours and statistics stay as they are
   for (long b = gtid; b < J.nb; b += gstride) {
     J.mask[b] = 0ull;
     J.winA[b] = -1ll;
@@ -295,10 +297,18 @@ __device__ __forceinline__ void colorStats(const ColorJob& J, long gtid, long gs
 }
 
 // job 0: manifolds over real bodies (skipped when ne = 0), job 1: contacts over body slots
+// reuse: a graph equal to the previous substep's keeps its colours and statistics (differ[0]: the
+// contact list changed, differ[1]: the manifold list changed; reuse = 0 forces both colourings)
 template <class R>
 __global__ void __launch_bounds__(kColorBlock) kColorBoth(Dev<R> d, ColorJob jm, ColorJob jc, int maxRounds,
-                                                          GridBar gb) {
+                                                          GridBar gb, const int* differ, int reuse) {
   const long gtid = (long)blockIdx.x * blockDim.x + threadIdx.x, gstride = (long)gridDim.x * blockDim.x;
+  if (reuse && !differ[1])
+    jm.ne = 0;  // uniform over the grid: the flags are written before the launch
+  if (reuse && !differ[0])
+    jc.ne = 0;
+  if (jm.ne <= 0 && jc.ne <= 0)
+    return;
   colorInit<R, true>(d, jm, gtid, gstride);
   colorInit<R, false>(d, jc, gtid, gstride);
   if (!gridBarrier(gb))

@@ -20,6 +20,7 @@
 namespace pdem {
 
 long gDeviceAllocs = 0;
+static const int kOne = 1;  // H2D source of a device flag set from the host
 
 void cudaCheck(cudaError_t e, const char* what) {
   if (e != cudaSuccess)
@@ -54,6 +55,10 @@ Sim<R>::~Sim() {
     cudaStreamSynchronize(stream_);
     cudaStreamDestroy(stream_);
   }
+  if (tStart_) {
+    cudaEventDestroy(tStart_);
+    cudaEventDestroy(tStop_);
+  }
 }
 
 // src/particles.hpp:194-288
@@ -85,6 +90,7 @@ void Sim<R>::allocate(int cap, int mp, int mc) {
 }
 template <class R>
 void Sim<R>::allocContactBuffers(int mc) {
+  topoValid_ = false;
   maxContacts_ = mc;
   cab_.ensure(mc, false, stream_);
   for (auto* b : {&cn_, &crA_, &crB_, &cbv_})
@@ -105,6 +111,7 @@ void Sim<R>::allocContactBuffers(int mc) {
 // src/particles.hpp:297-327 (matId grown too; the reference keeps it at the construction size)
 template <class R>
 void Sim<R>::ensureCapacity(int nc) {
+  topoValid_ = false;
   if (nc <= capacity_)
     return;
   for (auto* b : {&pos_, &vel_, &angVel_, &invI_, &posPred_, &velPred_, &angVelPred_, &quat_, &quatPred_,
@@ -572,6 +579,7 @@ void Sim<R>::setPositions(const R* xyz, int n) {
   maxScaleValid_ = false;
   vValid_ = false;
   bvhValid_ = false;
+  topoValid_ = false;
   numReal_ = n;
   numParticles_ = n;
   hzNumPairs_ = -1;
@@ -1077,6 +1085,20 @@ void Sim<R>::detectAll(R margin) {
   detectCounters_ = c;
   cudaCheck(cudaMemcpyAsync(ctr_.p, &detectCounters_, sizeof(Counters<R>), cudaMemcpyHostToDevice, stream_),
             "H2D counters");
+  // topology reuse: does this contact list equal the previous one? (recorded for the next substep)
+  const int ncs = c.contactCount;
+  topoFlags_.ensure(2, false, stream_);
+  const int differ0 = (ncs != prevNc_ || numParticles_ != prevNb_) ? 1 : 0;
+  cudaCheck(cudaMemsetAsync(topoFlags_.p, 0, 2 * sizeof(int), stream_), "memset");
+  if (differ0)
+    cudaCheck(cudaMemcpyAsync(topoFlags_.p, &kOne, sizeof(int), cudaMemcpyHostToDevice, stream_), "H2D");
+  if (ncs > 0) {
+    prevCab_.ensure(ncs, true, stream_);
+    ++launches_, kSameInt2<<<gridFor(ncs), kBlock, 0, stream_>>>(cab_.p, prevCab_.p, ncs, topoFlags_.p);
+    KCHECK("same contacts");
+  }
+  prevNc_ = ncs;
+  prevNb_ = numParticles_;
 }
 
 // src/contact_preprocessing.hpp:378-471
@@ -1084,6 +1106,26 @@ template <class R>
 int Sim<R>::reduceManifolds(int nc) {
   if (nc <= 0)
     return 0;
+  const int kb = bitsFor((long)numParticles_ + 1);
+  // the grouping (sorted keys, permutation, segments, manifold count) depends on the contact
+  // list's body pairs only: unchanged list -> keep it. The check costs a read-back, so it is made
+  // after a substep whose list was unchanged, and every 4th substep otherwise.
+  if (topoValid_ && nc == prevNcM_ && (lastSame_ || (topoChecks_++ & 3) == 0)) {
+    int differ = 1;
+    cudaCheck(cudaMemcpyAsync(&differ, topoFlags_.p, sizeof(int), cudaMemcpyDeviceToHost, stream_), "D2H");
+    sync();
+    lastSame_ = differ == 0;
+    if (lastSame_) {
+      ++reuse_[0];
+      const int nm = prevNm_;
+      ++launches_, kReduceManifolds<<<gridFor(nm), kBlock, 0, stream_>>>(d_, nm, nc, kb, segStart_.p, ckeysS_.p,
+                                                                          cperm_.p);
+      KCHECK("reduce manifolds");
+      return nm;
+    }
+  } else {
+    lastSame_ = false;
+  }
   ckeys_.ensure(nc, false, stream_);
   ckeysS_.ensure(nc, false, stream_);
   cpermIn_.ensure(nc, false, stream_);
@@ -1091,7 +1133,6 @@ int Sim<R>::reduceManifolds(int nc) {
   head_.ensure(nc, false, stream_);
   headScan_.ensure(nc, false, stream_);
   segStart_.ensure(nc + 1, false, stream_);
-  const int kb = bitsFor((long)numParticles_ + 1);
   ++launches_, kContactKeys<R><<<gridFor(nc), kBlock, 0, stream_>>>(d_, nc, kb, ckeys_.p, cpermIn_.p);
   KCHECK("contact keys");
   sortPairs(ckeys_.p, ckeysS_.p, cpermIn_.p, cperm_.p, nc, 2 * kb);
@@ -1105,6 +1146,8 @@ int Sim<R>::reduceManifolds(int nc) {
   KCHECK("seg starts");
   ++launches_, kReduceManifolds<<<gridFor(nm), kBlock, 0, stream_>>>(d_, nm, nc, kb, segStart_.p, ckeysS_.p, cperm_.p);
   KCHECK("reduce manifolds");
+  prevNm_ = nm;
+  prevNcM_ = nc;
   return nm;
 }
 
@@ -1129,12 +1172,18 @@ void Sim<R>::colorBoth(int nm, int nc, int& ncolV, int& velLeft, int& ncolP, int
   const ColorJob jc{neC, nbC, cColor_.p, winnerP_.p, winnerP2_.p, maskP_.p, colorAux_.p + 5};
   gbar_.ensure(2, false, stream_);
   const GridBar gb{gbar_.p, &ctr_.p->err};
-  launchCoopB(kColorBoth<R>, kColorBlock, d_, jm, jc, std::max(nbM, nbC) + 2, gb);
+  launchCoopB(kColorBoth<R>, kColorBlock, d_, jm, jc, std::max(nbM, nbC) + 2, gb, (const int*)topoFlags_.p,
+              topoValid_ ? 1 : 0);
   KCHECK("colour loop");
-  int res[10], err = 0;
+  int res[10], err = 0, differ[2] = {1, 1};
   cudaCheck(cudaMemcpyAsync(res, colorAux_.p, sizeof res, cudaMemcpyDeviceToHost, stream_), "D2H");
   cudaCheck(cudaMemcpyAsync(&err, &ctr_.p->err, sizeof err, cudaMemcpyDeviceToHost, stream_), "D2H");
+  cudaCheck(cudaMemcpyAsync(differ, topoFlags_.p, sizeof differ, cudaMemcpyDeviceToHost, stream_), "D2H");
   sync();
+  keptC_ = topoValid_ && differ[0] == 0;
+  keptM_ = topoValid_ && differ[1] == 0;
+  reuse_[1] += keptC_ ? 1 : 0;
+  reuse_[2] += keptM_ ? 1 : 0;
   if (err & kErrBarrier)
     throw CudaError("colouring: a grid-wide barrier timed out");
   if (neM > 0) {
@@ -1179,6 +1228,8 @@ void Sim<R>::colorOrder(bool manifold, int ne, int ncol) {
 // 1: contacts x real bodies, 2: contacts x raw body slots
 template <class R>
 void Sim<R>::buildIncidence(int kind, int ne, int nb) {
+  incKind_ = kind;
+  incNe_ = ne;
   const int n2 = 2 * ne;
   incKeys_.ensure(std::max(n2, 1), false, stream_);
   incKeysS_.ensure(std::max(n2, 1), false, stream_);
@@ -1250,6 +1301,15 @@ void Sim<R>::demStep() {
   const int nm = reduceManifolds(nc);
   if (batch_)
     batchBounds(nm);
+  // topology reuse, manifold side: real ends and activity of every manifold vs the previous substep
+  if (nm != prevNmSig_)
+    cudaCheck(cudaMemcpyAsync(topoFlags_.p + 1, &kOne, sizeof(int), cudaMemcpyHostToDevice, s), "H2D");
+  if (nm > 0) {
+    prevMsig_.ensure(nm, true, s);
+    ++launches_, kSameManifolds<<<gridFor(nm), B, 0, s>>>(d_, nm, prevMsig_.p, topoFlags_.p + 1);
+    KCHECK("same manifolds");
+  }
+  prevNmSig_ = nm;
   c0.manifoldCount = nm;
   c0.velDone = c0.stabRun = c0.stabDone = c0.posDone = 0;
   cudaCheck(cudaMemcpyAsync(ctr_.p, &c0, sizeof c0, cudaMemcpyHostToDevice, s), "H2D counters");
@@ -1268,19 +1328,21 @@ void Sim<R>::demStep() {
   mark(ST_COLOR_V);
   // both colourings now: the contact graph is fixed since the narrowphase
   int velLeft = 0, posLeft = 0, ncolV = 0, ncolP = 0;
+  keptM_ = keptC_ = false;
   if (useGS_)
     colorBoth(nm, nc, ncolV, velLeft, ncolP, posLeft);
   if (batch_ && (velLeft > 0 || posLeft > 0))
     throw std::runtime_error("batched scenes: uncoloured entries (Jacobi fallback) are not supported");
-  if (useGS_ && ncolV > 0)
+  // an unchanged graph keeps its colours, hence its colour order
+  if (useGS_ && ncolV > 0 && !keptM_)
     colorOrder(true, nm, ncolV);
-  if (useGS_ && ncolP > 0)
+  if (useGS_ && ncolP > 0 && !keptC_)
     colorOrder(false, nc, ncolP);
   const bool usePGS = gNZ && useGS_;
   const R gMag = std::sqrt(g_[0] * g_[0] + g_[1] * g_[1] + g_[2] * g_[2]);
   const V3<R> gHat = gNZ ? V3<R>{g_[0] / gMag, g_[1] / gMag, g_[2] / gMag} : V3<R>{0, 0, 0};
   const bool needInc = (usePGS && nm > 0) || ((velLeft > 0 || !useGS_) && nm > 0);
-  if (needInc)
+  if (needInc && !(keptM_ && incKind_ == 0 && incNe_ == nm))
     buildIncidence(0, nm, numReal_);
   Incidence incM{incOff_.p, incValsS_.p};
   mark(ST_WARM);
@@ -1411,8 +1473,10 @@ void Sim<R>::demStep() {
       lperm_.ensure(nm, false, s);
       const int kb = bitsFor((long)numParticles_ + 1);
       lkeysIn_.ensure(nm, false, s);
-      ++launches_, kLedgerKeys<<<gridFor(nm), B, 0, s>>>(nm, kb, pairKeys_.p, lkeysIn_.p, lpermIn_.p);
-      sortPairs(lkeysIn_.p, lkeysS_.p, lpermIn_.p, lperm_.p, nm, 2 * kb);
+      if (!keptM_) {  // the ledger order depends on the manifolds' real keys only
+        ++launches_, kLedgerKeys<<<gridFor(nm), B, 0, s>>>(nm, kb, pairKeys_.p, lkeysIn_.p, lpermIn_.p);
+        sortPairs(lkeysIn_.p, lkeysS_.p, lpermIn_.p, lperm_.p, nm, 2 * kb);
+      }
       ++launches_, kCommitLedger<<<gridFor(nm), B, 0, s>>>(d_, nm, lperm_.p);
       KCHECK("commit ledger");
     }
@@ -1537,12 +1601,16 @@ void Sim<R>::demStep() {
     sweeps_[2] += cc.posSweeps;
     sweeps_[3] += 1;
   }
-  sync();
+  // the colourings, orders and groupings of this substep are now the reference for the next one
+  topoValid_ = useGS_;
+  // no final synchronisation: the next call's launches queue behind this substep on the stream,
+  // and every getter synchronises before it reads
 }
 
 // src/sim.hpp:494-541
 template <class R>
 R Sim<R>::computeOverlaps() {
+  topoValid_ = false;  // detectAll records a contact list that no colouring follows
   if (batch_)
     batchBegin();
   const R maxRad = maxOwnedRadius();
@@ -1707,6 +1775,7 @@ long Sim<R>::getPosLambda(double* out, long cap) {
 // test hook: shrink (or grow) the contact capacity, as replacing the reference's contact View
 template <class R>
 void Sim<R>::setMaxContacts(int n) {
+  topoValid_ = false;
   if ((size_t)n > cab_.n)
     allocContactBuffers(n);
   maxContacts_ = n;
@@ -1793,6 +1862,7 @@ int Sim<R>::hertzWallCandidates(R skin) {
 template <class R>
 void Sim<R>::stepHertz(R dt, int nsteps, R skinFrac) {
   dt_ = dt;
+  topoValid_ = false;
   if (batch_)
     throw std::runtime_error("step_hertz: not supported for batched scenes");
   if (mixed_)
@@ -1980,6 +2050,7 @@ void Sim<R>::ensureGrounded() {
 // ---- instrumentation ----
 template <class R>
 void Sim<R>::profileEnable(bool on) {
+  reuse_[0] = reuse_[1] = reuse_[2] = 0;
   prof_ = on;
   for (int i = 0; i < ST_COUNT; ++i) {
     stageMs_[i] = 0;
@@ -2002,6 +2073,24 @@ void Sim<R>::mark(int stage) {
   }
   cudaCheck(cudaEventRecord(e, stream_), "cudaEventRecord");
   marks_.push_back({stage, e});
+}
+template <class R>
+void Sim<R>::timerStart() {
+  if (!tStart_) {
+    cudaCheck(cudaEventCreate(&tStart_), "cudaEventCreate");
+    cudaCheck(cudaEventCreate(&tStop_), "cudaEventCreate");
+  }
+  cudaCheck(cudaEventRecord(tStart_, stream_), "cudaEventRecord");
+}
+template <class R>
+double Sim<R>::timerStop() {
+  if (!tStart_)
+    return 0.0;
+  cudaCheck(cudaEventRecord(tStop_, stream_), "cudaEventRecord");
+  cudaCheck(cudaEventSynchronize(tStop_), "cudaEventSynchronize");
+  float ms = 0;
+  cudaCheck(cudaEventElapsedTime(&ms, tStart_, tStop_), "cudaEventElapsedTime");
+  return ms;
 }
 template <class R>
 void Sim<R>::flushMarks() {
@@ -2094,6 +2183,7 @@ void Sim<R>::setScenes(int S, const int* first) {
       throw std::invalid_argument("set_scenes: scene ranges must be non-decreasing");
   ensureGrounded();  // the logged support graphs index the previous scene layout
   bvhValid_ = false;  // the tree's leaf order must put every scene in one subtree
+  topoValid_ = false;
   vValid_ = false;
   numScenes_ = S;
   sceneFirstHost_.assign(first, first + S + 1);

@@ -77,7 +77,7 @@ class Sim {
   void setGravity(R gx, R gy, R gz) { g_[0] = gx, g_[1] = gy, g_[2] = gz; }
   void setThermostat(R T, R tau, R kB) { thT_ = T, thTau_ = tau, thKB_ = kB; }
   void setSolverIterations(int pos, int vel) { posIters_ = pos, velIters_ = vel; }
-  void setVelocityUseGS(bool b) { useGS_ = b; }
+  void setVelocityUseGS(bool b) { useGS_ = b, topoValid_ = false; }
   void setStabilizationMode(const std::string& m);
   void setHertzMaterial(int mat, R E, R nu);
   void setGlobalScale(R s) { gs_ = s, skin_ = R(0.1) * s, vValid_ = false; }
@@ -171,10 +171,15 @@ class Sim {
   };
   long launches_ = 0;
   long sweeps_[4] = {0, 0, 0, 0};  // velocity, stabilization, position sweeps; substeps (profiled)
+  long reuse_[3] = {0, 0, 0};      // substeps that kept: manifold grouping, contact colours, manifold colours
   bool prof_ = false;
   double stageMs_[ST_COUNT] = {};
   long stageCalls_[ST_COUNT] = {};
   void profileEnable(bool on);
+  // device-timeline interval between two calls (events on the library's stream; stop synchronises)
+  void timerStart();
+  double timerStop();
+  cudaEvent_t tStart_ = nullptr, tStop_ = nullptr;
   void mark(int stage);
   void flushMarks();
 
@@ -215,6 +220,13 @@ class Sim {
   bool bvhValid_ = false;
   int bvhN_ = 0, bvhReal_ = 0, bvhAge_ = 0;
   // Verlet candidate superset (skin = half the contact margin): the step's pairs are filtered from it
+  // topology reuse (contact list / manifold list equal to the previous substep's)
+  DBuf<int2> prevCab_;
+  DBuf<int4> prevMsig_;
+  DBuf<int> topoFlags_;  // [0] the contact list differs, [1] the manifold list differs
+  int prevNc_ = -1, prevNb_ = -1, prevNcM_ = -1, prevNm_ = 0, prevNmSig_ = -1, topoChecks_ = 0;
+  int incKind_ = -1, incNe_ = -1;  // what the incidence buffers hold
+  bool topoValid_ = false, lastSame_ = false, keptM_ = false, keptC_ = false;
   bool verlet_ = true, vValid_ = false;
   int vN_ = 0, vReal_ = 0, vCount_ = 0;
   R vMargin_ = R(0);

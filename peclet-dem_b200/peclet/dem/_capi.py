@@ -106,6 +106,9 @@ _SIGS = {
     "profile_read": (C.c_int, [_vp, _dbl_p, _long_p, C.c_int, _long_p]),
     "debug_sweeps": (C.c_int, [_vp, _long_p]),
     "debug_allocs": (C.c_long, []),
+    "timer_start": (C.c_int, [_vp]),
+    "debug_reuse": (C.c_int, [_vp, _long_p]),
+    "timer_stop": (C.c_int, [_vp, _dbl_p]),
     # batched form
     "set_scenes": (C.c_int, [_vp, C.c_int, _int_p]),
     "set_scene_material": (C.c_int, [_vp, C.c_int, C.c_double, C.c_double]),
@@ -311,6 +314,22 @@ class CApiSimulation:
                           center=(0.0, 0.0, 0.0)):
         a, b, c = _vec3(lin_vel), _vec3(ang_vel), _vec3(center)
         self._call("set_wall_velocity", int(wall_index), _ptr(a), _ptr(b), _ptr(c))
+
+    # ---- device-timeline timer (no reference counterpart) ------------------------------------------
+    def timer_start(self):
+        self._call("timer_start")
+
+    def debug_reuse(self):
+        """Substeps (since profile_enable) that kept: the manifold grouping, the contact colours,
+        the manifold colours."""
+        out = np.zeros(3, dtype=np.int64)
+        self._call("debug_reuse", out.ctypes.data_as(_long_p))
+        return {"grouping": int(out[0]), "contact_colours": int(out[1]), "manifold_colours": int(out[2])}
+
+    def timer_stop(self):
+        v = C.c_double(0.0)
+        self._call("timer_stop", C.byref(v))
+        return v.value
 
     # ---- batched form (no reference counterpart) -------------------------------------------------
     def set_scenes(self, first_body):
