@@ -211,6 +211,112 @@ def run_batched(args, rank, world, dist, dem):
                       "lower half, radii U[0.8,1.2] mm, mu U[0.2,0.8], e U[0.3,0.9], dt 5e-5 s / 10 substeps"}
 
 
+def run_calibration(args, rank, world, dist):
+    """Differentiable calibration: boxes of 2048 spheres (r 1 mm, 40 x 40 x 80 mm, six planes),
+    2000 Hertz substeps of 2e-5 s with checkpoints every 100, loss = mean squared distance of the
+    final positions to targets made by the same solver at hidden (E, e, mu) = (5e6, 0.7, 0.35);
+    gradients with respect to (E, e, mu) and the initial velocities from the adjoint, at the guess
+    (4e6, 0.6, 0.3). Scenes are split over ranks; the three material gradients are summed over
+    ranks with one all-reduce per backward pass. Reports forward-only and forward+adjoint rates
+    (device time, max over ranks), their cost ratio, the gradients' relative error against
+    central finite differences (relative step 1e-4, FP64) and the FP32 gradients' error against
+    FP64. Returns the sub-object of the JSON line."""
+    import torch
+    from peclet.dem import workloads as W
+    from peclet.dem.adjoint import HertzSpheres
+    per = 2048
+    c = W.calibration_boxes(scenes=args.calib_scenes)
+    lo, hi = (args.calib_scenes * rank) // world, (args.calib_scenes * (rank + 1)) // world
+    sl = slice(lo * per, hi * per)
+    n_all, n = args.calib_scenes * per, (hi - lo) * per
+    steps, ck, dt = args.calib_substeps, 100, 2e-5
+    hidden, guess = (5e6, 0.7, 0.35), (4e6, 0.6, 0.3)
+    dev = torch.device("cuda", torch.cuda.current_device())
+
+    def make(prec):
+        return HertzSpheres(c["r"][sl], c["m"][sl], c["I"][sl], np.arange(hi - lo + 1) * per, c["planes"], 0.3, dt,
+                            (0.0, 0.0, -9.81), prec, ck)
+
+    def timed(fn):
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        out = fn()
+        b.record()
+        torch.cuda.synchronize()
+        return out, max_over_ranks(a.elapsed_time(b) / 1e3, dist, "cuda")
+
+    x0 = torch.as_tensor(c["x0"][sl], device=dev)
+    v0 = torch.as_tensor(c["v0"][sl], device=dev)
+    w0 = torch.as_tensor(c["w0"][sl], device=dev)
+    s64 = make("fp64")
+    (xt, _, _), _ = s64.run(x0, v0, w0, hidden, steps)
+
+    def loss_of(sim, theta, vv=None):
+        (x, _, _), _ = sim.run(x0, v0 if vv is None else vv, w0, theta, steps)
+        part = ((x.double() - xt) ** 2).sum()
+        if dist is not None:
+            dist.all_reduce(part)
+        return float(part) / n_all
+
+    def fwd_adj(sim, nsteps=steps):
+        th = torch.tensor(guess, dtype=torch.float64, requires_grad=True)
+        vr = v0.to(sim.dtype).clone().requires_grad_(True)
+        x, _, _ = sim.rollout(x0.to(sim.dtype), vr, w0.to(sim.dtype), th, nsteps)
+        loss = ((x.double() - xt) ** 2).sum() / n_all
+        loss.backward()
+        g = th.grad.to(dev)
+        if dist is not None:
+            dist.all_reduce(g)  # the one exchange step: dL/d(E, e, mu) summed over ranks
+        return g.cpu().numpy(), vr.grad.double()
+
+    out = {}
+    grads = {}
+    for prec in ("fp64", "fp32"):
+        sim = s64 if prec == "fp64" else make("fp32")
+        fwd_adj(sim, min(steps, 2 * ck))  # warm-up: allocator, module loading, first launches
+        _, t_f = timed(lambda: sim.run(x0, v0, w0, guess, steps))
+        (g, gv), t_fa = timed(lambda: fwd_adj(sim))
+        grads[prec] = (g, gv)
+        out[prec] = {"forward": n_all * steps / t_f, "fwd_adjoint": n_all * steps / t_fa, "cost_ratio": t_fa / t_f,
+                     "ms_forward": 1e3 * t_f, "ms_fwd_adjoint": 1e3 * t_fa}
+    g64, gv64 = grads["fp64"]
+    fd, err = [], []
+    for k in range(3):
+        h = 1e-4 * guess[k]
+        tp, tm = list(guess), list(guess)
+        tp[k] += h
+        tm[k] -= h
+        d = (loss_of(s64, tp) - loss_of(s64, tm)) / (2 * h)
+        fd.append(d)
+        err.append(abs(g64[k] - d) / abs(d) if d else None)
+    gen = torch.Generator(device="cpu").manual_seed(5)
+    dv = torch.randn(v0.shape, generator=gen, dtype=torch.float64).to(dev)
+    h = 1e-4 * 0.2
+    d = (loss_of(s64, guess, v0 + h * dv) - loss_of(s64, guess, v0 - h * dv)) / (2 * h)
+    got = float((gv64 * dv).sum())
+    if dist is not None:
+        t = torch.tensor([got], dtype=torch.float64, device=dev)
+        dist.all_reduce(t)
+        got = float(t)
+    g32, gv32 = grads["fp32"]
+    fp32_err = {"E_e_mu": [float(abs(a - b) / abs(b)) for a, b in zip(g32, g64)],
+                "v0_max_abs_over_scale": float((gv32 - gv64).abs().max() / gv64.abs().max())}
+    return {"workload": f"calibration_boxes_{args.calib_scenes}x{per}", "particles": n_all, "substeps": steps,
+            "checkpoint_every": ck, "unit": METRIC, "scaling": "weak (scenes split over ranks)",
+            "path": "step_hertz force law (spheres, planes), hand-written adjoint",
+            "fp64": out["fp64"], "fp32": out["fp32"],
+            "grad_fp64": {"E": float(g64[0]), "e": float(g64[1]), "mu": float(g64[2])},
+            "fd_fp64": {"E": fd[0], "e": fd[1], "mu": fd[2], "v0_direction": d, "rel_step": 1e-4},
+            "rel_err_vs_fd": {"E": err[0], "e": err[1], "mu": err[2], "v0_direction": abs(got - d) / abs(d) if d else None},
+            "fp32_rel_err_vs_fp64": fp32_err, "windows_per_rollout": -(-steps // ck),
+            "window_reruns": s64.stats["reruns"], "loss_at_guess": loss_of(s64, guess),
+            "config": "64 scenes x 2048 spheres r 1 mm, box 40x40x80 mm (6 planes), lattice 8x8x32 + jitter 0.1 mm, "
+                      "v U(+-0.2) m/s, E 5e6 Pa hidden / 4e6 guess, e 0.7 / 0.6, mu 0.35 / 0.3, nu 0.3, dt 2e-5 s"}
+
+
 # ---------------------------------------------------------------------------------------------
 def cpu_reference(scene, substeps, threads):
     """Time the reference's own substep (OpenMP shim build) for `substeps` calls; returns
@@ -377,6 +483,7 @@ def run_ours(args):
                          f"OpenMP Kokkos-shim build, float), {el:.1f} s"}
 
     batched = run_batched(args, rank, world, dist, dem) if args.drums > 0 else None
+    calib = run_calibration(args, rank, world, dist) if args.calib_scenes > 0 else None
 
     if rank == 0:
         line = {
@@ -388,6 +495,7 @@ def run_ours(args):
             "clocks": clocks.summary(), "wall_ms_per_step": 1e3 * wall / args.steps,
             "stages_ms_per_step": {k: round(v[0], 4) for k, v in per_step.items()},
             "counts_last_substep": counts, "sweeps": sweeps, "topology_kept": reuse, "batched": batched,
+            "fwd_adjoint": calib,
             "device_allocations_timed": int(timed_allocs),
         }
         print(json.dumps(line))
@@ -406,6 +514,8 @@ def main():
     ap.add_argument("--cpu-substeps", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--drums", type=int, default=512, help="scenes of the batched line (0: skip it)")
+    ap.add_argument("--calib-scenes", type=int, default=64, help="scenes of the calibration line (0: skip it)")
+    ap.add_argument("--calib-substeps", type=int, default=2000)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)

@@ -312,3 +312,27 @@ def rotating_drums(seed=4, scenes=512, R=50e-3, length=20e-3, nmin=256, nmax=819
             sim.set_wall_velocity(wid, (0.0, 0.0, 0.0), (0.0, 0.0, w), (0.0, 0.0, 0.0))
         extras.append(extra)
     return out, extras
+
+
+def calibration_boxes(seed=5, scenes=64, per_scene=2048, radius=1e-3, box=(40e-3, 40e-3, 80e-3),
+                      lattice=(8, 8, 32), jitter=0.1e-3, vmax=0.2, density=2500.0):
+    """Differentiable-calibration workload: `scenes` independent boxes (six planes shared by every
+    scene) of `per_scene` spheres of radius `radius`, each on a lattice of `lattice` cells filling
+    the box with seeded jitter, initial velocities uniform in +-vmax, no spin.
+    Returns dict(x0, v0, w0 (n, 3); r, m, I (n,); first (scenes + 1); planes (6 x 6))."""
+    nx, ny, nz = lattice
+    if nx * ny * nz != per_scene:
+        raise ValueError("lattice cells must equal the spheres per scene")
+    rng = np.random.default_rng(seed)
+    h = np.array(box) / np.array(lattice)
+    cells = np.stack(np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij"), -1).reshape(-1, 3)
+    base = (cells + 0.5) * h
+    xs = [base + rng.uniform(-jitter, jitter, base.shape) for _ in range(scenes)]
+    n = scenes * per_scene
+    r = np.full(n, radius)
+    m = density * 4.0 / 3.0 * np.pi * r ** 3
+    (x1, y1, z1) = box
+    planes = [[0, 0, 0, 1, 0, 0], [x1, 0, 0, -1, 0, 0], [0, 0, 0, 0, 1, 0], [0, y1, 0, 0, -1, 0],
+              [0, 0, 0, 0, 0, 1], [0, 0, z1, 0, 0, -1]]
+    return dict(x0=np.concatenate(xs), v0=rng.uniform(-vmax, vmax, (n, 3)), w0=np.zeros((n, 3)), r=r, m=m,
+                I=0.4 * m * r * r, first=np.arange(scenes + 1) * per_scene, planes=planes)

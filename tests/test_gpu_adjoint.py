@@ -1,0 +1,161 @@
+"""The differentiable Hertz rollout on the GPU (peclet.dem.adjoint, pdem_hz_* C ABI): its forward
+against the CPU restatement, its adjoint gradients against the restatement's forward-mode dual
+numbers and against central finite differences of the GPU forward (relative step 1e-4, FP64), the
+checkpointed windows against one long window, the FP32 form against FP64, and the
+torch.autograd.Function path."""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+import hertz_cases as HC
+
+sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle"))
+import hertz_spheres as H  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+def _sim(c, precision="fp64", checkpoint=20, skin=None):
+    from peclet.dem.adjoint import HertzSpheres
+    return HertzSpheres(c["r"], c["m"], c["I"], c["first"], c["planes"], HC.NU, HC.DT, c["g"], precision,
+                        checkpoint, skin)
+
+
+def _oracle(c):
+    return H.Model(c["r"], c["m"], c["I"], c["first"], c["planes"], HC.NU, HC.DT, c["g"])
+
+
+def _t(a, sim):
+    return torch.as_tensor(np.asarray(a), dtype=sim.dtype, device=sim.device)
+
+
+def _grads(sim, c, steps, cx, cv, theta=HC.THETA):
+    """Gradients of L = sum(cx * x_T) + sum(cv * v_T) through the adjoint."""
+    (x, v, w), tape = sim.run(_t(c["x0"], sim), _t(c["v0"], sim), _t(c["w0"], sim), theta, steps, record=True)
+    gx, gv, gw, gt = sim.adjoint(tape, theta, _t(cx, sim), _t(cv, sim), torch.zeros_like(w))
+    return [a.double().cpu().numpy() for a in (gx, gv, gw, gt)]
+
+
+def _loss(sim, c, steps, cx, cv, theta=HC.THETA, x0=None, v0=None, w0=None):
+    (x, v, _), _ = sim.run(_t(c["x0"] if x0 is None else x0, sim), _t(c["v0"] if v0 is None else v0, sim),
+                           _t(c["w0"] if w0 is None else w0, sim), theta, steps)
+    return float((x.double().cpu().numpy() * cx).sum() + (v.double().cpu().numpy() * cv).sum())
+
+
+CASES = [("pair", 100), ("floor", 100), ("gas", 60)]
+
+
+@pytest.mark.parametrize("case,steps", CASES)
+def test_forward_matches_oracle(gpu_api, case, steps):
+    c = getattr(HC, case)()
+    sim = _sim(c)
+    (x, v, w), _ = sim.run(_t(c["x0"], sim), _t(c["v0"], sim), _t(c["w0"], sim), HC.THETA, steps)
+    xo, vo, wo = _oracle(c).rollout(c["x0"], c["v0"], c["w0"], *HC.THETA, steps)
+    # force sums are atomics on the GPU: agreement to rounding, not bit-exact
+    np.testing.assert_allclose(x.cpu().numpy(), xo, rtol=0, atol=1e-14)
+    np.testing.assert_allclose(v.cpu().numpy(), vo, rtol=1e-9, atol=1e-12)
+    np.testing.assert_allclose(w.cpu().numpy(), wo, rtol=1e-9, atol=1e-9)
+    assert sim.stats["windows"] == -(-steps // 20)
+
+
+@pytest.mark.parametrize("case,steps", CASES)
+def test_adjoint_matches_dual(gpu_api, case, steps):
+    """Adjoint (reverse) and dual (forward) derivatives of the same discrete map: equal to
+    rounding, along theta's axes and random directions of the initial state."""
+    c = getattr(HC, case)()
+    n = len(c["r"])
+    rng = np.random.default_rng(7)
+    cx, cv = rng.standard_normal((n, 3)), 1e-3 * rng.standard_normal((n, 3))
+    dx, dv, dw = (rng.standard_normal((n, 3)) for _ in range(3))
+    gx, gv, gw, gt = _grads(_sim(c), c, steps, cx, cv)
+    tans = [{"theta": np.eye(3)[k]} for k in range(3)] + [{"x": dx}, {"v": dv}, {"w": dw}]
+    xd, vd, _ = H.jvp(_oracle(c), c["x0"], c["v0"], c["w0"], HC.THETA, tans, steps)
+    want = (xd.d * cx[..., None]).sum((0, 1)) + (vd.d * cv[..., None]).sum((0, 1))
+    got = np.concatenate([gt, [(gx * dx).sum(), (gv * dv).sum(), (gw * dw).sum()]])
+    for k, (a, b) in enumerate(zip(got, want)):
+        assert abs(a - b) <= 1e-7 * abs(b) + 1e-24, f"{case}: direction {k}: adjoint {a} vs dual {b}"
+
+
+@pytest.mark.parametrize("case,steps", CASES)
+def test_adjoint_matches_finite_differences(gpu_api, case, steps):
+    """Central differences of the GPU forward, relative step 1e-4 on theta, within 1e-3."""
+    c = getattr(HC, case)()
+    n = len(c["r"])
+    rng = np.random.default_rng(5)
+    cx, cv = rng.standard_normal((n, 3)), np.zeros((n, 3))
+    sim = _sim(c)
+    _, gv, _, gt = _grads(sim, c, steps, cx, cv)
+    for k in range(3):
+        h = 1e-4 * HC.THETA[k]
+        tp, tm = HC.THETA.copy(), HC.THETA.copy()
+        tp[k] += h
+        tm[k] -= h
+        fd = (_loss(sim, c, steps, cx, cv, tp) - _loss(sim, c, steps, cx, cv, tm)) / (2 * h)
+        assert abs(gt[k] - fd) <= 1e-3 * abs(fd) + 1e-24, f"{case}: theta[{k}]: adjoint {gt[k]} vs FD {fd}"
+    dv = rng.standard_normal((n, 3))
+    h = 1e-4 * 0.1
+    fd = (_loss(sim, c, steps, cx, cv, v0=c["v0"] + h * dv) - _loss(sim, c, steps, cx, cv, v0=c["v0"] - h * dv)) / (2 * h)
+    got = (gv * dv).sum()
+    assert abs(got - fd) <= 1e-3 * abs(fd), f"{case}: v0 direction: adjoint {got} vs FD {fd}"
+
+
+def test_windows_match_one_window(gpu_api):
+    """Checkpoint windows of 7 substeps (pair lists rebuilt and histories carried by key, history
+    adjoints mapped back) give the single-window result."""
+    c = HC.gas()
+    n = len(c["r"])
+    rng = np.random.default_rng(9)
+    cx, cv = rng.standard_normal((n, 3)), rng.standard_normal((n, 3))
+    a = _grads(_sim(c, checkpoint=7), c, 60, cx, cv)
+    b = _grads(_sim(c, checkpoint=1000), c, 60, cx, cv)
+    for ga, gb in zip(a, b):
+        np.testing.assert_allclose(ga, gb, rtol=1e-9, atol=1e-12 * np.abs(gb).max())
+
+
+def test_fp32_gradients_near_fp64(gpu_api):
+    c = HC.gas()
+    n = len(c["r"])
+    rng = np.random.default_rng(4)
+    cx, cv = rng.standard_normal((n, 3)), np.zeros((n, 3))
+    g64 = _grads(_sim(c, "fp64"), c, 60, cx, cv)
+    g32 = _grads(_sim(c, "fp32"), c, 60, cx, cv)
+    for k, (a, b) in enumerate(zip(g32, g64)):
+        err = np.abs(a - b).max() / np.abs(b).max()
+        assert err < 2e-2, f"gradient {k}: FP32 max error {err:.2e} of the FP64 scale"
+
+
+def test_autograd_function(gpu_api):
+    """loss.backward() through HertzSpheres.rollout equals the explicit adjoint."""
+    c = HC.gas()
+    sim = _sim(c)
+    n = len(c["r"])
+    rng = np.random.default_rng(2)
+    target = _t(c["x0"] + 1e-4 * rng.standard_normal((n, 3)), sim)
+    x0 = _t(c["x0"], sim).requires_grad_(True)
+    v0 = _t(c["v0"], sim).requires_grad_(True)
+    w0 = _t(c["w0"], sim).requires_grad_(True)
+    theta = torch.tensor(HC.THETA, dtype=torch.float64, requires_grad=True)
+    x, v, w = sim.rollout(x0, v0, w0, theta, 40)
+    loss = ((x - target) ** 2).sum(dim=1).mean()
+    loss.backward()
+    gx = (2.0 / n) * (x.detach() - target)
+    bx, bv, bw, bt = _grads(sim, c, 40, gx.cpu().numpy(), np.zeros((n, 3)))
+    np.testing.assert_allclose(v0.grad.cpu().numpy(), bv, rtol=1e-9, atol=1e-12 * np.abs(bv).max())
+    np.testing.assert_allclose(theta.grad.numpy(), bt, rtol=1e-9)
+    assert theta.grad.dtype == torch.float64 and v0.grad.shape == (n, 3)
+
+
+def test_rejects_bad_arguments(gpu_api):
+    from peclet.dem.adjoint import HertzSpheres
+    c = HC.pair()
+    with pytest.raises(ValueError):
+        HertzSpheres(c["r"], c["m"][:1], c["I"], precision="fp64")
+    with pytest.raises(ValueError):
+        HertzSpheres(c["r"], c["m"], c["I"], scene_first=[0, 3])
+    sim = _sim(c)
+    with pytest.raises(ValueError):
+        sim.run(_t(c["x0"], sim), _t(c["v0"], sim), _t(c["w0"], sim), (0.0, 0.7, 0.35), 5)
