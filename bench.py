@@ -219,7 +219,8 @@ def run_calibration(args, rank, world, dist):
     (4e6, 0.6, 0.3). Scenes are split over ranks; the three material gradients are summed over
     ranks with one all-reduce per backward pass. Reports forward-only and forward+adjoint rates
     (device time, max over ranks), their cost ratio, the gradients' relative error against
-    central finite differences (relative step 1e-4, FP64) and the FP32 gradients' error against
+    central finite differences (relative steps 1e-4 and 1e-6, FP64) and against the tangent-linear
+    (forward-mode dual-number) run along one direction, and the FP32 gradients' error against
     FP64. Returns the sub-object of the JSON line."""
     import torch
     from peclet.dem import workloads as W
@@ -252,67 +253,95 @@ def run_calibration(args, rank, world, dist):
     v0 = torch.as_tensor(c["v0"][sl], device=dev)
     w0 = torch.as_tensor(c["w0"][sl], device=dev)
     s64 = make("fp64")
-    (xt, _, _), _ = s64.run(x0, v0, w0, hidden, steps)
+    (xt, _, _), _ = s64.run(x0, v0, w0, hidden, steps)  # targets at the hidden parameters
 
-    def loss_of(sim, theta, vv=None):
-        (x, _, _), _ = sim.run(x0, v0 if vv is None else vv, w0, theta, steps)
-        part = ((x.double() - xt) ** 2).sum()
+    def loss_of(sim, theta, target, nsteps, vv=None):
+        (x, _, _), _ = sim.run(x0, v0 if vv is None else vv, w0, tuple(theta), nsteps)
+        part = ((x.double() - target) ** 2).sum()
         if dist is not None:
             dist.all_reduce(part)
         return float(part) / n_all
 
-    def fwd_adj(sim, nsteps=steps):
+    def fwd_adj(sim, target, nsteps):
         th = torch.tensor(guess, dtype=torch.float64, requires_grad=True)
         vr = v0.to(sim.dtype).clone().requires_grad_(True)
         x, _, _ = sim.rollout(x0.to(sim.dtype), vr, w0.to(sim.dtype), th, nsteps)
-        loss = ((x.double() - xt) ** 2).sum() / n_all
+        loss = ((x.double() - target) ** 2).sum() / n_all
         loss.backward()
         g = th.grad.to(dev)
         if dist is not None:
             dist.all_reduce(g)  # the one exchange step: dL/d(E, e, mu) summed over ranks
         return g.cpu().numpy(), vr.grad.double()
 
+    def ranks_sum(x):
+        if dist is None:
+            return float(x)
+        t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+        dist.all_reduce(t)
+        return float(t)
+
+    rel = lambda a, b: abs(a - b) / abs(b) if b else None
+    gen = torch.Generator(device="cpu").manual_seed(5)
+    dv = torch.randn(v0.shape, generator=gen, dtype=torch.float64).to(dev)
+    dth = np.array([1e5, 0.01, 0.01])
+
+    def checks(nsteps, target, g64, gv64, g32, gv32):
+        """Gradients at one horizon against central finite differences of the FP64 forward
+        (relative steps 1e-4 and 1e-6), the directional derivative against the tangent-linear
+        run and FD, and the FP32 gradients against FP64."""
+        fd = {}
+        for rstep in (1e-4, 1e-6):
+            row = []
+            for k in range(3):
+                h = rstep * guess[k]
+                tp, tm = list(guess), list(guess)
+                tp[k] += h
+                tm[k] -= h
+                row.append((loss_of(s64, tp, target, nsteps) - loss_of(s64, tm, target, nsteps)) / (2 * h))
+            fd[rstep] = row
+        got = ranks_sum((gv64 * dv).sum()) + float((g64 * dth).sum())
+        h = 1e-4 * 0.2  # relative step 1e-4 of the largest initial speed component
+        fd_dir = (loss_of(s64, np.array(guess) + h * dth, target, nsteps, v0 + h * dv)
+                  - loss_of(s64, np.array(guess) - h * dth, target, nsteps, v0 - h * dv)) / (2 * h)
+        ((xj, _, _), (xdj, _, _)), t_j = timed(lambda: s64.jvp(x0, v0, w0, guess, torch.zeros_like(x0), dv,
+                                                              torch.zeros_like(w0), dth, nsteps))
+        jv = ranks_sum((2.0 * (xj - target) * xdj).sum()) / n_all
+        return {"substeps": nsteps,
+                "grad_fp64": {"E": float(g64[0]), "e": float(g64[1]), "mu": float(g64[2])},
+                "fd_fp64": {str(r): {"E": v[0], "e": v[1], "mu": v[2]} for r, v in fd.items()},
+                "rel_err_vs_fd": {str(r): {"E": rel(g64[0], v[0]), "e": rel(g64[1], v[1]), "mu": rel(g64[2], v[2])}
+                                  for r, v in fd.items()},
+                "direction": {"adjoint": got, "tangent_linear": jv, "rel_err_vs_tangent_linear": rel(got, jv),
+                              "fd_rel_step_1e-4": fd_dir, "rel_err_vs_fd": rel(got, fd_dir),
+                              "ms_tangent_linear": 1e3 * t_j,
+                              "what": "theta (1e5, 0.01, 0.01) and v0 ~ N(0, 1) per component"},
+                "fp32_rel_err_vs_fp64": {"E_e_mu": [float(abs(a - b) / abs(b)) for a, b in zip(g32, g64)],
+                                         "v0_rms": float((gv32 - gv64).norm() / gv64.norm()),
+                                         "v0_max_abs_over_scale": float((gv32 - gv64).abs().max()
+                                                                        / gv64.abs().max())}}
+
     out = {}
     grads = {}
-    for prec in ("fp64", "fp32"):
-        sim = s64 if prec == "fp64" else make("fp32")
-        fwd_adj(sim, min(steps, 2 * ck))  # warm-up: allocator, module loading, first launches
+    s32 = make("fp32")
+    for prec, sim in (("fp64", s64), ("fp32", s32)):
+        fwd_adj(sim, xt, min(steps, 2 * ck))  # warm-up: allocator, module loading, first launches
         _, t_f = timed(lambda: sim.run(x0, v0, w0, guess, steps))
-        (g, gv), t_fa = timed(lambda: fwd_adj(sim))
+        (g, gv), t_fa = timed(lambda: fwd_adj(sim, xt, steps))
         grads[prec] = (g, gv)
         out[prec] = {"forward": n_all * steps / t_f, "fwd_adjoint": n_all * steps / t_fa, "cost_ratio": t_fa / t_f,
                      "ms_forward": 1e3 * t_f, "ms_fwd_adjoint": 1e3 * t_fa}
-    g64, gv64 = grads["fp64"]
-    fd, err = [], []
-    for k in range(3):
-        h = 1e-4 * guess[k]
-        tp, tm = list(guess), list(guess)
-        tp[k] += h
-        tm[k] -= h
-        d = (loss_of(s64, tp) - loss_of(s64, tm)) / (2 * h)
-        fd.append(d)
-        err.append(abs(g64[k] - d) / abs(d) if d else None)
-    gen = torch.Generator(device="cpu").manual_seed(5)
-    dv = torch.randn(v0.shape, generator=gen, dtype=torch.float64).to(dev)
-    h = 1e-4 * 0.2
-    d = (loss_of(s64, guess, v0 + h * dv) - loss_of(s64, guess, v0 - h * dv)) / (2 * h)
-    got = float((gv64 * dv).sum())
-    if dist is not None:
-        t = torch.tensor([got], dtype=torch.float64, device=dev)
-        dist.all_reduce(t)
-        got = float(t)
-    g32, gv32 = grads["fp32"]
-    fp32_err = {"E_e_mu": [float(abs(a - b) / abs(b)) for a, b in zip(g32, g64)],
-                "v0_max_abs_over_scale": float((gv32 - gv64).abs().max() / gv64.abs().max())}
+    full = checks(steps, xt, *grads["fp64"], *grads["fp32"])
+    # the same checks on a 64-substep horizon (few contacts begin or end inside it)
+    short = min(64, steps)
+    (xs, _, _), _ = s64.run(x0, v0, w0, hidden, short)
+    window = checks(short, xs, *fwd_adj(s64, xs, short), *fwd_adj(s32, xs, short))
     return {"workload": f"calibration_boxes_{args.calib_scenes}x{per}", "particles": n_all, "substeps": steps,
             "checkpoint_every": ck, "unit": METRIC, "scaling": "weak (scenes split over ranks)",
             "path": "step_hertz force law (spheres, planes), hand-written adjoint",
             "fp64": out["fp64"], "fp32": out["fp32"],
-            "grad_fp64": {"E": float(g64[0]), "e": float(g64[1]), "mu": float(g64[2])},
-            "fd_fp64": {"E": fd[0], "e": fd[1], "mu": fd[2], "v0_direction": d, "rel_step": 1e-4},
-            "rel_err_vs_fd": {"E": err[0], "e": err[1], "mu": err[2], "v0_direction": abs(got - d) / abs(d) if d else None},
-            "fp32_rel_err_vs_fp64": fp32_err, "windows_per_rollout": -(-steps // ck),
-            "window_reruns": s64.stats["reruns"], "loss_at_guess": loss_of(s64, guess),
+            "checks_full_horizon": full, "checks_64_substeps": window, "checkpoints_per_rollout": -(-steps // ck),
+            "contact_list_every": s64.list_every, "window_reruns": s64.stats["reruns"],
+            "loss_at_guess": loss_of(s64, guess, xt, steps),
             "config": "64 scenes x 2048 spheres r 1 mm, box 40x40x80 mm (6 planes), lattice 8x8x32 + jitter 0.1 mm, "
                       "v U(+-0.2) m/s, E 5e6 Pa hidden / 4e6 guess, e 0.7 / 0.6, mu 0.35 / 0.3, nu 0.3, dt 2e-5 s"}
 

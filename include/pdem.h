@@ -209,40 +209,50 @@ int pdem_debug_sweeps(pdem_handle h, long* out4);
 int pdem_find_pairs_static(const double* d_xyz, const double* d_radius, int n, double margin, double box_cap,
                            int* d_pairs, long pair_cap, long* out_count, void* stream);
 
-/* ---- forward + adjoint of the Hertz-Mindlin substep for spheres (no counterpart in the reference;
- * the force law is the Hertz engine's, src/solver_hertz.hpp:88-144, its kick-drift
- * src/solver_hertz.hpp:374-425; planes are walls at rest with the same law) ----
+/* ---- forward, adjoint and tangent-linear runs of the Hertz-Mindlin substep for spheres (no
+ * counterpart in the reference; the force law is the Hertz engine's, src/solver_hertz.hpp:88-144,
+ * its kick-drift src/solver_hertz.hpp:374-425; planes are walls at rest with the same law) ----
  * All arrays are DEVICE arrays of the call's precision (32: float, 64: double) unless stated;
- * pairs are int. A state block is x, v, w (3 n each), pair histories (3 per pair), plane histories
- * (3 per sphere and plane, sphere-major): pdem_hz_state_size values. The pair list stays fixed
- * over the substeps of one call. Gradients with respect to (E, e, mu) accumulate into d_grad
- * (3 doubles, device, not cleared). Work goes to `stream`; forward and backward do not
- * synchronise it. */
+ * contacts are int pairs (i, j): j >= 0 the sphere j > i, j < 0 the plane -j - 1. A state block is
+ * x, v, w (3 n each) then the history of every contact (3 each): pdem_hz_state_size values. The
+ * contact list stays fixed over the substeps of one call. Work goes to `stream`; forward,
+ * backward and jvp do not synchronise it. */
 typedef struct {
-  int n, npair, nplane;
-  const int* pairs;     /* npair x (i, j), i < j */
+  int n, ncontact, nplane;
+  const int* contacts;  /* ncontact x (i, j) */
   const void* planes;   /* nplane x (point, unit normal into the domain) */
   const void* radius;   /* n */
   const void* mass;     /* n */
   const void* inertia;  /* n: scalar moment of inertia */
   double youngs, restitution, friction, poisson, dt, gravity[3];
 } pdem_hz_model;
-long pdem_hz_state_size(int n, int npair, int nplane);
-/* work buffer of forward and backward, in values of the precision */
-long pdem_hz_work_size(int n, int npair, int nplane);
-/* candidate pairs (i < j < d_end[i], |x_i - x_j| < r_i + r_j + skin; d_end[i] = exclusive end of
- * i's scene, NULL = n) in (i, j) order; d_cnt n ints and d_off n + 1 ints of scratch; when the
- * count exceeds cap nothing is written. Synchronises the stream. */
-int pdem_hz_pairs(int precision, const void* d_x, const void* d_radius, const int* d_end, int n, double skin,
-                  int* d_cnt, int* d_off, int* d_pairs, long cap, long* count, void* stream);
+long pdem_hz_state_size(int n, int ncontact);
+/* work buffer of forward, backward and jvp, in values of the precision */
+long pdem_hz_work_size(int n, int ncontact);
+/* candidate contacts per sphere i, in i order: the spheres i < j of i's scene (scenes are the
+ * ranges [first[s], first[s + 1]), nscene + 1 ints from 0 to n, given on the HOST (first) and the
+ * device (d_first) alike) with
+ * |x_i - x_j| < r_i + r_j + skin, then the planes k with (x_i - p0_k).n_k < r_i + skin.
+ * d_cnt n ints and d_off n + 1 ints of scratch; when the count exceeds cap nothing is written.
+ * Synchronises the stream. */
+int pdem_hz_contacts(int precision, const void* d_x, const void* d_radius, const int* first, const int* d_first,
+                     int nscene, const void* d_planes, int nplane, double skin, int* d_cnt, int* d_off, int* d_contacts,
+                     long cap, long* count, void* stream);
 /* `steps` substeps from the state in block 0 of d_traj: store = 1 writes substep k to block k
  * (steps + 1 blocks), store = 0 ping-pongs blocks 0 and 1 and leaves the final state in block 1 */
 int pdem_hz_forward(int precision, const pdem_hz_model* model, int steps, int store, void* d_traj, void* d_work,
                     void* stream);
 /* reverse of a stored forward (steps + 1 blocks in d_traj): d_adj holds the adjoint of the final
- * state on entry and that of block 0 on return */
+ * state on entry and that of block 0 on return; gradients with respect to (E, e, mu) accumulate
+ * into d_grad (3 doubles, device, not cleared). mode 0: hand reversal of each contact law;
+ * mode 1: dual-number local Jacobians (the cross-check, slower) */
 int pdem_hz_backward(int precision, const pdem_hz_model* model, int steps, const void* d_traj, void* d_adj,
-                     double* d_grad, void* d_work, void* stream);
+                     double* d_grad, void* d_work, int mode, void* stream);
+/* tangent-linear run: the state (2 blocks) and its tangent (2 blocks) advance `steps` substeps
+ * from block 0 together, with the parameter tangent theta_dot (3 doubles, HOST: dE, de, dmu);
+ * both end in block 1 */
+int pdem_hz_jvp(int precision, const pdem_hz_model* model, int steps, void* d_state, void* d_tangent,
+                const double* theta_dot, void* d_work, void* stream);
 
 #ifdef __cplusplus
 }

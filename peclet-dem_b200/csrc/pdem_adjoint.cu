@@ -1,28 +1,30 @@
-// Forward and hand-written adjoint of the explicit Hertz-Mindlin substep for spheres, for
+// Forward, adjoint and tangent-linear runs of the explicit Hertz-Mindlin substep for spheres, for
 // differentiable calibration: gradients of a loss on the final state with respect to Young's
 // modulus E, the restitution e, the friction mu and the initial state.
 //
 // The force law is the Hertz engine's (src/solver_hertz.hpp:88-144 for sphere pairs, the same law
 // against a wall at rest for the planes, src/solver_hertz.hpp:300-372), the integration its
 // symplectic kick-drift (src/solver_hertz.hpp:374-425) without orientation update:
-//   per pair (i, j) with overlap d = r_i + r_j - |x_i - x_j| > 0: force f(d, n, v_rel, xi; E, e, mu)
-//   and the new Mindlin history xi' (hertzForce, shared with the engine), torques r_A x f on i and
-//   r_B x (-f) on j; per sphere and plane the same law with the plane at rest; then
-//   v' = v + (F / m + g) dt, w' = w + T / I dt, x' = x + v' dt.
-// The pair list is fixed over a window of substeps (the caller builds it with a skin at each window
-// start); plane contacts are evaluated for every (sphere, plane).
+//   per contact with overlap d > 0 (pair: d = r_i + r_j - |x_i - x_j|, normal from j to i; plane:
+//   d = r_i - (x_i - p0).n): force f(d, n, v_rel, xi; E, e, mu) and the new Mindlin history xi',
+//   torques r_A x f on i (and r_B x (-f) on j); then v' = v + (F / m + g) dt, w' = w + T / I dt,
+//   x' = x + v' dt.
+// Contacts are candidates (sphere pairs of one scene and sphere-plane couples within a skin) built
+// by the caller at each window start; they stay fixed over the window's substeps.
 //
-// State of a substep (one contiguous block): x, v, w (3 n each), pair histories (3 per pair),
-// plane histories (3 per sphere and plane). The forward stores every substep of a window (or
-// ping-pongs two states); the backward walks the stored window in reverse.
+// State of a substep (one contiguous block): x, v, w (3 n each), then the history of every
+// contact (3 each). The forward stores every substep of a window (or ping-pongs two states); the
+// backward walks the stored window in reverse.
 //
 // Adjoint of one substep, given the adjoint of S_{k+1}: the integration is linear and reversed by
-// hand; each contact's local Jacobian (outputs: force, torques, new history; inputs: relative
-// position, relative velocity, both spins, history, E, e, mu) is taken in forward mode with dual
-// numbers through the same hertzForce the forward runs (so the recorded active set and friction
-// branch are exactly the forward's), and its transpose is applied to the outputs' adjoints.
-// Accumulation into bodies and parameters uses atomics, so gradients are summed in an unspecified
-// order (forward forces too: the forward is deterministic only up to that summation order).
+// hand; each contact's law is re-evaluated from the stored state with its intermediates kept in
+// registers (the same arithmetic as the forward, so the active set and the stick/slip branch are
+// the forward's) and reversed statement by statement. A second mode takes the contact's local
+// Jacobian with forward-mode dual numbers through the engine's own hertzForce instead; it is the
+// cross-check of the hand reversal. The tangent-linear run carries one dual tangent through the
+// whole rollout. Accumulation into bodies and parameters uses atomics, so sums come in an
+// unspecified order (forward forces too: the forward is deterministic up to summation order).
+#include <algorithm>
 #include <cmath>
 #include <string>
 #include <utility>
@@ -37,11 +39,17 @@ void setLastError(const std::string& msg);  // pdem_capi.cu
 
 namespace {
 
+using pdem::add;
+using pdem::cross;
+using pdem::dot;
+using pdem::mul;
+using pdem::sub;
 using pdem::V3;
 using std::fabs;  // the plain overloads stay visible beside the dual-number ones below
 using std::log;
 using std::sqrt;
 
+// ---------------------------------------------------------------------------------------------
 // forward-mode dual number over scalar S with N tangents
 template <class S, int N>
 struct Dn {
@@ -135,7 +143,41 @@ __device__ Dn<S, N> fabs(const Dn<S, N>& a) {
   return a.v < S(0) ? -a : a;
 }
 
-// material stars of one material against itself (hertzStars with E_i = E_j, nu_i = nu_j)
+// ---------------------------------------------------------------------------------------------
+template <class R>
+struct Model {
+  int n, nc, nplane;
+  const int* cont;  // [nc] (i, j): j >= 0 the sphere j (> i); j < 0 the plane -j - 1
+  const R *planes, *r, *m, *I;
+  R E, e, mu, dt, g[3];
+  double nu;
+};
+template <class R>
+struct StateView {
+  R *x, *v, *w, *xi;
+};
+inline size_t stateSize(long n, long nc) { return (size_t)(9 * n + 3 * nc); }
+template <class R>
+StateView<R> view(R* base, long n) {
+  return StateView<R>{base, base + 3 * n, base + 6 * n, base + 9 * n};
+}
+template <class R>
+__device__ V3<R> ld3(const R* p, long i) {
+  return V3<R>{p[3 * i], p[3 * i + 1], p[3 * i + 2]};
+}
+template <class R>
+__device__ void st3(R* p, long i, V3<R> a) {
+  p[3 * i] = a.x, p[3 * i + 1] = a.y, p[3 * i + 2] = a.z;
+}
+template <class R>
+__device__ void atomicAdd3(R* p, long i, V3<R> a) {
+  atomicAdd(&p[3 * i], a.x);
+  atomicAdd(&p[3 * i + 1], a.y);
+  atomicAdd(&p[3 * i + 2], a.z);
+}
+
+// material stars of one material against itself (hertzStars with E_i = E_j, nu_i = nu_j):
+// E* = E / (2 (1 - nu^2)), G* = E / (4 (2 - nu)(1 + nu))
 template <class T>
 __device__ void stars(T E, double nu, T& eS, T& gS) {
   const T one(1.0), two(2.0), a(1.0 - nu * nu), b((2.0 - nu) * (1.0 + nu));
@@ -143,147 +185,324 @@ __device__ void stars(T E, double nu, T& eS, T& gS) {
   gS = one / (two * b / E + two * b / E);
 }
 
-// sphere pair: in = dx(3) dv(3) wi(3) wj(3) xi(3) E e mu; out = f(3) Ti(3) Tj(3) xi'(3).
-// Returns false (no force, history cleared) when the spheres do not overlap.
-constexpr int kPairIn = 18, kPairOut = 12, kPlaneIn = 15, kPlaneOut = 9;
-template <class T, class S>
-__device__ bool pairLaw(const T* in, S ri, S rj, S mS, double nu, S dt, T* out) {
-  const V3<T> dx{in[0], in[1], in[2]}, dv{in[3], in[4], in[5]}, wi{in[6], in[7], in[8]}, wj{in[9], in[10], in[11]};
-  V3<T> xi{in[12], in[13], in[14]};
-  const T dd = sqrt(pdem::dot(dx, dx));
-  const T delta = T(ri + rj) - dd;
-  if (delta <= T(0.0) || dd < T(1e-12))
-    return false;
-  const V3<T> nh = pdem::mul(dx, T(1.0) / dd);
-  const V3<T> rA = pdem::mul(nh, -(T(ri) - T(0.5) * delta));
-  const V3<T> rB = pdem::mul(nh, T(rj) - T(0.5) * delta);
-  const V3<T> vr = pdem::sub(pdem::add(dv, pdem::cross(wi, rA)), pdem::cross(wj, rB));
-  T eS, gS;
-  stars(in[15], nu, eS, gS);
-  const V3<T> f = pdem::hertzForce(delta, nh, vr, T(ri * rj / (ri + rj)), T(mS), eS, gS, in[16], in[17], T(dt), xi);
-  const V3<T> ti = pdem::cross(rA, f), tj = pdem::cross(rB, pdem::mul(f, T(-1.0)));
-  out[0] = f.x, out[1] = f.y, out[2] = f.z;
-  out[3] = ti.x, out[4] = ti.y, out[5] = ti.z;
-  out[6] = tj.x, out[7] = tj.y, out[8] = tj.z;
-  out[9] = xi.x, out[10] = xi.y, out[11] = xi.z;
-  return true;
+// ---------------------------------------------------------------------------------------------
+// One contact with its intermediates: the engine's hertzForce statement by statement (same
+// operations in the same order), kept for the reversal.
+template <class R>
+struct Contact {
+  int i, j, k;  // spheres i, j (j < 0 for a plane k)
+  bool active, slip, sOk, stOk;
+  R ri, rj, rS, mS, dd, delta, eS, gS, sq, sn, st, kn, bd, qN, qT, etaN, etaT, vn, fs, fn, p, fl, fm, s;
+  V3<R> dx, nh, rA, rB, wi, wj, vr, vt, xi1, xi2, ft0, ft, f, xi3;
+};
+template <class R>
+constexpr R kEtaC() {
+  return R(-2) * R(0.9128709);
 }
-// sphere on plane (point p0, unit normal n into the domain): in = x(3) v(3) w(3) xi(3) E e mu;
-// out = f(3) T(3) xi'(3)
-template <class T, class S>
-__device__ bool planeLaw(const T* in, const S* pl, S ri, S mi, double nu, S dt, T* out) {
-  const V3<T> x{in[0], in[1], in[2]}, v{in[3], in[4], in[5]}, w{in[6], in[7], in[8]};
-  V3<T> xi{in[9], in[10], in[11]};
-  const V3<T> p0{T(pl[0]), T(pl[1]), T(pl[2])}, n{T(pl[3]), T(pl[4]), T(pl[5])};
-  const T delta = T(ri) - pdem::dot(pdem::sub(x, p0), n);
+
+template <class R>
+__device__ void contactPrimal(const Model<R>& M, long c, const StateView<R>& s, Contact<R>& C) {
+  C.i = M.cont[2 * c];
+  C.j = M.cont[2 * c + 1];
+  C.k = C.j < 0 ? -C.j - 1 : -1;
+  const int i = C.i;
+  C.ri = M.r[i];
+  // the activity test first, from positions and radii only (most candidates are apart)
+  if (C.j >= 0) {
+    const int j = C.j;
+    C.rj = M.r[j];
+    C.dx = sub(ld3(s.x, i), ld3(s.x, j));
+    C.dd = sqrt(dot(C.dx, C.dx));
+    C.delta = C.ri + C.rj - C.dd;
+    C.active = !(C.delta <= R(0) || C.dd < R(1e-12));
+    if (!C.active)
+      return;
+    C.wi = ld3(s.w, i);
+    C.nh = mul(C.dx, R(1) / C.dd);
+    C.rA = mul(C.nh, -(C.ri - R(0.5) * C.delta));
+    C.rB = mul(C.nh, (C.rj - R(0.5) * C.delta));
+    C.wj = ld3(s.w, j);
+    C.vr = sub(add(ld3(s.v, i), cross(C.wi, C.rA)), add(ld3(s.v, j), cross(C.wj, C.rB)));
+    C.rS = C.ri * C.rj / (C.ri + C.rj);
+    C.mS = R(1) / (R(1) / M.m[i] + R(1) / M.m[j]);
+  } else {
+    const R* pl = M.planes + 6 * C.k;
+    C.nh = V3<R>{pl[3], pl[4], pl[5]};
+    C.delta = C.ri - dot(sub(ld3(s.x, i), V3<R>{pl[0], pl[1], pl[2]}), C.nh);
+    C.active = !(C.delta <= R(0));
+    if (!C.active)
+      return;
+    C.wi = ld3(s.w, i);
+    C.rA = mul(C.nh, -(C.ri - R(0.5) * C.delta));
+    C.vr = add(ld3(s.v, i), cross(C.wi, C.rA));
+    C.rS = C.ri;
+    C.mS = M.m[i];
+  }
+  const V3<R> xi0 = ld3(s.xi, c);
+  stars(M.E, M.nu, C.eS, C.gS);
+  C.sq = sqrt(C.rS * C.delta);
+  C.sn = R(2) * C.eS * C.sq;
+  C.st = R(8) * C.gS * C.sq;
+  C.kn = (R(4) / R(3)) * C.eS * C.sq;
+  C.bd = pdem::hertzBetaD(M.e);
+  C.qN = sqrt(C.sn * C.mS);
+  C.qT = sqrt(C.st * C.mS);
+  C.etaN = kEtaC<R>() * C.bd * C.qN;
+  C.etaT = kEtaC<R>() * C.bd * C.qT;
+  C.vn = dot(C.vr, C.nh);
+  C.fs = C.kn * C.delta;
+  C.fn = C.fs - C.etaN * C.vn;
+  C.vt = sub(C.vr, mul(C.nh, C.vn));
+  C.xi1 = add(xi0, mul(C.vt, M.dt));
+  C.p = dot(C.xi1, C.nh);
+  C.xi2 = sub(C.xi1, mul(C.nh, C.p));
+  C.ft0 = add(mul(C.xi2, -C.st), mul(C.vt, -C.etaT));
+  C.fl = sqrt(dot(C.ft0, C.ft0));
+  C.fm = M.mu * fabs(C.fs);
+  C.slip = C.fl > C.fm;
+  C.ft = C.ft0;
+  C.xi3 = C.xi2;
+  if (C.slip) {
+    C.sOk = C.fl > R(1e-20);
+    C.s = C.sOk ? C.fm / C.fl : R(0);
+    C.ft = mul(C.ft0, C.s);
+    C.stOk = C.st > R(1e-20);
+    if (C.stOk)
+      C.xi3 = mul(add(C.ft, mul(C.vt, C.etaT)), R(-1) / C.st);
+  }
+  C.f = add(mul(C.nh, C.fn), C.ft);
+}
+
+// Reverse of one active contact. In: fb (adjoint of f, the force on i), tAb, tBb (adjoints of
+// the torques on i and j), xib (adjoint of the new history). Out: adjoints of x_i, x_j, v_i, v_j,
+// w_i, w_j (pair: the j parts are the negated dx / dv ones), of the old history, and of E, e, mu.
+template <class R>
+struct ContactBar {
+  V3<R> dx, dv, wi, wj, xi;
+  R E, e, mu;
+};
+template <class R>
+__device__ ContactBar<R> contactReverse(const Model<R>& M, const Contact<R>& C, V3<R> fb, V3<R> tAb, V3<R> tBb,
+                                        V3<R> xi3b) {
+  const V3<R> zero{R(0), R(0), R(0)};
+  ContactBar<R> B;
+  // torques: tA = rA x f, tB = rB x (-f)
+  V3<R> rAb = cross(C.f, tAb);
+  fb = add(fb, cross(tAb, C.rA));
+  V3<R> rBb = zero;
+  if (C.j >= 0) {
+    rBb = cross(tBb, C.f);
+    fb = add(fb, cross(C.rB, tBb));
+  }
+  // f = nh fn + ft
+  V3<R> nhb = mul(fb, C.fn);
+  const R fnb = dot(C.nh, fb);
+  V3<R> ftb = fb, ft0b = zero, xi2b = zero, vtb = zero;
+  R stb = 0, etaTb = 0, fmb = 0, flb = 0;
+  if (C.slip) {
+    if (C.stOk) {  // xi3 = (ft + vt etaT) (-1 / st)
+      const R inv = R(-1) / C.st;
+      ftb = add(ftb, mul(xi3b, inv));
+      etaTb += dot(xi3b, C.vt) * inv;
+      vtb = add(vtb, mul(xi3b, C.etaT * inv));
+      stb += -dot(xi3b, C.xi3) / C.st;
+    } else {
+      xi2b = add(xi2b, xi3b);
+    }
+    // ft = ft0 s, s = fm / fl
+    ft0b = add(ft0b, mul(ftb, C.s));
+    const R sb = dot(C.ft0, ftb);
+    if (C.sOk) {
+      fmb += sb / C.fl;
+      flb += -sb * C.s / C.fl;
+    }
+  } else {
+    ft0b = add(ft0b, ftb);
+    xi2b = add(xi2b, xi3b);
+  }
+  // fm = mu |fs|
+  const R mub = fabs(C.fs) * fmb;
+  R fsb = (C.fs >= R(0) ? M.mu : -M.mu) * fmb;
+  // fl = |ft0|
+  if (C.fl > R(0))
+    ft0b = add(ft0b, mul(C.ft0, flb / C.fl));
+  // ft0 = xi2 (-st) + vt (-etaT)
+  stb += -dot(C.xi2, ft0b);
+  xi2b = add(xi2b, mul(ft0b, -C.st));
+  etaTb += -dot(C.vt, ft0b);
+  vtb = add(vtb, mul(ft0b, -C.etaT));
+  // xi2 = xi1 - nh p, p = xi1 . nh
+  const R pb = -dot(C.nh, xi2b);
+  const V3<R> xi1b = add(xi2b, mul(C.nh, pb));
+  nhb = add(nhb, add(mul(xi2b, -C.p), mul(C.xi1, pb)));
+  // xi1 = xi0 + vt dt
+  B.xi = xi1b;
+  vtb = add(vtb, mul(xi1b, M.dt));
+  // vt = vr - nh vn
+  V3<R> vrb = vtb;
+  nhb = add(nhb, mul(vtb, -C.vn));
+  R vnb = -dot(C.nh, vtb);
+  // fn = fs - etaN vn
+  fsb += fnb;
+  const R etaNb = -C.vn * fnb;
+  vnb += -C.etaN * fnb;
+  // fs = kn delta
+  const R knb = C.delta * fsb;
+  R deltab = C.kn * fsb;
+  // vn = vr . nh
+  vrb = add(vrb, mul(C.nh, vnb));
+  nhb = add(nhb, mul(C.vr, vnb));
+  // etaN = c bd qN, etaT = c bd qT, q = sqrt(s mS)
+  const R bdb = kEtaC<R>() * (C.qT * etaTb + C.qN * etaNb);
+  R snb = 0;
+  if (C.qT > R(0))
+    stb += kEtaC<R>() * C.bd * etaTb * C.mS / (R(2) * C.qT);
+  if (C.qN > R(0))
+    snb += kEtaC<R>() * C.bd * etaNb * C.mS / (R(2) * C.qN);
+  // bd = ln e / sqrt(ln^2 e + pi^2) on 0 < e < 1, constant outside
+  B.e = 0;
+  if (M.e > R(0) && M.e < R(1)) {
+    const R le = log(M.e), den = le * le + R(9.8696044);
+    B.e = bdb * R(9.8696044) / (den * sqrt(den)) / M.e;
+  }
+  // kn = (4/3) eS sq, st = 8 gS sq, sn = 2 eS sq
+  const R eSb = (R(4) / R(3)) * C.sq * knb + R(2) * C.sq * snb;
+  const R gSb = R(8) * C.sq * stb;
+  const R sqb = (R(4) / R(3)) * C.eS * knb + R(8) * C.gS * stb + R(2) * C.eS * snb;
+  // sq = sqrt(rS delta)
+  if (C.sq > R(0))
+    deltab += sqb * C.rS / (R(2) * C.sq);
+  // eS, gS proportional to E
+  B.E = (eSb * C.eS + gSb * C.gS) / M.E;
+  B.mu = mub;
+  if (C.j >= 0) {
+    // vr = (v_i + wi x rA) - (v_j + wj x rB)
+    B.dv = vrb;
+    B.wi = cross(C.rA, vrb);
+    rAb = add(rAb, cross(vrb, C.wi));
+    B.wj = mul(cross(C.rB, vrb), R(-1));
+    rBb = add(rBb, mul(cross(vrb, C.wj), R(-1)));
+    // rA = nh (-(ri - delta / 2)), rB = nh (rj - delta / 2)
+    nhb = add(nhb, mul(rAb, -(C.ri - R(0.5) * C.delta)));
+    deltab += R(0.5) * dot(C.nh, rAb);
+    nhb = add(nhb, mul(rBb, C.rj - R(0.5) * C.delta));
+    deltab += R(-0.5) * dot(C.nh, rBb);
+    // delta = ri + rj - dd; nh = dx / dd; dd = |dx|
+    R ddb = -deltab;
+    B.dx = mul(nhb, R(1) / C.dd);
+    ddb += -dot(nhb, C.nh) / C.dd;
+    B.dx = add(B.dx, mul(C.nh, ddb));
+  } else {
+    // vr = v + wi x rA; rA = n (-(ri - delta / 2)); delta = ri - (x - p0) . n
+    B.dv = vrb;
+    B.wi = cross(C.rA, vrb);
+    rAb = add(rAb, cross(vrb, C.wi));
+    deltab += R(0.5) * dot(C.nh, rAb);
+    B.dx = mul(C.nh, -deltab);
+    B.wj = zero;
+  }
+  return B;
+}
+
+// ---------------------------------------------------------------------------------------------
+// the same contact through the engine's hertzForce on any scalar type T (plain, or dual numbers):
+// in = x_i(3) x_j(3) v_i(3) v_j(3) w_i(3) w_j(3) xi(3) E e mu; out = f(3) T_i(3) T_j(3) xi'(3)
+constexpr int kIn = 24, kOut = 12;
+template <class T, class R>
+__device__ bool contactLaw(const Model<R>& M, int i, int j, int k, const T* in, T* out) {
+  const V3<T> xi_{in[0], in[1], in[2]}, xj{in[3], in[4], in[5]}, vi{in[6], in[7], in[8]}, vj{in[9], in[10], in[11]};
+  const V3<T> wi{in[12], in[13], in[14]}, wj{in[15], in[16], in[17]};
+  V3<T> h{in[18], in[19], in[20]};
+  const T E = in[21], e = in[22], mu = in[23];
+  T eS, gS;
+  stars(E, M.nu, eS, gS);
+  const R ri = M.r[i];
+  if (j >= 0) {
+    const R rj = M.r[j];
+    const V3<T> dx = sub(xi_, xj);
+    const T dd = sqrt(dot(dx, dx));
+    const T delta = T(ri + rj) - dd;
+    if (delta <= T(0.0) || dd < T(1e-12))
+      return false;
+    const V3<T> nh = mul(dx, T(1.0) / dd);
+    const V3<T> rA = mul(nh, -(T(ri) - T(0.5) * delta));
+    const V3<T> rB = mul(nh, T(rj) - T(0.5) * delta);
+    const V3<T> vr = sub(add(vi, cross(wi, rA)), add(vj, cross(wj, rB)));
+    const R mS = R(1) / (R(1) / M.m[i] + R(1) / M.m[j]);
+    const V3<T> f = pdem::hertzForce(delta, nh, vr, T(ri * rj / (ri + rj)), T(mS), eS, gS, e, mu, T(M.dt), h);
+    const V3<T> ti = cross(rA, f), tj = cross(rB, mul(f, T(-1.0)));
+    out[0] = f.x, out[1] = f.y, out[2] = f.z, out[3] = ti.x, out[4] = ti.y, out[5] = ti.z;
+    out[6] = tj.x, out[7] = tj.y, out[8] = tj.z, out[9] = h.x, out[10] = h.y, out[11] = h.z;
+    return true;
+  }
+  const R* pl = M.planes + 6 * k;
+  const V3<T> n{T(pl[3]), T(pl[4]), T(pl[5])};
+  const T delta = T(ri) - dot(sub(xi_, V3<T>{T(pl[0]), T(pl[1]), T(pl[2])}), n);
   if (delta <= T(0.0))
     return false;
-  const V3<T> rA = pdem::mul(n, -(T(ri) - T(0.5) * delta));
-  const V3<T> vr = pdem::add(v, pdem::cross(w, rA));
-  T eS, gS;
-  stars(in[12], nu, eS, gS);
-  const V3<T> f = pdem::hertzForce(delta, n, vr, T(ri), T(mi), eS, gS, in[13], in[14], T(dt), xi);
-  const V3<T> t = pdem::cross(rA, f);
-  out[0] = f.x, out[1] = f.y, out[2] = f.z;
-  out[3] = t.x, out[4] = t.y, out[5] = t.z;
-  out[6] = xi.x, out[7] = xi.y, out[8] = xi.z;
+  const V3<T> rA = mul(n, -(T(ri) - T(0.5) * delta));
+  const V3<T> vr = add(vi, cross(wi, rA));
+  const V3<T> f = pdem::hertzForce(delta, n, vr, T(ri), T(M.m[i]), eS, gS, e, mu, T(M.dt), h);
+  const V3<T> t = cross(rA, f);
+  out[0] = f.x, out[1] = f.y, out[2] = f.z, out[3] = t.x, out[4] = t.y, out[5] = t.z;
+  out[6] = out[7] = out[8] = T(0.0);
+  out[9] = h.x, out[10] = h.y, out[11] = h.z;
   return true;
 }
 
+// ---------------------------------------------------------------------------------------------
+// forward: contact forces into F, T (atomics), new histories; then the kick-drift, which also
+// clears F, T for the next substep (they are cleared once at the window start)
 template <class R>
-struct StateView {
-  R *x, *v, *w, *xiP, *xiW;  // xiP: 3 per pair, xiW: 3 per (sphere, plane), sphere-major
-};
-inline size_t stateSize(long n, long npair, long nplane) { return (size_t)(9 * n + 3 * npair + 3 * n * nplane); }
-template <class R>
-StateView<R> view(R* base, long n, long npair) {
-  StateView<R> s;
-  s.x = base;
-  s.v = base + 3 * n;
-  s.w = base + 6 * n;
-  s.xiP = base + 9 * n;
-  s.xiW = s.xiP + 3 * npair;
-  return s;
-}
-
-template <class R>
-struct Model {
-  int n, npair, nplane;
-  const int* pairs;  // [npair] (i, j), i < j
-  const R *planes, *r, *m, *I;
-  R E, e, mu, dt, g[3];
-  double nu;
-};
-
-// ---- forward ----
-template <class R>
-__global__ void kPairForces(Model<R> M, StateView<R> s, StateView<R> t, R* F, R* T) {
-  GRID_STRIDE(p, M.npair) {
-    const int i = M.pairs[2 * p], j = M.pairs[2 * p + 1];
-    R in[kPairIn], out[kPairOut];
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      in[a] = s.x[3 * i + a] - s.x[3 * j + a];
-      in[3 + a] = s.v[3 * i + a] - s.v[3 * j + a];
-      in[6 + a] = s.w[3 * i + a];
-      in[9 + a] = s.w[3 * j + a];
-      in[12 + a] = s.xiP[3 * p + a];
-    }
-    in[15] = M.E, in[16] = M.e, in[17] = M.mu;
-    const R mS = R(1) / (R(1) / M.m[i] + R(1) / M.m[j]);
-    if (!pairLaw<R, R>(in, M.r[i], M.r[j], mS, M.nu, M.dt, out)) {
-      t.xiP[3 * p] = t.xiP[3 * p + 1] = t.xiP[3 * p + 2] = R(0);
+__global__ void kContacts(Model<R> M, StateView<R> s, StateView<R> t, R* F, R* T) {
+  GRID_STRIDE(c, M.nc) {
+    Contact<R> C;
+    contactPrimal(M, c, s, C);
+    if (!C.active) {
+      st3(t.xi, c, V3<R>{R(0), R(0), R(0)});
       continue;
     }
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      atomicAdd(&F[3 * i + a], out[a]);
-      atomicAdd(&F[3 * j + a], -out[a]);
-      atomicAdd(&T[3 * i + a], out[3 + a]);
-      atomicAdd(&T[3 * j + a], out[6 + a]);
-      t.xiP[3 * p + a] = out[9 + a];
+    st3(t.xi, c, C.xi3);
+    atomicAdd3(F, C.i, C.f);
+    atomicAdd3(T, C.i, cross(C.rA, C.f));
+    if (C.j >= 0) {
+      atomicAdd3(F, C.j, mul(C.f, R(-1)));
+      atomicAdd3(T, C.j, cross(C.rB, mul(C.f, R(-1))));
     }
   }
 }
-// plane contacts and the kick-drift of each sphere (one thread per sphere, planes in order)
 template <class R>
-__global__ void kPlanesIntegrate(Model<R> M, StateView<R> s, StateView<R> t, const R* F, const R* T) {
+__global__ void kIntegrate(Model<R> M, StateView<R> s, StateView<R> t, R* F, R* T) {
   GRID_STRIDE(i, M.n) {
-    R f[3] = {F[3 * i], F[3 * i + 1], F[3 * i + 2]}, tq[3] = {T[3 * i], T[3 * i + 1], T[3 * i + 2]};
-    const R ri = M.r[i], mi = M.m[i];
-    for (int k = 0; k < M.nplane; ++k) {
-      const long q = i * M.nplane + k;
-      R in[kPlaneIn], out[kPlaneOut];
-#pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        in[a] = s.x[3 * i + a];
-        in[3 + a] = s.v[3 * i + a];
-        in[6 + a] = s.w[3 * i + a];
-        in[9 + a] = s.xiW[3 * q + a];
-      }
-      in[12] = M.E, in[13] = M.e, in[14] = M.mu;
-      if (!planeLaw<R, R>(in, M.planes + 6 * k, ri, mi, M.nu, M.dt, out)) {
-        t.xiW[3 * q] = t.xiW[3 * q + 1] = t.xiW[3 * q + 2] = R(0);
-        continue;
-      }
-#pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        f[a] += out[a];
-        tq[a] += out[3 + a];
-        t.xiW[3 * q + a] = out[6 + a];
-      }
-    }
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      const R v = s.v[3 * i + a] + (f[a] / mi + M.g[a]) * M.dt;
-      t.v[3 * i + a] = v;
-      t.w[3 * i + a] = s.w[3 * i + a] + tq[a] / M.I[i] * M.dt;
-      t.x[3 * i + a] = s.x[3 * i + a] + v * M.dt;
-    }
+    // every load before the first store: the compiler cannot prove the buffers apart
+    const R mi = M.m[i], Ii = M.I[i];
+    const V3<R> x = ld3(s.x, i), v = ld3(s.v, i), w = ld3(s.w, i), f = ld3(F, i), tq = ld3(T, i);
+    const V3<R> v1{v.x + (f.x / mi + M.g[0]) * M.dt, v.y + (f.y / mi + M.g[1]) * M.dt,
+                   v.z + (f.z / mi + M.g[2]) * M.dt};
+    st3(t.v, i, v1);
+    st3(t.w, i, V3<R>{w.x + tq.x / Ii * M.dt, w.y + tq.y / Ii * M.dt, w.z + tq.z / Ii * M.dt});
+    st3(t.x, i, V3<R>{x.x + v1.x * M.dt, x.y + v1.y * M.dt, x.z + v1.z * M.dt});
+    st3(F, i, V3<R>{R(0), R(0), R(0)});
+    st3(T, i, V3<R>{R(0), R(0), R(0)});
   }
 }
 
 // ---- adjoint ----
+// b0.{x,v,w} = b1 carried back through x' = x + v' dt, v' = v + ..., w' = w + ...;
+// Fb, Tb = adjoints of the substep's force and torque sums
+template <class R>
+__global__ void kIntegrateAdj(Model<R> M, StateView<R> b1, StateView<R> b0, R* Fb, R* Tb) {
+  GRID_STRIDE(i, M.n) {
+    const R mi = M.m[i], Ii = M.I[i];
+    const V3<R> xb = ld3(b1.x, i), vb = ld3(b1.v, i), wb = ld3(b1.w, i);
+    const V3<R> vbt = add(vb, mul(xb, M.dt));  // v' feeds x' = x + v' dt
+    st3(b0.x, i, xb);
+    st3(b0.v, i, vbt);
+    st3(b0.w, i, wb);
+    st3(Fb, i, V3<R>{vbt.x * M.dt / mi, vbt.y * M.dt / mi, vbt.z * M.dt / mi});
+    st3(Tb, i, V3<R>{wb.x * M.dt / Ii, wb.y * M.dt / Ii, wb.z * M.dt / Ii});
+  }
+}
 __device__ inline void flushParams(double* thetaB, double gE, double ge, double gmu) {
   for (int o = 16; o > 0; o >>= 1) {
     gE += __shfl_xor_sync(0xffffffffu, gE, o);
@@ -296,191 +515,285 @@ __device__ inline void flushParams(double* thetaB, double gE, double ge, double 
     atomicAdd(&thetaB[2], gmu);
   }
 }
-// Integration: b0.{x,v,w} = b1 carried back through x' = x + v' dt, v' = v + ..., w' = w + ...;
-// Fb, Tb = adjoints of the substep's force and torque sums. Plane contacts are reversed here too
-// (one thread per sphere) into b0 and the plane history adjoints. Warps iterate in lockstep so the
-// parameter sums can be reduced with shuffles.
-template <class R, class S>
-__global__ void kIntegratePlanesAdj(Model<R> M, StateView<R> s, StateView<R> b1, StateView<R> b0, R* Fb, R* Tb,
-                                    double* thetaB) {
-  double gE = 0, ge = 0, gmu = 0;
-  const long n = M.n;
-  for (long i0 = (long)blockIdx.x * blockDim.x + threadIdx.x - (threadIdx.x & 31); i0 < n;
-       i0 += (long)gridDim.x * blockDim.x) {
-    const long i = i0 + (threadIdx.x & 31);
-    if (i < n) {
-      R xb[3], vb[3], wb[3], fb[3], tb[3];
-      const R mi = M.m[i], ri = M.r[i];
-#pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        const R vbt = b1.v[3 * i + a] + M.dt * b1.x[3 * i + a];  // v' feeds x' = x + v' dt
-        xb[a] = b1.x[3 * i + a];
-        vb[a] = vbt;
-        wb[a] = b1.w[3 * i + a];
-        fb[a] = vbt * M.dt / mi;
-        tb[a] = b1.w[3 * i + a] * M.dt / M.I[i];
-        Fb[3 * i + a] = fb[a];
-        Tb[3 * i + a] = tb[a];
-      }
-      for (int k = 0; k < M.nplane; ++k) {
-        const long q = i * M.nplane + k;
-        // contact test on plain values first: an inactive contact has a zero Jacobian apart from
-        // the cleared history, whose adjoint is zero
-        const R* pl = M.planes + 6 * k;
-        const R dist =
-            (s.x[3 * i] - pl[0]) * pl[3] + (s.x[3 * i + 1] - pl[1]) * pl[4] + (s.x[3 * i + 2] - pl[2]) * pl[5];
-        if (!(ri - dist > R(0))) {
-          b0.xiW[3 * q] = b0.xiW[3 * q + 1] = b0.xiW[3 * q + 2] = R(0);
-          continue;
-        }
-        Dn<S, kPlaneIn> in[kPlaneIn], out[kPlaneOut];
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-          in[a] = Dn<S, kPlaneIn>(s.x[3 * i + a]);
-          in[3 + a] = Dn<S, kPlaneIn>(s.v[3 * i + a]);
-          in[6 + a] = Dn<S, kPlaneIn>(s.w[3 * i + a]);
-          in[9 + a] = Dn<S, kPlaneIn>(s.xiW[3 * q + a]);
-        }
-        in[12] = Dn<S, kPlaneIn>(M.E), in[13] = Dn<S, kPlaneIn>(M.e), in[14] = Dn<S, kPlaneIn>(M.mu);
-#pragma unroll
-        for (int c = 0; c < kPlaneIn; ++c)
-          in[c].d[c] = S(1);
-        if (!planeLaw<Dn<S, kPlaneIn>, R>(in, pl, ri, mi, M.nu, M.dt, out)) {
-          b0.xiW[3 * q] = b0.xiW[3 * q + 1] = b0.xiW[3 * q + 2] = R(0);
-          continue;
-        }
-        S yb[kPlaneOut];
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-          yb[a] = fb[a];
-          yb[3 + a] = tb[a];
-          yb[6 + a] = b1.xiW[3 * q + a];
-        }
-        S cb[kPlaneIn];
-#pragma unroll
-        for (int c = 0; c < kPlaneIn; ++c) {
-          S acc = 0;
-#pragma unroll
-          for (int o = 0; o < kPlaneOut; ++o)
-            acc += out[o].d[c] * yb[o];
-          cb[c] = acc;
-        }
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-          xb[a] += R(cb[a]);
-          vb[a] += R(cb[3 + a]);
-          wb[a] += R(cb[6 + a]);
-          b0.xiW[3 * q + a] = R(cb[9 + a]);
-        }
-        gE += cb[12], ge += cb[13], gmu += cb[14];
-      }
-      // pair contributions are added to b0.{x,v,w} with atomics by kPairAdj, which runs after this
-#pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        b0.x[3 * i + a] = xb[a];
-        b0.v[3 * i + a] = vb[a];
-        b0.w[3 * i + a] = wb[a];
-      }
-    }
-  }
-  flushParams(thetaB, gE, ge, gmu);
-}
-template <class R, class S>
-__global__ void kPairAdj(Model<R> M, StateView<R> s, StateView<R> b1, StateView<R> b0, const R* Fb, const R* Tb,
-                         double* thetaB) {
-  double gE = 0, ge = 0, gmu = 0;
-  for (long p0 = (long)blockIdx.x * blockDim.x + threadIdx.x - (threadIdx.x & 31); p0 < M.npair;
-       p0 += (long)gridDim.x * blockDim.x) {
-    const long p = p0 + (threadIdx.x & 31);
-    if (p < M.npair) {
-      const int i = M.pairs[2 * p], j = M.pairs[2 * p + 1];
-      const R ri = M.r[i], rj = M.r[j];
-      R dx[3];
-#pragma unroll
-      for (int a = 0; a < 3; ++a)
-        dx[a] = s.x[3 * i + a] - s.x[3 * j + a];
-      const R dd = ::sqrt(dx[0] * dx[0] + dx[1] * dx[1] + dx[2] * dx[2]);
-      if (!(ri + rj - dd > R(0)) || dd < R(1e-12)) {
-        b0.xiP[3 * p] = b0.xiP[3 * p + 1] = b0.xiP[3 * p + 2] = R(0);
-        continue;
-      }
-      Dn<S, kPairIn> in[kPairIn], out[kPairOut];
-#pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        in[a] = Dn<S, kPairIn>(dx[a]);
-        in[3 + a] = Dn<S, kPairIn>(s.v[3 * i + a] - s.v[3 * j + a]);
-        in[6 + a] = Dn<S, kPairIn>(s.w[3 * i + a]);
-        in[9 + a] = Dn<S, kPairIn>(s.w[3 * j + a]);
-        in[12 + a] = Dn<S, kPairIn>(s.xiP[3 * p + a]);
-      }
-      in[15] = Dn<S, kPairIn>(M.E), in[16] = Dn<S, kPairIn>(M.e), in[17] = Dn<S, kPairIn>(M.mu);
-#pragma unroll
-      for (int k = 0; k < kPairIn; ++k)
-        in[k].d[k] = S(1);
-      const R mS = R(1) / (R(1) / M.m[i] + R(1) / M.m[j]);
-      if (!pairLaw<Dn<S, kPairIn>, R>(in, ri, rj, mS, M.nu, M.dt, out)) {
-        b0.xiP[3 * p] = b0.xiP[3 * p + 1] = b0.xiP[3 * p + 2] = R(0);
-        continue;
-      }
-      S yb[kPairOut];
-#pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        yb[a] = Fb[3 * i + a] - Fb[3 * j + a];  // f acts on i, -f on j
-        yb[3 + a] = Tb[3 * i + a];
-        yb[6 + a] = Tb[3 * j + a];
-        yb[9 + a] = b1.xiP[3 * p + a];
-      }
-      S cb[kPairIn];
-#pragma unroll
-      for (int k = 0; k < kPairIn; ++k) {
-        S acc = 0;
-#pragma unroll
-        for (int o = 0; o < kPairOut; ++o)
-          acc += out[o].d[k] * yb[o];
-        cb[k] = acc;
-      }
-#pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        atomicAdd(&b0.x[3 * i + a], R(cb[a]));
-        atomicAdd(&b0.x[3 * j + a], R(-cb[a]));
-        atomicAdd(&b0.v[3 * i + a], R(cb[3 + a]));
-        atomicAdd(&b0.v[3 * j + a], R(-cb[3 + a]));
-        atomicAdd(&b0.w[3 * i + a], R(cb[6 + a]));
-        atomicAdd(&b0.w[3 * j + a], R(cb[9 + a]));
-        b0.xiP[3 * p + a] = R(cb[12 + a]);
-      }
-      gE += cb[15], ge += cb[16], gmu += cb[17];
-    }
-  }
-  flushParams(thetaB, gE, ge, gmu);
-}
-
-// candidate pairs within scenes: i < j < end[i] (end = exclusive end of i's scene range),
-// |x_i - x_j| < r_i + r_j + skin; pass 1 counts per sphere, pass 2 writes at off[i]
+// contact adjoints (hand reversal): one thread per contact; warps iterate in lockstep so the
+// parameter sums reduce with shuffles
 template <class R>
-__global__ void kCandPairs(const R* x, const R* r, const int* end, int n, R skin, int* cnt, const int* off,
-                           int* out) {
-  GRID_STRIDE(i, n) {
-    int c = 0;
-    const int base = off ? off[i] : 0;
-    const int last = end ? end[i] : n;
-    const R xi = x[3 * i], yi = x[3 * i + 1], zi = x[3 * i + 2], ri = r[i];
-    for (int j = (int)i + 1; j < last; ++j) {
-      const R dx = xi - x[3 * j], dy = yi - x[3 * j + 1], dz = zi - x[3 * j + 2];
-      const R lim = ri + r[j] + skin;
-      if (dx * dx + dy * dy + dz * dz < lim * lim) {
-        if (off) {
-          out[2 * (base + c)] = (int)i;
-          out[2 * (base + c) + 1] = j;
+__global__ void kContactsAdj(Model<R> M, StateView<R> s, StateView<R> b1, StateView<R> b0, const R* Fb,
+                             const R* Tb, double* thetaB) {
+  double gE = 0, ge = 0, gmu = 0;
+  for (long c0 = (long)blockIdx.x * blockDim.x + threadIdx.x - (threadIdx.x & 31); c0 < M.nc;
+       c0 += (long)gridDim.x * blockDim.x) {
+    const long c = c0 + (threadIdx.x & 31);
+    if (c < M.nc) {
+      Contact<R> C;
+      contactPrimal(M, c, s, C);
+      if (!C.active) {
+        st3(b0.xi, c, V3<R>{R(0), R(0), R(0)});  // cleared history: no dependence on the old one
+      } else {
+        const int i = C.i, j = C.j;
+        V3<R> fb = ld3(Fb, i);
+        V3<R> tBb{R(0), R(0), R(0)};
+        if (j >= 0) {
+          fb = sub(fb, ld3(Fb, j));  // f acts on i, -f on j
+          tBb = ld3(Tb, j);
         }
-        ++c;
+        const ContactBar<R> B = contactReverse(M, C, fb, ld3(Tb, i), tBb, ld3(b1.xi, c));
+        st3(b0.xi, c, B.xi);
+        atomicAdd3(b0.x, i, B.dx);
+        atomicAdd3(b0.v, i, B.dv);
+        atomicAdd3(b0.w, i, B.wi);
+        if (j >= 0) {
+          atomicAdd3(b0.x, j, mul(B.dx, R(-1)));
+          atomicAdd3(b0.v, j, mul(B.dv, R(-1)));
+          atomicAdd3(b0.w, j, B.wj);
+        }
+        gE += B.E, ge += B.e, gmu += B.mu;
       }
     }
-    if (!off)
-      cnt[i] = c;
+  }
+  flushParams(thetaB, gE, ge, gmu);
+}
+// contact adjoints from the local Jacobian by dual numbers through hertzForce (the cross-check)
+template <class R>
+__global__ void kContactsAdjDual(Model<R> M, StateView<R> s, StateView<R> b1, StateView<R> b0, const R* Fb,
+                                 const R* Tb, double* thetaB) {
+  double gE = 0, ge = 0, gmu = 0;
+  for (long c0 = (long)blockIdx.x * blockDim.x + threadIdx.x - (threadIdx.x & 31); c0 < M.nc;
+       c0 += (long)gridDim.x * blockDim.x) {
+    const long c = c0 + (threadIdx.x & 31);
+    if (c < M.nc) {
+      const int i = M.cont[2 * c], j = M.cont[2 * c + 1], k = j < 0 ? -j - 1 : -1;
+      const int jj = j >= 0 ? j : i;  // a plane reads sphere i in the j slots (unused)
+      Dn<R, kIn> in[kIn], out[kOut];
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        in[a] = Dn<R, kIn>(s.x[3 * i + a]);
+        in[3 + a] = Dn<R, kIn>(s.x[3 * jj + a]);
+        in[6 + a] = Dn<R, kIn>(s.v[3 * i + a]);
+        in[9 + a] = Dn<R, kIn>(s.v[3 * jj + a]);
+        in[12 + a] = Dn<R, kIn>(s.w[3 * i + a]);
+        in[15 + a] = Dn<R, kIn>(s.w[3 * jj + a]);
+        in[18 + a] = Dn<R, kIn>(s.xi[3 * c + a]);
+      }
+      in[21] = Dn<R, kIn>(M.E), in[22] = Dn<R, kIn>(M.e), in[23] = Dn<R, kIn>(M.mu);
+#pragma unroll
+      for (int q = 0; q < kIn; ++q)
+        in[q].d[q] = R(1);
+      if (!contactLaw<Dn<R, kIn>, R>(M, i, j, k, in, out)) {
+        st3(b0.xi, c, V3<R>{R(0), R(0), R(0)});
+      } else {
+        R yb[kOut];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          yb[a] = Fb[3 * i + a] - (j >= 0 ? Fb[3 * j + a] : R(0));
+          yb[3 + a] = Tb[3 * i + a];
+          yb[6 + a] = j >= 0 ? Tb[3 * j + a] : R(0);
+          yb[9 + a] = b1.xi[3 * c + a];
+        }
+        R cb[kIn];
+#pragma unroll
+        for (int q = 0; q < kIn; ++q) {
+          R acc = 0;
+#pragma unroll
+          for (int o = 0; o < kOut; ++o)
+            acc += out[o].d[q] * yb[o];
+          cb[q] = acc;
+        }
+        atomicAdd3(b0.x, i, V3<R>{cb[0], cb[1], cb[2]});
+        atomicAdd3(b0.v, i, V3<R>{cb[6], cb[7], cb[8]});
+        atomicAdd3(b0.w, i, V3<R>{cb[12], cb[13], cb[14]});
+        if (j >= 0) {
+          atomicAdd3(b0.x, j, V3<R>{cb[3], cb[4], cb[5]});
+          atomicAdd3(b0.v, j, V3<R>{cb[9], cb[10], cb[11]});
+          atomicAdd3(b0.w, j, V3<R>{cb[15], cb[16], cb[17]});
+        }
+        st3(b0.xi, c, V3<R>{cb[18], cb[19], cb[20]});
+        gE += cb[21], ge += cb[22], gmu += cb[23];
+      }
+    }
+  }
+  flushParams(thetaB, gE, ge, gmu);
+}
+
+// ---- tangent-linear (forward mode, one tangent) ----
+template <class R>
+__global__ void kContactsJvp(Model<R> M, StateView<R> s, StateView<R> sd, StateView<R> t, StateView<R> td, R Ed,
+                             R ed, R mud, R* F, R* T, R* Fd, R* Td) {
+  GRID_STRIDE(c, M.nc) {
+    const int i = M.cont[2 * c], j = M.cont[2 * c + 1], k = j < 0 ? -j - 1 : -1;
+    const int jj = j >= 0 ? j : i;
+    Dn<R, 1> in[kIn], out[kOut];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      in[a].v = s.x[3 * i + a], in[a].d[0] = sd.x[3 * i + a];
+      in[3 + a].v = s.x[3 * jj + a], in[3 + a].d[0] = sd.x[3 * jj + a];
+      in[6 + a].v = s.v[3 * i + a], in[6 + a].d[0] = sd.v[3 * i + a];
+      in[9 + a].v = s.v[3 * jj + a], in[9 + a].d[0] = sd.v[3 * jj + a];
+      in[12 + a].v = s.w[3 * i + a], in[12 + a].d[0] = sd.w[3 * i + a];
+      in[15 + a].v = s.w[3 * jj + a], in[15 + a].d[0] = sd.w[3 * jj + a];
+      in[18 + a].v = s.xi[3 * c + a], in[18 + a].d[0] = sd.xi[3 * c + a];
+    }
+    in[21].v = M.E, in[21].d[0] = Ed;
+    in[22].v = M.e, in[22].d[0] = ed;
+    in[23].v = M.mu, in[23].d[0] = mud;
+    if (!contactLaw<Dn<R, 1>, R>(M, i, j, k, in, out)) {
+      st3(t.xi, c, V3<R>{R(0), R(0), R(0)});
+      st3(td.xi, c, V3<R>{R(0), R(0), R(0)});
+      continue;
+    }
+    st3(t.xi, c, V3<R>{out[9].v, out[10].v, out[11].v});
+    st3(td.xi, c, V3<R>{out[9].d[0], out[10].d[0], out[11].d[0]});
+    atomicAdd3(F, i, V3<R>{out[0].v, out[1].v, out[2].v});
+    atomicAdd3(Fd, i, V3<R>{out[0].d[0], out[1].d[0], out[2].d[0]});
+    atomicAdd3(T, i, V3<R>{out[3].v, out[4].v, out[5].v});
+    atomicAdd3(Td, i, V3<R>{out[3].d[0], out[4].d[0], out[5].d[0]});
+    if (j >= 0) {
+      atomicAdd3(F, j, V3<R>{-out[0].v, -out[1].v, -out[2].v});
+      atomicAdd3(Fd, j, V3<R>{-out[0].d[0], -out[1].d[0], -out[2].d[0]});
+      atomicAdd3(T, j, V3<R>{out[6].v, out[7].v, out[8].v});
+      atomicAdd3(Td, j, V3<R>{out[6].d[0], out[7].d[0], out[8].d[0]});
+    }
+  }
+}
+template <class R>
+__global__ void kIntegrateJvp(Model<R> M, StateView<R> s, StateView<R> sd, StateView<R> t, StateView<R> td, R* F,
+                              R* T, R* Fd, R* Td) {
+  GRID_STRIDE(i, M.n) {
+    const R mi = M.m[i], Ii = M.I[i];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const long q = 3 * i + a;
+      const R v = s.v[q] + (F[q] / mi + M.g[a]) * M.dt;
+      const R vd = sd.v[q] + Fd[q] / mi * M.dt;
+      t.v[q] = v, td.v[q] = vd;
+      t.w[q] = s.w[q] + T[q] / Ii * M.dt, td.w[q] = sd.w[q] + Td[q] / Ii * M.dt;
+      t.x[q] = s.x[q] + v * M.dt, td.x[q] = sd.x[q] + vd * M.dt;
+      F[q] = T[q] = Fd[q] = Td[q] = R(0);
+    }
   }
 }
 
+// Candidate contacts, `split` blocks per scene [first[s], first[s + 1]): for each sphere i of the
+// scene, the spheres i < j of the scene with |x_i - x_j| < r_i + r_j + skin, then the planes k with
+// (x_i - p0_k).n_k < r_i + skin, in that order. Each block stages the scene's positions and radii
+// in shared memory (structure of arrays: a warp reads consecutive entries) when they fit (SMEM),
+// else reads global memory. Rows are dealt in pairs (q, ns - 1 - q) so every thread scans about
+// ns / 2 partners; block b of a scene takes the pairs q = b, b + split, ... Pass 1 (off ==
+// nullptr) writes each sphere's count; pass 2 writes its contacts at off[i].
+constexpr int kCandBlock = 256;
+template <class R, bool SMEM>
+__global__ void __launch_bounds__(kCandBlock) kCandScene(const R* x, const R* r, const int* first, int split,
+                                                         const R* planes, int nplane, R skin, int* cnt, const int* off,
+                                                         int* out) {
+  extern __shared__ __align__(16) unsigned char smRaw[];
+  const int scene = blockIdx.x / split, part = blockIdx.x % split;
+  const int a = first[scene], ns = first[scene + 1] - a;
+  R* sx = reinterpret_cast<R*>(smRaw);
+  R *sy = sx + ns, *sz = sy + ns, *sr = sz + ns;
+  if (SMEM) {
+    for (int q = threadIdx.x; q < ns; q += blockDim.x) {
+      sx[q] = x[3 * (a + q)], sy[q] = x[3 * (a + q) + 1], sz[q] = x[3 * (a + q) + 2];
+      sr[q] = r[a + q];
+    }
+    __syncthreads();
+  }
+  auto px = [&](int q) { return SMEM ? sx[q] : x[3 * (a + q)]; };
+  auto py = [&](int q) { return SMEM ? sy[q] : x[3 * (a + q) + 1]; };
+  auto pz = [&](int q) { return SMEM ? sz[q] : x[3 * (a + q) + 2]; };
+  auto pr = [&](int q) { return SMEM ? sr[q] : r[a + q]; };
+  const int half = (ns + 1) / 2;
+  for (int q = part * blockDim.x + threadIdx.x; q < half; q += split * blockDim.x) {
+    for (int h = 0; h < 2; ++h) {
+      const int li = h == 0 ? q : ns - 1 - q;
+      if (h == 1 && li == q)
+        break;
+      const int i = a + li;
+      const R xi = px(li), yi = py(li), zi = pz(li), ri = pr(li) + skin;
+      int c = 0;
+      const int base = off ? off[i] : 0;
+      for (int lj = li + 1; lj < ns; ++lj) {
+        const R dx = xi - px(lj), dy = yi - py(lj), dz = zi - pz(lj);
+        const R lim = ri + pr(lj);
+        if (dx * dx + dy * dy + dz * dz < lim * lim) {
+          if (off) {
+            out[2 * (base + c)] = i;
+            out[2 * (base + c) + 1] = a + lj;
+          }
+          ++c;
+        }
+      }
+      for (int k = 0; k < nplane; ++k) {
+        const R* pl = planes + 6 * k;
+        const R dist = (xi - pl[0]) * pl[3] + (yi - pl[1]) * pl[4] + (zi - pl[2]) * pl[5];
+        if (dist < ri) {
+          if (off) {
+            out[2 * (base + c)] = i;
+            out[2 * (base + c) + 1] = -k - 1;
+          }
+          ++c;
+        }
+      }
+      if (!off)
+        cnt[i] = c;
+    }
+  }
+}
+// exclusive prefix sum of cnt[0, n) into off[0, n], off[n] = total; one block walks the array in
+// chunks of blockDim x kScanItems (each thread sums kScanItems consecutive counts, the block scans
+// the thread sums with warp shuffles, a running carry joins the chunks)
+constexpr int kScanBlock = 1024, kScanItems = 16;
+__global__ void __launch_bounds__(kScanBlock) kScanCounts(const int* cnt, int n, int* off) {
+  __shared__ int warpSum[kScanBlock / 32];
+  __shared__ long long carry;
+  if (threadIdx.x == 0)
+    carry = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (long base = 0; base < n; base += (long)blockDim.x * kScanItems) {
+    const long first = base + (long)threadIdx.x * kScanItems;
+    int item[kScanItems];
+    int v = 0;
+#pragma unroll
+    for (int q = 0; q < kScanItems; ++q) {
+      item[q] = first + q < n ? cnt[first + q] : 0;
+      v += item[q];
+    }
+    int incl = v;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int u = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o)
+        incl += u;
+    }
+    if (lane == 31)
+      warpSum[wid] = incl;
+    __syncthreads();
+    if (wid == 0) {
+      int ws = lane < (int)(blockDim.x >> 5) ? warpSum[lane] : 0;
+      for (int o = 1; o < 32; o <<= 1) {
+        const int u = __shfl_up_sync(0xffffffffu, ws, o);
+        if (lane >= o)
+          ws += u;
+      }
+      warpSum[lane] = ws;  // inclusive over warps
+    }
+    __syncthreads();
+    long long run = carry + (wid > 0 ? warpSum[wid - 1] : 0) + incl - v;
+#pragma unroll
+    for (int q = 0; q < kScanItems; ++q) {
+      if (first + q < n)
+        off[first + q] = (int)run;
+      run += item[q];
+    }
+    __syncthreads();
+    if (threadIdx.x == blockDim.x - 1)
+      carry = run;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    off[n] = (int)carry;
+}
+
+// ---------------------------------------------------------------------------------------------
 struct Fail {
   int status;
   std::string msg;
@@ -491,16 +804,16 @@ void check(cudaError_t e, const char* what) {
 }
 template <class R>
 Model<R> makeModel(const pdem_hz_model* h) {
-  if (!h || h->n < 0 || h->npair < 0 || h->nplane < 0)
+  if (!h || h->n < 0 || h->ncontact < 0 || h->nplane < 0)
     throw Fail{PDEM_ERR_INVALID, "hz model: negative sizes"};
   if (h->n > 0 && (!h->radius || !h->mass || !h->inertia))
     throw Fail{PDEM_ERR_INVALID, "hz model: radius, mass and inertia are required"};
-  if ((h->npair > 0 && !h->pairs) || (h->nplane > 0 && !h->planes))
-    throw Fail{PDEM_ERR_INVALID, "hz model: pair list or planes missing"};
+  if ((h->ncontact > 0 && !h->contacts) || (h->nplane > 0 && !h->planes))
+    throw Fail{PDEM_ERR_INVALID, "hz model: contact list or planes missing"};
   if (!(h->youngs > 0) || !(h->dt > 0))
     throw Fail{PDEM_ERR_INVALID, "hz model: Young's modulus and dt must be positive"};
   Model<R> M;
-  M.n = h->n, M.npair = h->npair, M.nplane = h->nplane, M.pairs = h->pairs;
+  M.n = h->n, M.nc = h->ncontact, M.nplane = h->nplane, M.cont = h->contacts;
   M.planes = static_cast<const R*>(h->planes);
   M.r = static_cast<const R*>(h->radius);
   M.m = static_cast<const R*>(h->mass);
@@ -523,40 +836,47 @@ void forward(const pdem_hz_model* h, int steps, int store, R* traj, R* work, cud
     return;
   if (!traj || !work)
     throw Fail{PDEM_ERR_INVALID, "hz forward: trajectory or work buffer missing"};
-  const size_t S = stateSize(M.n, M.npair, M.nplane);
+  const size_t S = stateSize(M.n, M.nc);
   R* F = work;
   R* T = work + 3 * (size_t)M.n;
+  check(cudaMemsetAsync(F, 0, 6 * (size_t)M.n * sizeof(R), st), "memset");
   for (int k = 0; k < steps; ++k) {
     const size_t a = store ? k : (k & 1), b = store ? k + 1 : ((k + 1) & 1);
-    const StateView<R> s = view(traj + S * a, M.n, M.npair), t = view(traj + S * b, M.n, M.npair);
-    check(cudaMemsetAsync(F, 0, 6 * (size_t)M.n * sizeof(R), st), "memset");
-    if (M.npair > 0)
-      kPairForces<R><<<pdem::gridFor(M.npair), pdem::kBlock, 0, st>>>(M, s, t, F, T);
-    kPlanesIntegrate<R><<<pdem::gridFor(M.n), pdem::kBlock, 0, st>>>(M, s, t, F, T);
+    const StateView<R> s = view(traj + S * a, M.n), t = view(traj + S * b, M.n);
+    if (M.nc > 0)
+      kContacts<R><<<pdem::gridFor(M.nc), pdem::kBlock, 0, st>>>(M, s, t, F, T);
+    kIntegrate<R><<<pdem::gridFor(M.n), pdem::kBlock, 0, st>>>(M, s, t, F, T);
   }
-  if (!store && (steps & 1) == 0)  // the final state of a ping-pong run always ends in slot 1
+  if (!store && (steps & 1) == 0)  // the final state of a ping-pong run always ends in block 1
     check(cudaMemcpyAsync(traj + S, traj, S * sizeof(R), cudaMemcpyDeviceToDevice, st), "D2D");
   check(cudaGetLastError(), "hz forward");
 }
 
-template <class R, class S>
-void backward(const pdem_hz_model* h, int steps, const R* traj, R* adj, double* thetaB, R* work, cudaStream_t st) {
+template <class R>
+void backward(const pdem_hz_model* h, int steps, const R* traj, R* adj, double* thetaB, R* work, int mode,
+              cudaStream_t st) {
   const Model<R> M = makeModel<R>(h);
   if (steps <= 0 || M.n == 0)
     return;
   if (!traj || !adj || !work)
     throw Fail{PDEM_ERR_INVALID, "hz backward: trajectory, adjoint or work buffer missing"};
-  const size_t SZ = stateSize(M.n, M.npair, M.nplane);
+  if (mode != 0 && mode != 1)
+    throw Fail{PDEM_ERR_INVALID, "hz backward: mode must be 0 (reversal) or 1 (dual Jacobians)"};
+  const size_t SZ = stateSize(M.n, M.nc);
   R* Fb = work;
   R* Tb = work + 3 * (size_t)M.n;
   R* other = work + 6 * (size_t)M.n;  // second adjoint state, ping-pong with adj
   R* cur = adj;
   for (int k = steps - 1; k >= 0; --k) {
-    const StateView<R> s = view(const_cast<R*>(traj) + SZ * k, M.n, M.npair);
-    const StateView<R> b1 = view(cur, M.n, M.npair), b0 = view(other, M.n, M.npair);
-    kIntegratePlanesAdj<R, S><<<pdem::gridFor(M.n), pdem::kBlock, 0, st>>>(M, s, b1, b0, Fb, Tb, thetaB);
-    if (M.npair > 0)
-      kPairAdj<R, S><<<pdem::gridFor(M.npair), pdem::kBlock, 0, st>>>(M, s, b1, b0, Fb, Tb, thetaB);
+    const StateView<R> s = view(const_cast<R*>(traj) + SZ * k, M.n);
+    const StateView<R> b1 = view(cur, M.n), b0 = view(other, M.n);
+    kIntegrateAdj<R><<<pdem::gridFor(M.n), pdem::kBlock, 0, st>>>(M, b1, b0, Fb, Tb);
+    if (M.nc > 0) {
+      if (mode == 0)
+        kContactsAdj<R><<<pdem::gridFor(M.nc), pdem::kBlock, 0, st>>>(M, s, b1, b0, Fb, Tb, thetaB);
+      else
+        kContactsAdjDual<R><<<pdem::gridFor(M.nc), pdem::kBlock, 0, st>>>(M, s, b1, b0, Fb, Tb, thetaB);
+    }
     std::swap(cur, other);
   }
   if (cur != adj)
@@ -565,25 +885,78 @@ void backward(const pdem_hz_model* h, int steps, const R* traj, R* adj, double* 
 }
 
 template <class R>
-void pairs(const R* x, const R* r, const int* end, int n, double skin, int* cnt, int* off, int* out, long cap,
-           long* count, cudaStream_t st) {
+void jvp(const pdem_hz_model* h, int steps, R* state, R* tangent, const double* thetaDot, R* work, cudaStream_t st) {
+  const Model<R> M = makeModel<R>(h);
+  if (steps <= 0 || M.n == 0)
+    return;
+  if (!state || !tangent || !thetaDot || !work)
+    throw Fail{PDEM_ERR_INVALID, "hz jvp: state, tangent, parameter tangent or work buffer missing"};
+  const size_t S = stateSize(M.n, M.nc), n3 = 3 * (size_t)M.n;
+  R *F = work, *T = work + n3, *Fd = work + 2 * n3, *Td = work + 3 * n3;
+  check(cudaMemsetAsync(work, 0, 4 * n3 * sizeof(R), st), "memset");
+  for (int k = 0; k < steps; ++k) {
+    const size_t a = k & 1, b = (k + 1) & 1;
+    const StateView<R> s = view(state + S * a, M.n), t = view(state + S * b, M.n);
+    const StateView<R> sd = view(tangent + S * a, M.n), td = view(tangent + S * b, M.n);
+    if (M.nc > 0)
+      kContactsJvp<R><<<pdem::gridFor(M.nc), pdem::kBlock, 0, st>>>(M, s, sd, t, td, R(thetaDot[0]), R(thetaDot[1]),
+                                                                     R(thetaDot[2]), F, T, Fd, Td);
+    kIntegrateJvp<R><<<pdem::gridFor(M.n), pdem::kBlock, 0, st>>>(M, s, sd, t, td, F, T, Fd, Td);
+  }
+  if ((steps & 1) == 0) {
+    check(cudaMemcpyAsync(state + S, state, S * sizeof(R), cudaMemcpyDeviceToDevice, st), "D2D");
+    check(cudaMemcpyAsync(tangent + S, tangent, S * sizeof(R), cudaMemcpyDeviceToDevice, st), "D2D");
+  }
+  check(cudaGetLastError(), "hz jvp");
+}
+
+template <class R>
+void candidates(const R* x, const R* r, const int* hFirst, const int* dFirst, int nscene, const R* planes, int nplane,
+                double skin, int* cnt, int* off, int* out, long cap, long* count, cudaStream_t st) {
   *count = 0;
-  if (n < 2)
+  if (nscene < 1)
     return;
-  kCandPairs<R><<<pdem::gridFor(n), pdem::kBlock, 0, st>>>(x, r, end, n, R(skin), cnt, nullptr, nullptr);
-  check(cudaGetLastError(), "hz pair count");
-  std::vector<int> c(n), o(n + 1, 0);
-  check(cudaMemcpyAsync(c.data(), cnt, n * sizeof(int), cudaMemcpyDeviceToHost, st), "D2H");
+  int maxScene = 0;
+  if (hFirst[0] != 0)
+    throw Fail{PDEM_ERR_INVALID, "hz contacts: scenes must start at sphere 0"};
+  for (int q = 0; q < nscene; ++q) {
+    if (hFirst[q + 1] < hFirst[q])
+      throw Fail{PDEM_ERR_INVALID, "hz contacts: scene offsets must not decrease"};
+    maxScene = std::max(maxScene, hFirst[q + 1] - hFirst[q]);
+  }
+  const int n = hFirst[nscene];
+  const size_t smem = 4 * sizeof(R) * (size_t)maxScene;
+  constexpr size_t kSmemCap = 200 * 1024;
+  const bool inSmem = smem <= kSmemCap;
+  static bool attrSet[2] = {false, false};
+  if (inSmem && !attrSet[sizeof(R) == 8]) {
+    check(cudaFuncSetAttribute(kCandScene<R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemCap),
+          "smem attribute");
+    attrSet[sizeof(R) == 8] = true;
+  }
+  // enough blocks for every SM (a few per scene), none without a row pair to scan
+  const int rows = (maxScene + 1) / 2;
+  int split = std::max(1, (4 * pdem::kNumSMs + nscene - 1) / nscene);
+  split = std::min(split, std::max(1, (rows + kCandBlock - 1) / kCandBlock * 4));
+  auto launch = [&](const int* o) {
+    if (inSmem)
+      kCandScene<R, true><<<nscene * split, kCandBlock, smem, st>>>(x, r, dFirst, split, planes, nplane, R(skin), cnt, o,
+                                                                    out);
+    else
+      kCandScene<R, false><<<nscene * split, kCandBlock, 0, st>>>(x, r, dFirst, split, planes, nplane, R(skin), cnt, o,
+                                                                  out);
+  };
+  launch(nullptr);
+  check(cudaGetLastError(), "hz candidate count");
+  kScanCounts<<<1, kScanBlock, 0, st>>>(cnt, n, off);
+  int total = 0;
+  check(cudaMemcpyAsync(&total, off + n, sizeof(int), cudaMemcpyDeviceToHost, st), "D2H");
   check(cudaStreamSynchronize(st), "sync");
-  for (int i = 0; i < n; ++i)
-    o[i + 1] = o[i] + c[i];
-  *count = o[n];
-  if (o[n] > cap || o[n] == 0)
+  *count = total;
+  if (total > cap || total == 0)
     return;
-  check(cudaMemcpyAsync(off, o.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice, st), "H2D");
-  kCandPairs<R><<<pdem::gridFor(n), pdem::kBlock, 0, st>>>(x, r, end, n, R(skin), nullptr, off, out);
-  check(cudaGetLastError(), "hz pair write");
-  check(cudaStreamSynchronize(st), "sync");  // o is released on return
+  launch(off);
+  check(cudaGetLastError(), "hz candidate write");
 }
 
 template <class F>
@@ -601,25 +974,29 @@ int guarded(F&& f) {
 
 extern "C" {
 
-long pdem_hz_state_size(int n, int npair, int nplane) {
-  return (n < 0 || npair < 0 || nplane < 0) ? -1 : (long)stateSize(n, npair, nplane);
+long pdem_hz_state_size(int n, int ncontact) {
+  return (n < 0 || ncontact < 0) ? -1 : (long)stateSize(n, ncontact);
 }
-long pdem_hz_work_size(int n, int npair, int nplane) {
-  return (n < 0 || npair < 0 || nplane < 0) ? -1 : (long)(6 * (size_t)n + stateSize(n, npair, nplane));
+long pdem_hz_work_size(int n, int ncontact) {
+  if (n < 0 || ncontact < 0)
+    return -1;
+  const size_t a = 6 * (size_t)n + stateSize(n, ncontact), b = 12 * (size_t)n;
+  return (long)(a > b ? a : b);
 }
 
-int pdem_hz_pairs(int precision, const void* d_x, const void* d_radius, const int* d_end, int n, double skin,
-                  int* d_cnt, int* d_off, int* d_pairs, long cap, long* count, void* stream) {
+int pdem_hz_contacts(int precision, const void* d_x, const void* d_radius, const int* first, const int* d_first,
+                     int nscene, const void* d_planes, int nplane, double skin, int* d_cnt, int* d_off, int* d_contacts,
+                     long cap, long* count, void* stream) {
   return guarded([&] {
-    if (!count || n < 0)
-      throw Fail{PDEM_ERR_INVALID, "hz pairs: bad arguments"};
+    if (!count || nscene < 0 || nplane < 0 || (nplane > 0 && !d_planes) || (nscene > 0 && (!d_first || !first)))
+      throw Fail{PDEM_ERR_INVALID, "hz contacts: bad arguments"};
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     if (precisionOf(precision) == 64)
-      pairs<double>(static_cast<const double*>(d_x), static_cast<const double*>(d_radius), d_end, n, skin, d_cnt, d_off,
-                    d_pairs, cap, count, st);
+      candidates<double>(static_cast<const double*>(d_x), static_cast<const double*>(d_radius), first, d_first, nscene,
+                         static_cast<const double*>(d_planes), nplane, skin, d_cnt, d_off, d_contacts, cap, count, st);
     else
-      pairs<float>(static_cast<const float*>(d_x), static_cast<const float*>(d_radius), d_end, n, skin, d_cnt, d_off,
-                   d_pairs, cap, count, st);
+      candidates<float>(static_cast<const float*>(d_x), static_cast<const float*>(d_radius), first, d_first, nscene,
+                        static_cast<const float*>(d_planes), nplane, skin, d_cnt, d_off, d_contacts, cap, count, st);
   });
 }
 
@@ -635,17 +1012,30 @@ int pdem_hz_forward(int precision, const pdem_hz_model* model, int steps, int st
 }
 
 int pdem_hz_backward(int precision, const pdem_hz_model* model, int steps, const void* d_traj, void* d_adj,
-                     double* d_grad, void* d_work, void* stream) {
+                     double* d_grad, void* d_work, int mode, void* stream) {
   return guarded([&] {
     if (!d_grad)
       throw Fail{PDEM_ERR_INVALID, "hz backward: parameter gradient buffer missing"};
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     if (precisionOf(precision) == 64)
-      backward<double, double>(model, steps, static_cast<const double*>(d_traj), static_cast<double*>(d_adj), d_grad,
-                               static_cast<double*>(d_work), st);
+      backward<double>(model, steps, static_cast<const double*>(d_traj), static_cast<double*>(d_adj), d_grad,
+                       static_cast<double*>(d_work), mode, st);
     else
-      backward<float, float>(model, steps, static_cast<const float*>(d_traj), static_cast<float*>(d_adj), d_grad,
-                             static_cast<float*>(d_work), st);
+      backward<float>(model, steps, static_cast<const float*>(d_traj), static_cast<float*>(d_adj), d_grad,
+                      static_cast<float*>(d_work), mode, st);
+  });
+}
+
+int pdem_hz_jvp(int precision, const pdem_hz_model* model, int steps, void* d_state, void* d_tangent,
+                const double* theta_dot, void* d_work, void* stream) {
+  return guarded([&] {
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (precisionOf(precision) == 64)
+      jvp<double>(model, steps, static_cast<double*>(d_state), static_cast<double*>(d_tangent), theta_dot,
+                  static_cast<double*>(d_work), st);
+    else
+      jvp<float>(model, steps, static_cast<float*>(d_state), static_cast<float*>(d_tangent), theta_dot,
+                 static_cast<float*>(d_work), st);
   });
 }
 

@@ -116,18 +116,20 @@ _SIGS = {
     "scene_counters": (C.c_long, [_vp, _dbl_p, C.c_long]),
     # candidate pairs over caller-owned device arrays, with no allocation (pdem_static.cu)
     "find_pairs_static": (C.c_int, [_vp, _vp, C.c_int, C.c_double, C.c_double, _vp, C.c_long, _long_p, _vp]),
-    # forward + adjoint of the Hertz sphere substep (pdem_adjoint.cu)
-    "hz_state_size": (C.c_long, [C.c_int, C.c_int, C.c_int]),
-    "hz_work_size": (C.c_long, [C.c_int, C.c_int, C.c_int]),
-    "hz_pairs": (C.c_int, [C.c_int, _vp, _vp, _vp, C.c_int, C.c_double, _vp, _vp, _vp, C.c_long, _long_p, _vp]),
+    # forward, adjoint and tangent-linear runs of the Hertz sphere substep (pdem_adjoint.cu)
+    "hz_state_size": (C.c_long, [C.c_int, C.c_int]),
+    "hz_work_size": (C.c_long, [C.c_int, C.c_int]),
+    "hz_contacts": (C.c_int, [C.c_int, _vp, _vp, _int_p, _vp, C.c_int, _vp, C.c_int, C.c_double, _vp, _vp, _vp,
+                              C.c_long, _long_p, _vp]),
     "hz_forward": (C.c_int, [C.c_int, _vp, C.c_int, C.c_int, _vp, _vp, _vp]),
-    "hz_backward": (C.c_int, [C.c_int, _vp, C.c_int, _vp, _vp, _vp, _vp, _vp]),
+    "hz_backward": (C.c_int, [C.c_int, _vp, C.c_int, _vp, _vp, _vp, _vp, C.c_int, _vp]),
+    "hz_jvp": (C.c_int, [C.c_int, _vp, C.c_int, _vp, _vp, _dbl_p, _vp, _vp]),
 }
 
 
 class HzModel(C.Structure):
     """pdem_hz_model (include/pdem.h): device pointers and scalars of one Hertz sphere rollout."""
-    _fields_ = [("n", C.c_int), ("npair", C.c_int), ("nplane", C.c_int), ("pairs", _vp), ("planes", _vp),
+    _fields_ = [("n", C.c_int), ("ncontact", C.c_int), ("nplane", C.c_int), ("contacts", _vp), ("planes", _vp),
                 ("radius", _vp), ("mass", _vp), ("inertia", _vp), ("youngs", C.c_double),
                 ("restitution", C.c_double), ("friction", C.c_double), ("poisson", C.c_double),
                 ("dt", C.c_double), ("gravity", C.c_double * 3)]

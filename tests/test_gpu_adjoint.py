@@ -19,10 +19,10 @@ pytestmark = pytest.mark.gpu
 torch = pytest.importorskip("torch")
 
 
-def _sim(c, precision="fp64", checkpoint=20, skin=None):
+def _sim(c, precision="fp64", checkpoint=20, skin=None, list_every=25):
     from peclet.dem.adjoint import HertzSpheres
     return HertzSpheres(c["r"], c["m"], c["I"], c["first"], c["planes"], HC.NU, HC.DT, c["g"], precision,
-                        checkpoint, skin)
+                        checkpoint, skin, list_every=list_every)
 
 
 def _oracle(c):
@@ -103,15 +103,19 @@ def test_adjoint_matches_finite_differences(gpu_api, case, steps):
     assert abs(got - fd) <= 1e-3 * abs(fd), f"{case}: v0 direction: adjoint {got} vs FD {fd}"
 
 
-def test_windows_match_one_window(gpu_api):
-    """Checkpoint windows of 7 substeps (pair lists rebuilt and histories carried by key, history
-    adjoints mapped back) give the single-window result."""
+@pytest.mark.parametrize("checkpoint,list_every", [(7, 3), (20, 6), (13, 13)])
+def test_windows_match_one_window(gpu_api, checkpoint, list_every):
+    """Contact lists rebuilt every `list_every` substeps (histories carried by key, history
+    adjoints mapped back) inside checkpoints of `checkpoint` substeps give the result of one
+    window over the whole rollout."""
     c = HC.gas()
     n = len(c["r"])
     rng = np.random.default_rng(9)
     cx, cv = rng.standard_normal((n, 3)), rng.standard_normal((n, 3))
-    a = _grads(_sim(c, checkpoint=7), c, 60, cx, cv)
-    b = _grads(_sim(c, checkpoint=1000), c, 60, cx, cv)
+    sim = _sim(c, checkpoint=checkpoint, list_every=list_every)
+    a = _grads(sim, c, 60, cx, cv)
+    assert sim.stats["windows"] > 60 // checkpoint
+    b = _grads(_sim(c, checkpoint=1000, list_every=1000), c, 60, cx, cv)
     for ga, gb in zip(a, b):
         np.testing.assert_allclose(ga, gb, rtol=1e-9, atol=1e-12 * np.abs(gb).max())
 
@@ -159,3 +163,54 @@ def test_rejects_bad_arguments(gpu_api):
     sim = _sim(c)
     with pytest.raises(ValueError):
         sim.run(_t(c["x0"], sim), _t(c["v0"], sim), _t(c["w0"], sim), (0.0, 0.7, 0.35), 5)
+
+
+def test_hand_reversal_matches_dual_jacobians(gpu_api):
+    """The hand reversal of each contact law (mode 0) against the contact's local Jacobian taken by
+    dual numbers through the engine's hertzForce (mode 1), on the same recorded rollout."""
+    c = HC.gas()
+    n = len(c["r"])
+    rng = np.random.default_rng(8)
+    sim = _sim(c)
+    (x, v, w), tape = sim.run(_t(c["x0"], sim), _t(c["v0"], sim), _t(c["w0"], sim), HC.THETA, 60, record=True)
+    g = [_t(rng.standard_normal((n, 3)), sim) for _ in range(3)]
+    a = [t.cpu().numpy() for t in sim.adjoint(tape, HC.THETA, *g, mode=0)]
+    b = [t.cpu().numpy() for t in sim.adjoint(tape, HC.THETA, *g, mode=1)]
+    for k, (ga, gb) in enumerate(zip(a, b)):
+        np.testing.assert_allclose(ga, gb, rtol=1e-10, atol=1e-12 * np.abs(gb).max(), err_msg=f"gradient {k}")
+
+
+@pytest.mark.parametrize("case,steps", CASES)
+def test_jvp_matches_oracle_dual(gpu_api, case, steps):
+    """The GPU tangent-linear run against the restatement's dual numbers, same direction."""
+    c = getattr(HC, case)()
+    n = len(c["r"])
+    rng = np.random.default_rng(12)
+    dx, dv, dw = (rng.standard_normal((n, 3)) for _ in range(3))
+    dth = np.array([1e5, 0.01, 0.01])
+    sim = _sim(c)
+    (x, v, w), (xd, vd, wd) = sim.jvp(_t(c["x0"], sim), _t(c["v0"], sim), _t(c["w0"], sim), HC.THETA,
+                                      _t(dx, sim), _t(dv, sim), _t(dw, sim), dth, steps)
+    ox, ov, ow = H.jvp(_oracle(c), c["x0"], c["v0"], c["w0"], HC.THETA, [{"x": dx, "v": dv, "w": dw, "theta": dth}],
+                       steps)
+    for got, want in ((xd, ox), (vd, ov), (wd, ow)):
+        want = want.d[..., 0]
+        np.testing.assert_allclose(got.cpu().numpy(), want, rtol=1e-8, atol=1e-10 * np.abs(want).max())
+    np.testing.assert_allclose(x.cpu().numpy(), ox.v, rtol=0, atol=1e-14)
+
+
+def test_adjoint_matches_jvp(gpu_api):
+    """<adjoint gradient, direction> = tangent-linear derivative along it, on the GPU alone."""
+    c = HC.gas()
+    n = len(c["r"])
+    rng = np.random.default_rng(13)
+    cx, cv = rng.standard_normal((n, 3)), rng.standard_normal((n, 3))
+    dx, dv, dw = (rng.standard_normal((n, 3)) for _ in range(3))
+    dth = np.array([1e5, 0.01, 0.01])
+    sim = _sim(c, checkpoint=13)
+    gx, gv, gw, gt = _grads(sim, c, 60, cx, cv)
+    _, (xd, vd, _) = sim.jvp(_t(c["x0"], sim), _t(c["v0"], sim), _t(c["w0"], sim), HC.THETA, _t(dx, sim),
+                             _t(dv, sim), _t(dw, sim), dth, 60)
+    lhs = (gx * dx).sum() + (gv * dv).sum() + (gw * dw).sum() + (gt * dth).sum()
+    rhs = (xd.cpu().numpy() * cx).sum() + (vd.cpu().numpy() * cv).sum()
+    assert abs(lhs - rhs) <= 1e-9 * abs(rhs), (lhs, rhs)
