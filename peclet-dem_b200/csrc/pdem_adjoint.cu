@@ -30,6 +30,8 @@
 #include <utility>
 #include <vector>
 
+#include <cub/cub.cuh>
+
 #include "../../include/pdem.h"
 #include "pdem_hertz.cuh"
 
@@ -738,6 +740,206 @@ __global__ void __launch_bounds__(kCandBlock) kCandScene(const R* x, const R* r,
     }
   }
 }
+// Candidate contacts on a cell grid, `split` blocks per scene, for scenes that fit in shared memory:
+// each block stages its scene (positions and radii as structure of arrays), bins the spheres into
+// cells of side h >= 2 r_max + skin over the scene's bounding box (coarser when the cells would not
+// fit), and takes the rows li = part, part + split, ... (strided over the block's threads). A row
+// scans the 27 cells around its sphere for partners j > i within r_i + r_j + skin, then the planes
+// within r_i + skin; it reserves room with one atomic and writes 64-bit keys
+// i (n + nplane) + (j, or n + plane) in no particular order (sorted afterwards). Keys past `cap`
+// are not written; *total counts them all.
+constexpr int kGridBlock = 256, kCellCap = 4096;
+template <class R>
+__global__ void __launch_bounds__(kGridBlock) kCandGrid(const R* x, const R* r, const int* first, int split, int n,
+                                                        const R* planes, int nplane, R skin, unsigned long long* keys,
+                                                        long cap, unsigned long long* total) {
+  extern __shared__ __align__(16) unsigned char smRaw[];
+  __shared__ R red[6][kGridBlock / 32];
+  __shared__ R redR[kGridBlock / 32];
+  __shared__ int cellStart[kCellCap + 1];
+  __shared__ int cursor[kCellCap];
+  __shared__ R lo[3], h;
+  __shared__ int dims[3];
+  const int scene = blockIdx.x / split, part = blockIdx.x % split;
+  const int a = first[scene], ns = first[scene + 1] - a;
+  R* sx = reinterpret_cast<R*>(smRaw);
+  R *sy = sx + ns, *sz = sy + ns, *sr = sz + ns;
+  int* order = reinterpret_cast<int*>(sr + ns);
+  R mn[3] = {R(INFINITY), R(INFINITY), R(INFINITY)}, mx[3] = {R(-INFINITY), R(-INFINITY), R(-INFINITY)}, rmax = 0;
+  for (int q = threadIdx.x; q < ns; q += blockDim.x) {
+    const R p[3] = {x[3 * (a + q)], x[3 * (a + q) + 1], x[3 * (a + q) + 2]};
+    sx[q] = p[0], sy[q] = p[1], sz[q] = p[2], sr[q] = r[a + q];
+    rmax = fmax(rmax, sr[q]);
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+      mn[c] = fmin(mn[c], p[c]), mx[c] = fmax(mx[c], p[c]);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    rmax = fmax(rmax, __shfl_xor_sync(0xffffffffu, rmax, o));
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      mn[c] = fmin(mn[c], __shfl_xor_sync(0xffffffffu, mn[c], o));
+      mx[c] = fmax(mx[c], __shfl_xor_sync(0xffffffffu, mx[c], o));
+    }
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  if (lane == 0) {
+    redR[wid] = rmax;
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+      red[c][wid] = mn[c], red[3 + c][wid] = mx[c];
+  }
+  for (int c = threadIdx.x; c < kCellCap; c += blockDim.x)
+    cursor[c] = 0;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    R m0[3] = {red[0][0], red[1][0], red[2][0]}, m1[3] = {red[3][0], red[4][0], red[5][0]}, rm = redR[0];
+    for (int w = 1; w < nw; ++w) {
+      rm = fmax(rm, redR[w]);
+      for (int c = 0; c < 3; ++c)
+        m0[c] = fmin(m0[c], red[c][w]), m1[c] = fmax(m1[c], red[3 + c][w]);
+    }
+    R side = R(2) * rm + skin;
+    if (!(side > R(0)))
+      side = R(1);
+    int d[3] = {1, 1, 1};
+    bool fit = false;
+    for (int it = 0; it < 64 && !fit; ++it) {  // coarser cells until they fit (a bounded search)
+      long cells = 1;
+      for (int c = 0; c < 3; ++c) {
+        const R ext = m1[c] - m0[c];
+        d[c] = ext > R(0) && ext < side * R(kCellCap) ? (int)(ext / side) + 1 : (ext > R(0) ? kCellCap : 1);
+        cells *= d[c];
+      }
+      fit = cells <= kCellCap;
+      if (!fit)
+        side *= R(1.26);
+    }
+    if (!fit) {  // non-finite extents: one cell holds the scene (every pair is tested)
+      d[0] = d[1] = d[2] = 1;
+      m0[0] = m0[1] = m0[2] = R(0);
+    }
+    for (int c = 0; c < 3; ++c)
+      lo[c] = m0[c], dims[c] = d[c];
+    h = side;
+  }
+  __syncthreads();
+  const int nx = dims[0], ny = dims[1], nz = dims[2], ncell = nx * ny * nz;
+  auto cellOf = [&](int q, int& cx, int& cy, int& cz) {
+    cx = min(max((int)((sx[q] - lo[0]) / h), 0), nx - 1);
+    cy = min(max((int)((sy[q] - lo[1]) / h), 0), ny - 1);
+    cz = min(max((int)((sz[q] - lo[2]) / h), 0), nz - 1);
+  };
+  for (int q = threadIdx.x; q < ns; q += blockDim.x) {
+    int cx, cy, cz;
+    cellOf(q, cx, cy, cz);
+    atomicAdd(&cursor[(cz * ny + cy) * nx + cx], 1);
+  }
+  __syncthreads();
+  {  // exclusive scan of the cell counts: kCellCap / blockDim consecutive cells per thread
+    constexpr int per = kCellCap / kGridBlock;
+    const int c0 = threadIdx.x * per;
+    int v = 0;
+    for (int q = 0; q < per; ++q)
+      v += c0 + q < ncell ? cursor[c0 + q] : 0;
+    int incl = v;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int u = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o)
+        incl += u;
+    }
+    __shared__ int wsum[kGridBlock / 32];
+    if (lane == 31)
+      wsum[wid] = incl;
+    __syncthreads();
+    int before = incl - v;
+    for (int w = 0; w < wid; ++w)
+      before += wsum[w];
+    for (int q = 0; q < per; ++q) {
+      if (c0 + q < ncell) {
+        cellStart[c0 + q] = before;
+        before += cursor[c0 + q];
+      }
+    }
+    if (threadIdx.x == blockDim.x - 1)
+      cellStart[ncell] = before;
+    __syncthreads();
+    for (int q = 0; q < per; ++q)
+      if (c0 + q < ncell)
+        cursor[c0 + q] = 0;
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < ns; q += blockDim.x) {
+    int cx, cy, cz;
+    cellOf(q, cx, cy, cz);
+    const int c = (cz * ny + cy) * nx + cx;
+    order[cellStart[c] + atomicAdd(&cursor[c], 1)] = q;
+  }
+  __syncthreads();
+  const unsigned long long np = (unsigned long long)(n + nplane);
+  for (int li = part * blockDim.x + threadIdx.x; li < ns; li += split * blockDim.x) {
+    int cx, cy, cz;
+    cellOf(li, cx, cy, cz);
+    const R xi = sx[li], yi = sy[li], zi = sz[li], ri = sr[li] + skin;
+    const int i = a + li;
+    unsigned long long base = 0;
+    for (int pass = 0; pass < 2; ++pass) {
+      int c = 0;
+      for (int dz = -1; dz <= 1; ++dz) {
+        const int zz = cz + dz;
+        if (zz < 0 || zz >= nz)
+          continue;
+        for (int dy = -1; dy <= 1; ++dy) {
+          const int yy = cy + dy;
+          if (yy < 0 || yy >= ny)
+            continue;
+          for (int dx = -1; dx <= 1; ++dx) {
+            const int xx = cx + dx;
+            if (xx < 0 || xx >= nx)
+              continue;
+            const int cell = (zz * ny + yy) * nx + xx;
+            for (int t = cellStart[cell]; t < cellStart[cell + 1]; ++t) {
+              const int lj = order[t];
+              if (lj <= li)
+                continue;
+              const R ex = xi - sx[lj], ey = yi - sy[lj], ez = zi - sz[lj];
+              const R lim = ri + sr[lj];
+              if (ex * ex + ey * ey + ez * ez < lim * lim) {
+                if (pass == 1 && base + c < (unsigned long long)cap)
+                  keys[base + c] = (unsigned long long)i * np + (unsigned long long)(a + lj);
+                ++c;
+              }
+            }
+          }
+        }
+      }
+      for (int k = 0; k < nplane; ++k) {
+        const R* pl = planes + 6 * k;
+        const R dist = (xi - pl[0]) * pl[3] + (yi - pl[1]) * pl[4] + (zi - pl[2]) * pl[5];
+        if (dist < ri) {
+          if (pass == 1 && base + c < (unsigned long long)cap)
+            keys[base + c] = (unsigned long long)i * np + (unsigned long long)(n + k);
+          ++c;
+        }
+      }
+      if (pass == 0) {
+        if (c == 0)
+          break;
+        base = atomicAdd(total, (unsigned long long)c);
+      }
+    }
+  }
+}
+// sorted keys back to (i, j) rows: j = key mod (n + nplane), a plane k when j >= n (stored -k - 1)
+__global__ void kDecodeKeys(const unsigned long long* keys, long count, int n, int nplane, int* out) {
+  GRID_STRIDE(p, count) {
+    const unsigned long long np = (unsigned long long)(n + nplane), k = keys[p];
+    const int i = (int)(k / np), j = (int)(k % np);
+    out[2 * p] = i;
+    out[2 * p + 1] = j < n ? j : -(j - n) - 1;
+  }
+}
+
 // exclusive prefix sum of cnt[0, n) into off[0, n], off[n] = total; one block walks the array in
 // chunks of blockDim x kScanItems (each thread sums kScanItems consecutive counts, the block scans
 // the thread sums with warp shuffles, a running carry joins the chunks)
@@ -910,6 +1112,24 @@ void jvp(const pdem_hz_model* h, int steps, R* state, R* tangent, const double* 
   check(cudaGetLastError(), "hz jvp");
 }
 
+// grow-only device scratch of the calling thread (one process per GPU, one stream per caller)
+struct Scratch {
+  void* p = nullptr;
+  size_t bytes = 0;
+  void* get(size_t want) {
+    if (want > bytes) {
+      if (p)
+        cudaFree(p);
+      p = nullptr;
+      bytes = 0;
+      check(cudaMalloc(&p, want), "hz scratch");
+      bytes = want;
+    }
+    return p;
+  }
+};
+thread_local Scratch gKeys, gCub, gTotal;
+
 template <class R>
 void candidates(const R* x, const R* r, const int* hFirst, const int* dFirst, int nscene, const R* planes, int nplane,
                 double skin, int* cnt, int* off, int* out, long cap, long* count, cudaStream_t st) {
@@ -925,28 +1145,53 @@ void candidates(const R* x, const R* r, const int* hFirst, const int* dFirst, in
     maxScene = std::max(maxScene, hFirst[q + 1] - hFirst[q]);
   }
   const int n = hFirst[nscene];
-  const size_t smem = 4 * sizeof(R) * (size_t)maxScene;
-  constexpr size_t kSmemCap = 200 * 1024;
-  const bool inSmem = smem <= kSmemCap;
-  static bool attrSet[2] = {false, false};
-  if (inSmem && !attrSet[sizeof(R) == 8]) {
-    check(cudaFuncSetAttribute(kCandScene<R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemCap),
-          "smem attribute");
-    attrSet[sizeof(R) == 8] = true;
+  if (n < 1)
+    return;
+  // cell-grid path: every scene staged in shared memory (positions, radii, cell order)
+  constexpr size_t kGridDyn = 160 * 1024;
+  const size_t gridSmem = (4 * sizeof(R) + sizeof(int)) * (size_t)maxScene;
+  if (gridSmem <= kGridDyn) {
+    static bool attr[2] = {false, false};
+    if (!attr[sizeof(R) == 8]) {
+      check(cudaFuncSetAttribute(kCandGrid<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGridDyn),
+            "smem attribute");
+      attr[sizeof(R) == 8] = true;
+    }
+    int split = std::max(1, (4 * pdem::kNumSMs + nscene - 1) / nscene);
+    split = std::min(split, std::max(1, (maxScene + kGridBlock - 1) / kGridBlock));
+    auto* total = static_cast<unsigned long long*>(gTotal.get(sizeof(unsigned long long)));
+    check(cudaMemsetAsync(total, 0, sizeof(unsigned long long), st), "memset");
+    auto* keys = reinterpret_cast<unsigned long long*>(out);  // cap x 2 ints = cap keys
+    kCandGrid<R><<<nscene * split, kGridBlock, gridSmem, st>>>(x, r, dFirst, split, n, planes, nplane, R(skin), keys,
+                                                               cap, total);
+    check(cudaGetLastError(), "hz candidate grid");
+    unsigned long long tot = 0;
+    check(cudaMemcpyAsync(&tot, total, sizeof(tot), cudaMemcpyDeviceToHost, st), "D2H");
+    check(cudaStreamSynchronize(st), "sync");
+    *count = (long)tot;
+    if ((long)tot > cap || tot == 0)
+      return;
+    auto* sorted = static_cast<unsigned long long*>(gKeys.get(tot * sizeof(unsigned long long)));
+    const unsigned long long maxKey = (unsigned long long)n * (unsigned long long)(n + nplane);
+    int endBit = 1;
+    while (endBit < 64 && (maxKey >> endBit))
+      ++endBit;
+    size_t bytes = 0;
+    check(cub::DeviceRadixSort::SortKeys(nullptr, bytes, keys, sorted, (int)tot, 0, endBit, st), "cub sort");
+    check(cub::DeviceRadixSort::SortKeys(gCub.get(bytes), bytes, keys, sorted, (int)tot, 0, endBit, st), "cub sort");
+    kDecodeKeys<<<pdem::gridFor((long)tot), pdem::kBlock, 0, st>>>(sorted, (long)tot, n, nplane, out);
+    check(cudaGetLastError(), "hz candidate decode");
+    return;
   }
-  // enough blocks for every SM (a few per scene), none without a row pair to scan
+  // scenes too large for shared memory: brute force over each scene from global memory, counted,
+  // scanned and written in (i, j) order
+  if (!cnt || !off)
+    throw Fail{PDEM_ERR_INVALID, "hz contacts: scenes this large need the count and offset scratch"};
   const int rows = (maxScene + 1) / 2;
   int split = std::max(1, (4 * pdem::kNumSMs + nscene - 1) / nscene);
-  split = std::min(split, std::max(1, (rows + kCandBlock - 1) / kCandBlock * 4));
-  auto launch = [&](const int* o) {
-    if (inSmem)
-      kCandScene<R, true><<<nscene * split, kCandBlock, smem, st>>>(x, r, dFirst, split, planes, nplane, R(skin), cnt, o,
-                                                                    out);
-    else
-      kCandScene<R, false><<<nscene * split, kCandBlock, 0, st>>>(x, r, dFirst, split, planes, nplane, R(skin), cnt, o,
-                                                                  out);
-  };
-  launch(nullptr);
+  split = std::min(split, std::max(1, (rows + kCandBlock - 1) / kCandBlock));
+  kCandScene<R, false><<<nscene * split, kCandBlock, 0, st>>>(x, r, dFirst, split, planes, nplane, R(skin), cnt,
+                                                              nullptr, out);
   check(cudaGetLastError(), "hz candidate count");
   kScanCounts<<<1, kScanBlock, 0, st>>>(cnt, n, off);
   int total = 0;
@@ -955,7 +1200,8 @@ void candidates(const R* x, const R* r, const int* hFirst, const int* dFirst, in
   *count = total;
   if (total > cap || total == 0)
     return;
-  launch(off);
+  kCandScene<R, false><<<nscene * split, kCandBlock, 0, st>>>(x, r, dFirst, split, planes, nplane, R(skin), cnt, off,
+                                                              out);
   check(cudaGetLastError(), "hz candidate write");
 }
 

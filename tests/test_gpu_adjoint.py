@@ -214,3 +214,39 @@ def test_adjoint_matches_jvp(gpu_api):
     lhs = (gx * dx).sum() + (gv * dv).sum() + (gw * dw).sum() + (gt * dth).sum()
     rhs = (xd.cpu().numpy() * cx).sum() + (vd.cpu().numpy() * cv).sum()
     assert abs(lhs - rhs) <= 1e-9 * abs(rhs), (lhs, rhs)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("scenes,per", [(3, 40), (2, 3000), (1, 9000)])
+def test_contact_candidates_match_brute_force(gpu_api, precision, scenes, per):
+    """Candidate lists (cell grid in shared memory, or the global-memory scan for scenes too large
+    for it) equal a brute-force enumeration, in (i, j) order with planes after spheres."""
+    rng = np.random.default_rng(scenes * 1000 + per)
+    L = 0.02 * (per / 40) ** (1 / 3)
+    n = scenes * per
+    x = rng.uniform(0, L, (n, 3))
+    r = rng.uniform(0.5e-3, 1e-3, n)
+    m, I = HC.props(r)
+    c = dict(x0=x, v0=np.zeros((n, 3)), w0=np.zeros((n, 3)), r=r, m=m, I=I, first=[per * s for s in range(scenes + 1)],
+             planes=HC.box(L), g=(0.0, 0.0, 0.0))
+    sim = _sim(c, precision)
+    skin = 0.3e-3
+    got = sim.contacts(_t(x, sim), skin).cpu().numpy()
+    xs = x.astype(np.float32).astype(np.float64) if precision == "fp32" else x
+    want = []
+    for s in range(scenes):
+        a, b = per * s, per * (s + 1)
+        for i in range(a, b):
+            d = np.linalg.norm(xs[i + 1:b] - xs[i], axis=1)
+            lim = r[i] + r[i + 1:b] + skin
+            for j in np.nonzero(d < lim)[0]:
+                want.append((i, i + 1 + j))
+            dist = [(xs[i] - np.array(p[:3])) @ np.array(p[3:]) for p in HC.box(L)]
+            for k, dk in enumerate(dist):
+                if dk < r[i] + skin:
+                    want.append((i, -k - 1))
+    want = np.array(want, dtype=np.int64).reshape(-1, 2)
+    if precision == "fp32":  # rounding at the threshold may differ: compare away from it
+        assert abs(len(got) - len(want)) <= max(3, len(want) // 1000)
+    else:
+        np.testing.assert_array_equal(got, want)
