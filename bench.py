@@ -346,6 +346,75 @@ def run_calibration(args, rank, world, dist):
                       "v U(+-0.2) m/s, E 5e6 Pa hidden / 4e6 guess, e 0.7 / 0.6, mu 0.35 / 0.3, nu 0.3, dt 2e-5 s"}
 
 
+def run_config_lines(args, dem):
+    """Throughput of the other named configurations on this GPU (device time over CUDA events on
+    the library's stream, state resident, after warm-up), each as particle-substeps/s:
+    - plain XPBD settling, 4,096 spheres, FP64, with the reference's own OpenMP build on the same
+      scene beside it (a bounded sample);
+    - the Hertz engine on the polydisperse packing (262,144 spheres), closed variant (the
+      reference's engine refuses periodic domains and planes: floor and sides are one SDF grid
+      wall), FP64 and FP32;
+    - 65,536 point-shell hollow cylinders with a 512-point stratified shell, FP64 and the
+      FP32-mixed form (box scaled so the bodies can be placed; see workloads.hollow_cylinders)."""
+    from peclet.dem import workloads as W
+
+    def timed(sim, one, steps, warm):
+        for _ in range(warm):
+            one()
+        sim.timer_start()
+        for _ in range(steps):
+            one()
+        return sim.timer_stop() / 1e3
+
+    out = {}
+    sc = W.plain_settling()
+    sim = sc.apply(dem.Simulation(sc.n + 8, "fp64"))
+    steps = 100
+    t = timed(sim, lambda: [sim.step(sc.dt) for _ in range(sc.substeps)], steps, 3)
+    line = {"workload": f"plain_settling_{sc.n}", "unit": METRIC, "dtype": "f64",
+            "value": sc.n * sc.substeps * steps / t, "ms_per_step": 1e3 * t / steps,
+            "substeps_timed": steps * sc.substeps, "contacts_last_substep": sim.num_contacts()}
+    sim.close()
+    if not args.no_cpu and os.path.exists(REF_OMP):
+        threads = os.cpu_count() or 1
+        v, el = cpu_reference(sc, 200, threads)
+        line["cpu_reference"] = {"value": v, "unit": METRIC, "cores": threads, "kind": "reference",
+                                 "sample": f"200 substeps of the same scene, {el:.1f} s"}
+    out["settling"] = line
+
+    sc, extra = W.polydisperse_hertz_closed()
+    line = {"workload": f"polydisperse_{sc.n}_closed_hertz", "unit": METRIC}
+    for prec in ("fp64", "fp32"):
+        sim = sc.apply(dem.Simulation(sc.n + 8, prec))
+        extra(sim)
+        steps = 5
+        t = timed(sim, lambda: sim.step_hertz(sc.dt, sc.substeps, 0.3), steps, 2)
+        line[prec] = {"value": sc.n * sc.substeps * steps / t, "ms_per_step": 1e3 * t / steps,
+                      "substeps_timed": steps * sc.substeps}
+        sim.close()
+    out["hertz"] = line
+
+    sc = W.hollow_cylinders(shell_points=W.hollow_cylinder_shell())
+    line = {"workload": f"hollow_cylinders_{sc.n}_shell512", "unit": METRIC,
+            "box_m": [float(v) for v in sc.domain[1]]}
+    for prec in ("fp64", "mixed"):
+        sim = sc.apply(dem.Simulation(sc.n + 8, prec))
+        steps = 3
+        t = timed(sim, lambda: [sim.step(sc.dt) for _ in range(sc.substeps)], steps, 1)
+        line[prec] = {"value": sc.n * sc.substeps * steps / t, "ms_per_step": 1e3 * t / steps,
+                      "substeps_timed": steps * sc.substeps, "contacts_last_substep": sim.num_contacts()}
+        if prec == "fp64":
+            x64 = sim.get_positions()
+        else:
+            err = np.linalg.norm(sim.get_positions() - x64, axis=1) / sc.global_scale
+            line[prec]["err_vs_fp64"] = {"max_position_error_radii": float(err.max()),
+                                         "median_position_error_radii": float(np.median(err)),
+                                         "after_substeps": (steps + 1) * sc.substeps}
+        sim.close()
+    out["shells"] = line
+    return out
+
+
 # ---------------------------------------------------------------------------------------------
 def cpu_reference(scene, substeps, threads):
     """Time the reference's own substep (OpenMP shim build) for `substeps` calls; returns
@@ -513,6 +582,7 @@ def run_ours(args):
 
     batched = run_batched(args, rank, world, dist, dem) if args.drums > 0 else None
     calib = run_calibration(args, rank, world, dist) if args.calib_scenes > 0 else None
+    configs = run_config_lines(args, dem) if (rank == 0 and not args.no_configs) else None
 
     if rank == 0:
         line = {
@@ -524,7 +594,7 @@ def run_ours(args):
             "clocks": clocks.summary(), "wall_ms_per_step": 1e3 * wall / args.steps,
             "stages_ms_per_step": {k: round(v[0], 4) for k, v in per_step.items()},
             "counts_last_substep": counts, "sweeps": sweeps, "topology_kept": reuse, "batched": batched,
-            "fwd_adjoint": calib,
+            "fwd_adjoint": calib, "configs": configs,
             "device_allocations_timed": int(timed_allocs),
         }
         print(json.dumps(line))
@@ -545,6 +615,7 @@ def main():
     ap.add_argument("--drums", type=int, default=512, help="scenes of the batched line (0: skip it)")
     ap.add_argument("--calib-scenes", type=int, default=64, help="scenes of the calibration line (0: skip it)")
     ap.add_argument("--calib-substeps", type=int, default=2000)
+    ap.add_argument("--no-configs", action="store_true", help="skip the settling / Hertz / shell lines")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)

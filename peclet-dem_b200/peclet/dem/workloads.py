@@ -117,42 +117,21 @@ def random_unit_quats(rng, n):
     return q
 
 
-def hollow_cylinders(seed=3, n=65536, r_out=1e-3, r_in=0.6e-3, length=3e-3, box=(60e-3, 60e-3, 120e-3),
+def hollow_cylinders(seed=3, n=65536, r_out=1e-3, r_in=0.6e-3, length=3e-3, box=None, fill=0.25,
                      density=1200.0, e=0.4, mu=0.3, dt_outer=5e-5, substeps=8, iterations=(20, 10),
-                     shell_points=None, max_tries=200) -> Scene:
+                     shell_points=None) -> Scene:
     """Point-shell hollow cylinders (body axis y), uniform random orientations, centres by random
-    sequential addition with bounding-sphere exclusion in a closed box (6 planes)."""
+    sequential addition with bounding-sphere exclusion (the compiled helper) in a closed box (6
+    planes). `box=None` sizes a 1 x 1 x 2 box so the bounding spheres fill `fill` of it: 65,536
+    bounding spheres (radius 1.80 mm) cannot be placed without overlap in 60 x 60 x 120 mm, which
+    they would fill to 3.7 times its volume."""
     rng = np.random.default_rng(seed)
     rb = float(np.hypot(r_out, 0.5 * length))  # bounding-sphere radius
-    lo = np.array([rb, rb, rb])
-    hi = np.array(box) - rb
-    cell = 2 * rb
-    dims = np.maximum(1, np.floor((hi - lo) / cell).astype(int) + 1)
-    grid = {}
-    pts = []
-    tries = 0
-    while len(pts) < n and tries < n * max_tries:
-        tries += 1
-        p = lo + rng.uniform(0, 1, 3) * (hi - lo)
-        c = tuple(np.minimum(((p - lo) / cell).astype(int), dims - 1))
-        ok = True
-        for dx in (-1, 0, 1):
-            for dy in (-1, 0, 1):
-                for dz in (-1, 0, 1):
-                    for q in grid.get((c[0] + dx, c[1] + dy, c[2] + dz), ()):
-                        if np.sum((pts[q] - p) ** 2) < (2 * rb) ** 2:
-                            ok = False
-                            break
-                    if not ok:
-                        break
-                if not ok:
-                    break
-            if not ok:
-                break
-        if ok:
-            grid.setdefault(c, []).append(len(pts))
-            pts.append(p)
-    pos = np.array(pts)
+    if box is None:
+        side = (n * 4.0 / 3.0 * np.pi * rb ** 3 / fill / 2.0) ** (1.0 / 3.0)
+        box = (side, side, 2.0 * side)
+    pos, placed = rsa_spheres(seed, np.full(n, rb), (0.0, 0.0, 0.0), tuple(box))
+    pos = pos[placed]
     n = pos.shape[0]
     vol = np.pi * (r_out ** 2 - r_in ** 2) * length
     m = density * vol
@@ -336,3 +315,68 @@ def calibration_boxes(seed=5, scenes=64, per_scene=2048, radius=1e-3, box=(40e-3
               [0, 0, 0, 0, 0, 1], [0, 0, z1, 0, 0, -1]]
     return dict(x0=np.concatenate(xs), v0=rng.uniform(-vmax, vmax, (n, 3)), w0=np.zeros((n, 3)), r=r, m=m,
                 I=0.4 * m * r * r, first=np.arange(scenes + 1) * per_scene, planes=planes)
+
+
+def hollow_cylinder_shell(n=512, seed=3, r_out=1.0, r_in=0.6, length=3.0):
+    """Seeded stratified point shell of a hollow cylinder (body axis y, canonical units), for
+    `set_shell_points`: points on the outer and inner lateral surfaces and the two annular caps,
+    allotted by area; on each surface the parameter square is cut into one stratum per point
+    (angle-major rows) and each point is jittered uniformly inside its stratum; the caps are
+    sampled uniformly in area (radius from the square root of a uniform in r^2)."""
+    rng = np.random.default_rng(seed)
+    areas = np.array([2 * np.pi * r_out * length, 2 * np.pi * r_in * length,
+                      np.pi * (r_out ** 2 - r_in ** 2), np.pi * (r_out ** 2 - r_in ** 2)])
+    counts = np.floor(n * areas / areas.sum()).astype(int)
+    for k in np.argsort(-(n * areas / areas.sum() - counts))[: n - counts.sum()]:
+        counts[k] += 1
+
+    def strata(m, aspect):
+        """m jittered points in [0, 1)^2 on a rows x cols grid of strata near the given aspect."""
+        cols = max(1, int(round(np.sqrt(m * aspect))))
+        rows = -(-m // cols)
+        cells = np.arange(rows * cols)
+        keep = np.sort(rng.permutation(cells)[:m])
+        u = (keep % cols + rng.uniform(0, 1, m)) / cols
+        v = (keep // cols + rng.uniform(0, 1, m)) / rows
+        return u, v
+
+    pts = []
+    for k, (m, rad) in enumerate(zip(counts[:2], (r_out, r_in))):
+        u, v = strata(m, 2 * np.pi * rad / length)
+        th = 2 * np.pi * u
+        pts.append(np.stack([rad * np.cos(th), (v - 0.5) * length, rad * np.sin(th)], 1))
+    for m, y in zip(counts[2:], (0.5 * length, -0.5 * length)):
+        u, v = strata(m, 2 * np.pi * 0.8 / (r_out - r_in))
+        th = 2 * np.pi * u
+        rr = np.sqrt(r_in ** 2 + v * (r_out ** 2 - r_in ** 2))
+        pts.append(np.stack([rr * np.cos(th), np.full(m, y), rr * np.sin(th)], 1))
+    return np.concatenate(pts)
+
+
+def box_wall_grid(L, H, h=2e-3, pad=2):
+    """An open-top box [0, L]^2 x [0, H] as one world-space SDF grid wall (positive inside: the
+    distance to the nearest of the floor and the four sides), for engines that take no planes."""
+    nx = ny = int(np.ceil(L / h)) + 1 + 2 * pad
+    nz = int(np.ceil(H / h)) + 1 + 2 * pad
+    origin = np.array([-pad * h, -pad * h, -pad * h])
+    x = origin[0] + h * np.arange(nx)
+    y = origin[1] + h * np.arange(ny)
+    z = origin[2] + h * np.arange(nz)
+    Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
+    grid = np.minimum.reduce([Z, X, L - X, Y, L - Y])  # x-fastest after ravel of (z, y, x)
+    return grid.ravel(), nx, ny, nz, origin, (h, h, h)
+
+
+def polydisperse_hertz_closed(seed=2, n=262144, **kw):
+    """The polydisperse packing for the Hertz engine, closed: the reference's engine refuses
+    periodic domains and analytic planes, so the box is closed in x and y and its floor and sides
+    are one SDF grid wall. Returns (scene, extra) where extra(sim) adds the wall."""
+    sc = polydisperse(seed=seed, n=n, periodic=False, **kw)
+    (mn, mx, _) = sc.domain
+    L, H = mx[0], mx[2]
+    sc.planes = []
+    grid = box_wall_grid(L, H)
+
+    def extra(sim):
+        sim.add_sdf_wall(*grid, sc.material[0], sc.material[2])
+    return sc, extra
