@@ -6,9 +6,10 @@
 // index — the canonical order the B200 implementation reproduces. At R = float the results are
 // bit-identical to the reference headers compiled against the serial Kokkos shim (the tests check
 // this); at R = double this is the FP64 oracle of the B200 FP64 step. Stabilization modes
-// "multilevel" (2) and "ordered" (4) are not restated (out of scope of the B200 build).
+// "multilevel" (2) is not restated (out of scope of the B200 build); "ordered" (4) is.
 #pragma once
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdint>
 #include <limits>
@@ -980,6 +981,88 @@ class Sim {
         }
       }
   }
+  // height-from-floor levels of the "ordered" pass (contact_preprocessing.hpp:263-305): 0 at a
+  // wall or plane contact, else 1 + min over supporting bodies, relaxed to a fixed point
+  static constexpr int kLevelInf = 1 << 28;
+  std::vector<int> heightLevel;
+  void computeHeightLevels(int nm, V3<R> gHat) {
+    heightLevel.assign(numReal, kLevelInf);
+    for (int s = 0; s < 1024; ++s) {
+      int changed = 0;
+      for (int i = 0; i < nm; ++i) {
+        const Manifold<R>& m = manifolds[i];
+        if (m.np <= 0)
+          continue;
+        const int ra = realIdx[m.a];
+        if (m.b < 0) {
+          if (heightLevel[ra] > 0) {
+            heightLevel[ra] = 0;
+            ++changed;
+          }
+          continue;
+        }
+        const int rb = realIdx[m.b];
+        const V3<R> dx = sub(posPred[m.a], posPred[m.b]);
+        const R up = -(dx.x * gHat.x + dx.y * gHat.y + dx.z * gHat.z);
+        const R thr = R(0.3) * std::sqrt(dot(dx, dx));
+        if (up > thr) {
+          const int cand = heightLevel[rb];
+          if (cand < kLevelInf && heightLevel[ra] > cand + 1) {
+            heightLevel[ra] = cand + 1;
+            ++changed;
+          }
+        } else if (up < -thr) {
+          const int cand = heightLevel[ra];
+          if (cand < kLevelInf && heightLevel[rb] > cand + 1) {
+            heightLevel[rb] = cand + 1;
+            ++changed;
+          }
+        }
+      }
+      if (changed == 0)
+        break;
+    }
+  }
+  // level-ordered symmetric sweeps (solver_velocity.hpp:914-989; sim.hpp:357-400): the coloured
+  // manifolds bucketed by (level, colour), key level * 64 + colour (stable), swept bottom-up then
+  // top-down per iteration until the residual drains
+  void orderedStabilization(int nm, V3<R> gHat, R vRestS) {
+    computeHeightLevels(nm, gHat);
+    std::vector<int> key(nm), perm(nm);
+    for (int i = 0; i < nm; ++i) {
+      perm[i] = i;
+      const Manifold<R>& m = manifolds[i];
+      if (m.np <= 0 || mColor[i] < 0) {
+        key[i] = INT_MAX;
+        continue;
+      }
+      int h = heightLevel[realIdx[m.a]];
+      if (m.b >= 0)
+        h = std::min(h, heightLevel[realIdx[m.b]]);
+      key[i] = std::min(h, 1023) * 64 + mColor[i];
+    }
+    std::stable_sort(perm.begin(), perm.end(), [&](int a, int b) { return key[a] < key[b]; });
+    std::vector<std::pair<int, int>> buckets;
+    for (int b = 0; b < nm && key[perm[b]] != INT_MAX;) {
+      int e = b + 1;
+      while (e < nm && key[perm[e]] == key[perm[b]])
+        ++e;
+      buckets.emplace_back(b, e);
+      b = e;
+    }
+    const int nb = (int)buckets.size();
+    for (int it = 0; it < 2 * velIters; ++it) {
+      maxApproach = 0;
+      for (int pass = 0; pass < 2; ++pass)
+        for (int q = 0; q < nb; ++q) {
+          const auto [b, e] = buckets[pass == 0 ? q : nb - 1 - q];
+          for (int t = b; t < e; ++t)
+            pgsOne(perm[t], vRestS, maxApproach);
+        }
+      if (maxApproach <= vRestS)
+        break;
+    }
+  }
   void commitLedger(int nm) {  // :160-192
     if (nm <= 0)
       return;
@@ -1830,8 +1913,10 @@ class Sim {
             if (maxApproach <= vRestS)
               break;
           }
+        } else if (stabMode == 4) {
+          orderedStabilization(nm, gHat, vRestS);
         } else {
-          throw std::runtime_error("oracle: stabilization modes 'multilevel'/'ordered' are not restated");
+          throw std::runtime_error("oracle: stabilization mode 'multilevel' is not restated");
         }
       }
     }

@@ -150,7 +150,7 @@ template <class R>
 struct Model {
   int n, nc, nplane;
   const int* cont;  // [nc] (i, j): j >= 0 the sphere j (> i); j < 0 the plane -j - 1
-  const R *planes, *r, *m, *I;
+  const R *planes, *r, *im, *iI;  // radius, inverse mass, inverse (scalar) moment of inertia
   R E, e, mu, dt, g[3];
   double nu;
 };
@@ -214,8 +214,13 @@ __device__ void contactPrimal(const Model<R>& M, long c, const StateView<R>& s, 
     const int j = C.j;
     C.rj = M.r[j];
     C.dx = sub(ld3(s.x, i), ld3(s.x, j));
-    C.dd = sqrt(dot(C.dx, C.dx));
-    C.delta = C.ri + C.rj - C.dd;
+    const R d2 = dot(C.dx, C.dx), rr = C.ri + C.rj;
+    if (d2 > rr * rr * R(1.0001)) {  // certainly apart: sqrt(d2) > rr whatever the rounding
+      C.active = false;
+      return;
+    }
+    C.dd = sqrt(d2);
+    C.delta = rr - C.dd;
     C.active = !(C.delta <= R(0) || C.dd < R(1e-12));
     if (!C.active)
       return;
@@ -226,7 +231,8 @@ __device__ void contactPrimal(const Model<R>& M, long c, const StateView<R>& s, 
     C.wj = ld3(s.w, j);
     C.vr = sub(add(ld3(s.v, i), cross(C.wi, C.rA)), add(ld3(s.v, j), cross(C.wj, C.rB)));
     C.rS = C.ri * C.rj / (C.ri + C.rj);
-    C.mS = R(1) / (R(1) / M.m[i] + R(1) / M.m[j]);
+    const R imS = M.im[i] + M.im[j];
+    C.mS = imS > R(0) ? R(1) / imS : R(0);
   } else {
     const R* pl = M.planes + 6 * C.k;
     C.nh = V3<R>{pl[3], pl[4], pl[5]};
@@ -238,7 +244,7 @@ __device__ void contactPrimal(const Model<R>& M, long c, const StateView<R>& s, 
     C.rA = mul(C.nh, -(C.ri - R(0.5) * C.delta));
     C.vr = add(ld3(s.v, i), cross(C.wi, C.rA));
     C.rS = C.ri;
-    C.mS = M.m[i];
+    C.mS = M.im[i] > R(0) ? R(1) / M.im[i] : R(0);
   }
   const V3<R> xi0 = ld3(s.xi, c);
   stars(M.E, M.nu, C.eS, C.gS);
@@ -430,7 +436,8 @@ __device__ bool contactLaw(const Model<R>& M, int i, int j, int k, const T* in, 
     const V3<T> rA = mul(nh, -(T(ri) - T(0.5) * delta));
     const V3<T> rB = mul(nh, T(rj) - T(0.5) * delta);
     const V3<T> vr = sub(add(vi, cross(wi, rA)), add(vj, cross(wj, rB)));
-    const R mS = R(1) / (R(1) / M.m[i] + R(1) / M.m[j]);
+    const R imS = M.im[i] + M.im[j];
+    const R mS = imS > R(0) ? R(1) / imS : R(0);
     const V3<T> f = pdem::hertzForce(delta, nh, vr, T(ri * rj / (ri + rj)), T(mS), eS, gS, e, mu, T(M.dt), h);
     const V3<T> ti = cross(rA, f), tj = cross(rB, mul(f, T(-1.0)));
     out[0] = f.x, out[1] = f.y, out[2] = f.z, out[3] = ti.x, out[4] = ti.y, out[5] = ti.z;
@@ -444,7 +451,8 @@ __device__ bool contactLaw(const Model<R>& M, int i, int j, int k, const T* in, 
     return false;
   const V3<T> rA = mul(n, -(T(ri) - T(0.5) * delta));
   const V3<T> vr = add(vi, cross(wi, rA));
-  const V3<T> f = pdem::hertzForce(delta, n, vr, T(ri), T(M.m[i]), eS, gS, e, mu, T(M.dt), h);
+  const R mS = M.im[i] > R(0) ? R(1) / M.im[i] : R(0);
+  const V3<T> f = pdem::hertzForce(delta, n, vr, T(ri), T(mS), eS, gS, e, mu, T(M.dt), h);
   const V3<T> t = cross(rA, f);
   out[0] = f.x, out[1] = f.y, out[2] = f.z, out[3] = t.x, out[4] = t.y, out[5] = t.z;
   out[6] = out[7] = out[8] = T(0.0);
@@ -477,12 +485,12 @@ template <class R>
 __global__ void kIntegrate(Model<R> M, StateView<R> s, StateView<R> t, R* F, R* T) {
   GRID_STRIDE(i, M.n) {
     // every load before the first store: the compiler cannot prove the buffers apart
-    const R mi = M.m[i], Ii = M.I[i];
+    const R im = M.im[i], iI = M.iI[i];
     const V3<R> x = ld3(s.x, i), v = ld3(s.v, i), w = ld3(s.w, i), f = ld3(F, i), tq = ld3(T, i);
-    const V3<R> v1{v.x + (f.x / mi + M.g[0]) * M.dt, v.y + (f.y / mi + M.g[1]) * M.dt,
-                   v.z + (f.z / mi + M.g[2]) * M.dt};
+    const V3<R> v1{v.x + (f.x * im + M.g[0]) * M.dt, v.y + (f.y * im + M.g[1]) * M.dt,
+                   v.z + (f.z * im + M.g[2]) * M.dt};
     st3(t.v, i, v1);
-    st3(t.w, i, V3<R>{w.x + tq.x / Ii * M.dt, w.y + tq.y / Ii * M.dt, w.z + tq.z / Ii * M.dt});
+    st3(t.w, i, V3<R>{w.x + tq.x * iI * M.dt, w.y + tq.y * iI * M.dt, w.z + tq.z * iI * M.dt});
     st3(t.x, i, V3<R>{x.x + v1.x * M.dt, x.y + v1.y * M.dt, x.z + v1.z * M.dt});
     st3(F, i, V3<R>{R(0), R(0), R(0)});
     st3(T, i, V3<R>{R(0), R(0), R(0)});
@@ -495,14 +503,14 @@ __global__ void kIntegrate(Model<R> M, StateView<R> s, StateView<R> t, R* F, R* 
 template <class R>
 __global__ void kIntegrateAdj(Model<R> M, StateView<R> b1, StateView<R> b0, R* Fb, R* Tb) {
   GRID_STRIDE(i, M.n) {
-    const R mi = M.m[i], Ii = M.I[i];
+    const R im = M.im[i], iI = M.iI[i];
     const V3<R> xb = ld3(b1.x, i), vb = ld3(b1.v, i), wb = ld3(b1.w, i);
     const V3<R> vbt = add(vb, mul(xb, M.dt));  // v' feeds x' = x + v' dt
     st3(b0.x, i, xb);
     st3(b0.v, i, vbt);
     st3(b0.w, i, wb);
-    st3(Fb, i, V3<R>{vbt.x * M.dt / mi, vbt.y * M.dt / mi, vbt.z * M.dt / mi});
-    st3(Tb, i, V3<R>{wb.x * M.dt / Ii, wb.y * M.dt / Ii, wb.z * M.dt / Ii});
+    st3(Fb, i, V3<R>{vbt.x * im * M.dt, vbt.y * im * M.dt, vbt.z * im * M.dt});
+    st3(Tb, i, V3<R>{wb.x * iI * M.dt, wb.y * iI * M.dt, wb.z * iI * M.dt});
   }
 }
 __device__ inline void flushParams(double* thetaB, double gE, double ge, double gmu) {
@@ -661,14 +669,14 @@ template <class R>
 __global__ void kIntegrateJvp(Model<R> M, StateView<R> s, StateView<R> sd, StateView<R> t, StateView<R> td, R* F,
                               R* T, R* Fd, R* Td) {
   GRID_STRIDE(i, M.n) {
-    const R mi = M.m[i], Ii = M.I[i];
+    const R im = M.im[i], iI = M.iI[i];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
       const long q = 3 * i + a;
-      const R v = s.v[q] + (F[q] / mi + M.g[a]) * M.dt;
-      const R vd = sd.v[q] + Fd[q] / mi * M.dt;
+      const R v = s.v[q] + (F[q] * im + M.g[a]) * M.dt;
+      const R vd = sd.v[q] + Fd[q] * im * M.dt;
       t.v[q] = v, td.v[q] = vd;
-      t.w[q] = s.w[q] + T[q] / Ii * M.dt, td.w[q] = sd.w[q] + Td[q] / Ii * M.dt;
+      t.w[q] = s.w[q] + T[q] * iI * M.dt, td.w[q] = sd.w[q] + Td[q] * iI * M.dt;
       t.x[q] = s.x[q] + v * M.dt, td.x[q] = sd.x[q] + vd * M.dt;
       F[q] = T[q] = Fd[q] = Td[q] = R(0);
     }
@@ -1008,8 +1016,8 @@ template <class R>
 Model<R> makeModel(const pdem_hz_model* h) {
   if (!h || h->n < 0 || h->ncontact < 0 || h->nplane < 0)
     throw Fail{PDEM_ERR_INVALID, "hz model: negative sizes"};
-  if (h->n > 0 && (!h->radius || !h->mass || !h->inertia))
-    throw Fail{PDEM_ERR_INVALID, "hz model: radius, mass and inertia are required"};
+  if (h->n > 0 && (!h->radius || !h->inv_mass || !h->inv_inertia))
+    throw Fail{PDEM_ERR_INVALID, "hz model: radius, inverse mass and inverse inertia are required"};
   if ((h->ncontact > 0 && !h->contacts) || (h->nplane > 0 && !h->planes))
     throw Fail{PDEM_ERR_INVALID, "hz model: contact list or planes missing"};
   if (!(h->youngs > 0) || !(h->dt > 0))
@@ -1018,8 +1026,8 @@ Model<R> makeModel(const pdem_hz_model* h) {
   M.n = h->n, M.nc = h->ncontact, M.nplane = h->nplane, M.cont = h->contacts;
   M.planes = static_cast<const R*>(h->planes);
   M.r = static_cast<const R*>(h->radius);
-  M.m = static_cast<const R*>(h->mass);
-  M.I = static_cast<const R*>(h->inertia);
+  M.im = static_cast<const R*>(h->inv_mass);
+  M.iI = static_cast<const R*>(h->inv_inertia);
   M.E = R(h->youngs), M.e = R(h->restitution), M.mu = R(h->friction), M.dt = R(h->dt), M.nu = h->poisson;
   for (int a = 0; a < 3; ++a)
     M.g[a] = R(h->gravity[a]);

@@ -1426,14 +1426,19 @@ void Sim<R>::demStep() {
   mark(ST_STAB);
   if (usePGS) {
     const R vRestS = R(2) * dt_ * gMag;
-    if (stabMode_ == 2 || stabMode_ == 4) {
-      throw std::runtime_error("stabilization modes 'multilevel' and 'ordered' are not supported by the B200 step");
-    }
+    if (stabMode_ == 2)
+      throw std::runtime_error("stabilization mode 'multilevel' is not supported by the B200 step");
+    if (stabMode_ == 4 && batch_)
+      throw std::runtime_error("batched scenes: stabilization mode 'ordered' is not supported");
     ctl(CTL_STAB_DECIDE, vRestS, stabMode_);
     // the pass runs only when the main sweeps left a residual (src/sim.hpp:282): read the
     // decision so an untriggered pass costs nothing
-    const bool stabRun = (stabMode_ == 1 || stabMode_ == 3) && readCounters().stabRun;
-    if (stabRun) {
+    const bool stabRun = (stabMode_ == 1 || stabMode_ == 3 || stabMode_ == 4) && readCounters().stabRun;
+    if (stabRun && stabMode_ == 4) {
+      SolveP<R> ss = sp;
+      ss.vRest = vRestS;
+      orderedStabilization(nm, gHat, ss, vRestS);
+    } else if (stabRun) {
       if (stabMode_ == 1 && nm > 0) {
         ensureGrounded();
         ++launches_, kSideFlags<<<gridFor(nm), B, 0, s>>>(d_, nm, gHat, R(8) * dt_ * gMag, R(8) * dt_ * gMag);
@@ -1978,6 +1983,61 @@ long Sim<R>::getHertz(unsigned long long* keys, double* xi, long cap) {
 // by the one-sided stabilization pass, so each substep just records its graph in a 32-slot ring and
 // the sweeps are replayed (from the last checkpoint, or from zero over the last 32 graphs) only when
 // the pass needs the levels. The result is identical to sweeping every substep.
+// "ordered" stabilization (src/sim.hpp:357-400): fresh height levels, manifolds bucketed by
+// (level, colour), symmetric sweeps bottom-up then top-down until the residual drains
+template <class R>
+void Sim<R>::orderedStabilization(int nm, V3<R> gHat, const SolveP<R>& ss, R vRestS) {
+  cudaStream_t s = stream_;
+  const int B = kBlock;
+  if (nm <= 0 || numReal_ <= 0)
+    return;
+  heights_.ensure(numReal_, false, s);
+  ordChanged_.ensure(1, false, s);
+  ++launches_, kHeightInit<<<gridFor(numReal_), B, 0, s>>>(heights_.p, numReal_);
+  // sweeps until none changes a level (at most 1024, as the reference); four per host check,
+  // which cannot change the result: a sweep at the fixed point changes nothing
+  for (int sweep = 0; sweep < 1024; sweep += 4) {
+    ordChanged_.zero(s);
+    for (int q = 0; q < 4; ++q)
+      ++launches_, kHeightSweep<<<gridFor(nm), B, 0, s>>>(d_, nm, gHat, heights_.p, ordChanged_.p);
+    int changed = 0;
+    cudaCheck(cudaMemcpyAsync(&changed, ordChanged_.p, sizeof changed, cudaMemcpyDeviceToHost, s), "D2H");
+    sync();
+    if (changed == 0)
+      break;
+  }
+  ordKeysIn_.ensure(nm, false, s);
+  ordKeys_.ensure(nm, false, s);
+  ordPermIn_.ensure(nm, false, s);
+  ordPerm_.ensure(nm, false, s);
+  ++launches_, kLevelKeys<<<gridFor(nm), B, 0, s>>>(d_, nm, heights_.p, ordKeysIn_.p, ordPermIn_.p);
+  sortPairs(ordKeysIn_.p, ordKeys_.p, ordPermIn_.p, ordPerm_.p, nm, 31);
+  std::vector<int> keys(nm);
+  cudaCheck(cudaMemcpyAsync(keys.data(), ordKeys_.p, nm * sizeof(int), cudaMemcpyDeviceToHost, s), "D2H");
+  sync();
+  std::vector<std::pair<int, int>> buckets;
+  for (int b = 0; b < nm && keys[b] != INT_MAX;) {
+    int e = b + 1;
+    while (e < nm && keys[e] == keys[b])
+      ++e;
+    buckets.emplace_back(b, e);
+    b = e;
+  }
+  const int nb = (int)buckets.size();
+  for (int it = 0; it < 2 * velIters_; ++it) {
+    ctl(CTL_STAB_BEGIN, R(0), 0);
+    for (int pass = 0; pass < 2; ++pass)
+      for (int q = 0; q < nb; ++q) {
+        const auto [b, e] = buckets[pass == 0 ? q : nb - 1 - q];
+        ++launches_, kPGSBucket<<<gridFor(e - b), B, 0, s>>>(d_, ordPerm_.p, b, e - b, keys[b] % 64, ss, 2);
+      }
+    ctl(CTL_STAB_END, vRestS, 0);
+    if (readCounters().stabDone)
+      break;
+  }
+  KCHECK("ordered stabilization");
+}
+
 template <class R>
 void Sim<R>::logSupportGraph(int nm, V3<R> gHat) {
   const int slot = (int)(gLog_ % kGroundRing);

@@ -13,6 +13,9 @@
 #include "pdem_common.cuh"
 
 namespace pdem {
+template <class R>
+struct SolveP;  // pdem_solve.cuh
+
 
 struct CudaError : std::runtime_error {
   using std::runtime_error::runtime_error;
@@ -202,6 +205,7 @@ class Sim {
   DBuf<Q4<R>> mN_, mTA_, mTB_, mrA_, mrB_, mwv_;
   DBuf<u64> pairKeys_, prevKeys_;
   DBuf<uint8_t> persistent_, sideFlags_;
+  DBuf<int> heights_, ordChanged_, ordKeysIn_, ordKeys_, ordPermIn_, ordPerm_;  // "ordered" pass
   DBuf<R> lambda_, prevLambda_, vn0_, posImp_, prevPosImp_;
   DBuf<Q4<R>> lambdaT_, prevLambdaT_, vt0_;
   DBuf<ShapeDesc<R>> shapeD_;
@@ -329,6 +333,7 @@ class Sim {
   void launchCoop(K kernel, A... args);
   template <class T>
   void sortPairs(const T* kin, T* kout, const int* vin, int* vout, int n, int endBit);
+  void orderedStabilization(int nm, V3<R> gHat, const SolveP<R>& ss, R vRestS);
   template <class T>
   void exclusiveSum(const T* in, T* out, int n);
   template <class T>

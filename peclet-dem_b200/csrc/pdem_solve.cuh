@@ -525,6 +525,81 @@ __global__ void kPGSColor(Dev<R> d, const int* order, const int* coff, int color
     warpMaxAtomic(&d.ctr->maxApproach, mx);
 }
 
+// ---- "ordered" stabilization (level-ordered symmetric sweeps) ----
+// height-from-floor levels (src/contact_preprocessing.hpp:263-305): 0 at a wall or plane contact,
+// else 1 + min over supporting bodies; one relaxation sweep per launch, *changed counts updates.
+// The relaxation's fixed point (shortest support paths) does not depend on the visit order.
+constexpr int kLevelInf = 1 << 28;
+static __global__ void kHeightInit(int* h, int n) {
+  GRID_STRIDE(i, n) { h[i] = kLevelInf; }
+}
+template <class R>
+__global__ void kHeightSweep(Dev<R> d, int nm, V3<R> gHat, int* h, int* changed) {
+  int c = 0;
+  GRID_STRIDE(idx, nm) {
+    if (d.mnp[idx] <= 0)
+      continue;
+    const int2 ab = d.mab[idx];
+    const int ra = d.realIdx[ab.x];
+    if (ab.y < 0) {
+      if (atomicMin(&h[ra], 0) > 0)
+        ++c;
+      continue;
+    }
+    const int rb = d.realIdx[ab.y];
+    const V3<R> dx = sub(v3(d.posPred[ab.x]), v3(d.posPred[ab.y]));
+    const R up = -(dx.x * gHat.x + dx.y * gHat.y + dx.z * gHat.z);
+    const R thr = R(0.3) * sqrt(dot(dx, dx));
+    if (up > thr) {
+      const int cand = atomicAdd(&h[rb], 0);
+      if (cand < kLevelInf && atomicMin(&h[ra], cand + 1) > cand + 1)
+        ++c;
+    } else if (up < -thr) {
+      const int cand = atomicAdd(&h[ra], 0);
+      if (cand < kLevelInf && atomicMin(&h[rb], cand + 1) > cand + 1)
+        ++c;
+    }
+  }
+  if (c)
+    atomicAdd(changed, c);
+}
+// bucket keys (src/solver_velocity.hpp:914-965): level * 64 + colour of every active coloured
+// manifold (its level is the lower of its bodies', clamped to 1023); the rest keyed out
+template <class R>
+__global__ void kLevelKeys(Dev<R> d, int nm, const int* h, int* keys, int* perm) {
+  GRID_STRIDE(idx, nm) {
+    perm[idx] = (int)idx;
+    const int c = d.mColor[idx];
+    if (d.mnp[idx] <= 0 || c < 0) {
+      keys[idx] = INT_MAX;
+      continue;
+    }
+    const int2 ab = d.mab[idx];
+    int lv = h[d.realIdx[ab.x]];
+    if (ab.y >= 0)
+      lv = min(lv, h[d.realIdx[ab.y]]);
+    keys[idx] = min(lv, 1023) * 64 + c;
+  }
+}
+// one (level, colour) bucket of the sorted permutation; the saturated colour runs serially in
+// permutation order, the others are independent sets
+template <class R>
+__global__ void kPGSBucket(Dev<R> d, const int* perm, int b, int n, int color, SolveP<R> P, int gate) {
+  if (!gateOpen(d.ctr, gate))
+    return;
+  const bool serial = color >= kSaturatedColor;
+  if (serial && (blockIdx.x | threadIdx.x))
+    return;
+  R mx = R(0);
+  for (long t = serial ? 0 : (long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+       t += serial ? 1 : (long)gridDim.x * blockDim.x)
+    pgsOne(d, perm[b + t], P, mx, gate);
+  if (serial)
+    atomicMaxNonNeg(&d.ctr->maxApproach, mx);
+  else
+    warpMaxAtomic(&d.ctr->maxApproach, mx);
+}
+
 // one-shot coloured GS of one colour, g = 0 path (src/solver_velocity.hpp:989-1137)
 template <class R>
 __device__ __forceinline__ void gsOne(const Dev<R>& d, int idx, const SolveP<R>& P, R& mx) {

@@ -38,6 +38,7 @@ class Scene:
     substeps: int = 10                   # demStep calls per outer step
     shell: np.ndarray | None = None      # optional explicit point shell
     hertz: tuple | None = None           # (E, nu) for the Hertz engine
+    sdf: tuple | None = None             # set_sdf_shape arguments: a grid-SDF particle shape
 
     @property
     def n(self) -> int:
@@ -45,7 +46,10 @@ class Scene:
 
     def apply(self, sim):
         """Configure `sim` (any object with the reference facade methods) with this scene."""
-        sim.initialize_shape(*self.shape)
+        if self.sdf is not None:
+            sim.set_sdf_shape(*self.sdf)
+        else:
+            sim.initialize_shape(*self.shape)
         if self.shell is not None:
             sim.set_shell_points(self.shell)
         sim.set_global_scale(self.global_scale)

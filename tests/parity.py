@@ -88,4 +88,7 @@ MATRIX = [
     ("growth", lambda: S.dense_spheres(gravity=(0, 0, 0), mu=0.0), lambda s: s.set_growth_params(50.0, 0.8), 5),
     ("pair_materials", lambda: S.dense_spheres(), _mats, 6),
     ("walton_beta", lambda: S.dense_spheres(), lambda s: s.set_material_params(0.5, 0.3, 0.5), 6),
+    ("grid_sdf_capsules", lambda: S.sdf_capsules(), None, 8),
+    ("ordered_column", lambda: S.settled_column(), lambda s: s.set_stabilization_mode("ordered"), 25),
+    ("ordered_dense", lambda: S.dense_spheres(), lambda s: s.set_stabilization_mode("ordered"), 8),
 ]

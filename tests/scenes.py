@@ -72,6 +72,48 @@ def cylinders(seed=14, n=24, L=8e-3, shape_type=W.HOLLOW_CYLINDER, shell=None):
                    iterations=(20, 10), dt=6.25e-6, shell=shell)
 
 
+def capsule_sdf(radius=0.6, half=0.6, h=0.1, pad=0.2, n_shell=240, seed=16):
+    """A capsule (axis y, canonical units) as a grid-SDF particle shape: the exact distance to its
+    core segment minus the radius, sampled on a grid, with a seeded point shell on its surface and
+    the unit-mass inverse inertia of a solid capsule (cylinder plus two hemispheres)."""
+    rng = np.random.default_rng(seed)
+    ext = half + radius + pad
+    n = int(round(2 * ext / h)) + 1
+    ax = -ext + h * np.arange(n)
+    Z, Y, X = np.meshgrid(ax, ax, ax, indexing="ij")
+    grid = np.sqrt(X ** 2 + (np.abs(Y) - np.minimum(np.abs(Y), half)) ** 2 + Z ** 2) - radius
+    # shell: the cylinder by area, then the two hemispheres
+    a_cyl, a_cap = 2 * np.pi * radius * 2 * half, 4 * np.pi * radius ** 2
+    n_cyl = int(round(n_shell * a_cyl / (a_cyl + a_cap)))
+    th = rng.uniform(0, 2 * np.pi, n_cyl)
+    cyl = np.stack([radius * np.cos(th), rng.uniform(-half, half, n_cyl), radius * np.sin(th)], 1)
+    d = rng.normal(size=(n_shell - n_cyl, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    cap = radius * d + np.stack([np.zeros(len(d)), np.sign(d[:, 1]) * half, np.zeros(len(d))], 1)
+    shell = np.concatenate([cyl, cap])
+    mc, ms = np.pi * radius ** 2 * 2 * half, 4 / 3 * np.pi * radius ** 3
+    m = mc + ms
+    iyy = mc * radius ** 2 / 2 + ms * 2 * radius ** 2 / 5
+    ixx = mc * (3 * radius ** 2 + (2 * half) ** 2) / 12 + ms * (2 * radius ** 2 / 5 + half ** 2 + 3 * half * radius / 4)
+    inv_i = np.array([m / ixx, m / iyy, m / ixx])
+    return (grid.ravel(), n, n, n, (-ext, -ext, -ext), (h, h, h), shell, inv_i, half + radius)
+
+
+def sdf_capsules(seed=17, n=30, L=8e-3):
+    """Capsules given as a grid-SDF shape (set_sdf_shape), random orientations, in a closed box."""
+    rng = np.random.default_rng(seed)
+    s = 1e-3
+    pos = _cluster(rng, n, ((0, 0, 0), (L, L, L)), 1.2 * s)
+    m = 1500.0 * (np.pi * 0.36 * 1.2 + 4 / 3 * np.pi * 0.216) * s ** 3
+    sdf = capsule_sdf()
+    iI = np.tile(np.asarray(sdf[7]) / (m * s * s), (n, 1))
+    return W.Scene(name="sdf_capsules", pos=pos, vel=rng.uniform(-0.3, 0.3, (n, 3)),
+                   inv_mass=np.full(n, 1.0 / m), inv_inertia=iI, quat=W.random_unit_quats(rng, n),
+                   global_scale=s, domain=((0, 0, 0), (L, L, L), (False, False, False)),
+                   planes=W.box_planes((0, 0, 0), (L, L, L)), material=(0.4, 0.0, 0.3),
+                   iterations=(20, 10), dt=6.25e-6, sdf=sdf)
+
+
 drum_wall_grid = W.drum_wall_grid
 
 
