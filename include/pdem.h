@@ -209,6 +209,13 @@ int pdem_debug_sweeps(pdem_handle h, long* out4);
 int pdem_find_pairs_static(const double* d_xyz, const double* d_radius, int n, double margin, double box_cap,
                            int* d_pairs, long pair_cap, long* out_count, void* stream);
 
+/* get_sdf_grid(resolution)                      src/dem_bindings.cpp:344-355, src/sim.hpp:1538-1542
+ * packed-bed SDF over the domain (src/output_sdf.hpp:25-196), flat x-fastest; returns rx*ry*rz
+ * (only cap written), or -1 with pdem_last_error() set */
+long pdem_get_sdf_grid(pdem_handle h, int rx, int ry, int rz, double* out, long cap);
+/* export_sdf(filename, resolution)              src/dem_bindings.cpp:369-376, src/sim.hpp:1478-1483 */
+int pdem_export_sdf(pdem_handle h, const char* filename, int rx, int ry, int rz);
+
 /* ---- forward, adjoint and tangent-linear runs of the Hertz-Mindlin substep for spheres (no
  * counterpart in the reference; the force law is the Hertz engine's, src/solver_hertz.hpp:88-144,
  * its kick-drift src/solver_hertz.hpp:374-425; planes are walls at rest with the same law) ----
@@ -221,9 +228,9 @@ typedef struct {
   int n, ncontact, nplane;
   const int* contacts;  /* ncontact x (i, j) */
   const void* planes;   /* nplane x (point, unit normal into the domain) */
-  const void* radius;   /* n */
-  const void* mass;     /* n */
-  const void* inertia;  /* n: scalar moment of inertia */
+  const void* radius;       /* n */
+  const void* inv_mass;     /* n: 1 / mass (0: fixed) */
+  const void* inv_inertia;  /* n: 1 / scalar moment of inertia */
   double youngs, restitution, friction, poisson, dt, gravity[3];
 } pdem_hz_model;
 long pdem_hz_state_size(int n, int ncontact);

@@ -242,6 +242,14 @@ int ref_export_lammps(void* h, const char* fn, int step) {
   return guard([&] { S(h)->exportLammps(fn, step); });
 }
 int ref_write_vtp(void* h, const char* fn) { return guard([&] { S(h)->writeVtp(fn); }); }
+long ref_get_sdf_grid(void* h, int rx, int ry, int rz, double* out, long cap) {
+  long n = -1;
+  const int st = guard([&] { n = copyOut(S(h)->getSdfGrid(rx, ry, rz), out, cap); });
+  return st == 0 ? n : -1;
+}
+int ref_export_sdf(void* h, const char* fn, int rx, int ry, int rz) {
+  return guard([&] { S(h)->exportSdf(fn, rx, ry, rz); });
+}
 
 // ---- debug getters: the step's intermediate products ----
 int ref_debug_counts(void* h, long* out) {

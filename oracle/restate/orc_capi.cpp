@@ -391,6 +391,18 @@ double orc_max_overlap(void* h) {
   with(h, [&](auto& S) { v = S.maxOverlap; });
   return v;
 }
+long orc_get_sdf_grid(void* h, int rx, int ry, int rz, double* out, long cap) {
+  long n = -1;
+  const int st = with(h, [&](auto& S) {
+    if (rx < 1 || ry < 1 || rz < 1)
+      throw std::invalid_argument("get_sdf_grid: resolution must be positive");
+    const auto g = S.generateSdf(rx, ry, rz);
+    n = (long)g.size();
+    for (long i = 0; i < n && i < cap; ++i)
+      out[i] = (double)g[i];
+  });
+  return st == 0 ? n : -1;
+}
 int orc_export_lammps(void*, const char*, int) {
   g_err = "oracle: export not restated";
   return 3;

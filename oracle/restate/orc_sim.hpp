@@ -1063,6 +1063,128 @@ class Sim {
         break;
     }
   }
+  // output_sdf.hpp:25-196 (get_sdf_grid): over the domain box, every voxel starts at 100; each
+  // particle writes min(analytic SDF x scale) over its band (bounding radius x scale x 1.2) and
+  // marks the voxels nearer than that radius fixed; then max(res) x 4 Jacobi Eikonal sweeps
+  // (spacing = the x voxel size) fill the rest, periodic axes wrapped. The particle scale alone
+  // scales the shape (the global scale is not applied), and box shapes splat nothing, as in the
+  // reference.
+  std::vector<R> generateSdf(int rx, int ry, int rz) {
+    const long total = (long)rx * ry * rz;
+    const V3<R> origin = dmin;
+    const V3<R> vox{(dmax.x - dmin.x) / R(rx), (dmax.y - dmin.y) / R(ry), (dmax.z - dmin.z) / R(rz)};
+    std::vector<R> grid(total, R(100));
+    std::vector<int> state(total, 0);
+    for (int i = 0; i < numReal; ++i) {
+      const V3<R> pw = pos[i];
+      const V4<R> q = quat[i];
+      const R sc = scale[i];
+      const Shape<R>& shp = shapes[shapeId[i]];
+      R rbound = R(1);
+      if (shp.type == HCYL) {
+        const R r = shp.par.x, h = shp.par.y;
+        rbound = std::sqrt(r * r + (h * R(0.5)) * (h * R(0.5)));
+      } else if (shp.type == SPHERE || shp.type == GRID) {
+        rbound = shp.par.x;
+      }
+      rbound *= sc;
+      rbound *= R(1.2);
+      int mnx = (int)std::floor((pw.x - rbound - origin.x) / vox.x), mxx = (int)std::ceil((pw.x + rbound - origin.x) / vox.x);
+      int mny = (int)std::floor((pw.y - rbound - origin.y) / vox.y), mxy = (int)std::ceil((pw.y + rbound - origin.y) / vox.y);
+      int mnz = (int)std::floor((pw.z - rbound - origin.z) / vox.z), mxz = (int)std::ceil((pw.z + rbound - origin.z) / vox.z);
+      if (!px)
+        mnx = std::max(mnx, 0), mxx = std::min(mxx, rx - 1);
+      if (!py)
+        mny = std::max(mny, 0), mxy = std::min(mxy, ry - 1);
+      if (!pz)
+        mnz = std::max(mnz, 0), mxz = std::min(mxz, rz - 1);
+      for (int z = mnz; z <= mxz; ++z)
+        for (int y = mny; y <= mxy; ++y)
+          for (int x = mnx; x <= mxx; ++x) {
+            const V3<R> vp{origin.x + (R(x) + R(0.5)) * vox.x, origin.y + (R(y) + R(0.5)) * vox.y,
+                           origin.z + (R(z) + R(0.5)) * vox.z};
+            const V3<R> pl = mul(invrot(q, sub(vp, pw)), R(1) / sc);
+            R distc = R(100);
+            if (shp.type == HCYL)
+              distc = sdfHollowCyl(pl, shp.par);
+            else if (shp.type == SPHERE)
+              distc = sdfSphere(pl, shp.par);
+            else if (shp.type == GRID)
+              distc = sdfShape(pl, shp, sdfGrid.data());
+            const R dist = distc * sc;
+            const int wx = (x % rx + rx) % rx, wy = (y % ry + ry) % ry, wz = (z % rz + rz) % rz;
+            if ((!px && (x < 0 || x >= rx)) || (!py && (y < 0 || y >= ry)) || (!pz && (z < 0 || z >= rz)))
+              continue;
+            const long vi = (long)wz * rx * ry + (long)wy * rx + wx;
+            grid[vi] = std::min(grid[vi], dist);
+            if (dist < rbound)
+              state[vi] = 1;
+          }
+    }
+    std::vector<R> out(total);
+    const int iters = std::max(std::max(rx, ry), rz) * 4;
+    const R h = vox.x;
+    for (int it = 0; it < iters; ++it) {
+      for (long idx = 0; idx < total; ++idx)
+        out[idx] = eikonalCell(grid, state, idx, rx, ry, rz, h);
+      grid.swap(out);
+    }
+    return grid;
+  }
+  R eikonalCell(const std::vector<R>& in, const std::vector<int>& st, long idx, int rx, int ry, int rz, R h) const {
+    if (st[idx] == 1)
+      return in[idx];
+    const long sy = rx, sz = (long)rx * ry;
+    const int z = (int)(idx / sz);
+    const long rem = idx % sz;
+    const int y = (int)(rem / sy), x = (int)(rem % sy);
+    R xm = 100, xp = 100, ym = 100, yp = 100, zm = 100, zp = 100;
+    if (x > 0)
+      xm = in[idx - 1];
+    else if (px)
+      xm = in[idx - 1 + rx];
+    if (x < rx - 1)
+      xp = in[idx + 1];
+    else if (px)
+      xp = in[idx + 1 - rx];
+    if (y > 0)
+      ym = in[idx - sy];
+    else if (py)
+      ym = in[(long)z * sz + (long)(ry - 1) * sy + x];
+    if (y < ry - 1)
+      yp = in[idx + sy];
+    else if (py)
+      yp = in[(long)z * sz + x];
+    if (z > 0)
+      zm = in[idx - sz];
+    else if (pz)
+      zm = in[(long)(rz - 1) * sz + (long)y * sy + x];
+    if (z < rz - 1)
+      zp = in[idx + sz];
+    else if (pz)
+      zp = in[(long)y * sy + x];
+    R a = std::fmin(xm, xp), b = std::fmin(ym, yp), c = std::fmin(zm, zp);
+    if (a > b)
+      std::swap(a, b);
+    if (b > c)
+      std::swap(b, c);
+    if (a > b)
+      std::swap(a, b);
+    R u = 100, u1 = a + h;
+    if (u1 <= b) {
+      u = u1;
+    } else {
+      const R d2 = R(2) * h * h - (a - b) * (a - b);
+      const R u2 = (d2 < R(0)) ? R(100) : (a + b + std::sqrt(d2)) * R(0.5);
+      if (u2 <= c) {
+        u = u2;
+      } else {
+        const R s = a + b + c, qd = s * s - R(3) * (a * a + b * b + c * c - h * h);
+        u = (qd < R(0)) ? R(100) : (s + std::sqrt(qd)) / R(3);
+      }
+    }
+    return u;
+  }
   void commitLedger(int nm) {  // :160-192
     if (nm <= 0)
       return;

@@ -96,6 +96,33 @@ void writeLammps(const std::string& fn, int step, const std::vector<double>& pos
       << quat[4 * i] << " " << quat[4 * i + 1] << " " << quat[4 * i + 2] << "\n";
 }
 // ParaView PolyData writer, format of src/sim.hpp:1560-1601 (points + Radius + Velocity)
+// ImageData VTI of an SDF grid (src/io.hpp:86-110): ASCII Float32 values in the stream's default
+// format, origin at the domain minimum, spacing (max - min) / (res - 1) per axis
+template <class T>
+void writeSdfVti(const std::string& fn, const std::vector<T>& grid, int rx, int ry, int rz, const float* mn,
+                 const float* mx) {
+  const double sx = rx > 1 ? (double(mx[0]) - mn[0]) / (rx - 1) : 1.0;
+  const double sy = ry > 1 ? (double(mx[1]) - mn[1]) / (ry - 1) : 1.0;
+  const double sz = rz > 1 ? (double(mx[2]) - mn[2]) / (rz - 1) : 1.0;
+  std::ofstream out(fn);
+  if (!out)
+    throw std::runtime_error("Could not open file for writing: " + fn);
+  out << "<?xml version=\"1.0\"?>\n";
+  out << "<VTKFile type=\"ImageData\" version=\"0.1\" byte_order=\"LittleEndian\">\n";
+  out << "  <ImageData WholeExtent=\"0 " << (rx - 1) << " 0 " << (ry - 1) << " 0 " << (rz - 1) << "\" Origin=\""
+      << mn[0] << " " << mn[1] << " " << mn[2] << "\" Spacing=\"" << sx << " " << sy << " " << sz << "\">\n";
+  out << "    <Piece Extent=\"0 " << (rx - 1) << " 0 " << (ry - 1) << " 0 " << (rz - 1) << "\">\n";
+  out << "      <PointData Scalars=\"sdf\">\n";
+  out << "        <DataArray type=\"Float32\" Name=\"sdf\" format=\"ascii\">\n";
+  for (const T v : grid)
+    out << (float)v << " ";
+  out << "\n        </DataArray>\n";
+  out << "      </PointData>\n";
+  out << "    </Piece>\n";
+  out << "  </ImageData>\n";
+  out << "</VTKFile>\n";
+  std::printf("Exported SDF VTI: %s\n", fn.c_str());
+}
 void writeVtp(const std::string& fn, const std::vector<double>& pos, const std::vector<double>& vel,
               const std::vector<double>& radii) {
   const size_t n = pos.size() / 3;
@@ -403,6 +430,25 @@ int pdem_write_vtp(pdem_handle h, const char* fn) {
     for (size_t i = 0; i < sc.size(); ++i)
       radii[i] = (double)((R)sc[i] * S.gs_ * S.baseRadius_);
     writeVtp(fn, pos, vel, radii);
+  });
+}
+
+long pdem_get_sdf_grid(pdem_handle h, int rx, int ry, int rz, double* out, long cap) {
+  long n = -1;
+  const int st = with(h, [&](auto& S) {
+    const auto g = S.sdfGrid(rx, ry, rz);
+    n = (long)g.size();
+    for (long i = 0; i < n && i < cap; ++i)
+      out[i] = (double)g[i];
+  });
+  return st == PDEM_OK ? n : -1;
+}
+int pdem_export_sdf(pdem_handle h, const char* fn, int rx, int ry, int rz) {
+  BODY({
+    const auto g = S.sdfGrid(rx, ry, rz);
+    const float mn[3] = {(float)S.dmin_[0], (float)S.dmin_[1], (float)S.dmin_[2]};
+    const float mx[3] = {(float)S.dmax_[0], (float)S.dmax_[1], (float)S.dmax_[2]};
+    writeSdfVti(fn, g, rx, ry, rz, mn, mx);
   });
 }
 

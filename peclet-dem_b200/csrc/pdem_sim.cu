@@ -15,6 +15,7 @@
 #include "pdem_persist.cuh"
 #include "pdem_shell.hpp"
 #include "pdem_sim.cuh"
+#include "pdem_sdf.cuh"
 #include "pdem_solve.cuh"
 
 namespace pdem {
@@ -1983,6 +1984,41 @@ long Sim<R>::getHertz(unsigned long long* keys, double* xi, long cap) {
 // by the one-sided stabilization pass, so each substep just records its graph in a 32-slot ring and
 // the sweeps are replayed (from the last checkpoint, or from zero over the last 32 graphs) only when
 // the pass needs the levels. The result is identical to sweeping every substep.
+// get_sdf_grid (src/sim.hpp:1538-1542, src/output_sdf.hpp:25-196), flat x-fastest
+template <class R>
+std::vector<R> Sim<R>::sdfGrid(int rx, int ry, int rz) {
+  if (rx < 1 || ry < 1 || rz < 1)
+    throw std::invalid_argument("get_sdf_grid: resolution must be positive");
+  cudaStream_t s = stream_;
+  const long total = (long)rx * ry * rz;
+  SdfGridP<R> G;
+  G.rx = rx, G.ry = ry, G.rz = rz;
+  G.px = per_[0], G.py = per_[1], G.pz = per_[2];
+  const int res[3] = {rx, ry, rz};
+  for (int a = 0; a < 3; ++a) {
+    G.o[a] = dmin_[a];
+    G.vox[a] = (dmax_[a] - dmin_[a]) / R(res[a]);
+  }
+  sdfA_.ensure(total, false, s);
+  sdfB_.ensure(total, false, s);
+  sdfState_.ensure(total, false, s);
+  ++launches_, kSdfInit<<<gridFor(total), kBlock, 0, s>>>(sdfA_.p, sdfState_.p, total);
+  if (numReal_ > 0)
+    ++launches_, kSdfSplat<<<gridFor(32L * numReal_, 128), 128, 0, s>>>(d_, numReal_, G, sdfA_.p, sdfState_.p);
+  const int iters = std::max(std::max(rx, ry), rz) * 4;
+  R* in = sdfA_.p;
+  R* out = sdfB_.p;
+  for (int it = 0; it < iters; ++it) {
+    ++launches_, kSdfEikonal<<<gridFor(total), kBlock, 0, s>>>(G, in, out, sdfState_.p, G.vox[0]);
+    std::swap(in, out);
+  }
+  KCHECK("sdf grid");
+  std::vector<R> h(total);
+  cudaCheck(cudaMemcpyAsync(h.data(), in, total * sizeof(R), cudaMemcpyDeviceToHost, s), "D2H");
+  sync();
+  return h;
+}
+
 // "ordered" stabilization (src/sim.hpp:357-400): fresh height levels, manifolds bucketed by
 // (level, colour), symmetric sweeps bottom-up then top-down until the residual drains
 template <class R>

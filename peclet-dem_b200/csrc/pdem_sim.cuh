@@ -206,6 +206,8 @@ class Sim {
   DBuf<u64> pairKeys_, prevKeys_;
   DBuf<uint8_t> persistent_, sideFlags_;
   DBuf<int> heights_, ordChanged_, ordKeysIn_, ordKeys_, ordPermIn_, ordPerm_;  // "ordered" pass
+  DBuf<R> sdfA_, sdfB_;  // get_sdf_grid ping-pong
+  DBuf<int> sdfState_;
   DBuf<R> lambda_, prevLambda_, vn0_, posImp_, prevPosImp_;
   DBuf<Q4<R>> lambdaT_, prevLambdaT_, vt0_;
   DBuf<ShapeDesc<R>> shapeD_;
@@ -334,6 +336,9 @@ class Sim {
   template <class T>
   void sortPairs(const T* kin, T* kout, const int* vin, int* vout, int n, int endBit);
   void orderedStabilization(int nm, V3<R> gHat, const SolveP<R>& ss, R vRestS);
+ public:
+  std::vector<R> sdfGrid(int rx, int ry, int rz);  // get_sdf_grid, flat x-fastest
+ private:
   template <class T>
   void exclusiveSum(const T* in, T* out, int n);
   template <class T>

@@ -86,6 +86,8 @@ _SIGS = {
     "max_overlap": (C.c_double, [_vp]),
     "export_lammps": (C.c_int, [_vp, C.c_char_p, C.c_int]),
     "write_vtp": (C.c_int, [_vp, C.c_char_p]),
+    "get_sdf_grid": (C.c_long, [_vp, C.c_int, C.c_int, C.c_int, _dbl_p, C.c_long]),
+    "export_sdf": (C.c_int, [_vp, C.c_char_p, C.c_int, C.c_int, C.c_int]),
     # diagnostics: the substep's intermediate products in the canonical order
     "debug_counts": (C.c_int, [_vp, _long_p]),
     "debug_pairs": (C.c_long, [_vp, _int_p, C.c_long]),
@@ -130,7 +132,7 @@ _SIGS = {
 class HzModel(C.Structure):
     """pdem_hz_model (include/pdem.h): device pointers and scalars of one Hertz sphere rollout."""
     _fields_ = [("n", C.c_int), ("ncontact", C.c_int), ("nplane", C.c_int), ("contacts", _vp), ("planes", _vp),
-                ("radius", _vp), ("mass", _vp), ("inertia", _vp), ("youngs", C.c_double),
+                ("radius", _vp), ("inv_mass", _vp), ("inv_inertia", _vp), ("youngs", C.c_double),
                 ("restitution", C.c_double), ("friction", C.c_double), ("poisson", C.c_double),
                 ("dt", C.c_double), ("gravity", C.c_double * 3)]
 
@@ -491,6 +493,21 @@ class CApiSimulation:
 
     def write_vtp(self, filename):
         self._call("write_vtp", os.fsencode(filename))
+
+    def get_sdf_grid(self, resolution):
+        """Packed-bed SDF over the domain (src/dem_bindings.cpp:344-355, src/output_sdf.hpp): the
+        flat x-fastest field returned as a C-order (rx, ry, rz) array, as the reference does."""
+        rx, ry, rz = (int(v) for v in resolution)
+        out = np.zeros(max(rx * ry * rz, 0), dtype=np.float64)
+        n = self._f["get_sdf_grid"](self._h, rx, ry, rz, _ptr(out), out.size)
+        if n < 0:
+            raise (ValueError if rx < 1 or ry < 1 or rz < 1 else RuntimeError)(f"get_sdf_grid: {self._api.error()}")
+        return out.astype(self._out_dtype).reshape(rx, ry, rz)
+
+    def export_sdf(self, filename, resolution):
+        """The same field written as a VTI image (src/dem_bindings.cpp:369-376, src/io.hpp:86-110)."""
+        rx, ry, rz = (int(v) for v in resolution)
+        self._call("export_sdf", os.fsencode(filename), rx, ry, rz)
 
     # ---- diagnostics (canonical-order intermediate products of the last substep) -----------------
     def debug_counts(self):
