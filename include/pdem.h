@@ -117,6 +117,20 @@ long pdem_get_scales(pdem_handle h, double* out, long cap);
 long pdem_get_masses(pdem_handle h, double* out, long cap);
 /* step(dt): ONE XPBD substep                    src/dem_bindings.cpp:342, src/sim.hpp:1456-1459,97-488 */
 int pdem_step(pdem_handle h, double dt);
+/* n substeps in one call (the caller's substep loop moved across the boundary; each substep is
+ * exactly pdem_step, and the step's own host reads stay, so this is not a captured graph) */
+int pdem_step_n(pdem_handle h, double dt, int n);
+/* the last substep's counters: candidate pairs P, contacts C, manifolds M, colours of the two
+ * colourings K, velocity / stabilization / position sweeps I_v / I_s / I_p, the error bits of
+ * bounded device loops (0 = none) and the maximum overlap */
+typedef struct {
+  long pairs, contacts, manifolds;
+  int colors_velocity, colors_position;
+  int velocity_sweeps, stabilization_sweeps, position_sweeps;
+  int status;
+  double max_overlap;
+} pdem_counters_t;
+int pdem_counters(pdem_handle h, pdem_counters_t* out);
 /* step_hertz(dt, substeps, skin_frac)           src/dem_bindings.cpp:139, src/sim.hpp:1167-1170,628-750 */
 int pdem_step_hertz(pdem_handle h, double dt, int substeps, double skin_frac);
 /* compute_overlaps                              src/dem_bindings.cpp:368, src/sim.hpp:1462,494-541 */

@@ -376,6 +376,31 @@ GETROWS(pdem_get_scales, 5, 1)
 GETROWS(pdem_get_masses, 6, 1)
 
 int pdem_step(pdem_handle h, double dt) { BODY(S.step((R)dt)); }
+int pdem_step_n(pdem_handle h, double dt, int n) {
+  BODY({
+    if (n < 0)
+      throw std::invalid_argument("step_n: n must be non-negative");
+    for (int k = 0; k < n; ++k)
+      S.step((R)dt);
+  });
+}
+int pdem_counters(pdem_handle h, pdem_counters_t* out) {
+  if (!out) {
+    g_err = "counters: null output";
+    return PDEM_ERR_INVALID;
+  }
+  return with(h, [&](auto& S) {
+    long sz[3];
+    int in[6];
+    double mo = 0;
+    S.lastCounters(sz, in, &mo);
+    out->pairs = sz[0], out->contacts = sz[1], out->manifolds = sz[2];
+    out->colors_velocity = in[0], out->colors_position = in[1];
+    out->velocity_sweeps = in[2], out->stabilization_sweeps = in[3], out->position_sweeps = in[4];
+    out->status = in[5];
+    out->max_overlap = mo;
+  });
+}
 int pdem_step_hertz(pdem_handle h, double dt, int substeps, double skin) {
   BODY(S.stepHertz((R)dt, substeps, (R)skin));
 }

@@ -10,14 +10,16 @@
 
 namespace pdem {
 
-// back-off iterations before a barrier wait gives up (a few seconds with __nanosleep(64))
+// polls before a barrier wait gives up (seconds at any back-off: each poll is an L2 round trip)
 constexpr long kBarrierSpins = 1L << 26;
 constexpr int kErrBarrier = 2;  // Counters::err bit: a grid barrier timed out
 
-// word[0] = arrivals, word[1] = generation; both zero before the launch
+// word[0] = arrivals, word[1] = generation; both zero before the launch; sleepNs = the back-off
+// of a waiting block between polls of the generation
 struct GridBar {
   unsigned* word;
   int* err;
+  unsigned sleepNs;
 };
 
 // Grid-wide barrier of a cooperative launch (all blocks co-resident). Thread 0 of each block
@@ -45,7 +47,8 @@ __device__ __forceinline__ bool gridBarrier(const GridBar& gb) {
           ok = 0;
           break;
         }
-        __nanosleep(64);
+        if (gb.sleepNs)
+          __nanosleep(gb.sleepNs);
       }
     }
     __threadfence();

@@ -1172,7 +1172,7 @@ void Sim<R>::colorBoth(int nm, int nc, int& ncolV, int& velLeft, int& ncolP, int
   const ColorJob jm{neM, nbM, mColor_.p, winner_.p, winner2_.p, mask_.p, colorAux_.p};
   const ColorJob jc{neC, nbC, cColor_.p, winnerP_.p, winnerP2_.p, maskP_.p, colorAux_.p + 5};
   gbar_.ensure(2, false, stream_);
-  const GridBar gb{gbar_.p, &ctr_.p->err};
+  const GridBar gb{gbar_.p, &ctr_.p->err, barrierSleepNs_};
   launchCoopB(kColorBoth<R>, kColorBlock, d_, jm, jc, std::max(nbM, nbC) + 2, gb, (const int*)topoFlags_.p,
               topoValid_ ? 1 : 0);
   KCHECK("colour loop");
@@ -1332,6 +1332,7 @@ void Sim<R>::demStep() {
   keptM_ = keptC_ = false;
   if (useGS_)
     colorBoth(nm, nc, ncolV, velLeft, ncolP, posLeft);
+  ncolVLast_ = ncolV, ncolPLast_ = ncolP;
   if (batch_ && (velLeft > 0 || posLeft > 0))
     throw std::runtime_error("batched scenes: uncoloured entries (Jacobi fallback) are not supported");
   // an unchanged graph keeps its colours, hence its colour order
@@ -1372,7 +1373,7 @@ void Sim<R>::demStep() {
   const bool velPersistent = useGS_ && !legacyFriction && velLeft == 0 && ncolV > 0 && velIters_ > 0;
   if (velPersistent) {
     gbar_.ensure(2, false, s);
-    const GridBar gb{gbar_.p, &ctr_.p->err};
+    const GridBar gb{gbar_.p, &ctr_.p->err, barrierSleepNs_};
     const R thr = usePGS ? R(0.02) * vRest : vRest;
     ctl(CTL_VEL_BEGIN, R(0), 0);
     if (batch_ && usePGS)
@@ -1450,7 +1451,7 @@ void Sim<R>::demStep() {
       const bool stabPersistent = ncolV > 0;
       if (stabPersistent) {
         gbar_.ensure(2, false, s);
-        const GridBar gb{gbar_.p, &ctr_.p->err};
+        const GridBar gb{gbar_.p, &ctr_.p->err, barrierSleepNs_};
         ctl(CTL_STAB_BEGIN, R(0), 0);
         if (batch_)
           ++launches_, kSweepScenes<R, 0, 2><<<numScenes_, kSceneBlock, 0, s>>>(d_, mOrder_.p, mOff_.p, iters, ss, vRestS);
@@ -1527,7 +1528,7 @@ void Sim<R>::demStep() {
   const bool posPersistent = useGS_ && posLeft == 0 && ncolP > 0 && posIters_ > 0;
   if (posPersistent) {
     gbar_.ensure(2, false, s);
-    const GridBar gb{gbar_.p, &ctr_.p->err};
+    const GridBar gb{gbar_.p, &ctr_.p->err, barrierSleepNs_};
     ctl(CTL_POS_BEGIN, R(0), 0);
     if (batch_)
       ++launches_, kSweepScenes<R, 2, 3><<<numScenes_, kSceneBlock, 0, s>>>(d_, cOrder_.p, cOff_.p, posIters_, sp, posTol);
@@ -1647,6 +1648,21 @@ R Sim<R>::maxOverlap() {
 // =============================================================================================
 // diagnostics
 // =============================================================================================
+// the last substep's sizes, colour counts, sweeps, overlap and error bits
+template <class R>
+void Sim<R>::lastCounters(long* sizes, int* ints, double* maxOverlap) {
+  const Counters<R> c = readCounters();
+  sizes[0] = c.pairCount;
+  sizes[1] = c.contactCount;
+  sizes[2] = c.manifoldCount;
+  ints[0] = ncolVLast_;
+  ints[1] = ncolPLast_;
+  ints[2] = c.velSweeps;
+  ints[3] = c.stabSweeps;
+  ints[4] = c.posSweeps;
+  ints[5] = c.err;
+  *maxOverlap = (double)c.maxOverlap;
+}
 template <class R>
 void Sim<R>::counts(long* out) {
   const Counters<R> c = readCounters();

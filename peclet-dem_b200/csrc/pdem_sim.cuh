@@ -1,6 +1,7 @@
 // Host side of the B200 substep: the Simulation facade state (src/sim.hpp:909-1670) and the step
 // orchestration (src/sim.hpp:97-488, 494-541, 628-750), owning all device memory.
 #pragma once
+#include <cstdlib>
 #include <cmath>
 #include <cstdint>
 #include <limits>
@@ -338,7 +339,15 @@ class Sim {
   void orderedStabilization(int nm, V3<R> gHat, const SolveP<R>& ss, R vRestS);
  public:
   std::vector<R> sdfGrid(int rx, int ry, int rz);  // get_sdf_grid, flat x-fastest
+  void lastCounters(long* sizes, int* ints, double* maxOverlap);
  private:
+  int ncolVLast_ = 0, ncolPLast_ = 0;  // colours of the last substep's two colourings
+  // back-off (ns) between polls of a waiting block at a grid barrier; PDEM_BARRIER_SLEEP_NS
+  // overrides it
+  unsigned barrierSleepNs_ = [] {
+    const char* e = std::getenv("PDEM_BARRIER_SLEEP_NS");
+    return e ? (unsigned)std::strtoul(e, nullptr, 10) : 64u;
+  }();
   template <class T>
   void exclusiveSum(const T* in, T* out, int n);
   template <class T>

@@ -78,6 +78,8 @@ _SIGS = {
     "get_scales": (C.c_long, [_vp, _dbl_p, C.c_long]),
     "get_masses": (C.c_long, [_vp, _dbl_p, C.c_long]),
     "step": (C.c_int, [_vp, C.c_double]),
+    "step_n": (C.c_int, [_vp, C.c_double, C.c_int]),
+    "counters": (C.c_int, [_vp, _vp]),
     "step_hertz": (C.c_int, [_vp, C.c_double, C.c_int, C.c_double]),
     "compute_overlaps": (C.c_int, [_vp, _dbl_p]),
     "num_particles": (C.c_int, [_vp]),
@@ -127,6 +129,14 @@ _SIGS = {
     "hz_backward": (C.c_int, [C.c_int, _vp, C.c_int, _vp, _vp, _vp, _vp, C.c_int, _vp]),
     "hz_jvp": (C.c_int, [C.c_int, _vp, C.c_int, _vp, _vp, _dbl_p, _vp, _vp]),
 }
+
+
+class Counters(C.Structure):
+    """pdem_counters_t (include/pdem.h): the last substep's sizes, colours, sweeps and status."""
+    _fields_ = [("pairs", C.c_long), ("contacts", C.c_long), ("manifolds", C.c_long),
+                ("colors_velocity", C.c_int), ("colors_position", C.c_int), ("velocity_sweeps", C.c_int),
+                ("stabilization_sweeps", C.c_int), ("position_sweeps", C.c_int), ("status", C.c_int),
+                ("max_overlap", C.c_double)]
 
 
 class HzModel(C.Structure):
@@ -457,6 +467,16 @@ class CApiSimulation:
     # ---- stepping ------------------------------------------------------------------------------
     def step(self, dt=0.0):
         self._call("step", float(dt))
+
+    def step_n(self, dt, n):
+        """n substeps in one call across the C ABI (each exactly `step(dt)`)."""
+        self._call("step_n", float(dt), int(n))
+
+    def counters(self):
+        """The last substep's P, C, M, colour counts, sweeps, error bits and max overlap."""
+        c = Counters()
+        self._call("counters", C.byref(c))
+        return {name: getattr(c, name) for name, _ in Counters._fields_}
 
     def step_hertz(self, dt, substeps=1, skin_frac=0.3):
         self._call("step_hertz", float(dt), int(substeps), float(skin_frac))

@@ -47,7 +47,7 @@ class HertzSpheres:
 
     def __init__(self, radius, mass, inertia, scene_first=None, planes=(), poisson=0.3, dt=2e-5,
                  gravity=(0.0, 0.0, -9.81), precision="fp64", checkpoint=100, skin=None, device=None,
-                 list_every=25):
+                 list_every=50):
         if precision not in ("fp64", "fp32"):
             raise ValueError("precision must be 'fp64' or 'fp32'")
         if not torch.cuda.is_available():
@@ -60,10 +60,15 @@ class HertzSpheres:
         self.device = torch.device(device or "cuda")
         as_t = lambda a: torch.as_tensor(np.asarray(a, np.float64).ravel(), dtype=self.dtype,
                                           device=self.device).contiguous()
-        self.r, self.m, self.I = as_t(radius), as_t(mass), as_t(inertia)
+        mass, inertia = np.asarray(mass, np.float64).ravel(), np.asarray(inertia, np.float64).ravel()
+        self.r = as_t(radius)
         self.n = int(self.r.numel())
-        if self.m.numel() != self.n or self.I.numel() != self.n:
+        if mass.size != self.n or inertia.size != self.n:
             raise ValueError("radius, mass and inertia must have one value per sphere")
+        if np.any(mass <= 0) or np.any(inertia <= 0):
+            raise ValueError("masses and moments of inertia must be positive")
+        # the engine's convention: inverse mass and inverse inertia, formed once in double
+        self.im, self.iI = as_t(1.0 / mass), as_t(1.0 / inertia)
         first = np.asarray(scene_first if scene_first is not None else [0, self.n], np.int64)
         if first[0] != 0 or first[-1] != self.n or np.any(np.diff(first) < 0):
             raise ValueError("scene_first must rise from 0 to the number of spheres")
@@ -105,7 +110,7 @@ class HertzSpheres:
         M.n, M.ncontact, M.nplane = self.n, nc, self.nplane
         M.contacts = _ptr(cont) if nc else None
         M.planes = _ptr(self.planes) if self.nplane else None
-        M.radius, M.mass, M.inertia = _ptr(self.r), _ptr(self.m), _ptr(self.I)
+        M.radius, M.inv_mass, M.inv_inertia = _ptr(self.r), _ptr(self.im), _ptr(self.iI)
         M.youngs, M.restitution, M.friction = theta
         M.poisson, M.dt = self.poisson, self.dt
         M.gravity[:] = self.gravity

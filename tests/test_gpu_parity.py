@@ -39,3 +39,24 @@ def test_fp64_vs_oracle(gpu_api, orc_api, name, mk, extra, steps):
 @pytest.mark.parametrize("name,mk,extra,steps", P.MATRIX[:8], ids=[m[0] for m in P.MATRIX[:8]])
 def test_fp32_bitexact_vs_reference(gpu_api, ref_api, name, mk, extra, steps):
     _run_pair(gpu_api, ref_api, name, mk, extra, steps, "fp32", 0.0)
+
+
+def test_step_n_and_counters(gpu_api):
+    """step_n(dt, n) is n calls of step(dt), bit for bit; counters() reports the last substep."""
+    import scenes as S
+    sc = S.dense_spheres()
+    a = P.build(gpu_api, sc, None, "fp32")
+    b = P.build(gpu_api, sc, None, "fp32")
+    for _ in range(5):
+        a.step(sc.dt)
+    b.step_n(sc.dt, 5)
+    assert not P.diff(P.snapshot(a), P.snapshot(b))
+    c = b.counters()
+    assert c["contacts"] == b.num_contacts() and c["manifolds"] == b.num_manifolds()
+    assert c["pairs"] >= c["manifolds"] > 0
+    assert c["colors_velocity"] > 0 and c["colors_position"] > 0
+    assert 1 <= c["velocity_sweeps"] <= sc.iterations[1] and 1 <= c["position_sweeps"] <= sc.iterations[0]
+    assert c["status"] == 0
+    assert c["max_overlap"] == b.max_overlap()
+    with pytest.raises(ValueError):
+        b.step_n(sc.dt, -1)
