@@ -25,6 +25,7 @@
 // whole rollout. Accumulation into bodies and parameters uses atomics, so sums come in an
 // unspecified order (forward forces too: the forward is deterministic up to summation order).
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <string>
 #include <utility>
@@ -200,6 +201,28 @@ struct Contact {
 template <class R>
 constexpr R kEtaC() {
   return R(-2) * R(0.9128709);
+}
+
+// contactPrimal's activity test alone (the same operations): touching spheres, or a sphere
+// overlapping its plane
+template <class R>
+__device__ bool contactActive(const Model<R>& M, long c, const StateView<R>& s) {
+  const int i = M.cont[2 * c], j = M.cont[2 * c + 1];
+  const R ri = M.r[i];
+  if (j >= 0) {
+    const R rj = M.r[j];
+    const V3<R> dx = sub(ld3(s.x, i), ld3(s.x, j));
+    const R d2 = dot(dx, dx), rr = ri + rj;
+    if (d2 > rr * rr * R(1.0001))
+      return false;
+    const R dd = sqrt(d2);
+    const R delta = rr - dd;
+    return !(delta <= R(0) || dd < R(1e-12));
+  }
+  const R* pl = M.planes + 6 * (-j - 1);
+  const V3<R> nh{pl[3], pl[4], pl[5]};
+  const R delta = ri - dot(sub(ld3(s.x, i), V3<R>{pl[0], pl[1], pl[2]}), nh);
+  return !(delta <= R(0));
 }
 
 template <class R>
@@ -481,19 +504,21 @@ __global__ void kContacts(Model<R> M, StateView<R> s, StateView<R> t, R* F, R* T
     }
   }
 }
+// one thread per component (coalesced, three times the threads of one per sphere); the
+// arithmetic per component is the engine's
 template <class R>
 __global__ void kIntegrate(Model<R> M, StateView<R> s, StateView<R> t, R* F, R* T) {
-  GRID_STRIDE(i, M.n) {
-    // every load before the first store: the compiler cannot prove the buffers apart
+  GRID_STRIDE(q, 3L * M.n) {
+    const int qi = (int)q, i = qi / 3, a = qi - 3 * i;  // 32-bit: the divide is a multiply
     const R im = M.im[i], iI = M.iI[i];
-    const V3<R> x = ld3(s.x, i), v = ld3(s.v, i), w = ld3(s.w, i), f = ld3(F, i), tq = ld3(T, i);
-    const V3<R> v1{v.x + (f.x * im + M.g[0]) * M.dt, v.y + (f.y * im + M.g[1]) * M.dt,
-                   v.z + (f.z * im + M.g[2]) * M.dt};
-    st3(t.v, i, v1);
-    st3(t.w, i, V3<R>{w.x + tq.x * iI * M.dt, w.y + tq.y * iI * M.dt, w.z + tq.z * iI * M.dt});
-    st3(t.x, i, V3<R>{x.x + v1.x * M.dt, x.y + v1.y * M.dt, x.z + v1.z * M.dt});
-    st3(F, i, V3<R>{R(0), R(0), R(0)});
-    st3(T, i, V3<R>{R(0), R(0), R(0)});
+    const R x = s.x[q], v = s.v[q], w = s.w[q], f = F[q], tq = T[q];
+    const R ga = a == 0 ? M.g[0] : (a == 1 ? M.g[1] : M.g[2]);  // no dynamic index into the parameters
+    const R v1 = v + (f * im + ga) * M.dt;
+    t.v[q] = v1;
+    t.w[q] = w + tq * iI * M.dt;
+    t.x[q] = x + v1 * M.dt;
+    F[q] = R(0);
+    T[q] = R(0);
   }
 }
 
@@ -502,15 +527,16 @@ __global__ void kIntegrate(Model<R> M, StateView<R> s, StateView<R> t, R* F, R* 
 // Fb, Tb = adjoints of the substep's force and torque sums
 template <class R>
 __global__ void kIntegrateAdj(Model<R> M, StateView<R> b1, StateView<R> b0, R* Fb, R* Tb) {
-  GRID_STRIDE(i, M.n) {
+  GRID_STRIDE(q, 3L * M.n) {
+    const int i = (int)q / 3;
     const R im = M.im[i], iI = M.iI[i];
-    const V3<R> xb = ld3(b1.x, i), vb = ld3(b1.v, i), wb = ld3(b1.w, i);
-    const V3<R> vbt = add(vb, mul(xb, M.dt));  // v' feeds x' = x + v' dt
-    st3(b0.x, i, xb);
-    st3(b0.v, i, vbt);
-    st3(b0.w, i, wb);
-    st3(Fb, i, V3<R>{vbt.x * im * M.dt, vbt.y * im * M.dt, vbt.z * im * M.dt});
-    st3(Tb, i, V3<R>{wb.x * iI * M.dt, wb.y * iI * M.dt, wb.z * iI * M.dt});
+    const R xb = b1.x[q], vb = b1.v[q], wb = b1.w[q];
+    const R vbt = vb + xb * M.dt;  // v' feeds x' = x + v' dt
+    b0.x[q] = xb;
+    b0.v[q] = vbt;
+    b0.w[q] = wb;
+    Fb[q] = vbt * im * M.dt;
+    Tb[q] = wb * iI * M.dt;
   }
 }
 __device__ inline void flushParams(double* thetaB, double gE, double ge, double gmu) {
@@ -525,20 +551,36 @@ __device__ inline void flushParams(double* thetaB, double gE, double ge, double 
     atomicAdd(&thetaB[2], gmu);
   }
 }
-// contact adjoints (hand reversal): one thread per contact; warps iterate in lockstep so the
-// parameter sums reduce with shuffles
+// contact adjoints (hand reversal), in two passes so that the few touching contacts do not set
+// the occupancy of the many apart: the scan clears the history adjoint of every apart contact
+// and lists the touching ones (count[slot]); the second pass reverses the listed contacts, its
+// warps in lockstep so the parameter sums reduce with shuffles, and clears the other counter
+// slot for the next substep's scan
+template <class R>
+__global__ void kContactsAdjScan(Model<R> M, StateView<R> s, StateView<R> b0, int* list, int* count) {
+  GRID_STRIDE(c, M.nc) {
+    if (contactActive(M, c, s))
+      list[atomicAdd(count, 1)] = (int)c;
+    else
+      st3(b0.xi, c, V3<R>{R(0), R(0), R(0)});  // cleared history: no dependence on the old one
+  }
+}
 template <class R>
 __global__ void kContactsAdj(Model<R> M, StateView<R> s, StateView<R> b1, StateView<R> b0, const R* Fb,
-                             const R* Tb, double* thetaB) {
+                             const R* Tb, double* thetaB, const int* list, const int* count, int* nextCount) {
   double gE = 0, ge = 0, gmu = 0;
-  for (long c0 = (long)blockIdx.x * blockDim.x + threadIdx.x - (threadIdx.x & 31); c0 < M.nc;
-       c0 += (long)gridDim.x * blockDim.x) {
-    const long c = c0 + (threadIdx.x & 31);
-    if (c < M.nc) {
+  const long na = *count;
+  if ((blockIdx.x | threadIdx.x) == 0)
+    *nextCount = 0;
+  for (long t0 = (long)blockIdx.x * blockDim.x + threadIdx.x - (threadIdx.x & 31); t0 < na;
+       t0 += (long)gridDim.x * blockDim.x) {
+    const long t = t0 + (threadIdx.x & 31);
+    if (t < na) {
+      const long c = list[t];
       Contact<R> C;
       contactPrimal(M, c, s, C);
-      if (!C.active) {
-        st3(b0.xi, c, V3<R>{R(0), R(0), R(0)});  // cleared history: no dependence on the old one
+      if (!C.active) {  // cannot happen (the scan ran the same test); kept for safety
+        st3(b0.xi, c, V3<R>{R(0), R(0), R(0)});
       } else {
         const int i = C.i, j = C.j;
         V3<R> fb = ld3(Fb, i);
@@ -1016,6 +1058,8 @@ template <class R>
 Model<R> makeModel(const pdem_hz_model* h) {
   if (!h || h->n < 0 || h->ncontact < 0 || h->nplane < 0)
     throw Fail{PDEM_ERR_INVALID, "hz model: negative sizes"};
+  if (3L * h->n > (long)INT_MAX)
+    throw Fail{PDEM_ERR_INVALID, "hz model: too many spheres (3 n must fit an int)"};
   if (h->n > 0 && (!h->radius || !h->inv_mass || !h->inv_inertia))
     throw Fail{PDEM_ERR_INVALID, "hz model: radius, inverse mass and inverse inertia are required"};
   if ((h->ncontact > 0 && !h->contacts) || (h->nplane > 0 && !h->planes))
@@ -1055,7 +1099,7 @@ void forward(const pdem_hz_model* h, int steps, int store, R* traj, R* work, cud
     const StateView<R> s = view(traj + S * a, M.n), t = view(traj + S * b, M.n);
     if (M.nc > 0)
       kContacts<R><<<pdem::gridFor(M.nc), pdem::kBlock, 0, st>>>(M, s, t, F, T);
-    kIntegrate<R><<<pdem::gridFor(M.n), pdem::kBlock, 0, st>>>(M, s, t, F, T);
+    kIntegrate<R><<<pdem::gridFor(3L * M.n), pdem::kBlock, 0, st>>>(M, s, t, F, T);
   }
   if (!store && (steps & 1) == 0)  // the final state of a ping-pong run always ends in block 1
     check(cudaMemcpyAsync(traj + S, traj, S * sizeof(R), cudaMemcpyDeviceToDevice, st), "D2D");
@@ -1076,16 +1120,24 @@ void backward(const pdem_hz_model* h, int steps, const R* traj, R* adj, double* 
   R* Fb = work;
   R* Tb = work + 3 * (size_t)M.n;
   R* other = work + 6 * (size_t)M.n;  // second adjoint state, ping-pong with adj
+  int* cnt = reinterpret_cast<int*>(other + SZ);  // two counter slots, then the active list
+  int* list = cnt + 2;
+  check(cudaMemsetAsync(cnt, 0, 2 * sizeof(int), st), "memset");
   R* cur = adj;
   for (int k = steps - 1; k >= 0; --k) {
     const StateView<R> s = view(const_cast<R*>(traj) + SZ * k, M.n);
     const StateView<R> b1 = view(cur, M.n), b0 = view(other, M.n);
-    kIntegrateAdj<R><<<pdem::gridFor(M.n), pdem::kBlock, 0, st>>>(M, b1, b0, Fb, Tb);
+    kIntegrateAdj<R><<<pdem::gridFor(3L * M.n), pdem::kBlock, 0, st>>>(M, b1, b0, Fb, Tb);
     if (M.nc > 0) {
-      if (mode == 0)
-        kContactsAdj<R><<<pdem::gridFor(M.nc), pdem::kBlock, 0, st>>>(M, s, b1, b0, Fb, Tb, thetaB);
-      else
+      if (mode == 0) {
+        kContactsAdjScan<R><<<pdem::gridFor(M.nc), pdem::kBlock, 0, st>>>(M, s, b0, list, cnt + (k & 1));
+        // the active list is a small part of the contacts: a grid of a few blocks per SM strides it
+        const int g = std::min(pdem::gridFor(M.nc), 4 * pdem::kNumSMs);
+        kContactsAdj<R><<<g, pdem::kBlock, 0, st>>>(M, s, b1, b0, Fb, Tb, thetaB, list, cnt + (k & 1),
+                                                    cnt + ((k + 1) & 1));
+      } else {
         kContactsAdjDual<R><<<pdem::gridFor(M.nc), pdem::kBlock, 0, st>>>(M, s, b1, b0, Fb, Tb, thetaB);
+      }
     }
     std::swap(cur, other);
   }
@@ -1234,7 +1286,9 @@ long pdem_hz_state_size(int n, int ncontact) {
 long pdem_hz_work_size(int n, int ncontact) {
   if (n < 0 || ncontact < 0)
     return -1;
-  const size_t a = 6 * (size_t)n + stateSize(n, ncontact), b = 12 * (size_t)n;
+  // backward: force/torque adjoints, a second adjoint state, then (as ints) two counters and the
+  // active-contact list; jvp: four force/torque arrays
+  const size_t a = 6 * (size_t)n + stateSize(n, ncontact) + (size_t)ncontact + 2, b = 12 * (size_t)n;
   return (long)(a > b ? a : b);
 }
 
