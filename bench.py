@@ -182,6 +182,7 @@ def run_batched(args, rank, world, dist, dem):
             sim.step(dt)
         t = max_over_ranks(sim.timer_stop() / 1e3, dist, "cuda")
         sweeps = sim.scene_counters()
+        tune = sim.scene_block()  # settled during the warm-up substeps
         x = sim.get_positions()  # the error is measured at the end of the timed substeps
         sim.profile_enable(True)
         for _ in range(args.steps * SUBSTEPS):
@@ -190,19 +191,19 @@ def run_batched(args, rank, world, dist, dem):
         sim.profile_enable(False)
         sim.close()
         per_step = {k: round(ms / args.steps, 3) for k, (ms, c) in stages.items() if c}
-        return t, per_step, launches, sweeps, x
+        return t, per_step, launches, sweeps, x, tune
 
-    t64, st64, l64, sw64, x64 = one("fp64")
-    tmx, stmx, lmx, _, xmx = one("mixed")
+    t64, st64, l64, sw64, x64, tu64 = one("fp64")
+    tmx, stmx, lmx, _, xmx, tumx = one("mixed")
     err = np.linalg.norm(xmx - x64, axis=1) / radius
     err_max = max_over_ranks(float(err.max()) if err.size else 0.0, dist, "cuda")
     rate = lambda t: n_all * SUBSTEPS * args.steps / t
     return {"workload": f"rotating_drums_{len(scenes)}_scenes", "scenes": len(scenes), "particles": n_all,
             "unit": METRIC, "scaling": "weak (scenes split over ranks)",
             "fp64": {"value": rate(t64), "ms_per_step": 1e3 * t64 / args.steps, "gpu_launches": l64,
-                     "stages_ms_per_step": st64, "err_vs_fp64": 0.0},
+                     "stages_ms_per_step": st64, "err_vs_fp64": 0.0, "autotuned_scene_block": tu64},
             "mixed": {"value": rate(tmx), "ms_per_step": 1e3 * tmx / args.steps, "gpu_launches": lmx,
-                      "stages_ms_per_step": stmx,
+                      "stages_ms_per_step": stmx, "autotuned_scene_block": tumx,
                       "err_vs_fp64": {"max_position_error_radii": err_max,
                                       "median_position_error_radii": float(np.median(err)) if err.size else 0.0,
                                       "after_substeps": (args.warmup + args.steps) * SUBSTEPS}},

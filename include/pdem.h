@@ -223,6 +223,11 @@ int pdem_debug_sweeps(pdem_handle h, long* out4);
 int pdem_find_pairs_static(const double* d_xyz, const double* d_radius, int n, double margin, double box_cap,
                            int* d_pairs, long pair_cap, long* out_count, void* stream);
 
+/* batched form: the block size the launch shape autotuner chose for the per-scene sweep loops
+ * (0 while it is still trying the candidates 64, 128, 256, 512 over the first batched substeps;
+ * the environment variable PDEM_SCENE_BLOCK fixes it instead) and the mean sweep-loop time of each
+ * candidate in ms (cap values) */
+int pdem_scene_block(pdem_handle h, int* block, double* ms, int cap);
 /* get_sdf_grid(resolution)                      src/dem_bindings.cpp:344-355, src/sim.hpp:1538-1542
  * packed-bed SDF over the domain (src/output_sdf.hpp:25-196), flat x-fastest; returns rx*ry*rz
  * (only cap written), or -1 with pdem_last_error() set */

@@ -458,6 +458,13 @@ int pdem_write_vtp(pdem_handle h, const char* fn) {
   });
 }
 
+int pdem_scene_block(pdem_handle h, int* block, double* ms, int cap) {
+  BODY({
+    *block = S.tunedSceneBlock();
+    for (int c = 0; c < cap && c < S.kTuneCands; ++c)
+      ms[c] = (double)S.tuneMs()[c];
+  });
+}
 long pdem_get_sdf_grid(pdem_handle h, int rx, int ry, int rz, double* out, long cap) {
   long n = -1;
   const int st = with(h, [&](auto& S) {

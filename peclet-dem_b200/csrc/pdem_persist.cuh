@@ -141,10 +141,11 @@ __global__ void __launch_bounds__(kBlock) kSweepLoop(Dev<R> d, const int* order,
 // blocks-worth of threads sweeps them in colour order with block barriers, and the block ends its
 // own loop at the scene's adaptive stop. No grid-wide barrier and no cooperative launch: scenes are
 // independent. The host has run the first sweep's BEGIN for every scene (kCtlScenes).
-constexpr int kSceneBlock = 128;
+constexpr int kSceneBlock = 128;      // default block of the per-scene sweep loops
+constexpr int kSceneBlockMax = 512;   // largest block the launch shape autotuner tries
 
 template <class R, int KIND, int LOOP>
-__global__ void __launch_bounds__(kSceneBlock) kSweepScenes(Dev<R> d, const int* order, const int* off, int iters,
+__global__ void __launch_bounds__(kSceneBlockMax) kSweepScenes(Dev<R> d, const int* order, const int* off, int iters,
                                                             SolveP<R> P, R thr) {
   const int s = blockIdx.x;
   SceneCtl<R>& q = d.scn[s];

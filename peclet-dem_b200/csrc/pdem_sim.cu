@@ -60,6 +60,10 @@ Sim<R>::~Sim() {
     cudaEventDestroy(tStart_);
     cudaEventDestroy(tStop_);
   }
+  for (auto& pr : tuneEv_)
+    for (auto& e : pr)
+      if (e)
+        cudaEventDestroy(e);
 }
 
 // src/particles.hpp:194-288
@@ -1376,10 +1380,12 @@ void Sim<R>::demStep() {
     const GridBar gb{gbar_.p, &ctr_.p->err, barrierSleepNs_};
     const R thr = usePGS ? R(0.02) * vRest : vRest;
     ctl(CTL_VEL_BEGIN, R(0), 0);
+    if (batch_)
+      tuneBegin();
     if (batch_ && usePGS)
-      ++launches_, kSweepScenes<R, 0, 1><<<numScenes_, kSceneBlock, 0, s>>>(d_, mOrder_.p, mOff_.p, velIters_, sp, thr);
+      ++launches_, kSweepScenes<R, 0, 1><<<numScenes_, sceneBlock(), 0, s>>>(d_, mOrder_.p, mOff_.p, velIters_, sp, thr);
     else if (batch_)
-      ++launches_, kSweepScenes<R, 1, 1><<<numScenes_, kSceneBlock, 0, s>>>(d_, mOrder_.p, mOff_.p, velIters_, sp, thr);
+      ++launches_, kSweepScenes<R, 1, 1><<<numScenes_, sceneBlock(), 0, s>>>(d_, mOrder_.p, mOff_.p, velIters_, sp, thr);
     else if (usePGS)
       launchCoop(kSweepLoop<R, 0, 1>, d_, (const int*)mOrder_.p, (const int*)mOff_.p, ncolV, velIters_, sp, thr, gb);
     else
@@ -1454,7 +1460,7 @@ void Sim<R>::demStep() {
         const GridBar gb{gbar_.p, &ctr_.p->err, barrierSleepNs_};
         ctl(CTL_STAB_BEGIN, R(0), 0);
         if (batch_)
-          ++launches_, kSweepScenes<R, 0, 2><<<numScenes_, kSceneBlock, 0, s>>>(d_, mOrder_.p, mOff_.p, iters, ss, vRestS);
+          ++launches_, kSweepScenes<R, 0, 2><<<numScenes_, sceneBlock(), 0, s>>>(d_, mOrder_.p, mOff_.p, iters, ss, vRestS);
         else
           launchCoop(kSweepLoop<R, 0, 2>, d_, (const int*)mOrder_.p, (const int*)mOff_.p, ncolV, iters, ss, vRestS, gb);
       }
@@ -1530,8 +1536,10 @@ void Sim<R>::demStep() {
     gbar_.ensure(2, false, s);
     const GridBar gb{gbar_.p, &ctr_.p->err, barrierSleepNs_};
     ctl(CTL_POS_BEGIN, R(0), 0);
-    if (batch_)
-      ++launches_, kSweepScenes<R, 2, 3><<<numScenes_, kSceneBlock, 0, s>>>(d_, cOrder_.p, cOff_.p, posIters_, sp, posTol);
+    if (batch_) {
+      ++launches_, kSweepScenes<R, 2, 3><<<numScenes_, sceneBlock(), 0, s>>>(d_, cOrder_.p, cOff_.p, posIters_, sp, posTol);
+      tuneEnd();
+    }
     else
       launchCoop(kSweepLoop<R, 2, 3>, d_, (const int*)cOrder_.p, (const int*)cOff_.p, ncolP, posIters_, sp, posTol, gb);
     KCHECK("position loop");
@@ -2284,6 +2292,55 @@ void Sim<R>::ctl(int op, R thr, int mode) {
   else
     ++launches_, kCtl<<<1, 1, 0, stream_>>>(ctr_.p, op, thr, mode);
 }
+// ---- launch shape autotuner of the per-scene sweep loops (batched form) ----
+// The block size of kSweepScenes does not change any result (a colour class is an independent set;
+// the saturated colour runs on one thread), so it is tuned online: the first kTuneRounds x
+// candidates batched substeps cycle through the candidate sizes, timing the main velocity and
+// position sweep loops with events; the fastest size then stays. PDEM_SCENE_BLOCK fixes a size
+// and turns the tuning off.
+template <class R>
+int Sim<R>::sceneBlock() const {
+  return tuning_ ? kTuneBlocks[tuneStep_ % kTuneCands] : sceneBlock_;
+}
+template <class R>
+void Sim<R>::tuneBegin() {
+  if (!tuning_)
+    return;
+  if (!tuneEv_[0][0])
+    for (auto& pr : tuneEv_)
+      for (auto& e : pr)
+        cudaCheck(cudaEventCreate(&e), "event");
+  const int slot = tuneStep_ % (kTuneCands * kTuneRounds);
+  cudaCheck(cudaEventRecord(tuneEv_[slot][0], stream_), "event");
+  tuneOpen_ = true;
+}
+template <class R>
+void Sim<R>::tuneEnd() {
+  if (!tuning_ || !tuneOpen_)
+    return;
+  tuneOpen_ = false;
+  const int slot = tuneStep_ % (kTuneCands * kTuneRounds);
+  cudaCheck(cudaEventRecord(tuneEv_[slot][1], stream_), "event");
+  if (++tuneStep_ < kTuneCands * kTuneRounds)
+    return;
+  sync();
+  float best = 0;
+  for (int c = 0; c < kTuneCands; ++c) {
+    float tot = 0;
+    for (int r = 0; r < kTuneRounds; ++r) {
+      float ms = 0;
+      cudaCheck(cudaEventElapsedTime(&ms, tuneEv_[r * kTuneCands + c][0], tuneEv_[r * kTuneCands + c][1]), "event");
+      tot += ms;
+    }
+    tuneMs_[c] = tot / kTuneRounds;
+    if (c == 0 || tot < best) {
+      best = tot;
+      sceneBlock_ = kTuneBlocks[c];
+    }
+  }
+  tuning_ = false;
+}
+
 template <class R>
 void Sim<R>::setScenes(int S, const int* first) {
   if (S < 1 || S > 1023)
@@ -2299,6 +2356,13 @@ void Sim<R>::setScenes(int S, const int* first) {
   vValid_ = false;
   numScenes_ = S;
   sceneFirstHost_.assign(first, first + S + 1);
+  if (const char* e = std::getenv("PDEM_SCENE_BLOCK")) {
+    sceneBlock_ = std::max(32, std::min(kSceneBlockMax, (int)std::strtol(e, nullptr, 10) / 32 * 32));
+    tuning_ = false;
+  } else {
+    tuning_ = true;
+    tuneStep_ = 0;
+  }
   maxSceneBodies_ = 0;
   for (int s = 0; s < S; ++s)
     maxSceneBodies_ = std::max(maxSceneBodies_, first[s + 1] - first[s]);

@@ -338,6 +338,21 @@ class Sim {
   void sortPairs(const T* kin, T* kout, const int* vin, int* vout, int n, int endBit);
   void orderedStabilization(int nm, V3<R> gHat, const SolveP<R>& ss, R vRestS);
  public:
+  // launch shape autotuner of the per-scene sweep loops: the chosen block (0 while tuning) and the
+  // mean sweep-loop time of each candidate (ms per substep)
+  int tunedSceneBlock() const { return tuning_ ? 0 : sceneBlock_; }
+  const float* tuneMs() const { return tuneMs_; }
+  static constexpr int kTuneCands = 4, kTuneRounds = 3;
+  static constexpr int kTuneBlocks[kTuneCands] = {64, 128, 256, 512};
+ private:
+  int sceneBlock() const;
+  void tuneBegin();
+  void tuneEnd();
+  int sceneBlock_ = 128, tuneStep_ = 0;
+  bool tuning_ = false, tuneOpen_ = false;
+  cudaEvent_t tuneEv_[kTuneCands * kTuneRounds][2] = {};
+  float tuneMs_[kTuneCands] = {0, 0, 0, 0};
+ public:
   std::vector<R> sdfGrid(int rx, int ry, int rz);  // get_sdf_grid, flat x-fastest
   void lastCounters(long* sizes, int* ints, double* maxOverlap);
  private:

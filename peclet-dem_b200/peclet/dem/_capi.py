@@ -118,6 +118,7 @@ _SIGS = {
     "set_scene_material": (C.c_int, [_vp, C.c_int, C.c_double, C.c_double]),
     "set_wall_scene": (C.c_int, [_vp, C.c_int, C.c_int]),
     "scene_counters": (C.c_long, [_vp, _dbl_p, C.c_long]),
+    "scene_block": (C.c_int, [_vp, _int_p, _dbl_p, C.c_int]),
     # candidate pairs over caller-owned device arrays, with no allocation (pdem_static.cu)
     "find_pairs_static": (C.c_int, [_vp, _vp, C.c_int, C.c_double, C.c_double, _vp, C.c_long, _long_p, _vp]),
     # forward, adjoint and tangent-linear runs of the Hertz sphere substep (pdem_adjoint.cu)
@@ -370,6 +371,14 @@ class CApiSimulation:
 
     def set_wall_scene(self, wall, scene):
         self._call("set_wall_scene", int(wall), int(scene))
+
+    def scene_block(self):
+        """The per-scene sweep block the launch shape autotuner chose (0 while tuning) and each
+        candidate's mean sweep-loop time (ms per substep)."""
+        b = C.c_int(0)
+        ms = np.zeros(4)
+        self._call("scene_block", C.byref(b), _ptr(ms), 4)
+        return {"block": b.value, "candidates": [64, 128, 256, 512], "ms": ms.tolist()}
 
     def scene_counters(self):
         """(S, 5): max overlap, max approach, velocity / stabilization / position sweeps."""

@@ -85,3 +85,25 @@ def test_batch_rejects_periodic(gpu_api):
     apply_batch(batch, [sc, S.polydisperse_periodic(seed=14)])
     with pytest.raises(RuntimeError):
         batch.step(sc.dt)
+
+
+def test_autotuned_block_keeps_results(gpu_api, monkeypatch):
+    """The launch shape autotuner cycles block sizes over the first substeps and keeps the fastest;
+    the results equal a run with the block fixed (the block size changes no result)."""
+    drums = _drums()
+    scenes = [d[0] for d in drums]
+    runs = []
+    for fixed in (None, "64"):
+        if fixed:
+            monkeypatch.setenv("PDEM_SCENE_BLOCK", fixed)
+        else:
+            monkeypatch.delenv("PDEM_SCENE_BLOCK", raising=False)
+        batch = CApiSimulation(gpu_api, sum(sc.n for sc in scenes) + 8, "fp32")
+        apply_batch(batch, scenes, [d[1] for d in drums])
+        for _ in range(16):
+            batch.step(scenes[0].dt)
+        runs.append((P.snapshot(batch, products=False), batch.scene_block()))
+    (a, ta), (b, tb) = runs
+    assert ta["block"] in (64, 128, 256, 512) and all(m > 0 for m in ta["ms"])
+    assert tb["block"] == 64
+    assert not P.diff(a, b)
