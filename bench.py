@@ -525,8 +525,10 @@ def run_ours(args):
     t_max = max_over_ranks(dev_ms / 1e3, dist, "cuda")
     value = aggregate_rate(world, n, SUBSTEPS, args.steps, t_max)
 
-    # ---- end to end through the public API with host buffers ----
-    force = np.zeros((n, 3))
+    # ---- end to end through the public API with host buffers (pinned, as a data loader's) ----
+    import torch
+    pinned = lambda: torch.zeros((n, 3), dtype=torch.float64, pin_memory=True).numpy()
+    force, pos, vel = pinned(), pinned(), pinned()
     barrier()
     te = time.perf_counter()
     allocs = dem._API.fn["debug_allocs"]
@@ -537,8 +539,8 @@ def run_ours(args):
         sim.set_external_forces(force)
         for _ in range(SUBSTEPS):
             sim.step(scene.dt)
-        pos = sim.get_positions()
-        vel = sim.get_velocities()
+        sim.get_positions(out=pos)
+        sim.get_velocities(out=vel)
         laps.append(round(1e3 * (time.perf_counter() - tl), 2))
     e2e_s = time.perf_counter() - te
     assert np.all(np.isfinite(pos)) and np.all(np.isfinite(vel))

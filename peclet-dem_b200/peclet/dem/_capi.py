@@ -443,26 +443,38 @@ class CApiSimulation:
     def get_growth_rate(self):
         return float(self._f["get_growth_rate"](self._h))
 
-    def _get(self, name, cols):
+    def _get(self, name, cols, out=None):
+        """Rows of a per-particle field. With `out` (an extension: a C-contiguous float64 array of at
+        least n x cols values, e.g. in pinned host memory) the values are written there and a view
+        of it is returned; otherwise a new array of the precision's dtype."""
         n = self.num_particles()
-        out = np.empty(n * cols, dtype=np.float64)
-        got = self._f[name](self._h, _ptr(out), int(out.size))
+        if out is not None:
+            buf = out.reshape(-1)
+            if out.dtype != np.float64 or not out.flags.c_contiguous or buf.size < n * cols:
+                raise ValueError(f"{name}: out must be C-contiguous float64 with {n * cols} values")
+            got = self._f[name](self._h, _ptr(buf), int(n * cols))
+            if got < 0:
+                self._api.check(ERR_RUNTIME, name)
+            res = buf[: min(got, n * cols)]
+            return res.reshape(-1, cols) if cols > 1 else res
+        buf = np.empty(n * cols, dtype=np.float64)
+        got = self._f[name](self._h, _ptr(buf), int(buf.size))
         if got < 0:
             self._api.check(ERR_RUNTIME, name)
-        out = out[: min(got, out.size)].astype(self._out_dtype)
-        return out.reshape(-1, cols) if cols > 1 else out
+        res = buf[: min(got, buf.size)].astype(self._out_dtype)
+        return res.reshape(-1, cols) if cols > 1 else res
 
-    def get_positions(self):
-        return self._get("get_positions", 3)
+    def get_positions(self, out=None):
+        return self._get("get_positions", 3, out)
 
-    def get_velocities(self):
-        return self._get("get_velocities", 3)
+    def get_velocities(self, out=None):
+        return self._get("get_velocities", 3, out)
 
-    def get_quaternions(self):
-        return self._get("get_quaternions", 4)
+    def get_quaternions(self, out=None):
+        return self._get("get_quaternions", 4, out)
 
-    def get_angular_velocities(self):
-        return self._get("get_angular_velocities", 3)
+    def get_angular_velocities(self, out=None):
+        return self._get("get_angular_velocities", 3, out)
 
     def get_inv_inertia(self):
         return self._get("get_inv_inertia", 3)
