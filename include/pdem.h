@@ -223,6 +223,14 @@ int pdem_debug_sweeps(pdem_handle h, long* out4);
 int pdem_find_pairs_static(const double* d_xyz, const double* d_radius, int n, double margin, double box_cap,
                            int* d_pairs, long pair_cap, long* out_count, void* stream);
 
+/* get_positions_view / get_velocities_view / get_external_forces_view / get_inv_mass_view
+ *                                               src/dem_bindings.cpp:302-334
+ * zero-copy device arrays: field 0 positions, 1 velocities, 2 external forces (writable: the step
+ * reads it), 3 inverse mass. Returns the device pointer, the number of rows, the row stride in
+ * elements (4: x, y, z and a pad; 1 for the inverse mass) and the element size (8 at FP64, 4 at
+ * FP32 and in the mixed form, whose positions here are the float state). The stream is
+ * synchronised first. Valid until a call that can grow the particle buffers. */
+int pdem_device_view(pdem_handle h, int field, void** ptr, long* rows, int* row_stride, int* elem_bytes);
 /* batched form: the block size the launch shape autotuner chose for the per-scene sweep loops
  * (0 while it is still trying the candidates 64, 128, 256, 512 over the first batched substeps;
  * the environment variable PDEM_SCENE_BLOCK fixes it instead) and the mean sweep-loop time of each

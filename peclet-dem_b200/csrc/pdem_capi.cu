@@ -458,6 +458,12 @@ int pdem_write_vtp(pdem_handle h, const char* fn) {
   });
 }
 
+int pdem_device_view(pdem_handle h, int field, void** ptr, long* rows, int* row_stride, int* elem_bytes) {
+  BODY({
+    S.deviceView(field, ptr, rows, row_stride);
+    *elem_bytes = (int)sizeof(R);
+  });
+}
 int pdem_scene_block(pdem_handle h, int* block, double* ms, int cap) {
   BODY({
     *block = S.tunedSceneBlock();

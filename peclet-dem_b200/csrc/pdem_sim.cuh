@@ -353,6 +353,16 @@ class Sim {
   cudaEvent_t tuneEv_[kTuneCands * kTuneRounds][2] = {};
   float tuneMs_[kTuneCands] = {0, 0, 0, 0};
  public:
+  // zero-copy device arrays (get_*_view): 0 positions, 1 velocities, 2 external forces (rows of 4,
+  // the first 3 used), 3 inverse mass (rows of 1); synchronises the stream first
+  void deviceView(int field, void** ptr, long* rows, int* rowStride) {
+    if (field < 0 || field > 3)
+      throw std::invalid_argument("device view: field must be 0..3");
+    sync();
+    *rows = numReal_;
+    *rowStride = field == 3 ? 1 : 4;
+    *ptr = field == 0 ? (void*)pos_.p : field == 1 ? (void*)vel_.p : field == 2 ? (void*)extF_.p : (void*)invMass_.p;
+  }
   std::vector<R> sdfGrid(int rx, int ry, int rz);  // get_sdf_grid, flat x-fastest
   void lastCounters(long* sizes, int* ints, double* maxOverlap);
  private:

@@ -119,6 +119,7 @@ _SIGS = {
     "set_wall_scene": (C.c_int, [_vp, C.c_int, C.c_int]),
     "scene_counters": (C.c_long, [_vp, _dbl_p, C.c_long]),
     "scene_block": (C.c_int, [_vp, _int_p, _dbl_p, C.c_int]),
+    "device_view": (C.c_int, [_vp, C.c_int, C.POINTER(_vp), _long_p, _int_p, _int_p]),
     # candidate pairs over caller-owned device arrays, with no allocation (pdem_static.cu)
     "find_pairs_static": (C.c_int, [_vp, _vp, C.c_int, C.c_double, C.c_double, _vp, C.c_long, _long_p, _vp]),
     # forward, adjoint and tangent-linear runs of the Hertz sphere substep (pdem_adjoint.cu)
@@ -371,6 +372,42 @@ class CApiSimulation:
 
     def set_wall_scene(self, wall, scene):
         self._call("set_wall_scene", int(wall), int(scene))
+
+    # ---- zero-copy device arrays (src/dem_bindings.cpp:302-334) --------------------------------
+    def _view(self, field, cols):
+        import torch
+
+        ptr, rows, stride, eb = _vp(), C.c_long(0), C.c_int(0), C.c_int(0)
+        self._call("device_view", int(field), C.byref(ptr), C.byref(rows), C.byref(stride), C.byref(eb))
+
+        class _DeviceArray:  # __cuda_array_interface__ v3 over the simulation's memory
+            pass
+
+        a = _DeviceArray()
+        a.owner = self  # the simulation outlives the array
+        shape = (rows.value, cols) if cols > 1 else (rows.value,)
+        strides = (stride.value * eb.value, eb.value) if cols > 1 else (eb.value,)
+        a.__cuda_array_interface__ = {"shape": shape, "strides": strides, "typestr": "<f8" if eb.value == 8 else "<f4",
+                                      "data": (ptr.value or 0, False), "version": 3, "stream": None}
+        return torch.as_tensor(a, device="cuda")
+
+    def get_positions_view(self):
+        """Zero-copy (N,3) device array of positions (a torch tensor aliasing the simulation's
+        memory; DLPack- and __cuda_array_interface__-capable). Take it after each step."""
+        return self._view(0, 3)
+
+    def get_velocities_view(self):
+        """Zero-copy (N,3) device array of velocities."""
+        return self._view(1, 3)
+
+    def get_external_forces_view(self):
+        """Zero-copy (N,3) device array of the external force; writes reach the next step once
+        they are complete (synchronise the writing stream before stepping)."""
+        return self._view(2, 3)
+
+    def get_inv_mass_view(self):
+        """Zero-copy (N,) device array of inverse masses (read-only use)."""
+        return self._view(3, 1)
 
     def scene_block(self):
         """The per-scene sweep block the launch shape autotuner chose (0 while tuning) and each

@@ -60,3 +60,31 @@ def test_step_n_and_counters(gpu_api):
     assert c["max_overlap"] == b.max_overlap()
     with pytest.raises(ValueError):
         b.step_n(sc.dt, -1)
+
+
+def test_device_views(gpu_api):
+    """get_*_view alias the simulation's device memory: they equal the getters, and forces written
+    into the external-force view drive the next steps exactly as set_external_forces does."""
+    import numpy as np
+    import scenes as S
+    sc = S.dense_spheres()
+    for prec in ("fp64", "fp32"):
+        a = P.build(gpu_api, sc, None, prec)
+        b = P.build(gpu_api, sc, None, prec)
+        a.step(sc.dt)
+        b.step(sc.dt)
+        pv, vv, mv = a.get_positions_view(), a.get_velocities_view(), a.get_inv_mass_view()
+        assert pv.shape == (sc.n, 3) and mv.shape == (sc.n,)
+        np.testing.assert_array_equal(pv.cpu().numpy(), a.get_positions())
+        np.testing.assert_array_equal(vv.cpu().numpy(), a.get_velocities())
+        np.testing.assert_array_equal(mv.cpu().numpy().astype(np.float64), np.asarray(sc.inv_mass, dtype=mv.cpu().numpy().dtype))
+        f = np.random.default_rng(3).normal(scale=1e-4, size=(sc.n, 3))
+        fv = a.get_external_forces_view()
+        torch = __import__("torch")
+        fv.copy_(torch.as_tensor(f, dtype=fv.dtype, device=fv.device))
+        torch.cuda.synchronize()  # the write (on torch's stream) completes before the next step
+        b.set_external_forces(f.astype(fv.cpu().numpy().dtype).astype(np.float64))
+        for _ in range(3):
+            a.step(sc.dt)
+            b.step(sc.dt)
+        assert not P.diff(P.snapshot(a), P.snapshot(b)), prec
