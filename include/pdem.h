@@ -223,6 +223,8 @@ int pdem_debug_sweeps(pdem_handle h, long* out4);
 int pdem_find_pairs_static(const double* d_xyz, const double* d_radius, int n, double margin, double box_cap,
                            int* d_pairs, long pair_cap, long* out_count, void* stream);
 
+/* get_domain_min / get_domain_max              src/dem_bindings.cpp:124-127, src/sim.hpp:1105-1110 */
+int pdem_get_domain(pdem_handle h, double* mn, double* mx);
 /* get_positions_view / get_velocities_view / get_external_forces_view / get_inv_mass_view
  *                                               src/dem_bindings.cpp:302-334
  * zero-copy device arrays: field 0 positions, 1 velocities, 2 external forces (writable: the step

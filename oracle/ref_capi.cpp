@@ -242,6 +242,14 @@ int ref_export_lammps(void* h, const char* fn, int step) {
   return guard([&] { S(h)->exportLammps(fn, step); });
 }
 int ref_write_vtp(void* h, const char* fn) { return guard([&] { S(h)->writeVtp(fn); }); }
+int ref_get_domain(void* h, double* mn, double* mx) {
+  return guard([&] {
+    const auto a = S(h)->getDomainMin();
+    const auto b = S(h)->getDomainMax();
+    mn[0] = std::get<0>(a), mn[1] = std::get<1>(a), mn[2] = std::get<2>(a);
+    mx[0] = std::get<0>(b), mx[1] = std::get<1>(b), mx[2] = std::get<2>(b);
+  });
+}
 long ref_get_sdf_grid(void* h, int rx, int ry, int rz, double* out, long cap) {
   long n = -1;
   const int st = guard([&] { n = copyOut(S(h)->getSdfGrid(rx, ry, rz), out, cap); });

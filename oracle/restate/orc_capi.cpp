@@ -391,6 +391,12 @@ double orc_max_overlap(void* h) {
   with(h, [&](auto& S) { v = S.maxOverlap; });
   return v;
 }
+int orc_get_domain(void* h, double* mn, double* mx) {
+  return with(h, [&](auto& S) {
+    mn[0] = S.dmin.x, mn[1] = S.dmin.y, mn[2] = S.dmin.z;
+    mx[0] = S.dmax.x, mx[1] = S.dmax.y, mx[2] = S.dmax.z;
+  });
+}
 long orc_get_sdf_grid(void* h, int rx, int ry, int rz, double* out, long cap) {
   long n = -1;
   const int st = with(h, [&](auto& S) {

@@ -458,6 +458,12 @@ int pdem_write_vtp(pdem_handle h, const char* fn) {
   });
 }
 
+int pdem_get_domain(pdem_handle h, double* mn, double* mx) {
+  BODY({
+    for (int a = 0; a < 3; ++a)
+      mn[a] = (double)S.dmin_[a], mx[a] = (double)S.dmax_[a];
+  });
+}
 int pdem_device_view(pdem_handle h, int field, void** ptr, long* rows, int* row_stride, int* elem_bytes) {
   BODY({
     S.deviceView(field, ptr, rows, row_stride);

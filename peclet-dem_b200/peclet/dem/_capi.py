@@ -120,6 +120,7 @@ _SIGS = {
     "scene_counters": (C.c_long, [_vp, _dbl_p, C.c_long]),
     "scene_block": (C.c_int, [_vp, _int_p, _dbl_p, C.c_int]),
     "device_view": (C.c_int, [_vp, C.c_int, C.POINTER(_vp), _long_p, _int_p, _int_p]),
+    "get_domain": (C.c_int, [_vp, _dbl_p, _dbl_p]),
     # candidate pairs over caller-owned device arrays, with no allocation (pdem_static.cu)
     "find_pairs_static": (C.c_int, [_vp, _vp, C.c_int, C.c_double, C.c_double, _vp, C.c_long, _long_p, _vp]),
     # forward, adjoint and tangent-linear runs of the Hertz sphere substep (pdem_adjoint.cu)
@@ -281,6 +282,19 @@ class CApiSimulation:
         px, py, pz = vals.get("px", True), vals.get("py", True), vals.get("pz", False)
         self._call("set_domain", float(vals["lx"]), float(vals["ly"]), float(vals["lz"]),
                    int(bool(px)), int(bool(py)), int(bool(pz)))
+
+    def _domain(self):
+        mn, mx = np.zeros(3), np.zeros(3)
+        self._call("get_domain", _ptr(mn), _ptr(mx))
+        return mn, mx
+
+    def get_domain_min(self):
+        """The domain minimum corner (x, y, z) (src/dem_bindings.cpp:124-125)."""
+        return tuple(float(self._out_dtype(v)) for v in self._domain()[0])
+
+    def get_domain_max(self):
+        """The domain maximum corner (x, y, z) (src/dem_bindings.cpp:126-127)."""
+        return tuple(float(self._out_dtype(v)) for v in self._domain()[1])
 
     def enable_periodicity(self, x, y, z):
         self._call("enable_periodicity", int(bool(x)), int(bool(y)), int(bool(z)))

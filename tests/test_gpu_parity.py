@@ -88,3 +88,12 @@ def test_device_views(gpu_api):
             a.step(sc.dt)
             b.step(sc.dt)
         assert not P.diff(P.snapshot(a), P.snapshot(b)), prec
+
+
+def test_domain_getters(gpu_api, orc_api):
+    import scenes as S
+    for setup in (lambda s: s.set_domain(0.02, 0.03, 0.04), lambda s: s.set_domain((-1e-3, 0, 2e-3), (5e-3, 6e-3, 7e-3))):
+        for prec in ("fp32", "fp64"):
+            a = P.build(gpu_api, S.dense_spheres(), setup, prec)
+            b = P.build(orc_api, S.dense_spheres(), setup, prec)
+            assert (a.get_domain_min(), a.get_domain_max()) == (b.get_domain_min(), b.get_domain_max())

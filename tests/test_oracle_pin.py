@@ -38,3 +38,13 @@ def test_hertz_restatement_bitexact_vs_reference(ref_api, orc_api):
         sb.update(hk=kb, hx=xb)
         bad = P.diff(sa, sb)
         assert not bad, f"hertz call {k}: {bad[:4]}"
+
+
+def test_domain_getters_match_reference(ref_api, orc_api):
+    """get_domain_min / get_domain_max (src/sim.hpp:1105-1110), both set_domain overloads."""
+    for setup in (lambda s: s.set_domain(0.02, 0.03, 0.04), lambda s: s.set_domain((-1e-3, 0, 2e-3), (5e-3, 6e-3, 7e-3))):
+        got = []
+        for api in (ref_api, orc_api):
+            sim = P.build(api, S.dense_spheres(), setup, "fp32")
+            got.append((sim.get_domain_min(), sim.get_domain_max()))
+        assert got[0] == got[1]
