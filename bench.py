@@ -487,7 +487,9 @@ def run_ours(args):
     scene = make_scene(args.particles)
     n = scene.n
     sim = scene.apply(dem.Simulation(n + 8, "fp64"))
-    for _ in range(args.warmup):
+    # the configuration runs 200 steps from rest; the timed steps sit in its middle (after
+    # `--presettle` untimed steps), where the first spheres reach the floor
+    for _ in range(args.presettle + args.warmup):
         for _ in range(SUBSTEPS):
             sim.step(scene.dt)
 
@@ -520,6 +522,7 @@ def run_ours(args):
     counts = sim.debug_counts()
     sweeps = sim.debug_sweeps() if hasattr(sim, "debug_sweeps") else None
     reuse = sim.debug_reuse()
+    last = sim.counters()
     sim.profile_enable(False)
     # max over ranks of the device time; value = all ranks' particle-substeps / that time
     t_max = max_over_ranks(dev_ms / 1e3, dist, "cuda")
@@ -592,11 +595,12 @@ def run_ours(args):
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-            "config": dict(workload_desc(n), parallelism="replicas" if world > 1 else "single"),
+            "config": dict(workload_desc(n), parallelism="replicas" if world > 1 else "single",
+                           timed_steps_from=args.presettle + args.warmup),
             "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu,
             "clocks": clocks.summary(), "wall_ms_per_step": 1e3 * wall / args.steps,
             "stages_ms_per_step": {k: round(v[0], 4) for k, v in per_step.items()},
-            "counts_last_substep": counts, "sweeps": sweeps, "topology_kept": reuse, "batched": batched,
+            "counts_last_substep": counts, "sweeps": sweeps, "topology_kept": reuse, "last_substep": last, "batched": batched,
             "fwd_adjoint": calib, "configs": configs,
             "device_allocations_timed": int(timed_allocs),
         }
@@ -619,6 +623,8 @@ def main():
     ap.add_argument("--calib-scenes", type=int, default=64, help="scenes of the calibration line (0: skip it)")
     ap.add_argument("--calib-substeps", type=int, default=2000)
     ap.add_argument("--no-configs", action="store_true", help="skip the settling / Hertz / shell lines")
+    ap.add_argument("--presettle", type=int, default=95,
+                    help="untimed steps of the 200-step run before the warm-up and timed steps")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)

@@ -122,13 +122,15 @@ int pdem_step(pdem_handle h, double dt);
 int pdem_step_n(pdem_handle h, double dt, int n);
 /* the last substep's counters: candidate pairs P, contacts C, manifolds M, colours of the two
  * colourings K, velocity / stabilization / position sweeps I_v / I_s / I_p, the error bits of
- * bounded device loops (0 = none) and the maximum overlap */
+ * bounded device loops (0 = none), the maximum overlap, and the Jones-Plassmann rounds of the two
+ * colourings */
 typedef struct {
   long pairs, contacts, manifolds;
   int colors_velocity, colors_position;
   int velocity_sweeps, stabilization_sweeps, position_sweeps;
   int status;
   double max_overlap;
+  int color_rounds_velocity, color_rounds_position;
 } pdem_counters_t;
 int pdem_counters(pdem_handle h, pdem_counters_t* out);
 /* step_hertz(dt, substeps, skin_frac)           src/dem_bindings.cpp:139, src/sim.hpp:1167-1170,628-750 */

@@ -391,13 +391,15 @@ int pdem_counters(pdem_handle h, pdem_counters_t* out) {
   }
   return with(h, [&](auto& S) {
     long sz[3];
-    int in[6];
+    int in[8];
     double mo = 0;
     S.lastCounters(sz, in, &mo);
     out->pairs = sz[0], out->contacts = sz[1], out->manifolds = sz[2];
     out->colors_velocity = in[0], out->colors_position = in[1];
     out->velocity_sweeps = in[2], out->stabilization_sweeps = in[3], out->position_sweeps = in[4];
     out->status = in[5];
+    out->color_rounds_velocity = in[6];
+    out->color_rounds_position = in[7];
     out->max_overlap = mo;
   });
 }

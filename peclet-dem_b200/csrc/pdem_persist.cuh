@@ -201,8 +201,15 @@ struct ColorJob {
   int* col;            // [ne] colours out
   long long *winA, *winB;
   u64* mask;           // [nb]
-  int* aux;            // [0..2] remaining counts by round % 3, [3] max colour, [4] left uncoloured
+  int* aux;            // [0..2] remaining counts by round % 3, [3] max colour, [4] left uncoloured,
+                       // [5] rounds run
+  int *listA, *listB;  // [ne] each: every block's still-uncoloured entries, in its own chunk
+  int* blockCount;     // [gridDim] the blocks' list lengths, published for the tail
+  int *tailA, *tailB;  // [kColorTail] each: the tail's worklists (block 0 alone)
 };
+// once at most this many entries (both colourings together) are left, block 0 alone runs the
+// remaining rounds with block barriers, and the other blocks wait at one grid barrier
+constexpr int kColorTail = 4096;
 
 template <class R, bool MANIFOLD>
 __device__ __forceinline__ void colorInit(const Dev<R>& d, const ColorJob& J, long gtid, long gstride) {
@@ -226,14 +233,32 @@ __device__ __forceinline__ void colorInit(const Dev<R>& d, const ColorJob& J, lo
     J.aux[4] = 0;
   }
 }
+// Worklists. Block b owns the entries [b chunk, (b + 1) chunk). Round 0 walks them all (skipping
+// the coloured ones); every later round walks only the block's losers of the round before, kept
+// in its own segment of listA / listB (ping-pong) and counted in shared memory. A round's outcome
+// does not depend on the order its entries are visited in: the winners at one end are unique,
+// winners never share an end, and losers only reset the next round's slots.
+struct ColorRange {
+  const int* list;  // nullptr: round 0, the whole chunk
+  long first, count;
+};
+__device__ __forceinline__ ColorRange colorRange(const ColorJob& J, int round, int inCount) {
+  const long chunk = (J.ne + gridDim.x - 1) / gridDim.x;
+  const long first = (long)blockIdx.x * chunk;
+  if (round == 0) {
+    const long last = first + chunk < J.ne ? first + chunk : J.ne;
+    return ColorRange{nullptr, first, last > first ? last - first : 0};
+  }
+  return ColorRange{((round & 1) ? J.listB : J.listA) + first, first, inCount};
+}
 template <class R, bool MANIFOLD>
-__device__ __forceinline__ void colorContend(const Dev<R>& d, const ColorJob& J, int round, long gtid,
-                                             long gstride) {
+__device__ __forceinline__ void colorContend(const Dev<R>& d, const ColorJob& J, int round, const ColorRange& rg) {
   long long* win = (round & 1) ? J.winB : J.winA;
-  if (gtid == 0)
+  if ((blockIdx.x | threadIdx.x) == 0)
     J.aux[(round + 1) % 3] = 0;
-  for (long i = gtid; i < J.ne; i += gstride) {
-    if (J.col[i] != -1)
+  for (long t = threadIdx.x; t < rg.count; t += blockDim.x) {
+    const long i = rg.list ? rg.list[t] : rg.first + t;
+    if (!rg.list && J.col[i] != -1)
       continue;
     int ea, eb;
     colorEnds<R, MANIFOLD>(d, (int)i, ea, eb);
@@ -243,28 +268,30 @@ __device__ __forceinline__ void colorContend(const Dev<R>& d, const ColorJob& J,
       atomicMax(&win[eb], k);
   }
 }
+// losers go to the block's next list (shared-memory counter *outCount); the grid's loser count
+// for the round's stop test is added once per block by the caller
 template <class R, bool MANIFOLD>
-__device__ __forceinline__ void colorCommit(const Dev<R>& d, const ColorJob& J, int round, long gtid,
-                                            long gstride) {
+__device__ __forceinline__ void colorCommitTo(const Dev<R>& d, const ColorJob& J, int round, const ColorRange& rg,
+                                              int* out, int* outCount) {
   long long* win = (round & 1) ? J.winB : J.winA;
   long long* nxt = (round & 1) ? J.winA : J.winB;
-  int lost = 0;
-  for (long i = gtid; i < J.ne; i += gstride) {
-    if (J.col[i] != -1)
+  for (long t = threadIdx.x; t < rg.count; t += blockDim.x) {
+    const long i = rg.list ? rg.list[t] : rg.first + t;
+    if (!rg.list && J.col[i] != -1)
       continue;
     int ea, eb;
     colorEnds<R, MANIFOLD>(d, (int)i, ea, eb);
     const long long k = entryKey<R, MANIFOLD>(d, (int)i, ea);
-    if (win[ea] != k || (eb >= 0 && win[eb] != k)) {
-      ++lost;
+    if (__ldcg(&win[ea]) != k || (eb >= 0 && __ldcg(&win[eb]) != k)) {
+      out[atomicAdd(outCount, 1)] = (int)i;
       nxt[ea] = -1;
       if (eb >= 0)
         nxt[eb] = -1;
       continue;
     }
-    u64 forb = J.mask[ea];
+    u64 forb = __ldcg(&J.mask[ea]);
     if (eb >= 0)
-      forb |= J.mask[eb];
+      forb |= __ldcg(&J.mask[eb]);
     int cc = 0;
     while (cc < 62 && (forb & (1ull << cc)))
       ++cc;
@@ -273,11 +300,11 @@ __device__ __forceinline__ void colorCommit(const Dev<R>& d, const ColorJob& J, 
     if (eb >= 0)
       J.mask[eb] |= 1ull << cc;
   }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1)
-    lost += __shfl_xor_sync(0xffffffffu, lost, o);
-  if ((threadIdx.x & 31) == 0 && lost)
-    atomicAdd(&J.aux[round % 3], lost);
+}
+template <class R, bool MANIFOLD>
+__device__ __forceinline__ void colorCommit(const Dev<R>& d, const ColorJob& J, int round, const ColorRange& rg,
+                                            int* outCount) {
+  colorCommitTo<R, MANIFOLD>(d, J, round, rg, (((round + 1) & 1) ? J.listB : J.listA) + rg.first, outCount);
 }
 __device__ __forceinline__ void colorStats(const ColorJob& J, long gtid, long gstride) {
   int mxc = INT_MIN, left = 0;
@@ -300,12 +327,100 @@ __device__ __forceinline__ void colorStats(const ColorJob& J, long gtid, long gs
   }
 }
 
+// The tail, in block 0 alone: gather every block's remaining entries into one list, then run the
+// remaining rounds as the grid does (same contend / commit / stop rule), with block barriers.
+// Global writes of one round are seen by the next through the barrier (and the L2 reads of win and
+// mask in colorCommit).
+template <class R, bool MANIFOLD>
+__device__ __forceinline__ int colorTailGather(const ColorJob& J, int round, int* dst) {
+  // thread b copies block b's list to its offset (an exclusive scan of the list lengths; the
+  // grid has at most blockDim blocks)
+  __shared__ int sWarp[kColorBlock / 32];
+  __shared__ int sTotal;
+  const long chunk = (J.ne + gridDim.x - 1) / gridDim.x;
+  const int* src = (round & 1) ? J.listB : J.listA;  // the lists this round reads
+  const int b = threadIdx.x, lane = b & 31, w = b >> 5;
+  const int n = b < (int)gridDim.x ? J.blockCount[b] : 0;
+  int incl = n;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int u = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o)
+      incl += u;
+  }
+  if (lane == 31)
+    sWarp[w] = incl;
+  __syncthreads();
+  if (b == 0) {
+    int run = 0;
+    for (int q = 0; q < (int)(blockDim.x >> 5); ++q) {
+      const int c = sWarp[q];
+      sWarp[q] = run;
+      run += c;
+    }
+    sTotal = run;
+  }
+  __syncthreads();
+  const int off = sWarp[w] + incl - n;
+  for (int t = 0; t < n; ++t)
+    dst[off + t] = src[(long)b * chunk + t];
+  __threadfence_block();
+  __syncthreads();
+  return sTotal;
+}
+template <class R>
+__device__ void colorTail(const Dev<R>& d, const ColorJob& jm, const ColorJob& jc, int round, int maxRounds,
+                          bool doneM, bool doneC, int prevM, int prevC) {
+  __shared__ int sOut[2];
+  int nM = doneM ? 0 : colorTailGather<R, true>(jm, round, jm.tailA);
+  int nC = doneC ? 0 : colorTailGather<R, false>(jc, round, jc.tailA);
+  for (int k = 0; round < maxRounds && !(doneM && doneC); ++round, ++k) {
+    const int* inM = (k & 1) ? jm.tailB : jm.tailA;
+    const int* inC = (k & 1) ? jc.tailB : jc.tailA;
+    int* outM = (k & 1) ? jm.tailA : jm.tailB;
+    int* outC = (k & 1) ? jc.tailA : jc.tailB;
+    if (threadIdx.x == 0)
+      sOut[0] = sOut[1] = 0;
+    const ColorRange rm{inM, 0, nM}, rc{inC, 0, nC};
+    if (!doneM)
+      colorContend<R, true>(d, jm, round, rm);
+    if (!doneC)
+      colorContend<R, false>(d, jc, round, rc);
+    __threadfence();
+    __syncthreads();
+    if (!doneM)
+      colorCommitTo<R, true>(d, jm, round, rm, outM, &sOut[0]);
+    if (!doneC)
+      colorCommitTo<R, false>(d, jc, round, rc, outC, &sOut[1]);
+    __threadfence();
+    __syncthreads();
+    const int remM = sOut[0], remC = sOut[1];
+    if (threadIdx.x == 0) {
+      if (!doneM)
+        jm.aux[round % 3] = remM;
+      if (!doneC)
+        jc.aux[round % 3] = remC;
+    }
+    if (!doneM) {
+      doneM = remM == 0 || remM == prevM;
+      prevM = remM;
+      nM = remM;
+    }
+    if (!doneC) {
+      doneC = remC == 0 || remC == prevC;
+      prevC = remC;
+      nC = remC;
+    }
+    __syncthreads();
+  }
+}
+
 // job 0: manifolds over real bodies (skipped when ne = 0), job 1: contacts over body slots
 // reuse: a graph equal to the previous substep's keeps its colours and statistics (differ[0]: the
 // contact list changed, differ[1]: the manifold list changed; reuse = 0 forces both colourings)
 template <class R>
 __global__ void __launch_bounds__(kColorBlock) kColorBoth(Dev<R> d, ColorJob jm, ColorJob jc, int maxRounds,
                                                           GridBar gb, const int* differ, int reuse) {
+  __shared__ int sCount[2][2];  // per job: this block's loser counts, ping-pong by round
   const long gtid = (long)blockIdx.x * blockDim.x + threadIdx.x, gstride = (long)gridDim.x * blockDim.x;
   if (reuse && !differ[1])
     jm.ne = 0;  // uniform over the grid: the flags are written before the launch
@@ -315,21 +430,35 @@ __global__ void __launch_bounds__(kColorBlock) kColorBoth(Dev<R> d, ColorJob jm,
     return;
   colorInit<R, true>(d, jm, gtid, gstride);
   colorInit<R, false>(d, jc, gtid, gstride);
+  if (threadIdx.x < 4)
+    sCount[threadIdx.x >> 1][threadIdx.x & 1] = 0;
   if (!gridBarrier(gb))
     return;
   int prevM = -1, prevC = -1;
   bool doneM = jm.ne <= 0, doneC = jc.ne <= 0;
-  for (int round = 0; round < maxRounds && !(doneM && doneC); ++round) {
+  int round = 0;
+  bool tail = false;
+  for (; round < maxRounds && !(doneM && doneC); ++round) {
+    const int in = round & 1, outS = in ^ 1;  // shared counter slots: this round's list, the next
+    const ColorRange rm = colorRange(jm, round, sCount[0][in]), rc = colorRange(jc, round, sCount[1][in]);
     if (!doneM)
-      colorContend<R, true>(d, jm, round, gtid, gstride);
+      colorContend<R, true>(d, jm, round, rm);
     if (!doneC)
-      colorContend<R, false>(d, jc, round, gtid, gstride);
+      colorContend<R, false>(d, jc, round, rc);
     if (!gridBarrier(gb))
       return;
     if (!doneM)
-      colorCommit<R, true>(d, jm, round, gtid, gstride);
+      colorCommit<R, true>(d, jm, round, rm, &sCount[0][outS]);
     if (!doneC)
-      colorCommit<R, false>(d, jc, round, gtid, gstride);
+      colorCommit<R, false>(d, jc, round, rc, &sCount[1][outS]);
+    __syncthreads();
+    if (threadIdx.x == 0) {  // this block's losers into the grid's count; its consumed slot reset
+      if (!doneM && sCount[0][outS])
+        atomicAdd(&jm.aux[round % 3], sCount[0][outS]);
+      if (!doneC && sCount[1][outS])
+        atomicAdd(&jc.aux[round % 3], sCount[1][outS]);
+      sCount[0][in] = sCount[1][in] = 0;
+    }
     if (!gridBarrier(gb))
       return;
     if (!doneM) {
@@ -342,6 +471,31 @@ __global__ void __launch_bounds__(kColorBlock) kColorBoth(Dev<R> d, ColorJob jm,
       doneC = rem == 0 || rem == prevC;
       prevC = rem;
     }
+    // few entries left: publish this block's lists, and block 0 takes over (uniform decision)
+    if (!(doneM && doneC) && round + 1 < maxRounds &&
+        (doneM ? 0 : prevM) + (doneC ? 0 : prevC) <= kColorTail) {
+      if (threadIdx.x == 0) {
+        jm.blockCount[blockIdx.x] = doneM ? 0 : sCount[0][(round + 1) & 1];
+        jc.blockCount[blockIdx.x] = doneC ? 0 : sCount[1][(round + 1) & 1];
+      }
+      tail = true;
+      ++round;
+      break;
+    }
+  }
+  if (tail) {
+    if (!gridBarrier(gb))  // the published lists are complete
+      return;
+    if (blockIdx.x == 0)
+      colorTail(d, jm, jc, round, maxRounds, doneM, doneC, prevM, prevC);
+    if (!gridBarrier(gb))  // the tail's colours are visible to every block
+      return;
+  }
+  if (gtid == 0) {
+    if (jm.ne > 0)
+      jm.aux[5] = round;
+    if (jc.ne > 0)
+      jc.aux[5] = round;
   }
   colorStats(jm, gtid, gstride);
   colorStats(jc, gtid, gstride);

@@ -1172,15 +1172,24 @@ void Sim<R>::colorBoth(int nm, int nc, int& ncolV, int& velLeft, int& ncolP, int
   winner2_.ensure(std::max(nbM, 1), false, stream_);
   winnerP_.ensure(std::max(nbC, 1), false, stream_);
   winnerP2_.ensure(std::max(nbC, 1), false, stream_);
-  colorAux_.ensure(10, false, stream_);
-  const ColorJob jm{neM, nbM, mColor_.p, winner_.p, winner2_.p, mask_.p, colorAux_.p};
-  const ColorJob jc{neC, nbC, cColor_.p, winnerP_.p, winnerP2_.p, maskP_.p, colorAux_.p + 5};
+  colorAux_.ensure(12, false, stream_);
+  colorListM_.ensure(2 * std::max(neM, 1), false, stream_);
+  colorListC_.ensure(2 * std::max(neC, 1), false, stream_);
+  // per job: the blocks' list lengths (up to 4 blocks per SM), then the tail's two lists
+  const int maxGrid = 4 * numSMs_;
+  colorTail_.ensure(2 * (maxGrid + 2 * kColorTail), false, stream_);
+  int* tm = colorTail_.p;
+  int* tc = colorTail_.p + maxGrid + 2 * kColorTail;
+  const ColorJob jm{neM, nbM, mColor_.p, winner_.p, winner2_.p, mask_.p, colorAux_.p, colorListM_.p,
+                    colorListM_.p + std::max(neM, 1), tm, tm + maxGrid, tm + maxGrid + kColorTail};
+  const ColorJob jc{neC, nbC, cColor_.p, winnerP_.p, winnerP2_.p, maskP_.p, colorAux_.p + 6, colorListC_.p,
+                    colorListC_.p + std::max(neC, 1), tc, tc + maxGrid, tc + maxGrid + kColorTail};
   gbar_.ensure(2, false, stream_);
   const GridBar gb{gbar_.p, &ctr_.p->err, barrierSleepNs_};
   launchCoopB(kColorBoth<R>, kColorBlock, d_, jm, jc, std::max(nbM, nbC) + 2, gb, (const int*)topoFlags_.p,
               topoValid_ ? 1 : 0);
   KCHECK("colour loop");
-  int res[10], err = 0, differ[2] = {1, 1};
+  int res[12], err = 0, differ[2] = {1, 1};
   cudaCheck(cudaMemcpyAsync(res, colorAux_.p, sizeof res, cudaMemcpyDeviceToHost, stream_), "D2H");
   cudaCheck(cudaMemcpyAsync(&err, &ctr_.p->err, sizeof err, cudaMemcpyDeviceToHost, stream_), "D2H");
   cudaCheck(cudaMemcpyAsync(differ, topoFlags_.p, sizeof differ, cudaMemcpyDeviceToHost, stream_), "D2H");
@@ -1194,10 +1203,12 @@ void Sim<R>::colorBoth(int nm, int nc, int& ncolV, int& velLeft, int& ncolP, int
   if (neM > 0) {
     ncolV = res[3] + 1;
     velLeft = res[4];
+    colorRounds_[0] = res[5];
   }
   if (neC > 0) {
-    ncolP = res[8] + 1;
-    posLeft = res[9];
+    ncolP = res[9] + 1;
+    posLeft = res[10];
+    colorRounds_[1] = res[11];
   }
 }
 // stable colour-sorted execution order: colour c occupies [off[c], off[c+1])
@@ -1658,7 +1669,7 @@ R Sim<R>::maxOverlap() {
 // =============================================================================================
 // the last substep's sizes, colour counts, sweeps, overlap and error bits
 template <class R>
-void Sim<R>::lastCounters(long* sizes, int* ints, double* maxOverlap) {
+void Sim<R>::lastCounters(long* sizes, int* ints, double* maxOverlap) {  // ints: 8 values
   const Counters<R> c = readCounters();
   sizes[0] = c.pairCount;
   sizes[1] = c.contactCount;
@@ -1669,6 +1680,8 @@ void Sim<R>::lastCounters(long* sizes, int* ints, double* maxOverlap) {
   ints[3] = c.stabSweeps;
   ints[4] = c.posSweeps;
   ints[5] = c.err;
+  ints[6] = colorRounds_[0];
+  ints[7] = colorRounds_[1];
   *maxOverlap = (double)c.maxOverlap;
 }
 template <class R>

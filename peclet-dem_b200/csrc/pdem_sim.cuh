@@ -208,6 +208,8 @@ class Sim {
   DBuf<uint8_t> persistent_, sideFlags_;
   DBuf<int> heights_, ordChanged_, ordKeysIn_, ordKeys_, ordPermIn_, ordPerm_;  // "ordered" pass
   DBuf<R> sdfA_, sdfB_;  // get_sdf_grid ping-pong
+  DBuf<int> colorListM_, colorListC_;  // colouring worklists (two halves each)
+  DBuf<int> colorTail_;                // block list lengths and the tail's worklists
   DBuf<int> sdfState_;
   DBuf<R> lambda_, prevLambda_, vn0_, posImp_, prevPosImp_;
   DBuf<Q4<R>> lambdaT_, prevLambdaT_, vt0_;
@@ -367,6 +369,7 @@ class Sim {
   void lastCounters(long* sizes, int* ints, double* maxOverlap);
  private:
   int ncolVLast_ = 0, ncolPLast_ = 0;  // colours of the last substep's two colourings
+  int colorRounds_[2] = {0, 0};         // Jones-Plassmann rounds of the last manifold / contact colouring
   // back-off (ns) between polls of a waiting block at a grid barrier; PDEM_BARRIER_SLEEP_NS
   // overrides it
   unsigned barrierSleepNs_ = [] {

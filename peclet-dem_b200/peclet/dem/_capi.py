@@ -139,7 +139,7 @@ class Counters(C.Structure):
     _fields_ = [("pairs", C.c_long), ("contacts", C.c_long), ("manifolds", C.c_long),
                 ("colors_velocity", C.c_int), ("colors_position", C.c_int), ("velocity_sweeps", C.c_int),
                 ("stabilization_sweeps", C.c_int), ("position_sweeps", C.c_int), ("status", C.c_int),
-                ("max_overlap", C.c_double)]
+                ("max_overlap", C.c_double), ("color_rounds_velocity", C.c_int), ("color_rounds_position", C.c_int)]
 
 
 class HzModel(C.Structure):
