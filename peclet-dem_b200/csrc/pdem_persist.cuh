@@ -472,7 +472,7 @@ __global__ void __launch_bounds__(kColorBlock) kColorBoth(Dev<R> d, ColorJob jm,
       prevC = rem;
     }
     // few entries left: publish this block's lists, and block 0 takes over (uniform decision)
-    if (!(doneM && doneC) && round + 1 < maxRounds &&
+    if (!(doneM && doneC) && round + 1 < maxRounds && gridDim.x <= blockDim.x &&
         (doneM ? 0 : prevM) + (doneC ? 0 : prevC) <= kColorTail) {
       if (threadIdx.x == 0) {
         jm.blockCount[blockIdx.x] = doneM ? 0 : sCount[0][(round + 1) & 1];

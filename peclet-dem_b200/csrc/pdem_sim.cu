@@ -1186,7 +1186,7 @@ void Sim<R>::colorBoth(int nm, int nc, int& ncolV, int& velLeft, int& ncolP, int
                     colorListC_.p + std::max(neC, 1), tc, tc + maxGrid, tc + maxGrid + kColorTail};
   gbar_.ensure(2, false, stream_);
   const GridBar gb{gbar_.p, &ctr_.p->err, barrierSleepNs_};
-  launchCoopB(kColorBoth<R>, kColorBlock, d_, jm, jc, std::max(nbM, nbC) + 2, gb, (const int*)topoFlags_.p,
+  launchCoopB(kColorBoth<R>, colorBlock_, d_, jm, jc, std::max(nbM, nbC) + 2, gb, (const int*)topoFlags_.p,
               topoValid_ ? 1 : 0);
   KCHECK("colour loop");
   int res[12], err = 0, differ[2] = {1, 1};

@@ -370,6 +370,12 @@ class Sim {
  private:
   int ncolVLast_ = 0, ncolPLast_ = 0;  // colours of the last substep's two colourings
   int colorRounds_[2] = {0, 0};         // Jones-Plassmann rounds of the last manifold / contact colouring
+  // block size of the colouring launch (PDEM_COLOR_BLOCK overrides: 256, 512 or 1024)
+  int colorBlock_ = [] {
+    const char* e = std::getenv("PDEM_COLOR_BLOCK");
+    const int b = e ? (int)std::strtol(e, nullptr, 10) : 1024;
+    return (b == 256 || b == 512) ? b : 1024;
+  }();
   // back-off (ns) between polls of a waiting block at a grid barrier; PDEM_BARRIER_SLEEP_NS
   // overrides it
   unsigned barrierSleepNs_ = [] {
