@@ -102,19 +102,32 @@ __global__ void kBoxes(Dev<R> d, int n, R margin, R boxCap, BvhNodes<R> bn, BvhB
         hi[a] = o > hi[a] ? o : hi[a];
       }
   }
-  // scene bounds: warp reduction, one atomic per warp and axis
+  // scene bounds: warp then block reduction, one atomic per block and bound (every warp has
+  // boxes, and same-address atomics from all of them would serialise at L2)
+  __shared__ u64 sLo[3][32], sHi[3][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
   for (int a = 0; a < 3; ++a) {
     for (int o = 16; o > 0; o >>= 1) {
       const u64 l = __shfl_xor_sync(0xffffffffu, lo[a], o), h = __shfl_xor_sync(0xffffffffu, hi[a], o);
       lo[a] = l < lo[a] ? l : lo[a];
       hi[a] = h > hi[a] ? h : hi[a];
     }
-    if ((threadIdx.x & 31) == 0) {
-      if (lo[a] != ~0ull)
-        atomicMin(&bb.bounds[a], lo[a]);
-      if (hi[a] != 0ull)
-        atomicMax(&bb.bounds[3 + a], hi[a]);
+    if (lane == 0)
+      sLo[a][w] = lo[a], sHi[a][w] = hi[a];
+  }
+  __syncthreads();
+  if (threadIdx.x < 6) {
+    const int a = threadIdx.x % 3;
+    const bool isLo = threadIdx.x < 3;
+    u64 v = isLo ? ~0ull : 0ull;
+    for (int k = 0; k < nw; ++k) {
+      const u64 x = isLo ? sLo[a][k] : sHi[a][k];
+      v = isLo ? (x < v ? x : v) : (x > v ? x : v);
     }
+    if (isLo && v != ~0ull)
+      atomicMin(&bb.bounds[a], v);
+    if (!isLo && v != 0ull)
+      atomicMax(&bb.bounds[3 + a], v);
   }
 }
 
@@ -631,7 +644,7 @@ __global__ void kVerletDisplacement(Dev<R> d, int n, const Q4<R>* ref, const int
       v = R(1e30);
     runMax(m, v);
   }
-  warpMaxAtomic(out, m);
+  blockMaxAtomic(out, m);
 }
 template <class R>
 __global__ void kFilterPairs(const int2* cand, int nc, const Box<R>* prim, int* keep) {

@@ -178,6 +178,28 @@ __device__ __forceinline__ void warpMaxAtomic(R* p, R v) {
   if ((threadIdx.x & 31) == 0)
     atomicMaxNonNeg(p, v);
 }
+// the same, reduced over the block first: one atomic per block instead of one per warp, for maxima
+// that every warp contributes to (thousands of same-address atomics serialise at L2). Every thread
+// of the block must call it.
+template <class R>
+__device__ __forceinline__ void blockMaxAtomic(R* p, R v) {
+  __shared__ R sMax[32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const R w = __shfl_xor_sync(0xffffffffu, v, o);
+    v = w > v ? w : v;
+  }
+  __syncthreads();  // a previous call's reads of sMax are done
+  if ((threadIdx.x & 31) == 0)
+    sMax[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    R m = sMax[0];
+    for (int k = 1; k < (int)((blockDim.x + 31) >> 5); ++k)
+      m = sMax[k] > m ? sMax[k] : m;
+    atomicMaxNonNeg(p, m);
+  }
+}
 // running max that ignores NaN (the reference's atomic max never stores NaN)
 template <class R>
 __device__ __forceinline__ void runMax(R& acc, R v) {

@@ -245,7 +245,7 @@ template <class R>
 __global__ void kMaxScale(Dev<R> d, int n, R* out) {
   R m = R(0);
   GRID_STRIDE(i, n) runMax(m, d.scale[i]);
-  warpMaxAtomic(out, m);
+  blockMaxAtomic(out, m);
 }
 
 // batched form: largest scale of every scene (out[s] zeroed by the host)
