@@ -199,6 +199,9 @@ long pdem_scene_counters(pdem_handle h, double* out, long cap);
  * hertz_rebuild, hertz_integrate */
 int pdem_profile_enable(pdem_handle h, int on);
 int pdem_profile_read(pdem_handle h, double* ms, long* calls, int cap, long* launches);
+/* host wall-clock milliseconds spent issuing each stage since profile_enable (same order): a stage
+ * whose host time matches its device time is paced by the host (launches, read-backs) */
+int pdem_profile_read_host(pdem_handle h, double* ms, int cap);
 /* device-timeline interval: timer_start records an event on the simulation's stream, timer_stop
  * records another, waits for it and returns the milliseconds between them (everything the stream
  * ran, and any idle time, in between) */

@@ -590,6 +590,16 @@ int pdem_debug_sweeps(pdem_handle h, long* out4) {
   BODY(for (int i = 0; i < 4; ++i) out4[i] = S.sweeps_[i]);
 }
 int pdem_profile_enable(pdem_handle h, int on) { BODY(S.profileEnable(on != 0)); }
+int pdem_profile_read_host(pdem_handle h, double* ms, int cap) {
+  int n = -1;
+  with(h, [&](auto& S) {
+    using T = std::remove_reference_t<decltype(S)>;
+    n = T::ST_COUNT;
+    for (int i = 0; i < n && i < cap; ++i)
+      ms[i] = S.stageHostMs_[i];
+  });
+  return n;
+}
 int pdem_profile_read(pdem_handle h, double* ms, long* calls, int cap, long* launches) {
   int n = -1;
   with(h, [&](auto& S) {

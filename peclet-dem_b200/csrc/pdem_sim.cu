@@ -40,6 +40,11 @@ Sim<R>::Sim(int capacity) {
     cudaCheck(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev), "cooperative launch attribute");
     if (!coop)
       throw CudaError("device does not support cooperative launches");
+    // the growable buffers come from the default pool: keep what they free for their regrowth
+    cudaMemPool_t pool;
+    cudaCheck(cudaDeviceGetDefaultMemPool(&pool, dev), "default memory pool");
+    uint64_t keep = UINT64_MAX;
+    cudaCheck(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep), "pool release threshold");
   }
   for (int i = 0; i < 8; ++i) {
     hzE_[i] = R(1.0e9);
@@ -210,15 +215,22 @@ Counters<R> Sim<R>::readCounters() {
   return c;
 }
 
-// blocks of a cooperative launch of `kernel`: resident blocks per SM (at most 4) x SMs
+// blocks of a cooperative launch of `kernel`: resident blocks per SM (at most 4) x SMs, the
+// occupancy query cached by (kernel, block). A grid sized down to a small scene's work was not
+// faster: a colour step there is bound by the latency of one PGS update, not by the barrier.
 template <class R>
 template <class K>
 int Sim<R>::coopGrid(K kernel, int block) {
-  int per = 0;
-  cudaCheck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, block, 0), "occupancy");
-  if (per < 1)
-    throw CudaError("persistent loop kernel cannot be resident");
-  return std::min(per, 4) * numSMs_;
+  const auto key = std::make_pair(reinterpret_cast<const void*>(kernel), block);
+  auto it = coopPer_.find(key);
+  if (it == coopPer_.end()) {
+    int per = 0;
+    cudaCheck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, block, 0), "occupancy");
+    if (per < 1)
+      throw CudaError("persistent loop kernel cannot be resident");
+    it = coopPer_.emplace(key, per).first;
+  }
+  return std::min(it->second, 4) * numSMs_;
 }
 template <class R>
 template <class K, class... A>
@@ -2187,6 +2199,7 @@ void Sim<R>::profileEnable(bool on) {
   prof_ = on;
   for (int i = 0; i < ST_COUNT; ++i) {
     stageMs_[i] = 0;
+    stageHostMs_[i] = 0;
     stageCalls_[i] = 0;
   }
   launches_ = 0;
@@ -2205,7 +2218,8 @@ void Sim<R>::mark(int stage) {
     evFree_.pop_back();
   }
   cudaCheck(cudaEventRecord(e, stream_), "cudaEventRecord");
-  marks_.push_back({stage, e});
+  const double now = std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+  marks_.push_back({stage, e, now});
 }
 template <class R>
 void Sim<R>::timerStart() {
@@ -2234,6 +2248,7 @@ void Sim<R>::flushMarks() {
     float ms = 0;
     cudaCheck(cudaEventElapsedTime(&ms, marks_[k].ev, marks_[k + 1].ev), "cudaEventElapsedTime");
     stageMs_[marks_[k].stage] += ms;
+    stageHostMs_[marks_[k].stage] += 1e3 * (marks_[k + 1].host - marks_[k].host);
     stageCalls_[marks_[k].stage] += 1;
   }
   for (auto& m : marks_)

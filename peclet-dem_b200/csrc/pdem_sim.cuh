@@ -2,9 +2,12 @@
 // orchestration (src/sim.hpp:97-488, 494-541, 628-750), owning all device memory.
 #pragma once
 #include <cstdlib>
+#include <chrono>
 #include <cmath>
 #include <cstdint>
 #include <limits>
+#include <map>
+#include <utility>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -23,11 +26,13 @@ struct CudaError : std::runtime_error {
 };
 void cudaCheck(cudaError_t e, const char* what);
 
-// device allocations made by growable buffers since load (instrumentation: a step that reallocates
-// stalls on cudaMalloc / cudaFree)
+// device allocations made by growable buffers since load (instrumentation)
 extern long gDeviceAllocs;
 
-// growable device buffer (contents not preserved unless asked)
+// growable device buffer (contents not preserved unless asked), allocated in stream order from the
+// device's default pool: growth neither waits for the device nor returns memory to the driver (the
+// pool keeps freed blocks; its release threshold is raised when a simulation is created), so a
+// scene whose contact count climbs while it settles reallocates without stalling its stream
 template <class T>
 struct DBuf {
   T* p = nullptr;
@@ -37,7 +42,7 @@ struct DBuf {
   DBuf& operator=(const DBuf&) = delete;
   ~DBuf() {
     if (p)
-      cudaFree(p);
+      cudaFree(p);  // the owner synchronised its stream; cudaFree accepts pool allocations
   }
   void ensure(size_t want, bool preserve = false, cudaStream_t s = 0) {
     if (want <= n && p)
@@ -47,14 +52,12 @@ struct DBuf {
       cap = n + n / 2;  // grow geometrically: counts that creep up each substep reallocate rarely
     T* q = nullptr;
     ++gDeviceAllocs;
-    cudaCheck(cudaMalloc(&q, cap * sizeof(T)), "cudaMalloc");
+    cudaCheck(cudaMallocAsync(reinterpret_cast<void**>(&q), cap * sizeof(T), s), "cudaMallocAsync");
     cudaCheck(cudaMemsetAsync(q, 0, cap * sizeof(T), s), "cudaMemset");
     if (preserve && p && n)
       cudaCheck(cudaMemcpyAsync(q, p, n * sizeof(T), cudaMemcpyDeviceToDevice, s), "cudaMemcpy");
-    if (p) {
-      cudaCheck(cudaStreamSynchronize(s), "sync");
-      cudaFree(p);
-    }
+    if (p)
+      cudaCheck(cudaFreeAsync(p, s), "cudaFreeAsync");  // after every use queued on s so far
     p = q;
     n = cap;
   }
@@ -178,6 +181,7 @@ class Sim {
   long reuse_[3] = {0, 0, 0};      // substeps that kept: manifold grouping, contact colours, manifold colours
   bool prof_ = false;
   double stageMs_[ST_COUNT] = {};
+  double stageHostMs_[ST_COUNT] = {};  // host wall time spent issuing each stage (launches, read-backs)
   long stageCalls_[ST_COUNT] = {};
   void profileEnable(bool on);
   // device-timeline interval between two calls (events on the library's stream; stop synchronises)
@@ -303,6 +307,7 @@ class Sim {
   struct Mark {
     int stage;
     cudaEvent_t ev;
+    double host;  // host steady-clock seconds when the stage's first launch was being issued
   };
   std::vector<Mark> marks_;
   std::vector<cudaEvent_t> evFree_;
@@ -336,6 +341,7 @@ class Sim {
   void launchCoopB(K kernel, int block, A... args);
   template <class K, class... A>
   void launchCoop(K kernel, A... args);
+  std::map<std::pair<const void*, int>, int> coopPer_;  // resident blocks per SM, by (kernel, block)
   template <class T>
   void sortPairs(const T* kin, T* kout, const int* vin, int* vout, int n, int endBit);
   void orderedStabilization(int nm, V3<R> gHat, const SolveP<R>& ss, R vRestS);

@@ -108,6 +108,7 @@ _SIGS = {
     # instrumentation
     "profile_enable": (C.c_int, [_vp, C.c_int]),
     "profile_read": (C.c_int, [_vp, _dbl_p, _long_p, C.c_int, _long_p]),
+    "profile_read_host": (C.c_int, [_vp, _dbl_p, C.c_int]),
     "debug_sweeps": (C.c_int, [_vp, _long_p]),
     "debug_allocs": (C.c_long, []),
     "timer_start": (C.c_int, [_vp]),
@@ -679,6 +680,12 @@ class CApiSimulation:
         n = self._f["profile_read"](self._h, _ptr(ms), calls.ctypes.data_as(_long_p), 32, C.byref(launches))
         stages = {STAGES[i]: (float(ms[i]), int(calls[i])) for i in range(min(n, len(STAGES)))}
         return stages, int(launches.value)
+
+    def profile_read_host(self):
+        """dict stage -> host wall-clock milliseconds spent issuing it since profile_enable."""
+        ms = np.zeros(32, dtype=np.float64)
+        n = self._f["profile_read_host"](self._h, _ptr(ms), 32)
+        return {STAGES[i]: float(ms[i]) for i in range(min(n, len(STAGES)))}
 
     def debug_sweeps(self):
         """Sweeps executed since profile_enable (velocity, stabilization, position) and substeps."""
