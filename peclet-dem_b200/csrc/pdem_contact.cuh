@@ -6,9 +6,13 @@
 // with the warp's points in shell order, the per-warp ballot prefix giving each contact its slot,
 // so contacts come out in (pair, k) / (particle, plane, k) / (particle, wall, k) order.
 #pragma once
+#include <cooperative_groups.h>
+#include <cooperative_groups/reduce.h>
+
 #include "pdem_common.cuh"
 
 namespace pdem {
+namespace cg = cooperative_groups;
 
 template <class R>
 struct NarrowP {
@@ -37,10 +41,17 @@ __device__ __forceinline__ R marginOf(const Dev<R>& d, const NarrowP<R>& P, int 
 }
 template <class R>
 __device__ __forceinline__ void overlapMax(const Dev<R>& d, int i, R v, R& mo) {
-  if (d.scn)
-    atomicMaxNonNeg(&d.scn[d.sceneOf[i]].maxOverlap, v);
-  else
+  if (d.scn) {
+    // the lanes here that share a scene (a scene's bodies are contiguous, so usually the whole
+    // warp) reduce first: one atomic per scene per warp, not one per overlapping body
+    const int sc = d.sceneOf[i];
+    const auto peers = cg::labeled_partition(cg::coalesced_threads(), sc);
+    const R m = cg::reduce(peers, v, cg::greater<R>());
+    if (peers.thread_rank() == 0)
+      atomicMaxNonNeg(&d.scn[sc].maxOverlap, m);
+  } else {
     runMax(mo, v);
+  }
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -334,13 +345,17 @@ __global__ void kBoundary(Dev<R> d, int numReal, NarrowP<R> P, int* cntP, int* c
     warpMaxAtomic(&d.ctr->maxOverlap, mo);
 }
 
-// single-point shapes (spheres): one thread per particle, same slots as kBoundary
+// single-point shapes (spheres): one thread per particle, same slots as kBoundary. The write pass
+// (MODE 1) writes the plane contacts only, visiting the particles that have some; the wall contacts
+// are written by kBoundaryWallSphere, one thread per contact.
 template <class R, int MODE>
 __global__ void kBoundarySphere(Dev<R> d, int numReal, NarrowP<R> P, int* cntP, int* cntW, const int* offP,
-                                const int* offW, int basePlanes, int baseWalls) {
+                                int basePlanes) {
   const ShapeDesc<R> sd = d.shapes[0];
   R mo = R(0);
   GRID_STRIDE(i, numReal) {
+    if (MODE == 1 && offP[i + 1] == offP[i])
+      continue;
     const R s = d.scale[i] * P.globalScale;
     int run = MODE ? basePlanes + offP[i] : 0, tot = 0;
     for (int pl = 0; pl < P.numPlanes; ++pl) {
@@ -354,27 +369,56 @@ __global__ void kBoundarySphere(Dev<R> d, int numReal, NarrowP<R> P, int* cntP, 
         ++tot;
       }
     }
-    if (MODE == 0)
-      cntP[i] = tot;
-    run = MODE ? baseWalls + offW[i] : 0;
+    if (MODE == 1)
+      continue;
+    cntP[i] = tot;
     tot = 0;
     for (int q = wallBegin(d, (int)i); q < wallEnd(d, P, (int)i); ++q) {
       const int wi = wallAt(d, q);
-      const BoundaryProbe<R> b = probeWall(d, (int)i, wi, 0, sd, s, marginOf(d, P, (int)i), MODE == 1);
-      if (MODE == 0 && b.dist < R(0))
+      const BoundaryProbe<R> b = probeWall(d, (int)i, wi, 0, sd, s, marginOf(d, P, (int)i), false);
+      if (b.dist < R(0))
         overlapMax(d, (int)i, -b.dist, mo);
-      if (b.hit) {
-        if (MODE == 1 && run < d.maxContacts)
-          writeBoundaryContact(d, run, (int)i, b, true, wi, P.haveMat);
-        ++run;
+      if (b.hit)
         ++tot;
-      }
     }
-    if (MODE == 0)
-      cntW[i] = tot;
+    cntW[i] = tot;
   }
   if (MODE == 0)
     warpMaxAtomic(&d.ctr->maxOverlap, mo);
+}
+// wall contacts of spheres, one thread per contact: contact t belongs to the particle i with
+// offW[i] <= t < offW[i + 1] (offW: exclusive scan of the count pass's wall hits, numReal + 1
+// entries) and is its (t - offW[i])-th hitting wall in wall order, the count pass's hit test
+// repeated; the slot is baseWalls + t, as in the per-particle order. Only the contacts pay for the
+// wall normal (six more grid samples), and no lane idles beside them.
+template <class R>
+__global__ void kBoundaryWallSphere(Dev<R> d, int total, int numReal, NarrowP<R> P, const int* offW, int baseWalls) {
+  const ShapeDesc<R> sd = d.shapes[0];
+  GRID_STRIDE(t, total) {
+    int lo = 0, hi = numReal;  // largest i with offW[i] <= t
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (offW[mid] <= (int)t)
+        lo = mid;
+      else
+        hi = mid - 1;
+    }
+    const int i = lo;
+    int k = (int)t - offW[i];
+    const R s = d.scale[i] * P.globalScale;
+    const R margin = marginOf(d, P, i);
+    for (int q = wallBegin(d, i); q < wallEnd(d, P, i); ++q) {
+      const int wi = wallAt(d, q);
+      if (!probeWall(d, i, wi, 0, sd, s, margin, false).hit)
+        continue;
+      if (k-- > 0)
+        continue;
+      const int slot = baseWalls + (int)t;
+      if (slot < d.maxContacts)
+        writeBoundaryContact(d, slot, i, probeWall(d, i, wi, 0, sd, s, margin, true), true, wi, P.haveMat);
+      break;
+    }
+  }
 }
 
 // =============================================================================================

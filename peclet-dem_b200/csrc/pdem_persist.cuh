@@ -140,22 +140,24 @@ __global__ void __launch_bounds__(kBlock) kSweepLoop(Dev<R> d, const int* order,
 // contiguous in the (scene, colour)-sorted order (off[s * 64 + c] .. off[s * 64 + c + 1]); its
 // blocks-worth of threads sweeps them in colour order with block barriers, and the block ends its
 // own loop at the scene's adaptive stop. No grid-wide barrier and no cooperative launch: scenes are
-// independent. The host has run the first sweep's BEGIN for every scene (kCtlScenes).
+// independent. Block b runs scene sceneOrder[b] (largest scenes first, so none is left to the last
+// wave). The host has run the first sweep's BEGIN for every scene (kCtlScenes).
 constexpr int kSceneBlock = 128;      // default block of the per-scene sweep loops
 constexpr int kSceneBlockMax = 512;   // largest block the launch shape autotuner tries
 
 template <class R, int KIND, int LOOP>
-__global__ void __launch_bounds__(kSceneBlockMax) kSweepScenes(Dev<R> d, const int* order, const int* off, int iters,
-                                                            SolveP<R> P, R thr) {
-  const int s = blockIdx.x;
+__global__ void __launch_bounds__(kSceneBlockMax) kSweepScenes(Dev<R> d, const int* sceneOrder, const int* order,
+                                                            const int* off, int iters, SolveP<R> P, R thr) {
+  const int s = sceneOrder[blockIdx.x];
   SceneCtl<R>& q = d.scn[s];
   volatile int* done = LOOP == 1 ? &q.velDone : LOOP == 2 ? &q.stabDone : &q.posDone;
   volatile R* mxp = KIND == 2 ? &q.maxOverlap : &q.maxApproach;
   if (*done)
     return;
   const int* so = off + (long)s * 64;
+  __shared__ R sMax[kSceneBlockMax / 32];
   for (int it = 0; it < iters; ++it) {
-    R mx = R(0);  // unused: batched entries take their scene's max atomically (loopMax)
+    R mx = R(0);  // this thread's running max of the sweep; the block reduces it at the END
     for (int col = 0; col < 63; ++col) {
       const int b = so[col], n = so[col + 1] - b;
       if (n == 0)
@@ -164,17 +166,29 @@ __global__ void __launch_bounds__(kSceneBlockMax) kSweepScenes(Dev<R> d, const i
       if (!serial || threadIdx.x == 0)
         for (int t = serial ? 0 : threadIdx.x; t < n; t += serial ? 1 : blockDim.x) {
           if (KIND == 0)
-            pgsOne(d, order[b + t], P, mx, LOOP);
+            pgsOne<R, true>(d, order[b + t], P, mx, LOOP);
           else if (KIND == 1)
-            gsOne(d, order[b + t], P, mx);
+            gsOne<R, true>(d, order[b + t], P, mx);
           else
-            posGSOne(d, order[b + t], mx);
+            posGSOne<R, true>(d, order[b + t], mx);
         }
       __syncthreads();
     }
+    // the sweep's max over the block (the scene): no atomics on the scene's one max word
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const R w = __shfl_xor_sync(0xffffffffu, mx, o);
+      mx = w > mx ? w : mx;
+    }
+    if ((threadIdx.x & 31) == 0)
+      sMax[threadIdx.x >> 5] = mx;
+    __syncthreads();
     // END of this sweep, then BEGIN of the next one (kCtlScenes' rule for this scene)
     if (threadIdx.x == 0) {
-      const R m = *mxp;
+      R m = sMax[0];
+      for (int k = 1; k < (int)(blockDim.x >> 5); ++k)
+        m = sMax[k] > m ? sMax[k] : m;
+      *mxp = m;  // BEGIN left it 0 and only this block writes it during the loop
       if (KIND == 2 ? (m < thr) : (m <= thr)) {
         *done = 1;
       } else if (it + 1 < iters) {

@@ -1056,7 +1056,7 @@ void Sim<R>::detectAll(R margin) {
     if (shell)
       ++launches_, kBoundary<R, 0><<<gridFor((long)nr * 32), kBlock, 0, stream_>>>(d_, nr, P, iC_.p, iD_.p, nullptr, nullptr, 0, 0);
     else
-      ++launches_, kBoundarySphere<R, 0><<<gridFor(nr), kBlock, 0, stream_>>>(d_, nr, P, iC_.p, iD_.p, nullptr, nullptr, 0, 0);
+      ++launches_, kBoundarySphere<R, 0><<<gridFor(nr), kBlock, 0, stream_>>>(d_, nr, P, iC_.p, iD_.p, nullptr, 0);
     KCHECK("boundary count");
   }
   exclusiveSum(iA_.p, iB_.p, np + 1);
@@ -1086,9 +1086,13 @@ void Sim<R>::detectAll(R margin) {
     if (shell)
       ++launches_, kBoundary<R, 1><<<gridFor((long)nr * 32), kBlock, 0, stream_>>>(d_, nr, P, nullptr, nullptr, offP, cntW,
                                                                                  tot[0], tot[0] + tot[1]);
-    else
-      ++launches_, kBoundarySphere<R, 1><<<gridFor(nr), kBlock, 0, stream_>>>(d_, nr, P, nullptr, nullptr, offP, cntW,
-                                                                              tot[0], tot[0] + tot[1]);
+    else {
+      if (tot[1] > 0)
+        ++launches_, kBoundarySphere<R, 1><<<gridFor(nr), kBlock, 0, stream_>>>(d_, nr, P, nullptr, nullptr, offP, tot[0]);
+      if (tot[2] > 0)
+        ++launches_, kBoundaryWallSphere<R><<<gridFor(tot[2]), kBlock, 0, stream_>>>(d_, tot[2], nr, P, cntW,
+                                                                                    tot[0] + tot[1]);
+    }
     KCHECK("boundary write");
   }
   const long total = (long)tot[0] + tot[1] + tot[2];
@@ -1406,9 +1410,9 @@ void Sim<R>::demStep() {
     if (batch_)
       tuneBegin();
     if (batch_ && usePGS)
-      ++launches_, kSweepScenes<R, 0, 1><<<numScenes_, sceneBlock(), 0, s>>>(d_, mOrder_.p, mOff_.p, velIters_, sp, thr);
+      ++launches_, kSweepScenes<R, 0, 1><<<numScenes_, sceneBlock(), 0, s>>>(d_, sceneLpt_.p, mOrder_.p, mOff_.p, velIters_, sp, thr);
     else if (batch_)
-      ++launches_, kSweepScenes<R, 1, 1><<<numScenes_, sceneBlock(), 0, s>>>(d_, mOrder_.p, mOff_.p, velIters_, sp, thr);
+      ++launches_, kSweepScenes<R, 1, 1><<<numScenes_, sceneBlock(), 0, s>>>(d_, sceneLpt_.p, mOrder_.p, mOff_.p, velIters_, sp, thr);
     else if (usePGS)
       launchCoop(kSweepLoop<R, 0, 1>, d_, (const int*)mOrder_.p, (const int*)mOff_.p, ncolV, velIters_, sp, thr, gb);
     else
@@ -1483,7 +1487,7 @@ void Sim<R>::demStep() {
         const GridBar gb{gbar_.p, &ctr_.p->err, barrierSleepNs_};
         ctl(CTL_STAB_BEGIN, R(0), 0);
         if (batch_)
-          ++launches_, kSweepScenes<R, 0, 2><<<numScenes_, sceneBlock(), 0, s>>>(d_, mOrder_.p, mOff_.p, iters, ss, vRestS);
+          ++launches_, kSweepScenes<R, 0, 2><<<numScenes_, sceneBlock(), 0, s>>>(d_, sceneLpt_.p, mOrder_.p, mOff_.p, iters, ss, vRestS);
         else
           launchCoop(kSweepLoop<R, 0, 2>, d_, (const int*)mOrder_.p, (const int*)mOff_.p, ncolV, iters, ss, vRestS, gb);
       }
@@ -1560,7 +1564,7 @@ void Sim<R>::demStep() {
     const GridBar gb{gbar_.p, &ctr_.p->err, barrierSleepNs_};
     ctl(CTL_POS_BEGIN, R(0), 0);
     if (batch_) {
-      ++launches_, kSweepScenes<R, 2, 3><<<numScenes_, sceneBlock(), 0, s>>>(d_, cOrder_.p, cOff_.p, posIters_, sp, posTol);
+      ++launches_, kSweepScenes<R, 2, 3><<<numScenes_, sceneBlock(), 0, s>>>(d_, sceneLpt_.p, cOrder_.p, cOff_.p, posIters_, sp, posTol);
       tuneEnd();
     }
     else
@@ -2402,6 +2406,15 @@ void Sim<R>::setScenes(int S, const int* first) {
   cudaCheck(cudaMemcpyAsync(sceneOf_.p, of.data(), numReal_ * sizeof(int), cudaMemcpyHostToDevice, stream_), "H2D");
   sceneFirstD_.ensure(S + 1, false, stream_);
   cudaCheck(cudaMemcpyAsync(sceneFirstD_.p, first, (S + 1) * sizeof(int), cudaMemcpyHostToDevice, stream_), "H2D");
+  // the per-scene sweep loops dispatch scenes largest first (longest-processing-time order): a
+  // large scene left to the last wave of blocks would set the kernel's tail
+  std::vector<int> lpt(S);
+  for (int k = 0; k < S; ++k)
+    lpt[k] = k;
+  std::stable_sort(lpt.begin(), lpt.end(),
+                   [&](int a, int b) { return first[a + 1] - first[a] > first[b + 1] - first[b]; });
+  sceneLpt_.ensure(std::max(S, 1), false, stream_);
+  cudaCheck(cudaMemcpyAsync(sceneLpt_.p, lpt.data(), S * sizeof(int), cudaMemcpyHostToDevice, stream_), "H2D");
   scn_.ensure(S, false, stream_);
   scn_.zero(stream_, S);
   sceneParams_.ensure(3 * (size_t)S, false, stream_);

@@ -257,6 +257,7 @@ class Sim {
   DBuf<Q4<double>> posD_, quatD_;  // FP32-mixed form: master positions and orientations
   DBuf<double> rowStage_;           // host rows staged on the device (set/get of 4-wide fields)
   DBuf<R> sceneParams_, sceneMaxScale_;
+  DBuf<int> sceneLpt_;  // scenes by decreasing body count: dispatch order of the per-scene loops
   int lastTot_[3] = {0, 0, 0};
   Counters<R> detectCounters_{};  // host copy of the counters after the narrowphase (H2D source)
   void batchBegin();

@@ -352,15 +352,16 @@ __device__ __forceinline__ bool sceneDone(const Dev<R>& d, int s, int loop) {
   const SceneCtl<R>& S = d.scn[s];
   return loop == 1 ? S.velDone != 0 : loop == 2 ? S.stabDone != 0 : S.posDone != 0;
 }
-template <class R>
+// LOCAL: the caller is one block per scene (kSweepScenes) and reduces the running max itself
+template <class R, bool LOCAL = false>
 __device__ __forceinline__ void loopMax(const Dev<R>& d, int s, bool position, R v, R& mx) {
-  if (d.scn)
+  if (d.scn && !LOCAL)
     atomicMaxNonNeg(position ? &d.scn[s].maxOverlap : &d.scn[s].maxApproach, v);
   else
     runMax(mx, v);
 }
 
-template <class R>
+template <class R, bool LOCAL = false>
 __device__ __forceinline__ void pgsOne(const Dev<R>& d, int idx, const SolveP<R>& P, R& mx, int loop) {
   int sc = 0;
   R eG = P.eN, muG = P.mu;
@@ -428,7 +429,7 @@ __device__ __forceinline__ void pgsOne(const Dev<R>& d, int idx, const SolveP<R>
   V3<R> vA2 = vA, wA2 = wA, vB2 = vB, wB2 = wB;
   if (dA != R(0)) {
     d.lambda[idx] = pNew;
-    loopMax(d, sc, false, fabs(dA) * wT / lenN, mx);
+    loopMax<R, LOCAL>(d, sc, false, fabs(dA) * wT / lenN, mx);
     const R lam = -sgn * dA;
     const V3<R> J = mul(v.N, lam), JA = mul(v.TA, lam), JB = mul(v.TB, lam);
     if (applyA) {
@@ -486,7 +487,7 @@ __device__ __forceinline__ void pgsOne(const Dev<R>& d, int idx, const SolveP<R>
       d.lambdaT[idx] = q4(ltNew);
       const R dl = sqrt(dot(dd, dd));
       if (wTt > R(1e-9))
-        loopMax(d, sc, false, dl * wTt, mx);
+        loopMax<R, LOCAL>(d, sc, false, dl * wTt, mx);
       if (applyA) {
         vA2 = add(vA2, mul(dd, v.imA));
         wA2 = add(wA2, angResponse(v.qA, cross(v.rAa, dd), v.iIA));
@@ -601,7 +602,7 @@ __global__ void kPGSBucket(Dev<R> d, const int* perm, int b, int n, int color, S
 }
 
 // one-shot coloured GS of one colour, g = 0 path (src/solver_velocity.hpp:989-1137)
-template <class R>
+template <class R, bool LOCAL = false>
 __device__ __forceinline__ void gsOne(const Dev<R>& d, int idx, const SolveP<R>& P, R& mx) {
   int sc = 0;
   R eG = P.eN;
@@ -647,7 +648,7 @@ __device__ __forceinline__ void gsOne(const Dev<R>& d, int idx, const SolveP<R>&
   const R wT = wAn + wBn;
   if (wT <= R(0))
     return;
-  loopMax(d, sc, false, fabs(vn) / lenN, mx);
+  loopMax<R, LOCAL>(d, sc, false, fabs(vn) / lenN, mx);
   if (fabs(vn) < P.vRest * lenN)
     e = R(0);
   const R lam = (-e * vn - vn) / wT;
@@ -989,7 +990,7 @@ __device__ __forceinline__ bool posConstraint(const Dev<R>& d, int idx, V3<R>& n
   wT = computeW(rA, n, imA, iA) + computeW(rB, n, imB, iB);
   return true;
 }
-template <class R>
+template <class R, bool LOCAL = false>
 __device__ __forceinline__ void posGSOne(const Dev<R>& d, int idx, R& mx) {
   int sc = 0;
   if (d.scn) {
@@ -1014,7 +1015,7 @@ __device__ __forceinline__ void posGSOne(const Dev<R>& d, int idx, R& mx) {
     const V3<R> pB = v3(d.posPred[B]);
     d.posPred[B] = q4(add(pB, V3<R>{-nv.x * dl * imB, -nv.y * dl * imB, -nv.z * dl * imB}));
   }
-  loopMax(d, sc, true, -C, mx);
+  loopMax<R, LOCAL>(d, sc, true, -C, mx);
 }
 template <class R>
 __global__ void kPosGSColor(Dev<R> d, const int* order, const int* coff, int color, int gate) {
