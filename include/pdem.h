@@ -210,6 +210,9 @@ int pdem_timer_stop(pdem_handle h, double* ms);
 /* substeps since profile_enable that kept the previous substep's manifold grouping, contact
  * colours and manifold colours (their lists were unchanged) */
 int pdem_debug_reuse(pdem_handle h, long* out3);
+/* substeps since profile_enable whose contact grouping took the rank scatter (the list in key
+ * order up to its boundary contacts), and those of them whose list the scatter rejected (sorted) */
+int pdem_debug_ranked(pdem_handle h, long* out2);
 /* device allocations made by this library's growable buffers since it was loaded */
 long pdem_debug_allocs(void);
 /* sweeps executed since profile_enable: velocity, stabilization, position; and substeps */

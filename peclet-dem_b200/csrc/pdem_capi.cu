@@ -583,6 +583,7 @@ long pdem_scene_counters(pdem_handle h, double* out, long cap) {
 
 // ---- instrumentation ----
 int pdem_timer_start(pdem_handle h) { BODY(S.timerStart()); }
+int pdem_debug_ranked(pdem_handle h, long* out2) { BODY(out2[0] = S.rankStats_[0]; out2[1] = S.rankStats_[1]); }
 int pdem_debug_reuse(pdem_handle h, long* out3) { BODY(for (int i = 0; i < 3; ++i) out3[i] = S.reuse_[i]); }
 int pdem_timer_stop(pdem_handle h, double* ms) { BODY(*ms = S.timerStop()); }
 long pdem_debug_allocs(void) { return pdem::gDeviceAllocs; }

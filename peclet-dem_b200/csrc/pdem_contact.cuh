@@ -444,6 +444,69 @@ __global__ void kContactKeys(Dev<R> d, int nc, int bits, u64* keys, int* vals) {
     vals[i] = (int)i;
   }
 }
+// The stable key sort of the contact list, done as a rank scatter. The narrowphase writes
+// [body-pair contacts in pair order] ++ [plane contacts by particle] ++ [wall contacts by particle];
+// the broadphase gives pairs (lo, hi), lo < hi, lo real, sorted by (lo, hi), so the pair contacts
+// are already in key order. A boundary key (i, none) sorts after every pair key (i, v) and before
+// (i + 1, ...), and the plane contacts of a particle precede its wall contacts (list order). Ranks:
+// pair contact p with first body a -> p + the boundary contacts of particles below a (offP[a] +
+// offW[a]); the k-th plane contact of particle i -> the pair contacts with first body <= i, +
+// offP[i] + offW[i] + k; its k-th wall contact -> the same base + offP[i + 1] - offP[i] + k. A list
+// that breaks these premises (pair contacts out of key order, a non-real first body, counts that do
+// not match the offsets) sets *bad and the caller sorts instead; every write stays inside [0, nc).
+template <class R>
+__global__ void kContactRanks(Dev<R> d, int nc, int nPair, int nPlane, int numReal, const int* offP,
+                              const int* offW, int bits, u64* keysOut, int* permOut, int* bad) {
+  const u64 none = (1ull << bits) - 1ull;
+  auto pairKey = [&](int2 ab) {
+    const unsigned u = ab.x < ab.y ? ab.x : ab.y, v = ab.x < ab.y ? ab.y : ab.x;
+    return ((u64)u << bits) | v;
+  };
+  GRID_STRIDE(t, nc) {
+    const int2 ab = d.cab[t];
+    long rank = -1;
+    u64 k = 0;
+    if (t < nPair) {
+      const int a = ab.x < ab.y ? ab.x : ab.y;
+      if (ab.y < 0 || a < 0 || a >= numReal || (t > 0 && pairKey(d.cab[t - 1]) > pairKey(ab))) {
+        atomicOr(bad, 1);
+        continue;
+      }
+      k = pairKey(ab);
+      rank = t + offP[a] + offW[a];
+    } else {
+      const int i = ab.x;
+      if (ab.y >= 0 || i < 0 || i >= numReal) {
+        atomicOr(bad, 1);
+        continue;
+      }
+      k = ((u64)(unsigned)i << bits) | none;
+      int lo = 0, hi = nPair;  // pair contacts with first body <= i
+      while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        const int2 m = d.cab[mid];
+        if ((m.x < m.y ? m.x : m.y) <= i)
+          lo = mid + 1;
+        else
+          hi = mid;
+      }
+      const bool plane = t < nPair + nPlane;
+      const long kk = plane ? t - nPair - offP[i] : t - nPair - nPlane - offW[i];
+      const long cnt = plane ? offP[i + 1] - offP[i] : offW[i + 1] - offW[i];
+      if (kk < 0 || kk >= cnt) {
+        atomicOr(bad, 1);
+        continue;
+      }
+      rank = (long)lo + (plane ? offP[i] : offP[i + 1]) + offW[i] + kk;
+    }
+    if (rank < 0 || rank >= nc) {
+      atomicOr(bad, 1);
+      continue;
+    }
+    keysOut[rank] = k;
+    permOut[rank] = (int)t;
+  }
+}
 __global__ void kSegHeads(int n, const u64* keys, int* head) {
   GRID_STRIDE(p, n) head[p] = (p == 0 || keys[p] != keys[p - 1]) ? 1 : 0;
 }

@@ -1154,15 +1154,42 @@ int Sim<R>::reduceManifolds(int nc) {
   head_.ensure(nc, false, stream_);
   headScan_.ensure(nc, false, stream_);
   segStart_.ensure(nc + 1, false, stream_);
-  ++launches_, kContactKeys<R><<<gridFor(nc), kBlock, 0, stream_>>>(d_, nc, kb, ckeys_.p, cpermIn_.p);
-  KCHECK("contact keys");
-  sortPairs(ckeys_.p, ckeysS_.p, cpermIn_.p, cperm_.p, nc, 2 * kb);
-  ++launches_, kSegHeads<<<gridFor(nc), kBlock, 0, stream_>>>(nc, ckeysS_.p, head_.p);
-  KCHECK("seg heads");
-  inclusiveSum(head_.p, headScan_.p, nc);
-  int nm = 0;
-  cudaCheck(cudaMemcpyAsync(&nm, headScan_.p + nc - 1, sizeof(int), cudaMemcpyDeviceToHost, stream_), "D2H");
-  sync();
+  // the narrowphase's list is in key order up to its boundary contacts: the stable sort is a rank
+  // scatter (kContactRanks), checked on the device; a list it rejects is sorted after all
+  static const bool forceSort = std::getenv("PDEM_CONTACT_SORT") != nullptr;
+  const bool ranked = !forceSort && numReal_ > 0 && (long)lastTot_[0] + lastTot_[1] + lastTot_[2] == nc;
+  int hostBad[2] = {0, 0};  // [0] manifold count, [1] the rank scatter's rejection
+  auto groups = [&](bool sortNow) {
+    if (sortNow) {
+      ++launches_, kContactKeys<R><<<gridFor(nc), kBlock, 0, stream_>>>(d_, nc, kb, ckeys_.p, cpermIn_.p);
+      KCHECK("contact keys");
+      sortPairs(ckeys_.p, ckeysS_.p, cpermIn_.p, cperm_.p, nc, 2 * kb);
+    } else {
+      const int nr = numReal_;
+      rankBad_.ensure(1, false, stream_);
+      rankBad_.zero(stream_, 1);
+      ++launches_, kContactRanks<R><<<gridFor(nc), kBlock, 0, stream_>>>(d_, nc, lastTot_[0], lastTot_[1], nr,
+                                                                         iE_.p + (nr + 1), iE_.p, kb, ckeysS_.p,
+                                                                         cperm_.p, rankBad_.p);
+      KCHECK("contact ranks");
+    }
+    ++launches_, kSegHeads<<<gridFor(nc), kBlock, 0, stream_>>>(nc, ckeysS_.p, head_.p);
+    KCHECK("seg heads");
+    inclusiveSum(head_.p, headScan_.p, nc);
+    cudaCheck(cudaMemcpyAsync(&hostBad[0], headScan_.p + nc - 1, sizeof(int), cudaMemcpyDeviceToHost, stream_), "D2H");
+    if (!sortNow)
+      cudaCheck(cudaMemcpyAsync(&hostBad[1], rankBad_.p, sizeof(int), cudaMemcpyDeviceToHost, stream_), "D2H");
+    sync();
+  };
+  groups(!ranked);
+  if (ranked && hostBad[1]) {
+    ++rankStats_[1];
+    hostBad[1] = 0;
+    groups(true);
+  } else if (ranked) {
+    ++rankStats_[0];
+  }
+  const int nm = hostBad[0];
   ++launches_, kSegStarts<<<gridFor(nc), kBlock, 0, stream_>>>(nc, headScan_.p, segStart_.p);
   KCHECK("seg starts");
   ++launches_, kReduceManifolds<<<gridFor(nm), kBlock, 0, stream_>>>(d_, nm, nc, kb, segStart_.p, ckeysS_.p, cperm_.p);
@@ -2200,6 +2227,7 @@ void Sim<R>::ensureGrounded() {
 template <class R>
 void Sim<R>::profileEnable(bool on) {
   reuse_[0] = reuse_[1] = reuse_[2] = 0;
+  rankStats_[0] = rankStats_[1] = 0;
   prof_ = on;
   for (int i = 0; i < ST_COUNT; ++i) {
     stageMs_[i] = 0;

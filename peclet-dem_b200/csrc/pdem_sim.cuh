@@ -258,6 +258,10 @@ class Sim {
   DBuf<double> rowStage_;           // host rows staged on the device (set/get of 4-wide fields)
   DBuf<R> sceneParams_, sceneMaxScale_;
   DBuf<int> sceneLpt_;  // scenes by decreasing body count: dispatch order of the per-scene loops
+  DBuf<int> rankBad_;   // the contact rank scatter's rejection flag
+ public:
+  long rankStats_[2] = {0, 0};  // substeps whose contact grouping was ranked, and ranked then rejected
+ private:
   int lastTot_[3] = {0, 0, 0};
   Counters<R> detectCounters_{};  // host copy of the counters after the narrowphase (H2D source)
   void batchBegin();

@@ -108,6 +108,7 @@ _SIGS = {
     # instrumentation
     "profile_enable": (C.c_int, [_vp, C.c_int]),
     "profile_read": (C.c_int, [_vp, _dbl_p, _long_p, C.c_int, _long_p]),
+    "debug_ranked": (C.c_int, [_vp, _long_p]),
     "profile_read_host": (C.c_int, [_vp, _dbl_p, C.c_int]),
     "debug_sweeps": (C.c_int, [_vp, _long_p]),
     "debug_allocs": (C.c_long, []),
@@ -686,6 +687,13 @@ class CApiSimulation:
         ms = np.zeros(32, dtype=np.float64)
         n = self._f["profile_read_host"](self._h, _ptr(ms), 32)
         return {STAGES[i]: float(ms[i]) for i in range(min(n, len(STAGES)))}
+
+    def debug_ranked(self):
+        """Substeps since profile_enable whose contact grouping was a rank scatter, and those whose
+        list the scatter rejected (then sorted)."""
+        out = np.zeros(2, dtype=np.int64)
+        self._call("debug_ranked", out.ctypes.data_as(_long_p))
+        return {"ranked": int(out[0]), "rejected": int(out[1])}
 
     def debug_sweeps(self):
         """Sweeps executed since profile_enable (velocity, stabilization, position) and substeps."""

@@ -97,3 +97,35 @@ def test_domain_getters(gpu_api, orc_api):
             a = P.build(gpu_api, S.dense_spheres(), setup, prec)
             b = P.build(orc_api, S.dense_spheres(), setup, prec)
             assert (a.get_domain_min(), a.get_domain_max()) == (b.get_domain_min(), b.get_domain_max())
+
+
+def test_contact_grouping_ranked(gpu_api):
+    """The stable key sort of the contact list runs as a rank scatter: the narrowphase's list is in
+    key order up to its boundary contacts, so every substep with contacts takes it and none of the
+    parity scenes' lists is rejected (the tests above check the product against the oracle)."""
+    ranked = 0
+    for name, mk, extra, steps in P.MATRIX:
+        sc = mk()
+        a = P.build(gpu_api, sc, extra, "fp64")
+        a.profile_enable(True)
+        for _ in range(min(steps, 4)):
+            a.step(sc.dt)
+        r = a.debug_ranked()
+        assert r["rejected"] == 0, name
+        ranked += r["ranked"]
+    assert ranked > 0
+
+
+def test_contact_grouping_sorted_path():
+    """PDEM_CONTACT_SORT=1 keeps the key sort (the rank scatter's fallback): scenes with ghosts,
+    planes, SDF walls and point shells stay bit-exact against the oracle that way."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sel = "test_fp32_bitexact_vs_oracle and (periodic_polydisperse or dense_spheres or drum_sdf_wall or hollow_cylinders or settled_column)"
+    r = subprocess.run([sys.executable, "-m", "pytest", "-q", "-m", "gpu", "-k", sel,
+                        os.path.join(root, "tests", "test_gpu_parity.py")],
+                       cwd=root, env={**os.environ, "PDEM_CONTACT_SORT": "1"}, capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    assert " passed" in r.stdout and "5 passed" in r.stdout, r.stdout[-500:]
