@@ -28,20 +28,25 @@ int with(pdem_handle h, F&& fn) {
     g_err = "null simulation handle";
     return PDEM_ERR_INVALID;
   }
+  Handle* H = static_cast<Handle*>(h);
+  // a read-back queued before an exception must not be delivered to a dead frame by a later sync
+  auto drop = [&] { H->f ? H->f->dropPending() : H->d->dropPending(); };
   try {
-    Handle* H = static_cast<Handle*>(h);
     if (H->f)
       fn(*H->f);
     else
       fn(*H->d);
     return PDEM_OK;
   } catch (const std::invalid_argument& e) {
+    drop();
     g_err = e.what();
     return PDEM_ERR_INVALID;
   } catch (const pdem::CudaError& e) {
+    drop();
     g_err = e.what();
     return PDEM_ERR_CUDA;
   } catch (const std::exception& e) {
+    drop();
     g_err = e.what();
     return PDEM_ERR_RUNTIME;
   }

@@ -32,6 +32,7 @@ void cudaCheck(cudaError_t e, const char* what) {
 template <class R>
 Sim<R>::Sim(int capacity) {
   cudaCheck(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+  cudaCheck(cudaHostAlloc(reinterpret_cast<void**>(&pin_), kPinBytes, cudaHostAllocDefault), "pinned read-back block");
   {
     int dev = 0;
     cudaCheck(cudaGetDevice(&dev), "cudaGetDevice");
@@ -61,6 +62,8 @@ Sim<R>::~Sim() {
     cudaStreamSynchronize(stream_);
     cudaStreamDestroy(stream_);
   }
+  if (pin_)
+    cudaFreeHost(pin_);
   if (tStart_) {
     cudaEventDestroy(tStart_);
     cudaEventDestroy(tStop_);
@@ -204,11 +207,25 @@ void Sim<R>::refreshDev() {
 template <class R>
 void Sim<R>::sync() {
   cudaCheck(cudaStreamSynchronize(stream_), "cudaStreamSynchronize");
+  for (const PendingRead& r : pending_)
+    std::memcpy(r.host, pin_ + r.off, r.bytes);
+  dropPending();
+}
+template <class R>
+void Sim<R>::readBack(void* host, const void* dev, size_t bytes) {
+  const size_t off = (pinOff_ + 15) & ~size_t(15);
+  if (!pin_ || off + bytes > kPinBytes) {  // no room: a direct copy, complete when it returns
+    cudaCheck(cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, stream_), "D2H");
+    return;
+  }
+  cudaCheck(cudaMemcpyAsync(pin_ + off, dev, bytes, cudaMemcpyDeviceToHost, stream_), "D2H");
+  pending_.push_back({host, off, bytes});
+  pinOff_ = off + bytes;
 }
 template <class R>
 Counters<R> Sim<R>::readCounters() {
   Counters<R> c;
-  cudaCheck(cudaMemcpyAsync(&c, ctr_.p, sizeof c, cudaMemcpyDeviceToHost, stream_), "D2H counters");
+  readBack(&c, ctr_.p, sizeof c);
   sync();
   if (c.err & kErrBarrier)
     throw CudaError("a grid-wide barrier of a persistent loop timed out (blocks not co-resident)");
@@ -783,7 +800,7 @@ R Sim<R>::maxOwnedRadius() {
     rA_.zero(stream_, 1);
     ++launches_, kMaxScale<<<gridFor(numReal_), kBlock, 0, stream_>>>(d_, numReal_, rA_.p);
     KCHECK("maxScale");
-    cudaCheck(cudaMemcpyAsync(&maxScaleHost_, rA_.p, sizeof(R), cudaMemcpyDeviceToHost, stream_), "D2H");
+    readBack(&maxScaleHost_, rA_.p, sizeof(R));
     sync();
     maxScaleValid_ = true;
   }
@@ -808,7 +825,7 @@ void Sim<R>::resetGhosts(R band) {
     KCHECK("ghostCount");
     exclusiveSum(iA_.p, iB_.p, numReal_ + 1);
     int total = 0;
-    cudaCheck(cudaMemcpyAsync(&total, iB_.p + numReal_, sizeof(int), cudaMemcpyDeviceToHost, stream_), "D2H");
+    readBack(&total, iB_.p + numReal_, sizeof(int));
     sync();
     ++launches_, kGhostWrite<<<gridFor(numReal_), kBlock, 0, stream_>>>(d_, numReal_, dom, band, iB_.p);
     KCHECK("ghostWrite");
@@ -905,9 +922,9 @@ int Sim<R>::findCollisions(R margin, int cap, int2* out, R extra) {
   KCHECK("query");
   exclusiveSum(rowCnt_.p, qoff_.p, numReal_ + 1);
   int total = 0, err = 0, overflow = 0;
-  cudaCheck(cudaMemcpyAsync(&total, qoff_.p + numReal_, sizeof(int), cudaMemcpyDeviceToHost, stream_), "D2H");
-  cudaCheck(cudaMemcpyAsync(&err, &ctr_.p->err, sizeof(int), cudaMemcpyDeviceToHost, stream_), "D2H");
-  cudaCheck(cudaMemcpyAsync(&overflow, bflag_.p, sizeof(int), cudaMemcpyDeviceToHost, stream_), "D2H");
+  readBack(&total, qoff_.p + numReal_, sizeof(int));
+  readBack(&err, &ctr_.p->err, sizeof(int));
+  readBack(&overflow, bflag_.p, sizeof(int));
   sync();
   if (err & 1)
     throw std::runtime_error("broadphase: BVH traversal exceeded its iteration bound (corrupt tree)");
@@ -918,8 +935,8 @@ int Sim<R>::findCollisions(R margin, int cap, int2* out, R extra) {
                                                                           nullptr, nullptr, 0);
     KCHECK("query count");
     exclusiveSum(rowCnt_.p, qoff_.p, numReal_ + 1);
-    cudaCheck(cudaMemcpyAsync(&total, qoff_.p + numReal_, sizeof(int), cudaMemcpyDeviceToHost, stream_), "D2H");
-    cudaCheck(cudaMemcpyAsync(&err, &ctr_.p->err, sizeof(int), cudaMemcpyDeviceToHost, stream_), "D2H");
+    readBack(&total, qoff_.p + numReal_, sizeof(int));
+    readBack(&err, &ctr_.p->err, sizeof(int));
     sync();
     if (err & 1)
       throw std::runtime_error("broadphase: BVH traversal exceeded its iteration bound (corrupt tree)");
@@ -1007,8 +1024,8 @@ int Sim<R>::findCollisionsVerlet(R margin) {
     KCHECK("verlet filter");
     int total = 0;
     R disp = 0;
-    cudaCheck(cudaMemcpyAsync(&total, vOff_.p + nc, sizeof(int), cudaMemcpyDeviceToHost, stream_), "D2H");
-    cudaCheck(cudaMemcpyAsync(&disp, rA_.p, sizeof(R), cudaMemcpyDeviceToHost, stream_), "D2H");
+    readBack(&total, vOff_.p + nc, sizeof(int));
+    readBack(&disp, rA_.p, sizeof(R));
     sync();
     if (useOld && !(disp <= R(0.5) * skin))
       continue;  // some body left its widened box: rebuild and filter again
@@ -1065,10 +1082,10 @@ void Sim<R>::detectAll(R margin) {
   // one read-back: the three totals and the counters the count passes updated (max overlap, errors)
   int tot[3] = {0, 0, 0};
   Counters<R> c;
-  cudaCheck(cudaMemcpyAsync(&tot[0], iB_.p + np, sizeof(int), cudaMemcpyDeviceToHost, stream_), "D2H");
-  cudaCheck(cudaMemcpyAsync(&tot[1], offP + nr, sizeof(int), cudaMemcpyDeviceToHost, stream_), "D2H");
-  cudaCheck(cudaMemcpyAsync(&tot[2], cntW + nr, sizeof(int), cudaMemcpyDeviceToHost, stream_), "D2H");
-  cudaCheck(cudaMemcpyAsync(&c, ctr_.p, sizeof c, cudaMemcpyDeviceToHost, stream_), "D2H counters");
+  readBack(&tot[0], iB_.p + np, sizeof(int));
+  readBack(&tot[1], offP + nr, sizeof(int));
+  readBack(&tot[2], cntW + nr, sizeof(int));
+  readBack(&c, ctr_.p, sizeof c);
   sync();
   if (c.err & kErrBarrier)
     throw CudaError("a grid-wide barrier of a persistent loop timed out (blocks not co-resident)");
@@ -1133,7 +1150,7 @@ int Sim<R>::reduceManifolds(int nc) {
   // after a substep whose list was unchanged, and every 4th substep otherwise.
   if (topoValid_ && nc == prevNcM_ && (lastSame_ || (topoChecks_++ & 3) == 0)) {
     int differ = 1;
-    cudaCheck(cudaMemcpyAsync(&differ, topoFlags_.p, sizeof(int), cudaMemcpyDeviceToHost, stream_), "D2H");
+    readBack(&differ, topoFlags_.p, sizeof(int));
     sync();
     lastSame_ = differ == 0;
     if (lastSame_) {
@@ -1176,9 +1193,9 @@ int Sim<R>::reduceManifolds(int nc) {
     ++launches_, kSegHeads<<<gridFor(nc), kBlock, 0, stream_>>>(nc, ckeysS_.p, head_.p);
     KCHECK("seg heads");
     inclusiveSum(head_.p, headScan_.p, nc);
-    cudaCheck(cudaMemcpyAsync(&hostBad[0], headScan_.p + nc - 1, sizeof(int), cudaMemcpyDeviceToHost, stream_), "D2H");
+    readBack(&hostBad[0], headScan_.p + nc - 1, sizeof(int));
     if (!sortNow)
-      cudaCheck(cudaMemcpyAsync(&hostBad[1], rankBad_.p, sizeof(int), cudaMemcpyDeviceToHost, stream_), "D2H");
+      readBack(&hostBad[1], rankBad_.p, sizeof(int));
     sync();
   };
   groups(!ranked);
@@ -1233,9 +1250,9 @@ void Sim<R>::colorBoth(int nm, int nc, int& ncolV, int& velLeft, int& ncolP, int
               topoValid_ ? 1 : 0);
   KCHECK("colour loop");
   int res[12], err = 0, differ[2] = {1, 1};
-  cudaCheck(cudaMemcpyAsync(res, colorAux_.p, sizeof res, cudaMemcpyDeviceToHost, stream_), "D2H");
-  cudaCheck(cudaMemcpyAsync(&err, &ctr_.p->err, sizeof err, cudaMemcpyDeviceToHost, stream_), "D2H");
-  cudaCheck(cudaMemcpyAsync(differ, topoFlags_.p, sizeof differ, cudaMemcpyDeviceToHost, stream_), "D2H");
+  readBack(res, colorAux_.p, sizeof res);
+  readBack(&err, &ctr_.p->err, sizeof err);
+  readBack(differ, topoFlags_.p, sizeof differ);
   sync();
   keptC_ = topoValid_ && differ[0] == 0;
   keptM_ = topoValid_ && differ[1] == 0;
@@ -1644,7 +1661,7 @@ void Sim<R>::demStep() {
     thermo_.ensure(2, false, s);
     ++launches_, kThermoEnergy<<<1, 1, 0, s>>>(d_, numReal_, thermo_.p);
     double ke[2];
-    cudaCheck(cudaMemcpyAsync(ke, thermo_.p, sizeof ke, cudaMemcpyDeviceToHost, s), "D2H");
+    readBack(ke, thermo_.p, sizeof ke);
     sync();
     const double ndof = 3.0 * numReal_, kB = (double)thKB_, tau = (double)thTau_, Tt = (double)thT_;
     auto lam = [&](double kin) -> R {

@@ -340,6 +340,24 @@ class Sim {
   void ensureGrounded();
   void demStep();
   Counters<R> readCounters();
+  // small read-backs: device -> a pinned block, queued without a host wait (a copy into pageable
+  // memory waits for its own completion, so a group of them cost a round trip each); sync() then
+  // copies each value to its host destination. Destinations must live until that sync().
+  void readBack(void* host, const void* dev, size_t bytes);
+  struct PendingRead {
+    void* host;
+    size_t off, bytes;
+  };
+  std::vector<PendingRead> pending_;
+  char* pin_ = nullptr;
+  size_t pinOff_ = 0;
+  static constexpr size_t kPinBytes = 1 << 16;
+ public:
+  void dropPending() {  // after an exception between a read-back and its sync
+    pending_.clear();
+    pinOff_ = 0;
+  }
+ private:
   template <class K>
   int coopGrid(K kernel, int block);
   template <class K, class... A>
