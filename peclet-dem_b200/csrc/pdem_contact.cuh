@@ -628,6 +628,26 @@ __global__ void kLedgerKeys(int nm, int bits, const u64* pairKeys, u64* packed, 
     vals[i] = (int)i;
   }
 }
+// The ledger's stable key sort when no body has a ghost image: a manifold's real key is then its
+// own body-pair key, and the manifold list is in that key order (it is the contact list's key
+// order, boundary key (i, none) after the pairs of i). Empty manifolds carry the all-ones key and
+// sort last in list order. So the sorted order is the non-empty manifolds, then the empty ones,
+// each in list order: flags -> exclusive scan (pos) -> this scatter.
+__global__ void kLedgerFlags(int nm, const u64* pairKeys, int* flag) {
+  GRID_STRIDE(i, nm) flag[i] = pairKeys[i] != ~0ull ? 1 : 0;
+}
+__global__ void kLedgerRanks(int nm, int bits, const u64* pairKeys, const int* flag, const int* pos, u64* keysOut,
+                             int* permOut) {
+  const u64 none = (1ull << bits) - 1ull;
+  const int live = pos[nm];
+  GRID_STRIDE(i, nm) {
+    const u64 k = pairKeys[i];
+    const u64 u = k >> 32, v = k & 0xFFFFFFFFull;
+    const int r = flag[i] ? pos[i] : live + (int)i - pos[i];
+    keysOut[r] = ((u == 0xFFFFFFFFull ? none : u) << bits) | (v == 0xFFFFFFFFull ? none : v);
+    permOut[r] = (int)i;
+  }
+}
 // commitPairKeysLambda (:160-192): keys/perm already stably sorted by key
 template <class R>
 __global__ void kCommitLedger(Dev<R> d, int nm, const int* perm) {

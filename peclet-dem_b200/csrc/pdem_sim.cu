@@ -1557,7 +1557,16 @@ void Sim<R>::demStep() {
       lperm_.ensure(nm, false, s);
       const int kb = bitsFor((long)numParticles_ + 1);
       lkeysIn_.ensure(nm, false, s);
-      if (!keptM_) {  // the ledger order depends on the manifolds' real keys only
+      if (!keptM_ && numParticles_ == numReal_) {  // no ghost images: the list is in real-key order
+        ledFlag_.ensure((size_t)nm + 1, false, s);
+        ledPos_.ensure((size_t)nm + 1, false, s);
+        ++launches_, kLedgerFlags<<<gridFor(nm), B, 0, s>>>(nm, pairKeys_.p, ledFlag_.p);
+        cudaCheck(cudaMemsetAsync(ledFlag_.p + nm, 0, sizeof(int), s), "memset");
+        exclusiveSum(ledFlag_.p, ledPos_.p, nm + 1);
+        ++launches_, kLedgerRanks<<<gridFor(nm), B, 0, s>>>(nm, kb, pairKeys_.p, ledFlag_.p, ledPos_.p, lkeysS_.p,
+                                                            lperm_.p);
+        KCHECK("ledger ranks");
+      } else if (!keptM_) {  // the ledger order depends on the manifolds' real keys only
         ++launches_, kLedgerKeys<<<gridFor(nm), B, 0, s>>>(nm, kb, pairKeys_.p, lkeysIn_.p, lpermIn_.p);
         sortPairs(lkeysIn_.p, lkeysS_.p, lpermIn_.p, lperm_.p, nm, 2 * kb);
       }
