@@ -220,6 +220,10 @@ struct ColorJob {
   int *listA, *listB;  // [ne] each: every block's still-uncoloured entries, in its own chunk
   int* blockCount;     // [gridDim] the blocks' list lengths, published for the tail
   int *tailA, *tailB;  // [kColorTail] each: the tail's worklists (block 0 alone)
+  // stable order by colour, built in the same launch when order is set: order[ne] (entry indices,
+  // colour-major, index order within a colour), off[65] (first position of each colour key, then
+  // ne), hist[64 * gridDim] (scratch)
+  int *order = nullptr, *off = nullptr, *hist = nullptr;
 };
 // once at most this many entries (both colourings together) are left, block 0 alone runs the
 // remaining rounds with block barriers, and the other blocks wait at one grid barrier
@@ -319,6 +323,105 @@ template <class R, bool MANIFOLD>
 __device__ __forceinline__ void colorCommit(const Dev<R>& d, const ColorJob& J, int round, const ColorRange& rg,
                                             int* outCount) {
   colorCommitTo<R, MANIFOLD>(d, J, round, rg, (((round + 1) & 1) ? J.listB : J.listA) + rg.first, outCount);
+}
+// ---- stable order by colour (counting sort over 64 keys: colours 0..62, 63 for uncoloured, the
+// order of the reference's stable sort by colour). Block b owns the contiguous chunk
+// [b * chunk, (b + 1) * chunk) of the entries; the colour-major histogram H[key * gridDim + b]
+// scanned exclusively gives each (key, block) its first position. Colours are read through L2
+// (__ldcg): other SMs wrote them in this launch.
+__device__ __forceinline__ int colorSortKey(int c) { return c >= 0 ? c : 63; }
+__device__ __forceinline__ void colorChunk(const ColorJob& J, long& b0, long& b1) {
+  const long chunk = ((long)J.ne + gridDim.x - 1) / gridDim.x;
+  b0 = min((long)J.ne, (long)blockIdx.x * chunk);
+  b1 = min((long)J.ne, b0 + chunk);
+}
+__device__ __forceinline__ void colorOrderCount(const ColorJob& J) {
+  __shared__ int h[64];
+  if (!J.order || J.ne <= 0)
+    return;  // uniform over the grid
+  long b0, b1;
+  colorChunk(J, b0, b1);
+  __syncthreads();
+  if (threadIdx.x < 64)
+    h[threadIdx.x] = 0;
+  __syncthreads();
+  for (long i = b0 + threadIdx.x; i < b1; i += blockDim.x)
+    atomicAdd(&h[colorSortKey(__ldcg(&J.col[i]))], 1);
+  __syncthreads();
+  if (threadIdx.x < 64)
+    J.hist[(long)threadIdx.x * gridDim.x + blockIdx.x] = h[threadIdx.x];
+}
+// one block: exclusive scan of the histogram in place, and the colour offsets
+__device__ __forceinline__ void colorOrderScan(const ColorJob& J) {
+  __shared__ int part[kColorBlock];
+  if (!J.order || J.ne <= 0)
+    return;
+  const long n = 64L * gridDim.x;
+  const long per = (n + blockDim.x - 1) / blockDim.x;
+  const long s0 = min(n, (long)threadIdx.x * per), s1 = min(n, s0 + per);
+  int sum = 0;
+  for (long k = s0; k < s1; ++k)
+    sum += __ldcg(&J.hist[k]);
+  __syncthreads();
+  part[threadIdx.x] = sum;
+  __syncthreads();
+  for (int o = 1; o < (int)blockDim.x; o <<= 1) {  // inclusive scan of the partial sums
+    const int v = threadIdx.x >= (unsigned)o ? part[threadIdx.x - o] : 0;
+    __syncthreads();
+    part[threadIdx.x] += v;
+    __syncthreads();
+  }
+  int run = threadIdx.x ? part[threadIdx.x - 1] : 0;
+  for (long k = s0; k < s1; ++k) {
+    const int v = __ldcg(&J.hist[k]);
+    J.hist[k] = run;
+    run += v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 64)
+    J.off[threadIdx.x] = J.hist[(long)threadIdx.x * gridDim.x];
+  if (threadIdx.x == 0)
+    J.off[64] = J.ne;
+}
+// every block: its chunk in tiles of blockDim entries; within a tile, the rank among equal keys is
+// the lanes below in the warp with that key plus the earlier warps' counts of it
+__device__ __forceinline__ void colorOrderScatter(const ColorJob& J) {
+  __shared__ int run[64];
+  __shared__ int cnt[kColorBlock / 32][64];
+  if (!J.order || J.ne <= 0)
+    return;
+  long b0, b1;
+  colorChunk(J, b0, b1);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  __syncthreads();
+  if (threadIdx.x < 64)
+    run[threadIdx.x] = __ldcg(&J.hist[(long)threadIdx.x * gridDim.x + blockIdx.x]);
+  for (long t0 = b0; t0 < b1; t0 += blockDim.x) {
+    for (int k = threadIdx.x; k < nw * 64; k += blockDim.x)
+      (&cnt[0][0])[k] = 0;
+    __syncthreads();
+    const long i = t0 + threadIdx.x;
+    const int key = i < b1 ? colorSortKey(__ldcg(&J.col[i])) : 64;
+    const unsigned peers = __match_any_sync(0xffffffffu, key);
+    const int below = __popc(peers & ((1u << lane) - 1u));
+    if (key < 64 && below == 0)
+      cnt[w][key] = __popc(peers);
+    __syncthreads();
+    if (key < 64) {
+      int pos = run[key] + below;
+      for (int v = 0; v < w; ++v)
+        pos += cnt[v][key];
+      J.order[pos] = (int)i;
+    }
+    __syncthreads();
+    if (threadIdx.x < 64) {
+      int tot = 0;
+      for (int v = 0; v < nw; ++v)
+        tot += cnt[v][threadIdx.x];
+      run[threadIdx.x] += tot;
+    }
+    __syncthreads();
+  }
 }
 __device__ __forceinline__ void colorStats(const ColorJob& J, long gtid, long gstride) {
   int mxc = INT_MIN, left = 0;
@@ -513,6 +616,21 @@ __global__ void __launch_bounds__(kColorBlock) kColorBoth(Dev<R> d, ColorJob jm,
   }
   colorStats(jm, gtid, gstride);
   colorStats(jc, gtid, gstride);
+  // both colour orders (unless kept or batched: then the host orders them)
+  if (!jm.order && !jc.order)
+    return;
+  colorOrderCount(jm);
+  colorOrderCount(jc);
+  if (!gridBarrier(gb))
+    return;
+  if (blockIdx.x == 0)
+    colorOrderScan(jm);
+  if (blockIdx.x == (gridDim.x > 1 ? 1 : 0))
+    colorOrderScan(jc);
+  if (!gridBarrier(gb))
+    return;
+  colorOrderScatter(jm);
+  colorOrderScatter(jc);
 }
 
 }  // namespace pdem

@@ -1240,10 +1240,23 @@ void Sim<R>::colorBoth(int nm, int nc, int& ncolV, int& velLeft, int& ncolP, int
   colorTail_.ensure(2 * (maxGrid + 2 * kColorTail), false, stream_);
   int* tm = colorTail_.p;
   int* tc = colorTail_.p + maxGrid + 2 * kColorTail;
-  const ColorJob jm{neM, nbM, mColor_.p, winner_.p, winner2_.p, mask_.p, colorAux_.p, colorListM_.p,
-                    colorListM_.p + std::max(neM, 1), tm, tm + maxGrid, tm + maxGrid + kColorTail};
-  const ColorJob jc{neC, nbC, cColor_.p, winnerP_.p, winnerP2_.p, maskP_.p, colorAux_.p + 6, colorListC_.p,
-                    colorListC_.p + std::max(neC, 1), tc, tc + maxGrid, tc + maxGrid + kColorTail};
+  ColorJob jm{neM, nbM, mColor_.p, winner_.p, winner2_.p, mask_.p, colorAux_.p, colorListM_.p,
+              colorListM_.p + std::max(neM, 1), tm, tm + maxGrid, tm + maxGrid + kColorTail};
+  ColorJob jc{neC, nbC, cColor_.p, winnerP_.p, winnerP2_.p, maskP_.p, colorAux_.p + 6, colorListC_.p,
+              colorListC_.p + std::max(neC, 1), tc, tc + maxGrid, tc + maxGrid + kColorTail};
+  if (!batch_) {  // the colour orders come out of the same launch (the batched form orders by scene)
+    colorHist_.ensure(2 * 64 * (size_t)maxGrid, false, stream_);
+    if (neM > 0) {
+      mOrder_.ensure(neM, false, stream_);
+      mOff_.ensure(66, false, stream_);
+      jm.order = mOrder_.p, jm.off = mOff_.p, jm.hist = colorHist_.p;
+    }
+    if (neC > 0) {
+      cOrder_.ensure(neC, false, stream_);
+      cOff_.ensure(66, false, stream_);
+      jc.order = cOrder_.p, jc.off = cOff_.p, jc.hist = colorHist_.p + 64 * maxGrid;
+    }
+  }
   gbar_.ensure(2, false, stream_);
   const GridBar gb{gbar_.p, &ctr_.p->err, barrierSleepNs_};
   launchCoopB(kColorBoth<R>, colorBlock_, d_, jm, jc, std::max(nbM, nbC) + 2, gb, (const int*)topoFlags_.p,
@@ -1411,9 +1424,9 @@ void Sim<R>::demStep() {
   if (batch_ && (velLeft > 0 || posLeft > 0))
     throw std::runtime_error("batched scenes: uncoloured entries (Jacobi fallback) are not supported");
   // an unchanged graph keeps its colours, hence its colour order
-  if (useGS_ && ncolV > 0 && !keptM_)
+  if (batch_ && useGS_ && ncolV > 0 && !keptM_)
     colorOrder(true, nm, ncolV);
-  if (useGS_ && ncolP > 0 && !keptC_)
+  if (batch_ && useGS_ && ncolP > 0 && !keptC_)
     colorOrder(false, nc, ncolP);
   const bool usePGS = gNZ && useGS_;
   const R gMag = std::sqrt(g_[0] * g_[0] + g_[1] * g_[1] + g_[2] * g_[2]);

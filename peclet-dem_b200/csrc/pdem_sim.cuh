@@ -259,6 +259,7 @@ class Sim {
   DBuf<R> sceneParams_, sceneMaxScale_;
   DBuf<int> sceneLpt_;  // scenes by decreasing body count: dispatch order of the per-scene loops
   DBuf<int> rankBad_;   // the contact rank scatter's rejection flag
+  DBuf<int> colorHist_;  // the colouring launch's per-block colour histograms (both graphs)
   DBuf<int> ledFlag_, ledPos_;  // ledger order without ghost images: live flags and their scan
  public:
   long rankStats_[2] = {0, 0};  // substeps whose contact grouping was ranked, and ranked then rejected
