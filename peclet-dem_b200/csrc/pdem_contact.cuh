@@ -842,17 +842,6 @@ __device__ __forceinline__ long long entryKey(const Dev<R>& d, int i, int ea) {
   const int s = d.sceneOf[ea];
   return colorKey(MANIFOLD ? localManifold(d, i, s) : localContact(d, i, s));
 }
-// batched form: (scene, colour) keys, so each scene's colour classes are contiguous and in colour
-// order (scene << 6 | colour, 63 = uncoloured)
-template <class R, bool MANIFOLD>
-__global__ void kColorSortKeysScenes(Dev<R> d, int ne, const int* col, unsigned* keys, int* vals) {
-  GRID_STRIDE(i, ne) {
-    const int c = col[i];
-    const int body = MANIFOLD ? d.mab[i].x : d.cab[i].x;
-    keys[i] = ((unsigned)d.sceneOf[body] << 6) | ((c >= 0) ? (unsigned)c : 63u);
-    vals[i] = (int)i;
-  }
-}
 // Topology reuse. The colourings, colour orders, manifold grouping, incidence lists and ledger
 // order are functions of the contact list's body pairs (and, for the manifold side, of each
 // manifold's real ends and whether it is active). When those equal the previous substep's, the
@@ -878,11 +867,71 @@ __global__ void kSameManifolds(Dev<R> d, int nm, int4* prev, int* differ) {
   }
 }
 // colour keys for the stable colour-sorted execution order
-__global__ void kColorSortKeys(int ne, const int* col, unsigned* keys, int* vals) {
-  GRID_STRIDE(i, ne) {
-    const int c = col[i];
-    keys[i] = (c >= 0) ? (unsigned)c : 63u;  // colours are 0..62; 63 sorts the uncoloured last
-    vals[i] = (int)i;
+// batched form: the (scene, colour) order in one launch, one block per scene. A scene's entries are
+// the concatenation, in index order, of its slice of each of nr body-sorted ranges (firsts: nr
+// arrays of S + 1 first entries; manifolds: one range; contacts: pairs, planes, walls), so the
+// stable sort by (scene, colour) is, per scene, a stable counting sort by colour placed after the
+// entries of the scenes before it. off[s * 64 + c] is the first position of (s, c); off[S * 64] = ne.
+__global__ void __launch_bounds__(256) kColorOrderScenes(const int* col, const int* firsts, int nr, int S, int ne,
+                                                         int* order, int* off) {
+  __shared__ int run[64];
+  __shared__ int cnt[8][64];
+  const int s = blockIdx.x;
+  int lo[3] = {0, 0, 0}, len[3] = {0, 0, 0}, base = 0, total = 0;
+  for (int r = 0; r < nr; ++r) {
+    const int* f = firsts + (long)r * (S + 1);
+    lo[r] = f[s];
+    len[r] = f[s + 1] - f[s];
+    base += f[s] - f[0];
+    total += len[r];
+  }
+  auto entry = [&](int v) { return v < len[0] ? lo[0] + v : v < len[0] + len[1] ? lo[1] + v - len[0] : lo[2] + v - len[0] - len[1]; };
+  if (threadIdx.x < 64)
+    run[threadIdx.x] = 0;
+  __syncthreads();
+  for (int v = threadIdx.x; v < total; v += blockDim.x) {
+    const int c = col[entry(v)];
+    atomicAdd(&run[c >= 0 ? c : 63], 1);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {  // counts -> first positions
+    int acc = base;
+    for (int c = 0; c < 64; ++c) {
+      const int n = run[c];
+      run[c] = acc;
+      off[(long)s * 64 + c] = acc;
+      acc += n;
+    }
+    if (s == 0)
+      off[(long)S * 64] = ne;
+  }
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  for (int t0 = 0; t0 < total; t0 += blockDim.x) {
+    for (int k = threadIdx.x; k < nw * 64; k += blockDim.x)
+      (&cnt[0][0])[k] = 0;
+    __syncthreads();
+    const int v = t0 + (int)threadIdx.x;
+    const int i = v < total ? entry(v) : -1;
+    const int key = i >= 0 ? (col[i] >= 0 ? col[i] : 63) : 64;
+    const unsigned peers = __match_any_sync(0xffffffffu, key);
+    const int below = __popc(peers & ((1u << lane) - 1u));
+    if (key < 64 && below == 0)
+      cnt[w][key] = __popc(peers);
+    __syncthreads();
+    if (key < 64) {
+      int pos = run[key] + below;
+      for (int u = 0; u < w; ++u)
+        pos += cnt[u][key];
+      order[pos] = i;
+    }
+    __syncthreads();
+    if (threadIdx.x < 64) {
+      int tot = 0;
+      for (int u = 0; u < nw; ++u)
+        tot += cnt[u][threadIdx.x];
+      run[threadIdx.x] += tot;
+    }
+    __syncthreads();
   }
 }
 }  // namespace pdem

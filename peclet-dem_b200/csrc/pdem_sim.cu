@@ -1284,34 +1284,20 @@ void Sim<R>::colorBoth(int nm, int nc, int& ncolV, int& velLeft, int& ncolP, int
     colorRounds_[1] = res[11];
   }
 }
-// stable colour-sorted execution order: colour c occupies [off[c], off[c+1])
+// batched form: the (scene, colour) execution order, scene s's colour c occupying
+// [off[s * 64 + c], off[s * 64 + c + 1]) (the single-scene orders come out of kColorBoth)
 template <class R>
 void Sim<R>::colorOrder(bool manifold, int ne, int ncol) {
+  (void)ncol;
   DBuf<int>& order = manifold ? mOrder_ : cOrder_;
   DBuf<int>& off = manifold ? mOff_ : cOff_;
   order.ensure(ne, false, stream_);
-  off.ensure(std::max(ncol, 0) + 2, false, stream_);
-  uA_.ensure(ne, false, stream_);
-  uB_.ensure(ne, false, stream_);
-  iE_.ensure(ne, false, stream_);
-  if (batch_) {  // (scene, colour) order: each scene's classes contiguous, for one block per scene
-    const int nk = numScenes_ * 64;
-    off.ensure(nk + 2, false, stream_);
-    if (manifold)
-      ++launches_, kColorSortKeysScenes<R, true><<<gridFor(ne), kBlock, 0, stream_>>>(d_, ne, mColor_.p, uA_.p, iE_.p);
-    else
-      ++launches_, kColorSortKeysScenes<R, false><<<gridFor(ne), kBlock, 0, stream_>>>(d_, ne, cColor_.p, uA_.p, iE_.p);
-    KCHECK("color keys");
-    sortPairs(uA_.p, uB_.p, iE_.p, order.p, ne, 6 + bitsFor(numScenes_));
-    ++launches_, kLowerBoundOffsets<unsigned><<<gridFor(nk + 1), kBlock, 0, stream_>>>(ne, uB_.p, nk, off.p);
-    KCHECK("color offsets");
-    return;
-  }
-  ++launches_, kColorSortKeys<<<gridFor(ne), kBlock, 0, stream_>>>(ne, manifold ? mColor_.p : cColor_.p, uA_.p, iE_.p);
-  KCHECK("color keys");
-  sortPairs(uA_.p, uB_.p, iE_.p, order.p, ne, 6);
-  ++launches_, kLowerBoundOffsets<unsigned><<<gridFor(ncol + 1), kBlock, 0, stream_>>>(ne, uB_.p, ncol, off.p);
-  KCHECK("color offsets");
+  off.ensure((size_t)numScenes_ * 64 + 2, false, stream_);
+  // one block per scene over its slice of the body-sorted ranges (batchBounds' first entries)
+  ++launches_, kColorOrderScenes<<<numScenes_, 256, 0, stream_>>>(manifold ? mColor_.p : cColor_.p,
+                                                                 manifold ? sceneManFirstD_.p : sceneConFirstD_.p,
+                                                                 manifold ? 1 : 3, numScenes_, ne, order.p, off.p);
+  KCHECK("color order (scenes)");
 }
 // per-body incidence lists in ascending source order. kind 0: manifolds x real bodies,
 // 1: contacts x real bodies, 2: contacts x raw body slots
