@@ -114,9 +114,9 @@ def substep_bytes(n, P, C, M, iv, ip, D=8):
 
 # DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum summed over a stage's kernels in one
 # ncu capture of one substep) at the default workload of 262,144 spheres, in bytes per substep;
-# stages and sizes not captured report none. The colouring stage covers both colourings, the
-# contact colour order and the manifold incidence lists.
-STAGE_DRAM_BYTES = {(262144, "colour_velocity"): 26.7e6}
+# stages and sizes not captured report none. The colouring stage covers both colourings with both
+# colour orders (one launch) and the manifold incidence lists.
+STAGE_DRAM_BYTES = {(262144, "colour_velocity"): 23.0e6}
 
 
 def measured_peaks():
