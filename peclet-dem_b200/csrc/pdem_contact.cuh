@@ -648,6 +648,87 @@ __global__ void kLedgerRanks(int nm, int bits, const u64* pairKeys, const int* f
     permOut[r] = (int)i;
   }
 }
+// The ledger's stable key sort with ghost images present. Three kinds of manifold:
+// - in order: live, second body not a ghost. The real key equals the list key, so these come in
+//   key order (unique keys);
+// - ghost: live, second body a ghost image. These are compacted in list order and sorted alone;
+// - empty: the all-ones key, last, in list order.
+// Ranks: an in-order manifold m -> rpos[m] + the ghost entries before (key, m); the ghost entry at
+// sorted place q -> q + the in-order manifolds before (key, index), i.e. rpos[L] for L = the lower
+// bound of the key among the list keys, plus the one with the same key if its index is smaller; an
+// empty manifold -> all live ones + its place among the empty ones (m - rpos[m] - gpos[m]).
+__device__ __forceinline__ u64 ledgerPack(u64 k, int bits) {
+  const u64 none = (1ull << bits) - 1ull;
+  const u64 u = k >> 32, v = k & 0xFFFFFFFFull;
+  return ((u == 0xFFFFFFFFull ? none : u) << bits) | (v == 0xFFFFFFFFull ? none : v);
+}
+template <class R>
+__global__ void kLedgerClass(Dev<R> d, int nm, int bits, int numReal, const u64* pairKeys, u64* keys, int* inOrder,
+                             int* ghost) {
+  GRID_STRIDE(m, nm) {
+    const u64 k = pairKeys[m];
+    keys[m] = ledgerPack(k, bits);
+    const bool live = k != ~0ull, g = d.mab[m].y >= numReal;  // a boundary's second body is -1
+    inOrder[m] = (live && !g) ? 1 : 0;
+    ghost[m] = (live && g) ? 1 : 0;
+  }
+}
+__global__ void kLedgerApart(int nm, const u64* keys, const int* ghost, const int* gpos, u64* oKeys, int* oIdx) {
+  GRID_STRIDE(m, nm) {
+    if (ghost[m]) {
+      oKeys[gpos[m]] = keys[m];
+      oIdx[gpos[m]] = (int)m;
+    }
+  }
+}
+template <class R>
+__global__ void kLedgerMerge(Dev<R> d, int nm, int nG, int bits, const u64* keys, const int* inOrder, const int* rpos,
+                             const int* ghost, const int* gpos, const u64* gKeys, const int* gIdx, u64* keysOut,
+                             int* permOut) {
+  const u64 none = (1ull << bits) - 1ull;
+  const int live = rpos[nm] + gpos[nm];
+  GRID_STRIDE(t, (long)nm + nG) {
+    u64 k;
+    int r, idx;
+    if (t < nm) {
+      idx = (int)t;
+      if (ghost[idx])
+        continue;  // placed by its sorted entry
+      k = keys[idx];
+      if (!inOrder[idx]) {
+        r = live + idx - rpos[idx] - gpos[idx];
+      } else {
+        int lo = 0, hi = nG;  // ghost entries before (k, idx)
+        while (lo < hi) {
+          const int mid = (lo + hi) >> 1;
+          if (gKeys[mid] < k || (gKeys[mid] == k && gIdx[mid] < idx))
+            lo = mid + 1;
+          else
+            hi = mid;
+        }
+        r = rpos[idx] + lo;
+      }
+    } else {
+      const int q = (int)(t - nm);
+      k = gKeys[q];
+      idx = gIdx[q];
+      int lo = 0, hi = nm;  // list keys below k
+      while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        const int2 ab = d.mab[mid];
+        const u64 raw = ((u64)(unsigned)ab.x << bits) | (ab.y >= 0 ? (u64)(unsigned)ab.y : none);
+        if (raw < k)
+          lo = mid + 1;
+        else
+          hi = mid;
+      }
+      r = q + rpos[lo] + ((lo < nm && inOrder[lo] && keys[lo] == k && lo < idx) ? 1 : 0);
+    }
+    keysOut[r] = k;
+    permOut[r] = idx;
+  }
+}
+
 // commitPairKeysLambda (:160-192): keys/perm already stably sorted by key
 template <class R>
 __global__ void kCommitLedger(Dev<R> d, int nm, const int* perm) {

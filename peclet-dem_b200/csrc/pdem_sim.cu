@@ -1509,6 +1509,25 @@ void Sim<R>::demStep() {
     if (stabMode_ == 4 && batch_)
       throw std::runtime_error("batched scenes: stabilization mode 'ordered' is not supported");
     ctl(CTL_STAB_DECIDE, vRestS, stabMode_);
+    // periodic scenes: split the manifolds for the ledger order now, so the number of ghost
+    // manifolds (the host sizes their sort with it) comes back with the decision below
+    ledgerSplit_ = nm > 0 && !keptM_ && numParticles_ != numReal_ && (stabMode_ == 1 || stabMode_ == 3 || stabMode_ == 4);
+    if (ledgerSplit_) {
+      const int kbL = bitsFor((long)numParticles_ + 1);
+      lkeysIn_.ensure(nm, false, s);
+      ledFlag_.ensure((size_t)nm + 1, false, s);
+      ledPos_.ensure((size_t)nm + 1, false, s);
+      ledGhost_.ensure((size_t)nm + 1, false, s);
+      ledGPos_.ensure((size_t)nm + 1, false, s);
+      ++launches_, kLedgerClass<R><<<gridFor(nm), B, 0, s>>>(d_, nm, kbL, numReal_, pairKeys_.p, lkeysIn_.p, ledFlag_.p,
+                                                             ledGhost_.p);
+      cudaCheck(cudaMemsetAsync(ledFlag_.p + nm, 0, sizeof(int), s), "memset");
+      cudaCheck(cudaMemsetAsync(ledGhost_.p + nm, 0, sizeof(int), s), "memset");
+      exclusiveSum(ledFlag_.p, ledPos_.p, nm + 1);
+      exclusiveSum(ledGhost_.p, ledGPos_.p, nm + 1);
+      KCHECK("ledger split");
+      readBack(&ledgerGhosts_, ledGPos_.p + nm, sizeof(int));
+    }
     // the pass runs only when the main sweeps left a residual (src/sim.hpp:282): read the
     // decision so an untriggered pass costs nothing
     const bool stabRun = (stabMode_ == 1 || stabMode_ == 3 || stabMode_ == 4) && readCounters().stabRun;
@@ -1565,6 +1584,22 @@ void Sim<R>::demStep() {
         ++launches_, kLedgerRanks<<<gridFor(nm), B, 0, s>>>(nm, kb, pairKeys_.p, ledFlag_.p, ledPos_.p, lkeysS_.p,
                                                             lperm_.p);
         KCHECK("ledger ranks");
+      } else if (ledgerSplit_) {  // ghost images: sort the ghost manifolds alone, then merge
+        const int nG = ledgerGhosts_;
+        ledOKeys_.ensure(std::max(nG, 1), false, s);
+        ledOKeysS_.ensure(std::max(nG, 1), false, s);
+        ledOIdx_.ensure(std::max(nG, 1), false, s);
+        ledOIdxS_.ensure(std::max(nG, 1), false, s);
+        if (nG > 0) {
+          ++launches_, kLedgerApart<<<gridFor(nm), B, 0, s>>>(nm, lkeysIn_.p, ledGhost_.p, ledGPos_.p, ledOKeys_.p,
+                                                              ledOIdx_.p);
+          sortPairs(ledOKeys_.p, ledOKeysS_.p, ledOIdx_.p, ledOIdxS_.p, nG, 2 * kb);
+        }
+        ++launches_, kLedgerMerge<R><<<gridFor((long)nm + nG), B, 0, s>>>(d_, nm, nG, kb, lkeysIn_.p, ledFlag_.p,
+                                                                         ledPos_.p, ledGhost_.p, ledGPos_.p,
+                                                                         ledOKeysS_.p, ledOIdxS_.p, lkeysS_.p,
+                                                                         lperm_.p);
+        KCHECK("ledger merge");
       } else if (!keptM_) {  // the ledger order depends on the manifolds' real keys only
         ++launches_, kLedgerKeys<<<gridFor(nm), B, 0, s>>>(nm, kb, pairKeys_.p, lkeysIn_.p, lpermIn_.p);
         sortPairs(lkeysIn_.p, lkeysS_.p, lpermIn_.p, lperm_.p, nm, 2 * kb);

@@ -260,7 +260,12 @@ class Sim {
   DBuf<int> sceneLpt_;  // scenes by decreasing body count: dispatch order of the per-scene loops
   DBuf<int> rankBad_;   // the contact rank scatter's rejection flag
   DBuf<int> colorHist_;  // the colouring launch's per-block colour histograms (both graphs)
-  DBuf<int> ledFlag_, ledPos_;  // ledger order without ghost images: live flags and their scan
+  DBuf<int> ledFlag_, ledPos_;  // ledger order: in-order (or live) flags and their scan
+  DBuf<int> ledGhost_, ledGPos_;    // ledger order with ghost images: ghost-manifold flags, scan
+  DBuf<u64> ledOKeys_, ledOKeysS_;  // the ghost manifolds' keys
+  DBuf<int> ledOIdx_, ledOIdxS_;    // and indices, before and after their sort
+  bool ledgerSplit_ = false;        // this substep's ledger order merges the sorted ghost manifolds
+  int ledgerGhosts_ = 0;            // their count (read back with the stabilization decision)
  public:
   long rankStats_[2] = {0, 0};  // substeps whose contact grouping was ranked, and ranked then rejected
  private:
