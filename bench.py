@@ -41,6 +41,7 @@ import numpy as np  # noqa: E402
 METRIC = "particle-substeps/s"
 SUBSTEPS = 10
 REF_OMP = os.path.join(ROOT, "oracle", "_ref", "libref_omp.so")
+REF_SERIAL = os.path.join(ROOT, "oracle", "_ref", "libref_serial.so")
 
 
 def workload_desc(n):
@@ -375,12 +376,29 @@ def run_config_lines(args, dem):
     line = {"workload": f"plain_settling_{sc.n}", "unit": METRIC, "dtype": "f64",
             "value": sc.n * sc.substeps * steps / t, "ms_per_step": 1e3 * t / steps,
             "substeps_timed": steps * sc.substeps, "contacts_last_substep": sim.num_contacts()}
+    # the working set fits in L2 (126 MB): the byte model's bandwidth is L2 context, not an HBM
+    # fraction (counts of the last substep stand for every timed substep)
+    c = sim.counters()
+    nb = sim.num_particles()
+    per_sub = substep_bytes(nb, c["pairs"], c["contacts"], c["manifolds"], c["velocity_sweeps"],
+                            c["position_sweeps"])
+    line["l2_resident"] = {
+        "working_set_mb": round((nb * 300 + c["pairs"] * 8 + c["contacts"] * 2 * (8 + 16 * 8)
+                                 + c["manifolds"] * (12 + 20 * 8)) / 1e6, 2),
+        "algorithmic_gbps": per_sub * sc.substeps * steps / t / 1e9,
+        "counts_last_substep": {k: c[k] for k in ("pairs", "contacts", "manifolds", "velocity_sweeps",
+                                                  "position_sweeps")}}
     sim.close()
     if not args.no_cpu and os.path.exists(REF_OMP):
         threads = os.cpu_count() or 1
         v, el = cpu_reference(sc, 200, threads)
         line["cpu_reference"] = {"value": v, "unit": METRIC, "cores": threads, "kind": "reference",
                                  "sample": f"200 substeps of the same scene, {el:.1f} s"}
+    if not args.no_cpu and os.path.exists(REF_SERIAL):
+        v, el = cpu_reference(sc, 100, 1, REF_SERIAL)
+        line["cpu_reference_serial"] = {"value": v, "unit": METRIC, "cores": 1, "kind": "reference",
+                                        "sample": f"100 substeps of the same scene, serial shim build, "
+                                                  f"{el:.1f} s"}
     out["settling"] = line
 
     sc, extra = W.polydisperse_hertz_closed()
@@ -417,13 +435,14 @@ def run_config_lines(args, dem):
 
 
 # ---------------------------------------------------------------------------------------------
-def cpu_reference(scene, substeps, threads):
-    """Time the reference's own substep (OpenMP shim build) for `substeps` calls; returns
-    particle-substeps/s. State set exactly as on the GPU (the reference computes in float)."""
+def cpu_reference(scene, substeps, threads, lib=REF_OMP):
+    """Time the reference's own substep (OpenMP shim build, or the serial one) for `substeps`
+    calls; returns particle-substeps/s. State set exactly as on the GPU (the reference computes in
+    float)."""
     os.environ["OMP_NUM_THREADS"] = str(threads)
     os.environ.setdefault("OMP_PROC_BIND", "close")
     from peclet.dem._capi import CApi, CApiSimulation
-    api = CApi(REF_OMP, "ref")
+    api = CApi(lib, "ref")
     sim = scene.apply(CApiSimulation(api, scene.n + 8, "fp32"))
     sim.step(scene.dt)  # warm-up: first-touch allocations and ghost capacity
     t = time.perf_counter()
