@@ -224,6 +224,28 @@ __device__ __forceinline__ BoundaryProbe<R> probePlane(const Dev<R>& d, int i, i
   r.hit = r.dist < margin;
   return r;
 }
+// A shell particle whose centre is farther from plane pl than its shell's reach plus the margin has
+// no point within the margin and none below the plane: every point's distance is the centre's plus
+// the projection of its offset rot(q, p s), and rot(q, v) = q v q* + (1 - |q|^2) v has norm at most
+// (|q|^2 + |1 - |q|^2|) |v| <= that factor * shellR * s. The test keeps a slack of 1e-4 of the
+// magnitudes involved (far above the rounding of either computation), so it only skips particles
+// whose probes would all miss.
+template <class R>
+__device__ __forceinline__ bool planeOutOfReach(const Dev<R>& d, int i, int pl, const ShapeDesc<R>& sd, R s,
+                                                R margin) {
+  if (sd.numPoints <= 0)
+    return false;
+  const PlaneDesc<R> P = d.planes[pl];
+  const V3<R> pp{P.p[0], P.p[1], P.p[2]}, pn{P.n[0], P.n[1], P.n[2]};
+  const V3<R> pA = v3(d.posPred[i]);
+  const R distC = dot(sub(pA, pp), pn);
+  const Q4<R> q = d.quatPred[i];
+  const R qn2 = q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w;
+  const R reach = sd.shellR * s * (qn2 + fabs(R(1) - qn2)) * sqrt(dot(pn, pn));
+  const R mag = fabs(distC) + reach + fabs(margin) + fabs(pA.x) + fabs(pA.y) + fabs(pA.z) + fabs(pp.x) +
+                fabs(pp.y) + fabs(pp.z);
+  return distC - reach > margin + R(1e-4) * mag;
+}
 template <class R>
 __device__ __forceinline__ BoundaryProbe<R> probeWall(const Dev<R>& d, int i, int wi, int k, const ShapeDesc<R>& sd,
                                                      R s, R margin, bool needNormal) {
@@ -294,7 +316,9 @@ __global__ void kBoundary(Dev<R> d, int numReal, NarrowP<R> P, int* cntP, int* c
   for (long i = warp; i < numReal; i += nwarps) {
     const R s = d.scale[i] * P.globalScale;
     int run = MODE ? basePlanes + offP[i] : 0, tot = 0;
-    for (int pl = 0; pl < P.numPlanes; ++pl)
+    for (int pl = 0; pl < P.numPlanes; ++pl) {
+      if (planeOutOfReach(d, (int)i, pl, sd, s, marginOf(d, P, (int)i)))
+        continue;  // uniform over the warp (one particle)
       for (int k0 = 0; k0 < K; k0 += 32) {
         const int k = k0 + lane;
         BoundaryProbe<R> b;
@@ -313,6 +337,7 @@ __global__ void kBoundary(Dev<R> d, int numReal, NarrowP<R> P, int* cntP, int* c
         run += __popc(m);
         tot += __popc(m);
       }
+    }
     if (MODE == 0 && lane == 0)
       cntP[i] = tot;
     run = MODE ? baseWalls + offW[i] : 0;

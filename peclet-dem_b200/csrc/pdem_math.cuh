@@ -114,6 +114,7 @@ struct ShapeDesc {
   int nx, ny, nz, pad;
   R gridOrigin[3];
   R gridInvSpacing[3];
+  R shellR;  // largest shell-point norm (canonical units, rounded up); 0 without a shell
 };
 
 template <class R>

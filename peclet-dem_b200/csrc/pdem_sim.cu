@@ -368,6 +368,12 @@ void Sim<R>::initializeShape(int type, R radius, R height, R thick) {
 }
 template <class R>
 void Sim<R>::uploadShape() {
+  double r2 = 0;
+  for (int k = 0; k < shape_.numPoints && k < (int)shellHost_.size(); ++k) {
+    const Q4<R>& q = shellHost_[k];
+    r2 = std::max(r2, (double)q.x * q.x + (double)q.y * q.y + (double)q.z * q.z);
+  }
+  shape_.shellR = std::nextafter((R)std::sqrt(r2), std::numeric_limits<R>::infinity());
   shapeD_.ensure(1, false, stream_);
   cudaCheck(cudaMemcpyAsync(shapeD_.p, &shape_, sizeof shape_, cudaMemcpyHostToDevice, stream_), "H2D shape");
   const size_t ns = std::max<size_t>(1, shellHost_.size());
