@@ -134,3 +134,29 @@ def spheres_in_drum(seed=15, n=120, R=6e-3, length=4e-3, omega=2.0, e=0.5, mu=0.
         wid = sim.add_sdf_wall(grid, nx, ny, nz, origin, spacing, 0.5, 0.6)
         sim.set_wall_velocity(wid, (0, 0, 0), (0, 0, omega), (0, 0, 0))
     return sc, extra
+
+
+def shells_at_floor(seed=18, L=40e-3):
+    """Hollow-cylinder shells held just above and below the reach of a floor plane (the largest
+    shell-point norm times the scale, plus the contact margin): bodies at heights stepping through
+    that bound, one orientation putting a rim corner straight down and others random."""
+    rng = np.random.default_rng(seed)
+    s = 1e-3
+    reach = np.sqrt(1.0 + 1.5 ** 2) * s  # farthest shell point of (r_out 1, length 3)
+    dz = np.array([-5e-4, -2e-4, -5e-5, 0.0, 5e-5, 1.2e-4, 1.6e-4, 1.8e-4, 2.0e-4, 2.4e-4, 5e-4])
+    a = -np.arctan(1.5)  # about x: the corner (0, 1.5, -1) straight down
+    corner = np.array([np.sin(a / 2), 0.0, 0.0, np.cos(a / 2)])
+    pos, quat = [], []
+    for k, h in enumerate(dz):
+        for j, q in enumerate((corner, W.random_unit_quats(rng, 1)[0])):
+            pos.append([3e-3 + 5.5e-3 * (k % 5), 3e-3 + 5.5e-3 * (2 * (k // 5) + j), reach + h])
+            quat.append(q)
+    pos, quat = np.array(pos), np.array(quat)
+    n = len(pos)
+    m = 1200.0 * np.pi * (1.0 - 0.36) * 3.0 * s ** 3
+    iI = np.tile([12 / (m * (3 * 1.36 + 9) * s * s), 2 / (m * 1.36 * s * s), 12 / (m * (3 * 1.36 + 9) * s * s)],
+                 (n, 1))
+    return W.Scene(name="shells_at_floor", pos=pos, vel=np.zeros((n, 3)), inv_mass=np.full(n, 1.0 / m),
+                   inv_inertia=iI, quat=quat, shape=(W.HOLLOW_CYLINDER, 1.0, 3.0, 0.4), global_scale=s,
+                   domain=((0, 0, 0), (L, L, L), (False, False, False)), planes=W.box_planes((0, 0, 0), (L, L, L)),
+                   material=(0.4, 0.0, 0.3), iterations=(20, 10), dt=6.25e-6)

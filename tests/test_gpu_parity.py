@@ -129,3 +129,12 @@ def test_contact_grouping_sorted_path():
                        cwd=root, env={**os.environ, "PDEM_CONTACT_SORT": "1"}, capture_output=True, text=True)
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
     assert " passed" in r.stdout and "5 passed" in r.stdout, r.stdout[-500:]
+
+
+@pytest.mark.parametrize("precision,rtol", [("fp32", 0.0), ("fp64", 1e-12)])
+def test_shell_plane_reach_cull(gpu_api, orc_api, precision, rtol):
+    """Shell bodies at heights stepping through the plane-reach bound (shell reach plus the contact
+    margin), one orientation with a rim corner straight down: the culled boundary probes leave the
+    contacts, overlaps and state identical to the oracle's full probing."""
+    import scenes as S
+    _run_pair(gpu_api, orc_api, "shells_at_floor", S.shells_at_floor, None, 4, precision, rtol)
