@@ -434,10 +434,12 @@ __global__ void kHertzGatherIntegrate(Dev<R> d, int n, const int* incOff, const 
 
 template <class R>
 __global__ void kHertzMaxDisp2(Dev<R> d, int n, const Q4<R>* ref, R* out) {
+  R mx = R(0);
   GRID_STRIDE(i, n) {
     const V3<R> dd = sub(v3(d.pos[i]), v3(ref[i]));
-    atomicMaxNonNeg(out, dot(dd, dd));
+    runMax(mx, dot(dd, dd));
   }
+  blockMaxAtomic(out, mx);  // one atomic per block on the one word
 }
 // carry the shear history onto the rebuilt list (src/sim.hpp:558-585)
 template <class R>
