@@ -62,8 +62,20 @@ __device__ __forceinline__ bool gridBarrier(const GridBar& gb) {
 // Coloured sweep loop. KIND 0: projected GS velocity sweep (pgsOne), 1: one-shot GS velocity
 // sweep (gsOne), 2: position sweep (posGSOne). LOOP selects the control flags: 1 main velocity
 // loop, 2 stabilization loop, 3 position loop. The host has already run the first sweep's BEGIN
-// (kCtl): each END here is fused with the next sweep's BEGIN.
-template <class R, int KIND, int LOOP>
+// (kCtl): each END here is fused with the next sweep's BEGIN. CLUSTER: the launch is one thread-block
+// cluster (a small graph), and the hardware cluster barrier (arrive with release, wait with acquire
+// semantics at cluster scope) replaces the grid-wide one.
+constexpr int kSweepCluster = 8;                                  // blocks of the small-graph launch
+constexpr int kSweepClusterEntries = 4 * kSweepCluster * kBlock;  // largest graph it takes
+template <bool CLUSTER>
+__device__ __forceinline__ bool loopBarrier(const GridBar& gb) {
+  if (CLUSTER) {
+    cg::this_cluster().sync();
+    return true;
+  }
+  return gridBarrier(gb);
+}
+template <class R, int KIND, int LOOP, bool CLUSTER = false>
 __global__ void __launch_bounds__(kBlock) kSweepLoop(Dev<R> d, const int* order, const int* coff, int ncol, int iters,
                                                      SolveP<R> P, R thr, GridBar gb) {
   Counters<R>* c = d.ctr;
@@ -92,7 +104,7 @@ __global__ void __launch_bounds__(kBlock) kSweepLoop(Dev<R> d, const int* order,
         }
       if (col == ncol - 1)
         warpMaxAtomic(mxp, mx);
-      if (!gridBarrier(gb))
+      if (!loopBarrier<CLUSTER>(gb))
         return;
     }
     // END of this sweep, then BEGIN of the next one
@@ -128,7 +140,7 @@ __global__ void __launch_bounds__(kBlock) kSweepLoop(Dev<R> d, const int* order,
         *sweeps += 1;
       }
     }
-    if (!gridBarrier(gb))
+    if (!loopBarrier<CLUSTER>(gb))
       return;
     if (*done)
       break;

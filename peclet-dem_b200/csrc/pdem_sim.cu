@@ -265,6 +265,34 @@ template <class K, class... A>
 void Sim<R>::launchCoop(K kernel, A... args) {
   launchCoopB(kernel, kBlock, args...);
 }
+template <class R>
+template <class K, class... A>
+bool Sim<R>::launchCluster(K kernel, A... args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(kSweepCluster);
+  cfg.blockDim = dim3(kBlock);
+  cfg.stream = stream_;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = kSweepCluster;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  const void* key = reinterpret_cast<const void*>(kernel);
+  auto it = clusterOk_.find(key);
+  if (it == clusterOk_.end()) {
+    int clusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&clusters, kernel, &cfg) != cudaSuccess)
+      (void)cudaGetLastError();
+    it = clusterOk_.emplace(key, clusters >= 1 ? 1 : 0).first;
+  }
+  if (!it->second)
+    return false;
+  ++launches_;
+  cudaCheck(cudaLaunchKernelEx(&cfg, kernel, args...), "cluster launch");
+  return true;
+}
 
 // ---- CUB helpers ----
 template <class R>
@@ -1462,9 +1490,13 @@ void Sim<R>::demStep() {
       ++launches_, kSweepScenes<R, 0, 1><<<numScenes_, sceneBlock(), 0, s>>>(d_, sceneLpt_.p, mOrder_.p, mOff_.p, velIters_, sp, thr);
     else if (batch_)
       ++launches_, kSweepScenes<R, 1, 1><<<numScenes_, sceneBlock(), 0, s>>>(d_, sceneLpt_.p, mOrder_.p, mOff_.p, velIters_, sp, thr);
-    else if (usePGS)
+    else if (usePGS && !(nm <= kSweepClusterEntries &&
+                         launchCluster(kSweepLoop<R, 0, 1, true>, d_, (const int*)mOrder_.p, (const int*)mOff_.p,
+                                       ncolV, velIters_, sp, thr, gb)))
       launchCoop(kSweepLoop<R, 0, 1>, d_, (const int*)mOrder_.p, (const int*)mOff_.p, ncolV, velIters_, sp, thr, gb);
-    else
+    else if (!usePGS && !(nm <= kSweepClusterEntries &&
+                          launchCluster(kSweepLoop<R, 1, 1, true>, d_, (const int*)mOrder_.p, (const int*)mOff_.p,
+                                        ncolV, velIters_, sp, thr, gb)))
       launchCoop(kSweepLoop<R, 1, 1>, d_, (const int*)mOrder_.p, (const int*)mOff_.p, ncolV, velIters_, sp, thr, gb);
     KCHECK("velocity loop");
   }
@@ -1556,7 +1588,9 @@ void Sim<R>::demStep() {
         ctl(CTL_STAB_BEGIN, R(0), 0);
         if (batch_)
           ++launches_, kSweepScenes<R, 0, 2><<<numScenes_, sceneBlock(), 0, s>>>(d_, sceneLpt_.p, mOrder_.p, mOff_.p, iters, ss, vRestS);
-        else
+        else if (!(nm <= kSweepClusterEntries &&
+                   launchCluster(kSweepLoop<R, 0, 2, true>, d_, (const int*)mOrder_.p, (const int*)mOff_.p, ncolV,
+                                 iters, ss, vRestS, gb)))
           launchCoop(kSweepLoop<R, 0, 2>, d_, (const int*)mOrder_.p, (const int*)mOff_.p, ncolV, iters, ss, vRestS, gb);
       }
       for (int it = 0; it < (stabPersistent ? 0 : iters); ++it) {
@@ -1660,7 +1694,9 @@ void Sim<R>::demStep() {
       ++launches_, kSweepScenes<R, 2, 3><<<numScenes_, sceneBlock(), 0, s>>>(d_, sceneLpt_.p, cOrder_.p, cOff_.p, posIters_, sp, posTol);
       tuneEnd();
     }
-    else
+    else if (!(nc <= kSweepClusterEntries &&
+               launchCluster(kSweepLoop<R, 2, 3, true>, d_, (const int*)cOrder_.p, (const int*)cOff_.p, ncolP,
+                             posIters_, sp, posTol, gb)))
       launchCoop(kSweepLoop<R, 2, 3>, d_, (const int*)cOrder_.p, (const int*)cOff_.p, ncolP, posIters_, sp, posTol, gb);
     KCHECK("position loop");
   }

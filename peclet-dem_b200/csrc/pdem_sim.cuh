@@ -371,6 +371,10 @@ class Sim {
   void launchCoopB(K kernel, int block, A... args);
   template <class K, class... A>
   void launchCoop(K kernel, A... args);
+  // one thread-block cluster of kSweepCluster blocks; false when such a cluster cannot be resident
+  template <class K, class... A>
+  bool launchCluster(K kernel, A... args);
+  std::map<const void*, int> clusterOk_;  // per kernel: 1 resident, 0 not
   std::map<std::pair<const void*, int>, int> coopPer_;  // resident blocks per SM, by (kernel, block)
   template <class T>
   void sortPairs(const T* kin, T* kout, const int* vin, int* vout, int n, int endBit);
