@@ -363,35 +363,59 @@ __device__ __forceinline__ void colorOrderCount(const ColorJob& J) {
   if (threadIdx.x < 64)
     J.hist[(long)threadIdx.x * gridDim.x + blockIdx.x] = h[threadIdx.x];
 }
-// one block: exclusive scan of the histogram in place, and the colour offsets
+// one block: exclusive scan of the colour-major histogram in place, and the colour offsets. Each
+// warp scans whole rows (colours) with shuffles over coalesced loads, then one warp scans the 64
+// row totals, and each row gets its offset.
 __device__ __forceinline__ void colorOrderScan(const ColorJob& J) {
-  __shared__ int part[kColorBlock];
+  __shared__ int rowTot[64], rowOff[64];
   if (!J.order || J.ne <= 0)
     return;
-  const long n = 64L * gridDim.x;
-  const long per = (n + blockDim.x - 1) / blockDim.x;
-  const long s0 = min(n, (long)threadIdx.x * per), s1 = min(n, s0 + per);
-  int sum = 0;
-  for (long k = s0; k < s1; ++k)
-    sum += __ldcg(&J.hist[k]);
-  __syncthreads();
-  part[threadIdx.x] = sum;
-  __syncthreads();
-  for (int o = 1; o < (int)blockDim.x; o <<= 1) {  // inclusive scan of the partial sums
-    const int v = threadIdx.x >= (unsigned)o ? part[threadIdx.x - o] : 0;
-    __syncthreads();
-    part[threadIdx.x] += v;
-    __syncthreads();
+  const int G = gridDim.x, lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  __syncthreads();  // rowTot / rowOff free (a previous call's reads are done)
+  for (int c = w; c < 64; c += nw) {
+    int* row = J.hist + (long)c * G;
+    int run = 0;
+    for (int b0 = 0; b0 < G; b0 += 32) {
+      const int b = b0 + lane;
+      const int v = b < G ? __ldcg(&row[b]) : 0;
+      int x = v;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o)
+          x += y;
+      }
+      if (b < G)
+        row[b] = run + x - v;
+      run += __shfl_sync(0xffffffffu, x, 31);
+    }
+    if (lane == 0)
+      rowTot[c] = run;
   }
-  int run = threadIdx.x ? part[threadIdx.x - 1] : 0;
-  for (long k = s0; k < s1; ++k) {
-    const int v = __ldcg(&J.hist[k]);
-    J.hist[k] = run;
-    run += v;
+  __syncthreads();
+  if (w == 0) {
+    const int a = rowTot[lane], b = rowTot[lane + 32];
+    int xa = a, xb = b;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int ya = __shfl_up_sync(0xffffffffu, xa, o), yb = __shfl_up_sync(0xffffffffu, xb, o);
+      if (lane >= o) {
+        xa += ya;
+        xb += yb;
+      }
+    }
+    const int totA = __shfl_sync(0xffffffffu, xa, 31);
+    rowOff[lane] = xa - a;
+    rowOff[lane + 32] = totA + xb - b;
   }
   __syncthreads();
+  for (int c = w; c < 64; c += nw) {  // the same thread wrote these entries above
+    int* row = J.hist + (long)c * G;
+    for (int b = lane; b < G; b += 32)
+      row[b] += rowOff[c];
+  }
   if (threadIdx.x < 64)
-    J.off[threadIdx.x] = J.hist[(long)threadIdx.x * gridDim.x];
+    J.off[threadIdx.x] = rowOff[threadIdx.x];
   if (threadIdx.x == 0)
     J.off[64] = J.ne;
 }
@@ -514,14 +538,12 @@ __device__ void colorTail(const Dev<R>& d, const ColorJob& jm, const ColorJob& j
       colorContend<R, true>(d, jm, round, rm);
     if (!doneC)
       colorContend<R, false>(d, jc, round, rc);
-    __threadfence();
-    __syncthreads();
+    __syncthreads();  // block 0 alone: the block barrier orders its global accesses
     if (!doneM)
       colorCommitTo<R, true>(d, jm, round, rm, outM, &sOut[0]);
     if (!doneC)
       colorCommitTo<R, false>(d, jc, round, rc, outC, &sOut[1]);
-    __threadfence();
-    __syncthreads();
+    __syncthreads();  // block 0 alone: the block barrier orders its global accesses
     const int remM = sOut[0], remC = sOut[1];
     if (threadIdx.x == 0) {
       if (!doneM)
