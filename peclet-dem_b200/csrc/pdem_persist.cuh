@@ -231,7 +231,8 @@ struct ColorJob {
                        // [5] rounds run
   int *listA, *listB;  // [ne] each: every block's still-uncoloured entries, in its own chunk
   int* blockCount;     // [gridDim] the blocks' list lengths, published for the tail
-  int *tailA, *tailB;  // [kColorTail] each: the tail's worklists (block 0 alone)
+  int *tailA, *tailB;  // [kColorTailMax] each: the tail's worklists (block 0 alone)
+  int tailAt;          // block 0 takes over once at most this many entries (both graphs) are left
   // stable order by colour, built in the same launch when order is set: order[ne] (entry indices,
   // colour-major, index order within a colour), off[65] (first position of each colour key, then
   // ne), hist[64 * gridDim] (scratch)
@@ -239,7 +240,8 @@ struct ColorJob {
 };
 // once at most this many entries (both colourings together) are left, block 0 alone runs the
 // remaining rounds with block barriers, and the other blocks wait at one grid barrier
-constexpr int kColorTail = 4096;
+constexpr int kColorMaxChunks = 20;    // histogram row chunks of 32 blocks (grids up to 640 blocks)
+constexpr int kColorTailMax = 65536;  // largest tail hand-over the worklists are sized for
 
 template <class R, bool MANIFOLD>
 __device__ __forceinline__ void colorInit(const Dev<R>& d, const ColorJob& J, long gtid, long gstride) {
@@ -375,9 +377,17 @@ __device__ __forceinline__ void colorOrderScan(const ColorJob& J) {
   for (int c = w; c < 64; c += nw) {
     int* row = J.hist + (long)c * G;
     int run = 0;
-    for (int b0 = 0; b0 < G; b0 += 32) {
+    int vals[kColorMaxChunks];  // the row's loads, issued together (G <= 32 * kColorMaxChunks)
+#pragma unroll
+    for (int k = 0; k < kColorMaxChunks; ++k)
+      vals[k] = (32 * k + lane < G) ? __ldcg(&row[32 * k + lane]) : 0;
+#pragma unroll
+    for (int k = 0; k < kColorMaxChunks; ++k) {
+      const int b0 = 32 * k;
+      if (b0 >= G)
+        break;
       const int b = b0 + lane;
-      const int v = b < G ? __ldcg(&row[b]) : 0;
+      const int v = vals[k];
       int x = v;
 #pragma unroll
       for (int o = 1; o < 32; o <<= 1) {
@@ -624,7 +634,7 @@ __global__ void __launch_bounds__(kColorBlock) kColorBoth(Dev<R> d, ColorJob jm,
     }
     // few entries left: publish this block's lists, and block 0 takes over (uniform decision)
     if (!(doneM && doneC) && round + 1 < maxRounds && gridDim.x <= blockDim.x &&
-        (doneM ? 0 : prevM) + (doneC ? 0 : prevC) <= kColorTail) {
+        (doneM ? 0 : prevM) + (doneC ? 0 : prevC) <= jm.tailAt) {
       if (threadIdx.x == 0) {
         jm.blockCount[blockIdx.x] = doneM ? 0 : sCount[0][(round + 1) & 1];
         jc.blockCount[blockIdx.x] = doneC ? 0 : sCount[1][(round + 1) & 1];

@@ -1271,13 +1271,13 @@ void Sim<R>::colorBoth(int nm, int nc, int& ncolV, int& velLeft, int& ncolP, int
   colorListC_.ensure(2 * std::max(neC, 1), false, stream_);
   // per job: the blocks' list lengths (up to 4 blocks per SM), then the tail's two lists
   const int maxGrid = 4 * numSMs_;
-  colorTail_.ensure(2 * (maxGrid + 2 * kColorTail), false, stream_);
+  colorTail_.ensure(2 * (maxGrid + 2 * (size_t)kColorTailMax), false, stream_);
   int* tm = colorTail_.p;
-  int* tc = colorTail_.p + maxGrid + 2 * kColorTail;
+  int* tc = colorTail_.p + maxGrid + 2 * kColorTailMax;
   ColorJob jm{neM, nbM, mColor_.p, winner_.p, winner2_.p, mask_.p, colorAux_.p, colorListM_.p,
-              colorListM_.p + std::max(neM, 1), tm, tm + maxGrid, tm + maxGrid + kColorTail};
+              colorListM_.p + std::max(neM, 1), tm, tm + maxGrid, tm + maxGrid + kColorTailMax, std::min(colorTailAt_, kColorTailMax)};
   ColorJob jc{neC, nbC, cColor_.p, winnerP_.p, winnerP2_.p, maskP_.p, colorAux_.p + 6, colorListC_.p,
-              colorListC_.p + std::max(neC, 1), tc, tc + maxGrid, tc + maxGrid + kColorTail};
+              colorListC_.p + std::max(neC, 1), tc, tc + maxGrid, tc + maxGrid + kColorTailMax, std::min(colorTailAt_, kColorTailMax)};
   if (!batch_) {  // the colour orders come out of the same launch (the batched form orders by scene)
     colorHist_.ensure(2 * 64 * (size_t)maxGrid, false, stream_);
     if (neM > 0) {

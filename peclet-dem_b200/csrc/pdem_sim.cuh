@@ -416,6 +416,14 @@ class Sim {
     const int b = e ? (int)std::strtol(e, nullptr, 10) : 1024;
     return (b == 256 || b == 512) ? b : 1024;
   }();
+  // entries left (both colourings) at which block 0 alone finishes the colouring; PDEM_COLOR_TAIL
+  // overrides it (0 .. kColorTailMax). Measured: 1024 and 4096 alike on the 262k-sphere step, 1024
+  // 6 % faster on the batched drums, 16384 and up far slower (one block, many entries a round)
+  int colorTailAt_ = [] {
+    const char* e = std::getenv("PDEM_COLOR_TAIL");
+    const long v = e ? std::strtol(e, nullptr, 10) : 1024;
+    return (int)std::max(0L, std::min(v, 1L << 30));  // capped at kColorTailMax where used
+  }();
   // back-off (ns) between polls of a waiting block at a grid barrier; PDEM_BARRIER_SLEEP_NS
   // overrides it
   unsigned barrierSleepNs_ = [] {
