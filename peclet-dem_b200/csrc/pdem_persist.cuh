@@ -233,6 +233,7 @@ struct ColorJob {
   int* blockCount;     // [gridDim] the blocks' list lengths, published for the tail
   int *tailA, *tailB;  // [kColorTailMax] each: the tail's worklists (block 0 alone)
   int tailAt;          // block 0 takes over once at most this many entries (both graphs) are left
+  int tailShared;      // the launch has the shared-memory tail's tables (dynamic shared memory)
   // stable order by colour, built in the same launch when order is set: order[ne] (entry indices,
   // colour-major, index order within a colour), off[65] (first position of each colour key, then
   // ne), hist[64 * gridDim] (scratch)
@@ -575,6 +576,136 @@ __device__ void colorTail(const Dev<R>& d, const ColorJob& jm, const ColorJob& j
   }
 }
 
+// The tail in shared memory (block 0 alone, at most kTailShEntries entries of both graphs): every
+// body the remaining entries touch gets a slot of a hash table (code body * 2 + graph), holding its
+// winner word and colour mask, so a round touches no global memory but the final colours. The
+// rounds, winners and colours are those of colorTail: contend (max of the keys at both ends), win
+// with the maximum at both ends, take the lowest colour free at both ends; the losers contend
+// again. One winner word per slot suffices: after each commit the words of every end touched that
+// round go back to -1, and the next round's contenders are that round's losers.
+constexpr int kTailShEntries = 1024;
+constexpr int kTailShSlots = 4096;  // a power of two, at least 2 ends x entries x 2
+struct TailShared {
+  u64 mask[kTailShSlots];
+  long long win[kTailShSlots];
+  long long key[kTailShEntries];
+  int body[kTailShSlots];  // code of the slot's body, -1 free
+  int ent[kTailShEntries];
+  short la[kTailShEntries], lb[kTailShEntries];  // slots of the ends (lb -1: no second body)
+  short list[2][kTailShEntries];                 // entries of this round and the next
+  unsigned char g[kTailShEntries];               // 0 manifold graph, 1 contact graph
+};
+__device__ __forceinline__ int tailSlot(TailShared& S, int code) {
+  const unsigned h = (unsigned)code * 2654435761u;
+  for (int probe = 0; probe < kTailShSlots; ++probe) {  // at most 2 x kTailShEntries codes: a slot is free
+    const int s = (int)((h + (unsigned)probe) & (kTailShSlots - 1));
+    const int prev = atomicCAS(&S.body[s], -1, code);
+    if (prev == -1 || prev == code)
+      return s;
+  }
+  return 0;
+}
+template <class R, bool MANIFOLD>
+__device__ __forceinline__ void tailEntry(const Dev<R>& d, TailShared& S, int t, int i, int g) {
+  int ea, eb;
+  colorEnds<R, MANIFOLD>(d, i, ea, eb);
+  S.ent[t] = i;
+  S.g[t] = (unsigned char)g;
+  S.key[t] = entryKey<R, MANIFOLD>(d, i, ea);
+  S.la[t] = (short)tailSlot(S, 2 * ea + g);
+  S.lb[t] = (short)(eb >= 0 ? tailSlot(S, 2 * eb + g) : -1);
+  S.list[0][t] = (short)t;
+}
+template <class R>
+__device__ void colorTailShared(const Dev<R>& d, const ColorJob& jm, const ColorJob& jc, int round, int maxRounds,
+                                bool doneM, bool doneC, int prevM, int prevC) {
+  extern __shared__ __align__(16) unsigned char tailSmem[];
+  TailShared& S = *reinterpret_cast<TailShared*>(tailSmem);
+  __shared__ int sLose[2], sNext;
+  const int nM = doneM ? 0 : colorTailGather<R, true>(jm, round, jm.tailA);
+  const int nC = doneC ? 0 : colorTailGather<R, false>(jc, round, jc.tailA);
+  for (int s = threadIdx.x; s < kTailShSlots; s += blockDim.x)
+    S.body[s] = -1;
+  __syncthreads();
+  for (int t = threadIdx.x; t < nM + nC; t += blockDim.x) {
+    if (t < nM)
+      tailEntry<R, true>(d, S, t, jm.tailA[t], 0);
+    else
+      tailEntry<R, false>(d, S, t, jc.tailA[t - nM], 1);
+  }
+  __syncthreads();
+  for (int s = threadIdx.x; s < kTailShSlots; s += blockDim.x) {
+    const int code = S.body[s];
+    if (code >= 0)
+      S.mask[s] = __ldcg(&((code & 1) ? jc.mask : jm.mask)[code >> 1]);
+    S.win[s] = -1;
+  }
+  int cnt = nM + nC;
+  for (int k = 0; round < maxRounds && !(doneM && doneC); ++round, ++k) {
+    const short* in = S.list[k & 1];
+    short* out = S.list[(k + 1) & 1];
+    if (threadIdx.x == 0)
+      sLose[0] = sLose[1] = sNext = 0;
+    __syncthreads();  // the slots' words and masks, and the counters, are set
+    for (int j = threadIdx.x; j < cnt; j += blockDim.x) {
+      const int t = in[j];
+      if (S.g[t] ? doneC : doneM)
+        continue;
+      atomicMax(&S.win[S.la[t]], S.key[t]);
+      if (S.lb[t] >= 0)
+        atomicMax(&S.win[S.lb[t]], S.key[t]);
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < cnt; j += blockDim.x) {
+      const int t = in[j];
+      const int g = S.g[t];
+      if (g ? doneC : doneM)
+        continue;
+      const int la = S.la[t], lb = S.lb[t];
+      const long long key = S.key[t];
+      if (S.win[la] != key || (lb >= 0 && S.win[lb] != key)) {
+        out[atomicAdd(&sNext, 1)] = (short)t;
+        atomicAdd(&sLose[g], 1);
+        continue;
+      }
+      const u64 forb = S.mask[la] | (lb >= 0 ? S.mask[lb] : 0ull);
+      int cc = 0;
+      while (cc < 62 && (forb & (1ull << cc)))
+        ++cc;
+      (g ? jc : jm).col[S.ent[t]] = cc;
+      S.mask[la] |= 1ull << cc;  // the round's winners share no end
+      if (lb >= 0)
+        S.mask[lb] |= 1ull << cc;
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < cnt; j += blockDim.x) {
+      const int t = in[j];
+      if (S.g[t] ? doneC : doneM)
+        continue;
+      S.win[S.la[t]] = -1;
+      if (S.lb[t] >= 0)
+        S.win[S.lb[t]] = -1;
+    }
+    const int remM = sLose[0], remC = sLose[1];
+    cnt = sNext;
+    if (threadIdx.x == 0) {
+      if (!doneM)
+        jm.aux[round % 3] = remM;
+      if (!doneC)
+        jc.aux[round % 3] = remC;
+    }
+    if (!doneM) {
+      doneM = remM == 0 || remM == prevM;
+      prevM = remM;
+    }
+    if (!doneC) {
+      doneC = remC == 0 || remC == prevC;
+      prevC = remC;
+    }
+    __syncthreads();  // the counters are read before the next round resets them
+  }
+}
+
 // job 0: manifolds over real bodies (skipped when ne = 0), job 1: contacts over body slots
 // reuse: a graph equal to the previous substep's keeps its colours and statistics (differ[0]: the
 // contact list changed, differ[1]: the manifold list changed; reuse = 0 forces both colourings)
@@ -647,8 +778,12 @@ __global__ void __launch_bounds__(kColorBlock) kColorBoth(Dev<R> d, ColorJob jm,
   if (tail) {
     if (!gridBarrier(gb))  // the published lists are complete
       return;
-    if (blockIdx.x == 0)
-      colorTail(d, jm, jc, round, maxRounds, doneM, doneC, prevM, prevC);
+    if (blockIdx.x == 0) {
+      if (jm.tailShared)
+        colorTailShared(d, jm, jc, round, maxRounds, doneM, doneC, prevM, prevC);
+      else
+        colorTail(d, jm, jc, round, maxRounds, doneM, doneC, prevM, prevC);
+    }
     if (!gridBarrier(gb))  // the tail's colours are visible to every block
       return;
   }

@@ -267,6 +267,27 @@ void Sim<R>::launchCoop(K kernel, A... args) {
 }
 template <class R>
 template <class K, class... A>
+void Sim<R>::launchCoopSmem(K kernel, int block, size_t smem, A... args) {
+  const auto key = std::make_pair(reinterpret_cast<const void*>(kernel), smem);
+  auto it = coopPerSmem_.find(key);
+  if (it == coopPerSmem_.end()) {
+    cudaCheck(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem attribute");
+    int per = 0;
+    cudaCheck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, block, smem), "occupancy");
+    if (per < 1)
+      throw CudaError("persistent loop kernel cannot be resident");
+    it = coopPerSmem_.emplace(key, per).first;
+  }
+  gbar_.ensure(2, false, stream_);
+  cudaCheck(cudaMemsetAsync(gbar_.p, 0, 2 * sizeof(unsigned), stream_), "memset barrier");
+  void* argv[] = {static_cast<void*>(&args)...};
+  ++launches_;
+  cudaCheck(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(kernel), dim3(std::min(it->second, 4) * numSMs_),
+                                        dim3(block), argv, smem, stream_),
+            "cooperative launch");
+}
+template <class R>
+template <class K, class... A>
 bool Sim<R>::launchCluster(K kernel, A... args) {
   cudaLaunchConfig_t cfg{};
   cfg.gridDim = dim3(kSweepCluster);
@@ -1293,8 +1314,11 @@ void Sim<R>::colorBoth(int nm, int nc, int& ncolV, int& velLeft, int& ncolP, int
   }
   gbar_.ensure(2, false, stream_);
   const GridBar gb{gbar_.p, &ctr_.p->err, barrierSleepNs_};
-  launchCoopB(kColorBoth<R>, colorBlock_, d_, jm, jc, std::max(nbM, nbC) + 2, gb, (const int*)topoFlags_.p,
-              topoValid_ ? 1 : 0);
+  // the tail in shared memory when the hand-over fits its tables
+  const bool tailShared = std::min(colorTailAt_, kColorTailMax) <= kTailShEntries;
+  jm.tailShared = jc.tailShared = tailShared ? 1 : 0;
+  launchCoopSmem(kColorBoth<R>, colorBlock_, tailShared ? sizeof(TailShared) : 0, d_, jm, jc, std::max(nbM, nbC) + 2,
+                 gb, (const int*)topoFlags_.p, topoValid_ ? 1 : 0);
   KCHECK("colour loop");
   int res[12], err = 0, differ[2] = {1, 1};
   readBack(res, colorAux_.p, sizeof res);

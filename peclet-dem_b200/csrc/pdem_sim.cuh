@@ -371,6 +371,10 @@ class Sim {
   void launchCoopB(K kernel, int block, A... args);
   template <class K, class... A>
   void launchCoop(K kernel, A... args);
+  // cooperative launch with `smem` bytes of dynamic shared memory (resident blocks counted with it)
+  template <class K, class... A>
+  void launchCoopSmem(K kernel, int block, size_t smem, A... args);
+  std::map<std::pair<const void*, size_t>, int> coopPerSmem_;
   // one thread-block cluster of kSweepCluster blocks; false when such a cluster cannot be resident
   template <class K, class... A>
   bool launchCluster(K kernel, A... args);
