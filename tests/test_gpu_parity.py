@@ -138,3 +138,21 @@ def test_shell_plane_reach_cull(gpu_api, orc_api, precision, rtol):
     contacts, overlaps and state identical to the oracle's full probing."""
     import scenes as S
     _run_pair(gpu_api, orc_api, "shells_at_floor", S.shells_at_floor, None, 4, precision, rtol)
+
+
+@pytest.mark.parametrize("tail", ["0", "4096"])
+def test_colouring_tail_settings(tail):
+    """The colouring's hand-over to one block is a launch-shape setting: with no tail (0) and with
+    the global-memory tail (4096, beyond the shared-memory tables) scenes of every kind stay
+    bit-exact against the oracle (the default, the shared-memory tail, runs in every test above)."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sel = ("test_fp32_bitexact_vs_oracle and (periodic_polydisperse or dense_spheres or drum_sdf_wall "
+           "or hollow_cylinders or settled_column)")
+    r = subprocess.run([sys.executable, "-m", "pytest", "-q", "-m", "gpu", "-k", sel,
+                        os.path.join(root, "tests", "test_gpu_parity.py")],
+                       cwd=root, env={**os.environ, "PDEM_COLOR_TAIL": tail}, capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    assert "5 passed" in r.stdout, r.stdout[-500:]
