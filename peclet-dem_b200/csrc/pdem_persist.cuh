@@ -239,8 +239,9 @@ struct ColorJob {
   // ne), hist[64 * gridDim] (scratch)
   int *order = nullptr, *off = nullptr, *hist = nullptr;
 };
-// once at most this many entries (both colourings together) are left, block 0 alone runs the
-// remaining rounds with block barriers, and the other blocks wait at one grid barrier
+// once at most ColorJob::tailAt entries (both colourings together) are left, block 0 alone runs the
+// remaining rounds with block barriers (in shared memory when they fit its tables), and the other
+// blocks wait at one grid barrier
 constexpr int kColorMaxChunks = 20;    // histogram row chunks of 32 blocks (grids up to 640 blocks)
 constexpr int kColorTailMax = 65536;  // largest tail hand-over the worklists are sized for
 
