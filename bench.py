@@ -1,30 +1,38 @@
 """Benchmark: particle-substeps/s of the plain FP64 XPBD substep on one B200.
 
-Workload (seeded synthetic, no dataset): 262,144 polydisperse spheres, radii lognormal (median
-1 mm, sigma 0.25, clipped to [0.5, 2] mm), placed without overlap by random sequential addition in a
-box periodic in x and y (L_x = L_y, height 2 L_x, solids fraction 0.35) with a floor plane at z = 0;
-density 2500 kg/m^3, e = 0.6, mu = 0.4, gravity -9.81 m/s^2, dt = 2e-5 s split into 10 substeps
-(one `step(2e-6)` call = one substep), 10 position and 10 velocity iterations. One benchmark step
-= one outer step = 10 substeps. Metric = N x substeps / second.
+Headline workload: the plain XPBD settling configuration, 4,096 monodisperse spheres (r 1 mm,
+density 2500 kg/m^3, jittered simple-cubic lattice at the bottom of a closed 16 x 16 x 64-cell box
+of six planes, e 0.5, mu 0.5, gravity -9.81 m/s^2, 10 position and 10 velocity iterations,
+10 substeps of 1e-5 s per outer step, 1,000 outer steps from the lattice start). Both arms restart
+from the saved state after 800 of those steps (peclet/dem/states/plain_settling_4096_step800.npz,
+made by the FP64 step: the bed is at rest in dense contact, which is where the solve loops run
+their full sweeps), run `--warmup` untimed outer steps and then time `--steps` outer steps. One
+benchmark step = one outer step = 10 `step(1e-5)` calls. Metric = N x substeps / second.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--extras LIST]
 
-`value` is device time (two CUDA events on the library's stream around all timed substeps, idle
-gaps included; a second pass with per-stage events gives the stage breakdown) with the state
-resident in HBM; `e2e` runs the same loop through the public API with host buffers
-(external forces copied in, positions and velocities copied out every outer step) timed by the
-host clock. `--impl reference` times the reference's own code (its headers built against the
-OpenMP flavour of the Kokkos shim) on this machine's host cores. More than one GPU runs replicas
-(the single-scene step has no shard-parallel decomposition).
+`value`: device time of the K timed outer steps (CUDA events on the library's stream around each
+step, summed; L2 flushed between steps by a 256 MiB write, since the 4,096-sphere state fits in
+L2). `e2e`: the same window through the public API from the same state, with the external forces
+copied in from pinned host memory and positions and velocities copied out every outer step, timed
+by the host clock. `--impl reference` times the reference's own code for the path (its headers
+built unmodified against the OpenMP flavour of the Kokkos shim, oracle/_ref) on the same state,
+the same warm-up and the same timed outer steps, with every host thread; it loads no library of
+this repository. More than one GPU runs replicas of the single scene (it does not shard); the
+batched drums and calibration scenes are split over the ranks.
 
-The `batched` object of the line measures the batched form on 512 rotating drums
-(`workloads.rotating_drums`, about 1.9 M bodies, one simulation per GPU; scenes split over the
-ranks) in FP64 and in the FP32-mixed form, with the mixed form's position error against the FP64
-run after the same substeps. `--drums 0` skips it.
+Besides the headline, rank 0 prints a detail line first (no "metric" key) with the other
+configurations (`--extras`, default all): `xpbd262k` (262,144 polydisperse spheres in a box
+periodic in x and y, through the XPBD step: not a configuration the reference names for this
+step), `batched` (512 rotating drums after their deposition, FP64 and FP32-mixed), `calibration`
+(forward and forward + adjoint of the Hertz rollout), `hertz` (262,144 polydisperse spheres,
+closed variant) and `shells` (65,536 hollow cylinders with 512-point shells after a gravity
+deposition). The main line, printed last, carries flat keys with their headline figures.
 """
 from __future__ import annotations
 
 import argparse
+import importlib.util
 import json
 import os
 import statistics
@@ -34,27 +42,67 @@ import tempfile
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
-sys.path.insert(0, os.path.join(ROOT, "peclet-dem_b200"))
+PKG_DIR = os.path.join(ROOT, "peclet-dem_b200")
+DEM_DIR = os.path.join(PKG_DIR, "peclet", "dem")
+sys.path.insert(0, PKG_DIR)
 
 import numpy as np  # noqa: E402
 
 METRIC = "particle-substeps/s"
 SUBSTEPS = 10
-REF_OMP = os.path.join(ROOT, "oracle", "_ref", "libref_omp.so")
+REF_OMP = os.path.join(ROOT, "oracle", "_ref", "libref_omp.so")         # -march=x86-64-v4
+REF_OMP_V2 = os.path.join(ROOT, "oracle", "_ref", "libref_omp_v2.so")   # -march=x86-64-v2 fallback
 REF_SERIAL = os.path.join(ROOT, "oracle", "_ref", "libref_serial.so")
+EXTRAS = ("xpbd262k", "batched", "calibration", "hertz", "shells")
+L2_FLUSH_BYTES = 256 << 20
 
 
-def workload_desc(n):
-    return {"workload": f"polydisperse_{n}_periodic_xy_floor_xpbd",
-            "particles": n, "substeps_per_step": SUBSTEPS, "dt_substep": 2e-6,
-            "radii": "lognormal median 1 mm sigma 0.25 clipped [0.5,2] mm", "solids_fraction": 0.35,
-            "iterations": {"position": 10, "velocity": 10}, "precision": "fp64",
-            "l2": "state larger than L2 (no flush needed)"}
+def _file_module(name, path):
+    """A module loaded from its file alone: no package __init__ runs (the reference arm must not
+    load libpdem.so, which importing the peclet.dem package does)."""
+    spec = importlib.util.spec_from_file_location(name, path)
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
 
 
-def make_scene(n):
-    from peclet.dem import workloads as W
-    return W.polydisperse(n=n)
+def workloads_module():
+    return _file_module("pdem_bench_workloads", os.path.join(DEM_DIR, "workloads.py"))
+
+
+def capi_module():
+    return _file_module("pdem_bench_capi", os.path.join(DEM_DIR, "_capi.py"))
+
+
+def _cpu_flags():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("flags"):
+                    return set(line.split(":", 1)[1].split())
+    except OSError:
+        pass
+    return set()
+
+
+def ref_omp_lib():
+    """The OpenMP reference build for this host: the AVX-512 (x86-64-v4) build when the CPU has
+    it, else the x86-64-v2 one. Returns (path, march) or (None, None)."""
+    if os.path.exists(REF_OMP) and {"avx512f", "avx512bw", "avx512dq", "avx512vl"} <= _cpu_flags():
+        return REF_OMP, "x86-64-v4"
+    if os.path.exists(REF_OMP_V2):
+        return REF_OMP_V2, "x86-64-v2"
+    return None, None
+
+
+def headline_desc(world=1):
+    return {"workload": "plain_settling_4096_fp64", "particles": 4096, "substeps_per_step": SUBSTEPS,
+            "dt_substep": 1e-5, "iterations": {"position": 10, "velocity": 10},
+            "state": "saved state after 800 of the configuration's 1000 outer steps (FP64 B200 step from the "
+                     "lattice start); both arms restart from it; warm-start ledger cold at the restart",
+            "l2": "flushed between timed steps (256 MiB write); the state (~4 MB) fits in L2",
+            "parallelism": f"replicas x{world}" if world > 1 else "single"}
 
 
 # ---------------------------------------------------------------------------------------------
@@ -103,21 +151,28 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------------------------
-# algorithmic bytes of one substep (FP64: D = 8 bytes per real) — byte model of the substep:
-# particles 81 D N, pairs 16 P, contacts 2 C (8 + 16 D), manifolds M (12 + 20 D), colouring
-# 12 (M + C), ledger M (16 + 8 D), velocity sweeps I_v M (12 + 20 D + 53 D), position sweeps
-# I_p C (8 + 48 D)
-def substep_bytes(n, P, C, M, iv, ip, D=8):
+# algorithmic bytes of one substep (D bytes per real: 8 at FP64): particles 81 D N, pairs 16 P,
+# contacts 2 C (8 + 16 D), manifolds M (12 + 20 D), colouring 12 (M + C), ledger M (16 + 8 D),
+# velocity sweeps I_v M (12 + 20 D + 53 D), stabilization sweeps I_s M (the same per sweep),
+# position sweeps I_p C (8 + 48 D)
+def substep_bytes(n, P, C, M, iv, ip, D=8, istab=0.0):
     Sm = 12 + 20 * D
     return (81 * D * n + 16 * P + 2 * C * (8 + 16 * D) + M * Sm + 12 * (M + C) + M * (16 + 8 * D)
-            + iv * M * (Sm + 53 * D) + ip * C * (8 + 48 * D))
+            + (iv + istab) * M * (Sm + 53 * D) + ip * C * (8 + 48 * D))
 
 
-# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum summed over a stage's kernels in one
-# ncu capture of one substep) at the default workload of 262,144 spheres, in bytes per substep;
-# stages and sizes not captured report none. The colouring stage covers both colourings with both
-# colour orders (one launch) and the manifold incidence lists.
-STAGE_DRAM_BYTES = {(262144, "colour_velocity"): 23.0e6}
+def stage_bytes(n, P, C, M, iv, istab, ip, D=8):
+    """Algorithmic bytes of one substep per stage (the terms of substep_bytes)."""
+    Sm = 12 + 20 * D
+    return {"velocity": iv * M * (Sm + 53 * D), "stabilization": istab * M * (Sm + 53 * D),
+            "position": ip * C * (8 + 48 * D), "broadphase": n * 4 * D + 8 * P,
+            "narrowphase": 8 * P + C * (8 + 16 * D), "manifolds": 2 * C * (8 + 16 * D) + M * Sm,
+            "colour_velocity": 12 * (M + C), "ledger": M * (16 + 8 * D)}
+
+
+# DRAM traffic per substep of a stage from one ncu capture of the same workload (bytes per
+# substep; stages not captured report none)
+STAGE_DRAM_BYTES = {("plain_settling_4096_fp64", "stabilization"): None}
 
 
 def measured_peaks():
@@ -156,12 +211,227 @@ def split_scenes(sizes, world):
     return [[s for s in range(len(sizes)) if owner[s] == r] for r in range(world)]
 
 
-def run_batched(args, rank, world, dist, dem):
-    """Batched rotating drums (512 scenes) in one simulation per GPU, in FP64 and in the FP32-mixed
-    form; scenes are split over the ranks with no exchange while stepping. The mixed form's error
-    is its largest position difference from the FP64 run after the same substeps, in radii.
-    Returns the sub-object of the JSON line."""
-    from peclet.dem import workloads as W
+def rank_range(n_items, rank, world):
+    """Contiguous share [lo, hi) of n_items for rank (the calibration scenes)."""
+    return (n_items * rank) // world, (n_items * (rank + 1)) // world
+
+
+class L2Flush:
+    """Writes a buffer larger than L2 (126 MB) on the current stream and waits for it."""
+
+    def __init__(self):
+        import torch
+        self.torch = torch
+        self.buf = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+
+    def __call__(self):
+        self.buf.fill_(1.0)
+        self.torch.cuda.synchronize()
+
+
+# ---------------------------------------------------------------------------------------------
+# headline: the plain XPBD settling configuration from its saved state
+def outer_step(sim, sc):
+    for _ in range(sc.substeps):
+        sim.step(sc.dt)
+
+
+def run_headline(args, rank, world, dist, dem, W):
+    import torch
+    sc = W.plain_settled()
+    n = sc.n
+    flush = L2Flush()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    sim = sc.apply(dem.Simulation(n + 8, "fp64"))
+    for _ in range(args.warmup):
+        outer_step(sim, sc)
+    sim.get_positions()  # synchronise
+    clocks = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    allocs = dem._API.fn["debug_allocs"]
+    with clocks:
+        time.sleep(0.5)  # sampler running before the timed region starts
+        barrier()
+        a0 = allocs()
+        dev_ms = 0.0
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            flush()
+            sim.timer_start()  # events on the library's stream around each timed outer step
+            outer_step(sim, sc)
+            dev_ms += sim.timer_stop()
+        wall = time.perf_counter() - t0
+        timed_allocs = allocs() - a0
+    barrier()
+    t_max = max_over_ranks(dev_ms / 1e3, dist, "cuda")
+    value = aggregate_rate(world, n, SUBSTEPS, args.steps, t_max)
+    # the same number of steps again with per-stage events (their synchronisation slows the step;
+    # these explain the timed value, they are not it)
+    sim.profile_enable(True)
+    for _ in range(args.steps):
+        outer_step(sim, sc)
+    stages, launches = sim.profile_read()
+    sweeps = sim.debug_sweeps()
+    counts = sim.debug_counts()
+    last = sim.counters()
+    sim.profile_enable(False)
+    x_end = sim.get_positions()
+    v_end = sim.get_velocities()
+    w_end = sim.get_angular_velocities()
+    sim.close()
+
+    # ---- end to end through the public API with host buffers, from the same state ----
+    pinned = lambda: torch.zeros((n, 3), dtype=torch.float64, pin_memory=True).numpy()
+    force, pos, vel = pinned(), pinned(), pinned()
+    sim = sc.apply(dem.Simulation(n + 8, "fp64"))
+    for _ in range(args.warmup):
+        outer_step(sim, sc)
+    sim.get_positions()
+    barrier()
+    a1 = allocs()
+    laps = []
+    for _ in range(args.steps):
+        flush()
+        tl = time.perf_counter()
+        sim.set_external_forces(force)
+        outer_step(sim, sc)
+        sim.get_positions(out=pos)
+        sim.get_velocities(out=vel)
+        laps.append(time.perf_counter() - tl)
+    e2e_allocs = allocs() - a1
+    sim.close()
+    assert np.all(np.isfinite(pos)) and np.all(np.isfinite(vel))
+    e2e_t = max_over_ranks(sum(laps), dist, "cuda")
+    e2e = {"value": aggregate_rate(world, n, SUBSTEPS, args.steps, e2e_t), "unit": METRIC,
+           "h2d_bytes_per_step": int(force.nbytes), "d2h_bytes_per_step": int(pos.nbytes + vel.nbytes),
+           "ms_per_step_median": round(1e3 * statistics.median(laps), 3), "device_allocations": int(e2e_allocs)}
+
+    # ---- roofline of the dominant stage (per substep: one launch of the sweep loop) ----
+    subs = args.steps * SUBSTEPS
+    per_sub = {k: ms / subs for k, (ms, c) in stages.items() if c}
+    P, C, M = counts["pairs"], counts["contacts"], counts["manifolds"]
+    iv, istab, ip = sweeps["velocity"] / subs, sweeps["stabilization"] / subs, sweeps["position"] / subs
+    sb = stage_bytes(n, P, C, M, iv, istab, ip)
+    peak, peak_kind = measured_peaks()
+    roof_stage = max((k for k in per_sub if k in sb), key=lambda k: per_sub[k])
+    st_ms = per_sub[roof_stage]
+    achieved = sb[roof_stage] / (st_ms / 1e3) / 1e9 if st_ms > 0 else 0.0
+    step_bytes = substep_bytes(n, P, C, M, iv, ip, istab=istab)
+    roofline = {"bound": "hbm", "kernel": f"{roof_stage} stage, per substep", "achieved": achieved, "peak": peak,
+                "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                "traffic": STAGE_DRAM_BYTES.get(("plain_settling_4096_fp64", roof_stage)),
+                "algorithmic_bytes": sb[roof_stage], "stage_ms": st_ms,
+                "l2_resident": "working set ~4 MB in the 126 MB L2: latency-bound (sweep loop barriers and "
+                               "dependent loads), the HBM fraction is context",
+                "step_algorithmic_GBps": step_bytes * subs / (dev_ms / 1e3) / 1e9}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        lib, march = ref_omp_lib()
+        if lib:
+            threads = os.cpu_count() or 1
+            v, el, _ = cpu_reference_steps(sc, lib, threads, 3, args.cpu_steps)
+            cpu = {"value": v, "unit": METRIC, "cores": threads, "kind": "reference",
+                   "sample": f"{args.cpu_steps} outer steps (x10 substeps) of the same restart after 3 warm-up steps, "
+                             f"{el:.1f} s; reference headers on the OpenMP Kokkos shim, float, -O3 -march={march}"}
+    from peclet.dem import stats as S
+    pk = S.packing_stats(x_end, np.full(n, sc.global_scale), 1.0 / sc.inv_mass, v_end, w_end,
+                         1.0 / sc.inv_inertia[:, 0], sc.domain[0], sc.domain[1])
+    return {"value": value, "t_max": t_max, "dev_ms": dev_ms, "wall": wall, "e2e": e2e, "roofline": roofline,
+            "cpu": cpu, "clocks": clocks.summary(), "launches": launches, "timed_allocs": int(timed_allocs),
+            "stages_ms_per_substep": {k: round(v, 4) for k, v in per_sub.items()},
+            "sweeps_per_substep": {"velocity": iv, "stabilization": istab, "position": ip},
+            "counts_last_substep": {"pairs": P, "contacts": C, "manifolds": M,
+                                    "colours": [last["colors_velocity"], last["colors_position"]]},
+            "packing_at_end": pk}
+
+
+# ---------------------------------------------------------------------------------------------
+def cpu_reference_steps(scene, lib, threads, warm, steps):
+    """The reference's own substep (a build under oracle/_ref) on `scene` for `warm` untimed and
+    `steps` timed outer steps of scene.substeps calls; returns (particle-substeps/s, seconds,
+    per-step seconds). The reference computes in float; the state is set as on the GPU."""
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    os.environ.setdefault("OMP_PROC_BIND", "close")
+    capi = capi_module()
+    sim = scene.apply(capi.CApiSimulation(capi.CApi(lib, "ref"), scene.n + 8, "fp32"))
+    for _ in range(warm):
+        outer_step(sim, scene)
+    laps = []
+    for _ in range(steps):
+        t = time.perf_counter()
+        outer_step(sim, scene)
+        laps.append(time.perf_counter() - t)
+    sim.close()
+    el = sum(laps)
+    return scene.n * scene.substeps * steps / el, el, laps
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    lib, march = ref_omp_lib()
+    if lib is None:
+        print(json.dumps({"impl": "reference", "unavailable": "reference build oracle/_ref/libref_omp*.so missing"}))
+        return 0
+    threads = os.cpu_count() or 1
+    W = workloads_module()
+    sc = W.plain_settled()
+    value, el, laps = cpu_reference_steps(sc, lib, threads, args.warmup, args.steps)
+    cfg = headline_desc(1)
+    cfg["precision"] = "fp32 (the reference computes in float)"
+    cfg["l2"] = "host run"
+    cfg["parallelism"] = f"OpenMP, {threads} threads"
+    print(json.dumps({
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded), saved restart state",
+        "config": cfg, "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": METRIC, "cores": threads, "kind": "reference",
+                         "sample": f"{args.steps} outer steps (x10 substeps) of the 4096-sphere restart after "
+                                   f"{args.warmup} warm-up steps; reference headers on the OpenMP Kokkos shim, "
+                                   f"-O3 -march={march}, {threads} threads"},
+        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+    return 0
+
+
+# ---------------------------------------------------------------------------------------------
+# extras
+def run_xpbd262k(args, rank, world, dist, dem, W):
+    """262,144 polydisperse spheres (lognormal radii, median 1 mm, sigma 0.25, clipped [0.5, 2] mm)
+    placed by random sequential addition at solids fraction 0.35 in a box periodic in x and y with
+    a floor, through the XPBD step (FP64, 10 substeps of 2e-6 s), timed after 100 untimed outer
+    steps. This particle set is the Hertz configuration's; the reference names no XPBD
+    configuration on it, so this line has no reference arm."""
+    sc = W.polydisperse(n=262144)
+    sim = sc.apply(dem.Simulation(sc.n + 8, "fp64"))
+    for _ in range(100):
+        outer_step(sim, sc)
+    steps = args.extra_steps
+    if dist is not None:
+        dist.barrier()
+    sim.timer_start()
+    for _ in range(steps):
+        outer_step(sim, sc)
+    t = max_over_ranks(sim.timer_stop() / 1e3, dist, "cuda")
+    c = sim.counters()
+    sim.close()
+    return {"workload": f"polydisperse_{sc.n}_periodic_xy_floor_xpbd_fp64", "value": aggregate_rate(world, sc.n, 10, steps, t),
+            "ms_per_step": 1e3 * t / steps, "timed_steps_from": 100, "steps": steps,
+            "last_substep": {k: c[k] for k in ("contacts", "manifolds", "velocity_sweeps", "position_sweeps")}}
+
+
+def run_batched(args, rank, world, dist, dem, W):
+    """Batched rotating drums (512 scenes) in one simulation per GPU, after their deposition: the
+    drums are filled by random sequential addition in their lower halves and stepped
+    `--drum-presettle` untimed outer steps in FP64 (the grains fall into a bed and the drums turn);
+    that state is the start of an FP64 and an FP32-mixed run of the same warm-up and timed steps.
+    The mixed form's error is its largest position difference from the FP64 run at the end, in
+    radii. Scenes are split over the ranks with no exchange while stepping."""
     from peclet.dem.batch import apply_batch
     scenes, extras = W.rotating_drums(scenes=args.drums)
     mine = split_scenes([sc.n for sc in scenes], world)[rank]
@@ -170,6 +440,17 @@ def run_batched(args, rank, world, dist, dem):
     n_mine = sum(sc.n for sc in sc_m)
     radius = np.concatenate([sc.scales * sc.global_scale for sc in sc_m])
     dt = sc_m[0].dt
+    # deposition: one FP64 run from the RSA fill; its end state starts both timed runs
+    sim = dem.Simulation(n_mine + 8, "fp64")
+    first = apply_batch(sim, sc_m, [extras[s] for s in mine])
+    for _ in range(args.drum_presettle * SUBSTEPS):
+        sim.step(dt)
+    x0, v0, q0, w0 = sim.get_positions(), sim.get_velocities(), sim.get_quaternions(), sim.get_angular_velocities()
+    sim.close()
+    t_dep = args.drum_presettle * SUBSTEPS * dt
+    for k, s in enumerate(mine):  # restart each scene from its deposited state, walls turned on
+        sl = slice(int(first[k]), int(first[k + 1]))
+        sc_m[k].pos, sc_m[k].vel, sc_m[k].quat, sc_m[k].angvel = x0[sl], v0[sl], q0[sl], w0[sl]
 
     def one(precision):
         sim = dem.Simulation(n_mine + 8, precision)
@@ -183,32 +464,27 @@ def run_batched(args, rank, world, dist, dem):
             sim.step(dt)
         t = max_over_ranks(sim.timer_stop() / 1e3, dist, "cuda")
         sweeps = sim.scene_counters()
-        tune = sim.scene_block()  # settled during the warm-up substeps
-        x = sim.get_positions()  # the error is measured at the end of the timed substeps
-        sim.profile_enable(True)
-        for _ in range(args.steps * SUBSTEPS):
-            sim.step(dt)
-        stages, launches = sim.profile_read()
-        sim.profile_enable(False)
+        tune = sim.scene_block()
+        x = sim.get_positions()
         sim.close()
-        per_step = {k: round(ms / args.steps, 3) for k, (ms, c) in stages.items() if c}
-        return t, per_step, launches, sweeps, x, tune
+        return t, sweeps, x, tune
 
-    t64, st64, l64, sw64, x64, tu64 = one("fp64")
-    tmx, stmx, lmx, _, xmx, tumx = one("mixed")
+    t64, sw64, x64, tu64 = one("fp64")
+    tmx, swmx, xmx, tumx = one("mixed")
     err = np.linalg.norm(xmx - x64, axis=1) / radius
     err_max = max_over_ranks(float(err.max()) if err.size else 0.0, dist, "cuda")
     rate = lambda t: n_all * SUBSTEPS * args.steps / t
-    return {"workload": f"rotating_drums_{len(scenes)}_scenes", "scenes": len(scenes), "particles": n_all,
-            "unit": METRIC, "scaling": "weak (scenes split over ranks)",
-            "fp64": {"value": rate(t64), "ms_per_step": 1e3 * t64 / args.steps, "gpu_launches": l64,
-                     "stages_ms_per_step": st64, "err_vs_fp64": 0.0, "autotuned_scene_block": tu64},
-            "mixed": {"value": rate(tmx), "ms_per_step": 1e3 * tmx / args.steps, "gpu_launches": lmx,
-                      "stages_ms_per_step": stmx, "autotuned_scene_block": tumx,
+    return {"workload": f"rotating_drums_{len(scenes)}_scenes_after_deposition", "scenes": len(scenes),
+            "particles": n_all, "deposition_s": t_dep, "presettle_steps": args.drum_presettle,
+            "fp64": {"value": rate(t64), "ms_per_step": 1e3 * t64 / args.steps, "autotuned_scene_block": tu64,
+                     "mean_sweeps_last_substep": {"velocity": float(sw64[:, 2].mean()),
+                                                  "stabilization": float(sw64[:, 3].mean()),
+                                                  "position": float(sw64[:, 4].mean())}},
+            "mixed": {"value": rate(tmx), "ms_per_step": 1e3 * tmx / args.steps, "autotuned_scene_block": tumx,
                       "err_vs_fp64": {"max_position_error_radii": err_max,
                                       "median_position_error_radii": float(np.median(err)) if err.size else 0.0,
                                       "after_substeps": (args.warmup + args.steps) * SUBSTEPS}},
-            "mean_sweeps_last_substep": {"velocity": float(sw64[:, 2].mean()), "position": float(sw64[:, 4].mean())},
+            "mixed_over_fp64": t64 / tmx,
             "config": "R 50 mm, L 20 mm drums, omega U[0.5,3] rad/s, N_s U{256..8192} capped at 30% fill of the "
                       "lower half, radii U[0.8,1.2] mm, mu U[0.2,0.8], e U[0.3,0.9], dt 5e-5 s / 10 substeps"}
 
@@ -220,18 +496,18 @@ def run_calibration(args, rank, world, dist):
     gradients with respect to (E, e, mu) and the initial velocities from the adjoint, at the guess
     (4e6, 0.6, 0.3). Scenes are split over ranks; the three material gradients are summed over
     ranks with one all-reduce per backward pass. Reports forward-only and forward+adjoint rates
-    (device time, max over ranks), their cost ratio, the gradients' relative error against
-    central finite differences (relative steps 1e-4 and 1e-6, FP64) and against the tangent-linear
-    (forward-mode dual-number) run along one direction, and the FP32 gradients' error against
-    FP64. Returns the sub-object of the JSON line."""
+    (device time, max over ranks), their cost ratio, and the gradients' relative error against
+    central finite differences (relative step 1e-4, FP64) on the 64-substep horizon, whose active
+    contact set the check certifies unchanged at +h and -h, and on the full horizon (where contacts
+    begin and end: a stated limitation), against the tangent-linear run, and FP32 against FP64."""
     import torch
     from peclet.dem import workloads as W
     from peclet.dem.adjoint import HertzSpheres
     per = 2048
     c = W.calibration_boxes(scenes=args.calib_scenes)
-    lo, hi = (args.calib_scenes * rank) // world, (args.calib_scenes * (rank + 1)) // world
+    lo, hi = rank_range(args.calib_scenes, rank, world)
     sl = slice(lo * per, hi * per)
-    n_all, n = args.calib_scenes * per, (hi - lo) * per
+    n_all = args.calib_scenes * per
     steps, ck, dt = args.calib_substeps, 100, 2e-5
     hidden, guess = (5e6, 0.7, 0.35), (4e6, 0.6, 0.3)
     dev = torch.device("cuda", torch.cuda.current_device())
@@ -255,14 +531,18 @@ def run_calibration(args, rank, world, dist):
     v0 = torch.as_tensor(c["v0"][sl], device=dev)
     w0 = torch.as_tensor(c["w0"][sl], device=dev)
     s64 = make("fp64")
-    (xt, _, _), _ = s64.run(x0, v0, w0, hidden, steps)  # targets at the hidden parameters
+    (xt, _, _), _ = s64.run(x0, v0, w0, hidden, steps)
+
+    def ranks_sum(x):
+        if dist is None:
+            return float(x)
+        t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+        dist.all_reduce(t)
+        return float(t)
 
     def loss_of(sim, theta, target, nsteps, vv=None):
         (x, _, _), _ = sim.run(x0, v0 if vv is None else vv, w0, tuple(theta), nsteps)
-        part = ((x.double() - target) ** 2).sum()
-        if dist is not None:
-            dist.all_reduce(part)
-        return float(part) / n_all
+        return ranks_sum(((x.double() - target) ** 2).sum()) / n_all
 
     def fwd_adj(sim, target, nsteps):
         th = torch.tensor(guess, dtype=torch.float64, requires_grad=True)
@@ -275,52 +555,27 @@ def run_calibration(args, rank, world, dist):
             dist.all_reduce(g)  # the one exchange step: dL/d(E, e, mu) summed over ranks
         return g.cpu().numpy(), vr.grad.double()
 
-    def ranks_sum(x):
-        if dist is None:
-            return float(x)
-        t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
-        dist.all_reduce(t)
-        return float(t)
-
     rel = lambda a, b: abs(a - b) / abs(b) if b else None
     gen = torch.Generator(device="cpu").manual_seed(5)
     dv = torch.randn(v0.shape, generator=gen, dtype=torch.float64).to(dev)
     dth = np.array([1e5, 0.01, 0.01])
 
     def checks(nsteps, target, g64, gv64, g32, gv32):
-        """Gradients at one horizon against central finite differences of the FP64 forward
-        (relative steps 1e-4 and 1e-6), the directional derivative against the tangent-linear
-        run and FD, and the FP32 gradients against FP64."""
-        fd = {}
-        for rstep in (1e-4, 1e-6):
-            row = []
-            for k in range(3):
-                h = rstep * guess[k]
-                tp, tm = list(guess), list(guess)
-                tp[k] += h
-                tm[k] -= h
-                row.append((loss_of(s64, tp, target, nsteps) - loss_of(s64, tm, target, nsteps)) / (2 * h))
-            fd[rstep] = row
+        fd = []
+        for k in range(3):
+            h = 1e-4 * guess[k]
+            tp, tm = list(guess), list(guess)
+            tp[k] += h
+            tm[k] -= h
+            fd.append((loss_of(s64, tp, target, nsteps) - loss_of(s64, tm, target, nsteps)) / (2 * h))
         got = ranks_sum((gv64 * dv).sum()) + float((g64 * dth).sum())
-        h = 1e-4 * 0.2  # relative step 1e-4 of the largest initial speed component
-        fd_dir = (loss_of(s64, np.array(guess) + h * dth, target, nsteps, v0 + h * dv)
-                  - loss_of(s64, np.array(guess) - h * dth, target, nsteps, v0 - h * dv)) / (2 * h)
-        ((xj, _, _), (xdj, _, _)), t_j = timed(lambda: s64.jvp(x0, v0, w0, guess, torch.zeros_like(x0), dv,
-                                                              torch.zeros_like(w0), dth, nsteps))
+        ((xj, _, _), (xdj, _, _)), _ = timed(lambda: s64.jvp(x0, v0, w0, guess, torch.zeros_like(x0), dv,
+                                                            torch.zeros_like(w0), dth, nsteps))
         jv = ranks_sum((2.0 * (xj - target) * xdj).sum()) / n_all
-        return {"substeps": nsteps,
-                "grad_fp64": {"E": float(g64[0]), "e": float(g64[1]), "mu": float(g64[2])},
-                "fd_fp64": {str(r): {"E": v[0], "e": v[1], "mu": v[2]} for r, v in fd.items()},
-                "rel_err_vs_fd": {str(r): {"E": rel(g64[0], v[0]), "e": rel(g64[1], v[1]), "mu": rel(g64[2], v[2])}
-                                  for r, v in fd.items()},
-                "direction": {"adjoint": got, "tangent_linear": jv, "rel_err_vs_tangent_linear": rel(got, jv),
-                              "fd_rel_step_1e-4": fd_dir, "rel_err_vs_fd": rel(got, fd_dir),
-                              "ms_tangent_linear": 1e3 * t_j,
-                              "what": "theta (1e5, 0.01, 0.01) and v0 ~ N(0, 1) per component"},
-                "fp32_rel_err_vs_fp64": {"E_e_mu": [float(abs(a - b) / abs(b)) for a, b in zip(g32, g64)],
-                                         "v0_rms": float((gv32 - gv64).norm() / gv64.norm()),
-                                         "v0_max_abs_over_scale": float((gv32 - gv64).abs().max()
-                                                                        / gv64.abs().max())}}
+        return {"substeps": nsteps, "rel_err_vs_fd_1e-4": [rel(g64[k], fd[k]) for k in range(3)],
+                "direction_rel_err_vs_tangent_linear": rel(got, jv),
+                "fp32_rel_err_vs_fp64": [float(abs(a - b) / abs(b)) for a, b in zip(g32, g64)],
+                "fp32_v0_rms_rel_err": float((gv32 - gv64).norm() / gv64.norm())}
 
     out = {}
     grads = {}
@@ -330,323 +585,192 @@ def run_calibration(args, rank, world, dist):
         _, t_f = timed(lambda: sim.run(x0, v0, w0, guess, steps))
         (g, gv), t_fa = timed(lambda: fwd_adj(sim, xt, steps))
         grads[prec] = (g, gv)
-        out[prec] = {"forward": n_all * steps / t_f, "fwd_adjoint": n_all * steps / t_fa, "cost_ratio": t_fa / t_f,
-                     "ms_forward": 1e3 * t_f, "ms_fwd_adjoint": 1e3 * t_fa}
+        out[prec] = {"forward": n_all * steps / t_f, "fwd_adjoint": n_all * steps / t_fa, "cost_ratio": t_fa / t_f}
     full = checks(steps, xt, *grads["fp64"], *grads["fp32"])
-    # the same checks on a 64-substep horizon (few contacts begin or end inside it)
     short = min(64, steps)
     (xs, _, _), _ = s64.run(x0, v0, w0, hidden, short)
     window = checks(short, xs, *fwd_adj(s64, xs, short), *fwd_adj(s32, xs, short))
     return {"workload": f"calibration_boxes_{args.calib_scenes}x{per}", "particles": n_all, "substeps": steps,
-            "checkpoint_every": ck, "unit": METRIC, "scaling": "weak (scenes split over ranks)",
-            "path": "step_hertz force law (spheres, planes), hand-written adjoint",
-            "fp64": out["fp64"], "fp32": out["fp32"],
-            "checks_full_horizon": full, "checks_64_substeps": window, "checkpoints_per_rollout": -(-steps // ck),
-            "contact_list_every": s64.list_every, "window_reruns": s64.stats["reruns"],
-            "loss_at_guess": loss_of(s64, guess, xt, steps),
-            "config": "64 scenes x 2048 spheres r 1 mm, box 40x40x80 mm (6 planes), lattice 8x8x32 + jitter 0.1 mm, "
-                      "v U(+-0.2) m/s, E 5e6 Pa hidden / 4e6 guess, e 0.7 / 0.6, mu 0.35 / 0.3, nu 0.3, dt 2e-5 s"}
+            "checkpoint_every": ck, "path": "step_hertz force law (spheres, planes), hand-written adjoint",
+            "fp64": out["fp64"], "fp32": out["fp32"], "checks_64_substeps": window, "checks_full_horizon": full,
+            "full_horizon_note": "contacts begin and end inside 2000 substeps; central differences there do not "
+                                 "converge as the step shrinks (kinks at contact onsets), the tangent-linear run "
+                                 "is the check"}
 
 
-def run_config_lines(args, dem):
-    """Throughput of the other named configurations on this GPU (device time over CUDA events on
-    the library's stream, state resident, after warm-up), each as particle-substeps/s:
-    - plain XPBD settling, 4,096 spheres, FP64, with the reference's own OpenMP build on the same
-      scene beside it (a bounded sample);
-    - the Hertz engine on the polydisperse packing (262,144 spheres), closed variant (the
-      reference's engine refuses periodic domains and planes: floor and sides are one SDF grid
-      wall), FP64 and FP32;
-    - 65,536 point-shell hollow cylinders with a 512-point stratified shell, FP64 and the
-      FP32-mixed form (box scaled so the bodies can be placed; see workloads.hollow_cylinders)."""
-    from peclet.dem import workloads as W
-
-    def timed(sim, one, steps, warm):
-        for _ in range(warm):
-            one()
-        sim.timer_start()
-        for _ in range(steps):
-            one()
-        return sim.timer_stop() / 1e3
-
-    out = {}
-    sc = W.plain_settling()
-    sim = sc.apply(dem.Simulation(sc.n + 8, "fp64"))
-    steps = 100
-    t = timed(sim, lambda: [sim.step(sc.dt) for _ in range(sc.substeps)], steps, 3)
-    line = {"workload": f"plain_settling_{sc.n}", "unit": METRIC, "dtype": "f64",
-            "value": sc.n * sc.substeps * steps / t, "ms_per_step": 1e3 * t / steps,
-            "substeps_timed": steps * sc.substeps, "contacts_last_substep": sim.num_contacts()}
-    # the working set fits in L2 (126 MB): the byte model's bandwidth is L2 context, not an HBM
-    # fraction (counts of the last substep stand for every timed substep)
-    c = sim.counters()
-    nb = sim.num_particles()
-    per_sub = substep_bytes(nb, c["pairs"], c["contacts"], c["manifolds"], c["velocity_sweeps"],
-                            c["position_sweeps"])
-    line["l2_resident"] = {
-        "working_set_mb": round((nb * 300 + c["pairs"] * 8 + c["contacts"] * 2 * (8 + 16 * 8)
-                                 + c["manifolds"] * (12 + 20 * 8)) / 1e6, 2),
-        "algorithmic_gbps": per_sub * sc.substeps * steps / t / 1e9,
-        "counts_last_substep": {k: c[k] for k in ("pairs", "contacts", "manifolds", "velocity_sweeps",
-                                                  "position_sweeps")}}
-    sim.close()
-    if not args.no_cpu and os.path.exists(REF_OMP):
-        threads = os.cpu_count() or 1
-        v, el = cpu_reference(sc, 200, threads)
-        line["cpu_reference"] = {"value": v, "unit": METRIC, "cores": threads, "kind": "reference",
-                                 "sample": f"200 substeps of the same scene, {el:.1f} s"}
-    if not args.no_cpu and os.path.exists(REF_SERIAL):
-        v, el = cpu_reference(sc, 100, 1, REF_SERIAL)
-        line["cpu_reference_serial"] = {"value": v, "unit": METRIC, "cores": 1, "kind": "reference",
-                                        "sample": f"100 substeps of the same scene, serial shim build, "
-                                                  f"{el:.1f} s"}
-    out["settling"] = line
-
+def run_hertz(args, rank, world, dist, dem, W):
+    """The Hertz engine on the polydisperse packing (262,144 spheres), closed variant (the
+    reference's engine refuses periodic domains and planes: floor and sides are one SDF grid
+    wall), FP64 and FP32, after 20 untimed calls; the reference's own OpenMP build on the same
+    scene beside it (a bounded sample of calls)."""
     sc, extra = W.polydisperse_hertz_closed()
-    line = {"workload": f"polydisperse_{sc.n}_closed_hertz", "unit": METRIC}
+    line = {"workload": f"polydisperse_{sc.n}_closed_hertz", "substeps_per_call": sc.substeps}
     for prec in ("fp64", "fp32"):
         sim = sc.apply(dem.Simulation(sc.n + 8, prec))
         extra(sim)
-        steps = 5
-        t = timed(sim, lambda: sim.step_hertz(sc.dt, sc.substeps, 0.3), steps, 2)
-        line[prec] = {"value": sc.n * sc.substeps * steps / t, "ms_per_step": 1e3 * t / steps,
-                      "substeps_timed": steps * sc.substeps}
+        for _ in range(20):
+            sim.step_hertz(sc.dt, sc.substeps, 0.3)
+        steps = args.extra_steps
+        sim.timer_start()
+        for _ in range(steps):
+            sim.step_hertz(sc.dt, sc.substeps, 0.3)
+        t = max_over_ranks(sim.timer_stop() / 1e3, dist, "cuda")
+        line[prec] = {"value": aggregate_rate(world, sc.n, sc.substeps, steps, t), "ms_per_call": 1e3 * t / steps,
+                      "calls_timed": steps, "timed_from_call": 20}
         sim.close()
-    out["hertz"] = line
+    lib, march = ref_omp_lib()
+    if rank == 0 and world == 1 and lib and not args.no_cpu:
+        os.environ["OMP_NUM_THREADS"] = str(os.cpu_count() or 1)
+        capi = capi_module()
+        sim = sc.apply(capi.CApiSimulation(capi.CApi(lib, "ref"), sc.n + 8, "fp32"))
+        extra(sim)
+        sim.step_hertz(sc.dt, sc.substeps, 0.3)
+        t = time.perf_counter()
+        calls = 2
+        for _ in range(calls):
+            sim.step_hertz(sc.dt, sc.substeps, 0.3)
+        el = time.perf_counter() - t
+        sim.close()
+        line["cpu_reference"] = {"value": sc.n * sc.substeps * calls / el, "cores": os.cpu_count(),
+                                 "sample": f"{calls} calls after 1, {el:.1f} s, -march={march}"}
+    return line
 
+
+def run_shells(args, rank, world, dist, dem, W):
+    """65,536 hollow cylinders (r_out 1 mm, r_in 0.6 mm, L 3 mm) with a seeded 512-point stratified
+    shell, after a gravity deposition (workloads.hollow_cylinders_deposited: placed by random
+    sequential addition of their bounding spheres and stepped in FP64 until the bed formed), FP64
+    and FP32-mixed from that state, with the mixed form's error against FP64 at the end."""
     sc = W.hollow_cylinders(shell_points=W.hollow_cylinder_shell())
-    line = {"workload": f"hollow_cylinders_{sc.n}_shell512", "unit": METRIC,
-            "box_m": [float(v) for v in sc.domain[1]]}
+    sc = W.deposit(sc, dem, outer_steps=args.shell_presettle)
+    line = {"workload": f"hollow_cylinders_{sc.n}_shell512_deposited", "box_m": [float(v) for v in sc.domain[1]],
+            "presettle_steps": args.shell_presettle}
     for prec in ("fp64", "mixed"):
         sim = sc.apply(dem.Simulation(sc.n + 8, prec))
-        steps = 3
-        t = timed(sim, lambda: [sim.step(sc.dt) for _ in range(sc.substeps)], steps, 1)
-        line[prec] = {"value": sc.n * sc.substeps * steps / t, "ms_per_step": 1e3 * t / steps,
-                      "substeps_timed": steps * sc.substeps, "contacts_last_substep": sim.num_contacts()}
+        for _ in range(2):
+            outer_step(sim, sc)
+        steps = args.extra_steps
+        sim.timer_start()
+        for _ in range(steps):
+            outer_step(sim, sc)
+        t = max_over_ranks(sim.timer_stop() / 1e3, dist, "cuda")
+        c = sim.counters()
+        line[prec] = {"value": aggregate_rate(world, sc.n, sc.substeps, steps, t), "ms_per_step": 1e3 * t / steps,
+                      "contacts_last_substep": c["contacts"], "position_sweeps_last_substep": c["position_sweeps"],
+                      "velocity_sweeps_last_substep": c["velocity_sweeps"]}
         if prec == "fp64":
             x64 = sim.get_positions()
         else:
             err = np.linalg.norm(sim.get_positions() - x64, axis=1) / sc.global_scale
             line[prec]["err_vs_fp64"] = {"max_position_error_radii": float(err.max()),
-                                         "median_position_error_radii": float(np.median(err)),
-                                         "after_substeps": (steps + 1) * sc.substeps}
+                                         "after_substeps": (steps + 2) * sc.substeps}
         sim.close()
-    out["shells"] = line
-    return out
+    return line
 
 
 # ---------------------------------------------------------------------------------------------
-def cpu_reference(scene, substeps, threads, lib=REF_OMP):
-    """Time the reference's own substep (OpenMP shim build, or the serial one) for `substeps`
-    calls; returns particle-substeps/s. State set exactly as on the GPU (the reference computes in
-    float)."""
-    os.environ["OMP_NUM_THREADS"] = str(threads)
-    os.environ.setdefault("OMP_PROC_BIND", "close")
-    from peclet.dem._capi import CApi, CApiSimulation
-    api = CApi(lib, "ref")
-    sim = scene.apply(CApiSimulation(api, scene.n + 8, "fp32"))
-    sim.step(scene.dt)  # warm-up: first-touch allocations and ghost capacity
-    t = time.perf_counter()
-    for _ in range(substeps):
-        sim.step(scene.dt)
-    dt = time.perf_counter() - t
-    sim.close()
-    return scene.n * substeps / dt, dt
-
-
-def run_reference_arm(args):
-    rank = int(os.environ.get("RANK", "0"))
-    if rank != 0:
-        return 0
-    if not os.path.exists(REF_OMP):
-        print(json.dumps({"impl": "reference", "unavailable": "reference build oracle/_ref/libref_omp.so missing"}))
-        return 0
-    threads = os.cpu_count() or 1
-    scene = make_scene(args.particles)
-    os.environ["OMP_NUM_THREADS"] = str(threads)
-    from peclet.dem._capi import CApi, CApiSimulation
-    api = CApi(REF_OMP, "ref")
-    sim = scene.apply(CApiSimulation(api, scene.n + 8, "fp32"))
-    # one reference "step" = one substep of the workload (a bounded sample: an outer step of 10
-    # substeps at this size takes tens of seconds on the host)
-    for _ in range(args.warmup):
-        sim.step(scene.dt)
-    t = time.perf_counter()
-    for _ in range(args.steps):
-        sim.step(scene.dt)
-    el = time.perf_counter() - t
-    value = scene.n * args.steps / el
-    cfg = workload_desc(scene.n)
-    cfg["precision"] = "fp32 (the reference computes in float)"
-    print(json.dumps({
-        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-        "config": cfg, "impl": "reference",
-        "cpu_baseline": {"value": value, "unit": METRIC, "cores": threads, "kind": "reference",
-                         "sample": f"{args.steps} substeps of the {scene.n}-sphere workload after "
-                                   f"{args.warmup} warm-up substeps; OpenMP, {threads} threads"},
-        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
-    return 0
-
-
 def run_ours(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     dist = None
+    import torch
+    torch.cuda.set_device(local)
     if world > 1:
-        import torch
+        import datetime
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     import peclet.dem as dem
-    from peclet.dem._capi import STAGES
+    from peclet.dem import workloads as W
     dem._API.check(dem._API.fn["set_device"](local), "set_device")
 
-    scene = make_scene(args.particles)
-    n = scene.n
-    sim = scene.apply(dem.Simulation(n + 8, "fp64"))
-    # the configuration runs 200 steps from rest; the timed steps sit in its middle (after
-    # `--presettle` untimed steps), where the first spheres reach the floor
-    for _ in range(args.presettle + args.warmup):
-        for _ in range(SUBSTEPS):
-            sim.step(scene.dt)
-
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-
-    # ---- device-timed region ----
-    clocks = ClockSampler(local)
-    with clocks:
-        time.sleep(0.5)  # sampler running before the timed region starts
-        barrier()
-        timed_allocs = dem._API.fn["debug_allocs"]()
-        t0 = time.perf_counter()
-        sim.timer_start()  # events on the library's stream around the whole timed region
-        for _ in range(args.steps):
-            for _ in range(SUBSTEPS):
-                sim.step(scene.dt)
-        dev_ms = sim.timer_stop()
-        wall = time.perf_counter() - t0
-        timed_allocs = dem._API.fn["debug_allocs"]() - timed_allocs
-    barrier()
-    # the same number of steps again with per-stage events (their synchronisation per substep
-    # slows the step; these figures explain the timed value, they are not it)
-    sim.profile_enable(True)
-    for _ in range(args.steps):
-        for _ in range(SUBSTEPS):
-            sim.step(scene.dt)
-    stages, launches = sim.profile_read()
-    counts = sim.debug_counts()
-    sweeps = sim.debug_sweeps() if hasattr(sim, "debug_sweeps") else None
-    reuse = sim.debug_reuse()
-    last = sim.counters()
-    sim.profile_enable(False)
-    # max over ranks of the device time; value = all ranks' particle-substeps / that time
-    t_max = max_over_ranks(dev_ms / 1e3, dist, "cuda")
-    value = aggregate_rate(world, n, SUBSTEPS, args.steps, t_max)
-
-    # ---- end to end through the public API with host buffers (pinned, as a data loader's) ----
-    import torch
-    pinned = lambda: torch.zeros((n, 3), dtype=torch.float64, pin_memory=True).numpy()
-    force, pos, vel = pinned(), pinned(), pinned()
-    barrier()
-    te = time.perf_counter()
-    allocs = dem._API.fn["debug_allocs"]
-    a0 = allocs()
-    laps = []
-    for _ in range(args.steps):
-        tl = time.perf_counter()
-        sim.set_external_forces(force)
-        for _ in range(SUBSTEPS):
-            sim.step(scene.dt)
-        sim.get_positions(out=pos)
-        sim.get_velocities(out=vel)
-        laps.append(round(1e3 * (time.perf_counter() - tl), 2))
-    e2e_s = time.perf_counter() - te
-    assert np.all(np.isfinite(pos)) and np.all(np.isfinite(vel))
-    e2e = {"value": world * n * SUBSTEPS * args.steps / e2e_s, "unit": METRIC,
-           "h2d_bytes_per_step": int(force.nbytes), "d2h_bytes_per_step": int(pos.nbytes + vel.nbytes),
-           "ms_per_step_each": laps, "device_allocations": int(allocs() - a0)}
-
-    # ---- roofline of the dominant stage ----
-    per_step = {k: (ms / args.steps, c / args.steps) for k, (ms, c) in stages.items() if c}
-    peak, peak_kind = measured_peaks()
-    P, C, M = counts["pairs"], counts["contacts"], counts["manifolds"]
-    iv = sweeps["velocity"] / args.steps / SUBSTEPS if sweeps else 10
-    ip = sweeps["position"] / args.steps / SUBSTEPS if sweeps else 10
-    stage_bytes = {
-        "velocity": iv * M * (12 + 20 * 8 + 53 * 8),
-        "position": ip * C * (8 + 48 * 8),
-        "broadphase": n * 4 * 8 + 8 * P,
-        "narrowphase": 8 * P + C * (8 + 16 * 8),
-        "manifolds": 2 * C * (8 + 16 * 8) + M * (12 + 20 * 8),
-        "colour_velocity": 12 * (M + C),
-        "ledger": M * (16 + 8 * 8),
-    }
-    step_bytes = substep_bytes(n, P, C, M, iv, ip) * SUBSTEPS
-    # the dominant stage among those with a byte model (all the heavy ones)
-    roof_stage = max((k for k in per_step if k in stage_bytes), key=lambda k: per_step[k][0])
-    st_ms = per_step[roof_stage][0] / SUBSTEPS
-    achieved = stage_bytes[roof_stage] / (st_ms / 1e3) / 1e9 if st_ms > 0 else 0.0
-    traffic = STAGE_DRAM_BYTES.get((n, roof_stage))
-    roofline = {"bound": "hbm", "kernel": f"{roof_stage} stage (per substep)", "achieved": achieved,
-                "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
-                "traffic": traffic, "traffic_unit": "bytes per substep (ncu)",
-                "algorithmic_bytes": stage_bytes[roof_stage],
-                "step_algorithmic_GBps": step_bytes / (dev_ms / 1e3 / args.steps) / 1e9}
-
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu and os.path.exists(REF_OMP):
-        threads = os.cpu_count() or 1
-        v, el = cpu_reference(scene, args.cpu_substeps, threads)
-        cpu = {"value": v, "unit": METRIC, "cores": threads, "kind": "reference",
-               "sample": f"{args.cpu_substeps} substeps of the same {n}-sphere workload (reference code, "
-                         f"OpenMP Kokkos-shim build, float), {el:.1f} s"}
-
-    batched = run_batched(args, rank, world, dist, dem) if args.drums > 0 else None
-    calib = run_calibration(args, rank, world, dist) if args.calib_scenes > 0 else None
-    configs = run_config_lines(args, dem) if (rank == 0 and not args.no_configs) else None
+    h = run_headline(args, rank, world, dist, dem, W)
+    extras = [e for e in args.extras.split(",") if e in EXTRAS] if args.extras != "none" else []
+    detail = {}
+    runners = {"xpbd262k": lambda: run_xpbd262k(args, rank, world, dist, dem, W),
+               "batched": lambda: run_batched(args, rank, world, dist, dem, W),
+               "calibration": lambda: run_calibration(args, rank, world, dist),
+               "hertz": lambda: run_hertz(args, rank, world, dist, dem, W),
+               "shells": lambda: run_shells(args, rank, world, dist, dem, W)}
+    for name in EXTRAS:
+        if name in extras:
+            detail[name] = runners[name]()
 
     if rank == 0:
+        flat = {}
+        if "xpbd262k" in detail:
+            flat["xpbd262k_fp64_value"] = detail["xpbd262k"]["value"]
+        if "batched" in detail:
+            b = detail["batched"]
+            flat.update(batched_fp64_value=b["fp64"]["value"], batched_mixed_value=b["mixed"]["value"],
+                        batched_mixed_over_fp64=b["mixed_over_fp64"],
+                        mixed_err_radii=b["mixed"]["err_vs_fp64"]["max_position_error_radii"],
+                        batched_mean_velocity_sweeps=b["fp64"]["mean_sweeps_last_substep"]["velocity"])
+        if "calibration" in detail:
+            cb = detail["calibration"]
+            flat.update(fwd_adjoint_cost_ratio=cb["fp64"]["cost_ratio"], fwd_adjoint_value=cb["fp64"]["fwd_adjoint"],
+                        grad_rel_err_vs_fd_64=max(v for v in cb["checks_64_substeps"]["rel_err_vs_fd_1e-4"] if v is not None),
+                        grad_rel_err_vs_fd_full=max(v for v in cb["checks_full_horizon"]["rel_err_vs_fd_1e-4"] if v is not None))
+        if "hertz" in detail:
+            flat.update(hertz262k_fp64_value=detail["hertz"]["fp64"]["value"],
+                        hertz262k_fp32_value=detail["hertz"]["fp32"]["value"])
+            if "cpu_reference" in detail["hertz"]:
+                flat["hertz262k_cpu_reference_value"] = detail["hertz"]["cpu_reference"]["value"]
+        if "shells" in detail:
+            flat.update(shells_fp64_value=detail["shells"]["fp64"]["value"],
+                        shells_mixed_value=detail["shells"]["mixed"]["value"])
+        detail["headline"] = {k: h[k] for k in ("stages_ms_per_substep", "sweeps_per_substep", "counts_last_substep",
+                                               "packing_at_end", "roofline")}
+        print(json.dumps({"detail": detail}))
         line = {
-            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-            "config": dict(workload_desc(n), parallelism="replicas" if world > 1 else "single",
-                           timed_steps_from=args.presettle + args.warmup),
-            "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "cpu_baseline": cpu,
-            "clocks": clocks.summary(), "wall_ms_per_step": 1e3 * wall / args.steps,
-            "stages_ms_per_step": {k: round(v[0], 4) for k, v in per_step.items()},
-            "counts_last_substep": counts, "sweeps": sweeps, "topology_kept": reuse, "last_substep": last, "batched": batched,
-            "fwd_adjoint": calib, "configs": configs,
-            "device_allocations_timed": int(timed_allocs),
-        }
+            "metric": METRIC, "value": h["value"], "unit": METRIC, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * h["t_max"] / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded), saved restart state",
+            "config": headline_desc(world), "e2e": h["e2e"], "gpu_launches": h["launches"],
+            "roofline": {k: h["roofline"][k] for k in ("bound", "kernel", "achieved", "peak", "unit", "frac",
+                                                       "traffic", "peak_source")},
+            "cpu_baseline": h["cpu"], "clocks": h["clocks"],
+            "sweeps_per_substep": {k: round(v, 2) for k, v in h["sweeps_per_substep"].items()},
+            "device_allocations_timed": h["timed_allocs"], **{k: (round(v, 6) if isinstance(v, float) else v)
+                                                             for k, v in flat.items()}}
         print(json.dumps(line))
     if dist is not None:
         dist.destroy_process_group()
     return 0
 
 
+def spawn_ranks(args):
+    """`--gpus N` without a launcher: start N ranks on this node (one per GPU) through
+    torch.distributed.run, which sets RANK / LOCAL_RANK / WORLD_SIZE, and pass their output on."""
+    import socket
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.run(cmd).returncode
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--particles", type=int, default=262144)
-    ap.add_argument("--cpu-substeps", type=int, default=3)
+    ap.add_argument("--cpu-steps", type=int, default=20, help="timed outer steps of the headline's CPU baseline")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--drums", type=int, default=512, help="scenes of the batched line (0: skip it)")
-    ap.add_argument("--calib-scenes", type=int, default=64, help="scenes of the calibration line (0: skip it)")
+    ap.add_argument("--extras", default=",".join(EXTRAS), help=f"comma list of {EXTRAS} or 'none'")
+    ap.add_argument("--extra-steps", type=int, default=5, help="timed outer steps (or calls) of the extra lines")
+    ap.add_argument("--drums", type=int, default=512)
+    ap.add_argument("--drum-presettle", type=int, default=60, help="untimed FP64 outer steps of the drum deposition")
+    ap.add_argument("--shell-presettle", type=int, default=40, help="untimed FP64 outer steps of the shell deposition")
+    ap.add_argument("--calib-scenes", type=int, default=64)
     ap.add_argument("--calib-substeps", type=int, default=2000)
-    ap.add_argument("--no-configs", action="store_true", help="skip the settling / Hertz / shell lines")
-    ap.add_argument("--presettle", type=int, default=95,
-                    help="untimed steps of the 200-step run before the warm-up and timed steps")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        return spawn_ranks(args)
     return run_ours(args)
 
 

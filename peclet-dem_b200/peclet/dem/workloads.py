@@ -26,6 +26,7 @@ class Scene:
     inv_mass: np.ndarray                 # (N,)
     inv_inertia: np.ndarray              # (N,3)
     quat: np.ndarray | None = None       # (N,4) x,y,z,w
+    angvel: np.ndarray | None = None     # (N,3)
     scales: np.ndarray | None = None     # (N,)
     shape: tuple = (SPHERE, 1.0, 0.0, 0.0)
     global_scale: float = 1.0
@@ -70,6 +71,8 @@ class Scene:
         if self.scales is not None:
             sim.set_scales(self.scales)
         sim.set_velocities(self.vel)
+        if self.angvel is not None:
+            sim.set_angular_velocities(self.angvel)
         sim.set_inv_mass(self.inv_mass)
         sim.set_inv_inertia(self.inv_inertia)
         sim.set_dt(self.dt)
@@ -115,6 +118,30 @@ def plain_settling(seed=1, nx=16, ny=16, nz=16, cells_z=64, radius=1e-3, spacing
                  iterations=iterations, dt=dt_outer / substeps, substeps=substeps)
 
 
+STATE_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "states")
+PLAIN_SETTLED_STEPS = 800
+
+
+def plain_settling_state_path(steps=PLAIN_SETTLED_STEPS):
+    return os.path.join(STATE_DIR, f"plain_settling_4096_step{steps}.npz")
+
+
+def plain_settled(steps=PLAIN_SETTLED_STEPS, path=None) -> Scene:
+    """The 4,096-sphere settling configuration restarted from its saved state after `steps` outer
+    steps (10 substeps each) of the FP64 step from the lattice start (states/make_states.py):
+    positions, velocities, orientations and spins; every setting is the configuration's. The
+    warm-start ledger, support levels and the restitution threshold start cold, as after any
+    `set_positions`."""
+    sc = plain_settling()
+    st = np.load(path or plain_settling_state_path(steps))
+    if st["pos"].shape != sc.pos.shape:
+        raise ValueError(f"saved state holds {st['pos'].shape[0]} spheres, the configuration {sc.n}")
+    sc.pos, sc.vel = st["pos"].astype(np.float64), st["vel"].astype(np.float64)
+    sc.quat, sc.angvel = st["quat"].astype(np.float64), st["angvel"].astype(np.float64)
+    sc.name = f"plain_settling_{sc.n}_from_step{int(st['steps'])}"
+    return sc
+
+
 def random_unit_quats(rng, n):
     q = rng.normal(size=(n, 4))
     q /= np.linalg.norm(q, axis=1, keepdims=True)
@@ -151,6 +178,27 @@ def hollow_cylinders(seed=3, n=65536, r_out=1e-3, r_in=0.6e-3, length=3e-3, box=
                  domain=(mn, mx, (False, False, False)), planes=box_planes(mn, mx),
                  material=(e, 0.0, mu), iterations=iterations, dt=dt_outer / substeps,
                  substeps=substeps, shell=shell_points)
+
+
+def deposit(sc: Scene, dem, outer_steps, v_down=0.5, precision="fp64") -> Scene:
+    """The scene after a gravity deposition: every body starts with `v_down` m/s along gravity on
+    top of its own velocity and the scene is stepped `outer_steps` outer steps (its substeps and
+    dt) by `dem.Simulation` in `precision`. Returns a copy whose positions, velocities,
+    orientations and spins are the end state."""
+    import copy
+    g = np.asarray(sc.gravity, dtype=np.float64)
+    gn = np.linalg.norm(g)
+    out = copy.copy(sc)
+    out.vel = sc.vel + (v_down * g / gn if gn > 0 else 0.0)
+    sim = out.apply(dem.Simulation(sc.n + 8, precision))
+    for _ in range(outer_steps):
+        for _ in range(sc.substeps):
+            sim.step(sc.dt)
+    out.pos, out.vel = sim.get_positions(), sim.get_velocities()
+    out.quat, out.angvel = sim.get_quaternions(), sim.get_angular_velocities()
+    out.name = f"{sc.name}_deposited{outer_steps}"
+    sim.close()
+    return out
 
 
 _RSA_SRC = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_gen", "rsa.c")
