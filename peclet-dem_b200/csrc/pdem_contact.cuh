@@ -836,7 +836,8 @@ __global__ void kGroundEdges(Dev<R> d, int nm, V3<R> gHat, int4* edges) {
 //             source level changed inside the window, that is exactly the sequential result;
 //  exact path: otherwise each lane's source level is recomputed from the pre-window level and the
 //             pushes of EARLIER lanes whose destination is that source (fixed point over the
-//             window), and the exact pushes are applied. Fast-path pushes never exceed the exact
+//             window; those lanes are found once per window from the destinations in shared
+//             memory), and the exact pushes are applied. Fast-path pushes never exceed the exact
 //             ones (levels only grow), so applying both gives the sequential result.
 // A sweep that changes nothing ends the loop (later sweeps would repeat it unchanged).
 // Levels live in shared memory when they fit, else in a global scratch array.
@@ -845,6 +846,7 @@ constexpr int kGroundPF = 8;
 __device__ __forceinline__ void groundSweepsWarp(int nm, int b0, int nb, int sweeps, const int4* edges,
                                                  uint8_t* grounded, int* L) {
   const int lane = threadIdx.x & 31;
+  __shared__ int sDst[32], sPush[32];  // one warp per block: the window's destinations and pushes
   for (int i = lane; i < nb; i += 32)
     L[i] = grounded[b0 + i];
   __threadfence_block();
@@ -878,19 +880,29 @@ __device__ __forceinline__ void groundSweepsWarp(int nm, int b0, int nb, int swe
         if (__any_sync(0xffffffffu, dstMoved))
           sweepChanged = 1;
         if (__any_sync(0xffffffffu, srcMoved)) {
+          // earlier lanes of the window that push to this lane's source: one scan of the window's
+          // destinations, then fixed-point rounds that read only those lanes' pushes
+          sDst[lane] = (kind != 0) ? dst : -1;
+          __syncwarp();
+          unsigned from = 0;
+#pragma unroll
+          for (int t = 0; t < 32; ++t)
+            if (t < lane && kind == 2 && sDst[t] == src)
+              from |= 1u << t;
           for (int it = 0; it < 33; ++it) {
+            sPush[lane] = contrib ? c : -1;
+            __syncwarp();
             int best = L0s;
-            for (int t = 0; t < 32; ++t) {
-              const int dT = __shfl_sync(0xffffffffu, dst, t);
-              const int cT = __shfl_sync(0xffffffffu, c, t);
-              const int okT = __shfl_sync(0xffffffffu, contrib ? 1 : 0, t);
-              if (t < lane && kind == 2 && okT && dT == src && cT > best)
+            for (unsigned m = from; m; m &= m - 1) {
+              const int cT = sPush[__ffs(m) - 1];
+              if (cT > best)
                 best = cT;
             }
             const int nc = (kind == 2) ? best - 1 : c;
             const bool ch = nc != c;
             c = nc;
             contrib = (kind == 1) || (kind == 2 && c > 0);
+            __syncwarp();  // this round's reads of the pushes come before the next round's writes
             if (!__any_sync(0xffffffffu, ch))
               break;
           }

@@ -65,8 +65,8 @@ __device__ __forceinline__ bool gridBarrier(const GridBar& gb) {
 // (kCtl): each END here is fused with the next sweep's BEGIN. CLUSTER: the launch is one thread-block
 // cluster (a small graph), and the hardware cluster barrier (arrive with release, wait with acquire
 // semantics at cluster scope) replaces the grid-wide one.
-constexpr int kSweepCluster = 8;                                  // blocks of the small-graph launch
-constexpr int kSweepClusterEntries = 4 * kSweepCluster * kBlock;  // largest graph it takes
+constexpr int kSweepCluster = 8;                                  // blocks of the portable cluster
+constexpr int kSweepClusterEntries = 4 * kSweepCluster * kBlock;  // default largest graph it takes
 template <bool CLUSTER>
 __device__ __forceinline__ bool loopBarrier(const GridBar& gb) {
   if (CLUSTER) {

@@ -290,12 +290,12 @@ template <class R>
 template <class K, class... A>
 bool Sim<R>::launchCluster(K kernel, A... args) {
   cudaLaunchConfig_t cfg{};
-  cfg.gridDim = dim3(kSweepCluster);
+  cfg.gridDim = dim3(sweepClusterBlocks_);
   cfg.blockDim = dim3(kBlock);
   cfg.stream = stream_;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeClusterDimension;
-  attr[0].val.clusterDim.x = kSweepCluster;
+  attr[0].val.clusterDim.x = sweepClusterBlocks_;
   attr[0].val.clusterDim.y = 1;
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
@@ -304,6 +304,9 @@ bool Sim<R>::launchCluster(K kernel, A... args) {
   auto it = clusterOk_.find(key);
   if (it == clusterOk_.end()) {
     int clusters = 0;
+    if (sweepClusterBlocks_ > 8 &&
+        cudaFuncSetAttribute(kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
+      (void)cudaGetLastError();
     if (cudaOccupancyMaxActiveClusters(&clusters, kernel, &cfg) != cudaSuccess)
       (void)cudaGetLastError();
     it = clusterOk_.emplace(key, clusters >= 1 ? 1 : 0).first;
@@ -1514,11 +1517,11 @@ void Sim<R>::demStep() {
       ++launches_, kSweepScenes<R, 0, 1><<<numScenes_, sceneBlock(), 0, s>>>(d_, sceneLpt_.p, mOrder_.p, mOff_.p, velIters_, sp, thr);
     else if (batch_)
       ++launches_, kSweepScenes<R, 1, 1><<<numScenes_, sceneBlock(), 0, s>>>(d_, sceneLpt_.p, mOrder_.p, mOff_.p, velIters_, sp, thr);
-    else if (usePGS && !(nm <= kSweepClusterEntries &&
+    else if (usePGS && !(nm <= sweepClusterEntries_ &&
                          launchCluster(kSweepLoop<R, 0, 1, true>, d_, (const int*)mOrder_.p, (const int*)mOff_.p,
                                        ncolV, velIters_, sp, thr, gb)))
       launchCoop(kSweepLoop<R, 0, 1>, d_, (const int*)mOrder_.p, (const int*)mOff_.p, ncolV, velIters_, sp, thr, gb);
-    else if (!usePGS && !(nm <= kSweepClusterEntries &&
+    else if (!usePGS && !(nm <= sweepClusterEntries_ &&
                           launchCluster(kSweepLoop<R, 1, 1, true>, d_, (const int*)mOrder_.p, (const int*)mOff_.p,
                                         ncolV, velIters_, sp, thr, gb)))
       launchCoop(kSweepLoop<R, 1, 1>, d_, (const int*)mOrder_.p, (const int*)mOff_.p, ncolV, velIters_, sp, thr, gb);
@@ -1612,7 +1615,7 @@ void Sim<R>::demStep() {
         ctl(CTL_STAB_BEGIN, R(0), 0);
         if (batch_)
           ++launches_, kSweepScenes<R, 0, 2><<<numScenes_, sceneBlock(), 0, s>>>(d_, sceneLpt_.p, mOrder_.p, mOff_.p, iters, ss, vRestS);
-        else if (!(nm <= kSweepClusterEntries &&
+        else if (!(nm <= sweepClusterEntries_ &&
                    launchCluster(kSweepLoop<R, 0, 2, true>, d_, (const int*)mOrder_.p, (const int*)mOff_.p, ncolV,
                                  iters, ss, vRestS, gb)))
           launchCoop(kSweepLoop<R, 0, 2>, d_, (const int*)mOrder_.p, (const int*)mOff_.p, ncolV, iters, ss, vRestS, gb);
@@ -1718,7 +1721,7 @@ void Sim<R>::demStep() {
       ++launches_, kSweepScenes<R, 2, 3><<<numScenes_, sceneBlock(), 0, s>>>(d_, sceneLpt_.p, cOrder_.p, cOff_.p, posIters_, sp, posTol);
       tuneEnd();
     }
-    else if (!(nc <= kSweepClusterEntries &&
+    else if (!(nc <= sweepClusterEntries_ &&
                launchCluster(kSweepLoop<R, 2, 3, true>, d_, (const int*)cOrder_.p, (const int*)cOff_.p, ncolP,
                              posIters_, sp, posTol, gb)))
       launchCoop(kSweepLoop<R, 2, 3>, d_, (const int*)cOrder_.p, (const int*)cOff_.p, ncolP, posIters_, sp, posTol, gb);

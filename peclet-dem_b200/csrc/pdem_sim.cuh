@@ -375,10 +375,26 @@ class Sim {
   template <class K, class... A>
   void launchCoopSmem(K kernel, int block, size_t smem, A... args);
   std::map<std::pair<const void*, size_t>, int> coopPerSmem_;
-  // one thread-block cluster of kSweepCluster blocks; false when such a cluster cannot be resident
+  // one thread-block cluster of sweepClusterBlocks_ blocks; false when such a cluster cannot be
+  // resident
   template <class K, class... A>
   bool launchCluster(K kernel, A... args);
   std::map<const void*, int> clusterOk_;  // per kernel: 1 resident, 0 not
+  // blocks of the one-cluster sweep loop (PDEM_SWEEP_CLUSTER: 8, the portable size, or 16, which
+  // needs the non-portable cluster attribute) and the largest entry list it takes
+  // (PDEM_SWEEP_CLUSTER_ENTRIES); larger lists sweep on the cooperative grid
+  int sweepClusterBlocks_ = [] {
+    const char* e = std::getenv("PDEM_SWEEP_CLUSTER");
+    const long v = e ? std::strtol(e, nullptr, 10) : 16;
+    return v == 8 ? 8 : 16;
+  }();
+  long sweepClusterEntries_ = [] {
+    const char* e = std::getenv("PDEM_SWEEP_CLUSTER_ENTRIES");
+    // default: up to 8 entries a thread of 16 x 256 (about one entry a thread per colour step at
+    // the 8-12 colours of a settled pile). Measured on the 4,096-sphere settled bed (12.4k
+    // manifolds): the velocity loop 0.57 ms per substep on the cooperative grid, 0.47 in one cluster
+    return e ? std::max(0L, std::strtol(e, nullptr, 10)) : 32768L;
+  }();
   std::map<std::pair<const void*, int>, int> coopPer_;  // resident blocks per SM, by (kernel, block)
   template <class T>
   void sortPairs(const T* kin, T* kout, const int* vin, int* vout, int n, int endBit);

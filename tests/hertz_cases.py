@@ -57,3 +57,20 @@ def floor():
     m, I = props(r)
     return dict(x0=x0, v0=np.array([[0.1, 0.05, -0.1]]), w0=np.array([[1.0, 2, 3]]), r=r, m=m, I=I, first=[0, 1],
                 planes=[[0, 0, 0, 0, 0, 1]], g=(0.0, 0.0, -9.81))
+
+
+def shape_pairs(seed=31, n=40, L=8e-3, shell=None, calls_substeps=(4, 10)):
+    """Hollow cylinders (point shells) under the Hertz engine: the shape-pair force path
+    (src/solver_hertz.hpp:454, called at src/sim.hpp:696) and shell-wall contacts. The engine
+    refuses analytic planes, so the container is one SDF grid wall (floor and sides of an open
+    box). Returns (scene, extra)."""
+    import scenes as S
+    from peclet.dem import workloads as W
+    sc = S.cylinders(seed=seed, n=n, L=L, shell=shell)
+    sc.planes = []
+    grid = W.box_wall_grid(L, L, h=0.5e-3)
+
+    def extra(s):
+        s.add_sdf_wall(*grid, 0.4, 0.3)
+        s.set_hertz_material(0, 1e7, 0.3)
+    return sc, extra

@@ -29,7 +29,21 @@ def _dense_drum():
     return sc, extra
 
 
-CASES = [("drum_spheres", _drum_spheres, 4, 10, 0.3), ("dense_drum", _dense_drum, 3, 20, 0.2)]
+def _shape_pairs():
+    import hertz_cases as HC
+    return HC.shape_pairs()
+
+
+def _shape_pairs_512():
+    import hertz_cases as HC
+    from peclet.dem import workloads as W
+    return HC.shape_pairs(seed=32, n=64, L=10e-3, shell=W.hollow_cylinder_shell())
+
+
+# (name, scene, calls, substeps per call, skin fraction); the shape cases drive the shape-pair
+# forces (src/solver_hertz.hpp:454) with the analytic shell and the 512-point stratified shell
+CASES = [("drum_spheres", _drum_spheres, 4, 10, 0.3), ("dense_drum", _dense_drum, 3, 20, 0.2),
+         ("shape_pairs", _shape_pairs, 3, 10, 0.3), ("shape_pairs_512", _shape_pairs_512, 2, 10, 0.3)]
 
 
 @pytest.mark.parametrize("precision,rtol", [("fp32", 0.0), ("fp64", 1e-12)])

@@ -48,3 +48,23 @@ def test_domain_getters_match_reference(ref_api, orc_api):
             sim = P.build(api, S.dense_spheres(), setup, "fp32")
             got.append((sim.get_domain_min(), sim.get_domain_max()))
         assert got[0] == got[1]
+
+
+def test_hertz_shape_pairs_restatement_bitexact_vs_reference(ref_api, orc_api):
+    """Hollow cylinders (point shells) under the Hertz engine: the shape-pair forces
+    (hertzShapePairForcesKokkos, src/solver_hertz.hpp:454) and shell-wall contacts, bit-exact."""
+    import hertz_cases as HC
+    sc, extra = HC.shape_pairs()
+    a = P.build(ref_api, sc, extra, "fp32")
+    b = P.build(orc_api, sc, extra, "fp32")
+    for k in range(3):
+        a.step_hertz(2e-6, 10, 0.3)
+        b.step_hertz(2e-6, 10, 0.3)
+        sa, sb = P.snapshot(a, products=False), P.snapshot(b, products=False)
+        ka, xa = a.debug_hertz()
+        kb, xb = b.debug_hertz()
+        assert len(ka) > 0 and np.count_nonzero(xa) > 0  # touching shell pairs carry history
+        sa.update(hk=ka, hx=xa)
+        sb.update(hk=kb, hx=xb)
+        bad = P.diff(sa, sb)
+        assert not bad, f"hertz shape pairs call {k}: {bad[:4]}"
