@@ -71,6 +71,16 @@ struct SceneCtl {
   int velSweeps, stabSweeps, posSweeps, pad2;
 };
 
+// colour-ordered records of the coloured velocity sweeps (layout and packing in pdem_solve.cuh,
+// kPackPgs): kPgsSlots slots of 4 values per entry, slot-major, and the entry's ids
+constexpr int kPgsSlots = 11;
+template <class R>
+struct PgsRecs {
+  Q4<R>* q;
+  int4* ids;
+  long cap;
+};
+
 template <class R>
 struct Dev {
   int cap = 0, maxPairs = 0, maxContacts = 0;

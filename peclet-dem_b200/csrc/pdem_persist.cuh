@@ -75,9 +75,13 @@ __device__ __forceinline__ bool loopBarrier(const GridBar& gb) {
   }
   return gridBarrier(gb);
 }
+// KIND 3: the projected GS velocity sweep of KIND 0 from the colour-ordered records of kPackPgs
+// (entry t of the order is record t), the same arithmetic with fewer dependent loads. The colour
+// offsets (at most 63 colours) are read once into shared memory.
 template <class R, int KIND, int LOOP, bool CLUSTER = false>
 __global__ void __launch_bounds__(kBlock) kSweepLoop(Dev<R> d, const int* order, const int* coff, int ncol, int iters,
-                                                     SolveP<R> P, R thr, GridBar gb) {
+                                                     SolveP<R> P, R thr, GridBar gb, PgsRecs<R> recs) {
+  __shared__ int sOff[kSaturatedColor + 2];
   Counters<R>* c = d.ctr;
   volatile int* done = LOOP == 1 ? &c->velDone : LOOP == 2 ? &c->stabDone : &c->posDone;
   int* sweeps = LOOP == 1 ? &c->velSweeps : LOOP == 2 ? &c->stabSweeps : &c->posSweeps;
@@ -86,21 +90,29 @@ __global__ void __launch_bounds__(kBlock) kSweepLoop(Dev<R> d, const int* order,
   const long gtid = (long)blockIdx.x * blockDim.x + threadIdx.x, gstride = (long)gridDim.x * blockDim.x;
   if (*done)
     return;
+  for (int k = threadIdx.x; k <= ncol && k < kSaturatedColor + 2; k += blockDim.x)
+    sOff[k] = coff[k];
+  __syncthreads();
   for (int it = 0; it < iters; ++it) {
     R mx = R(0);
     for (int col = 0; col < ncol; ++col) {
-      const int b = coff[col], n = coff[col + 1] - b;
+      const int b = sOff[col], n = sOff[col + 1] - b;
       // colour 62 is where the 62-colour mask saturates: not an independent set, so one thread
       // runs it in manifold order, as the reference's serial sweep does
       const bool serial = col >= kSaturatedColor;
       if (!serial || lead)
         for (long t = serial ? 0 : gtid; t < n; t += serial ? 1 : gstride) {
-          if (KIND == 0)
+          if (KIND == 0) {
             pgsOne(d, order[b + t], P, mx, LOOP);
-          else if (KIND == 1)
+          } else if (KIND == 1) {
             gsOne(d, order[b + t], P, mx);
-          else
+          } else if (KIND == 3) {
+            int idx;
+            const PgsStatic<R> st = pgsRecord(recs, b + t, idx);
+            pgsCore<R>(d, idx, st, P.eN, P.mu, 0, P, mx);
+          } else {
             posGSOne(d, order[b + t], mx);
+          }
         }
       if (col == ncol - 1)
         warpMaxAtomic(mxp, mx);

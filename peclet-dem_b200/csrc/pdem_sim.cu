@@ -318,6 +318,23 @@ bool Sim<R>::launchCluster(K kernel, A... args) {
   return true;
 }
 
+// the colour-ordered velocity-sweep records of this substep's manifolds, packed at the first
+// request of a substep (the orientations and masses they hold do not change until the
+// integration after the stabilization pass)
+template <class R>
+PgsRecs<R> Sim<R>::packPgs(int nm, int ncol) {
+  if (pgsPackedAt_ != substepId_) {
+    pgsQ_.ensure((size_t)kPgsSlots * nm, false, stream_);
+    pgsIds_.ensure((size_t)nm, false, stream_);
+    pgsCap_ = (long)(pgsIds_.n);
+    ++launches_, kPackPgs<R><<<gridFor(nm), kBlock, 0, stream_>>>(d_, mOrder_.p, mOff_.p, ncol,
+                                                                 PgsRecs<R>{pgsQ_.p, pgsIds_.p, pgsCap_});
+    KCHECK("pack velocity records");
+    pgsPackedAt_ = substepId_;
+  }
+  return PgsRecs<R>{pgsQ_.p, pgsIds_.p, pgsCap_};
+}
+
 // ---- CUB helpers ----
 template <class R>
 template <class T>
@@ -1403,6 +1420,7 @@ template <class R>
 void Sim<R>::demStep() {
   const int B = kBlock;
   cudaStream_t s = stream_;
+  ++substepId_;
   mark(ST_PREDICT);
   if (batch_)
     batchBegin();
@@ -1518,13 +1536,15 @@ void Sim<R>::demStep() {
     else if (batch_)
       ++launches_, kSweepScenes<R, 1, 1><<<numScenes_, sceneBlock(), 0, s>>>(d_, sceneLpt_.p, mOrder_.p, mOff_.p, velIters_, sp, thr);
     else if (usePGS && !(nm <= sweepClusterEntries_ &&
-                         launchCluster(kSweepLoop<R, 0, 1, true>, d_, (const int*)mOrder_.p, (const int*)mOff_.p,
-                                       ncolV, velIters_, sp, thr, gb)))
-      launchCoop(kSweepLoop<R, 0, 1>, d_, (const int*)mOrder_.p, (const int*)mOff_.p, ncolV, velIters_, sp, thr, gb);
+                         launchCluster(kSweepLoop<R, 3, 1, true>, d_, (const int*)mOrder_.p, (const int*)mOff_.p,
+                                       ncolV, velIters_, sp, thr, gb, packPgs(nm, ncolV))))
+      launchCoop(kSweepLoop<R, 0, 1>, d_, (const int*)mOrder_.p, (const int*)mOff_.p, ncolV, velIters_, sp, thr, gb,
+                 PgsRecs<R>{});
     else if (!usePGS && !(nm <= sweepClusterEntries_ &&
                           launchCluster(kSweepLoop<R, 1, 1, true>, d_, (const int*)mOrder_.p, (const int*)mOff_.p,
-                                        ncolV, velIters_, sp, thr, gb)))
-      launchCoop(kSweepLoop<R, 1, 1>, d_, (const int*)mOrder_.p, (const int*)mOff_.p, ncolV, velIters_, sp, thr, gb);
+                                        ncolV, velIters_, sp, thr, gb, PgsRecs<R>{})))
+      launchCoop(kSweepLoop<R, 1, 1>, d_, (const int*)mOrder_.p, (const int*)mOff_.p, ncolV, velIters_, sp, thr, gb,
+                 PgsRecs<R>{});
     KCHECK("velocity loop");
   }
   // no colours and no fallback: the first sweep is empty, its END finds maxApproach = 0 <= thr
@@ -1616,9 +1636,10 @@ void Sim<R>::demStep() {
         if (batch_)
           ++launches_, kSweepScenes<R, 0, 2><<<numScenes_, sceneBlock(), 0, s>>>(d_, sceneLpt_.p, mOrder_.p, mOff_.p, iters, ss, vRestS);
         else if (!(nm <= sweepClusterEntries_ &&
-                   launchCluster(kSweepLoop<R, 0, 2, true>, d_, (const int*)mOrder_.p, (const int*)mOff_.p, ncolV,
-                                 iters, ss, vRestS, gb)))
-          launchCoop(kSweepLoop<R, 0, 2>, d_, (const int*)mOrder_.p, (const int*)mOff_.p, ncolV, iters, ss, vRestS, gb);
+                   launchCluster(kSweepLoop<R, 3, 2, true>, d_, (const int*)mOrder_.p, (const int*)mOff_.p, ncolV,
+                                 iters, ss, vRestS, gb, packPgs(nm, ncolV))))
+          launchCoop(kSweepLoop<R, 0, 2>, d_, (const int*)mOrder_.p, (const int*)mOff_.p, ncolV, iters, ss, vRestS, gb,
+                     PgsRecs<R>{});
       }
       for (int it = 0; it < (stabPersistent ? 0 : iters); ++it) {
         ctl(CTL_STAB_BEGIN, R(0), 0);
@@ -1723,8 +1744,9 @@ void Sim<R>::demStep() {
     }
     else if (!(nc <= sweepClusterEntries_ &&
                launchCluster(kSweepLoop<R, 2, 3, true>, d_, (const int*)cOrder_.p, (const int*)cOff_.p, ncolP,
-                             posIters_, sp, posTol, gb)))
-      launchCoop(kSweepLoop<R, 2, 3>, d_, (const int*)cOrder_.p, (const int*)cOff_.p, ncolP, posIters_, sp, posTol, gb);
+                             posIters_, sp, posTol, gb, PgsRecs<R>{})))
+      launchCoop(kSweepLoop<R, 2, 3>, d_, (const int*)cOrder_.p, (const int*)cOff_.p, ncolP, posIters_, sp, posTol, gb,
+                 PgsRecs<R>{});
     KCHECK("position loop");
   }
   const bool posEmpty = useGS_ && posLeft == 0 && ncolP <= 0 && posIters_ > 0 && posTol > R(0);

@@ -380,6 +380,12 @@ class Sim {
   template <class K, class... A>
   bool launchCluster(K kernel, A... args);
   std::map<const void*, int> clusterOk_;  // per kernel: 1 resident, 0 not
+  // velocity-sweep records of the one-cluster loops (kPackPgs), packed once per substep
+  PgsRecs<R> packPgs(int nm, int ncol);
+  DBuf<Q4<R>> pgsQ_;
+  DBuf<int4> pgsIds_;
+  long pgsCap_ = 0;
+  long substepId_ = 0, pgsPackedAt_ = -1;
   // blocks of the one-cluster sweep loop (PDEM_SWEEP_CLUSTER: 8, the portable size, or 16, which
   // needs the non-portable cluster attribute) and the largest entry list it takes
   // (PDEM_SWEEP_CLUSTER_ENTRIES); larger lists sweep on the cooperative grid

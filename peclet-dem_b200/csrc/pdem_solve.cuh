@@ -361,20 +361,114 @@ __device__ __forceinline__ void loopMax(const Dev<R>& d, int s, bool position, R
     runMax(mx, v);
 }
 
-template <class R, bool LOCAL = false>
-__device__ __forceinline__ void pgsOne(const Dev<R>& d, int idx, const SolveP<R>& P, R& mx, int loop) {
-  int sc = 0;
-  R eG = P.eN, muG = P.mu;
-  if (d.scn) {
-    sc = d.sceneOf[d.mab[idx].x];
-    if (sceneDone(d, sc, loop))
-      return;
-    eG = d.scn[sc].eN;
-    muG = d.scn[sc].mu;
-  }
+// The per-substep constants of one manifold in the coloured velocity sweeps: its bodies' inverse
+// masses, inverse inertias and orientations (fixed while the velocity solve runs), its averaged
+// normal, lever arms, wall velocity, restitution and friction, and the normal's generalized inverse
+// masses. Every value is the expression the sweep evaluates, so reading them from a record packed
+// once per substep gives the same bits as recomputing them every sweep.
+template <class R>
+struct PgsStatic {
+  int ra, rb;
+  bool hasB;
+  R imA, imB;
+  V3<R> iIA, iIB;
+  Q4<R> qA, qB;
+  V3<R> N, TA, TB, rAa, rBa, dc, wvN;
+  R eAvg, muAvg, lenN, Nsq, wAn0, wBn0;
+};
+template <class R>
+__device__ __forceinline__ PgsStatic<R> pgsStatic(const Dev<R>& d, int idx) {
   const ManifoldView<R> v = loadManifold(d, idx);
+  PgsStatic<R> s;
+  s.ra = v.ra;
+  s.rb = v.rb;
+  s.hasB = d.mab[idx].y >= 0;
+  s.imA = v.imA;
+  s.imB = v.imB;
+  s.iIA = v.iIA;
+  s.iIB = v.iIB;
+  s.qA = v.qA;
+  s.qB = v.qB;
+  s.N = v.N;
+  s.TA = v.TA;
+  s.TB = v.TB;
+  s.rAa = v.rAa;
+  s.rBa = v.rBa;
+  s.dc = v.dc;
+  s.wvN = mul(v.wv, v.invN);
+  s.eAvg = v.eSum * v.invN;
+  s.muAvg = v.muSum * v.invN;
+  s.Nsq = dot(v.N, v.N);
+  s.lenN = sqrt(s.Nsq);
+  s.wAn0 = s.Nsq * v.imA + genInvMass(v.TA, v.iIA, v.qA);
+  s.wBn0 = s.Nsq * v.imB + genInvMass(v.TB, v.iIB, v.qB);
+  return s;
+}
+// The records of a colour-ordered manifold list (PgsRecs), slot-major (slot k of entry t at
+// q[k * cap + t]): 0 (N, lenN), 1 (TA, Nsq), 2 (TB, wAn0), 3 (dc, wBn0), 4 (rAa, imA), 5 (rBa, imB),
+// 6 (wvN, eAvg), 7 (iIA, muAvg), 8 (iIB, 0), 9 qA, 10 qB; ids (manifold, ra, rb, hasB). A sweep
+// reads its entry's record with coalesced loads, then only the bodies' velocities depend on it.
+// Entries [0, coff[ncol]) of the colour order: the coloured manifolds.
+template <class R>
+__global__ void kPackPgs(Dev<R> d, const int* order, const int* coff, int ncol, PgsRecs<R> r) {
+  const long n = coff[ncol];
+  GRID_STRIDE(t, n) {
+    const int idx = order[t];
+    const PgsStatic<R> s = pgsStatic(d, idx);
+    const long c = r.cap;
+    r.q[t] = Q4<R>{s.N.x, s.N.y, s.N.z, s.lenN};
+    r.q[c + t] = Q4<R>{s.TA.x, s.TA.y, s.TA.z, s.Nsq};
+    r.q[2 * c + t] = Q4<R>{s.TB.x, s.TB.y, s.TB.z, s.wAn0};
+    r.q[3 * c + t] = Q4<R>{s.dc.x, s.dc.y, s.dc.z, s.wBn0};
+    r.q[4 * c + t] = Q4<R>{s.rAa.x, s.rAa.y, s.rAa.z, s.imA};
+    r.q[5 * c + t] = Q4<R>{s.rBa.x, s.rBa.y, s.rBa.z, s.imB};
+    r.q[6 * c + t] = Q4<R>{s.wvN.x, s.wvN.y, s.wvN.z, s.eAvg};
+    r.q[7 * c + t] = Q4<R>{s.iIA.x, s.iIA.y, s.iIA.z, s.muAvg};
+    r.q[8 * c + t] = Q4<R>{s.iIB.x, s.iIB.y, s.iIB.z, R(0)};
+    r.q[9 * c + t] = s.qA;
+    r.q[10 * c + t] = s.qB;
+    r.ids[t] = make_int4(idx, s.ra, s.rb, s.hasB ? 1 : 0);
+  }
+}
+template <class R>
+__device__ __forceinline__ PgsStatic<R> pgsRecord(const PgsRecs<R>& r, long t, int& idx) {
+  const long c = r.cap;
+  const int4 id = r.ids[t];
+  const Q4<R> a = r.q[t], b = r.q[c + t], e = r.q[2 * c + t], f = r.q[3 * c + t], g = r.q[4 * c + t],
+              h = r.q[5 * c + t], w = r.q[6 * c + t], ia = r.q[7 * c + t], ib = r.q[8 * c + t];
+  PgsStatic<R> s;
+  idx = id.x;
+  s.ra = id.y;
+  s.rb = id.z;
+  s.hasB = id.w != 0;
+  s.N = v3(a);
+  s.lenN = a.w;
+  s.TA = v3(b);
+  s.Nsq = b.w;
+  s.TB = v3(e);
+  s.wAn0 = e.w;
+  s.dc = v3(f);
+  s.wBn0 = f.w;
+  s.rAa = v3(g);
+  s.imA = g.w;
+  s.rBa = v3(h);
+  s.imB = h.w;
+  s.wvN = v3(w);
+  s.eAvg = w.w;
+  s.iIA = v3(ia);
+  s.muAvg = ia.w;
+  s.iIB = v3(ib);
+  s.qA = r.q[9 * c + t];
+  s.qB = r.q[10 * c + t];
+  return s;
+}
+
+// one projected Gauss-Seidel update of manifold idx from its per-substep constants v
+template <class R, bool LOCAL = false>
+__device__ __forceinline__ void pgsCore(const Dev<R>& d, int idx, const PgsStatic<R>& v, R eG, R muG, int sc,
+                                        const SolveP<R>& P, R& mx) {
   const int ra = v.ra, rb = v.rb;
-  const bool hasB = d.mab[idx].y >= 0;
+  const bool hasB = v.hasB;
   const V3<R> vA = v3(d.velPred[ra]), wA = v3(d.angVelPred[ra]);
   V3<R> vB{0, 0, 0}, wB{0, 0, 0};
   R e = eG;
@@ -382,14 +476,11 @@ __device__ __forceinline__ void pgsOne(const Dev<R>& d, int idx, const SolveP<R>
     vB = v3(d.velPred[rb]);
     wB = v3(d.angVelPred[rb]);
   } else {
-    vB = mul(v.wv, v.invN);
+    vB = v.wvN;
   }
-  {
-    const R ra2 = v.eSum * v.invN;
-    if (ra2 >= R(0))
-      e = ra2;
-  }
-  const R lenN = sqrt(dot(v.N, v.N));
+  if (v.eAvg >= R(0))
+    e = v.eAvg;
+  const R lenN = v.lenN;
   if (lenN < R(1e-9))
     return;
   const V3<R> vG = mul(v.dc, P.growthRate);
@@ -397,9 +488,8 @@ __device__ __forceinline__ void pgsOne(const Dev<R>& d, int idx, const SolveP<R>
   vn += dot(vG, v.N);
   const R al = dot(v.N, v.dc);
   const R sgn = (al > R(0)) ? R(1) : R(-1);
-  const R Nsq = dot(v.N, v.N);
-  R wAn = Nsq * v.imA + genInvMass(v.TA, v.iIA, v.qA);
-  R wBn = Nsq * v.imB + genInvMass(v.TB, v.iIB, v.qB);
+  R wAn = v.wAn0;
+  R wBn = v.wBn0;
   bool applyA = true, applyB = true;
   const uint8_t sf = d.sideFlags[idx];
   if (sf == 1) {
@@ -443,14 +533,13 @@ __device__ __forceinline__ void pgsOne(const Dev<R>& d, int idx, const SolveP<R>
   }
   // friction cone
   R mu = muG;
-  const R fa = v.muSum * v.invN;
-  if (fa >= R(0))
-    mu = fa;
+  if (v.muAvg >= R(0))
+    mu = v.muAvg;
   const V3<R> ltOld = v3(d.lambdaT[idx]);
   const bool haveOld = nonzero(ltOld);
   if (mu > R(0) || haveOld) {
     const V3<R> nh = mul(v.N, R(1) / lenN);
-    const V3<R> vBf = hasB ? vB2 : mul(v.wv, v.invN);
+    const V3<R> vBf = hasB ? vB2 : v.wvN;
     const V3<R> wBf = hasB ? wB2 : V3<R>{0, 0, 0};
     const V3<R> vr = sub(add(vA2, cross(wA2, v.rAa)), add(vBf, cross(wBf, v.rBa)));
     const V3<R> vtv = sub(vr, mul(nh, dot(vr, nh)));
@@ -504,6 +593,20 @@ __device__ __forceinline__ void pgsOne(const Dev<R>& d, int idx, const SolveP<R>
     d.velPred[rb] = q4(vB2);
     d.angVelPred[rb] = q4(wB2);
   }
+}
+
+template <class R, bool LOCAL = false>
+__device__ __forceinline__ void pgsOne(const Dev<R>& d, int idx, const SolveP<R>& P, R& mx, int loop) {
+  int sc = 0;
+  R eG = P.eN, muG = P.mu;
+  if (d.scn) {
+    sc = d.sceneOf[d.mab[idx].x];
+    if (sceneDone(d, sc, loop))
+      return;
+    eG = d.scn[sc].eN;
+    muG = d.scn[sc].mu;
+  }
+  pgsCore<R, LOCAL>(d, idx, pgsStatic(d, idx), eG, muG, sc, P, mx);
 }
 template <class R>
 __global__ void kPGSColor(Dev<R> d, const int* order, const int* coff, int color, SolveP<R> P, int gate) {
