@@ -171,6 +171,11 @@ long pdem_debug_pos_lambda(pdem_handle h, double* out, long cap);
 long pdem_debug_hertz(pdem_handle h, unsigned long long* keys, double* xi, long cap);
 /* test hook: set the contact buffer capacity (overflow / clamp behaviour) */
 int pdem_debug_set_max_contacts(pdem_handle h, int max_contacts);
+/* test hook: polls before a grid-wide barrier wait of the persistent loops gives up (<= 0: the
+ * default, seconds of waiting). A wait that gives up sets an error bit; the kernel returns, the
+ * step reports PDEM_ERR_CUDA at its next read-back and clears the bit; the substep's state is then
+ * partial and the caller sets the bodies' state again. Lets a test make the wait run out. */
+int pdem_debug_set_barrier_spins(pdem_handle h, long spins);
 
 /* ---- batched form (no reference counterpart: the reference steps one scene per Simulation) ----
  * Several independent scenes share one simulation: scene s owns the bodies

@@ -566,6 +566,7 @@ long pdem_debug_hertz(pdem_handle h, unsigned long long* keys, double* xi, long 
   return n;
 }
 int pdem_debug_set_max_contacts(pdem_handle h, int n) { BODY(S.setMaxContacts(n)); }
+int pdem_debug_set_barrier_spins(pdem_handle h, long spins) { BODY(S.setBarrierSpins(spins)); }
 
 // ---- batched form ----
 int pdem_set_scenes(pdem_handle h, int nscenes, const int* first_body) {

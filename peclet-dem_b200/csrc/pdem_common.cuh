@@ -71,6 +71,10 @@ struct SceneCtl {
   int velSweeps, stabSweeps, posSweeps, pad2;
 };
 
+// polls before a grid-barrier wait of a persistent loop gives up (seconds at any back-off: each
+// poll is an L2 round trip)
+constexpr long kBarrierSpins = 1L << 26;
+
 // colour-ordered records of the coloured velocity sweeps (layout and packing in pdem_solve.cuh,
 // kPackPgs): kPgsSlots slots of 4 values per entry, slot-major, and the entry's ids
 constexpr int kPgsSlots = 11;

@@ -925,6 +925,101 @@ __global__ void kGroundSweeps(int nm, int numReal, int sweeps, const int4* edges
   extern __shared__ int slvl[];
   groundSweepsWarp(nm, 0, numReal, sweeps, edges, grounded, useShared ? slvl : gscratch);
 }
+// The same support levels from the least fixed point, in parallel. The serial sweeps only raise
+// levels, each raise is an edge relaxation (wall: 255; support: the source's level - 1 when
+// positive), so they climb towards the least fixed point F above the decayed levels L0, the same
+// whatever the order of relaxations; when they reach F within `sweeps` sweeps, their result is F.
+// One block (a) computes F by parallel relaxation passes, (b) finds, for every body, the sweep in
+// which the serial order first gives it F: a body at L0 = F before sweep 1; otherwise the earliest
+// (sweep, edge) over the edges that deliver F, where a support edge e from u delivers in u's sweep
+// if e comes after the edge that finished u, else in the next sweep (a shortest-path relaxation on
+// that acyclic edge set: F drops by one along it). (c) If every body is final within `sweeps`
+// sweeps the levels are F; otherwise warp 0 runs the exact serial sweeps from L0 (still in
+// `grounded`). Shared memory: the times (8 bytes a body), the edges (8 bytes each: kind in the top
+// bits of the source, then the destination) and the levels (4 bytes a body).
+constexpr int kGroundBlock = 1024;
+constexpr int kGroundPassCap = 4096;  // relaxation passes before the exact serial sweeps take over
+__global__ void __launch_bounds__(kGroundBlock) kGroundLevels(int nm, int nb, int sweeps, const int4* edges,
+                                                              uint8_t* grounded) {
+  extern __shared__ __align__(16) unsigned char gsm[];
+  using ull = unsigned long long;
+  ull* T = reinterpret_cast<ull*>(gsm);
+  int2* E = reinterpret_cast<int2*>(T + nb);
+  int* L = reinterpret_cast<int*>(E + nm);
+  volatile int* VL = L;
+  volatile ull* VT = T;
+  const int tid = threadIdx.x;
+  for (int i = tid; i < nb; i += blockDim.x)
+    L[i] = grounded[i];
+  for (int e = tid; e < nm; e += blockDim.x) {
+    const int4 g = edges[e];
+    E[e] = make_int2((int)(((unsigned)g.x << 30) | (unsigned)g.y), g.z);
+  }
+  __syncthreads();
+  // every thread walks a contiguous run of edges in index order
+  const int per = (nm + (int)blockDim.x - 1) / (int)blockDim.x;
+  const int e0 = min(nm, tid * per), e1 = min(nm, e0 + per);
+  bool fast = true;
+  for (int pass = 0;; ++pass) {  // (a) F
+    int ch = 0;
+    for (int e = e0; e < e1; ++e) {
+      const int2 g = E[e];
+      const int kind = (int)((unsigned)g.x >> 30), src = g.x & 0x3fffffff, dst = g.y;
+      const int c = kind == 1 ? 255 : (kind == 2 ? VL[src] - 1 : 0);
+      if (c > 0 && c > VL[dst]) {
+        atomicMax(&L[dst], c);
+        ch = 1;
+      }
+    }
+    if (!__syncthreads_or(ch))
+      break;
+    if (pass + 1 >= kGroundPassCap) {
+      fast = false;
+      break;
+    }
+  }
+  const ull kInf = ~0ull, kStart = 1ull << 32;  // (sweep << 32) | (edge + 1); 1 << 32: final before sweep 1
+  for (int i = tid; i < nb; i += blockDim.x)
+    T[i] = L[i] == (int)grounded[i] ? kStart : kInf;
+  __syncthreads();
+  for (int pass = 0; fast; ++pass) {  // (b) the sweep in which each body becomes final
+    int ch = 0;
+    for (int e = e0; e < e1; ++e) {
+      const int2 g = E[e];
+      const int kind = (int)((unsigned)g.x >> 30), src = g.x & 0x3fffffff, dst = g.y;
+      ull te = kInf;
+      if (kind == 1 && VL[dst] == 255) {
+        te = kStart | (ull)(e + 1);
+      } else if (kind == 2 && VL[dst] > 0 && VL[src] - 1 == VL[dst]) {
+        const ull tu = VT[src];
+        if (tu != kInf) {
+          const ull ku = tu >> 32;
+          const long iu = (long)(tu & 0xffffffffull) - 1;
+          te = (((long)e > iu ? ku : ku + 1) << 32) | (ull)(e + 1);
+        }
+      }
+      if (te < VT[dst]) {
+        atomicMin(&T[dst], te);
+        ch = 1;
+      }
+    }
+    if (!__syncthreads_or(ch))
+      break;
+    if (pass + 1 >= kGroundPassCap)
+      fast = false;
+  }
+  int late = !fast;
+  for (int i = tid; i < nb && !late; i += blockDim.x)
+    late = T[i] == kInf || (T[i] >> 32) > (ull)sweeps;
+  late = __syncthreads_or(late);
+  if (!late) {  // (c)
+    for (int i = tid; i < nb; i += blockDim.x)
+      grounded[i] = (uint8_t)L[i];
+    return;
+  }
+  if (tid < 32)
+    groundSweepsWarp(nm, 0, nb, sweeps, edges, grounded, L);
+}
 // batched form: one warp (block) per scene over its own edge range manFirst[s..s+1) and bodies
 // bodyFirst[s..s+1): the sweeps of independent scenes are independent, and each stops on its own
 __global__ void kGroundSweepsScenes(const int* manFirst, const int* bodyFirst, int sweeps, const int4* edges,

@@ -10,16 +10,16 @@
 
 namespace pdem {
 
-// polls before a barrier wait gives up (seconds at any back-off: each poll is an L2 round trip)
-constexpr long kBarrierSpins = 1L << 26;
 constexpr int kErrBarrier = 2;  // Counters::err bit: a grid barrier timed out
 
 // word[0] = arrivals, word[1] = generation; both zero before the launch; sleepNs = the back-off
-// of a waiting block between polls of the generation
+// of a waiting block between polls of the generation; spins = the polls before a wait gives up
+// (kBarrierSpins unless a test shortens it to make the wait run out)
 struct GridBar {
   unsigned* word;
   int* err;
   unsigned sleepNs;
+  long spins;
 };
 
 // Grid-wide barrier of a cooperative launch (all blocks co-resident). Thread 0 of each block
@@ -42,7 +42,7 @@ __device__ __forceinline__ bool gridBarrier(const GridBar& gb) {
     } else {
       long spins = 0;
       while (*gen == g) {
-        if (++spins > kBarrierSpins) {
+        if (++spins > gb.spins) {
           atomicOr(gb.err, kErrBarrier);
           ok = 0;
           break;

@@ -222,13 +222,23 @@ void Sim<R>::readBack(void* host, const void* dev, size_t bytes) {
   pending_.push_back({host, off, bytes});
   pinOff_ = off + bytes;
 }
+// a timed-out barrier has been reported: clear its error bit so the next substep starts clean (the
+// barrier words are zeroed before every cooperative launch)
+template <class R>
+void Sim<R>::clearLoopError() {
+  dropPending();
+  cudaCheck(cudaMemsetAsync(&ctr_.p->err, 0, sizeof(int), stream_), "memset error bits");
+  sync();
+}
 template <class R>
 Counters<R> Sim<R>::readCounters() {
   Counters<R> c;
   readBack(&c, ctr_.p, sizeof c);
   sync();
-  if (c.err & kErrBarrier)
+  if (c.err & kErrBarrier) {
+    clearLoopError();
     throw CudaError("a grid-wide barrier of a persistent loop timed out (blocks not co-resident)");
+  }
   return c;
 }
 
@@ -1162,8 +1172,10 @@ void Sim<R>::detectAll(R margin) {
   readBack(&tot[2], cntW + nr, sizeof(int));
   readBack(&c, ctr_.p, sizeof c);
   sync();
-  if (c.err & kErrBarrier)
+  if (c.err & kErrBarrier) {
+    clearLoopError();
     throw CudaError("a grid-wide barrier of a persistent loop timed out (blocks not co-resident)");
+  }
   if (np > 0 && tot[0] > 0) {
     if (shell)
       ++launches_, kNarrowShell<R, 1><<<gridFor((long)np * 32), kBlock, 0, stream_>>>(d_, np, P, nullptr, iB_.p);
@@ -1333,7 +1345,7 @@ void Sim<R>::colorBoth(int nm, int nc, int& ncolV, int& velLeft, int& ncolP, int
     }
   }
   gbar_.ensure(2, false, stream_);
-  const GridBar gb{gbar_.p, &ctr_.p->err, barrierSleepNs_};
+  const GridBar gb{gbar_.p, &ctr_.p->err, barrierSleepNs_, barrierSpins_};
   // the tail in shared memory when the hand-over fits its tables
   const bool tailShared = std::min(colorTailAt_, kColorTailMax) <= kTailShEntries;
   jm.tailShared = jc.tailShared = tailShared ? 1 : 0;
@@ -1349,8 +1361,10 @@ void Sim<R>::colorBoth(int nm, int nc, int& ncolV, int& velLeft, int& ncolP, int
   keptM_ = topoValid_ && differ[1] == 0;
   reuse_[1] += keptC_ ? 1 : 0;
   reuse_[2] += keptM_ ? 1 : 0;
-  if (err & kErrBarrier)
+  if (err & kErrBarrier) {
+    clearLoopError();
     throw CudaError("colouring: a grid-wide barrier timed out");
+  }
   if (neM > 0) {
     ncolV = res[3] + 1;
     velLeft = res[4];
@@ -1526,7 +1540,7 @@ void Sim<R>::demStep() {
   const bool velPersistent = useGS_ && !legacyFriction && velLeft == 0 && ncolV > 0 && velIters_ > 0;
   if (velPersistent) {
     gbar_.ensure(2, false, s);
-    const GridBar gb{gbar_.p, &ctr_.p->err, barrierSleepNs_};
+    const GridBar gb{gbar_.p, &ctr_.p->err, barrierSleepNs_, barrierSpins_};
     const R thr = usePGS ? R(0.02) * vRest : vRest;
     ctl(CTL_VEL_BEGIN, R(0), 0);
     if (batch_)
@@ -1631,7 +1645,7 @@ void Sim<R>::demStep() {
       const bool stabPersistent = ncolV > 0;
       if (stabPersistent) {
         gbar_.ensure(2, false, s);
-        const GridBar gb{gbar_.p, &ctr_.p->err, barrierSleepNs_};
+        const GridBar gb{gbar_.p, &ctr_.p->err, barrierSleepNs_, barrierSpins_};
         ctl(CTL_STAB_BEGIN, R(0), 0);
         if (batch_)
           ++launches_, kSweepScenes<R, 0, 2><<<numScenes_, sceneBlock(), 0, s>>>(d_, sceneLpt_.p, mOrder_.p, mOff_.p, iters, ss, vRestS);
@@ -1736,7 +1750,7 @@ void Sim<R>::demStep() {
   const bool posPersistent = useGS_ && posLeft == 0 && ncolP > 0 && posIters_ > 0;
   if (posPersistent) {
     gbar_.ensure(2, false, s);
-    const GridBar gb{gbar_.p, &ctr_.p->err, barrierSleepNs_};
+    const GridBar gb{gbar_.p, &ctr_.p->err, barrierSleepNs_, barrierSpins_};
     ctl(CTL_POS_BEGIN, R(0), 0);
     if (batch_) {
       ++launches_, kSweepScenes<R, 2, 3><<<numScenes_, sceneBlock(), 0, s>>>(d_, sceneLpt_.p, cOrder_.p, cOff_.p, posIters_, sp, posTol);
@@ -2347,6 +2361,7 @@ void Sim<R>::ensureGrounded() {
   if (!attr) {
     cudaFuncSetAttribute(kGroundSweeps, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     cudaFuncSetAttribute(kGroundSweepsScenes, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(kGroundLevels, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     attr = true;
   }
   for (long e = start; e < gLog_; ++e) {
@@ -2362,6 +2377,9 @@ void Sim<R>::ensureGrounded() {
         gscratch_.ensure(nr, false, stream_);
       ++launches_, kGroundSweepsScenes<<<S, 32, smem ? maxSceneBodies_ * sizeof(int) : 0, stream_>>>(
           gRingScn_[slot].p, sceneFirstD_.p, 8, gRing_[slot].p, grounded_.p, gscratch_.p, smem);
+    } else if (nm > 0 && (size_t)nr * 12 + (size_t)nm * 8 <= 200 * 1024 && nr < (1 << 30)) {
+      ++launches_, kGroundLevels<<<1, kGroundBlock, (size_t)nr * 12 + (size_t)nm * 8, stream_>>>(
+          nm, nr, 8, gRing_[slot].p, grounded_.p);
     } else if (nm > 0) {
       const bool smem = (size_t)nr * sizeof(int) <= 200 * 1024;
       if (!smem)

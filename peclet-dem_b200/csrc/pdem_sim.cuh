@@ -452,6 +452,12 @@ class Sim {
   }();
   // back-off (ns) between polls of a waiting block at a grid barrier; PDEM_BARRIER_SLEEP_NS
   // overrides it
+  // polls before a grid-barrier wait gives up (setBarrierSpins; <= 0 restores kBarrierSpins)
+  long barrierSpins_ = kBarrierSpins;
+ public:
+  void setBarrierSpins(long n) { barrierSpins_ = n > 0 ? n : kBarrierSpins; }
+ private:
+  void clearLoopError();
   unsigned barrierSleepNs_ = [] {
     const char* e = std::getenv("PDEM_BARRIER_SLEEP_NS");
     return e ? (unsigned)std::strtoul(e, nullptr, 10) : 64u;

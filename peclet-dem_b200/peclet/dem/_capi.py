@@ -105,6 +105,7 @@ _SIGS = {
     "debug_pos_lambda": (C.c_long, [_vp, _dbl_p, C.c_long]),
     "debug_hertz": (C.c_long, [_vp, _u64_p, _dbl_p, C.c_long]),
     "debug_set_max_contacts": (C.c_int, [_vp, C.c_int]),
+    "debug_set_barrier_spins": (C.c_int, [_vp, C.c_long]),
     # instrumentation
     "profile_enable": (C.c_int, [_vp, C.c_int]),
     "profile_read": (C.c_int, [_vp, _dbl_p, _long_p, C.c_int, _long_p]),
@@ -667,6 +668,10 @@ class CApiSimulation:
 
     def debug_set_max_contacts(self, n):
         self._call("debug_set_max_contacts", int(n))
+
+    def debug_set_barrier_spins(self, n):
+        """Polls before a grid-barrier wait of the persistent loops gives up (0: the default)."""
+        self._call("debug_set_barrier_spins", int(n))
 
     # ---- instrumentation -------------------------------------------------------------------------
     def profile_enable(self, on=True):

@@ -89,6 +89,7 @@ MATRIX = [
     ("pair_materials", lambda: S.dense_spheres(), _mats, 6),
     ("walton_beta", lambda: S.dense_spheres(), lambda s: s.set_material_params(0.5, 0.3, 0.5), 6),
     ("grid_sdf_capsules", lambda: S.sdf_capsules(), None, 8),
+    ("reversed_column", lambda: S.reversed_column(), None, 40),
     ("ordered_column", lambda: S.settled_column(), lambda s: s.set_stabilization_mode("ordered"), 25),
     ("ordered_dense", lambda: S.dense_spheres(), lambda s: s.set_stabilization_mode("ordered"), 8),
 ]

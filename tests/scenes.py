@@ -38,6 +38,18 @@ def settled_column(seed=12, nx=5, ny=5, nz=12, iters=(10, 10)):
     return sc
 
 
+def reversed_column(seed=12, nx=3, ny=3, nz=24):
+    """A tall lattice column numbered top to bottom: every support chain runs against the
+    manifold order, so the serial support-level sweeps move one level a sweep and stop short of
+    the fixed point (the exact-sweep path of the support levels)."""
+    sc = settled_column(seed=seed, nx=nx, ny=ny, nz=nz)
+    r = slice(None, None, -1)
+    sc.pos, sc.vel = sc.pos[r].copy(), sc.vel[r].copy()
+    sc.inv_mass, sc.inv_inertia = sc.inv_mass[r].copy(), sc.inv_inertia[r].copy()
+    sc.name = "reversed_column"
+    return sc
+
+
 def polydisperse_periodic(seed=13, n=250, L=8e-3, H=6e-3, radius=1e-3):
     """Polydisperse spheres in a box periodic in x and y with a floor plane (ghost images)."""
     rng = np.random.default_rng(seed)

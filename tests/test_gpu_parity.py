@@ -156,3 +156,38 @@ def test_colouring_tail_settings(tail):
                        cwd=root, env={**os.environ, "PDEM_COLOR_TAIL": tail}, capture_output=True, text=True)
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
     assert "5 passed" in r.stdout, r.stdout[-500:]
+
+
+def _restore_bodies(sim, sc):
+    """Set the scene's per-body state again (as Scene.apply orders the setters)."""
+    sim.set_positions(sc.pos)
+    if sc.quat is not None:
+        sim.set_quaternions(sc.quat)
+    if sc.scales is not None:
+        sim.set_scales(sc.scales)
+    sim.set_velocities(sc.vel)
+    sim.set_inv_mass(sc.inv_mass)
+    sim.set_inv_inertia(sc.inv_inertia)
+
+
+def test_grid_barrier_time_out_reports_and_recovers(gpu_api, orc_api, monkeypatch):
+    """A grid-wide barrier wait of the persistent loops that runs out (its poll limit cut to one)
+    makes the kernel return and the step report an error, leaving the device usable; with the
+    default limit restored and the bodies' state set again, the next substeps match the oracle."""
+    import scenes as S
+    monkeypatch.setenv("PDEM_SWEEP_CLUSTER_ENTRIES", "0")  # every sweep loop on the cooperative grid
+    sc = S.dense_spheres()
+    sim = P.build(gpu_api, sc, None, "fp64")
+    sim.debug_set_barrier_spins(1)
+    with pytest.raises(RuntimeError, match="barrier"):
+        for _ in range(3):
+            sim.step(sc.dt)
+    sim.debug_set_barrier_spins(0)
+    _restore_bodies(sim, sc)
+    ref = P.build(orc_api, sc, None, "fp64")
+    for k in range(4):
+        sim.step(sc.dt)
+        ref.step(sc.dt)
+        bad = P.diff(P.snapshot(sim), P.snapshot(ref), rtol=1e-12)
+        assert not bad, f"after the time-out, substep {k}: {bad[:4]}"
+    assert sim.counters()["status"] == 0

@@ -88,3 +88,63 @@ def test_static_pairs_capacity_and_limits(gpu_api):
                                          ctypes.c_void_p(1), 0, ctypes.byref(count), None)
     assert st == 2
     assert str(MAX_BODIES) in gpu_api.error()
+
+
+def _brute_pairs(pos, radius, margin, box_cap):
+    """The closed-box predicate of the broadphase over all i < j, with the parking rule: a body
+    whose padded half-width b = r + margin or position is not finite, or whose b exceeds box_cap,
+    sits at (-1e30)^3 with b = 0 (parked bodies meet only each other)."""
+    x = np.array(pos, np.float64)
+    b = np.asarray(radius, np.float64) + margin
+    park = ~np.isfinite(b) | np.any(np.isnan(x), axis=1) | ((box_cap > 0) & (b > box_cap))
+    x[park] = -1.0e30
+    b = np.where(park, 0.0, b)
+    lo, hi = x - b[:, None], x + b[:, None]
+    out = []
+    for i in range(x.shape[0] - 1):
+        ok = np.all((lo[i] <= hi[i + 1:]) & (lo[i + 1:] <= hi[i]), axis=1)
+        out.extend((i, i + 1 + j) for j in np.nonzero(ok)[0])
+    return np.array(out, dtype=np.int32).reshape(-1, 2)
+
+
+def test_static_pairs_at_the_limit_parked_bodies_and_no_allocation(gpu_api):
+    """16,384 bodies (the fixed limit) with non-finite and oversized radii and a non-finite position
+    among them, then 9,000 bodies, called back to back: each list equals the brute-force predicate
+    with the parking rule. After a first call, further calls leave this library's allocation count
+    and the device's free memory unchanged."""
+    import torch
+    rng = np.random.default_rng(77)
+    cases = []
+    for n, L in ((MAX_BODIES, 60e-3), (9000, 50e-3)):
+        pos = rng.uniform(0.0, L, (n, 3))
+        radius = rng.uniform(0.5e-3, 1.5e-3, n)
+        radius[rng.choice(n, 5, replace=False)] = np.nan
+        radius[rng.choice(n, 3, replace=False)] = np.inf
+        radius[rng.choice(n, 4, replace=False)] = 0.5  # far above box_cap
+        pos[rng.choice(n, 2, replace=False), 1] = np.nan
+        cases.append((pos, radius, 0.15e-3, 0.05))
+    want = [_brute_pairs(*c) for c in cases]
+    # every device array the calls use is made before the allocation baseline
+    dev = [(torch.as_tensor(p, device="cuda"), torch.as_tensor(r, device="cuda"),
+            torch.full((4 * w.shape[0] + 16, 2), -1, dtype=torch.int32, device="cuda")) for (p, r, _, _), w in zip(cases, want)]
+    stream = torch.cuda.current_stream().cuda_stream
+
+    def call(k):
+        (p, r, m, cap), (dp, dr, do) = cases[k], dev[k]
+        count = ctypes.c_long(-1)
+        st = gpu_api.fn["find_pairs_static"](ctypes.c_void_p(dp.data_ptr()), ctypes.c_void_p(dr.data_ptr()), p.shape[0],
+                                             m, cap, ctypes.c_void_p(do.data_ptr()), do.shape[0], ctypes.byref(count),
+                                             ctypes.c_void_p(stream))
+        torch.cuda.synchronize()
+        assert st == 0, gpu_api.error()
+        return count.value, do[: count.value].cpu().numpy()
+
+    call(1)  # set-up call
+    torch.cuda.synchronize()
+    allocs0, free0 = gpu_api.fn["debug_allocs"](), torch.cuda.mem_get_info()[0]
+    for k in (0, 1, 0):
+        n, got = call(k)
+        assert n == want[k].shape[0]
+        np.testing.assert_array_equal(got, want[k])
+    assert gpu_api.fn["debug_allocs"]() == allocs0
+    assert torch.cuda.mem_get_info()[0] == free0
