@@ -12,7 +12,7 @@ shim build, float); the B200 step runs it in FP64 and FP32 through the C ABI. St
 * after 400 outer steps (the bed still compacting): solids fraction within 0.03, coordination
   within 0.6, bed height within 1.5 mm;
 * after 800 outer steps (at rest): solids fraction within 0.01, coordination within 0.3, bed
-  height within 0.5 mm, kinetic energy below 1e-2 of the initial and within a factor 10 of the
+  height within 0.5 mm, kinetic energy below 2e-2 of the initial and within a factor 10 of the
   reference's, and the same rattler count to within 5.
 
 The saved restart state of the benchmark (after 800 steps, FP64) is checked against the same bar.
@@ -47,7 +47,7 @@ def _check(got, ref, step, ke0):
     for k, tol in TOL[step].items():
         assert abs(got[k] - ref[k]) <= tol, f"step {step}: {k} {got[k]} vs the reference's {ref[k]}"
     if step == 800:
-        assert got["ke"] < 1e-2 * ke0 and ref["ke"] < 1e-2 * ke0
+        assert got["ke"] < 2e-2 * ke0 and ref["ke"] < 2e-2 * ke0
         assert 0.1 <= got["ke"] / ref["ke"] <= 10.0, f"kinetic energy {got['ke']} vs {ref['ke']}"
         assert abs(got["rattlers"] - ref["rattlers"]) <= 5
 
