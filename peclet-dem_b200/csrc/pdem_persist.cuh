@@ -719,10 +719,12 @@ __device__ void colorTailShared(const Dev<R>& d, const ColorJob& jm, const Color
   }
 }
 
-// job 0: manifolds over real bodies (skipped when ne = 0), job 1: contacts over body slots
+// job 0: manifolds over real bodies (skipped when ne = 0), job 1: contacts over body slots.
+// CLUSTER: the launch is one thread-block cluster (graphs of a few tens of thousands of entries)
+// and the hardware cluster barrier replaces the grid-wide one, as in kSweepLoop.
 // reuse: a graph equal to the previous substep's keeps its colours and statistics (differ[0]: the
 // contact list changed, differ[1]: the manifold list changed; reuse = 0 forces both colourings)
-template <class R>
+template <class R, bool CLUSTER = false>
 __global__ void __launch_bounds__(kColorBlock) kColorBoth(Dev<R> d, ColorJob jm, ColorJob jc, int maxRounds,
                                                           GridBar gb, const int* differ, int reuse) {
   __shared__ int sCount[2][2];  // per job: this block's loser counts, ping-pong by round
@@ -737,7 +739,7 @@ __global__ void __launch_bounds__(kColorBlock) kColorBoth(Dev<R> d, ColorJob jm,
   colorInit<R, false>(d, jc, gtid, gstride);
   if (threadIdx.x < 4)
     sCount[threadIdx.x >> 1][threadIdx.x & 1] = 0;
-  if (!gridBarrier(gb))
+  if (!loopBarrier<CLUSTER>(gb))
     return;
   int prevM = -1, prevC = -1;
   bool doneM = jm.ne <= 0, doneC = jc.ne <= 0;
@@ -750,7 +752,7 @@ __global__ void __launch_bounds__(kColorBlock) kColorBoth(Dev<R> d, ColorJob jm,
       colorContend<R, true>(d, jm, round, rm);
     if (!doneC)
       colorContend<R, false>(d, jc, round, rc);
-    if (!gridBarrier(gb))
+    if (!loopBarrier<CLUSTER>(gb))
       return;
     if (!doneM)
       colorCommit<R, true>(d, jm, round, rm, &sCount[0][outS]);
@@ -764,7 +766,7 @@ __global__ void __launch_bounds__(kColorBlock) kColorBoth(Dev<R> d, ColorJob jm,
         atomicAdd(&jc.aux[round % 3], sCount[1][outS]);
       sCount[0][in] = sCount[1][in] = 0;
     }
-    if (!gridBarrier(gb))
+    if (!loopBarrier<CLUSTER>(gb))
       return;
     if (!doneM) {
       const int rem = *reinterpret_cast<volatile int*>(&jm.aux[round % 3]);
@@ -789,7 +791,7 @@ __global__ void __launch_bounds__(kColorBlock) kColorBoth(Dev<R> d, ColorJob jm,
     }
   }
   if (tail) {
-    if (!gridBarrier(gb))  // the published lists are complete
+    if (!loopBarrier<CLUSTER>(gb))  // the published lists are complete
       return;
     if (blockIdx.x == 0) {
       if (jm.tailShared)
@@ -797,7 +799,7 @@ __global__ void __launch_bounds__(kColorBlock) kColorBoth(Dev<R> d, ColorJob jm,
       else
         colorTail(d, jm, jc, round, maxRounds, doneM, doneC, prevM, prevC);
     }
-    if (!gridBarrier(gb))  // the tail's colours are visible to every block
+    if (!loopBarrier<CLUSTER>(gb))  // the tail's colours are visible to every block
       return;
   }
   if (gtid == 0) {
@@ -813,13 +815,13 @@ __global__ void __launch_bounds__(kColorBlock) kColorBoth(Dev<R> d, ColorJob jm,
     return;
   colorOrderCount(jm);
   colorOrderCount(jc);
-  if (!gridBarrier(gb))
+  if (!loopBarrier<CLUSTER>(gb))
     return;
   if (blockIdx.x == 0)
     colorOrderScan(jm);
   if (blockIdx.x == (gridDim.x > 1 ? 1 : 0))
     colorOrderScan(jc);
-  if (!gridBarrier(gb))
+  if (!loopBarrier<CLUSTER>(gb))
     return;
   colorOrderScatter(jm);
   colorOrderScatter(jc);

@@ -299,13 +299,19 @@ void Sim<R>::launchCoopSmem(K kernel, int block, size_t smem, A... args) {
 template <class R>
 template <class K, class... A>
 bool Sim<R>::launchCluster(K kernel, A... args) {
+  return launchClusterCfg(kernel, sweepClusterBlocks_, kBlock, 0, args...);
+}
+template <class R>
+template <class K, class... A>
+bool Sim<R>::launchClusterCfg(K kernel, int blocks, int block, size_t smem, A... args) {
   cudaLaunchConfig_t cfg{};
-  cfg.gridDim = dim3(sweepClusterBlocks_);
-  cfg.blockDim = dim3(kBlock);
+  cfg.gridDim = dim3(blocks);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = smem;
   cfg.stream = stream_;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeClusterDimension;
-  attr[0].val.clusterDim.x = sweepClusterBlocks_;
+  attr[0].val.clusterDim.x = blocks;
   attr[0].val.clusterDim.y = 1;
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
@@ -314,8 +320,10 @@ bool Sim<R>::launchCluster(K kernel, A... args) {
   auto it = clusterOk_.find(key);
   if (it == clusterOk_.end()) {
     int clusters = 0;
-    if (sweepClusterBlocks_ > 8 &&
-        cudaFuncSetAttribute(kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
+    if (blocks > 8 && cudaFuncSetAttribute(kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
+      (void)cudaGetLastError();
+    if (smem > 48 * 1024 &&
+        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
       (void)cudaGetLastError();
     if (cudaOccupancyMaxActiveClusters(&clusters, kernel, &cfg) != cudaSuccess)
       (void)cudaGetLastError();
@@ -1349,8 +1357,15 @@ void Sim<R>::colorBoth(int nm, int nc, int& ncolV, int& velLeft, int& ncolP, int
   // the tail in shared memory when the hand-over fits its tables
   const bool tailShared = std::min(colorTailAt_, kColorTailMax) <= kTailShEntries;
   jm.tailShared = jc.tailShared = tailShared ? 1 : 0;
-  launchCoopSmem(kColorBoth<R>, colorBlock_, tailShared ? sizeof(TailShared) : 0, d_, jm, jc, std::max(nbM, nbC) + 2,
-                 gb, (const int*)topoFlags_.p, topoValid_ ? 1 : 0);
+  const size_t tailSmem = tailShared ? sizeof(TailShared) : 0;
+  const bool inCluster =
+      std::max(neM, neC) <= colorClusterEntries_ && colorBlock_ == kColorBlock &&
+      (cudaMemsetAsync(gbar_.p, 0, 2 * sizeof(unsigned), stream_) == cudaSuccess) &&
+      launchClusterCfg(kColorBoth<R, true>, sweepClusterBlocks_, kColorBlock, tailSmem, d_, jm, jc,
+                       std::max(nbM, nbC) + 2, gb, (const int*)topoFlags_.p, topoValid_ ? 1 : 0);
+  if (!inCluster)
+    launchCoopSmem(kColorBoth<R>, colorBlock_, tailSmem, d_, jm, jc, std::max(nbM, nbC) + 2, gb,
+                   (const int*)topoFlags_.p, topoValid_ ? 1 : 0);
   KCHECK("colour loop");
   int res[12], err = 0, differ[2] = {1, 1};
   readBack(res, colorAux_.p, sizeof res);

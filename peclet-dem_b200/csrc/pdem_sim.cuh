@@ -379,6 +379,15 @@ class Sim {
   // resident
   template <class K, class... A>
   bool launchCluster(K kernel, A... args);
+  // one cluster of `blocks` blocks of `block` threads with `smem` bytes of dynamic shared memory;
+  // false (nothing launched) when such a cluster cannot be resident. Residency is cached per kernel.
+  template <class K, class... A>
+  bool launchClusterCfg(K kernel, int blocks, int block, size_t smem, A... args);
+  // largest colouring (entries of the larger graph) run in one cluster (PDEM_COLOR_CLUSTER_ENTRIES)
+  long colorClusterEntries_ = [] {
+    const char* e = std::getenv("PDEM_COLOR_CLUSTER_ENTRIES");
+    return e ? std::max(0L, std::strtol(e, nullptr, 10)) : 32768L;
+  }();
   std::map<const void*, int> clusterOk_;  // per kernel: 1 resident, 0 not
   // velocity-sweep records of the one-cluster loops (kPackPgs), packed once per substep
   PgsRecs<R> packPgs(int nm, int ncol);
