@@ -53,7 +53,9 @@ SUBSTEPS = 10
 REF_OMP = os.path.join(ROOT, "oracle", "_ref", "libref_omp.so")         # -march=x86-64-v4
 REF_OMP_V2 = os.path.join(ROOT, "oracle", "_ref", "libref_omp_v2.so")   # -march=x86-64-v2 fallback
 REF_SERIAL = os.path.join(ROOT, "oracle", "_ref", "libref_serial.so")
-EXTRAS = ("xpbd262k", "batched", "calibration", "hertz", "shells")
+# calibration first: it allocates through torch, which later lines' pooled simulation buffers
+# would crowd
+EXTRAS = ("calibration", "xpbd262k", "batched", "hertz", "shells")
 L2_FLUSH_BYTES = 256 << 20
 
 
@@ -171,8 +173,10 @@ def stage_bytes(n, P, C, M, iv, istab, ip, D=8):
 
 
 # DRAM traffic per substep of a stage from one ncu capture of the same workload (bytes per
-# substep; stages not captured report none)
-STAGE_DRAM_BYTES = {("plain_settling_4096_fp64", "stabilization"): None}
+# substep; stages not captured report none): the stabilization sweep loop of the 4,096-sphere
+# restart (kSweepLoop<double, 3, 2, true>, one launch a substep: 3.23 MB read + 0.03 MB written;
+# the state is L2-resident, so DRAM sees little of the loop's 148 MB of algorithmic traffic)
+STAGE_DRAM_BYTES = {("plain_settling_4096_fp64", "stabilization"): 3.257e6}
 
 
 def measured_peaks():
@@ -441,6 +445,8 @@ def run_batched(args, rank, world, dist, dem, W):
     radius = np.concatenate([sc.scales * sc.global_scale for sc in sc_m])
     dt = sc_m[0].dt
     # deposition: one FP64 run from the RSA fill; its end state starts both timed runs
+    for sc in sc_m:  # deposition: the grains start falling at 0.5 m/s (gravity is -y)
+        sc.vel = sc.vel + np.array([0.0, -0.5, 0.0])
     sim = dem.Simulation(n_mine + 8, "fp64")
     first = apply_batch(sim, sc_m, [extras[s] for s in mine])
     for _ in range(args.drum_presettle * SUBSTEPS):
@@ -638,12 +644,18 @@ def run_hertz(args, rank, world, dist, dem, W):
 
 def run_shells(args, rank, world, dist, dem, W):
     """65,536 hollow cylinders (r_out 1 mm, r_in 0.6 mm, L 3 mm) with a seeded 512-point stratified
-    shell, after a gravity deposition (workloads.hollow_cylinders_deposited: placed by random
-    sequential addition of their bounding spheres and stepped in FP64 until the bed formed), FP64
-    and FP32-mixed from that state, with the mixed form's error against FP64 at the end."""
+    shell. The configuration's 60 x 60 x 120 mm box cannot hold them (their solid volume is 91 % of
+    it), so their bounding spheres are placed by random sequential addition at 25 % of a 1 x 1 x 2
+    box (workloads.hollow_cylinders) and the line times the first outer steps from there, in FP64
+    and the FP32-mixed form, with the mixed form's error against FP64 at the end. `--shell-presettle`
+    steps of a gravity deposition (2 m/s downwards, substeps of four times the configuration's) run
+    first when given; a dense shell bed is slow to build and to step (each touching pair carries up
+    to 512 contacts), so the default is none."""
     sc = W.hollow_cylinders(shell_points=W.hollow_cylinder_shell())
-    sc = W.deposit(sc, dem, outer_steps=args.shell_presettle)
-    line = {"workload": f"hollow_cylinders_{sc.n}_shell512_deposited", "box_m": [float(v) for v in sc.domain[1]],
+    if args.shell_presettle > 0:
+        sc = W.deposit(sc, dem, outer_steps=args.shell_presettle, v_down=2.0, dt_scale=4.0)
+    line = {"workload": f"hollow_cylinders_{sc.n}_shell512" + ("_deposited" if args.shell_presettle else ""),
+            "box_m": [float(v) for v in sc.domain[1]],
             "presettle_steps": args.shell_presettle}
     for prec in ("fp64", "mixed"):
         sim = sc.apply(dem.Simulation(sc.n + 8, prec))
@@ -762,8 +774,8 @@ def main():
     ap.add_argument("--extras", default=",".join(EXTRAS), help=f"comma list of {EXTRAS} or 'none'")
     ap.add_argument("--extra-steps", type=int, default=5, help="timed outer steps (or calls) of the extra lines")
     ap.add_argument("--drums", type=int, default=512)
-    ap.add_argument("--drum-presettle", type=int, default=60, help="untimed FP64 outer steps of the drum deposition")
-    ap.add_argument("--shell-presettle", type=int, default=40, help="untimed FP64 outer steps of the shell deposition")
+    ap.add_argument("--drum-presettle", type=int, default=150, help="untimed FP64 outer steps of the drum deposition")
+    ap.add_argument("--shell-presettle", type=int, default=0, help="untimed FP64 outer steps of a shell deposition")
     ap.add_argument("--calib-scenes", type=int, default=64)
     ap.add_argument("--calib-substeps", type=int, default=2000)
     args = ap.parse_args()

@@ -342,9 +342,10 @@ bool Sim<R>::launchClusterCfg(K kernel, int blocks, int block, size_t smem, A...
 template <class R>
 PgsRecs<R> Sim<R>::packPgs(int nm, int ncol) {
   if (pgsPackedAt_ != substepId_) {
-    pgsQ_.ensure((size_t)kPgsSlots * nm, false, stream_);
+    // the slot stride is the ids' capacity, so the slots are sized from it after it grew
     pgsIds_.ensure((size_t)nm, false, stream_);
     pgsCap_ = (long)(pgsIds_.n);
+    pgsQ_.ensure((size_t)kPgsSlots * pgsIds_.n, false, stream_);
     ++launches_, kPackPgs<R><<<gridFor(nm), kBlock, 0, stream_>>>(d_, mOrder_.p, mOff_.p, ncol,
                                                                  PgsRecs<R>{pgsQ_.p, pgsIds_.p, pgsCap_});
     KCHECK("pack velocity records");

@@ -180,11 +180,12 @@ def hollow_cylinders(seed=3, n=65536, r_out=1e-3, r_in=0.6e-3, length=3e-3, box=
                  substeps=substeps, shell=shell_points)
 
 
-def deposit(sc: Scene, dem, outer_steps, v_down=0.5, precision="fp64") -> Scene:
+def deposit(sc: Scene, dem, outer_steps, v_down=0.5, precision="fp64", dt_scale=1.0) -> Scene:
     """The scene after a gravity deposition: every body starts with `v_down` m/s along gravity on
-    top of its own velocity and the scene is stepped `outer_steps` outer steps (its substeps and
-    dt) by `dem.Simulation` in `precision`. Returns a copy whose positions, velocities,
-    orientations and spins are the end state."""
+    top of its own velocity and the scene is stepped `outer_steps` outer steps of its substeps, each
+    of dt_scale times its dt (a preparation run may take longer substeps than the configuration),
+    by `dem.Simulation` in `precision`. Returns a copy whose positions, velocities, orientations and
+    spins are the end state; its own dt is unchanged."""
     import copy
     g = np.asarray(sc.gravity, dtype=np.float64)
     gn = np.linalg.norm(g)
@@ -193,7 +194,7 @@ def deposit(sc: Scene, dem, outer_steps, v_down=0.5, precision="fp64") -> Scene:
     sim = out.apply(dem.Simulation(sc.n + 8, precision))
     for _ in range(outer_steps):
         for _ in range(sc.substeps):
-            sim.step(sc.dt)
+            sim.step(sc.dt * dt_scale)
     out.pos, out.vel = sim.get_positions(), sim.get_velocities()
     out.quat, out.angvel = sim.get_quaternions(), sim.get_angular_velocities()
     out.name = f"{sc.name}_deposited{outer_steps}"
