@@ -287,6 +287,30 @@ def run_headline(args, rank, world, dist, dem, W):
     w_end = sim.get_angular_velocities()
     sim.close()
 
+    # ---- the float step and the FP32-mixed form on the same window, and their distance from the
+    # FP64 run after the same outer steps (warm-up, timed, and the profiled ones) ----
+    other = {}
+    for prec in ("fp32", "mixed"):
+        sim = sc.apply(dem.Simulation(n + 8, prec))
+        for _ in range(args.warmup):
+            outer_step(sim, sc)
+        sim.get_positions()
+        ms = 0.0
+        for _ in range(args.steps):
+            flush()
+            sim.timer_start()
+            outer_step(sim, sc)
+            ms += sim.timer_stop()
+        for _ in range(args.steps):
+            outer_step(sim, sc)
+        err = np.linalg.norm(sim.get_positions() - x_end, axis=1) / sc.global_scale
+        sim.close()
+        t = max_over_ranks(ms / 1e3, dist, "cuda")
+        other[prec] = {"value": aggregate_rate(world, n, SUBSTEPS, args.steps, t),
+                       "max_position_error_radii": max_over_ranks(float(err.max()), dist, "cuda"),
+                       "median_position_error_radii": float(np.median(err)),
+                       "after_outer_steps": args.warmup + 2 * args.steps}
+
     # ---- end to end through the public API with host buffers, from the same state ----
     pinned = lambda: torch.zeros((n, 3), dtype=torch.float64, pin_memory=True).numpy()
     force, pos, vel = pinned(), pinned(), pinned()
@@ -350,7 +374,7 @@ def run_headline(args, rank, world, dist, dem, W):
             "sweeps_per_substep": {"velocity": iv, "stabilization": istab, "position": ip},
             "counts_last_substep": {"pairs": P, "contacts": C, "manifolds": M,
                                     "colours": [last["colors_velocity"], last["colors_position"]]},
-            "packing_at_end": pk}
+            "packing_at_end": pk, "other_precisions": other}
 
 
 # ---------------------------------------------------------------------------------------------
@@ -732,7 +756,11 @@ def run_ours(args):
             flat.update(shells_fp64_value=detail["shells"]["fp64"]["value"],
                         shells_mixed_value=detail["shells"]["mixed"]["value"])
         detail["headline"] = {k: h[k] for k in ("stages_ms_per_substep", "sweeps_per_substep", "counts_last_substep",
-                                               "packing_at_end", "roofline")}
+                                               "packing_at_end", "roofline", "other_precisions")}
+        o = h["other_precisions"]
+        flat.update(headline_fp32_value=o["fp32"]["value"], headline_mixed_value=o["mixed"]["value"],
+                    headline_mixed_err_radii=o["mixed"]["max_position_error_radii"],
+                    headline_fp32_err_radii=o["fp32"]["max_position_error_radii"])
         print(json.dumps({"detail": detail}))
         line = {
             "metric": METRIC, "value": h["value"], "unit": METRIC, "n_gpus": world, "steps": args.steps,

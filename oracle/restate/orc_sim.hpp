@@ -6,7 +6,7 @@
 // index — the canonical order the B200 implementation reproduces. At R = float the results are
 // bit-identical to the reference headers compiled against the serial Kokkos shim (the tests check
 // this); at R = double this is the FP64 oracle of the B200 FP64 step. Stabilization modes
-// "multilevel" (2) is not restated (out of scope of the B200 build); "ordered" (4) is.
+// "multilevel" (2) and "ordered" (4) are restated.
 #pragma once
 #include <algorithm>
 #include <climits>
@@ -1026,6 +1026,262 @@ class Sim {
   // level-ordered symmetric sweeps (solver_velocity.hpp:914-989; sim.hpp:357-400): the coloured
   // manifolds bucketed by (level, colour), key level * 64 + colour (stable), swept bottom-up then
   // top-down per iteration until the residual drains
+  // ---------------- multilevel stabilization (src/sim.hpp:303-356, src/solver_multilevel.hpp) ----------------
+  // Greedy pairwise aggregation of the quasi-static contact graph into super-bodies, per level a
+  // colouring of the manifolds that cross aggregate boundaries; per iteration one fine PGS sweep,
+  // then on every level a restriction (momentum-weighted group velocity), two translation-only
+  // coarse PGS sweeps at the aggregate masses on the shared normal accumulator, and a
+  // prolongation; the loop stops on the quasi-static residual.
+  static constexpr int kMlMaxLevels = 10, kMlSkip = 63, kMlGateSlip = 4;
+  std::vector<long long> mlPacked;
+  std::vector<int> mlParent, mlGrp, mlMate;
+  std::vector<R> mlMassG, mlInvMassG;
+  std::vector<V3<R>> mlVelG, mlVelG0;
+  struct MlLevel {
+    int groupOff, numGroups, parentOff, numColors;
+  };
+  static R mlEffMass(R im) { return R(1) / std::fmax(im, R(1e-30)); }  // solver_multilevel.hpp:79-81
+  bool mlEligible(int idx, R qsThr) const {  // solver_multilevel.hpp:97-128, gates = slip
+    const Manifold<R>& m = manifolds[idx];
+    if (m.np <= 0 || mColor[idx] < 0)
+      return false;
+    if (std::fabs(vn0[idx]) > qsThr)
+      return false;
+    if (dot(vt0[idx], vt0[idx]) > qsThr * qsThr)
+      return false;
+    return true;
+  }
+  std::vector<MlLevel> mlBuild(int nm, R qsThr) {  // solver_multilevel.hpp:134-323
+    std::vector<MlLevel> H;
+    if (nm <= 0 || numReal <= 0)
+      return H;
+    mlPacked.assign(nm, ~0ll);
+    mlGrp.resize(numReal);
+    for (int i = 0; i < numReal; ++i)
+      mlGrp[i] = i;
+    const int parentCap = 5 * capacity, groupCap = 4 * capacity;
+    mlParent.resize(parentCap);
+    mlMassG.resize(groupCap);
+    mlInvMassG.resize(groupCap);
+    mlVelG.resize(groupCap);
+    mlVelG0.resize(groupCap);
+    mlMate.resize(std::max(numReal, 1));
+    std::vector<long long> winner(std::max(numReal, 1));
+    std::vector<u64> mask(std::max(numReal, 1));
+    int ngPrev = numReal, parentOff = 0, groupOff = 0;
+    for (int lvl = 1; lvl <= kMlMaxLevels; ++lvl) {
+      if (parentOff + ngPrev > parentCap)
+        break;
+      for (int g = 0; g < ngPrev; ++g)
+        winner[g] = -1;
+      auto ends = [&](int idx, int& gA, int& gB) {
+        const Manifold<R>& m = manifolds[idx];
+        gA = mlGrp[realIdx[m.a]];
+        gB = m.b >= 0 ? mlGrp[realIdx[m.b]] : -1;
+      };
+      for (int idx = 0; idx < nm; ++idx) {  // matching: contend
+        if (manifolds[idx].b < 0 || !mlEligible(idx, qsThr))
+          continue;
+        int gA, gB;
+        ends(idx, gA, gB);
+        if (gA == gB)
+          continue;
+        const long long key = colorKey(idx);
+        winner[gA] = std::max(winner[gA], key);
+        winner[gB] = std::max(winner[gB], key);
+      }
+      for (int g = 0; g < ngPrev; ++g)
+        mlMate[g] = g;
+      for (int idx = 0; idx < nm; ++idx) {  // matching: sole winner of both ends
+        if (manifolds[idx].b < 0 || !mlEligible(idx, qsThr))
+          continue;
+        int gA, gB;
+        ends(idx, gA, gB);
+        if (gA == gB)
+          continue;
+        const long long key = colorKey(idx);
+        if (winner[gA] == key && winner[gB] == key) {
+          mlMate[gA] = gB;
+          mlMate[gB] = gA;
+        }
+      }
+      int ngNew = 0;  // compaction: a matched pair -> one id (leader = the smaller)
+      for (int g = 0; g < ngPrev; ++g)
+        if (mlMate[g] >= g)
+          mlParent[parentOff + g] = ngNew++;
+      for (int g = 0; g < ngPrev; ++g)
+        if (mlMate[g] < g)
+          mlParent[parentOff + g] = mlParent[parentOff + mlMate[g]];
+      if (ngNew >= ngPrev || ngNew > (9 * ngPrev) / 10)
+        break;
+      if (groupOff + ngNew > groupCap)
+        break;
+      for (int i = 0; i < numReal; ++i)
+        mlGrp[i] = mlParent[parentOff + mlGrp[i]];
+      for (int g = 0; g < ngNew; ++g)
+        mlMassG[groupOff + g] = 0;
+      for (int i = 0; i < numReal; ++i)
+        mlMassG[groupOff + mlGrp[i]] += mlEffMass(invMass[i]);
+      for (int g = 0; g < ngNew; ++g)
+        mlInvMassG[groupOff + g] = R(1) / mlMassG[groupOff + g];
+      // colouring of the crossing manifolds on the group graph (this level's 6-bit slot)
+      const int shift = 6 * (lvl - 1);
+      for (int g = 0; g < ngNew; ++g)
+        mask[g] = 0;
+      int remaining = 1, prevRemaining = -1, maxc = -1;
+      for (int round = 0; round < 64 && remaining > 0; ++round) {
+        for (int g = 0; g < ngNew; ++g)
+          winner[g] = -1;
+        auto pending = [&](int idx, int& gA, int& gB) {
+          if (!mlEligible(idx, qsThr) || ((mlPacked[idx] >> shift) & 63) != kMlSkip)
+            return false;
+          ends(idx, gA, gB);
+          return gB != gA;
+        };
+        for (int idx = 0; idx < nm; ++idx) {
+          int gA, gB;
+          if (!pending(idx, gA, gB))
+            continue;
+          const long long key = colorKey(idx);
+          winner[gA] = std::max(winner[gA], key);
+          if (gB >= 0)
+            winner[gB] = std::max(winner[gB], key);
+        }
+        int rem = 0;
+        for (int idx = 0; idx < nm; ++idx) {
+          int gA, gB;
+          if (!pending(idx, gA, gB))
+            continue;
+          const long long key = colorKey(idx);
+          if (winner[gA] != key || (gB >= 0 && winner[gB] != key)) {
+            ++rem;
+            continue;
+          }
+          u64 forb = mask[gA] | (gB >= 0 ? mask[gB] : 0ull);
+          int c = 0;
+          while (c < kMlSkip - 1 && (forb & (1ull << c)))
+            ++c;
+          mlPacked[idx] = (mlPacked[idx] & ~(63ll << shift)) | ((long long)c << shift);
+          mask[gA] |= 1ull << c;
+          if (gB >= 0)
+            mask[gB] |= 1ull << c;
+        }
+        if (rem == prevRemaining)
+          break;
+        prevRemaining = rem;
+        remaining = rem;
+      }
+      for (int idx = 0; idx < nm; ++idx) {
+        const int c = (int)((mlPacked[idx] >> shift) & 63);
+        if (c != kMlSkip && c > maxc)
+          maxc = c;
+      }
+      H.push_back(MlLevel{groupOff, ngNew, parentOff, maxc + 1});
+      parentOff += ngPrev;
+      groupOff += ngNew;
+      ngPrev = ngNew;
+      if (ngNew <= 32)
+        break;
+    }
+    return H;
+  }
+  void mlCoarseCycle(int nm, const std::vector<MlLevel>& H, R& maxQS, int coarseSweeps) {  // :331-478
+    for (int i = 0; i < numReal; ++i)
+      mlGrp[i] = i;
+    for (int lvl = 1; lvl <= (int)H.size(); ++lvl) {
+      const MlLevel& L = H[lvl - 1];
+      const int off = L.groupOff, shift = 6 * (lvl - 1);
+      for (int i = 0; i < numReal; ++i)
+        mlGrp[i] = mlParent[L.parentOff + mlGrp[i]];
+      for (int g = 0; g < L.numGroups; ++g)
+        mlVelG[off + g] = V3<R>{0, 0, 0};
+      for (int i = 0; i < numReal; ++i) {
+        const R m = mlEffMass(invMass[i]);
+        V3<R>& vg = mlVelG[off + mlGrp[i]];
+        vg.x += m * velPred[i].x;
+        vg.y += m * velPred[i].y;
+        vg.z += m * velPred[i].z;
+      }
+      for (int g = 0; g < L.numGroups; ++g) {
+        const R invM = R(1) / mlMassG[off + g];
+        mlVelG[off + g].x *= invM;
+        mlVelG[off + g].y *= invM;
+        mlVelG[off + g].z *= invM;
+        mlVelG0[off + g] = mlVelG[off + g];
+      }
+      for (int sw = 0; sw < coarseSweeps; ++sw)
+        for (int color = 0; color < L.numColors; ++color)
+          for (int idx = 0; idx < nm; ++idx) {
+            if ((int)((mlPacked[idx] >> shift) & 63) != color)
+              continue;
+            const Manifold<R>& m = manifolds[idx];
+            const int gA = mlGrp[realIdx[m.a]];
+            const int gB = m.b >= 0 ? mlGrp[realIdx[m.b]] : -1;
+            const R invN = R(1) / static_cast<R>(m.np);
+            const V3<R> N = m.N;
+            const R lenN = std::sqrt(dot(N, N));
+            if (lenN < R(1e-9))
+              continue;
+            const V3<R> rAa = mul(m.rA, invN), rBa = mul(m.rB, invN);
+            const V3<R> dc = gB < 0 ? rAa : sub(rAa, rBa);
+            const V3<R> vA = mlVelG[off + gA];
+            const V3<R> vB = gB >= 0 ? mlVelG[off + gB] : mul(m.wv, invN);
+            const R vn = dot(sub(vA, vB), N);
+            const R al = dot(N, dc);
+            const R sgn = al > R(0) ? R(1) : R(-1);
+            const R iA = mlInvMassG[off + gA];
+            const R iB = gB >= 0 ? mlInvMassG[off + gB] : R(0);
+            const R w = dot(N, N) * (iA + iB);
+            if (w <= R(0))
+              continue;
+            const R dp = (sgn * vn) / w;
+            const R pOld = lambdaAcc[idx];
+            R pNew = pOld + dp;
+            if (pNew < R(0))
+              pNew = 0;
+            const R d = pNew - pOld;
+            if (d == R(0))
+              continue;
+            lambdaAcc[idx] = pNew;
+            maxQS = std::max(maxQS, std::fabs(d) * w / lenN);
+            const V3<R> J = mul(N, -sgn * d);
+            V3<R>& a = mlVelG[off + gA];
+            a.x += J.x * iA;
+            a.y += J.y * iA;
+            a.z += J.z * iA;
+            if (gB >= 0) {
+              V3<R>& b = mlVelG[off + gB];
+              b.x -= J.x * iB;
+              b.y -= J.y * iB;
+              b.z -= J.z * iB;
+            }
+          }
+      for (int i = 0; i < numReal; ++i) {
+        const V3<R>& vg = mlVelG[off + mlGrp[i]];
+        const V3<R>& v0 = mlVelG0[off + mlGrp[i]];
+        velPred[i].x += vg.x - v0.x;
+        velPred[i].y += vg.y - v0.y;
+        velPred[i].z += vg.z - v0.z;
+      }
+    }
+  }
+  void multilevelStabilization(int nm, int ncol, V3<R> gHat, R vRestS, R gMag) {  // sim.hpp:303-356
+    (void)gHat;
+    const R qsThr = R(8) * dt * gMag;
+    const std::vector<MlLevel> H = mlBuild(nm, qsThr);
+    for (int it = 0; it < 2 * velIters; ++it) {
+      R maxQS = 0;
+      for (int c = 0; c < ncol; ++c)
+        for (int i = 0; i < nm; ++i)
+          if (mColor[i] == c)
+            pgsOne(i, vRestS, maxApproach, &maxQS);
+      if (!H.empty())
+        mlCoarseCycle(nm, H, maxQS, 2);
+      if (maxQS <= vRestS)
+        break;
+    }
+  }
+
   void orderedStabilization(int nm, V3<R> gHat, R vRestS) {
     computeHeightLevels(nm, gHat);
     std::vector<int> key(nm), perm(nm);
@@ -1535,7 +1791,9 @@ class Sim {
     }
   }
   // :641-858 PGSManifoldSweep::solveOne
-  void pgsOne(int idx, R vRest, R& maxApp) {
+  // maxQS (the multilevel pass): also the largest correction on quasi-static contacts,
+  // |vn0| <= 4 vRest |N| (src/solver_velocity.hpp:722-723, 829-830)
+  void pgsOne(int idx, R vRest, R& maxApp, R* maxQS = nullptr) {
     const Manifold<R>& m = manifolds[idx];
     const MView v = view(m);
     const int ra = v.ra, rb = v.rb;
@@ -1592,6 +1850,8 @@ class Sim {
     if (dA != R(0)) {
       lambdaAcc[idx] = pNew;
       maxApp = std::max(maxApp, std::fabs(dA) * wT / lenN);
+      if (maxQS && std::fabs(vn0[idx]) <= R(4) * vRest * lenN)
+        *maxQS = std::max(*maxQS, std::fabs(dA) * wT / lenN);
       const R lam = -sgn * dA;
       const V3<R> J = mul(v.N, lam), JA = mul(v.TA, lam), JB = mul(v.TB, lam);
       if (applyA) {
@@ -1655,8 +1915,11 @@ class Sim {
     if (d.x != R(0) || d.y != R(0) || d.z != R(0)) {
       lambdaT[idx] = ltNew;
       const R dl = std::sqrt(dot(d, d));
-      if (wTt > R(1e-9))
+      if (wTt > R(1e-9)) {
         maxApp = std::max(maxApp, dl * wTt);
+        if (maxQS && std::fabs(vn0[idx]) <= R(4) * vRest * lenN)
+          *maxQS = std::max(*maxQS, dl * wTt);
+      }
       if (applyA) {
         velPred[ra] = add(velPred[ra], mul(d, v.imA));
         angVelPred[ra] = add(angVelPred[ra], angDelta(v.qA, cross(v.rAa, d), v.iIA));
@@ -2038,7 +2301,7 @@ class Sim {
         } else if (stabMode == 4) {
           orderedStabilization(nm, gHat, vRestS);
         } else {
-          throw std::runtime_error("oracle: stabilization mode 'multilevel' is not restated");
+          multilevelStabilization(nm, ncolV, gHat, vRestS, gMag);
         }
       }
     }

@@ -12,6 +12,7 @@
 #include "pdem_contact.cuh"
 #include "pdem_hertz.cuh"
 #include "pdem_kernels.cuh"
+#include "pdem_multilevel.cuh"
 #include "pdem_persist.cuh"
 #include "pdem_shell.hpp"
 #include "pdem_sim.cuh"
@@ -1619,10 +1620,10 @@ void Sim<R>::demStep() {
   mark(ST_STAB);
   if (usePGS) {
     const R vRestS = R(2) * dt_ * gMag;
-    if (stabMode_ == 2)
-      throw std::runtime_error("stabilization mode 'multilevel' is not supported by the B200 step");
     if (stabMode_ == 4 && batch_)
       throw std::runtime_error("batched scenes: stabilization mode 'ordered' is not supported");
+    if (stabMode_ == 2 && batch_)
+      throw std::runtime_error("batched scenes: stabilization mode 'multilevel' is not supported");
     ctl(CTL_STAB_DECIDE, vRestS, stabMode_);
     // periodic scenes: split the manifolds for the ledger order now, so the number of ghost
     // manifolds (the host sizes their sort with it) comes back with the decision below
@@ -1645,11 +1646,15 @@ void Sim<R>::demStep() {
     }
     // the pass runs only when the main sweeps left a residual (src/sim.hpp:282): read the
     // decision so an untriggered pass costs nothing
-    const bool stabRun = (stabMode_ == 1 || stabMode_ == 3 || stabMode_ == 4) && readCounters().stabRun;
+    const bool stabRun = stabMode_ != 0 && readCounters().stabRun;
     if (stabRun && stabMode_ == 4) {
       SolveP<R> ss = sp;
       ss.vRest = vRestS;
       orderedStabilization(nm, gHat, ss, vRestS);
+    } else if (stabRun && stabMode_ == 2) {
+      SolveP<R> ss = sp;
+      ss.vRest = vRestS;
+      multilevelStabilization(nm, ncolV, ss, vRestS, gMag);
     } else if (stabRun) {
       if (stabMode_ == 1 && nm > 0) {
         ensureGrounded();
@@ -2282,6 +2287,120 @@ std::vector<R> Sim<R>::sdfGrid(int rx, int ry, int rz) {
 
 // "ordered" stabilization (src/sim.hpp:357-400): fresh height levels, manifolds bucketed by
 // (level, colour), symmetric sweeps bottom-up then top-down until the residual drains
+// the multilevel pass (src/sim.hpp:303-356): the hierarchy, then the smoothing / coarse loop,
+// driven from the host (pdem_multilevel.cuh)
+template <class R>
+void Sim<R>::multilevelStabilization(int nm, int ncol, const SolveP<R>& ss, R vRestS, R gMag) {
+  cudaStream_t s = stream_;
+  const int B = kBlock;
+  const int nr = numReal_;
+  if (nm <= 0 || nr <= 0)
+    return;
+  const R qsThr = R(8) * dt_ * gMag;
+  const int parentCap = 5 * capacity_, groupCap = 4 * capacity_;
+  mlPacked_.ensure(nm, false, s);
+  mlParent_.ensure(parentCap, false, s);
+  mlGrp_.ensure(nr, false, s);
+  mlMate_.ensure(nr, false, s);
+  mlFlag_.ensure((size_t)nr + 1, false, s);
+  mlPos_.ensure((size_t)nr + 1, false, s);
+  mlWin_.ensure(nr, false, s);
+  mlMask_.ensure(nr, false, s);
+  mlMassG_.ensure(groupCap, false, s);
+  mlInvMassG_.ensure(groupCap, false, s);
+  mlVelG_.ensure(groupCap, false, s);
+  mlVelG0_.ensure(groupCap, false, s);
+  mlInt_.ensure(2, false, s);
+  mlQS_.ensure(1, false, s);
+  cudaCheck(cudaMemsetAsync(mlPacked_.p, 0xff, nm * sizeof(long long), s), "memset");  // every slot 63
+  ++launches_, kMlIota<<<gridFor(nr), B, 0, s>>>(mlGrp_.p, nr);
+  struct Level {
+    int groupOff, numGroups, parentOff, numColors;
+  };
+  std::vector<Level> H;
+  auto readInt = [&](const int* dev) {
+    int v = 0;
+    cudaCheck(cudaMemcpyAsync(&v, dev, sizeof v, cudaMemcpyDeviceToHost, s), "D2H");
+    sync();
+    return v;
+  };
+  int ngPrev = nr, parentOff = 0, groupOff = 0;
+  for (int lvl = 1; lvl <= kMlMaxLevels; ++lvl) {  // src/solver_multilevel.hpp:154-322
+    if (parentOff + ngPrev > parentCap)
+      break;
+    cudaCheck(cudaMemsetAsync(mlWin_.p, 0xff, ngPrev * sizeof(long long), s), "memset");
+    ++launches_, kMlMatchContend<<<gridFor(nm), B, 0, s>>>(d_, nm, qsThr, mlGrp_.p, mlWin_.p);
+    ++launches_, kMlIota<<<gridFor(ngPrev), B, 0, s>>>(mlMate_.p, ngPrev);
+    ++launches_, kMlMatchCommit<<<gridFor(nm), B, 0, s>>>(d_, nm, qsThr, mlGrp_.p, mlWin_.p, mlMate_.p);
+    ++launches_, kMlLeader<<<gridFor(ngPrev), B, 0, s>>>(mlMate_.p, ngPrev, mlFlag_.p);
+    cudaCheck(cudaMemsetAsync(mlFlag_.p + ngPrev, 0, sizeof(int), s), "memset");
+    exclusiveSum(mlFlag_.p, mlPos_.p, ngPrev + 1);
+    ++launches_, kMlParent<<<gridFor(ngPrev), B, 0, s>>>(mlMate_.p, mlFlag_.p, mlPos_.p, ngPrev,
+                                                         mlParent_.p + parentOff);
+    KCHECK("multilevel matching");
+    const int ngNew = readInt(mlPos_.p + ngPrev);
+    if (ngNew >= ngPrev || ngNew > (9 * ngPrev) / 10)
+      break;
+    if (groupOff + ngNew > groupCap)
+      break;
+    ++launches_, kMlCompose<<<gridFor(nr), B, 0, s>>>(mlGrp_.p, nr, mlParent_.p + parentOff);
+    ++launches_, kMlGroupMass<<<1, 1, 0, s>>>(d_, nr, mlGrp_.p, mlMassG_.p + groupOff, mlInvMassG_.p + groupOff, ngNew);
+    const int shift = 6 * (lvl - 1);
+    cudaCheck(cudaMemsetAsync(mlMask_.p, 0, ngNew * sizeof(u64), s), "memset");
+    int remaining = 1, prevRemaining = -1;
+    for (int round = 0; round < 64 && remaining > 0; ++round) {
+      cudaCheck(cudaMemsetAsync(mlWin_.p, 0xff, ngNew * sizeof(long long), s), "memset");
+      ++launches_, kMlColorContend<<<gridFor(nm), B, 0, s>>>(d_, nm, qsThr, mlGrp_.p, mlPacked_.p, shift, mlWin_.p);
+      cudaCheck(cudaMemsetAsync(mlInt_.p, 0, sizeof(int), s), "memset");
+      ++launches_, kMlColorCommit<<<gridFor(nm), B, 0, s>>>(d_, nm, qsThr, mlGrp_.p, mlPacked_.p, shift, mlWin_.p,
+                                                            mlMask_.p, mlInt_.p);
+      KCHECK("multilevel colouring");
+      const int rem = readInt(mlInt_.p);
+      if (rem == prevRemaining)
+        break;
+      prevRemaining = rem;
+      remaining = rem;
+    }
+    cudaCheck(cudaMemsetAsync(mlInt_.p + 1, 0xff, sizeof(int), s), "memset");  // -1
+    ++launches_, kMlMaxColor<<<gridFor(nm), B, 0, s>>>(mlPacked_.p, nm, shift, mlInt_.p + 1);
+    const int maxc = readInt(mlInt_.p + 1);
+    H.push_back(Level{groupOff, ngNew, parentOff, maxc + 1});
+    parentOff += ngPrev;
+    groupOff += ngNew;
+    ngPrev = ngNew;
+    if (ngNew <= 32)
+      break;
+  }
+  for (int it = 0; it < 2 * velIters_; ++it) {  // src/sim.hpp:337-355
+    mlQS_.zero(s);
+    for (int col = 0; col < ncol; ++col)
+      ++launches_, kPGSColorQS<<<gridFor(nm), B, 0, s>>>(d_, mOrder_.p, mOff_.p, col, ss, mlQS_.p);
+    if (!H.empty()) {  // src/solver_multilevel.hpp:331-478
+      ++launches_, kMlIota<<<gridFor(nr), B, 0, s>>>(mlGrp_.p, nr);
+      for (size_t l = 0; l < H.size(); ++l) {
+        const Level& L = H[l];
+        const int shift = 6 * (int)l;
+        ++launches_, kMlCompose<<<gridFor(nr), B, 0, s>>>(mlGrp_.p, nr, mlParent_.p + L.parentOff);
+        ++launches_, kMlRestrict<<<1, 1, 0, s>>>(d_, nr, mlGrp_.p, mlVelG_.p + L.groupOff, mlVelG0_.p + L.groupOff,
+                                                 mlMassG_.p + L.groupOff, L.numGroups);
+        for (int sw = 0; sw < 2; ++sw)
+          for (int color = 0; color < L.numColors; ++color)
+            ++launches_, kMlCoarsePGS<<<gridFor(nm), B, 0, s>>>(d_, nm, mlGrp_.p, mlPacked_.p, shift, color,
+                                                                mlVelG_.p + L.groupOff, mlInvMassG_.p + L.groupOff,
+                                                                mlQS_.p);
+        ++launches_, kMlProlong<<<gridFor(nr), B, 0, s>>>(d_, nr, mlGrp_.p, mlVelG_.p + L.groupOff,
+                                                          mlVelG0_.p + L.groupOff);
+      }
+    }
+    KCHECK("multilevel cycle");
+    R qs = 0;
+    cudaCheck(cudaMemcpyAsync(&qs, mlQS_.p, sizeof qs, cudaMemcpyDeviceToHost, s), "D2H");
+    sync();
+    if (qs <= vRestS)
+      break;
+  }
+}
+
 template <class R>
 void Sim<R>::orderedStabilization(int nm, V3<R> gHat, const SolveP<R>& ss, R vRestS) {
   cudaStream_t s = stream_;

@@ -414,6 +414,13 @@ class Sim {
   template <class T>
   void sortPairs(const T* kin, T* kout, const int* vin, int* vout, int n, int endBit);
   void orderedStabilization(int nm, V3<R> gHat, const SolveP<R>& ss, R vRestS);
+  // the multilevel stabilization pass and its buffers (pdem_multilevel.cuh)
+  void multilevelStabilization(int nm, int ncol, const SolveP<R>& ss, R vRestS, R gMag);
+  DBuf<long long> mlPacked_, mlWin_;
+  DBuf<int> mlParent_, mlGrp_, mlMate_, mlFlag_, mlPos_, mlInt_;
+  DBuf<u64> mlMask_;
+  DBuf<R> mlMassG_, mlInvMassG_, mlQS_;
+  DBuf<Q4<R>> mlVelG_, mlVelG0_;
  public:
   // launch shape autotuner of the per-scene sweep loops: the chosen block (0 while tuning) and the
   // mean sweep-loop time of each candidate (ms per substep)

@@ -463,10 +463,12 @@ __device__ __forceinline__ PgsStatic<R> pgsRecord(const PgsRecs<R>& r, long t, i
   return s;
 }
 
-// one projected Gauss-Seidel update of manifold idx from its per-substep constants v
-template <class R, bool LOCAL = false>
+// one projected Gauss-Seidel update of manifold idx from its per-substep constants v; with QS it
+// also raises *qs by the corrections of quasi-static contacts, |vn0| <= 4 vRest |N| (the residual
+// of the multilevel pass, src/solver_velocity.hpp:722-723, 829-830)
+template <class R, bool LOCAL = false, bool QS = false>
 __device__ __forceinline__ void pgsCore(const Dev<R>& d, int idx, const PgsStatic<R>& v, R eG, R muG, int sc,
-                                        const SolveP<R>& P, R& mx) {
+                                        const SolveP<R>& P, R& mx, R* qs = nullptr) {
   const int ra = v.ra, rb = v.rb;
   const bool hasB = v.hasB;
   const V3<R> vA = v3(d.velPred[ra]), wA = v3(d.angVelPred[ra]);
@@ -520,6 +522,8 @@ __device__ __forceinline__ void pgsCore(const Dev<R>& d, int idx, const PgsStati
   if (dA != R(0)) {
     d.lambda[idx] = pNew;
     loopMax<R, LOCAL>(d, sc, false, fabs(dA) * wT / lenN, mx);
+    if (QS && fabs(vn0) <= R(4) * P.vRest * lenN)
+      runMax(*qs, fabs(dA) * wT / lenN);
     const R lam = -sgn * dA;
     const V3<R> J = mul(v.N, lam), JA = mul(v.TA, lam), JB = mul(v.TB, lam);
     if (applyA) {
@@ -575,8 +579,11 @@ __device__ __forceinline__ void pgsCore(const Dev<R>& d, int idx, const PgsStati
     if (nonzero(dd)) {
       d.lambdaT[idx] = q4(ltNew);
       const R dl = sqrt(dot(dd, dd));
-      if (wTt > R(1e-9))
+      if (wTt > R(1e-9)) {
         loopMax<R, LOCAL>(d, sc, false, dl * wTt, mx);
+        if (QS && fabs(vn0) <= R(4) * P.vRest * lenN)
+          runMax(*qs, dl * wTt);
+      }
       if (applyA) {
         vA2 = add(vA2, mul(dd, v.imA));
         wA2 = add(wA2, angResponse(v.qA, cross(v.rAa, dd), v.iIA));

@@ -92,4 +92,7 @@ MATRIX = [
     ("reversed_column", lambda: S.reversed_column(), None, 40),
     ("ordered_column", lambda: S.settled_column(), lambda s: s.set_stabilization_mode("ordered"), 25),
     ("ordered_dense", lambda: S.dense_spheres(), lambda s: s.set_stabilization_mode("ordered"), 8),
+    ("multilevel_column", lambda: S.settled_column(), lambda s: s.set_stabilization_mode("multilevel"), 25),
+    ("multilevel_dense", lambda: S.dense_spheres(), lambda s: s.set_stabilization_mode("multilevel"), 10),
+    ("multilevel_periodic", lambda: S.polydisperse_periodic(), lambda s: s.set_stabilization_mode("multilevel"), 10),
 ]
