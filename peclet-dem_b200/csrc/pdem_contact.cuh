@@ -63,7 +63,7 @@ struct Probe {
 };
 template <class R>
 __device__ __forceinline__ Probe<R> probeBody(const Dev<R>& d, int A, int B, int k, const ShapeDesc<R>& dA,
-                                             const ShapeDesc<R>& dB, R gs) {
+                                             const ShapeDesc<R>& dB, R gs, const Q4<R>* shell = nullptr) {
   const V3<R> pA = v3(d.posPred[A]), pB = v3(d.posPred[B]);
   const Q4<R> qA = d.quatPred[A], qB = d.quatPred[B];
   const R sA = d.scale[A] * gs, sB = d.scale[B] * gs;
@@ -71,7 +71,7 @@ __device__ __forceinline__ Probe<R> probeBody(const Dev<R>& d, int A, int B, int
   Probe<R> r;
   r.prad = R(0);
   if (dA.numPoints > 0)
-    pl = v3(d.shell[dA.shellOffset + k]);
+    pl = v3(shell ? shell[k] : d.shell[dA.shellOffset + k]);
   else if (dA.type == SHAPE_SPHERE)
     r.prad = dA.par[0] * sA;
   r.pw = add(pA, rot(qA, mul(pl, sA)));
@@ -152,10 +152,62 @@ __global__ void kNarrowSphereWrite(Dev<R> d, int nhit, NarrowP<R> P, const int* 
   }
 }
 
-// point shells: one warp per pair, lanes over shell points in order
+// ---- one-dimensional bulk copies (TMA) into shared memory, completed on an mbarrier ----
+__device__ __forceinline__ unsigned smemAddr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbarInit(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smemAddr(bar)), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbarExpectTx(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smemAddr(bar)), "r"(bytes) : "memory");
+}
+// src and dst 16-byte aligned, bytes a multiple of 16
+__device__ __forceinline__ void bulkCopyToShared(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smemAddr(dst)),
+               "l"(src), "r"(bytes), "r"(smemAddr(bar))
+               : "memory");
+}
+__device__ __forceinline__ bool mbarTryWait(unsigned long long* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smemAddr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+constexpr long kStageSpins = 1L << 22;  // polls of a staging wait before the block reads global memory
+
+// point shells: one warp per pair, lanes over shell points in order. With stageBytes > 0 (the
+// shape's whole shell, kept small) the block first copies the shell into shared memory with one
+// bulk copy: every warp of the block probes the same points. A staging wait that runs out (it
+// should not: the copy is a few KB) leaves the block reading the shell from global memory, after
+// waiting, bounded again, for the copy so that none is in flight when the block ends.
 template <class R, int MODE>
-__global__ void kNarrowShell(Dev<R> d, int np, NarrowP<R> P, int* cnt, const int* off) {
+__global__ void kNarrowShell(Dev<R> d, int np, NarrowP<R> P, int* cnt, const int* off, int stageBytes) {
+  extern __shared__ __align__(128) unsigned char shellSmem[];
+  __shared__ __align__(8) unsigned long long stageBar;
   const ShapeDesc<R> dA = d.shapes[0], dB = d.shapes[0];
+  const Q4<R>* shell = nullptr;
+  if (stageBytes > 0) {
+    if (threadIdx.x == 0) {
+      mbarInit(&stageBar, 1);
+      mbarExpectTx(&stageBar, (unsigned)stageBytes);
+      bulkCopyToShared(shellSmem, d.shell + dA.shellOffset, (unsigned)stageBytes, &stageBar);
+    }
+    __syncthreads();  // the barrier is initialised before anyone polls it
+    long spins = 0;
+    bool ok = false;
+    while (!(ok = mbarTryWait(&stageBar, 0)) && ++spins < kStageSpins) {
+    }
+    if (__syncthreads_and(ok)) {
+      shell = reinterpret_cast<const Q4<R>*>(shellSmem);
+    } else {
+      while (!mbarTryWait(&stageBar, 0) && ++spins < 2 * kStageSpins) {
+      }
+    }
+  }
   const int lane = threadIdx.x & 31;
   const long warp = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const long nwarps = ((long)gridDim.x * blockDim.x) >> 5;
@@ -170,7 +222,7 @@ __global__ void kNarrowShell(Dev<R> d, int np, NarrowP<R> P, int* cnt, const int
       bool hit = false;
       Probe<R> p;
       if (k < K) {
-        p = probeBody(d, pr.x, pr.y, k, dA, dB, P.globalScale);
+        p = probeBody(d, pr.x, pr.y, k, dA, dB, P.globalScale, shell);
         hit = p.eff < marginOf(d, P, pr.x);
         if (MODE == 0 && p.eff < R(0))
           overlapMax(d, pr.x, -p.eff, mo);

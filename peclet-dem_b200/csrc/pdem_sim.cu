@@ -1158,7 +1158,8 @@ void Sim<R>::detectAll(R margin) {
   // counts
   if (np > 0) {
     if (shell)
-      ++launches_, kNarrowShell<R, 0><<<gridFor((long)np * 32), kBlock, 0, stream_>>>(d_, np, P, iA_.p, nullptr);
+      ++launches_, kNarrowShell<R, 0><<<gridFor((long)np * 32), kBlock, shellStageBytes(), stream_>>>(
+          d_, np, P, iA_.p, nullptr, shellStageBytes());
     else
       ++launches_, kNarrowSphere<R, 0><<<gridFor(np), kBlock, 0, stream_>>>(d_, np, P, iA_.p, nullptr);
     KCHECK("narrow count");
@@ -1188,7 +1189,8 @@ void Sim<R>::detectAll(R margin) {
   }
   if (np > 0 && tot[0] > 0) {
     if (shell)
-      ++launches_, kNarrowShell<R, 1><<<gridFor((long)np * 32), kBlock, 0, stream_>>>(d_, np, P, nullptr, iB_.p);
+      ++launches_, kNarrowShell<R, 1><<<gridFor((long)np * 32), kBlock, shellStageBytes(), stream_>>>(
+          d_, np, P, nullptr, iB_.p, shellStageBytes());
     else {
       // iA_ (the 0/1 counts) is free after the scan: it receives the hit pair of every slot
       ++launches_, kHitIndex<<<gridFor(np), kBlock, 0, stream_>>>(np, iB_.p, iA_.p);

@@ -134,6 +134,12 @@ class Sim {
   // host-side facade state
   int capacity_ = 0, numReal_ = 0, numParticles_ = 0, maxPairs_ = 0, maxContacts_ = 0;
   int shellPoints_ = 0;
+  // bytes of the active shape's point shell that the shell narrowphase stages in shared memory
+  // (0: too large, read from global memory)
+  int shellStageBytes() const {
+    const long b = (long)shellPoints_ * (long)sizeof(Q4<R>);
+    return (shellPoints_ > 0 && b <= 32 * 1024) ? (int)b : 0;
+  }
   R baseRadius_ = 1, defInvI_[3] = {R(2.5), R(2.5), R(2.5)};
   R dmin_[3] = {0, 0, 0}, dmax_[3] = {0, 0, 0}, dsize_[3] = {0, 0, 0};
   bool per_[3] = {false, false, false};

@@ -31,3 +31,28 @@ def test_mixed_master_is_fp64(gpu_api):
     sim = P.build(gpu_api, sc, None, "mixed")
     x = sim.get_positions()
     np.testing.assert_array_equal(x, sc.pos)
+
+
+def test_mixed_error_vs_fp64_on_settled_bed(gpu_api):
+    """The mixed form against the FP64 step on the benchmark's settled 4,096-sphere bed, from the
+    same restart: within 5e-4 radii (max over the spheres) after one outer step of 10 substeps,
+    within 1e-2 after ten (measured on a B200: 1.1e-4 and 2.4e-3); after ten steps its error is no
+    larger than 1.5 times the plain FP32 step's (which is the reference's own precision), since
+    its FP64 master state only removes rounding."""
+    from peclet.dem import workloads as W
+    sc = W.plain_settled()
+    sims = {p: P.build(gpu_api, sc, None, p) for p in ("fp64", "mixed", "fp32")}
+    errs = {}
+    for step in range(1, 11):
+        for _ in range(sc.substeps):
+            for s in sims.values():
+                s.step(sc.dt)
+        if step in (1, 10):
+            x64 = sims["fp64"].get_positions()
+            for p in ("mixed", "fp32"):
+                errs[(p, step)] = float((np.linalg.norm(sims[p].get_positions() - x64, axis=1)).max()) / sc.global_scale
+    for s in sims.values():
+        s.close()
+    assert errs[("mixed", 1)] < 5e-4, errs
+    assert errs[("mixed", 10)] < 1e-2, errs
+    assert errs[("mixed", 10)] <= 1.5 * errs[("fp32", 10)], errs
