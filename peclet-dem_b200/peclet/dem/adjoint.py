@@ -312,6 +312,58 @@ class HertzSpheres:
             k += K
         return (x.clone(), v.clone(), w.clone()), (xd.clone(), vd.clone(), wd.clone())
 
+    def active_sets(self, x0, v0, w0, theta, steps):
+        """The touching contacts of every substep of a rollout (the branches its force law takes):
+        a list of `steps` sorted int64 key tensors (key i (n + nplane) + j of a sphere pair i < j,
+        i (n + nplane) + n + p of sphere i on plane p), each from the state the substep starts from:
+        overlap r_i + r_j - |x_i - x_j| > 0 (and |x_i - x_j| >= 1e-12) for a pair,
+        r_i - (x_i - p0) . n > 0 for a plane. Two rollouts with equal lists take the same branches
+        everywhere, so central differences between them see no contact onset or release."""
+        n = self.n
+        theta = tuple(float(t) for t in theta)
+        x, v, w = (torch.as_tensor(a, device=self.device).to(self.dtype).reshape(n, 3).contiguous()
+                   for a in (x0, v0, w0))
+        pl = self.planes.view(-1, 6)
+        prev_keys = prev_xi = None
+        out = []
+        k, rate = 0, None
+        while k < steps:
+            K = self._window_len(k, steps)
+            skin = self._skin(v, K) if rate is None else max(self.skin_min, 2.5 * rate * K)
+            while True:
+                cont, keys, idx, valid, start = self._start(x, v, w, skin, prev_keys, prev_xi)
+                traj = self.forward_window(start, cont, theta, K, store=True)
+                S = start.numel()
+                end = traj[K * S:(K + 1) * S]
+                disp = float((end[:3 * n] - start[:3 * n]).reshape(n, 3).norm(dim=1).max()) if n else 0.0
+                if disp <= 0.5 * skin:
+                    break
+                skin *= 2.0
+            rate = disp / K
+            i, j = cont[:, 0].long(), cont[:, 1].long()
+            pair = j >= 0
+            for q in range(K):
+                xq = traj[q * S:q * S + 3 * n].view(n, 3)
+                delta = torch.empty(i.shape, dtype=self.dtype, device=self.device)
+                if bool(pair.any()):
+                    d = (xq[i[pair]] - xq[j[pair]]).norm(dim=1)
+                    delta[pair] = torch.where(d >= 1e-12, self.r[i[pair]] + self.r[j[pair]] - d,
+                                              torch.zeros_like(d))
+                if bool((~pair).any()):
+                    p = -1 - j[~pair]
+                    dist = ((xq[i[~pair]] - pl[p, :3]) * pl[p, 3:]).sum(dim=1)
+                    delta[~pair] = self.r[i[~pair]] - dist
+                out.append(torch.sort(keys[delta > 0]).values)
+            x, v, w, prev_xi = self._split(end, int(cont.shape[0]))
+            prev_keys = keys
+            k += K
+        return out
+
+    @staticmethod
+    def same_branches(a, b):
+        """True when two active_sets lists are equal substep by substep."""
+        return len(a) == len(b) and all(p.numel() == q.numel() and bool(torch.equal(p, q)) for p, q in zip(a, b))
+
     def rollout(self, x0, v0, w0, theta, steps):
         """Differentiable rollout: (x, v, w) after `steps` substeps; gradients flow to x0, v0, w0
         and theta = tensor([E, e, mu])."""
