@@ -494,7 +494,7 @@ def run_batched(args, rank, world, dist, dem, W):
             sim.step(dt)
         t = max_over_ranks(sim.timer_stop() / 1e3, dist, "cuda")
         sweeps = sim.scene_counters()
-        tune = sim.scene_block()
+        tune = {"sweep_loops": sim.scene_block(), "colouring": sim.color_block()}
         x = sim.get_positions()
         sim.close()
         return t, sweeps, x, tune
@@ -506,11 +506,11 @@ def run_batched(args, rank, world, dist, dem, W):
     rate = lambda t: n_all * SUBSTEPS * args.steps / t
     return {"workload": f"rotating_drums_{len(scenes)}_scenes_after_deposition", "scenes": len(scenes),
             "particles": n_all, "deposition_s": t_dep, "presettle_steps": args.drum_presettle,
-            "fp64": {"value": rate(t64), "ms_per_step": 1e3 * t64 / args.steps, "autotuned_scene_block": tu64,
+            "fp64": {"value": rate(t64), "ms_per_step": 1e3 * t64 / args.steps, "autotuned_launch_shapes": tu64,
                      "mean_sweeps_last_substep": {"velocity": float(sw64[:, 2].mean()),
                                                   "stabilization": float(sw64[:, 3].mean()),
                                                   "position": float(sw64[:, 4].mean())}},
-            "mixed": {"value": rate(tmx), "ms_per_step": 1e3 * tmx / args.steps, "autotuned_scene_block": tumx,
+            "mixed": {"value": rate(tmx), "ms_per_step": 1e3 * tmx / args.steps, "autotuned_launch_shapes": tumx,
                       "err_vs_fp64": {"max_position_error_radii": err_max,
                                       "median_position_error_radii": float(np.median(err)) if err.size else 0.0,
                                       "after_substeps": (args.warmup + args.steps) * SUBSTEPS}},

@@ -251,6 +251,10 @@ int pdem_device_view(pdem_handle h, int field, void** ptr, long* rows, int* row_
  * the environment variable PDEM_SCENE_BLOCK fixes it instead) and the mean sweep-loop time of each
  * candidate in ms (cap values) */
 int pdem_scene_block(pdem_handle h, int* block, double* ms, int cap);
+/* batched form: the block size the autotuner chose for the colouring launch (0 while it is still
+ * timing the candidates 256, 512, 1024 over the first batched colourings; PDEM_COLOR_BLOCK fixes it
+ * instead) and each candidate's mean launch time in ms (cap values) */
+int pdem_color_block(pdem_handle h, int* block, double* ms, int cap);
 /* get_sdf_grid(resolution)                      src/dem_bindings.cpp:344-355, src/sim.hpp:1538-1542
  * packed-bed SDF over the domain (src/output_sdf.hpp:25-196), flat x-fastest; returns rx*ry*rz
  * (only cap written), or -1 with pdem_last_error() set */

@@ -484,6 +484,13 @@ int pdem_scene_block(pdem_handle h, int* block, double* ms, int cap) {
       ms[c] = (double)S.tuneMs()[c];
   });
 }
+int pdem_color_block(pdem_handle h, int* block, double* ms, int cap) {
+  BODY({
+    *block = S.tunedColorBlock();
+    for (int c = 0; c < cap && c < S.kColorTuneCands; ++c)
+      ms[c] = (double)S.colorTuneMs()[c];
+  });
+}
 long pdem_get_sdf_grid(pdem_handle h, int rx, int ry, int rz, double* out, long cap) {
   long n = -1;
   const int st = with(h, [&](auto& S) {

@@ -25,8 +25,10 @@ long gDeviceAllocs = 0;
 static const int kOne = 1;  // H2D source of a device flag set from the host
 
 void cudaCheck(cudaError_t e, const char* what) {
-  if (e != cudaSuccess)
+  if (e != cudaSuccess) {
+    cudaGetLastError();  // a refused launch leaves its (non-sticky) error for the next check
     throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
+  }
 }
 #define KCHECK(name) cudaCheck(cudaGetLastError(), name)
 
@@ -279,7 +281,7 @@ void Sim<R>::launchCoop(K kernel, A... args) {
 template <class R>
 template <class K, class... A>
 void Sim<R>::launchCoopSmem(K kernel, int block, size_t smem, A... args) {
-  const auto key = std::make_pair(reinterpret_cast<const void*>(kernel), smem);
+  const auto key = std::make_tuple(reinterpret_cast<const void*>(kernel), block, smem);
   auto it = coopPerSmem_.find(key);
   if (it == coopPerSmem_.end()) {
     cudaCheck(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem attribute");
@@ -1367,9 +1369,42 @@ void Sim<R>::colorBoth(int nm, int nc, int& ncolV, int& velLeft, int& ncolP, int
       (cudaMemsetAsync(gbar_.p, 0, 2 * sizeof(unsigned), stream_) == cudaSuccess) &&
       launchClusterCfg(kColorBoth<R, true>, sweepClusterBlocks_, kColorBlock, tailSmem, d_, jm, jc,
                        std::max(nbM, nbC) + 2, gb, (const int*)topoFlags_.p, topoValid_ ? 1 : 0);
+  // batched form: the launch-shape autotuner's colouring candidates (see colorTuning_)
+  const bool tuneColor = !inCluster && batch_ && colorTuning_;
+  const int slot = colorTuneStep_ % (kColorTuneCands * kTuneRounds);
+  if (tuneColor) {
+    if (!colorTuneEv_[0][0])
+      for (auto& pr : colorTuneEv_)
+        for (auto& e : pr)
+          cudaCheck(cudaEventCreate(&e), "event");
+    colorBlock_ = kColorTuneBlocks[colorTuneStep_ % kColorTuneCands];
+    cudaCheck(cudaEventRecord(colorTuneEv_[slot][0], stream_), "event");
+  }
   if (!inCluster)
     launchCoopSmem(kColorBoth<R>, colorBlock_, tailSmem, d_, jm, jc, std::max(nbM, nbC) + 2, gb,
                    (const int*)topoFlags_.p, topoValid_ ? 1 : 0);
+  if (tuneColor) {
+    cudaCheck(cudaEventRecord(colorTuneEv_[slot][1], stream_), "event");
+    if (++colorTuneStep_ == kColorTuneCands * kTuneRounds) {
+      sync();
+      float best = 0;
+      for (int c = 0; c < kColorTuneCands; ++c) {
+        float tot = 0;
+        for (int r = 0; r < kTuneRounds; ++r) {
+          float ms = 0;
+          cudaCheck(cudaEventElapsedTime(&ms, colorTuneEv_[r * kColorTuneCands + c][0],
+                                         colorTuneEv_[r * kColorTuneCands + c][1]), "event");
+          tot += ms;
+        }
+        colorTuneMs_[c] = tot / kTuneRounds;
+        if (c == 0 || tot < best) {
+          best = tot;
+          colorBlock_ = kColorTuneBlocks[c];
+        }
+      }
+      colorTuning_ = false;
+    }
+  }
   KCHECK("colour loop");
   int res[12], err = 0, differ[2] = {1, 1};
   readBack(res, colorAux_.p, sizeof res);

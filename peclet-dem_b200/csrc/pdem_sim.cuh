@@ -7,6 +7,7 @@
 #include <cstdint>
 #include <limits>
 #include <map>
+#include <tuple>
 #include <utility>
 #include <stdexcept>
 #include <string>
@@ -380,7 +381,7 @@ class Sim {
   // cooperative launch with `smem` bytes of dynamic shared memory (resident blocks counted with it)
   template <class K, class... A>
   void launchCoopSmem(K kernel, int block, size_t smem, A... args);
-  std::map<std::pair<const void*, size_t>, int> coopPerSmem_;
+  std::map<std::tuple<const void*, int, size_t>, int> coopPerSmem_;  // by (kernel, block, smem)
   // one thread-block cluster of sweepClusterBlocks_ blocks; false when such a cluster cannot be
   // resident
   template <class K, class... A>
@@ -458,12 +459,27 @@ class Sim {
  private:
   int ncolVLast_ = 0, ncolPLast_ = 0;  // colours of the last substep's two colourings
   int colorRounds_[2] = {0, 0};         // Jones-Plassmann rounds of the last manifold / contact colouring
-  // block size of the colouring launch (PDEM_COLOR_BLOCK overrides: 256, 512 or 1024)
+  // block size of the colouring launch (PDEM_COLOR_BLOCK fixes it: 256, 512 or 1024). In the
+  // batched form, without the variable, it is tuned online: the first kColorTuneCands x
+  // kTuneRounds colourings cycle through the candidates, timed with events, and the fastest stays
+  // (the colours do not depend on it: the rounds' winners are maxima of keys)
   int colorBlock_ = [] {
     const char* e = std::getenv("PDEM_COLOR_BLOCK");
     const int b = e ? (int)std::strtol(e, nullptr, 10) : 1024;
     return (b == 256 || b == 512) ? b : 1024;
   }();
+  bool colorTuning_ = std::getenv("PDEM_COLOR_BLOCK") == nullptr;
+  int colorTuneStep_ = 0;
+  cudaEvent_t colorTuneEv_[3 * 3][2] = {};
+  float colorTuneMs_[3] = {0, 0, 0};
+ public:
+  static constexpr int kColorTuneCands = 3;
+  static constexpr int kColorTuneBlocks[kColorTuneCands] = {256, 512, 1024};
+  // the colouring block the batched form's autotuner chose (0 while tuning) and each candidate's
+  // mean colouring-launch time (ms)
+  int tunedColorBlock() const { return (batch_ && colorTuning_) ? 0 : colorBlock_; }
+  const float* colorTuneMs() const { return colorTuneMs_; }
+ private:
   // entries left (both colourings) at which block 0 alone finishes the colouring; PDEM_COLOR_TAIL
   // overrides it (0 .. kColorTailMax). Measured: 1024 and 4096 alike on the 262k-sphere step, 1024
   // 6 % faster on the batched drums, 16384 and up far slower (one block, many entries a round)

@@ -122,6 +122,7 @@ _SIGS = {
     "set_wall_scene": (C.c_int, [_vp, C.c_int, C.c_int]),
     "scene_counters": (C.c_long, [_vp, _dbl_p, C.c_long]),
     "scene_block": (C.c_int, [_vp, _int_p, _dbl_p, C.c_int]),
+    "color_block": (C.c_int, [_vp, _int_p, _dbl_p, C.c_int]),
     "device_view": (C.c_int, [_vp, C.c_int, C.POINTER(_vp), _long_p, _int_p, _int_p]),
     "get_domain": (C.c_int, [_vp, _dbl_p, _dbl_p]),
     # candidate pairs over caller-owned device arrays, with no allocation (pdem_static.cu)
@@ -433,6 +434,14 @@ class CApiSimulation:
         ms = np.zeros(4)
         self._call("scene_block", C.byref(b), _ptr(ms), 4)
         return {"block": b.value, "candidates": [64, 128, 256, 512], "ms": ms.tolist()}
+
+    def color_block(self):
+        """The colouring launch block the batched form's autotuner chose (0 while tuning) and each
+        candidate's mean colouring-launch time (ms)."""
+        b = C.c_int(0)
+        ms = np.zeros(3)
+        self._call("color_block", C.byref(b), _ptr(ms), 3)
+        return {"block": b.value, "candidates": [256, 512, 1024], "ms": ms.tolist()}
 
     def scene_counters(self):
         """(S, 5): max overlap, max approach, velocity / stabilization / position sweeps."""

@@ -107,3 +107,27 @@ def test_autotuned_block_keeps_results(gpu_api, monkeypatch):
     assert ta["block"] in (64, 128, 256, 512) and all(m > 0 for m in ta["ms"])
     assert tb["block"] == 64
     assert not P.diff(a, b)
+
+
+def test_autotuned_colour_block_keeps_results(gpu_api, monkeypatch):
+    """The batched form also tunes the colouring launch's block (256, 512, 1024, timed over the
+    first colourings); the colours do not depend on it, so the run equals one with the block
+    fixed. The colourings run on the cooperative grid here (the one-cluster path takes no block)."""
+    monkeypatch.setenv("PDEM_COLOR_CLUSTER_ENTRIES", "0")
+    drums = _drums()
+    scenes = [d[0] for d in drums]
+    runs = []
+    for fixed in (None, "256"):
+        if fixed:
+            monkeypatch.setenv("PDEM_COLOR_BLOCK", fixed)
+        else:
+            monkeypatch.delenv("PDEM_COLOR_BLOCK", raising=False)
+        batch = CApiSimulation(gpu_api, sum(sc.n for sc in scenes) + 8, "fp32")
+        apply_batch(batch, scenes, [d[1] for d in drums])
+        for _ in range(16):
+            batch.step(scenes[0].dt)
+        runs.append((P.snapshot(batch, products=False), batch.color_block()))
+    (a, ta), (b, tb) = runs
+    assert ta["block"] in (256, 512, 1024) and all(m > 0 for m in ta["ms"])
+    assert tb["block"] == 256
+    assert not P.diff(a, b)
