@@ -307,6 +307,35 @@ int pdem_hz_backward(int precision, const pdem_hz_model* model, int steps, const
 int pdem_hz_jvp(int precision, const pdem_hz_model* model, int steps, void* d_state, void* d_tangent,
                 const double* theta_dot, void* d_work, void* stream);
 
+/* ---- adjoint of the XPBD substep (added form; no reference counterpart) ----
+ * The plain FP64 step (pdem_step, src/sim.hpp:97-488) differentiated over a recorded rollout:
+ * one scene of spheres without point shells, planes as walls, gravity on with the coloured
+ * Gauss-Seidel (PGS) velocity solve, stabilization "off" or "onesided", no periodicity, growth,
+ * thermostat or pair materials; every entry coloured (no Jacobi leftovers). Other set-ups are
+ * refused with PDEM_ERR_INVALID at pdem_xa_begin / pdem_xa_step. Rows are DEVICE doubles:
+ * positions, velocities and angular velocities n x 3, quaternions n x 4 (x, y, z, w).
+ * pdem_xa_begin sets the start state of a rollout (n = every particle), clears the warm-start
+ * ledger, the support levels and the topology caches (a rollout is a function of its start
+ * state and the material only) and starts a new record; pdem_xa_step runs `substeps` substeps
+ * of pdem_step (dt <= 0: the current substep length), recording each one's start state, ledger
+ * and frozen active set (contacts, manifolds, colourings, side flags, sweep counts);
+ * pdem_xa_state returns the current state rows. pdem_xa_backward takes the adjoint of the
+ * rollout's end state and returns the gradients with respect to its start state (rows as
+ * above) and to (eN, eT, mu) of pdem_set_material_params (dtheta: 3 doubles, HOST); it replays
+ * each substep from its record and reverses it, the sweeps in reverse colour and sweep order
+ * over the frozen colouring. Synchronise the caller's stream before these calls; each returns
+ * with the library's stream synchronised. pdem_xa_info: out[0] substeps recorded, out[1] bytes
+ * of the record, out[2] bytes of the reverse workspace, out[3] the largest sweep count;
+ * err[0] the largest deviation of a replayed substep's end positions from the recorded next
+ * state over the last backward, in units of the global scale, err[1] the same for velocities
+ * (m/s). */
+int pdem_xa_begin(pdem_handle h, const double* x, const double* q, const double* v, const double* w, int n);
+int pdem_xa_step(pdem_handle h, double dt, int substeps);
+int pdem_xa_state(pdem_handle h, double* x, double* q, double* v, double* w);
+int pdem_xa_backward(pdem_handle h, const double* gx, const double* gq, const double* gv, const double* gw,
+                     double* dx, double* dq, double* dv, double* dw, double* dtheta);
+int pdem_xa_info(pdem_handle h, long* out, double* err);
+
 #ifdef __cplusplus
 }
 #endif

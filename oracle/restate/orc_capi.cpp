@@ -2,13 +2,16 @@
 //
 // Exposes orc::Sim<float> / orc::Sim<double> behind the same `<prefix>_*` ABI as the B200 library
 // (include/pdem.h), with prefix `orc`, so the parity tests drive the oracle and the GPU through one
-// Python facade. Precision 32 restates the reference's float arithmetic; 64 is the FP64 oracle.
+// Python facade. Precision 32 restates the reference's float arithmetic; 64 is the FP64 oracle;
+// 65 is the FP64 oracle on forward-mode dual numbers (orc_dual.hpp): the same value run, with
+// tangents seeded by orc_dual_seed and read by orc_dual_get (the adjoint's forward-mode check).
 #include <cstring>
 #include <exception>
 #include <stdexcept>
 #include <string>
 #include <vector>
 
+#include "orc_dual.hpp"  // before the oracle: its std:: overloads must be visible to the templates
 #include "orc_sim.hpp"
 
 namespace {
@@ -17,6 +20,7 @@ thread_local std::string g_err;
 struct Handle {
   orc::Sim<float>* f = nullptr;
   orc::Sim<double>* d = nullptr;
+  orc::Sim<orc::Dual>* x = nullptr;
 };
 
 template <class F>
@@ -25,6 +29,8 @@ int with(void* h, F&& fn) {
     Handle* H = static_cast<Handle*>(h);
     if (H->f)
       fn(*H->f);
+    else if (H->x)
+      fn(*H->x);
     else
       fn(*H->d);
     return 0;
@@ -36,6 +42,10 @@ int with(void* h, F&& fn) {
     return 1;
   }
 }
+// a value as double (the value part of a dual number)
+inline double dv(double x) { return x; }
+inline double dv(float x) { return x; }
+inline double dv(const orc::Dual& x) { return x.v; }
 template <class R>
 std::vector<R> vec(const double* p, long n) {
   std::vector<R> v(n > 0 ? n : 0);
@@ -58,6 +68,8 @@ int orc_create(int capacity, int precision, void** out) {
     Handle* H = new Handle;
     if (precision == 32)
       H->f = new orc::Sim<float>(capacity);
+    else if (precision == 65)
+      H->x = new orc::Sim<orc::Dual>(capacity);
     else
       H->d = new orc::Sim<double>(capacity);
     *out = H;
@@ -71,6 +83,7 @@ void orc_destroy(void* h) {
   Handle* H = static_cast<Handle*>(h);
   delete H->f;
   delete H->d;
+  delete H->x;
   delete H;
 }
 
@@ -298,12 +311,12 @@ int orc_set_growth_params(void* h, double rate, double nf) {  // sim.hpp:1416-14
 }
 double orc_get_growth_factor(void* h) {
   double v = 0;
-  with(h, [&](auto& S) { v = S.growthFactor; });
+  with(h, [&](auto& S) { v = dv(S.growthFactor); });
   return v;
 }
 double orc_get_growth_rate(void* h) {
   double v = 0;
-  with(h, [&](auto& S) { v = S.growthRate; });
+  with(h, [&](auto& S) { v = dv(S.growthRate); });
   return v;
 }
 #define ORC_GET3(NAME, FIELD)                                          \
@@ -312,9 +325,9 @@ double orc_get_growth_rate(void* h) {
     with(h, [&](auto& S) {                                             \
       n = 3L * S.numReal;                                              \
       for (long i = 0; i < S.numReal && 3 * i + 2 < cap; ++i) {        \
-        out[3 * i] = S.FIELD[i].x;                                     \
-        out[3 * i + 1] = S.FIELD[i].y;                                 \
-        out[3 * i + 2] = S.FIELD[i].z;                                 \
+        out[3 * i] = dv(S.FIELD[i].x);                                     \
+        out[3 * i + 1] = dv(S.FIELD[i].y);                                 \
+        out[3 * i + 2] = dv(S.FIELD[i].z);                                 \
       }                                                                \
     });                                                                \
     return n;                                                          \
@@ -328,10 +341,10 @@ long orc_get_quaternions(void* h, double* out, long cap) {
   with(h, [&](auto& S) {
     n = 4L * S.numReal;
     for (long i = 0; i < S.numReal && 4 * i + 3 < cap; ++i) {
-      out[4 * i] = S.quat[i].x;
-      out[4 * i + 1] = S.quat[i].y;
-      out[4 * i + 2] = S.quat[i].z;
-      out[4 * i + 3] = S.quat[i].w;
+      out[4 * i] = dv(S.quat[i].x);
+      out[4 * i + 1] = dv(S.quat[i].y);
+      out[4 * i + 2] = dv(S.quat[i].z);
+      out[4 * i + 3] = dv(S.quat[i].w);
     }
   });
   return n;
@@ -341,7 +354,7 @@ long orc_get_scales(void* h, double* out, long cap) {
   with(h, [&](auto& S) {
     n = S.numReal;
     for (long i = 0; i < n && i < cap; ++i)
-      out[i] = S.scale[i];
+      out[i] = dv(S.scale[i]);
   });
   return n;
 }
@@ -369,7 +382,7 @@ int orc_step_hertz(void* h, double dt, int substeps, double skin) {
   });
 }
 int orc_compute_overlaps(void* h, double* out) {
-  return with(h, [&](auto& S) { *out = S.computeOverlaps(); });
+  return with(h, [&](auto& S) { *out = dv(S.computeOverlaps()); });
 }
 int orc_num_particles(void* h) {
   int n = 0;
@@ -388,13 +401,13 @@ int orc_num_manifolds(void* h) {
 }
 double orc_max_overlap(void* h) {
   double v = 0;
-  with(h, [&](auto& S) { v = S.maxOverlap; });
+  with(h, [&](auto& S) { v = dv(S.maxOverlap); });
   return v;
 }
 int orc_get_domain(void* h, double* mn, double* mx) {
   return with(h, [&](auto& S) {
-    mn[0] = S.dmin.x, mn[1] = S.dmin.y, mn[2] = S.dmin.z;
-    mx[0] = S.dmax.x, mx[1] = S.dmax.y, mx[2] = S.dmax.z;
+    mn[0] = dv(S.dmin.x), mn[1] = dv(S.dmin.y), mn[2] = dv(S.dmin.z);
+    mx[0] = dv(S.dmax.x), mx[1] = dv(S.dmax.y), mx[2] = dv(S.dmax.z);
   });
 }
 long orc_get_sdf_grid(void* h, int rx, int ry, int rz, double* out, long cap) {
@@ -448,8 +461,8 @@ long orc_debug_contacts(void* h, double* out, long cap) {
     n = S.contactCount;
     for (long i = 0; i < n && 17 * i + 16 < cap; ++i) {
       const auto& c = S.contacts[i];
-      const double v[17] = {(double)c.a, (double)c.b, c.n.x, c.n.y, c.n.z, c.rA.x, c.rA.y, c.rA.z,
-                            c.rB.x, c.rB.y, c.rB.z, c.dist, c.lamN, c.bvel.x, c.bvel.y, c.bvel.z, c.e};
+      const double v[17] = {(double)c.a, (double)c.b, dv(c.n.x), dv(c.n.y), dv(c.n.z), dv(c.rA.x), dv(c.rA.y), dv(c.rA.z),
+                            dv(c.rB.x), dv(c.rB.y), dv(c.rB.z), dv(c.dist), dv(c.lamN), dv(c.bvel.x), dv(c.bvel.y), dv(c.bvel.z), dv(c.e)};
       std::memcpy(out + 17 * i, v, sizeof v);
     }
   });
@@ -460,7 +473,7 @@ long orc_debug_contact_mu(void* h, double* out, long cap) {
   with(h, [&](auto& S) {
     n = S.contactCount;
     for (long i = 0; i < n && i < cap; ++i)
-      out[i] = S.contacts[i].mu;
+      out[i] = dv(S.contacts[i].mu);
   });
   return n;
 }
@@ -470,10 +483,10 @@ long orc_debug_manifolds(void* h, double* out, long cap) {
     n = S.manifoldCount;
     for (long i = 0; i < n && 23 * i + 22 < cap; ++i) {
       const auto& m = S.manifolds[i];
-      const double v[23] = {(double)m.a, (double)m.b, m.N.x,  m.N.y,  m.N.z,  m.TA.x,
-                            m.TA.y,      m.TA.z,      m.TB.x, m.TB.y, m.TB.z, m.rA.x,
-                            m.rA.y,      m.rA.z,      m.rB.x, m.rB.y, m.rB.z, (double)m.np,
-                            m.wv.x,      m.wv.y,      m.wv.z, m.e,    m.mu};
+      const double v[23] = {(double)m.a, (double)m.b, dv(m.N.x),  dv(m.N.y),  dv(m.N.z),  dv(m.TA.x),
+                            dv(m.TA.y),      dv(m.TA.z),      dv(m.TB.x), dv(m.TB.y), dv(m.TB.z), dv(m.rA.x),
+                            dv(m.rA.y),      dv(m.rA.z),      dv(m.rB.x), dv(m.rB.y), dv(m.rB.z), (double)m.np,
+                            dv(m.wv.x),      dv(m.wv.y),      dv(m.wv.z), dv(m.e),    dv(m.mu)};
       std::memcpy(out + 23 * i, v, sizeof v);
     }
   });
@@ -502,10 +515,10 @@ long orc_debug_lambda(void* h, double* out, long cap) {
   with(h, [&](auto& S) {
     n = S.manifoldCount;
     for (long i = 0; i < n && 4 * i + 3 < cap; ++i) {
-      out[4 * i] = S.lambdaAcc[i];
-      out[4 * i + 1] = S.lambdaT[i].x;
-      out[4 * i + 2] = S.lambdaT[i].y;
-      out[4 * i + 3] = S.lambdaT[i].z;
+      out[4 * i] = dv(S.lambdaAcc[i]);
+      out[4 * i + 1] = dv(S.lambdaT[i].x);
+      out[4 * i + 2] = dv(S.lambdaT[i].y);
+      out[4 * i + 3] = dv(S.lambdaT[i].z);
     }
   });
   return n;
@@ -525,11 +538,11 @@ long orc_debug_ledger(void* h, unsigned long long* keys, double* vals, long cap)
     n = S.prevPairCount;
     for (long i = 0; i < n && i < cap; ++i) {
       keys[i] = S.prevPairKeys[i];
-      vals[5 * i] = S.prevLambda[i];
-      vals[5 * i + 1] = S.prevLambdaT[i].x;
-      vals[5 * i + 2] = S.prevLambdaT[i].y;
-      vals[5 * i + 3] = S.prevLambdaT[i].z;
-      vals[5 * i + 4] = S.prevPosImpulse[i];
+      vals[5 * i] = dv(S.prevLambda[i]);
+      vals[5 * i + 1] = dv(S.prevLambdaT[i].x);
+      vals[5 * i + 2] = dv(S.prevLambdaT[i].y);
+      vals[5 * i + 3] = dv(S.prevLambdaT[i].z);
+      vals[5 * i + 4] = dv(S.prevPosImpulse[i]);
     }
   });
   return n;
@@ -548,7 +561,7 @@ long orc_debug_pos_lambda(void* h, double* out, long cap) {
   with(h, [&](auto& S) {
     n = S.contactCount;
     for (long i = 0; i < n && i < cap; ++i)
-      out[i] = S.posLambdaContact[i];
+      out[i] = dv(S.posLambdaContact[i]);
   });
   return n;
 }
@@ -558,9 +571,9 @@ long orc_debug_hertz(void* h, unsigned long long* keys, double* xi, long cap) {
     n = S.hzNumPairs;
     for (long i = 0; i < n && i < cap; ++i) {
       keys[i] = S.hzKeys[i];
-      xi[3 * i] = S.hzXi[i].x;
-      xi[3 * i + 1] = S.hzXi[i].y;
-      xi[3 * i + 2] = S.hzXi[i].z;
+      xi[3 * i] = dv(S.hzXi[i].x);
+      xi[3 * i + 1] = dv(S.hzXi[i].y);
+      xi[3 * i + 2] = dv(S.hzXi[i].z);
     }
   });
   return n;
@@ -572,5 +585,61 @@ int orc_debug_set_max_contacts(void* h, int maxC) {
     S.maxContacts = maxC;
   });
 }
+
+// Tangent lanes of the dual-number oracle (precision 65). `which`: 0 positions, 1 velocities,
+// 2 angular velocities (n x 3 each), 3 quaternions (n x 4), 4 the material (eN, eT, mu). Seeding
+// sets lane `lane` of those values to t; reading returns it. Status 2 when the handle is not dual.
+}  // extern "C"
+namespace {
+template <class F>
+int dualDo(void* h, F&& fn) {
+  Handle* H = static_cast<Handle*>(h);
+  if (!H->x) {
+    g_err = "not a dual-number oracle (precision 65)";
+    return 2;
+  }
+  fn(*H->x);
+  return 0;
+}
+template <class G>
+void dualFields(orc::Sim<orc::Dual>& S, int which, long n, G&& g) {
+  if (which >= 0 && which <= 2) {
+    auto& f = which == 0 ? S.pos : which == 1 ? S.vel : S.angVel;
+    for (long i = 0; i < n; ++i) {
+      g(f[i].x, 3 * i);
+      g(f[i].y, 3 * i + 1);
+      g(f[i].z, 3 * i + 2);
+    }
+  } else if (which == 3) {
+    for (long i = 0; i < n; ++i) {
+      g(S.quat[i].x, 4 * i);
+      g(S.quat[i].y, 4 * i + 1);
+      g(S.quat[i].z, 4 * i + 2);
+      g(S.quat[i].w, 4 * i + 3);
+    }
+  } else if (which == 4) {
+    g(S.eN, 0);
+    g(S.eT, 1);
+    g(S.mu, 2);
+  }
+}
+}  // namespace
+extern "C" {
+
+int orc_dual_seed(void* h, int which, int lane, const double* t, long n) {
+  if (lane < 0 || lane >= orc::kDualLanes || which < 0 || which > 4)
+    return 2;
+  return dualDo(h, [&](orc::Sim<orc::Dual>& S) {
+    dualFields(S, which, std::min<long>(n, S.numReal), [&](orc::Dual& x, long k) { x.d[lane] = t[k]; });
+  });
+}
+int orc_dual_get(void* h, int which, int lane, double* t, long n) {
+  if (lane < 0 || lane >= orc::kDualLanes || which < 0 || which > 4)
+    return 2;
+  return dualDo(h, [&](orc::Sim<orc::Dual>& S) {
+    dualFields(S, which, std::min<long>(n, S.numReal), [&](orc::Dual& x, long k) { t[k] = x.d[lane]; });
+  });
+}
+int orc_dual_lanes() { return orc::kDualLanes; }
 
 }  // extern "C"

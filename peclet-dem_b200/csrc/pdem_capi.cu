@@ -10,6 +10,7 @@
 
 #include "../../include/pdem.h"
 #include "pdem_sim.cuh"
+#include "pdem_xadj_api.cuh"
 
 using pdem::Sim;
 
@@ -630,5 +631,18 @@ int pdem_profile_read(pdem_handle h, double* ms, long* calls, int cap, long* lau
   });
   return n;
 }
+
+int pdem_xa_begin(pdem_handle h, const double* x, const double* q, const double* v, const double* w, int n) {
+  BODY(pdem::xadjBegin(S, x, q, v, w, n));
+}
+int pdem_xa_step(pdem_handle h, double dt, int substeps) { BODY(pdem::xadjStep(S, dt, substeps)); }
+int pdem_xa_state(pdem_handle h, double* x, double* q, double* v, double* w) {
+  BODY(pdem::xadjState(S, x, q, v, w));
+}
+int pdem_xa_backward(pdem_handle h, const double* gx, const double* gq, const double* gv, const double* gw,
+                     double* dx, double* dq, double* dv, double* dw, double* dtheta) {
+  BODY(pdem::xadjBackward(S, gx, gq, gv, gw, dx, dq, dv, dw, dtheta));
+}
+int pdem_xa_info(pdem_handle h, long* out, double* err) { BODY(pdem::xadjInfo(S, out, err)); }
 
 }  // extern "C"

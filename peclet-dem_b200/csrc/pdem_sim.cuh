@@ -7,6 +7,7 @@
 #include <cstdint>
 #include <limits>
 #include <map>
+#include <memory>
 #include <tuple>
 #include <utility>
 #include <stdexcept>
@@ -68,11 +69,17 @@ struct DBuf {
   }
 };
 
+struct XAdjAccess;  // the XPBD adjoint (pdem_xadj.cu) reads the step's buffers
+
 template <class R>
 class Sim {
+  friend struct XAdjAccess;
+
  public:
   explicit Sim(int capacity);
   ~Sim();
+  // the XPBD adjoint's record and workspace (pdem_xadj.cu), created by its first use
+  std::shared_ptr<void> xadj_;
 
   // ---- facade (src/sim.hpp:943-1424) ----
   void initializeShape(int type, R radius, R height, R thick);

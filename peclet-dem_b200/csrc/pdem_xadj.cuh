@@ -1,0 +1,669 @@
+// Adjoint of the XPBD substep (plain FP64 path, spheres and planes): the per-entry local maps
+// and their vector-Jacobian products.
+//
+// Every stage of the substep that the reverse pass differentiates is written once here as a
+// local map from a flat array of active inputs to a flat array of outputs, templated on the
+// scalar type:
+//   - with T = double it is the replay: the same expressions, in the same order, as the forward
+//     step (src/integration.hpp:44-148, src/narrowphase.hpp:179-268 and :371-449,
+//     src/contact_preprocessing.hpp:339-374, src/solver_velocity.hpp:390-605 and :641-858,
+//     src/solver_position.hpp:248-331), so the replay takes the forward's branches;
+//   - with T = Dd<K> (forward-mode dual numbers with K tangent lanes) it yields K columns of the
+//     map's Jacobian at once; vjp() seeds the inputs K at a time and contracts the output
+//     tangents with the output adjoints, which is the map's vector-Jacobian product.
+// The branch decisions (active contact, clamps of the normal impulse and of the friction cone,
+// restitution cut-off, side flags) are taken on the values, so the derivative is the one of the
+// branch the forward took. The sweep-level reversal (colours and sweeps in reverse order over the
+// frozen colouring, checkpoints and replays) is in pdem_xadj.cu.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "pdem_math.cuh"
+
+namespace pdem {
+namespace xadj {
+
+// ---- forward-mode dual numbers ------------------------------------------------------------
+// K = 7 lanes: sizeof(Dd<7>) = 64 B, so Q4<Dd<7>> (aligned to 4 x its element) stays a power of 2
+constexpr int kLanes = 7;
+
+template <int K>
+struct Dd {
+  double v;
+  double d[K];
+  PD Dd() : v(0.0) {
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+      d[k] = 0.0;
+  }
+  PD Dd(double x) : v(x) {
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+      d[k] = 0.0;
+  }
+};
+template <int K>
+PD Dd<K> operator+(const Dd<K>& a, const Dd<K>& b) {
+  Dd<K> r(a.v + b.v);
+#pragma unroll
+  for (int k = 0; k < K; ++k)
+    r.d[k] = a.d[k] + b.d[k];
+  return r;
+}
+template <int K>
+PD Dd<K> operator-(const Dd<K>& a, const Dd<K>& b) {
+  Dd<K> r(a.v - b.v);
+#pragma unroll
+  for (int k = 0; k < K; ++k)
+    r.d[k] = a.d[k] - b.d[k];
+  return r;
+}
+template <int K>
+PD Dd<K> operator-(const Dd<K>& a) {
+  Dd<K> r(-a.v);
+#pragma unroll
+  for (int k = 0; k < K; ++k)
+    r.d[k] = -a.d[k];
+  return r;
+}
+template <int K>
+PD Dd<K> operator*(const Dd<K>& a, const Dd<K>& b) {
+  Dd<K> r(a.v * b.v);
+#pragma unroll
+  for (int k = 0; k < K; ++k)
+    r.d[k] = a.d[k] * b.v + a.v * b.d[k];
+  return r;
+}
+template <int K>
+PD Dd<K> operator/(const Dd<K>& a, const Dd<K>& b) {
+  const double q = a.v / b.v;
+  Dd<K> r(q);
+#pragma unroll
+  for (int k = 0; k < K; ++k)
+    r.d[k] = (a.d[k] - q * b.d[k]) / b.v;
+  return r;
+}
+// mixed forms with a plain double (a constant of the map), value arithmetic unchanged
+template <int K>
+PD Dd<K> operator+(const Dd<K>& a, double b) {
+  Dd<K> r = a;
+  r.v = a.v + b;
+  return r;
+}
+template <int K>
+PD Dd<K> operator+(double a, const Dd<K>& b) {
+  Dd<K> r = b;
+  r.v = a + b.v;
+  return r;
+}
+template <int K>
+PD Dd<K> operator-(const Dd<K>& a, double b) {
+  Dd<K> r = a;
+  r.v = a.v - b;
+  return r;
+}
+template <int K>
+PD Dd<K> operator-(double a, const Dd<K>& b) {
+  Dd<K> r(a - b.v);
+#pragma unroll
+  for (int k = 0; k < K; ++k)
+    r.d[k] = -b.d[k];
+  return r;
+}
+template <int K>
+PD Dd<K> operator*(const Dd<K>& a, double b) {
+  Dd<K> r(a.v * b);
+#pragma unroll
+  for (int k = 0; k < K; ++k)
+    r.d[k] = a.d[k] * b;
+  return r;
+}
+template <int K>
+PD Dd<K> operator*(double a, const Dd<K>& b) {
+  Dd<K> r(a * b.v);
+#pragma unroll
+  for (int k = 0; k < K; ++k)
+    r.d[k] = a * b.d[k];
+  return r;
+}
+template <int K>
+PD Dd<K> operator/(const Dd<K>& a, double b) {
+  Dd<K> r(a.v / b);
+#pragma unroll
+  for (int k = 0; k < K; ++k)
+    r.d[k] = a.d[k] / b;
+  return r;
+}
+template <int K>
+PD Dd<K> operator/(double a, const Dd<K>& b) {
+  const double q = a / b.v;
+  Dd<K> r(q);
+#pragma unroll
+  for (int k = 0; k < K; ++k)
+    r.d[k] = -q * b.d[k] / b.v;
+  return r;
+}
+template <int K>
+PD Dd<K>& operator+=(Dd<K>& a, const Dd<K>& b) {
+  return a = a + b;
+}
+template <int K>
+PD bool operator<(const Dd<K>& a, const Dd<K>& b) { return a.v < b.v; }
+template <int K>
+PD bool operator>(const Dd<K>& a, const Dd<K>& b) { return a.v > b.v; }
+template <int K>
+PD bool operator<=(const Dd<K>& a, const Dd<K>& b) { return a.v <= b.v; }
+template <int K>
+PD bool operator>=(const Dd<K>& a, const Dd<K>& b) { return a.v >= b.v; }
+template <int K>
+PD bool operator==(const Dd<K>& a, const Dd<K>& b) { return a.v == b.v; }
+template <int K>
+PD bool operator!=(const Dd<K>& a, const Dd<K>& b) { return a.v != b.v; }
+template <int K>
+PD bool operator<(const Dd<K>& a, double b) { return a.v < b; }
+template <int K>
+PD bool operator>(const Dd<K>& a, double b) { return a.v > b; }
+template <int K>
+PD bool operator<=(const Dd<K>& a, double b) { return a.v <= b; }
+template <int K>
+PD bool operator>=(const Dd<K>& a, double b) { return a.v >= b; }
+template <int K>
+PD bool operator!=(const Dd<K>& a, double b) { return a.v != b; }
+template <int K>
+PD bool operator==(const Dd<K>& a, double b) { return a.v == b; }
+
+template <int K>
+PD Dd<K> sqrt(const Dd<K>& a) {
+  const double s = ::sqrt(a.v);
+  const double g = s > 0.0 ? 0.5 / s : 0.0;
+  Dd<K> r(s);
+#pragma unroll
+  for (int k = 0; k < K; ++k)
+    r.d[k] = g * a.d[k];
+  return r;
+}
+template <int K>
+PD Dd<K> fabs(const Dd<K>& a) {
+  return a.v < 0.0 ? -a : a;
+}
+template <int K>
+PD Dd<K> fmax(const Dd<K>& a, const Dd<K>& b) {
+  return (b.v > a.v) ? b : a;
+}
+
+// the same functions on plain doubles (the replay instantiation), which the templates above hide
+PD double sqrt(double a) { return ::sqrt(a); }
+PD double fabs(double a) { return ::fabs(a); }
+PD double fmax(double a, double b) { return ::fmax(a, b); }
+
+// value of a scalar of either kind
+PD double val(double x) { return x; }
+template <int K>
+PD double val(const Dd<K>& x) {
+  return x.v;
+}
+
+// ---- constants of the maps (not differentiated) ---------------------------------------------
+struct BodyC {     // one body
+  double im;       // inverse mass
+  V3<double> iI;   // inverse inertia (body frame)
+};
+struct StepC {     // the substep
+  double dt;
+  V3<double> g;
+  double vRest;    // 2 dt |g| (main sweeps) or the stabilization threshold
+  double eps;      // central-difference step of the SDF normal (canonical units)
+};
+
+// flat views of vectors in an input/output array
+template <class T>
+PD V3<T> ld3(const T* a, int o) {
+  return V3<T>{a[o], a[o + 1], a[o + 2]};
+}
+template <class T>
+PD Q4<T> ld4(const T* a, int o) {
+  return Q4<T>{a[o], a[o + 1], a[o + 2], a[o + 3]};
+}
+template <class T>
+PD void st3(T* a, int o, V3<T> v) {
+  a[o] = v.x, a[o + 1] = v.y, a[o + 2] = v.z;
+}
+template <class T>
+PD void st4(T* a, int o, Q4<T> v) {
+  a[o] = v.x, a[o + 1] = v.y, a[o + 2] = v.z, a[o + 3] = v.w;
+}
+template <class T>
+PD V3<T> cv3(V3<double> a) {
+  return V3<T>{T(a.x), T(a.y), T(a.z)};
+}
+
+// ---- predictVelocity (src/integration.hpp:44-93) ------------------------------------------
+// in: x[0..3) q[3..7) v[7..10) w[10..13)   out: vP[0..3) wP[3..6) xP[6..9)
+constexpr int kPredIn = 13, kPredOut = 9;
+template <class T>
+PD void predictMap(const T* in, T* out, const BodyC& b, const StepC& s, V3<double> F) {
+  const double im = b.im, dtt = s.dt;
+  V3<T> v = ld3(in, 7);
+  if (im > 0.0) {
+    v = add(v, cv3<T>(mul(s.g, dtt)));
+    v = add(v, cv3<T>(mul(F, im * dtt)));
+  }
+  V3<T> wp = ld3(in, 10);
+  if (im > 0.0) {
+    const V3<double> ii = b.iI;
+    if (ii.x > 0.0 || ii.y > 0.0 || ii.z > 0.0) {
+      const Q4<T> q = ld4(in, 3);
+      V3<T> wb = invrot(q, ld3(in, 10));
+      const V3<double> Ib{(ii.x > 1e-9) ? 1.0 / ii.x : 0.0, (ii.y > 1e-9) ? 1.0 / ii.y : 0.0,
+                          (ii.z > 1e-9) ? 1.0 / ii.z : 0.0};
+      const V3<T> Lb{T(Ib.x) * wb.x, T(Ib.y) * wb.y, T(Ib.z) * wb.z};
+      const V3<T> wxL = cross(wb, Lb);
+      const V3<T> al{T(-ii.x) * wxL.x, T(-ii.y) * wxL.y, T(-ii.z) * wxL.z};
+      wb = add(wb, mul(al, T(dtt)));
+      wp = rot(q, wb);
+    }
+  }
+  V3<T> x = ld3(in, 0);
+  if (im > 0.0)
+    x = add(x, mul(v, T(dtt)));
+  st3(out, 0, v);
+  st3(out, 3, wp);
+  st3(out, 6, x);
+}
+
+// ---- sphere-sphere contact (src/narrowphase.hpp:179-268, spheres: no shell points) ----------
+// in: xA[0..3) qA[3..7) xB[7..10) qB[10..14)   out: n[0..3) rA[3..6) rB[6..9) dist[9]
+constexpr int kConIn = 14, kConOut = 10;
+struct ConC {
+  double sA, sB;     // scale x global scale of each body
+  double parA, parB; // canonical sphere radii
+  double eps;
+};
+template <class T>
+PD T sdfSph(V3<T> p, double r) {
+  return vlen(p) - T(r);
+}
+template <class T>
+PD void contactMap(const T* in, T* out, const ConC& c) {
+  const V3<T> pA = ld3(in, 0), pB = ld3(in, 7);
+  const Q4<T> qA = ld4(in, 3), qB = ld4(in, 10);
+  const T sA(c.sA), sB(c.sB);
+  const T prad = T(c.parA) * sA;
+  const V3<T> pl{T(0.0), T(0.0), T(0.0)};
+  const V3<T> pw = add(pA, rot(qA, mul(pl, sA)));
+  const V3<T> plB = invrot(qB, sub(pw, pB));
+  const V3<T> pc = mul(plB, T(1.0) / sB);
+  const T dist = sdfSph(pc, c.parB) * sB;
+  const T eff = dist - prad;
+  const T eps(c.eps);
+  V3<T> nl{sdfSph(V3<T>{pc.x + eps, pc.y, pc.z}, c.parB) - sdfSph(V3<T>{pc.x - eps, pc.y, pc.z}, c.parB),
+           sdfSph(V3<T>{pc.x, pc.y + eps, pc.z}, c.parB) - sdfSph(V3<T>{pc.x, pc.y - eps, pc.z}, c.parB),
+           sdfSph(V3<T>{pc.x, pc.y, pc.z + eps}, c.parB) - sdfSph(V3<T>{pc.x, pc.y, pc.z - eps}, c.parB)};
+  const T l = vlen(nl);
+  nl = (l > T(1e-9)) ? mul(nl, T(1.0) / l) : V3<T>{T(0.0), T(1.0), T(0.0)};
+  const V3<T> nw = rot(qB, nl);
+  const V3<T> ps = sub(pw, mul(nw, prad));
+  st3(out, 0, nw);
+  st3(out, 3, sub(ps, pA));
+  st3(out, 6, sub(sub(ps, mul(nw, eff)), pB));
+  out[9] = eff;
+}
+
+// ---- contact -> manifold contribution (src/contact_preprocessing.hpp:339-374) --------------
+// in: n[0..3) rA[3..6) rB[6..9) dist[9]   out: N[0..3) TA[3..6) TB[6..9) rA[9..12) rB[12..15)
+constexpr int kManIn = 10, kManOut = 15;
+template <class T>
+PD void manifoldMap(const T* in, T* out, bool flip) {
+  const V3<T> n = ld3(in, 0), rA = ld3(in, 3), rB = ld3(in, 6);
+  const T dist = in[9];
+  const V3<T> na = flip ? n : neg(n);
+  const V3<T> sh{n.x * dist * T(0.5), n.y * dist * T(0.5), n.z * dist * T(0.5)};
+  const V3<T> ra = sub(rA, sh);
+  const V3<T> rb = add(rB, sh);
+  const V3<T> rc = flip ? rb : ra, ro = flip ? ra : rb;
+  st3(out, 0, na);
+  st3(out, 3, cross(rc, na));
+  st3(out, 6, cross(ro, neg(na)));
+  st3(out, 9, rc);
+  st3(out, 12, ro);
+}
+
+// manifold geometry in a flat array: N[0..3) TA[3..6) TB[6..9) rA[9..12) rB[12..15) (sums)
+constexpr int kGeo = 15;
+struct ManC {
+  double invN;        // 1 / number of penetrating contacts
+  bool hasB;          // body-body (else a wall manifold)
+  V3<double> wv;      // summed wall velocity (wall manifolds)
+  double imA, imB;
+  V3<double> iIA, iIB;
+  double eAvg, muAvg; // summed pair restitution / friction x invN (negative: the globals)
+  int sf;             // side flag of the sweep
+};
+
+// ---- approach velocity before the solve (src/solver_velocity.hpp:390-453) -----------------
+// in: vA[0..3) wA[3..6) vB[6..9) wB[9..12) geo[12..27)   out: vn0[0] vt0[1..4)
+constexpr int kVn0In = 27, kVn0Out = 4;
+template <class T>
+PD void vn0Map(const T* in, T* out, const ManC& m) {
+  const V3<T> vA = ld3(in, 0), wA = ld3(in, 3);
+  V3<T> vB{T(0.0), T(0.0), T(0.0)}, wB{T(0.0), T(0.0), T(0.0)};
+  const T invN(m.invN);
+  if (m.hasB) {
+    vB = ld3(in, 6);
+    wB = ld3(in, 9);
+  } else {
+    vB = mul(cv3<T>(m.wv), invN);
+  }
+  const V3<T> N = ld3(in, 12), TA = ld3(in, 15), TB = ld3(in, 18);
+  const V3<T> rAa = mul(ld3(in, 21), invN), rBa = mul(ld3(in, 24), invN);
+  const V3<T> dc = m.hasB ? sub(rAa, rBa) : rAa;
+  const V3<T> vG = mul(dc, T(0.0));  // growth rate 0 (growth is outside the adjoint's scope)
+  T vn = dot(vA, N) + dot(wA, TA) + dot(vB, neg(N)) + dot(wB, TB);
+  vn += dot(vG, N);
+  const T lenN = sqrt(dot(N, N));
+  V3<T> vt{T(0.0), T(0.0), T(0.0)};
+  if (lenN > T(1e-9)) {
+    const V3<T> nh = mul(N, T(1.0) / lenN);
+    const V3<T> wBv = m.hasB ? wB : V3<T>{T(0.0), T(0.0), T(0.0)};
+    const V3<T> vr = sub(add(vA, cross(wA, rAa)), add(vB, cross(wBv, rBa)));
+    vt = sub(vr, mul(nh, dot(vr, nh)));
+  }
+  out[0] = vn;
+  st3(out, 1, vt);
+}
+
+// ---- warm start (src/solver_velocity.hpp:498-605) -----------------------------------------
+// in: vA[0..3) wA[3..6) vB[6..9) wB[9..12) p[12] lt[13..16) geo[16..31) qA[31..35) qB[35..39)
+// out: vA[0..3) wA[3..6) vB[6..9) wB[9..12) lt[12..15)
+constexpr int kWarmIn = 39, kWarmOut = 15;
+template <class T>
+PD void warmMap(const T* in, T* out, const ManC& m) {
+  V3<T> vA = ld3(in, 0), wA = ld3(in, 3), vB = ld3(in, 6), wB = ld3(in, 9);
+  const T p = in[12];
+  V3<T> lt = ld3(in, 13);
+  const V3<T> N = ld3(in, 16), TA = ld3(in, 19), TB = ld3(in, 22);
+  const Q4<T> qA = ld4(in, 31), qB = ld4(in, 35);
+  const T invN(m.invN);
+  const bool hasT = lt.x != T(0.0) || lt.y != T(0.0) || lt.z != T(0.0);
+  if (p != T(0.0) || hasT) {
+    const V3<T> rAa = mul(ld3(in, 25), invN), rBa = mul(ld3(in, 28), invN);
+    const V3<T> dc = m.hasB ? sub(rAa, rBa) : rAa;
+    const T al = dot(N, dc);
+    const T sgn = (al > T(0.0)) ? T(1.0) : T(-1.0);
+    const T lam = -sgn * p;
+    const V3<T> J = mul(N, lam);
+    const T imA(m.imA), imB(m.imB);
+    const V3<T> iIA = cv3<T>(m.iIA), iIB = cv3<T>(m.iIB);
+    vA = add(vA, mul(J, imA));
+    wA = add(wA, angResponse(qA, mul(TA, lam), iIA));
+    if (m.hasB) {
+      vB = add(vB, mul(neg(J), imB));
+      wB = add(wB, angResponse(qB, mul(TB, lam), iIB));
+    }
+    if (hasT) {
+      const T l2 = sqrt(dot(N, N));
+      if (l2 > T(1e-9)) {
+        const V3<T> nh = mul(N, T(1.0) / l2);
+        lt = sub(lt, mul(nh, dot(lt, nh)));
+      }
+      vA = add(vA, mul(lt, imA));
+      wA = add(wA, angResponse(qA, cross(rAa, lt), iIA));
+      if (m.hasB) {
+        vB = add(vB, mul(neg(lt), imB));
+        wB = add(wB, angResponse(qB, cross(rBa, mul(lt, T(-1.0))), iIB));
+      }
+    }
+  }
+  st3(out, 0, vA);
+  st3(out, 3, wA);
+  st3(out, 6, vB);
+  st3(out, 9, wB);
+  st3(out, 12, lt);
+}
+
+// ---- one PGS update of a manifold (src/solver_velocity.hpp:641-858) -----------------------
+// in: vA[0..3) wA[3..6) vB[6..9) wB[9..12) p[12] lt[13..16) geo[16..31) qA[31..35) qB[35..39)
+//     vn0[39] vt0[40..43) posImp[43] eN[44] eT[45] mu[46]
+// out: vA[0..3) wA[3..6) vB[6..9) wB[9..12) p[12] lt[13..16)
+constexpr int kPgsIn = 47, kPgsOut = 16;
+template <class T>
+PD void pgsMap(const T* in, T* out, const ManC& m, double vRest) {
+  const V3<T> vA = ld3(in, 0), wA = ld3(in, 3);
+  const T invN(m.invN);
+  V3<T> vB{T(0.0), T(0.0), T(0.0)}, wB{T(0.0), T(0.0), T(0.0)};
+  if (m.hasB) {
+    vB = ld3(in, 6);
+    wB = ld3(in, 9);
+  } else {
+    vB = mul(cv3<T>(m.wv), invN);
+  }
+  const V3<T> N = ld3(in, 16), TA = ld3(in, 19), TB = ld3(in, 22);
+  const V3<T> rAa = mul(ld3(in, 25), invN), rBa = mul(ld3(in, 28), invN);
+  const V3<T> dc = m.hasB ? sub(rAa, rBa) : rAa;
+  const Q4<T> qA = ld4(in, 31), qB = ld4(in, 35);
+  const T vn0 = in[39];
+  const T posImp = in[43];
+  const T imA(m.imA), imB(m.imB);
+  const V3<T> iIA = cv3<T>(m.iIA), iIB = cv3<T>(m.iIB);
+  T pOld = in[12];
+  V3<T> ltOld = ld3(in, 13);
+  // outputs default to the inputs (an early return leaves the entry unchanged)
+  for (int k = 0; k < 12; ++k)
+    out[k] = in[k];
+  out[12] = pOld;
+  st3(out, 13, ltOld);
+  T e = in[44];
+  if (m.eAvg >= 0.0)
+    e = T(m.eAvg);
+  const T lenN = sqrt(dot(N, N));
+  if (lenN < T(1e-9))
+    return;
+  const V3<T> vG = mul(dc, T(0.0));
+  T vn = dot(vA, N) + dot(wA, TA) + dot(vB, neg(N)) + dot(wB, TB);
+  vn += dot(vG, N);
+  const T al = dot(N, dc);
+  const T sgn = (al > T(0.0)) ? T(1.0) : T(-1.0);
+  const T Nsq = dot(N, N);
+  T wAn = Nsq * imA + genInvMass(TA, iIA, qA);
+  T wBn = Nsq * imB + genInvMass(TB, iIB, qB);
+  bool applyA = true, applyB = true;
+  if (m.sf == 1) {
+    wBn = T(0.0);
+    applyB = false;
+    e = T(0.0);
+  } else if (m.sf == 2) {
+    wAn = T(0.0);
+    applyA = false;
+    e = T(0.0);
+  }
+  const T wT = wAn + wBn;
+  if (wT <= T(0.0))
+    return;
+  const T v0 = sgn * vn0;
+  if (fabs(vn0) < T(vRest) * lenN)
+    e = T(0.0);
+  const T target = (v0 > T(0.0)) ? -e * v0 : T(0.0);
+  const T vt = sgn * vn;
+  const T dp = (vt - target) / wT;
+  T pNew = pOld + dp;
+  if (pNew < T(0.0))
+    pNew = T(0.0);
+  const T dA = pNew - pOld;
+  V3<T> vA2 = vA, wA2 = wA, vB2 = vB, wB2 = wB;
+  T pCur = pOld;
+  if (dA != T(0.0)) {
+    pCur = pNew;
+    const T lam = -sgn * dA;
+    const V3<T> J = mul(N, lam), JA = mul(TA, lam), JB = mul(TB, lam);
+    if (applyA) {
+      vA2 = add(vA2, mul(J, imA));
+      wA2 = add(wA2, angResponse(qA, JA, iIA));
+    }
+    if (m.hasB && applyB) {
+      vB2 = add(vB2, mul(neg(J), imB));
+      wB2 = add(wB2, angResponse(qB, JB, iIB));
+    }
+  }
+  V3<T> ltCur = ltOld;
+  T mu = in[46];
+  if (m.muAvg >= 0.0)
+    mu = T(m.muAvg);
+  const bool haveOld = ltOld.x != T(0.0) || ltOld.y != T(0.0) || ltOld.z != T(0.0);
+  if (mu > T(0.0) || haveOld) {
+    const V3<T> nh = mul(N, T(1.0) / lenN);
+    const V3<T> vBf = m.hasB ? vB2 : mul(cv3<T>(m.wv), invN);
+    const V3<T> wBf = m.hasB ? wB2 : V3<T>{T(0.0), T(0.0), T(0.0)};
+    const V3<T> vr = sub(add(vA2, cross(wA2, rAa)), add(vBf, cross(wBf, rBa)));
+    const V3<T> vtv = sub(vr, mul(nh, dot(vr, nh)));
+    T beta = in[45];
+    if (beta != T(0.0) && (m.sf != 0 || fabs(vn0) < T(vRest) * lenN))
+      beta = T(0.0);
+    V3<T> err = vtv;
+    if (beta != T(0.0)) {
+      V3<T> w0 = ld3(in, 40);
+      w0 = sub(w0, mul(nh, dot(w0, nh)));
+      err = add(vtv, mul(w0, beta));
+    }
+    const T vl = sqrt(dot(err, err));
+    V3<T> ltNew = ltOld;
+    T wTt = imA + imB;
+    if (vl > T(1e-9)) {
+      const V3<T> th = mul(err, T(1.0) / vl);
+      const T wAt = (m.sf == 2) ? T(0.0) : imA + genInvMass(cross(rAa, th), iIA, qA);
+      const T wBt = (m.sf == 1 || !m.hasB) ? T(0.0) : imB + genInvMass(cross(rBa, th), iIB, qB);
+      wTt = wAt + wBt;
+      if (wTt > T(1e-9))
+        ltNew = add(ltOld, mul(th, -vl / wTt));
+    }
+    ltNew = sub(ltNew, mul(nh, dot(ltNew, nh)));
+    T nTot = fmax(pCur, T(0.0)) * lenN;
+    if (fabs(vn0) < T(vRest) * lenN)
+      nTot += fmax(posImp, T(0.0));
+    const T bound = mu * nTot;
+    const T ll = sqrt(dot(ltNew, ltNew));
+    if (ll > bound)
+      ltNew = (bound > T(0.0)) ? mul(ltNew, bound / ll) : V3<T>{T(0.0), T(0.0), T(0.0)};
+    const V3<T> dd = sub(ltNew, ltOld);
+    if (dd.x != T(0.0) || dd.y != T(0.0) || dd.z != T(0.0)) {
+      ltCur = ltNew;
+      if (applyA) {
+        vA2 = add(vA2, mul(dd, imA));
+        wA2 = add(wA2, angResponse(qA, cross(rAa, dd), iIA));
+      }
+      if (m.hasB && applyB) {
+        vB2 = add(vB2, mul(neg(dd), imB));
+        wB2 = add(wB2, angResponse(qB, cross(rBa, mul(dd, T(-1.0))), iIB));
+      }
+    }
+  }
+  st3(out, 0, vA2);
+  st3(out, 3, wA2);
+  if (m.hasB) {
+    st3(out, 6, vB2);
+    st3(out, 9, wB2);
+  }
+  out[12] = pCur;
+  st3(out, 13, ltCur);
+}
+
+// ---- one position update of a contact (src/solver_position.hpp:55-99, :266-331) ------------
+// in: xA[0..3) xB[3..6) qPA[6..10) qPB[10..14) qA[14..18) qB[18..22) n[22..25) rA[25..28) rB[28..31)
+// out: xA[0..3) xB[3..6) dl[6]
+constexpr int kPosIn = 31, kPosOut = 7;
+struct PosC {
+  bool hasB;
+  double imA, imB;
+  V3<double> iIA, iIB;
+};
+template <class T>
+PD void posMap(const T* in, T* out, const PosC& c) {
+  const V3<T> pA = ld3(in, 0);
+  V3<T> pB{T(0.0), T(0.0), T(0.0)};
+  Q4<T> qB{T(0.0), T(0.0), T(0.0), T(1.0)};
+  if (c.hasB) {
+    pB = ld3(in, 3);
+    qB = ld4(in, 10);
+  }
+  const Q4<T> qAd = qmul(ld4(in, 6), qinv(ld4(in, 14)));
+  const V3<T> rA = rot(qAd, ld3(in, 25));
+  V3<T> rB = ld3(in, 28);
+  V3<T> n = ld3(in, 22);
+  if (c.hasB) {
+    const Q4<T> qBd = qmul(qB, qinv(ld4(in, 18)));
+    rB = rot(qBd, rB);
+    n = rot(qBd, n);
+  }
+  T C;
+  if (!c.hasB)
+    C = dot(sub(add(pA, rA), ld3(in, 28)), n);
+  else
+    C = dot(sub(add(pA, rA), add(pB, rB)), n);
+  for (int k = 0; k < 6; ++k)
+    out[k] = in[k];
+  out[6] = T(0.0);
+  if (C >= T(0.0))
+    return;
+  const T imA(c.imA), imB(c.imB);
+  const T wT = computeW(rA, n, imA, cv3<T>(c.iIA)) + computeW(rB, n, imB, cv3<T>(c.iIB));
+  if (wT < T(1e-6))
+    return;
+  const T dl = -C / wT;
+  st3(out, 0, add(pA, V3<T>{n.x * dl * imA, n.y * dl * imA, n.z * dl * imA}));
+  if (c.hasB)
+    st3(out, 3, add(pB, V3<T>{-n.x * dl * imB, -n.y * dl * imB, -n.z * dl * imB}));
+  out[6] = dl;
+}
+
+// ---- velocity commit and position prediction (src/integration.hpp:112-148) ----------------
+// in: x[0..3) q[3..7) vs[7..10) vf[10..13) w[13..16)   out: xP[0..3) qP[3..7)
+constexpr int kIntIn = 16, kIntOut = 7;
+template <class T>
+PD void integrateMap(const T* in, T* out, double im, double dt) {
+  V3<T> x = ld3(in, 0);
+  const Q4<T> q = ld4(in, 3);
+  const V3<T> w = ld3(in, 13);
+  if (im > 0.0)
+    x = add(x, mul(add(ld3(in, 7), ld3(in, 10)), T(0.5 * dt)));
+  Q4<T> qp = q;
+  if (im > 0.0) {
+    const T h(0.5 * dt);
+    qp.x = qp.x + h * (w.x * q.w + w.y * q.z - w.z * q.y);
+    qp.y = qp.y + h * (w.y * q.w + w.z * q.x - w.x * q.z);
+    qp.z = qp.z + h * (w.z * q.w + w.x * q.y - w.y * q.x);
+    qp.w = qp.w + h * (-w.x * q.x - w.y * q.y - w.z * q.z);
+    const T l = sqrt(qp.x * qp.x + qp.y * qp.y + qp.z * qp.z + qp.w * qp.w);
+    if (l > T(1e-9)) {
+      const T s = T(1.0) / l;
+      qp = Q4<T>{qp.x * s, qp.y * s, qp.z * s, qp.w * s};
+    }
+  }
+  st3(out, 0, x);
+  st4(out, 3, qp);
+}
+
+// ---- vector-Jacobian product of a local map by forward-mode chunks ------------------------
+// xbar[i] += sum_o ybar[o] d out[o] / d in[i]; `f(in, out)` is the map on Dd<kLanes> scalars.
+template <int NI, int NO, class F>
+__device__ __forceinline__ void vjp(const double* in, const double* ybar, double* xbar, F f) {
+  using D = Dd<kLanes>;
+  for (int c0 = 0; c0 < NI; c0 += kLanes) {
+    D x[NI];
+    D y[NO];
+    for (int i = 0; i < NI; ++i) {
+      x[i] = D(in[i]);
+      const int l = i - c0;
+      if (l >= 0 && l < kLanes)
+        x[i].d[l] = 1.0;
+    }
+    f(x, y);
+    for (int l = 0; l < kLanes && c0 + l < NI; ++l) {
+      double s = 0.0;
+      for (int o = 0; o < NO; ++o)
+        s += ybar[o] * y[o].d[l];
+      xbar[c0 + l] += s;
+    }
+  }
+}
+
+}  // namespace xadj
+}  // namespace pdem

@@ -127,6 +127,12 @@ _SIGS = {
     "get_domain": (C.c_int, [_vp, _dbl_p, _dbl_p]),
     # candidate pairs over caller-owned device arrays, with no allocation (pdem_static.cu)
     "find_pairs_static": (C.c_int, [_vp, _vp, C.c_int, C.c_double, C.c_double, _vp, C.c_long, _long_p, _vp]),
+    # recorded rollout and adjoint of the XPBD substep (pdem_xadj.cu); device row pointers
+    "xa_begin": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_int]),
+    "xa_step": (C.c_int, [_vp, C.c_double, C.c_int]),
+    "xa_state": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
+    "xa_backward": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _dbl_p]),
+    "xa_info": (C.c_int, [_vp, _long_p, _dbl_p]),
     # forward, adjoint and tangent-linear runs of the Hertz sphere substep (pdem_adjoint.cu)
     "hz_state_size": (C.c_long, [C.c_int, C.c_int]),
     "hz_work_size": (C.c_long, [C.c_int, C.c_int]),
