@@ -55,7 +55,7 @@ REF_OMP_V2 = os.path.join(ROOT, "oracle", "_ref", "libref_omp_v2.so")   # -march
 REF_SERIAL = os.path.join(ROOT, "oracle", "_ref", "libref_serial.so")
 # calibration first: it allocates through torch, which later lines' pooled simulation buffers
 # would crowd
-EXTRAS = ("calibration", "xpbd262k", "batched", "hertz", "shells")
+EXTRAS = ("calibration", "xpbd_adjoint", "xpbd262k", "batched", "hertz", "shells")
 L2_FLUSH_BYTES = 256 << 20
 
 
@@ -657,6 +657,107 @@ def run_calibration(args, rank, world, dist):
                                  "is the check (a stated limitation, not certified)"}
 
 
+def run_xpbd_adjoint(args, rank, world, dist, dem, W):
+    """Adjoint of the XPBD substep on the headline scene (the 4,096-sphere bed of the plain settling
+    configuration, FP64, from its saved restart): `--xadj-substeps` substeps recorded, then the
+    backward of L = sum(a . x_end) + sum(b . v_end) with seeded weights. Reports the plain forward,
+    the recording forward and the backward (device time on the library's stream, max over ranks;
+    each rank runs its own replica), the cost ratio (recording forward + backward) / plain
+    forward, and the gradients' relative error against central differences (relative step 1e-5;
+    eN, mu and a direction of the start velocities), each marked certified when the +h and -h
+    rollouts took the nominal one's contact sets, colourings and adaptive stops (equal
+    signatures). The dual-number check of the same gradients runs in the GPU tests."""
+    import ctypes
+    import torch
+    from peclet.dem.xpbd_adjoint import XpbdRollout
+    sc = W.plain_settled()
+    T = args.xadj_substeps
+    sim = sc.apply(dem.Simulation(sc.n + 8, "fp64"))
+    roll = XpbdRollout(sim)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    q0 = sc.quat if sc.quat is not None else np.tile([0.0, 0.0, 0.0, 1.0], (sc.n, 1))
+    w0 = sc.angvel if sc.angvel is not None else np.zeros((sc.n, 3))
+    start = [torch.tensor(np.asarray(a, np.float64), device=dev) for a in (sc.pos, q0, sc.vel, w0)]
+    theta0 = np.array(sc.material, np.float64)
+    rng = np.random.default_rng(7)
+    A = torch.tensor(rng.normal(size=(sc.n, 3)), device=dev)
+    Bv = torch.tensor(rng.normal(size=(sc.n, 3)) * 1e-3, device=dev)
+    f, h = sim._f, sim._h
+    P = lambda t: ctypes.c_void_p(t.data_ptr())
+
+    def begin(th, v=None):
+        sim.set_material_params(*[float(x) for x in th])
+        rows = [start[0], start[1], start[2] if v is None else v, start[3]]
+        torch.cuda.synchronize()
+        roll._check(f["xa_begin"](h, *[P(t) for t in rows], sc.n), "xa_begin")
+
+    def timed(fn):
+        sim.timer_start()
+        fn()
+        return max_over_ranks(sim.timer_stop() / 1e3, dist, "cuda")  # ms -> s
+
+    # warm-up, then the plain forward, the recording forward and the backward
+    begin(theta0)
+    roll._check(f["xa_step"](h, sc.dt, min(T, 10)), "xa_step")
+    begin(theta0)
+    t_plain = timed(lambda: [sim.step(sc.dt) for _ in range(T)])
+    begin(theta0)
+    t_rec = timed(lambda: roll._check(f["xa_step"](h, sc.dt, T), "xa_step"))
+    sig0 = roll.signature()
+    z = {c: torch.zeros((sc.n, c), dtype=torch.float64, device=dev) for c in (3, 4)}
+    d = [torch.empty((sc.n, c), dtype=torch.float64, device=dev) for c in (3, 4, 3, 3)]
+    dth = (ctypes.c_double * 3)()
+    torch.cuda.synchronize()
+    t_bwd = timed(lambda: roll._check(f["xa_backward"](h, P(A), P(z[4]), P(Bv), P(z[3]), *[P(t) for t in d], dth),
+                                      "xa_backward"))
+    info = roll.info()
+    # central differences on a window of `win` substeps: over many substeps of a settled bed the
+    # adaptive stops (sweep counts) flip with any perturbation, and a flipped stop is a jump of the
+    # loss that no derivative sees; the window's differences are certified when they do not flip
+    win = min(T, args.xadj_fd_substeps)
+    begin(theta0)
+    roll._check(f["xa_step"](h, sc.dt, win), "xa_step")
+    sigw = roll.signature()
+    torch.cuda.synchronize()
+    roll._check(f["xa_backward"](h, P(A), P(z[4]), P(Bv), P(z[3]), *[P(t) for t in d], dth), "xa_backward")
+    grads = {"eN": dth[0], "mu": dth[2]}
+    rel = lambda a, b: abs(a - b) / abs(b) if b else None
+    fd, cert = {}, {}
+
+    def lossw(th, v=None):
+        begin(th, v)
+        roll._check(f["xa_step"](h, sc.dt, win), "xa_step")
+        x, v1 = sim.get_positions(), sim.get_velocities()
+        return float((A.cpu().numpy() * x).sum() + (Bv.cpu().numpy() * v1).sum()), roll.signature()
+
+    for name, k in (("eN", 0), ("mu", 2)):
+        hh = 1e-5 * theta0[k]
+        tp, tm = theta0.copy(), theta0.copy()
+        tp[k] += hh
+        tm[k] -= hh
+        (lp, sp), (lm, sm) = lossw(tp), lossw(tm)
+        fd[name] = (lp - lm) / (2 * hh)
+        cert[name] = bool(np.array_equal(sp, sigw) and np.array_equal(sm, sigw))
+    dv = torch.tensor(np.random.default_rng(8).normal(size=(sc.n, 3)), device=dev)
+    hv = 1e-5 * 0.05
+    (lp, sp), (lm, sm) = lossw(theta0, start[2] + hv * dv), lossw(theta0, start[2] - hv * dv)
+    fd["v0"] = (lp - lm) / (2 * hv)
+    cert["v0"] = bool(np.array_equal(sp, sigw) and np.array_equal(sm, sigw))
+    grads["v0"] = float((d[2] * dv).sum())
+    rate = lambda t: sc.n * T / t
+    return {"workload": f"plain_settling_4096 restart (step {W.PLAIN_SETTLED_STEPS}), {T} substeps",
+            "path": "plain FP64 XPBD step (coloured PGS, one-sided stabilization, position GS), recorded; "
+                    "hand-written reversal over the frozen colouring",
+            "forward_plain": rate(t_plain), "forward_recording": rate(t_rec), "fwd_adjoint": rate(t_rec + t_bwd),
+            "cost_ratio": (t_rec + t_bwd) / t_plain, "backward_ms_per_substep": 1e3 * t_bwd / T,
+            "forward_ms_per_substep": 1e3 * t_plain / T, "record_mb": info["record_bytes"] / 1e6,
+            "work_mb": info["work_bytes"] / 1e6, "replay_dx_scale_units": info["replay_dx"],
+            "fd_window_substeps": win, "grad": grads, "fd_1e-5": fd,
+            "rel_err_vs_fd": {k: rel(grads[k], fd[k]) for k in fd},
+            "fd_certified": cert, "mean_sweeps": {k: float(v) for k, v in zip(
+                ("velocity", "stabilization", "position"), sig0[:, 4:7].mean(axis=0))}}
+
+
 def run_hertz(args, rank, world, dist, dem, W):
     """The Hertz engine on the polydisperse packing (262,144 spheres), closed variant (the
     reference's engine refuses periodic domains and planes: floor and sides are one SDF grid
@@ -755,6 +856,7 @@ def run_ours(args):
     runners = {"xpbd262k": lambda: run_xpbd262k(args, rank, world, dist, dem, W),
                "batched": lambda: run_batched(args, rank, world, dist, dem, W),
                "calibration": lambda: run_calibration(args, rank, world, dist),
+               "xpbd_adjoint": lambda: run_xpbd_adjoint(args, rank, world, dist, dem, W),
                "hertz": lambda: run_hertz(args, rank, world, dist, dem, W),
                "shells": lambda: run_shells(args, rank, world, dist, dem, W)}
     for name in EXTRAS:
@@ -780,6 +882,11 @@ def run_ours(args):
                         grad_fd_64_certified=all(c64["fd_certified"].values()),
                         grad_rel_err_vs_fd_full=max(v for v in cb["checks_full_horizon"]["rel_err_vs_fd_1e-4"]
                                                     if v is not None))
+        if "xpbd_adjoint" in detail:
+            xa = detail["xpbd_adjoint"]
+            flat.update(xpbd_fwd_adjoint_cost_ratio=xa["cost_ratio"], xpbd_fwd_adjoint_value=xa["fwd_adjoint"],
+                        xpbd_grad_rel_err_vs_fd=max(v for v in xa["rel_err_vs_fd"].values() if v is not None),
+                        xpbd_grad_fd_certified=all(xa["fd_certified"].values()))
         if "hertz" in detail:
             flat.update(hertz262k_fp64_value=detail["hertz"]["fp64"]["value"],
                         hertz262k_fp32_value=detail["hertz"]["fp32"]["value"])
@@ -839,6 +946,8 @@ def main():
     ap.add_argument("--shell-presettle", type=int, default=0, help="untimed FP64 outer steps of a shell deposition")
     ap.add_argument("--calib-scenes", type=int, default=64)
     ap.add_argument("--calib-substeps", type=int, default=2000)
+    ap.add_argument("--xadj-substeps", type=int, default=100, help="substeps of the XPBD adjoint line")
+    ap.add_argument("--xadj-fd-substeps", type=int, default=10, help="window of its finite-difference check")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)

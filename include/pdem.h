@@ -335,6 +335,11 @@ int pdem_xa_state(pdem_handle h, double* x, double* q, double* v, double* w);
 int pdem_xa_backward(pdem_handle h, const double* gx, const double* gq, const double* gv, const double* gw,
                      double* dx, double* dq, double* dv, double* dw, double* dtheta);
 int pdem_xa_info(pdem_handle h, long* out, double* err);
+/* the record's discrete decisions, 7 longs per substep (contacts, manifolds, colours of the
+ * velocity and position colourings, main, stabilization and position sweeps), at most cap values;
+ * returns the number of substeps recorded (or -1 on error). Equal signatures of two rollouts mean
+ * the same contact sets, colourings and adaptive stops (a certified finite difference). */
+long pdem_xa_signature(pdem_handle h, long* out, long cap);
 
 #ifdef __cplusplus
 }

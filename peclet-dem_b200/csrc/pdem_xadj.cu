@@ -32,6 +32,7 @@
 // thermostat or pair materials, every entry coloured (no Jacobi leftovers) and no saturated
 // colour.
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <initializer_list>
 #include <memory>
@@ -555,7 +556,8 @@ __global__ void kxIntegrateRev(XScene sc, XView r, XWork w) {
   }
 }
 
-__global__ void kxPgsRev(XScene sc, XView r, XWork w, int col, int sweep, double vRest, int stab) {
+// mode 0: the hand-written reverse (pgsRev); mode 1: the forward-mode local Jacobian (the check)
+__global__ void kxPgsRev(XScene sc, XView r, XWork w, int col, int sweep, double vRest, int stab, int mode) {
   const int b = r.mOff[col], cnt = r.mOff[col + 1] - b;
   GRID_STRIDE(t, cnt) {
     const int m = r.mOrder[b + t];
@@ -594,7 +596,10 @@ __global__ void kxPgsRev(XScene sc, XView r, XWork w, int col, int sweep, double
     for (int j = 0; j < kPgsIn; ++j)
       xb[j] = 0.0;
     const ManC mc = manC(sc, r, w, m, stab ? (int)r.sf[m] : 0);
-    vjp<kPgsIn, kPgsOut>(in, yb, xb, [&](const Dd<kLanes>* x, Dd<kLanes>* y) { pgsMap(x, y, mc, vRest); });
+    if (mode == 0)
+      pgsRev(in, yb, xb, mc, vRest);
+    else
+      vjp<kPgsIn, kPgsOut>(in, yb, xb, [&](const Dd<kLanes>* x, Dd<kLanes>* y) { pgsMap(x, y, mc, vRest); });
     w.avP[ab.x] = get3(xb, 0);
     w.awP[ab.x] = get3(xb, 3);
     add4(w.aq[ab.x], xb + 31);
@@ -909,6 +914,12 @@ struct XAdj {
   DBuf<int> mint;
   double err[2] = {0, 0};
   size_t workBytes = 0;
+  // PDEM_XADJ_DUAL=1: the PGS updates reversed through forward-mode local Jacobians instead of the
+  // hand-written reverse (the cross-check of the hand derivation; slower)
+  int dualCheck = [] {
+    const char* e = std::getenv("PDEM_XADJ_DUAL");
+    return (e && e[0] == '1') ? 1 : 0;
+  }();
   int maxSweeps = 0;
 };
 
@@ -1214,7 +1225,7 @@ struct XAdjAccess {
     cudaCheck(cudaGetLastError(), "xadj replay");
   }
 
-  static void reverse(S& s, const XScene& sc, const XRec& R, const XView& r, const XWork& w) {
+  static void reverse(S& s, const XAdj& A, const XScene& sc, const XRec& R, const XView& r, const XWork& w) {
     cudaStream_t st = s.stream_;
     const int n = sc.n;
     const int gn = gridFor(n), gc = gridFor(std::max(R.nc, 1)), gm = gridFor(std::max(R.nm, 1));
@@ -1229,10 +1240,10 @@ struct XAdjAccess {
     if (R.nm > 0) {
       for (int it = R.stabSweeps - 1; it >= 0; --it)
         for (int c = R.ncolV - 1; c >= 0; --c)
-          kxPgsRev<<<gm, kBR, 0, st>>>(sc, r, w, c, R.velSweeps + it, vRest, 1);
+          kxPgsRev<<<gm, kBR, 0, st>>>(sc, r, w, c, R.velSweeps + it, vRest, 1, A.dualCheck);
       for (int it = R.velSweeps - 1; it >= 0; --it)
         for (int c = R.ncolV - 1; c >= 0; --c)
-          kxPgsRev<<<gm, kBR, 0, st>>>(sc, r, w, c, it, vRest, 0);
+          kxPgsRev<<<gm, kBR, 0, st>>>(sc, r, w, c, it, vRest, 0, A.dualCheck);
       for (int c = 0; c < R.ncolV; ++c)
         kxWarmRev<<<gm, kBR, 0, st>>>(sc, r, w, c);
       for (int c = 0; c < R.ncolV; ++c)
@@ -1279,7 +1290,7 @@ struct XAdjAccess {
       const XRec& R = *A.recs[t];
       const XView r = view(R);
       replay(s, sc, R, r, w, t + 1 < T ? A.recs[t + 1].get() : nullptr);
-      reverse(s, sc, R, r, w);
+      reverse(s, A, sc, R, r, w);
       if (t > 0) {
         const XRec& P = *A.recs[t - 1];
         const size_t pm = std::max(P.nm, 1);
@@ -1325,6 +1336,17 @@ struct XAdjAccess {
     s.sync();
   }
 
+  static long signature(S& s, long* out, long cap) {
+    XAdj& A = get(s);
+    long k = 0;
+    for (auto& r : A.recs) {
+      const long v[7] = {r->nc, r->nm, r->ncolV, r->ncolP, r->velSweeps, r->stabSweeps, r->posSweeps};
+      for (long j = 0; j < 7; ++j, ++k)
+        if (k < cap)
+          out[k] = v[j];
+    }
+    return (long)A.recs.size();
+  }
   static void info(S& s, long* out, double* err) {
     XAdj& A = get(s);
     size_t bytes = 0;
@@ -1349,5 +1371,6 @@ void xadjBackward(Sim<double>& S, const double* gx, const double* gq, const doub
   XAdjAccess::backward(S, gx, gq, gv, gw, dx, dq, dv, dw, dtheta);
 }
 void xadjInfo(Sim<double>& S, long* out, double* err) { XAdjAccess::info(S, out, err); }
+long xadjSignature(Sim<double>& S, long* out, long cap) { return XAdjAccess::signature(S, out, cap); }
 
 }  // namespace pdem

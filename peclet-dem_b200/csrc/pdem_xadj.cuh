@@ -641,6 +641,418 @@ PD void integrateMap(const T* in, T* out, double im, double dt) {
   st4(out, 3, qp);
 }
 
+// ---- hand-written reverse of the PGS update ---------------------------------------------------
+// Vector-Jacobian products of the vector pieces (adjoints accumulate with +=):
+//   c = a x b:          abar += b x cbar,  bbar += cbar x a
+//   y = rot(q, v) = v + w t + qv x t, t = 2 qv x v:
+//     vbar += ybar, wbar += t . ybar, tbar = w ybar + ybar x qv, qvbar += t x ybar,
+//     then with ubar = 2 tbar (u = qv x v): qvbar += v x ubar, vbar += ubar x qv
+//   invrot(q, v) = rot((-qv, w), v)
+//   angResponse(q, J, iI) = rot(q, iI * invrot(q, J))
+using V3d = V3<double>;
+using Q4d = Q4<double>;
+PD void acc(V3d& a, V3d b) { a.x += b.x, a.y += b.y, a.z += b.z; }
+PD void acc(Q4d& a, Q4d b) { a.x += b.x, a.y += b.y, a.z += b.z, a.w += b.w; }
+PD void crossVjp(V3d a, V3d b, V3d cb, V3d& ab, V3d& bb) {
+  acc(ab, cross(b, cb));
+  acc(bb, cross(cb, a));
+}
+PD void rotVjp(Q4d q, V3d v, V3d yb, Q4d& qb, V3d& vb) {
+  const V3d qv{q.x, q.y, q.z};
+  const V3d t = mul(cross(qv, v), 2.0);
+  acc(vb, yb);
+  qb.w += dot(t, yb);
+  const V3d tb = add(mul(yb, q.w), cross(yb, qv));
+  V3d qvb = cross(t, yb);
+  const V3d ub = mul(tb, 2.0);
+  acc(qvb, cross(v, ub));
+  acc(vb, cross(ub, qv));
+  qb.x += qvb.x, qb.y += qvb.y, qb.z += qvb.z;
+}
+PD void invrotVjp(Q4d q, V3d v, V3d yb, Q4d& qb, V3d& vb) {
+  Q4d c{0.0, 0.0, 0.0, 0.0};
+  rotVjp(Q4d{-q.x, -q.y, -q.z, q.w}, v, yb, c, vb);
+  qb.x -= c.x, qb.y -= c.y, qb.z -= c.z, qb.w += c.w;
+}
+PD void angResponseVjp(Q4d q, V3d J, V3d iI, V3d yb, Q4d& qb, V3d& Jb) {
+  const V3d u = invrot(q, J);
+  const V3d sv{u.x * iI.x, u.y * iI.y, u.z * iI.z};
+  V3d sb{0.0, 0.0, 0.0};
+  rotVjp(q, sv, yb, qb, sb);
+  invrotVjp(q, J, V3d{sb.x * iI.x, sb.y * iI.y, sb.z * iI.z}, qb, Jb);
+}
+// y = x - n (x . n):  xbar += ybar - n (n . ybar),  nbar += -(x . n) ybar - (n . ybar) x
+PD void projVjp(V3d x, V3d n, V3d yb, V3d& xb, V3d& nb) {
+  const double ny = dot(n, yb), xn = dot(x, n);
+  acc(xb, sub(yb, mul(n, ny)));
+  acc(nb, add(mul(yb, -xn), mul(x, -ny)));
+}
+
+// Reverse of pgsMap<double> (same inputs, outputs and branches); isotropic inverse inertia (the
+// generalised inverse mass |tau|^2 iI does not depend on the orientation), as the adjoint's scope
+// requires. xb += J^T yb.
+PD void pgsRev(const double* in, const double* yb, double* xb, const ManC& m, double vRest) {
+  // ---- forward, keeping what the reverse needs ----
+  const V3d vA = ld3(in, 0), wA = ld3(in, 3);
+  const double invN = m.invN;
+  V3d vB{0.0, 0.0, 0.0}, wB{0.0, 0.0, 0.0};
+  if (m.hasB) {
+    vB = ld3(in, 6);
+    wB = ld3(in, 9);
+  } else {
+    vB = mul(m.wv, invN);
+  }
+  const V3d N = ld3(in, 16), TA = ld3(in, 19), TB = ld3(in, 22);
+  const V3d rAa = mul(ld3(in, 25), invN), rBa = mul(ld3(in, 28), invN);
+  const V3d dc = m.hasB ? sub(rAa, rBa) : rAa;
+  const Q4d qA = ld4(in, 31), qB = ld4(in, 35);
+  const double vn0 = in[39], posImp = in[43];
+  const double imA = m.imA, imB = m.imB;
+  const V3d iIA = m.iIA, iIB = m.iIB;
+  const double pOld = in[12];
+  const V3d ltOld = ld3(in, 13);
+  // adjoints of the outputs (identity when the update returns early)
+  V3d vAb = ld3(yb, 0), wAb = ld3(yb, 3), vBb = ld3(yb, 6), wBb = ld3(yb, 9);
+  double pb = yb[12];
+  V3d ltb = ld3(yb, 13);
+  auto flush = [&](V3d vab, V3d wab, V3d vbb, V3d wbb, double p0b, V3d lt0b) {
+    xb[0] += vab.x, xb[1] += vab.y, xb[2] += vab.z;
+    xb[3] += wab.x, xb[4] += wab.y, xb[5] += wab.z;
+    if (m.hasB) {
+      xb[6] += vbb.x, xb[7] += vbb.y, xb[8] += vbb.z;
+      xb[9] += wbb.x, xb[10] += wbb.y, xb[11] += wbb.z;
+    }
+    xb[12] += p0b;
+    xb[13] += lt0b.x, xb[14] += lt0b.y, xb[15] += lt0b.z;
+  };
+  double e = in[44];
+  bool eFromN = true;
+  if (m.eAvg >= 0.0) {
+    e = m.eAvg;
+    eFromN = false;
+  }
+  const double lenN = ::sqrt(dot(N, N));
+  if (lenN < 1e-9) {
+    flush(vAb, wAb, vBb, wBb, pb, ltb);
+    return;
+  }
+  const double vn0N = dot(vA, N) + dot(wA, TA) + dot(vB, neg(N)) + dot(wB, TB);
+  const double vn = vn0N + dot(mul(dc, 0.0), N);
+  const double al = dot(N, dc);
+  const double sgn = (al > 0.0) ? 1.0 : -1.0;
+  const double Nsq = dot(N, N);
+  double wAn = Nsq * imA + genInvMass(TA, iIA, qA);
+  double wBn = Nsq * imB + genInvMass(TB, iIB, qB);
+  bool applyA = true, applyB = true, useA = true, useB = true;
+  if (m.sf == 1) {
+    wBn = 0.0;
+    applyB = false;
+    useB = false;
+    e = 0.0;
+    eFromN = false;
+  } else if (m.sf == 2) {
+    wAn = 0.0;
+    applyA = false;
+    useA = false;
+    e = 0.0;
+    eFromN = false;
+  }
+  const double wT = wAn + wBn;
+  if (wT <= 0.0) {
+    flush(vAb, wAb, vBb, wBb, pb, ltb);
+    return;
+  }
+  const double v0 = sgn * vn0;
+  const bool rest = ::fabs(vn0) < vRest * lenN;
+  if (rest) {
+    e = 0.0;
+    eFromN = false;
+  }
+  const bool tgt = v0 > 0.0;
+  const double target = tgt ? -e * v0 : 0.0;
+  const double vt = sgn * vn;
+  const double dp = (vt - target) / wT;
+  double pNew = pOld + dp;
+  const bool clampN = pNew < 0.0;
+  if (clampN)
+    pNew = 0.0;
+  const double dA = pNew - pOld;
+  const bool act = dA != 0.0;
+  V3d vA2 = vA, wA2 = wA, vB2 = vB, wB2 = wB;
+  double pCur = pOld;
+  const double lam = -sgn * dA;
+  const V3d J = mul(N, lam), JA = mul(TA, lam), JB = mul(TB, lam);
+  if (act) {
+    pCur = pNew;
+    if (applyA) {
+      vA2 = add(vA2, mul(J, imA));
+      wA2 = add(wA2, angResponse(qA, JA, iIA));
+    }
+    if (m.hasB && applyB) {
+      vB2 = add(vB2, mul(neg(J), imB));
+      wB2 = add(wB2, angResponse(qB, JB, iIB));
+    }
+  }
+  double mu = in[46];
+  bool muFromIn = true;
+  if (m.muAvg >= 0.0) {
+    mu = m.muAvg;
+    muFromIn = false;
+  }
+  const bool haveOld = ltOld.x != 0.0 || ltOld.y != 0.0 || ltOld.z != 0.0;
+  // accumulators of the input adjoints
+  V3d vAi{0, 0, 0}, wAi{0, 0, 0}, vBi{0, 0, 0}, wBi{0, 0, 0}, lt0i{0, 0, 0};
+  V3d Nb{0, 0, 0}, TAb{0, 0, 0}, TBb{0, 0, 0}, rAab{0, 0, 0}, rBab{0, 0, 0}, vt0b{0, 0, 0};
+  Q4d qAb{0, 0, 0, 0}, qBb{0, 0, 0, 0};
+  double p0b = 0.0, vn0b = 0.0, posImpb = 0.0, eNb = 0.0, eTb = 0.0, mub = 0.0, lenNb = 0.0;
+  // adjoints of the velocities after the normal update and of pCur
+  V3d vA2b = vAb, wA2b = wAb, vB2b = vBb, wB2b = wBb;
+  double pCurb = pb;
+  if (mu > 0.0 || haveOld) {
+    const V3d nh = mul(N, 1.0 / lenN);
+    const V3d vBf = m.hasB ? vB2 : mul(m.wv, invN);
+    const V3d wBf = m.hasB ? wB2 : V3d{0.0, 0.0, 0.0};
+    const V3d vr = sub(add(vA2, cross(wA2, rAa)), add(vBf, cross(wBf, rBa)));
+    const V3d vtv = sub(vr, mul(nh, dot(vr, nh)));
+    double beta = in[45];
+    bool betaFromIn = true;
+    if (beta != 0.0 && (m.sf != 0 || rest)) {
+      beta = 0.0;
+      betaFromIn = false;
+    }
+    V3d err = vtv;
+    V3d w0p{0, 0, 0};
+    const V3d vt0 = ld3(in, 40);
+    if (beta != 0.0) {
+      w0p = sub(vt0, mul(nh, dot(vt0, nh)));
+      err = add(vtv, mul(w0p, beta));
+    }
+    const double vl = ::sqrt(dot(err, err));
+    V3d ltNew = ltOld;
+    double wTt = imA + imB;
+    const bool vOn = vl > 1e-9;
+    V3d th{0, 0, 0}, uA{0, 0, 0}, uB{0, 0, 0};
+    bool wOn = false;
+    if (vOn) {
+      th = mul(err, 1.0 / vl);
+      uA = cross(rAa, th);
+      uB = cross(rBa, th);
+      const double wAt = (m.sf == 2) ? 0.0 : imA + genInvMass(uA, iIA, qA);
+      const double wBt = (m.sf == 1 || !m.hasB) ? 0.0 : imB + genInvMass(uB, iIB, qB);
+      wTt = wAt + wBt;
+      wOn = wTt > 1e-9;
+      if (wOn)
+        ltNew = add(ltOld, mul(th, -vl / wTt));
+    }
+    const V3d ltP = sub(ltNew, mul(nh, dot(ltNew, nh)));
+    const bool pPos = !(0.0 > pCur);  // fmax(pCur, 0) takes pCur (also at 0)
+    double nTot = (pPos ? pCur : 0.0) * lenN;
+    const bool posOn = rest && !(0.0 > posImp);
+    if (rest)
+      nTot += (!(0.0 > posImp)) ? posImp : 0.0;
+    const double bound = mu * nTot;
+    const double ll = ::sqrt(dot(ltP, ltP));
+    const bool cone = ll > bound;
+    V3d ltC = ltP;
+    if (cone)
+      ltC = (bound > 0.0) ? mul(ltP, bound / ll) : V3d{0.0, 0.0, 0.0};
+    const V3d dd = sub(ltC, ltOld);
+    if (dd.x != 0.0 || dd.y != 0.0 || dd.z != 0.0) {
+      // ---- reverse of the friction update ----
+      V3d ddb = ltb;  // ltCur = ltC
+      V3d ltCb{0, 0, 0};
+      acc(ltCb, ltb);
+      ddb = V3d{0, 0, 0};
+      if (applyA) {
+        acc(ddb, mul(vAb, imA));
+        const V3d c = cross(rAa, dd);
+        V3d cb{0, 0, 0};
+        angResponseVjp(qA, c, iIA, wAb, qAb, cb);
+        crossVjp(rAa, dd, cb, rAab, ddb);
+      }
+      if (m.hasB && applyB) {
+        acc(ddb, mul(vBb, -imB));
+        const V3d nd = mul(dd, -1.0);
+        const V3d c = cross(rBa, nd);
+        V3d cb{0, 0, 0}, ndb{0, 0, 0};
+        angResponseVjp(qB, c, iIB, wBb, qBb, cb);
+        crossVjp(rBa, nd, cb, rBab, ndb);
+        acc(ddb, mul(ndb, -1.0));
+      }
+      acc(ltCb, ddb);
+      acc(lt0i, mul(ddb, -1.0));
+      // cone
+      V3d ltPb{0, 0, 0};
+      double boundb = 0.0;
+      if (cone) {
+        if (bound > 0.0) {
+          const double sc = bound / ll;
+          acc(ltPb, mul(ltCb, sc));
+          const double scb = dot(ltCb, ltP);
+          boundb += scb / ll;
+          const double llb = -scb * bound / (ll * ll);
+          if (ll > 0.0)
+            acc(ltPb, mul(ltP, llb / ll));
+        }
+      } else {
+        acc(ltPb, ltCb);
+      }
+      if (muFromIn)
+        mub += boundb * nTot;
+      const double nTotb = boundb * mu;
+      if (pPos) {
+        pCurb += nTotb * lenN;
+        lenNb += nTotb * pCur;
+      }
+      if (posOn)
+        posImpb += nTotb;
+      // projection onto the tangent plane
+      V3d ltNewb{0, 0, 0}, nhb{0, 0, 0};
+      projVjp(ltNew, nh, ltPb, ltNewb, nhb);
+      V3d errb{0, 0, 0};
+      if (vOn && wOn) {
+        const double k = -vl / wTt;
+        acc(lt0i, ltNewb);
+        V3d thb = mul(ltNewb, k);
+        const double kb = dot(ltNewb, th);
+        double vlb = -kb / wTt;
+        const double wTtb = kb * vl / (wTt * wTt);
+        if (m.sf != 2) {  // wAt = imA + |rAa x th|^2 iIA
+          const V3d ub = mul(uA, 2.0 * iIA.x * wTtb);
+          crossVjp(rAa, th, ub, rAab, thb);
+        }
+        if (!(m.sf == 1 || !m.hasB)) {
+          const V3d ub = mul(uB, 2.0 * iIB.x * wTtb);
+          crossVjp(rBa, th, ub, rBab, thb);
+        }
+        // th = err / vl
+        acc(errb, mul(thb, 1.0 / vl));
+        vlb += -dot(thb, err) / (vl * vl);
+        acc(errb, mul(err, vlb / vl));
+      } else {
+        acc(lt0i, ltNewb);
+      }
+      V3d vtvb = errb;
+      if (beta != 0.0) {
+        const V3d w0pb = mul(errb, beta);
+        const double betab = dot(errb, w0p);
+        if (betaFromIn)
+          eTb += betab;
+        projVjp(vt0, nh, w0pb, vt0b, nhb);
+      }
+      V3d vrb{0, 0, 0};
+      projVjp(vr, nh, vtvb, vrb, nhb);
+      acc(vA2b, vrb);
+      crossVjp(wA2, rAa, vrb, wA2b, rAab);
+      if (m.hasB) {
+        const V3d nvrb = mul(vrb, -1.0);
+        acc(vB2b, nvrb);
+        crossVjp(wB2, rBa, nvrb, wB2b, rBab);
+      }
+      // nh = N / lenN
+      acc(Nb, mul(nhb, 1.0 / lenN));
+      lenNb += -dot(nhb, N) / (lenN * lenN);
+    } else {
+      acc(lt0i, ltb);  // ltCur = ltOld
+    }
+  } else {
+    acc(lt0i, ltb);
+  }
+  // ---- reverse of the normal update ----
+  double dpb = 0.0;
+  if (act) {
+    double lamb = 0.0;
+    if (applyA) {
+      acc(vAi, vA2b);
+      acc(Nb, mul(vA2b, lam * imA));  // J = N lam: Jbar = vA2b imA
+      lamb += dot(vA2b, N) * imA;
+      acc(wAi, wA2b);
+      V3d JAb{0, 0, 0};
+      angResponseVjp(qA, JA, iIA, wA2b, qAb, JAb);
+      acc(TAb, mul(JAb, lam));
+      lamb += dot(JAb, TA);
+    } else {
+      acc(vAi, vA2b);
+      acc(wAi, wA2b);
+    }
+    if (m.hasB) {
+      acc(vBi, vB2b);
+      acc(wBi, wB2b);
+      if (applyB) {
+        acc(Nb, mul(vB2b, -lam * imB));
+        lamb += -dot(vB2b, N) * imB;
+        V3d JBb{0, 0, 0};
+        angResponseVjp(qB, JB, iIB, wB2b, qBb, JBb);
+        acc(TBb, mul(JBb, lam));
+        lamb += dot(JBb, TB);
+      }
+    }
+    const double dAb = -sgn * lamb;
+    double pNewb = pCurb + dAb;
+    p0b -= dAb;
+    if (!clampN) {
+      p0b += pNewb;
+      dpb = pNewb;
+    }
+  } else {
+    acc(vAi, vA2b);
+    acc(wAi, wA2b);
+    if (m.hasB) {
+      acc(vBi, vB2b);
+      acc(wBi, wB2b);
+    }
+    p0b += pCurb;
+  }
+  // dp = (vt - target) / wT
+  const double vtb = dpb / wT;
+  const double targetb = -dpb / wT;
+  const double wTb = -dpb * dp / wT;
+  const double vnb = sgn * vtb;
+  if (tgt) {
+    const double eb = -targetb * v0;
+    if (eFromN)
+      eNb += eb;
+    vn0b += sgn * (-targetb * e);
+  }
+  double Nsqb = 0.0;
+  if (useA) {
+    Nsqb += wTb * imA;
+    acc(TAb, mul(TA, 2.0 * iIA.x * wTb));
+  }
+  if (useB) {
+    Nsqb += wTb * imB;
+    acc(TBb, mul(TB, 2.0 * iIB.x * wTb));
+  }
+  acc(Nb, mul(N, 2.0 * Nsqb));
+  // vn = vA . N + wA . TA - vB . N + wB . TB
+  acc(vAi, mul(N, vnb));
+  acc(wAi, mul(TA, vnb));
+  acc(Nb, mul(sub(vA, vB), vnb));
+  acc(TAb, mul(wA, vnb));
+  if (m.hasB) {
+    acc(vBi, mul(N, -vnb));
+    acc(wBi, mul(TB, vnb));
+    acc(TBb, mul(wB, vnb));
+  }
+  // lenN = |N|
+  acc(Nb, mul(N, lenNb / lenN));
+  // store
+  flush(vAi, wAi, vBi, wBi, p0b, lt0i);
+  xb[16] += Nb.x, xb[17] += Nb.y, xb[18] += Nb.z;
+  xb[19] += TAb.x, xb[20] += TAb.y, xb[21] += TAb.z;
+  xb[22] += TBb.x, xb[23] += TBb.y, xb[24] += TBb.z;
+  xb[25] += rAab.x * invN, xb[26] += rAab.y * invN, xb[27] += rAab.z * invN;
+  xb[28] += rBab.x * invN, xb[29] += rBab.y * invN, xb[30] += rBab.z * invN;
+  xb[31] += qAb.x, xb[32] += qAb.y, xb[33] += qAb.z, xb[34] += qAb.w;
+  xb[35] += qBb.x, xb[36] += qBb.y, xb[37] += qBb.z, xb[38] += qBb.w;
+  xb[39] += vn0b;
+  xb[40] += vt0b.x, xb[41] += vt0b.y, xb[42] += vt0b.z;
+  xb[43] += posImpb;
+  xb[44] += eNb;
+  xb[45] += eTb;
+  xb[46] += mub;
+}
+
 // ---- vector-Jacobian product of a local map by forward-mode chunks ------------------------
 // xbar[i] += sum_o ybar[o] d out[o] / d in[i]; `f(in, out)` is the map on Dd<kLanes> scalars.
 template <int NI, int NO, class F>

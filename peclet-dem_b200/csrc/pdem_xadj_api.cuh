@@ -23,6 +23,14 @@ void xadjBackward(Sim<double>& S, const double* gx, const double* gq, const doub
 // state (in units of the global scale) over the last backward, err[1] the same for velocities (m/s)
 void xadjInfo(Sim<double>& S, long* out, double* err);
 
+// the record's discrete decisions, 7 per substep: contacts, manifolds, colours of the two
+// colourings, main / stabilization / position sweeps; returns the number of substeps
+long xadjSignature(Sim<double>& S, long* out, long cap);
+
+template <class SIM>
+long xadjSignature(SIM&, long*, long) {
+  throw std::invalid_argument("the XPBD adjoint runs on the FP64 plain path (precision fp64)");
+}
 template <class SIM>
 void xadjBegin(SIM&, const double*, const double*, const double*, const double*, int) {
   throw std::invalid_argument("the XPBD adjoint runs on the FP64 plain path (precision fp64)");

@@ -66,6 +66,17 @@ class XpbdRollout:
         return {"substeps": out[0], "record_bytes": out[1], "work_bytes": out[2], "max_sweeps": out[3],
                 "replay_dx": err[0], "replay_dv": err[1]}
 
+    def signature(self):
+        """The last rollout's discrete decisions, one row per substep: contacts, manifolds, colours
+        of the velocity and position colourings, main / stabilization / position sweeps. Two
+        rollouts with equal signatures took the same contact sets, colourings and adaptive stops."""
+        n = int(self.sim._f["xa_signature"](self.sim._h, None, 0))
+        if n < 0:
+            self._check(1, "xa_signature")
+        out = np.zeros(7 * max(n, 1), np.int64)
+        self.sim._f["xa_signature"](self.sim._h, out.ctypes.data_as(C.POINTER(C.c_long)), out.size)
+        return out[: 7 * n].reshape(n, 7)
+
     def rollout(self, x0, q0, v0, w0, theta, substeps: int, dt: float = 0.0):
         """End state (x, q, v, w) after `substeps` substeps of length dt (0: the simulation's)."""
         if substeps < 1:

@@ -32,6 +32,12 @@ def _impacts():
     return sc
 
 
+def _settled():
+    """The benchmark's bed: 4,096 spheres of the plain settling configuration at its saved restart."""
+    from peclet.dem import workloads as W
+    return W.plain_settled()
+
+
 def _weights(n, seed=5):
     rng = np.random.default_rng(seed)
     return [rng.normal(size=(n, c)) for c in (3, 4, 3, 3)]  # x, q, v, w
@@ -76,8 +82,9 @@ def _dual(orc_api, sc, T, direction):
     return np.array(tans), end
 
 
-@pytest.mark.parametrize("name,mk,T", [("column", _column, 10), ("column", _column, 40), ("impacts", _impacts, 20)],
-                         ids=["column-10", "column-40", "impacts-20"])
+@pytest.mark.parametrize("name,mk,T", [("column", _column, 10), ("column", _column, 40), ("impacts", _impacts, 20),
+                                       ("settled", _settled, 10)],
+                         ids=["column-10", "column-40", "impacts-20", "settled4096-10"])
 def test_adjoint_matches_dual_numbers(gpu_api, orc_api, name, mk, T):
     sc = mk()
     rng = np.random.default_rng(17)
@@ -104,3 +111,15 @@ def test_rollout_refuses_what_it_does_not_reverse(gpu_api):
         roll(*start, torch.tensor(sc.material, dtype=torch.float64), 2)
     with pytest.raises(ValueError):
         XpbdRollout(P.build(gpu_api, _column(), None, "fp32"))
+
+
+def test_hand_reverse_equals_dual_jacobians(gpu_api, monkeypatch):
+    """The hand-written reverse of the PGS update against the same update reversed through its
+    forward-mode local Jacobian (PDEM_XADJ_DUAL=1): the same gradients to rounding."""
+    sc = _impacts()
+    _, g0, t0, _, _ = _gpu(gpu_api, sc, 20)
+    monkeypatch.setenv("PDEM_XADJ_DUAL", "1")
+    _, g1, t1, _, _ = _gpu(gpu_api, sc, 20)
+    np.testing.assert_allclose(t0, t1, rtol=1e-10)
+    for a, b in zip(g0, g1):
+        np.testing.assert_allclose(a, b, rtol=1e-9, atol=1e-12 * np.abs(b).max())
