@@ -340,6 +340,12 @@ int pdem_xa_info(pdem_handle h, long* out, double* err);
  * returns the number of substeps recorded (or -1 on error). Equal signatures of two rollouts mean
  * the same contact sets, colourings and adaptive stops (a certified finite difference). */
 long pdem_xa_signature(pdem_handle h, long* out, long cap);
+/* the branch signature of the record: every substep replayed (no reverse) and every sweep
+ * update's branch decisions (normal impulse clamp, restitution cut-off, friction cone, active
+ * position contact) hashed into *hash. With equal signatures (pdem_xa_signature) and equal branch
+ * hashes, two rollouts ran the same smooth piece of the step: their central difference is a
+ * certified check of the gradient. */
+int pdem_xa_branches(pdem_handle h, unsigned long long* hash);
 
 #ifdef __cplusplus
 }

@@ -70,7 +70,20 @@ def build(verbose: bool = False, jobs: int | None = None) -> str:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    _check_undefined(OUT)
     return OUT
+
+
+def _check_undefined(lib: str) -> None:
+    """A template of the library used in one file but defined in another links into an undefined
+    symbol that only the loader reports: fail the build on any undefined symbol of our namespace."""
+    nm = shutil.which("nm")
+    if not nm:
+        return
+    r = subprocess.run([nm, "-D", "--undefined-only", "-C", lib], capture_output=True, text=True)
+    bad = [ln.strip() for ln in r.stdout.splitlines() if "pdem::" in ln]
+    if bad:
+        raise RuntimeError("undefined symbols in " + lib + ":\n" + "\n".join(bad[:10]))
 
 
 if __name__ == "__main__":

@@ -644,6 +644,7 @@ int pdem_xa_backward(pdem_handle h, const double* gx, const double* gq, const do
   BODY(pdem::xadjBackward(S, gx, gq, gv, gw, dx, dq, dv, dw, dtheta));
 }
 int pdem_xa_info(pdem_handle h, long* out, double* err) { BODY(pdem::xadjInfo(S, out, err)); }
+int pdem_xa_branches(pdem_handle h, unsigned long long* hash) { BODY(*hash = pdem::xadjBranches(S)); }
 long pdem_xa_signature(pdem_handle h, long* out, long cap) {
   long n = -1;
   if (with(h, [&](auto& S) { n = pdem::xadjSignature(S, out, cap); }) != PDEM_OK)

@@ -39,6 +39,8 @@
 #include <stdexcept>
 #include <vector>
 
+#include <cooperative_groups.h>
+
 #include "pdem_sim.cuh"
 #include "pdem_xadj.cuh"
 #include "pdem_xadj_api.cuh"
@@ -47,11 +49,17 @@ namespace pdem {
 
 using namespace xadj;
 using D4 = Q4<double>;
+namespace cg = cooperative_groups;
 
 namespace {
 
 constexpr int kB = 256;
-constexpr int kBR = 128;  // the reverse kernels (up to 255 registers a thread)
+constexpr int kBR = 128;   // the reverse kernels (up to 255 registers a thread)
+constexpr int kBPgs = 64;  // the hand-written PGS reverse: one entry a thread, few entries a colour
+// the persistent sweep loops: one cluster of kClusterBlocks blocks (the non-portable size 16),
+// for manifold lists up to kClusterEntries (larger ones sweep colour by colour in separate launches)
+constexpr int kClusterBlocks = 16;
+constexpr int kClusterEntries = 1 << 16;
 constexpr int kMaxColours = 62;  // the first saturated colour of the 62-colour masks
 
 __device__ __forceinline__ u64 manKey(int2 ab) {
@@ -128,7 +136,7 @@ struct XScene {
 
 // one recorded substep, device side
 struct XView {
-  int nc, nm, L;
+  int nc, nm, L, ncolV, ncolP;
   const int2* cab;
   const int* cSlot;
   const int* cOrder;
@@ -175,7 +183,23 @@ struct XWork {
   D4* tp;                         // [sweeps][nc][2]: xA, xB
   double* theta;                  // [3] d/d(eN, eT, mu)
   double* err;                    // [2] replay deviation from the recorded next state (max)
+  u64* hash;                      // branch signature of the replays (null: not collected)
 };
+
+// order-free branch signature: a sum over the sweep updates of a mixed (substep, sweep, entry,
+// branch bits) word (splitmix64 finaliser), summed per warp before one atomic
+__device__ __forceinline__ u64 mixWord(u64 x) {
+  x += 0x9E3779B97F4A7C15ull;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+  return x ^ (x >> 31);
+}
+__device__ __forceinline__ void warpHashAdd(u64* h, u64 v) {
+  for (int o = 16; o > 0; o >>= 1)
+    v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0 && v)
+    atomicAdd(reinterpret_cast<unsigned long long*>(h), (unsigned long long)v);
+}
 
 __device__ __forceinline__ void atomicMaxPos(double* p, double v) {
   if (v > 0.0)
@@ -381,25 +405,55 @@ __device__ __forceinline__ void pgsIn(const XScene& sc, const XView& r, const XW
   in[46] = sc.mu;
 }
 
-__global__ void kxPgs(XScene sc, XView r, XWork w, int col, int sweep, double vRest, int stab) {
+// one PGS update of the replay: manifold m at sweep `sweep` (its inputs kept on the tape)
+__device__ __forceinline__ void pgsFwdEntry(const XScene& sc, const XView& r, const XWork& w, int m, int sweep,
+                                            double vRest, int stab, int tag, u64& hs) {
+  if (w.np[m] <= 0)
+    return;
+  const int2 ab = r.mab[m];
+  double in[kPgsIn], out[kPgsOut];
+  velIn(w, ab, in);
+  pgsIn(sc, r, w, m, ab, in);
+  D4* tape = w.tv + 4 * ((long)sweep * r.nm + m);
+  tape[0] = get3(in, 0, in[12]);
+  tape[1] = get3(in, 3, in[13]);
+  tape[2] = get3(in, 6, in[14]);
+  tape[3] = get3(in, 9, in[15]);
+  unsigned bits = 0;
+  pgsMap<double>(in, out, manC(sc, r, w, m, stab ? (int)r.sf[m] : 0), vRest, w.hash ? &bits : nullptr);
+  if (w.hash)
+    hs += mixWord(((u64)(unsigned)tag << 40) ^ ((u64)(unsigned)sweep << 28) ^ ((u64)(unsigned)m << 8) ^ bits);
+  velOut(w, ab, out);
+  w.lam[m] = get3(out, 13, out[12]);
+}
+
+__global__ void kxPgs(XScene sc, XView r, XWork w, int col, int sweep, double vRest, int stab, int tag) {
   const int b = r.mOff[col], cnt = r.mOff[col + 1] - b;
-  GRID_STRIDE(t, cnt) {
-    const int m = r.mOrder[b + t];
-    if (w.np[m] <= 0)
-      continue;
-    const int2 ab = r.mab[m];
-    double in[kPgsIn], out[kPgsOut];
-    velIn(w, ab, in);
-    pgsIn(sc, r, w, m, ab, in);
-    D4* tape = w.tv + 4 * ((long)sweep * r.nm + m);
-    tape[0] = get3(in, 0, in[12]);
-    tape[1] = get3(in, 3, in[13]);
-    tape[2] = get3(in, 6, in[14]);
-    tape[3] = get3(in, 9, in[15]);
-    pgsMap<double>(in, out, manC(sc, r, w, m, stab ? (int)r.sf[m] : 0), vRest);
-    velOut(w, ab, out);
-    w.lam[m] = get3(out, 13, out[12]);
+  u64 hs = 0;
+  GRID_STRIDE(t, cnt) { pgsFwdEntry(sc, r, w, r.mOrder[b + t], sweep, vRest, stab, tag, hs); }
+  if (w.hash)
+    warpHashAdd(w.hash, hs);
+}
+
+// the replay's main and stabilization sweeps in one persistent launch of one thread-block
+// cluster: colour by colour, a cluster barrier between colours (the blocks take fixed contiguous
+// slices of each colour, so an entry's constants stay in its SM's L1 across the sweeps)
+__global__ void __launch_bounds__(kB) kxPgsCluster(XScene sc, XView r, XWork w, int velSweeps, int stabSweeps,
+                                                   double vRest, int tag) {
+  const int nb = gridDim.x;
+  u64 hs = 0;
+  for (int it = 0; it < velSweeps + stabSweeps; ++it) {
+    const int stab = it >= velSweeps ? 1 : 0;
+    for (int c = 0; c < r.ncolV; ++c) {
+      const int b = r.mOff[c], cnt = r.mOff[c + 1] - b;
+      const int lo = (int)((long)cnt * blockIdx.x / nb), hi = (int)((long)cnt * (blockIdx.x + 1) / nb);
+      for (int t = lo + threadIdx.x; t < hi; t += blockDim.x)
+        pgsFwdEntry(sc, r, w, r.mOrder[b + t], it, vRest, stab, tag, hs);
+      cg::this_cluster().sync();
+    }
   }
+  if (w.hash)
+    warpHashAdd(w.hash, hs);
 }
 
 __global__ void kxIntegrate(XScene sc, XView r, XWork w) {
@@ -442,8 +496,9 @@ __device__ __forceinline__ void posIn(const XScene& sc, const XView& r, const XW
   put3(in, 28, w.cgB[k]);
 }
 
-__global__ void kxPos(XScene sc, XView r, XWork w, int col, int sweep) {
+__global__ void kxPos(XScene sc, XView r, XWork w, int col, int sweep, int tag) {
   const int b = r.cOff[col], cnt = r.cOff[col + 1] - b;
+  u64 hs = 0;
   GRID_STRIDE(t, cnt) {
     const int k = r.cOrder[b + t];
     const int2 ab = r.cab[k];
@@ -453,12 +508,17 @@ __global__ void kxPos(XScene sc, XView r, XWork w, int col, int sweep) {
     tape[1] = xB;
     double in[kPosIn], out[kPosOut];
     posIn(sc, r, w, k, ab, xA, xB, in);
-    posMap<double>(in, out, posC(sc, ab));
+    unsigned bits = 0;
+    posMap<double>(in, out, posC(sc, ab), w.hash ? &bits : nullptr);
+    if (w.hash)
+      hs += mixWord(((u64)(unsigned)tag << 40) ^ ((u64)(unsigned)(sweep + 4096) << 28) ^ ((u64)(unsigned)k << 8) ^ bits);
     w.xP[ab.x] = get3(out, 0);
     if (ab.y >= 0)
       w.xP[ab.y] = get3(out, 3);
     w.posLam[k] += out[6];
   }
+  if (w.hash)
+    warpHashAdd(w.hash, hs);
 }
 
 // the replay's end state against the recorded start of the next substep
@@ -498,29 +558,75 @@ __global__ void kxRevInit(XScene sc, XView r, XWork w) {
   }
 }
 
-__global__ void kxPosRev(XScene sc, XView r, XWork w, int col, int sweep) {
+__global__ void __launch_bounds__(kBR) kxPosRev(XScene sc, XView r, XWork w, int col, int sweep) {
+  __shared__ double sx[kBR / kGroup][kPosIn];
+  const int b = r.cOff[col], cnt = r.cOff[col + 1] - b;
+  const int lane = threadIdx.x % kGroup, slot = threadIdx.x / kGroup, per = blockDim.x / kGroup;
+  for (long t0 = (long)blockIdx.x * per; t0 < cnt; t0 += (long)gridDim.x * per) {
+    const long t = t0 + slot;
+    const int k = t < cnt ? r.cOrder[b + t] : -1;
+    int2 ab{0, -1};
+    if (k >= 0) {
+      ab = r.cab[k];
+      if (lane * kLanes < kPosIn) {
+        const D4* tape = w.tp + 2 * ((long)sweep * r.nc + k);
+        double in[kPosIn], yb[kPosOut], part[kLanes];
+        posIn(sc, r, w, k, ab, tape[0], tape[1], in);
+        for (int j = 0; j < kPosOut; ++j)
+          yb[j] = 0.0;
+        put3(yb, 0, w.axP[ab.x]);
+        if (ab.y >= 0)
+          put3(yb, 3, w.axP[ab.y]);
+        yb[6] = w.aposLam[k];
+        const PosC pc = posC(sc, ab);
+        vjpChunk<kPosIn, kPosOut>(in, yb, part, lane, [&](const Dd<kLanes>* x, Dd<kLanes>* y) { posMap(x, y, pc); });
+        for (int l = 0; l < kLanes && lane * kLanes + l < kPosIn; ++l)
+          sx[slot][lane * kLanes + l] = part[l];
+      }
+    }
+    __syncthreads();
+    if (k >= 0 && lane == 0) {
+      const double* xb = sx[slot];
+      w.axP[ab.x] = get3(xb, 0);
+      add4(w.aqP[ab.x], xb + 6);
+      add4(w.aq[ab.x], xb + 14);
+      if (ab.y >= 0) {
+        w.axP[ab.y] = get3(xb, 3);
+        add4(w.aqP[ab.y], xb + 10);
+        add4(w.aq[ab.y], xb + 18);
+      }
+      add3(w.acgN[k], xb + 22);
+      add3(w.acgA[k], xb + 25);
+      add3(w.acgB[k], xb + 28);
+    }
+    __syncthreads();
+  }
+}
+
+// the hand-written reverses of the position update, the warm start and the approach velocity:
+// one entry a thread (the grouped kernels above and below reverse the same maps through
+// forward-mode chunks: the cross-check)
+__global__ void kxPosRevH(XScene sc, XView r, XWork w, int col, int sweep) {
   const int b = r.cOff[col], cnt = r.cOff[col + 1] - b;
   GRID_STRIDE(t, cnt) {
     const int k = r.cOrder[b + t];
     const int2 ab = r.cab[k];
-    const bool hasB = ab.y >= 0;
     const D4* tape = w.tp + 2 * ((long)sweep * r.nc + k);
     double in[kPosIn], yb[kPosOut], xb[kPosIn];
     posIn(sc, r, w, k, ab, tape[0], tape[1], in);
     for (int j = 0; j < kPosOut; ++j)
       yb[j] = 0.0;
     put3(yb, 0, w.axP[ab.x]);
-    if (hasB)
+    if (ab.y >= 0)
       put3(yb, 3, w.axP[ab.y]);
     yb[6] = w.aposLam[k];
     for (int j = 0; j < kPosIn; ++j)
       xb[j] = 0.0;
-    const PosC pc = posC(sc, ab);
-    vjp<kPosIn, kPosOut>(in, yb, xb, [&](const Dd<kLanes>* x, Dd<kLanes>* y) { posMap(x, y, pc); });
+    posRev(in, yb, xb, posC(sc, ab));
     w.axP[ab.x] = get3(xb, 0);
     add4(w.aqP[ab.x], xb + 6);
     add4(w.aq[ab.x], xb + 14);
-    if (hasB) {
+    if (ab.y >= 0) {
       w.axP[ab.y] = get3(xb, 3);
       add4(w.aqP[ab.y], xb + 10);
       add4(w.aq[ab.y], xb + 18);
@@ -530,107 +636,17 @@ __global__ void kxPosRev(XScene sc, XView r, XWork w, int col, int sweep) {
     add3(w.acgB[k], xb + 28);
   }
 }
-
-__global__ void kxIntegrateRev(XScene sc, XView r, XWork w) {
-  GRID_STRIDE(i, sc.n) {
-    double in[kIntIn], yb[kIntOut], xb[kIntIn];
-    put3(in, 0, r.st[i]);
-    put4(in, 3, r.st[sc.n + i]);
-    put3(in, 7, r.st[2 * sc.n + i]);
-    put3(in, 10, w.vF[i]);
-    put3(in, 13, w.wF[i]);
-    put3(yb, 0, w.axP[i]);
-    put4(yb, 3, w.aqP[i]);
-    for (int j = 0; j < kIntIn; ++j)
-      xb[j] = 0.0;
-    const double im = sc.invMass[i], dt = sc.dt;
-    vjp<kIntIn, kIntOut>(in, yb, xb, [&](const Dd<kLanes>* x, Dd<kLanes>* y) { integrateMap(x, y, im, dt); });
-    add3(w.ax[i], xb);
-    add4(w.aq[i], xb + 3);
-    add3(w.av[i], xb + 7);
-    D4 a = w.gv[i], b = w.gw[i];
-    add3(a, xb + 10);
-    add3(b, xb + 13);
-    w.avP[i] = a;
-    w.awP[i] = b;
-  }
-}
-
-// mode 0: the hand-written reverse (pgsRev); mode 1: the forward-mode local Jacobian (the check)
-__global__ void kxPgsRev(XScene sc, XView r, XWork w, int col, int sweep, double vRest, int stab, int mode) {
-  const int b = r.mOff[col], cnt = r.mOff[col + 1] - b;
-  GRID_STRIDE(t, cnt) {
-    const int m = r.mOrder[b + t];
+// over every manifold in one launch: the body adjoints it reads are the sweeps' (not changed
+// here), and its orientation adjoints accumulate with atomics
+__global__ void kxWarmRevH(XScene sc, XView r, XWork w) {
+  GRID_STRIDE(t, r.nm) {
+    const int m = (int)t;
     if (w.np[m] <= 0)
       continue;
     const int2 ab = r.mab[m];
-    const bool hasB = ab.y >= 0;
-    const D4* tape = w.tv + 4 * ((long)sweep * r.nm + m);
-    double in[kPgsIn], yb[kPgsOut], xb[kPgsIn];
-    put3(in, 0, tape[0]);
-    put3(in, 3, tape[1]);
-    put3(in, 6, tape[2]);
-    put3(in, 9, tape[3]);
-    in[12] = tape[0].w;
-    in[13] = tape[1].w;
-    in[14] = tape[2].w;
-    in[15] = tape[3].w;
-    geoIn(w, m, in, 16);
-    quatIn(sc, r, ab, in, 31);
-    in[39] = w.vn[m].w;
-    put3(in, 40, w.vn[m]);
-    in[43] = w.posIn[m];
-    in[44] = sc.eN;
-    in[45] = sc.eT;
-    in[46] = sc.mu;
-    for (int j = 0; j < kPgsOut; ++j)
-      yb[j] = 0.0;
-    put3(yb, 0, w.avP[ab.x]);
-    put3(yb, 3, w.awP[ab.x]);
-    if (hasB) {
-      put3(yb, 6, w.avP[ab.y]);
-      put3(yb, 9, w.awP[ab.y]);
-    }
-    yb[12] = w.alam[m].w;
-    put3(yb, 13, w.alam[m]);
-    for (int j = 0; j < kPgsIn; ++j)
-      xb[j] = 0.0;
-    const ManC mc = manC(sc, r, w, m, stab ? (int)r.sf[m] : 0);
-    if (mode == 0)
-      pgsRev(in, yb, xb, mc, vRest);
-    else
-      vjp<kPgsIn, kPgsOut>(in, yb, xb, [&](const Dd<kLanes>* x, Dd<kLanes>* y) { pgsMap(x, y, mc, vRest); });
-    w.avP[ab.x] = get3(xb, 0);
-    w.awP[ab.x] = get3(xb, 3);
-    add4(w.aq[ab.x], xb + 31);
-    if (hasB) {
-      w.avP[ab.y] = get3(xb, 6);
-      w.awP[ab.y] = get3(xb, 9);
-      add4(w.aq[ab.y], xb + 35);
-    }
-    w.alam[m] = get3(xb, 13, xb[12]);
-    for (int j = 0; j < 5; ++j)
-      add3(w.ageo[5 * m + j], xb + 16 + 3 * j);
-    D4 av = w.avn[m];
-    av.w += xb[39];
-    add3(av, xb + 40);
-    w.avn[m] = av;
-    w.aposIn[m] += xb[43];
-    add3(w.ath[m], xb + 44);
-  }
-}
-
-__global__ void kxWarmRev(XScene sc, XView r, XWork w, int col) {
-  const int b = r.mOff[col], cnt = r.mOff[col + 1] - b;
-  GRID_STRIDE(t, cnt) {
-    const int m = r.mOrder[b + t];
-    if (w.np[m] <= 0)
-      continue;
-    const int2 ab = r.mab[m];
-    const bool hasB = ab.y >= 0;
     double in[kWarmIn], yb[kWarmOut], xb[kWarmIn];
     for (int j = 0; j < 12; ++j)
-      in[j] = 0.0;  // the increments do not depend on the velocities
+      in[j] = 0.0;
     in[12] = w.lam0[m].w;
     put3(in, 13, w.lam0[m]);
     geoIn(w, m, in, 16);
@@ -639,39 +655,36 @@ __global__ void kxWarmRev(XScene sc, XView r, XWork w, int col) {
       yb[j] = 0.0;
     put3(yb, 0, w.avP[ab.x]);
     put3(yb, 3, w.awP[ab.x]);
-    if (hasB) {
+    if (ab.y >= 0) {
       put3(yb, 6, w.avP[ab.y]);
       put3(yb, 9, w.awP[ab.y]);
     }
     put3(yb, 12, w.alam[m]);
     for (int j = 0; j < kWarmIn; ++j)
       xb[j] = 0.0;
-    const ManC mc = manC(sc, r, w, m, 0);
-    vjp<kWarmIn, kWarmOut>(in, yb, xb, [&](const Dd<kLanes>* x, Dd<kLanes>* y) { warmMap(x, y, mc); });
-    // lambda enters the sweeps unchanged and the warm start; lambda_T only through the warm start
+    warmRev(in, yb, xb, manC(sc, r, w, m, 0));
     w.alam[m] = get3(xb, 13, w.alam[m].w + xb[12]);
     for (int j = 0; j < 5; ++j)
       add3(w.ageo[5 * m + j], xb + 16 + 3 * j);
-    add4(w.aq[ab.x], xb + 31);
-    if (hasB)
-      add4(w.aq[ab.y], xb + 35);
+    atomicAdd4(&w.aq[ab.x], xb + 31);
+    if (ab.y >= 0)
+      atomicAdd4(&w.aq[ab.y], xb + 35);
   }
 }
-
-__global__ void kxVn0Rev(XScene sc, XView r, XWork w, int col) {
-  const int b = r.mOff[col], cnt = r.mOff[col + 1] - b;
-  GRID_STRIDE(t, cnt) {
-    const int m = r.mOrder[b + t];
+// over every manifold in one launch, after every warm-start reverse: the velocity adjoints become
+// those of the predicted velocities (atomics: manifolds share bodies)
+__global__ void kxVn0RevH(XScene sc, XView r, XWork w) {
+  GRID_STRIDE(t, r.nm) {
+    const int m = (int)t;
     if (w.np[m] <= 0)
       continue;
     const int2 ab = r.mab[m];
-    const bool hasB = ab.y >= 0;
     double in[kVn0In], yb[kVn0Out], xb[kVn0In];
     for (int j = 0; j < 12; ++j)
       in[j] = 0.0;
     put3(in, 0, w.vP0[ab.x]);
     put3(in, 3, w.wP0[ab.x]);
-    if (hasB) {
+    if (ab.y >= 0) {
       put3(in, 6, w.vP0[ab.y]);
       put3(in, 9, w.wP0[ab.y]);
     }
@@ -680,16 +693,233 @@ __global__ void kxVn0Rev(XScene sc, XView r, XWork w, int col) {
     put3(yb, 1, w.avn[m]);
     for (int j = 0; j < kVn0In; ++j)
       xb[j] = 0.0;
-    const ManC mc = manC(sc, r, w, m, 0);
-    vjp<kVn0In, kVn0Out>(in, yb, xb, [&](const Dd<kLanes>* x, Dd<kLanes>* y) { vn0Map(x, y, mc); });
-    add3(w.avP[ab.x], xb);
-    add3(w.awP[ab.x], xb + 3);
-    if (hasB) {
-      add3(w.avP[ab.y], xb + 6);
-      add3(w.awP[ab.y], xb + 9);
+    vn0Rev(in, yb, xb, manC(sc, r, w, m, 0));
+    atomicAdd3(&w.avP[ab.x], xb);
+    atomicAdd3(&w.awP[ab.x], xb + 3);
+    if (ab.y >= 0) {
+      atomicAdd3(&w.avP[ab.y], xb + 6);
+      atomicAdd3(&w.awP[ab.y], xb + 9);
     }
     for (int j = 0; j < 5; ++j)
       add3(w.ageo[5 * m + j], xb + 12 + 3 * j);
+  }
+}
+
+__global__ void __launch_bounds__(kBR) kxIntegrateRev(XScene sc, XView r, XWork w) {
+  __shared__ double sx[kBR / kGroup][kIntIn];
+  const int lane = threadIdx.x % kGroup, slot = threadIdx.x / kGroup, per = blockDim.x / kGroup;
+  for (long t0 = (long)blockIdx.x * per; t0 < sc.n; t0 += (long)gridDim.x * per) {
+    const long i = t0 + slot;
+    if (i < sc.n && lane * kLanes < kIntIn) {
+      double in[kIntIn], yb[kIntOut], part[kLanes];
+      put3(in, 0, r.st[i]);
+      put4(in, 3, r.st[sc.n + i]);
+      put3(in, 7, r.st[2 * sc.n + i]);
+      put3(in, 10, w.vF[i]);
+      put3(in, 13, w.wF[i]);
+      put3(yb, 0, w.axP[i]);
+      put4(yb, 3, w.aqP[i]);
+      const double im = sc.invMass[i], dt = sc.dt;
+      vjpChunk<kIntIn, kIntOut>(in, yb, part, lane, [&](const Dd<kLanes>* x, Dd<kLanes>* y) { integrateMap(x, y, im, dt); });
+      for (int l = 0; l < kLanes && lane * kLanes + l < kIntIn; ++l)
+        sx[slot][lane * kLanes + l] = part[l];
+    }
+    __syncthreads();
+    if (i < sc.n && lane == 0) {
+      const double* xb = sx[slot];
+      add3(w.ax[i], xb);
+      add4(w.aq[i], xb + 3);
+      add3(w.av[i], xb + 7);
+      D4 a = w.gv[i], c = w.gw[i];
+      add3(a, xb + 10);
+      add3(c, xb + 13);
+      w.avP[i] = a;
+      w.awP[i] = c;
+    }
+    __syncthreads();
+  }
+}
+
+// the reverse of one PGS update (manifold m at sweep `sweep`). MODE 0: the hand-written reverse
+// (pgsRev); MODE 1: the forward-mode local Jacobian (the check)
+template <int MODE>
+__device__ __forceinline__ void pgsRevEntry(const XScene& sc, const XView& r, const XWork& w, int m, int sweep,
+                                            double vRest, int stab) {
+  if (w.np[m] <= 0)
+    return;
+  const int2 ab = r.mab[m];
+  const bool hasB = ab.y >= 0;
+  const D4* tape = w.tv + 4 * ((long)sweep * r.nm + m);
+  double in[kPgsIn], yb[kPgsOut], xb[kPgsIn];
+  put3(in, 0, tape[0]);
+  put3(in, 3, tape[1]);
+  put3(in, 6, tape[2]);
+  put3(in, 9, tape[3]);
+  in[12] = tape[0].w;
+  in[13] = tape[1].w;
+  in[14] = tape[2].w;
+  in[15] = tape[3].w;
+  geoIn(w, m, in, 16);
+  quatIn(sc, r, ab, in, 31);
+  in[39] = w.vn[m].w;
+  put3(in, 40, w.vn[m]);
+  in[43] = w.posIn[m];
+  in[44] = sc.eN;
+  in[45] = sc.eT;
+  in[46] = sc.mu;
+  for (int j = 0; j < kPgsOut; ++j)
+    yb[j] = 0.0;
+  put3(yb, 0, w.avP[ab.x]);
+  put3(yb, 3, w.awP[ab.x]);
+  if (hasB) {
+    put3(yb, 6, w.avP[ab.y]);
+    put3(yb, 9, w.awP[ab.y]);
+  }
+  yb[12] = w.alam[m].w;
+  put3(yb, 13, w.alam[m]);
+  for (int j = 0; j < kPgsIn; ++j)
+    xb[j] = 0.0;
+  const ManC mc = manC(sc, r, w, m, stab ? (int)r.sf[m] : 0);
+  if (MODE == 0)
+    pgsRev(in, yb, xb, mc, vRest);
+  else
+    vjp<kPgsIn, kPgsOut>(in, yb, xb, [&](const Dd<kLanes>* x, Dd<kLanes>* y) { pgsMap(x, y, mc, vRest); });
+  w.avP[ab.x] = get3(xb, 0);
+  w.awP[ab.x] = get3(xb, 3);
+  add4(w.aq[ab.x], xb + 31);
+  if (hasB) {
+    w.avP[ab.y] = get3(xb, 6);
+    w.awP[ab.y] = get3(xb, 9);
+    add4(w.aq[ab.y], xb + 35);
+  }
+  w.alam[m] = get3(xb, 13, xb[12]);
+  for (int j = 0; j < 5; ++j)
+    add3(w.ageo[5 * m + j], xb + 16 + 3 * j);
+  D4 av = w.avn[m];
+  av.w += xb[39];
+  add3(av, xb + 40);
+  w.avn[m] = av;
+  w.aposIn[m] += xb[43];
+  add3(w.ath[m], xb + 44);
+}
+
+template <int MODE>
+__global__ void kxPgsRev(XScene sc, XView r, XWork w, int col, int sweep, double vRest, int stab) {
+  const int b = r.mOff[col], cnt = r.mOff[col + 1] - b;
+  GRID_STRIDE(t, cnt) { pgsRevEntry<MODE>(sc, r, w, r.mOrder[b + t], sweep, vRest, stab); }
+}
+
+// the reverse of both PGS loops in one persistent cluster launch: sweeps and colours in reverse
+// order, the same slices of each colour per block as the replay's
+__global__ void __launch_bounds__(kB) kxPgsRevCluster(XScene sc, XView r, XWork w, int velSweeps, int stabSweeps,
+                                                      double vRest) {
+  const int nb = gridDim.x;
+  for (int it = velSweeps + stabSweeps - 1; it >= 0; --it) {
+    const int stab = it >= velSweeps ? 1 : 0;
+    for (int c = r.ncolV - 1; c >= 0; --c) {
+      const int b = r.mOff[c], cnt = r.mOff[c + 1] - b;
+      const int lo = (int)((long)cnt * blockIdx.x / nb), hi = (int)((long)cnt * (blockIdx.x + 1) / nb);
+      for (int t = lo + threadIdx.x; t < hi; t += blockDim.x)
+        pgsRevEntry<0>(sc, r, w, r.mOrder[b + t], it, vRest, stab);
+      cg::this_cluster().sync();
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kBR) kxWarmRev(XScene sc, XView r, XWork w, int col) {
+  __shared__ double sx[kBR / kGroup][kWarmIn];
+  const int b = r.mOff[col], cnt = r.mOff[col + 1] - b;
+  const int lane = threadIdx.x % kGroup, slot = threadIdx.x / kGroup, per = blockDim.x / kGroup;
+  for (long t0 = (long)blockIdx.x * per; t0 < cnt; t0 += (long)gridDim.x * per) {
+    const long t = t0 + slot;
+    int m = t < cnt ? r.mOrder[b + t] : -1;
+    if (m >= 0 && w.np[m] <= 0)
+      m = -1;
+    int2 ab{0, -1};
+    if (m >= 0) {
+      ab = r.mab[m];
+      if (lane * kLanes < kWarmIn) {
+        double in[kWarmIn], yb[kWarmOut], part[kLanes];
+        for (int j = 0; j < 12; ++j)
+          in[j] = 0.0;  // the increments do not depend on the velocities
+        in[12] = w.lam0[m].w;
+        put3(in, 13, w.lam0[m]);
+        geoIn(w, m, in, 16);
+        quatIn(sc, r, ab, in, 31);
+        for (int j = 0; j < kWarmOut; ++j)
+          yb[j] = 0.0;
+        put3(yb, 0, w.avP[ab.x]);
+        put3(yb, 3, w.awP[ab.x]);
+        if (ab.y >= 0) {
+          put3(yb, 6, w.avP[ab.y]);
+          put3(yb, 9, w.awP[ab.y]);
+        }
+        put3(yb, 12, w.alam[m]);
+        const ManC mc = manC(sc, r, w, m, 0);
+        vjpChunk<kWarmIn, kWarmOut>(in, yb, part, lane, [&](const Dd<kLanes>* x, Dd<kLanes>* y) { warmMap(x, y, mc); });
+        for (int l = 0; l < kLanes && lane * kLanes + l < kWarmIn; ++l)
+          sx[slot][lane * kLanes + l] = part[l];
+      }
+    }
+    __syncthreads();
+    if (m >= 0 && lane == 0) {
+      const double* xb = sx[slot];
+      // lambda enters the sweeps unchanged and the warm start; lambda_T only through the warm start
+      w.alam[m] = get3(xb, 13, w.alam[m].w + xb[12]);
+      for (int j = 0; j < 5; ++j)
+        add3(w.ageo[5 * m + j], xb + 16 + 3 * j);
+      add4(w.aq[ab.x], xb + 31);
+      if (ab.y >= 0)
+        add4(w.aq[ab.y], xb + 35);
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(kBR) kxVn0Rev(XScene sc, XView r, XWork w, int col) {
+  __shared__ double sx[kBR / kGroup][kVn0In];
+  const int b = r.mOff[col], cnt = r.mOff[col + 1] - b;
+  const int lane = threadIdx.x % kGroup, slot = threadIdx.x / kGroup, per = blockDim.x / kGroup;
+  for (long t0 = (long)blockIdx.x * per; t0 < cnt; t0 += (long)gridDim.x * per) {
+    const long t = t0 + slot;
+    int m = t < cnt ? r.mOrder[b + t] : -1;
+    if (m >= 0 && w.np[m] <= 0)
+      m = -1;
+    int2 ab{0, -1};
+    if (m >= 0) {
+      ab = r.mab[m];
+      if (lane * kLanes < kVn0In) {
+        double in[kVn0In], yb[kVn0Out], part[kLanes];
+        for (int j = 0; j < 12; ++j)
+          in[j] = 0.0;
+        put3(in, 0, w.vP0[ab.x]);
+        put3(in, 3, w.wP0[ab.x]);
+        if (ab.y >= 0) {
+          put3(in, 6, w.vP0[ab.y]);
+          put3(in, 9, w.wP0[ab.y]);
+        }
+        geoIn(w, m, in, 12);
+        yb[0] = w.avn[m].w;
+        put3(yb, 1, w.avn[m]);
+        const ManC mc = manC(sc, r, w, m, 0);
+        vjpChunk<kVn0In, kVn0Out>(in, yb, part, lane, [&](const Dd<kLanes>* x, Dd<kLanes>* y) { vn0Map(x, y, mc); });
+        for (int l = 0; l < kLanes && lane * kLanes + l < kVn0In; ++l)
+          sx[slot][lane * kLanes + l] = part[l];
+      }
+    }
+    __syncthreads();
+    if (m >= 0 && lane == 0) {
+      const double* xb = sx[slot];
+      add3(w.avP[ab.x], xb);
+      add3(w.awP[ab.x], xb + 3);
+      if (ab.y >= 0) {
+        add3(w.avP[ab.y], xb + 6);
+        add3(w.awP[ab.y], xb + 9);
+      }
+      for (int j = 0; j < 5; ++j)
+        add3(w.ageo[5 * m + j], xb + 12 + 3 * j);
+    }
+    __syncthreads();
   }
 }
 
@@ -703,78 +933,110 @@ __global__ void kxGatherRev(XScene sc, XView r, XWork w) {
   }
 }
 
-__global__ void kxManifoldRev(XScene sc, XView r, XWork w) {
-  GRID_STRIDE(k, r.nc) {
-    if (!(w.cgN[k].w <= 0.0))
-      continue;
-    const int m = r.cSlot[k];
-    const int2 ab = r.cab[k];
-    double in[kManIn], yb[kManOut], xb[kManIn];
-    conIn(w, k, in);
-    for (int j = 0; j < 5; ++j)
-      put3(yb, 3 * j, w.ageo[5 * m + j]);
-    for (int j = 0; j < kManIn; ++j)
-      xb[j] = 0.0;
-    const bool flip = ab.y >= 0 && ab.y < ab.x;
-    vjp<kManIn, kManOut>(in, yb, xb, [&](const Dd<kLanes>* x, Dd<kLanes>* y) { manifoldMap(x, y, flip); });
-    add3(w.acgN[k], xb);
-    add3(w.acgA[k], xb + 3);
-    add3(w.acgB[k], xb + 6);
-    w.acgN[k].w += xb[9];
-  }
-}
-
-__global__ void kxContactRev(XScene sc, XView r, XWork w) {
-  GRID_STRIDE(k, r.nc) {
-    const int2 ab = r.cab[k];
-    if (ab.y >= 0) {
-      double in[kConIn], yb[kConOut], xb[kConIn];
-      put3(in, 0, w.xP0[ab.x]);
-      put4(in, 3, r.st[sc.n + ab.x]);
-      put3(in, 7, w.xP0[ab.y]);
-      put4(in, 10, r.st[sc.n + ab.y]);
-      put3(yb, 0, w.acgN[k]);
-      put3(yb, 3, w.acgA[k]);
-      put3(yb, 6, w.acgB[k]);
-      yb[9] = w.acgN[k].w;
-      for (int j = 0; j < kConIn; ++j)
-        xb[j] = 0.0;
-      const ConC cc = conC(sc, ab.x, ab.y);
-      vjp<kConIn, kConOut>(in, yb, xb, [&](const Dd<kLanes>* x, Dd<kLanes>* y) { contactMap(x, y, cc); });
-      atomicAdd3(&w.axP0[ab.x], xb);
-      atomicAdd4(&w.aq[ab.x], xb + 3);
-      atomicAdd3(&w.axP0[ab.y], xb + 7);
-      atomicAdd4(&w.aq[ab.y], xb + 10);
-    } else {
-      // only the distance of a plane contact moves with the body: dist = (x - p) . n - radius
-      const D4 n = w.cgN[k];
-      const double g = w.acgN[k].w;
-      const double v[3] = {g * n.x, g * n.y, g * n.z};
-      atomicAdd3(&w.axP0[ab.x], v);
+__global__ void __launch_bounds__(kBR) kxManifoldRev(XScene sc, XView r, XWork w) {
+  __shared__ double sx[kBR / kGroup][kManIn];
+  const int lane = threadIdx.x % kGroup, slot = threadIdx.x / kGroup, per = blockDim.x / kGroup;
+  for (long t0 = (long)blockIdx.x * per; t0 < r.nc; t0 += (long)gridDim.x * per) {
+    const long k = t0 + slot;
+    const bool on = k < r.nc && w.cgN[k].w <= 0.0;
+    if (on && lane * kLanes < kManIn) {
+      const int m = r.cSlot[k];
+      const int2 ab = r.cab[k];
+      double in[kManIn], yb[kManOut], part[kLanes];
+      conIn(w, (int)k, in);
+      for (int j = 0; j < 5; ++j)
+        put3(yb, 3 * j, w.ageo[5 * m + j]);
+      const bool flip = ab.y >= 0 && ab.y < ab.x;
+      vjpChunk<kManIn, kManOut>(in, yb, part, lane, [&](const Dd<kLanes>* x, Dd<kLanes>* y) { manifoldMap(x, y, flip); });
+      for (int l = 0; l < kLanes && lane * kLanes + l < kManIn; ++l)
+        sx[slot][lane * kLanes + l] = part[l];
     }
+    __syncthreads();
+    if (on && lane == 0) {
+      const double* xb = sx[slot];
+      add3(w.acgN[k], xb);
+      add3(w.acgA[k], xb + 3);
+      add3(w.acgB[k], xb + 6);
+      w.acgN[k].w += xb[9];
+    }
+    __syncthreads();
   }
 }
 
-__global__ void kxPredictRev(XScene sc, XView r, XWork w) {
-  GRID_STRIDE(i, sc.n) {
-    double in[kPredIn], yb[kPredOut], xb[kPredIn];
-    put3(in, 0, r.st[i]);
-    put4(in, 3, r.st[sc.n + i]);
-    put3(in, 7, r.st[2 * sc.n + i]);
-    put3(in, 10, r.st[3 * sc.n + i]);
-    put3(yb, 0, w.avP[i]);
-    put3(yb, 3, w.awP[i]);
-    put3(yb, 6, w.axP0[i]);
-    for (int j = 0; j < kPredIn; ++j)
-      xb[j] = 0.0;
-    const BodyC bc{sc.invMass[i], v3d(sc.invI[i])};
-    const StepC st{sc.dt, sc.g, 0.0, sc.eps};
-    const V3<double> F = v3d(sc.extF[i]);
-    vjp<kPredIn, kPredOut>(in, yb, xb, [&](const Dd<kLanes>* x, Dd<kLanes>* y) { predictMap(x, y, bc, st, F); });
-    add3(w.ax[i], xb);
-    add4(w.aq[i], xb + 3);
-    add3(w.av[i], xb + 7);
-    add3(w.aw[i], xb + 10);
+__global__ void __launch_bounds__(kBR) kxContactRev(XScene sc, XView r, XWork w) {
+  __shared__ double sx[kBR / kGroup][kConIn];
+  const int lane = threadIdx.x % kGroup, slot = threadIdx.x / kGroup, per = blockDim.x / kGroup;
+  for (long t0 = (long)blockIdx.x * per; t0 < r.nc; t0 += (long)gridDim.x * per) {
+    const long k = t0 + slot;
+    int2 ab{0, -1};
+    if (k < r.nc) {
+      ab = r.cab[k];
+      if (ab.y >= 0 && lane * kLanes < kConIn) {
+        double in[kConIn], yb[kConOut], part[kLanes];
+        put3(in, 0, w.xP0[ab.x]);
+        put4(in, 3, r.st[sc.n + ab.x]);
+        put3(in, 7, w.xP0[ab.y]);
+        put4(in, 10, r.st[sc.n + ab.y]);
+        put3(yb, 0, w.acgN[k]);
+        put3(yb, 3, w.acgA[k]);
+        put3(yb, 6, w.acgB[k]);
+        yb[9] = w.acgN[k].w;
+        const ConC cc = conC(sc, ab.x, ab.y);
+        vjpChunk<kConIn, kConOut>(in, yb, part, lane, [&](const Dd<kLanes>* x, Dd<kLanes>* y) { contactMap(x, y, cc); });
+        for (int l = 0; l < kLanes && lane * kLanes + l < kConIn; ++l)
+          sx[slot][lane * kLanes + l] = part[l];
+      }
+    }
+    __syncthreads();
+    if (k < r.nc && lane == 0) {
+      if (ab.y >= 0) {
+        const double* xb = sx[slot];
+        atomicAdd3(&w.axP0[ab.x], xb);
+        atomicAdd4(&w.aq[ab.x], xb + 3);
+        atomicAdd3(&w.axP0[ab.y], xb + 7);
+        atomicAdd4(&w.aq[ab.y], xb + 10);
+      } else {
+        // only the distance of a plane contact moves with the body: dist = (x - p) . n - radius
+        const D4 n = w.cgN[k];
+        const double g = w.acgN[k].w;
+        const double v[3] = {g * n.x, g * n.y, g * n.z};
+        atomicAdd3(&w.axP0[ab.x], v);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(kBR) kxPredictRev(XScene sc, XView r, XWork w) {
+  __shared__ double sx[kBR / kGroup][kPredIn];
+  const int lane = threadIdx.x % kGroup, slot = threadIdx.x / kGroup, per = blockDim.x / kGroup;
+  for (long t0 = (long)blockIdx.x * per; t0 < sc.n; t0 += (long)gridDim.x * per) {
+    const long i = t0 + slot;
+    if (i < sc.n && lane * kLanes < kPredIn) {
+      double in[kPredIn], yb[kPredOut], part[kLanes];
+      put3(in, 0, r.st[i]);
+      put4(in, 3, r.st[sc.n + i]);
+      put3(in, 7, r.st[2 * sc.n + i]);
+      put3(in, 10, r.st[3 * sc.n + i]);
+      put3(yb, 0, w.avP[i]);
+      put3(yb, 3, w.awP[i]);
+      put3(yb, 6, w.axP0[i]);
+      const BodyC bc{sc.invMass[i], v3d(sc.invI[i])};
+      const StepC st{sc.dt, sc.g, 0.0, sc.eps};
+      const V3<double> F = v3d(sc.extF[i]);
+      vjpChunk<kPredIn, kPredOut>(in, yb, part, lane, [&](const Dd<kLanes>* x, Dd<kLanes>* y) { predictMap(x, y, bc, st, F); });
+      for (int l = 0; l < kLanes && lane * kLanes + l < kPredIn; ++l)
+        sx[slot][lane * kLanes + l] = part[l];
+    }
+    __syncthreads();
+    if (i < sc.n && lane == 0) {
+      const double* xb = sx[slot];
+      add3(w.ax[i], xb);
+      add4(w.aq[i], xb + 3);
+      add3(w.av[i], xb + 7);
+      add3(w.aw[i], xb + 10);
+    }
+    __syncthreads();
   }
 }
 
@@ -887,6 +1149,37 @@ __global__ void kxLedgerVals(int L, const double* lam, const D4* lt, D4* out) {
 }  // namespace
 
 // ---------------- host side ----------------
+// one cluster of `blocks` blocks on `st`; false (nothing launched) when such a cluster cannot be
+// resident (the answer is cached per kernel)
+template <class K, class... A>
+bool launchOneCluster(K kernel, int blocks, int block, cudaStream_t st, A... args) {
+  static int ok = -1;  // one cache per kernel instantiation
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(blocks);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = blocks;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  if (ok < 0) {
+    int clusters = 0;
+    if (blocks > 8 && cudaFuncSetAttribute(kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
+      (void)cudaGetLastError();
+    if (cudaOccupancyMaxActiveClusters(&clusters, kernel, &cfg) != cudaSuccess)
+      (void)cudaGetLastError();
+    ok = clusters >= 1 ? 1 : 0;
+  }
+  if (!ok)
+    return false;
+  cudaCheck(cudaLaunchKernelEx(&cfg, kernel, args...), "xadj cluster launch");
+  return true;
+}
+
 struct XRec {
   int nc = 0, nm = 0, L = 0, ncolV = 0, ncolP = 0, velSweeps = 0, stabSweeps = 0, posSweeps = 0;
   bool stab = false;
@@ -912,10 +1205,12 @@ struct XAdj {
   DBuf<D4> body, cont, man, alLB, tv, tp;
   DBuf<double> cdbl, mdbl, ldbl, small;
   DBuf<int> mint;
+  DBuf<u64> hashBuf;
   double err[2] = {0, 0};
   size_t workBytes = 0;
-  // PDEM_XADJ_DUAL=1: the PGS updates reversed through forward-mode local Jacobians instead of the
-  // hand-written reverse (the cross-check of the hand derivation; slower)
+  // PDEM_XADJ_DUAL=1: the PGS, warm-start, approach-velocity and position updates reversed through
+  // forward-mode local Jacobians instead of the hand-written reverses (the cross-check of the hand
+  // derivations; slower)
   int dualCheck = [] {
     const char* e = std::getenv("PDEM_XADJ_DUAL");
     return (e && e[0] == '1') ? 1 : 0;
@@ -1123,7 +1418,7 @@ struct XAdjAccess {
 
   static XView view(const XRec& R) {
     XView v;
-    v.nc = R.nc, v.nm = R.nm, v.L = R.L;
+    v.nc = R.nc, v.nm = R.nm, v.L = R.L, v.ncolV = R.ncolV, v.ncolP = R.ncolP;
     const int* I = R.ints.p;
     v.cab = reinterpret_cast<const int2*>(I + R.oCab);
     v.cSlot = I + R.oSlot;
@@ -1188,10 +1483,12 @@ struct XAdjAccess {
     w.alL = A.alLB.p, w.apL = A.ldbl.p;
     w.tv = A.tv.p, w.tp = A.tp.p;
     w.theta = A.small.p, w.err = A.small.p + 4;
+    w.hash = nullptr;
     return w;
   }
 
-  static void replay(S& s, const XScene& sc, const XRec& R, const XView& r, const XWork& w, const XRec* next) {
+  static void replay(S& s, const XScene& sc, const XRec& R, const XView& r, const XWork& w, const XRec* next,
+                     int tag) {
     cudaStream_t st = s.stream_;
     const int n = sc.n;
     const int gn = gridFor(n), gc = gridFor(std::max(R.nc, 1)), gm = gridFor(std::max(R.nm, 1));
@@ -1206,48 +1503,72 @@ struct XAdjAccess {
       kxVn0<<<gm, kB, 0, st>>>(sc, r, w);
       for (int c = 0; c < R.ncolV; ++c)
         kxWarm<<<gm, kB, 0, st>>>(sc, r, w, c);
-      for (int it = 0; it < R.velSweeps; ++it)
-        for (int c = 0; c < R.ncolV; ++c)
-          kxPgs<<<gm, kB, 0, st>>>(sc, r, w, c, it, vRest, 0);
-      for (int it = 0; it < R.stabSweeps; ++it)
-        for (int c = 0; c < R.ncolV; ++c)
-          kxPgs<<<gm, kB, 0, st>>>(sc, r, w, c, R.velSweeps + it, vRest, 1);
+      if (!(R.nm <= kClusterEntries && R.ncolV > 0 &&
+            launchOneCluster(kxPgsCluster, kClusterBlocks, kB, st, sc, r, w, R.velSweeps, R.stabSweeps, vRest, tag))) {
+        for (int it = 0; it < R.velSweeps; ++it)
+          for (int c = 0; c < R.ncolV; ++c)
+            kxPgs<<<gm, kB, 0, st>>>(sc, r, w, c, it, vRest, 0, tag);
+        for (int it = 0; it < R.stabSweeps; ++it)
+          for (int c = 0; c < R.ncolV; ++c)
+            kxPgs<<<gm, kB, 0, st>>>(sc, r, w, c, R.velSweeps + it, vRest, 1, tag);
+      }
     }
     kxIntegrate<<<gn, kB, 0, st>>>(sc, r, w);
     if (R.nc > 0) {
       cudaCheck(cudaMemsetAsync(w.posLam, 0, R.nc * sizeof(double), st), "memset");
       for (int it = 0; it < R.posSweeps; ++it)
         for (int c = 0; c < R.ncolP; ++c)
-          kxPos<<<gc, kB, 0, st>>>(sc, r, w, c, it);
+          kxPos<<<gc, kB, 0, st>>>(sc, r, w, c, it, tag);
     }
     if (next)
       kxCheck<<<gn, kB, 0, st>>>(sc, view(*next), w);
     cudaCheck(cudaGetLastError(), "xadj replay");
   }
 
+  static void pgsRevLaunch(const XAdj& A, int grid, cudaStream_t st, const XScene& sc, const XView& r, const XWork& w,
+                           int c, int sweep, double vRest, int stab) {
+    if (A.dualCheck)
+      kxPgsRev<1><<<grid, kBR, 0, st>>>(sc, r, w, c, sweep, vRest, stab);
+    else
+      kxPgsRev<0><<<gridFor(std::max(r.nm, 1), kBPgs), kBPgs, 0, st>>>(sc, r, w, c, sweep, vRest, stab);
+  }
   static void reverse(S& s, const XAdj& A, const XScene& sc, const XRec& R, const XView& r, const XWork& w) {
     cudaStream_t st = s.stream_;
     const int n = sc.n;
     const int gn = gridFor(n), gc = gridFor(std::max(R.nc, 1)), gm = gridFor(std::max(R.nm, 1));
     const double gMag = std::sqrt(sc.g.x * sc.g.x + sc.g.y * sc.g.y + sc.g.z * sc.g.z);
     const double vRest = 2.0 * sc.dt * gMag;
+    // the grouped reverse kernels: kGroup threads an entry
+    const int gnG = gridFor((long)kGroup * n, kBR), gcG = gridFor((long)kGroup * std::max(R.nc, 1), kBR),
+              gmG = gridFor((long)kGroup * std::max(R.nm, 1), kBR);
     kxRevInit<<<gridFor(std::max(n, std::max(R.nc, R.nm))), kB, 0, st>>>(sc, r, w);
     if (R.nc > 0)
       for (int it = R.posSweeps - 1; it >= 0; --it)
         for (int c = R.ncolP - 1; c >= 0; --c)
-          kxPosRev<<<gc, kBR, 0, st>>>(sc, r, w, c, it);
-    kxIntegrateRev<<<gn, kBR, 0, st>>>(sc, r, w);
+          if (A.dualCheck)
+            kxPosRev<<<gcG, kBR, 0, st>>>(sc, r, w, c, it);
+          else
+            kxPosRevH<<<gridFor(std::max(R.nc, 1), kBPgs), kBPgs, 0, st>>>(sc, r, w, c, it);
+    kxIntegrateRev<<<gnG, kBR, 0, st>>>(sc, r, w);
     if (R.nm > 0) {
-      for (int it = R.stabSweeps - 1; it >= 0; --it)
-        for (int c = R.ncolV - 1; c >= 0; --c)
-          kxPgsRev<<<gm, kBR, 0, st>>>(sc, r, w, c, R.velSweeps + it, vRest, 1, A.dualCheck);
-      for (int it = R.velSweeps - 1; it >= 0; --it)
-        for (int c = R.ncolV - 1; c >= 0; --c)
-          kxPgsRev<<<gm, kBR, 0, st>>>(sc, r, w, c, it, vRest, 0, A.dualCheck);
-      for (int c = 0; c < R.ncolV; ++c)
-        kxWarmRev<<<gm, kBR, 0, st>>>(sc, r, w, c);
-      for (int c = 0; c < R.ncolV; ++c)
-        kxVn0Rev<<<gm, kBR, 0, st>>>(sc, r, w, c);
+      if (!(!A.dualCheck && R.nm <= kClusterEntries && R.ncolV > 0 &&
+            launchOneCluster(kxPgsRevCluster, kClusterBlocks, kB, st, sc, r, w, R.velSweeps, R.stabSweeps, vRest))) {
+        for (int it = R.stabSweeps - 1; it >= 0; --it)
+          for (int c = R.ncolV - 1; c >= 0; --c)
+            pgsRevLaunch(A, gm, st, sc, r, w, c, R.velSweeps + it, vRest, 1);
+        for (int it = R.velSweeps - 1; it >= 0; --it)
+          for (int c = R.ncolV - 1; c >= 0; --c)
+            pgsRevLaunch(A, gm, st, sc, r, w, c, it, vRest, 0);
+      }
+      if (A.dualCheck) {
+        for (int c = 0; c < R.ncolV; ++c)
+          kxWarmRev<<<gmG, kBR, 0, st>>>(sc, r, w, c);
+        for (int c = 0; c < R.ncolV; ++c)
+          kxVn0Rev<<<gmG, kBR, 0, st>>>(sc, r, w, c);
+      } else {
+        kxWarmRevH<<<gridFor(std::max(R.nm, 1), kBPgs), kBPgs, 0, st>>>(sc, r, w);
+        kxVn0RevH<<<gridFor(std::max(R.nm, 1), kBPgs), kBPgs, 0, st>>>(sc, r, w);
+      }
       if (R.L > 0) {
         cudaCheck(cudaMemsetAsync(w.alL, 0, R.L * sizeof(D4), st), "memset");
         cudaCheck(cudaMemsetAsync(w.apL, 0, R.L * sizeof(double), st), "memset");
@@ -1256,10 +1577,10 @@ struct XAdjAccess {
       kxThetaSum<<<std::min(gm, 64), kB, 0, st>>>(r, w);
     }
     if (R.nc > 0) {
-      kxManifoldRev<<<gc, kBR, 0, st>>>(sc, r, w);
-      kxContactRev<<<gc, kBR, 0, st>>>(sc, r, w);
+      kxManifoldRev<<<gcG, kBR, 0, st>>>(sc, r, w);
+      kxContactRev<<<gcG, kBR, 0, st>>>(sc, r, w);
     }
-    kxPredictRev<<<gn, kBR, 0, st>>>(sc, r, w);
+    kxPredictRev<<<gnG, kBR, 0, st>>>(sc, r, w);
     cudaCheck(cudaGetLastError(), "xadj reverse");
   }
 
@@ -1289,7 +1610,7 @@ struct XAdjAccess {
     for (int t = T - 1; t >= 0; --t) {
       const XRec& R = *A.recs[t];
       const XView r = view(R);
-      replay(s, sc, R, r, w, t + 1 < T ? A.recs[t + 1].get() : nullptr);
+      replay(s, sc, R, r, w, t + 1 < T ? A.recs[t + 1].get() : nullptr, t);
       reverse(s, A, sc, R, r, w);
       if (t > 0) {
         const XRec& P = *A.recs[t - 1];
@@ -1336,6 +1657,29 @@ struct XAdjAccess {
     s.sync();
   }
 
+  // the branch signature of the recorded rollout: every substep replayed (no reverse), the branch
+  // decisions of every sweep update hashed
+  static unsigned long long branches(S& s) {
+    XAdj& A = get(s);
+    if (A.recs.empty())
+      throw std::invalid_argument("XPBD adjoint: nothing recorded (xa_begin, then xa_step)");
+    checkScope(s);
+    cudaStream_t st = s.stream_;
+    const XScene sc = scene(s, A);
+    XWork w = work(s, A);
+    A.hashBuf.ensure(1, false, st);
+    cudaCheck(cudaMemsetAsync(A.hashBuf.p, 0, sizeof(u64), st), "memset");
+    w.hash = A.hashBuf.p;
+    const int T = (int)A.recs.size();
+    for (int t = 0; t < T; ++t) {
+      const XRec& R = *A.recs[t];
+      replay(s, sc, R, view(R), w, nullptr, t);
+    }
+    u64 h = 0;
+    cudaCheck(cudaMemcpyAsync(&h, A.hashBuf.p, sizeof h, cudaMemcpyDeviceToHost, st), "D2H");
+    s.sync();
+    return h;
+  }
   static long signature(S& s, long* out, long cap) {
     XAdj& A = get(s);
     long k = 0;
@@ -1372,5 +1716,6 @@ void xadjBackward(Sim<double>& S, const double* gx, const double* gq, const doub
 }
 void xadjInfo(Sim<double>& S, long* out, double* err) { XAdjAccess::info(S, out, err); }
 long xadjSignature(Sim<double>& S, long* out, long cap) { return XAdjAccess::signature(S, out, cap); }
+unsigned long long xadjBranches(Sim<double>& S) { return XAdjAccess::branches(S); }
 
 }  // namespace pdem

@@ -426,8 +426,9 @@ PD void warmMap(const T* in, T* out, const ManC& m) {
 //     vn0[39] vt0[40..43) posImp[43] eN[44] eT[45] mu[46]
 // out: vA[0..3) wA[3..6) vB[6..9) wB[9..12) p[12] lt[13..16)
 constexpr int kPgsIn = 47, kPgsOut = 16;
+// `bits` (optional): the update's branch decisions, one bit each (the replay's branch signature)
 template <class T>
-PD void pgsMap(const T* in, T* out, const ManC& m, double vRest) {
+PD void pgsMap(const T* in, T* out, const ManC& m, double vRest, unsigned* bits = nullptr) {
   const V3<T> vA = ld3(in, 0), wA = ld3(in, 3);
   const T invN(m.invN);
   V3<T> vB{T(0.0), T(0.0), T(0.0)}, wB{T(0.0), T(0.0), T(0.0)};
@@ -456,8 +457,12 @@ PD void pgsMap(const T* in, T* out, const ManC& m, double vRest) {
   if (m.eAvg >= 0.0)
     e = T(m.eAvg);
   const T lenN = sqrt(dot(N, N));
-  if (lenN < T(1e-9))
+  unsigned bb = 0;
+  if (lenN < T(1e-9)) {
+    if (bits)
+      *bits = 1u;
     return;
+  }
   const V3<T> vG = mul(dc, T(0.0));
   T vn = dot(vA, N) + dot(wA, TA) + dot(vB, neg(N)) + dot(wB, TB);
   vn += dot(vG, N);
@@ -477,21 +482,33 @@ PD void pgsMap(const T* in, T* out, const ManC& m, double vRest) {
     e = T(0.0);
   }
   const T wT = wAn + wBn;
-  if (wT <= T(0.0))
+  if (wT <= T(0.0)) {
+    if (bits)
+      *bits = 2u;
     return;
+  }
   const T v0 = sgn * vn0;
-  if (fabs(vn0) < T(vRest) * lenN)
+  if (fabs(vn0) < T(vRest) * lenN) {
     e = T(0.0);
+    bb |= 4u;
+  }
+  if (v0 > T(0.0))
+    bb |= 8u;
+  if (sgn > T(0.0))
+    bb |= 16u;
   const T target = (v0 > T(0.0)) ? -e * v0 : T(0.0);
   const T vt = sgn * vn;
   const T dp = (vt - target) / wT;
   T pNew = pOld + dp;
-  if (pNew < T(0.0))
+  if (pNew < T(0.0)) {
     pNew = T(0.0);
+    bb |= 32u;
+  }
   const T dA = pNew - pOld;
   V3<T> vA2 = vA, wA2 = wA, vB2 = vB, wB2 = wB;
   T pCur = pOld;
   if (dA != T(0.0)) {
+    bb |= 64u;
     pCur = pNew;
     const T lam = -sgn * dA;
     const V3<T> J = mul(N, lam), JA = mul(TA, lam), JB = mul(TB, lam);
@@ -510,6 +527,7 @@ PD void pgsMap(const T* in, T* out, const ManC& m, double vRest) {
     mu = T(m.muAvg);
   const bool haveOld = ltOld.x != T(0.0) || ltOld.y != T(0.0) || ltOld.z != T(0.0);
   if (mu > T(0.0) || haveOld) {
+    bb |= 128u;
     const V3<T> nh = mul(N, T(1.0) / lenN);
     const V3<T> vBf = m.hasB ? vB2 : mul(cv3<T>(m.wv), invN);
     const V3<T> wBf = m.hasB ? wB2 : V3<T>{T(0.0), T(0.0), T(0.0)};
@@ -520,6 +538,7 @@ PD void pgsMap(const T* in, T* out, const ManC& m, double vRest) {
       beta = T(0.0);
     V3<T> err = vtv;
     if (beta != T(0.0)) {
+      bb |= 256u;
       V3<T> w0 = ld3(in, 40);
       w0 = sub(w0, mul(nh, dot(w0, nh)));
       err = add(vtv, mul(w0, beta));
@@ -528,23 +547,31 @@ PD void pgsMap(const T* in, T* out, const ManC& m, double vRest) {
     V3<T> ltNew = ltOld;
     T wTt = imA + imB;
     if (vl > T(1e-9)) {
+      bb |= 512u;
       const V3<T> th = mul(err, T(1.0) / vl);
       const T wAt = (m.sf == 2) ? T(0.0) : imA + genInvMass(cross(rAa, th), iIA, qA);
       const T wBt = (m.sf == 1 || !m.hasB) ? T(0.0) : imB + genInvMass(cross(rBa, th), iIB, qB);
       wTt = wAt + wBt;
-      if (wTt > T(1e-9))
+      if (wTt > T(1e-9)) {
+        bb |= 1024u;
         ltNew = add(ltOld, mul(th, -vl / wTt));
+      }
     }
     ltNew = sub(ltNew, mul(nh, dot(ltNew, nh)));
     T nTot = fmax(pCur, T(0.0)) * lenN;
     if (fabs(vn0) < T(vRest) * lenN)
       nTot += fmax(posImp, T(0.0));
+    if (posImp > T(0.0))
+      bb |= 2048u;
     const T bound = mu * nTot;
     const T ll = sqrt(dot(ltNew, ltNew));
-    if (ll > bound)
+    if (ll > bound) {
+      bb |= 4096u;
       ltNew = (bound > T(0.0)) ? mul(ltNew, bound / ll) : V3<T>{T(0.0), T(0.0), T(0.0)};
+    }
     const V3<T> dd = sub(ltNew, ltOld);
     if (dd.x != T(0.0) || dd.y != T(0.0) || dd.z != T(0.0)) {
+      bb |= 8192u;
       ltCur = ltNew;
       if (applyA) {
         vA2 = add(vA2, mul(dd, imA));
@@ -564,6 +591,8 @@ PD void pgsMap(const T* in, T* out, const ManC& m, double vRest) {
   }
   out[12] = pCur;
   st3(out, 13, ltCur);
+  if (bits)
+    *bits = bb | 16384u;
 }
 
 // ---- one position update of a contact (src/solver_position.hpp:55-99, :266-331) ------------
@@ -576,7 +605,7 @@ struct PosC {
   V3<double> iIA, iIB;
 };
 template <class T>
-PD void posMap(const T* in, T* out, const PosC& c) {
+PD void posMap(const T* in, T* out, const PosC& c, unsigned* bits = nullptr) {
   const V3<T> pA = ld3(in, 0);
   V3<T> pB{T(0.0), T(0.0), T(0.0)};
   Q4<T> qB{T(0.0), T(0.0), T(0.0), T(1.0)};
@@ -601,12 +630,18 @@ PD void posMap(const T* in, T* out, const PosC& c) {
   for (int k = 0; k < 6; ++k)
     out[k] = in[k];
   out[6] = T(0.0);
+  if (bits)
+    *bits = 1u;
   if (C >= T(0.0))
     return;
   const T imA(c.imA), imB(c.imB);
   const T wT = computeW(rA, n, imA, cv3<T>(c.iIA)) + computeW(rB, n, imB, cv3<T>(c.iIB));
+  if (bits)
+    *bits = 2u;
   if (wT < T(1e-6))
     return;
+  if (bits)
+    *bits = 4u;
   const T dl = -C / wT;
   st3(out, 0, add(pA, V3<T>{n.x * dl * imA, n.y * dl * imA, n.z * dl * imA}));
   if (c.hasB)
@@ -1051,6 +1086,250 @@ PD void pgsRev(const double* in, const double* yb, double* xb, const ManC& m, do
   xb[44] += eNb;
   xb[45] += eTb;
   xb[46] += mub;
+}
+
+// ---- hand-written reverses of the approach velocity, the warm start and the position update -----
+// Reverse of vn0Map<double>: xb += J^T yb (inputs and outputs as vn0Map's)
+PD void vn0Rev(const double* in, const double* yb, double* xb, const ManC& m) {
+  const V3d vA = ld3(in, 0), wA = ld3(in, 3);
+  const double invN = m.invN;
+  const V3d vB = m.hasB ? ld3(in, 6) : mul(m.wv, invN);
+  const V3d wB = m.hasB ? ld3(in, 9) : V3d{0.0, 0.0, 0.0};
+  const V3d N = ld3(in, 12), TA = ld3(in, 15), TB = ld3(in, 18);
+  const V3d rAa = mul(ld3(in, 21), invN), rBa = mul(ld3(in, 24), invN);
+  const double vnb = yb[0];
+  const V3d vtb = ld3(yb, 1);
+  V3d vAb = mul(N, vnb), wAb = mul(TA, vnb), vBb = mul(N, -vnb), wBb = mul(TB, vnb);
+  V3d Nb = mul(sub(vA, vB), vnb), TAb = mul(wA, vnb), TBb = mul(wB, vnb), rAab{0, 0, 0}, rBab{0, 0, 0};
+  const double lenN = ::sqrt(dot(N, N));
+  if (lenN > 1e-9) {
+    const V3d nh = mul(N, 1.0 / lenN);
+    const V3d vr = sub(add(vA, cross(wA, rAa)), add(vB, cross(wB, rBa)));
+    V3d vrb{0, 0, 0}, nhb{0, 0, 0};
+    projVjp(vr, nh, vtb, vrb, nhb);
+    acc(vAb, vrb);
+    crossVjp(wA, rAa, vrb, wAb, rAab);
+    const V3d nvrb = mul(vrb, -1.0);
+    acc(vBb, nvrb);
+    crossVjp(wB, rBa, nvrb, wBb, rBab);
+    acc(Nb, mul(nhb, 1.0 / lenN));
+    acc(Nb, mul(N, -dot(nhb, N) / (lenN * lenN * lenN)));
+  }
+  for (int k = 0; k < 3; ++k) {
+    xb[k] += (&vAb.x)[k];
+    xb[3 + k] += (&wAb.x)[k];
+    if (m.hasB) {
+      xb[6 + k] += (&vBb.x)[k];
+      xb[9 + k] += (&wBb.x)[k];
+    }
+    xb[12 + k] += (&Nb.x)[k];
+    xb[15 + k] += (&TAb.x)[k];
+    xb[18 + k] += (&TBb.x)[k];
+    xb[21 + k] += (&rAab.x)[k] * invN;
+    xb[24 + k] += (&rBab.x)[k] * invN;
+  }
+}
+
+// Reverse of warmMap<double> with respect to its non-velocity inputs (the velocities pass through
+// with the identity, which the caller keeps): xb[12..39) += J^T yb
+PD void warmRev(const double* in, const double* yb, double* xb, const ManC& m) {
+  const double p = in[12];
+  const V3d lt0 = ld3(in, 13);
+  const V3d N = ld3(in, 16), TA = ld3(in, 19), TB = ld3(in, 22);
+  const Q4d qA = ld4(in, 31), qB = ld4(in, 35);
+  const double invN = m.invN;
+  const V3d vAb = ld3(yb, 0), wAb = ld3(yb, 3), vBb = ld3(yb, 6), wBb = ld3(yb, 9);
+  const V3d ltOutb = ld3(yb, 12);
+  const bool hasT = lt0.x != 0.0 || lt0.y != 0.0 || lt0.z != 0.0;
+  if (!(p != 0.0 || hasT)) {
+    xb[13] += ltOutb.x, xb[14] += ltOutb.y, xb[15] += ltOutb.z;
+    return;
+  }
+  const V3d rAa = mul(ld3(in, 25), invN), rBa = mul(ld3(in, 28), invN);
+  const V3d dc = m.hasB ? sub(rAa, rBa) : rAa;
+  const double sgn = (dot(N, dc) > 0.0) ? 1.0 : -1.0;
+  const double lam = -sgn * p;
+  const V3d JA = mul(TA, lam), JB = mul(TB, lam);
+  V3d Nb{0, 0, 0}, TAb{0, 0, 0}, TBb{0, 0, 0}, rAab{0, 0, 0}, rBab{0, 0, 0}, lt0b{0, 0, 0};
+  Q4d qAb{0, 0, 0, 0}, qBb{0, 0, 0, 0};
+  double lamb = 0.0;
+  // normal impulse
+  {
+    const V3d Jb = m.hasB ? sub(mul(vAb, m.imA), mul(vBb, m.imB)) : mul(vAb, m.imA);
+    acc(Nb, mul(Jb, lam));
+    lamb += dot(Jb, N);
+    V3d JAb{0, 0, 0};
+    angResponseVjp(qA, JA, m.iIA, wAb, qAb, JAb);
+    acc(TAb, mul(JAb, lam));
+    lamb += dot(JAb, TA);
+    if (m.hasB) {
+      V3d JBb{0, 0, 0};
+      angResponseVjp(qB, JB, m.iIB, wBb, qBb, JBb);
+      acc(TBb, mul(JBb, lam));
+      lamb += dot(JBb, TB);
+    }
+  }
+  if (hasT) {
+    const double l2 = ::sqrt(dot(N, N));
+    V3d lt1 = lt0, nh{0, 0, 0};
+    if (l2 > 1e-9) {
+      nh = mul(N, 1.0 / l2);
+      lt1 = sub(lt0, mul(nh, dot(lt0, nh)));
+    }
+    V3d lt1b = ltOutb;
+    acc(lt1b, mul(vAb, m.imA));
+    {
+      const V3d c = cross(rAa, lt1);
+      V3d cb{0, 0, 0};
+      angResponseVjp(qA, c, m.iIA, wAb, qAb, cb);
+      crossVjp(rAa, lt1, cb, rAab, lt1b);
+    }
+    if (m.hasB) {
+      acc(lt1b, mul(vBb, -m.imB));
+      const V3d nd = mul(lt1, -1.0);
+      const V3d c = cross(rBa, nd);
+      V3d cb{0, 0, 0}, ndb{0, 0, 0};
+      angResponseVjp(qB, c, m.iIB, wBb, qBb, cb);
+      crossVjp(rBa, nd, cb, rBab, ndb);
+      acc(lt1b, mul(ndb, -1.0));
+    }
+    if (l2 > 1e-9) {
+      V3d nhb{0, 0, 0};
+      projVjp(lt0, nh, lt1b, lt0b, nhb);
+      acc(Nb, mul(nhb, 1.0 / l2));
+      acc(Nb, mul(N, -dot(nhb, N) / (l2 * l2 * l2)));
+    } else {
+      acc(lt0b, lt1b);
+    }
+  } else {
+    acc(lt0b, ltOutb);
+  }
+  xb[12] += -sgn * lamb;
+  for (int k = 0; k < 3; ++k) {
+    xb[13 + k] += (&lt0b.x)[k];
+    xb[16 + k] += (&Nb.x)[k];
+    xb[19 + k] += (&TAb.x)[k];
+    xb[22 + k] += (&TBb.x)[k];
+    xb[25 + k] += (&rAab.x)[k] * invN;
+    xb[28 + k] += (&rBab.x)[k] * invN;
+  }
+  xb[31] += qAb.x, xb[32] += qAb.y, xb[33] += qAb.z, xb[34] += qAb.w;
+  xb[35] += qBb.x, xb[36] += qBb.y, xb[37] += qBb.z, xb[38] += qBb.w;
+}
+
+// y = qmul(a, b): abar, bbar += (the transposed product)
+PD void qmulVjp(Q4d a, Q4d b, Q4d y, Q4d& ab, Q4d& bb) {
+  ab.x += y.x * b.w - y.y * b.z + y.z * b.y - y.w * b.x;
+  ab.y += y.x * b.z + y.y * b.w - y.z * b.x - y.w * b.y;
+  ab.z += -y.x * b.y + y.y * b.x + y.z * b.w - y.w * b.z;
+  ab.w += y.x * b.x + y.y * b.y + y.z * b.z + y.w * b.w;
+  bb.x += y.x * a.w + y.y * a.z - y.z * a.y - y.w * a.x;
+  bb.y += -y.x * a.z + y.y * a.w + y.z * a.x - y.w * a.y;
+  bb.z += y.x * a.y - y.y * a.x + y.z * a.w - y.w * a.z;
+  bb.w += y.x * a.x + y.y * a.y + y.z * a.z + y.w * a.w;
+}
+// W = im + sum_k (r x d)_k^2 iI_k:  rbar, dbar += ...
+PD void computeWVjp(V3d r, V3d d, V3d iI, double Wb, V3d& rb, V3d& db) {
+  const V3d rn = cross(r, d);
+  crossVjp(r, d, V3d{2.0 * rn.x * iI.x * Wb, 2.0 * rn.y * iI.y * Wb, 2.0 * rn.z * iI.z * Wb}, rb, db);
+}
+
+// Reverse of posMap<double>: xb += J^T yb
+PD void posRev(const double* in, const double* yb, double* xb, const PosC& c) {
+  const V3d pA = ld3(in, 0);
+  const V3d pB = c.hasB ? ld3(in, 3) : V3d{0.0, 0.0, 0.0};
+  const Q4d qPA = ld4(in, 6), qA0 = ld4(in, 14);
+  const Q4d qPB = c.hasB ? ld4(in, 10) : Q4d{0.0, 0.0, 0.0, 1.0};
+  const V3d nc = ld3(in, 22), rAc = ld3(in, 25), rBc = ld3(in, 28);
+  const Q4d qAd = qmul(qPA, qinv(qA0));
+  const V3d rA = rot(qAd, rAc);
+  V3d rB = rBc, n = nc;
+  Q4d qBd{0.0, 0.0, 0.0, 1.0};
+  if (c.hasB) {
+    qBd = qmul(qPB, qinv(ld4(in, 18)));
+    rB = rot(qBd, rBc);
+    n = rot(qBd, nc);
+  }
+  const V3d d = c.hasB ? sub(add(pA, rA), add(pB, rB)) : sub(add(pA, rA), rBc);
+  const double C = dot(d, n);
+  // the positions pass through (identity); dl and the updates only on the active branch
+  xb[0] += yb[0], xb[1] += yb[1], xb[2] += yb[2];
+  if (c.hasB)
+    xb[3] += yb[3], xb[4] += yb[4], xb[5] += yb[5];
+  if (C >= 0.0)
+    return;
+  const double wT = computeW(rA, n, c.imA, c.iIA) + computeW(rB, n, c.imB, c.iIB);
+  if (wT < 1e-6)
+    return;
+  const double dl = -C / wT;
+  const V3d pAb = ld3(yb, 0), pBb = c.hasB ? ld3(yb, 3) : V3d{0.0, 0.0, 0.0};
+  double dlb = yb[6] + dot(pAb, n) * c.imA;
+  V3d nb = mul(pAb, dl * c.imA);
+  if (c.hasB) {
+    dlb -= dot(pBb, n) * c.imB;
+    acc(nb, mul(pBb, -dl * c.imB));
+  }
+  const double Cb = -dlb / wT;
+  const double wTb = dlb * C / (wT * wT);
+  V3d rAb{0, 0, 0}, rBb{0, 0, 0};
+  computeWVjp(rA, n, c.iIA, wTb, rAb, nb);
+  computeWVjp(rB, n, c.iIB, wTb, rBb, nb);
+  // C = d . n
+  acc(nb, mul(d, Cb));
+  const V3d dn = mul(n, Cb);
+  xb[0] += dn.x, xb[1] += dn.y, xb[2] += dn.z;
+  acc(rAb, dn);
+  V3d rBcb{0, 0, 0}, ncb{0, 0, 0};
+  if (c.hasB) {
+    xb[3] -= dn.x, xb[4] -= dn.y, xb[5] -= dn.z;
+    acc(rBb, mul(dn, -1.0));
+    Q4d qBdb{0, 0, 0, 0};
+    rotVjp(qBd, nc, nb, qBdb, ncb);
+    rotVjp(qBd, rBc, rBb, qBdb, rBcb);
+    Q4d qPBb{0, 0, 0, 0}, qiBb{0, 0, 0, 0};
+    const Q4d qB0 = ld4(in, 18);
+    qmulVjp(qPB, qinv(qB0), qBdb, qPBb, qiBb);
+    xb[10] += qPBb.x, xb[11] += qPBb.y, xb[12] += qPBb.z, xb[13] += qPBb.w;
+    xb[18] -= qiBb.x, xb[19] -= qiBb.y, xb[20] -= qiBb.z, xb[21] += qiBb.w;
+  } else {
+    acc(rBcb, mul(dn, -1.0));
+    acc(ncb, nb);
+  }
+  Q4d qAdb{0, 0, 0, 0};
+  V3d rAcb{0, 0, 0};
+  rotVjp(qAd, rAc, rAb, qAdb, rAcb);
+  Q4d qPAb{0, 0, 0, 0}, qiAb{0, 0, 0, 0};
+  qmulVjp(qPA, qinv(qA0), qAdb, qPAb, qiAb);
+  xb[6] += qPAb.x, xb[7] += qPAb.y, xb[8] += qPAb.z, xb[9] += qPAb.w;
+  xb[14] -= qiAb.x, xb[15] -= qiAb.y, xb[16] -= qiAb.z, xb[17] += qiAb.w;
+  xb[22] += ncb.x, xb[23] += ncb.y, xb[24] += ncb.z;
+  xb[25] += rAcb.x, xb[26] += rAcb.y, xb[27] += rAcb.z;
+  xb[28] += rBcb.x, xb[29] += rBcb.y, xb[30] += rBcb.z;
+}
+
+// ---- one chunk of a vector-Jacobian product -------------------------------------------------
+// part[l] = sum_o ybar[o] d out[o] / d in[chunk kLanes + l]: the threads of a group each take one
+// chunk of the inputs, so the chunks of one entry run side by side
+constexpr int kGroup = 8;  // 8 chunks of kLanes cover up to 56 inputs
+template <int NI, int NO, class F>
+__device__ __forceinline__ void vjpChunk(const double* in, const double* ybar, double* part, int chunk, F f) {
+  using D = Dd<kLanes>;
+  const int c0 = chunk * kLanes;
+  D x[NI];
+  D y[NO];
+  for (int i = 0; i < NI; ++i) {
+    x[i] = D(in[i]);
+    const int l = i - c0;
+    if (l >= 0 && l < kLanes)
+      x[i].d[l] = 1.0;
+  }
+  f(x, y);
+  for (int l = 0; l < kLanes; ++l) {
+    double s = 0.0;
+    for (int o = 0; o < NO; ++o)
+      s += ybar[o] * y[o].d[l];
+    part[l] = s;
+  }
 }
 
 // ---- vector-Jacobian product of a local map by forward-mode chunks ------------------------

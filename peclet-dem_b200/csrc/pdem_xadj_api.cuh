@@ -27,6 +27,13 @@ void xadjInfo(Sim<double>& S, long* out, double* err);
 // colourings, main / stabilization / position sweeps; returns the number of substeps
 long xadjSignature(Sim<double>& S, long* out, long cap);
 
+// the branch signature of the record: a hash of every sweep update's branch decisions (impulse
+// clamps, restitution cut-off, friction cone, active position contacts) over a replay
+unsigned long long xadjBranches(Sim<double>& S);
+template <class SIM>
+unsigned long long xadjBranches(SIM&) {
+  throw std::invalid_argument("the XPBD adjoint runs on the FP64 plain path (precision fp64)");
+}
 template <class SIM>
 long xadjSignature(SIM&, long*, long) {
   throw std::invalid_argument("the XPBD adjoint runs on the FP64 plain path (precision fp64)");

@@ -77,6 +77,15 @@ class XpbdRollout:
         self.sim._f["xa_signature"](self.sim._h, out.ctypes.data_as(C.POINTER(C.c_long)), out.size)
         return out[: 7 * n].reshape(n, 7)
 
+    def branches(self):
+        """Hash of the branch decisions of every sweep update of the last rollout (impulse clamps,
+        restitution cut-off, friction cone, active position contacts), from a replay of its record.
+        Equal `signature()` and equal `branches()` mean two rollouts ran the same smooth piece of the
+        step, so their central difference certifies the gradient."""
+        h = C.c_ulonglong(0)
+        self._check(self.sim._f["xa_branches"](self.sim._h, C.byref(h)), "xa_branches")
+        return int(h.value)
+
     def rollout(self, x0, q0, v0, w0, theta, substeps: int, dt: float = 0.0):
         """End state (x, q, v, w) after `substeps` substeps of length dt (0: the simulation's)."""
         if substeps < 1:

@@ -123,3 +123,19 @@ def test_hand_reverse_equals_dual_jacobians(gpu_api, monkeypatch):
     np.testing.assert_allclose(t0, t1, rtol=1e-10)
     for a, b in zip(g0, g1):
         np.testing.assert_allclose(a, b, rtol=1e-9, atol=1e-12 * np.abs(b).max())
+
+
+def test_branch_signature_certifies_differences(gpu_api):
+    """The record's branch hash is a function of the rollout's branches: the same rollout twice gives
+    the same hash; a large change of friction changes it (the cone clamps move)."""
+    from peclet.dem.xpbd_adjoint import XpbdRollout
+    sc = _impacts()
+    sim = P.build(gpu_api, sc, None, "fp64")
+    roll = XpbdRollout(sim)
+    start = [torch.tensor(a, dtype=torch.float64, device="cuda") for a in _start(sc)]
+    hashes = []
+    for mu in (0.4, 0.4, 0.05):
+        roll(*start, torch.tensor([0.7, 0.2, mu], dtype=torch.float64), 10)
+        hashes.append((roll.signature(), roll.branches()))
+    assert np.array_equal(hashes[0][0], hashes[1][0]) and hashes[0][1] == hashes[1][1]
+    assert hashes[0][1] != hashes[2][1]
