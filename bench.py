@@ -662,11 +662,9 @@ def run_xpbd_adjoint(args, rank, world, dist, dem, W):
     configuration, FP64, from its saved restart): `--xadj-substeps` substeps recorded, then the
     backward of L = sum(a . x_end) + sum(b . v_end) with seeded weights. Reports the plain forward,
     the recording forward and the backward (device time on the library's stream, max over ranks;
-    each rank runs its own replica), the cost ratio (recording forward + backward) / plain
-    forward, and the gradients' relative error against central differences (relative step 1e-5;
-    eN, mu and a direction of the start velocities), each marked certified when the +h and -h
-    rollouts took the nominal one's contact sets, colourings and adaptive stops (equal
-    signatures). The dual-number check of the same gradients runs in the GPU tests."""
+    each rank runs its own replica) and the cost ratio (recording forward + backward) / plain
+    forward; the finite-difference check runs on a calibration box (xpbd_fd_check). The
+    dual-number check of the gradients, on this bed too, runs in the GPU tests."""
     import ctypes
     import torch
     from peclet.dem.xpbd_adjoint import XpbdRollout
@@ -711,40 +709,7 @@ def run_xpbd_adjoint(args, rank, world, dist, dem, W):
     t_bwd = timed(lambda: roll._check(f["xa_backward"](h, P(A), P(z[4]), P(Bv), P(z[3]), *[P(t) for t in d], dth),
                                       "xa_backward"))
     info = roll.info()
-    # central differences on a window of `win` substeps: over many substeps of a settled bed the
-    # adaptive stops (sweep counts) flip with any perturbation, and a flipped stop is a jump of the
-    # loss that no derivative sees; the window's differences are certified when they do not flip
-    win = min(T, args.xadj_fd_substeps)
-    begin(theta0)
-    roll._check(f["xa_step"](h, sc.dt, win), "xa_step")
-    sigw = (roll.signature(), roll.branches())
-    torch.cuda.synchronize()
-    roll._check(f["xa_backward"](h, P(A), P(z[4]), P(Bv), P(z[3]), *[P(t) for t in d], dth), "xa_backward")
-    grads = {"eN": dth[0], "mu": dth[2]}
-    rel = lambda a, b: abs(a - b) / abs(b) if b else None
-    fd, cert = {}, {}
-
-    def lossw(th, v=None):
-        begin(th, v)
-        roll._check(f["xa_step"](h, sc.dt, win), "xa_step")
-        x, v1 = sim.get_positions(), sim.get_velocities()
-        return float((A.cpu().numpy() * x).sum() + (Bv.cpu().numpy() * v1).sum()), (roll.signature(), roll.branches())
-
-    same = lambda a, b: bool(np.array_equal(a[0], b[0]) and a[1] == b[1])
-    for name, k in (("eN", 0), ("mu", 2)):
-        hh = 1e-5 * theta0[k]
-        tp, tm = theta0.copy(), theta0.copy()
-        tp[k] += hh
-        tm[k] -= hh
-        (lp, sp), (lm, sm) = lossw(tp), lossw(tm)
-        fd[name] = (lp - lm) / (2 * hh)
-        cert[name] = same(sp, sigw) and same(sm, sigw)
-    dv = torch.tensor(np.random.default_rng(8).normal(size=(sc.n, 3)), device=dev)
-    hv = 1e-5 * 0.05
-    (lp, sp), (lm, sm) = lossw(theta0, start[2] + hv * dv), lossw(theta0, start[2] - hv * dv)
-    fd["v0"] = (lp - lm) / (2 * hv)
-    cert["v0"] = same(sp, sigw) and same(sm, sigw)
-    grads["v0"] = float((d[2] * dv).sum())
+    fd_check = xpbd_fd_check(args, dem, W)
     rate = lambda t: sc.n * T / t
     return {"workload": f"plain_settling_4096 restart (step {W.PLAIN_SETTLED_STEPS}), {T} substeps",
             "path": "plain FP64 XPBD step (coloured PGS, one-sided stabilization, position GS), recorded; "
@@ -753,10 +718,82 @@ def run_xpbd_adjoint(args, rank, world, dist, dem, W):
             "cost_ratio": (t_rec + t_bwd) / t_plain, "backward_ms_per_substep": 1e3 * t_bwd / T,
             "forward_ms_per_substep": 1e3 * t_plain / T, "record_mb": info["record_bytes"] / 1e6,
             "work_mb": info["work_bytes"] / 1e6, "replay_dx_scale_units": info["replay_dx"],
-            "fd_window_substeps": win, "grad": grads, "fd_1e-5": fd,
-            "rel_err_vs_fd": {k: rel(grads[k], fd[k]) for k in fd},
-            "fd_certified": cert, "mean_sweeps": {k: float(v) for k, v in zip(
+            "fd_check": fd_check, "mean_sweeps": {k: float(v) for k, v in zip(
                 ("velocity", "stabilization", "position"), sig0[:, 4:7].mean(axis=0))}}
+
+
+def xpbd_fd_check(args, dem, W):
+    """Central differences (relative step 1e-5, FP64) of L = sum(a . x_end) + sum(b . v_end) along
+    eN, mu and a direction of the start velocities, against the adjoint, on the first box of the
+    calibration workload (2048 spheres, the plain XPBD step at dt 2e-5) after `--xadj-fd-presettle`
+    substeps (the collisional regime, about 200 contacts). A difference is certified when the +h
+    and -h rollouts took the nominal one's discrete decisions (record signature) and branches
+    (branch hash): the longest of the windows 16, 8, 4, 2 substeps that certifies all three is
+    reported (a contact onset, a flipped clamp or adaptive stop is a jump the derivative does not
+    see). On a settled bed no window certifies: contacts sit at the restitution cut-off and the
+    impulse clamps, and any perturbation flips some; the dual-number check of the tests covers it."""
+    import ctypes
+    import torch
+    from peclet.dem.xpbd_adjoint import XpbdRollout
+    sc = W.calibration_box_scene(0)
+    sim = sc.apply(dem.Simulation(sc.n + 8, "fp64"))
+    for _ in range(args.xadj_fd_presettle):
+        sim.step(sc.dt)
+    roll = XpbdRollout(sim)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    state = (sim.get_positions(), sim.get_quaternions(), sim.get_velocities(), sim.get_angular_velocities())
+    start = [torch.tensor(np.asarray(a, np.float64), device=dev) for a in state]
+    th0 = np.array(sc.material, np.float64)
+    rng = np.random.default_rng(7)
+    A = torch.tensor(rng.normal(size=(sc.n, 3)), device=dev)
+    Bv = torch.tensor(rng.normal(size=(sc.n, 3)) * 1e-3, device=dev)
+    dv = torch.tensor(np.random.default_rng(8).normal(size=(sc.n, 3)), device=dev)
+    f, h = sim._f, sim._h
+    P = lambda t: ctypes.c_void_p(t.data_ptr())
+
+    def run(th, nsub, v=None):
+        sim.set_material_params(*[float(x) for x in th])
+        rows = [start[0], start[1], start[2] if v is None else v, start[3]]
+        torch.cuda.synchronize()
+        roll._check(f["xa_begin"](h, *[P(t) for t in rows], sc.n), "xa_begin")
+        roll._check(f["xa_step"](h, sc.dt, nsub), "xa_step")
+        x, v1 = sim.get_positions(), sim.get_velocities()
+        L = float((A.cpu().numpy() * x).sum() + (Bv.cpu().numpy() * v1).sum())
+        return L, (roll.signature(), roll.branches())
+
+    same = lambda a, b: bool(np.array_equal(a[0], b[0]) and a[1] == b[1])
+    rel = lambda a, b: abs(a - b) / abs(b) if b else None
+    tried = []
+    for win in (16, 8, 4, 2):
+        _, sig = run(th0, win)
+        d = [torch.empty((sc.n, c), dtype=torch.float64, device=dev) for c in (3, 4, 3, 3)]
+        z = {c: torch.zeros((sc.n, c), dtype=torch.float64, device=dev) for c in (3, 4)}
+        dth = (ctypes.c_double * 3)()
+        torch.cuda.synchronize()
+        roll._check(f["xa_backward"](h, P(A), P(z[4]), P(Bv), P(z[3]), *[P(t) for t in d], dth), "xa_backward")
+        grads = {"eN": dth[0], "mu": dth[2], "v0": float((d[2] * dv).sum())}
+        fd, cert = {}, {}
+        for name, k in (("eN", 0), ("mu", 2)):
+            hh = 1e-5 * th0[k]
+            tp, tm = th0.copy(), th0.copy()
+            tp[k] += hh
+            tm[k] -= hh
+            (lp, sp), (lm, sm) = run(tp, win), run(tm, win)
+            fd[name] = (lp - lm) / (2 * hh)
+            cert[name] = same(sp, sig) and same(sm, sig)
+        hv = 1e-5 * 0.2
+        (lp, sp), (lm, sm) = run(th0, win, start[2] + hv * dv), run(th0, win, start[2] - hv * dv)
+        fd["v0"] = (lp - lm) / (2 * hv)
+        cert["v0"] = same(sp, sig) and same(sm, sig)
+        out = {"window_substeps": win, "grad": grads, "fd_1e-5": fd,
+               "rel_err_vs_fd": {k: rel(grads[k], fd[k]) for k in fd}, "certified": cert}
+        tried.append(win)
+        if all(cert.values()):
+            break
+    out["workload"] = (f"calibration box 0 (2048 spheres, plain XPBD, dt 2e-5, (eN, eT, mu) = (0.6, 0, 0.3)) after "
+                       f"{args.xadj_fd_presettle} substeps")
+    out["windows_tried"] = tried
+    return out
 
 
 def run_hertz(args, rank, world, dist, dem, W):
@@ -885,9 +922,12 @@ def run_ours(args):
                                                     if v is not None))
         if "xpbd_adjoint" in detail:
             xa = detail["xpbd_adjoint"]
+            fc = xa["fd_check"]
+            errs = [v for v in fc["rel_err_vs_fd"].values() if v is not None]
             flat.update(xpbd_fwd_adjoint_cost_ratio=xa["cost_ratio"], xpbd_fwd_adjoint_value=xa["fwd_adjoint"],
-                        xpbd_grad_rel_err_vs_fd=max(v for v in xa["rel_err_vs_fd"].values() if v is not None),
-                        xpbd_grad_fd_certified=all(xa["fd_certified"].values()))
+                        xpbd_grad_rel_err_vs_fd=max(errs) if errs else None,
+                        xpbd_grad_fd_certified=all(fc["certified"].values()),
+                        xpbd_grad_fd_window=fc["window_substeps"])
         if "hertz" in detail:
             flat.update(hertz262k_fp64_value=detail["hertz"]["fp64"]["value"],
                         hertz262k_fp32_value=detail["hertz"]["fp32"]["value"])
@@ -912,12 +952,18 @@ def run_ours(args):
                                                        "traffic", "peak_source")},
             "cpu_baseline": h["cpu"], "clocks": h["clocks"],
             "sweeps_per_substep": {k: round(v, 2) for k, v in h["sweeps_per_substep"].items()},
-            "device_allocations_timed": h["timed_allocs"], **{k: (round(v, 6) if isinstance(v, float) else v)
-                                                             for k, v in flat.items()}}
+            "device_allocations_timed": h["timed_allocs"], **{k: _compact(v) for k, v in flat.items()}}
         print(json.dumps(line))
     if dist is not None:
         dist.destroy_process_group()
     return 0
+
+
+def _compact(v):
+    """Six decimals for ordinary figures, three significant digits for small ones (errors)."""
+    if not isinstance(v, float):
+        return v
+    return round(v, 6) if v == 0.0 or abs(v) >= 1e-3 else float(f"{v:.3g}")
 
 
 def spawn_ranks(args):
@@ -948,7 +994,7 @@ def main():
     ap.add_argument("--calib-scenes", type=int, default=64)
     ap.add_argument("--calib-substeps", type=int, default=2000)
     ap.add_argument("--xadj-substeps", type=int, default=100, help="substeps of the XPBD adjoint line")
-    ap.add_argument("--xadj-fd-substeps", type=int, default=10, help="window of its finite-difference check")
+    ap.add_argument("--xadj-fd-presettle", type=int, default=200, help="substeps before its finite-difference check")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)

@@ -370,6 +370,22 @@ def calibration_boxes(seed=5, scenes=64, per_scene=2048, radius=1e-3, box=(40e-3
                 I=0.4 * m * r * r, first=np.arange(scenes + 1) * per_scene, planes=planes)
 
 
+def calibration_box_scene(index=0, material=(0.6, 0.0, 0.3), dt=2e-5, **kw):
+    """Box `index` of `calibration_boxes` (2048 spheres on a jittered lattice, velocities uniform in
+    +-0.2 m/s) as a Scene for the plain XPBD step: six planes, gravity, the given material
+    (e_n, e_t, mu), substep dt, iterations (10, 10)."""
+    c = calibration_boxes(**kw)
+    lo, hi = c["first"][index], c["first"][index + 1]
+    r = float(c["r"][lo])
+    im, iI = 1.0 / c["m"][lo:hi], 1.0 / c["I"][lo:hi]
+    pl = [tuple(p) for p in c["planes"]]
+    box = (pl[1][0], pl[3][1], pl[5][2])
+    return Scene(name=f"calibration_box_{index}", pos=c["x0"][lo:hi].copy(), vel=c["v0"][lo:hi].copy(),
+                 inv_mass=im, inv_inertia=np.repeat(iI[:, None], 3, axis=1), angvel=c["w0"][lo:hi].copy(),
+                 global_scale=r, domain=((0.0, 0.0, 0.0), box, (False, False, False)), planes=pl,
+                 material=tuple(material), iterations=(10, 10), dt=dt)
+
+
 def hollow_cylinder_shell(n=512, seed=3, r_out=1.0, r_in=0.6, length=3.0):
     """Seeded stratified point shell of a hollow cylinder (body axis y, canonical units), for
     `set_shell_points`: points on the outer and inner lateral surfaces and the two annular caps,
