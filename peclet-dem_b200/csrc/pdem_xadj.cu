@@ -1201,11 +1201,23 @@ struct XAdj {
   bool open = false;
   int n = 0;
   double dt = 0;
-  // workspace
-  DBuf<D4> body, cont, man, alLB, tv, tp;
-  DBuf<double> cdbl, mdbl, ldbl, small;
-  DBuf<int> mint;
+  // workspace: two sets of replay buffers (the replay of a substep runs beside the reverse of the
+  // next one, on the side stream) and one set of adjoint buffers
+  DBuf<D4> rbody[2], rcont[2], rman[2], tv[2], tp[2];
+  DBuf<double> rcdbl[2], rmdbl[2];
+  DBuf<int> rmint[2];
+  DBuf<D4> abody, acont, aman, alLB;
+  DBuf<double> acdbl, amdbl, ldbl, small;
   DBuf<u64> hashBuf;
+  cudaStream_t side = nullptr;
+  cudaEvent_t evStart = nullptr, evRep[2] = {nullptr, nullptr}, evRev[2] = {nullptr, nullptr};
+  ~XAdj() {
+    for (cudaEvent_t e : {evStart, evRep[0], evRep[1], evRev[0], evRev[1]})
+      if (e)
+        cudaEventDestroy(e);
+    if (side)
+      cudaStreamDestroy(side);
+  }
   double err[2] = {0, 0};
   size_t workBytes = 0;
   // PDEM_XADJ_DUAL=1: the PGS, warm-start, approach-velocity and position updates reversed through
@@ -1439,7 +1451,9 @@ struct XAdjAccess {
   }
 
   // carve the workspace for the largest substep of the record
-  static XWork work(S& s, XAdj& A) {
+  // carve the workspace for the largest substep of the record: W[0] and W[1] have their own replay
+  // buffers and share the adjoint ones
+  static void work(S& s, XAdj& A, XWork* W) {
     int n = std::max(A.n, 1), nc = 1, nm = 1, L = 1, sv = 1, sp = 1;
     for (auto& r : A.recs) {
       nc = std::max(nc, r->nc);
@@ -1450,46 +1464,60 @@ struct XAdjAccess {
     }
     A.maxSweeps = std::max(sv, sp);
     cudaStream_t st = s.stream_;
-    A.body.ensure(22 * (size_t)n, false, st);
-    A.cont.ensure(6 * (size_t)nc, false, st);
-    A.man.ensure(21 * (size_t)nm, false, st);
+    size_t bytes = 0;
+    for (int k = 0; k < 2; ++k) {
+      A.rbody[k].ensure(9 * (size_t)n, false, st);
+      A.rcont[k].ensure(3 * (size_t)nc, false, st);
+      A.rman[k].ensure(8 * (size_t)nm, false, st);
+      A.tv[k].ensure(4 * (size_t)sv * nm, false, st);
+      A.tp[k].ensure(2 * (size_t)sp * nc, false, st);
+      A.rcdbl[k].ensure((size_t)nc, false, st);
+      A.rmdbl[k].ensure((size_t)nm, false, st);
+      A.rmint[k].ensure(2 * (size_t)nm, false, st);
+      bytes += (A.rbody[k].n + A.rcont[k].n + A.rman[k].n + A.tv[k].n + A.tp[k].n) * sizeof(D4) +
+               (A.rcdbl[k].n + A.rmdbl[k].n) * sizeof(double) + A.rmint[k].n * sizeof(int);
+    }
+    A.abody.ensure(13 * (size_t)n, false, st);
+    A.acont.ensure(3 * (size_t)nc, false, st);
+    A.aman.ensure(10 * (size_t)nm, false, st);
     A.alLB.ensure((size_t)L, false, st);
-    A.tv.ensure(4 * (size_t)sv * nm, false, st);
-    A.tp.ensure(2 * (size_t)sp * nc, false, st);
-    A.cdbl.ensure(2 * (size_t)nc, false, st);
-    A.mdbl.ensure(4 * (size_t)nm, false, st);
+    A.acdbl.ensure((size_t)nc, false, st);
+    A.amdbl.ensure(3 * (size_t)nm, false, st);
     A.ldbl.ensure((size_t)L, false, st);
     A.small.ensure(8, false, st);
-    A.mint.ensure(2 * (size_t)nm, false, st);
-    A.workBytes = (A.body.n + A.cont.n + A.man.n + A.alLB.n + A.tv.n + A.tp.n) * sizeof(D4) +
-                  (A.cdbl.n + A.mdbl.n + A.ldbl.n + A.small.n) * sizeof(double) + A.mint.n * sizeof(int);
-    XWork w;
-    D4* b = A.body.p;
-    w.vP0 = b, w.wP0 = b + n, w.xP0 = b + 2 * n, w.vP = b + 3 * n, w.wP = b + 4 * n, w.vF = b + 5 * n,
-    w.wF = b + 6 * n, w.xP = b + 7 * n, w.qP = b + 8 * n;
-    w.gx = b + 9 * n, w.gq = b + 10 * n, w.gv = b + 11 * n, w.gw = b + 12 * n;
-    w.ax = b + 13 * n, w.aq = b + 14 * n, w.av = b + 15 * n, w.aw = b + 16 * n;
-    w.axP = b + 17 * n, w.aqP = b + 18 * n, w.avP = b + 19 * n, w.awP = b + 20 * n, w.axP0 = b + 21 * n;
-    D4* c = A.cont.p;
-    w.cgN = c, w.cgA = c + nc, w.cgB = c + 2 * nc, w.acgN = c + 3 * nc, w.acgA = c + 4 * nc, w.acgB = c + 5 * nc;
-    w.posLam = A.cdbl.p, w.aposLam = A.cdbl.p + nc;
-    D4* m = A.man.p;
-    w.geo = m, w.ageo = m + 5 * (size_t)nm;
-    w.lam0 = m + 10 * (size_t)nm, w.lam = m + 11 * (size_t)nm, w.vn = m + 12 * (size_t)nm;
-    w.alam = m + 13 * (size_t)nm, w.avn = m + 14 * (size_t)nm, w.ath = m + 15 * (size_t)nm;
-    w.alamOut = m + 16 * (size_t)nm, w.alamPrev = m + 17 * (size_t)nm;
-    w.np = A.mint.p, w.src = A.mint.p + nm;
-    w.posIn = A.mdbl.p, w.aposIn = A.mdbl.p + nm, w.aposOut = A.mdbl.p + 2 * nm, w.aposPrev = A.mdbl.p + 3 * nm;
-    w.alL = A.alLB.p, w.apL = A.ldbl.p;
-    w.tv = A.tv.p, w.tp = A.tp.p;
-    w.theta = A.small.p, w.err = A.small.p + 4;
-    w.hash = nullptr;
-    return w;
+    A.workBytes = bytes + (A.abody.n + A.acont.n + A.aman.n + A.alLB.n) * sizeof(D4) +
+                  (A.acdbl.n + A.amdbl.n + A.ldbl.n + A.small.n) * sizeof(double);
+    for (int k = 0; k < 2; ++k) {
+      XWork& w = W[k];
+      D4* b = A.rbody[k].p;
+      w.vP0 = b, w.wP0 = b + n, w.xP0 = b + 2 * n, w.vP = b + 3 * n, w.wP = b + 4 * n, w.vF = b + 5 * n,
+      w.wF = b + 6 * n, w.xP = b + 7 * n, w.qP = b + 8 * n;
+      D4* a = A.abody.p;
+      w.gx = a, w.gq = a + n, w.gv = a + 2 * n, w.gw = a + 3 * n;
+      w.ax = a + 4 * n, w.aq = a + 5 * n, w.av = a + 6 * n, w.aw = a + 7 * n;
+      w.axP = a + 8 * n, w.aqP = a + 9 * n, w.avP = a + 10 * n, w.awP = a + 11 * n, w.axP0 = a + 12 * n;
+      D4* c = A.rcont[k].p;
+      w.cgN = c, w.cgA = c + nc, w.cgB = c + 2 * nc;
+      D4* ac = A.acont.p;
+      w.acgN = ac, w.acgA = ac + nc, w.acgB = ac + 2 * nc;
+      w.posLam = A.rcdbl[k].p, w.aposLam = A.acdbl.p;
+      D4* m = A.rman[k].p;
+      w.geo = m, w.lam0 = m + 5 * (size_t)nm, w.lam = m + 6 * (size_t)nm, w.vn = m + 7 * (size_t)nm;
+      D4* am = A.aman.p;
+      w.ageo = am, w.alam = am + 5 * (size_t)nm, w.avn = am + 6 * (size_t)nm, w.ath = am + 7 * (size_t)nm;
+      w.alamOut = am + 8 * (size_t)nm, w.alamPrev = am + 9 * (size_t)nm;
+      w.np = A.rmint[k].p, w.src = A.rmint[k].p + nm;
+      w.posIn = A.rmdbl[k].p;
+      w.aposIn = A.amdbl.p, w.aposOut = A.amdbl.p + nm, w.aposPrev = A.amdbl.p + 2 * nm;
+      w.alL = A.alLB.p, w.apL = A.ldbl.p;
+      w.tv = A.tv[k].p, w.tp = A.tp[k].p;
+      w.theta = A.small.p, w.err = A.small.p + 4;
+      w.hash = nullptr;
+    }
   }
 
-  static void replay(S& s, const XScene& sc, const XRec& R, const XView& r, const XWork& w, const XRec* next,
-                     int tag) {
-    cudaStream_t st = s.stream_;
+  static void replay(cudaStream_t st, const XScene& sc, const XRec& R, const XView& r, const XWork& w,
+                     const XRec* next, int tag) {
     const int n = sc.n;
     const int gn = gridFor(n), gc = gridFor(std::max(R.nc, 1)), gm = gridFor(std::max(R.nm, 1));
     const double gMag = std::sqrt(sc.g.x * sc.g.x + sc.g.y * sc.g.y + sc.g.z * sc.g.z);
@@ -1594,23 +1622,49 @@ struct XAdjAccess {
       deviceRows({gx, gq, gv, gw, dx, dq, dv, dw});
     cudaStream_t st = s.stream_;
     const XScene sc = scene(s, A);
-    XWork w = work(s, A);
+    XWork W[2];
+    work(s, A, W);
+    if (!A.side) {
+      cudaCheck(cudaStreamCreateWithFlags(&A.side, cudaStreamNonBlocking), "xadj stream");
+      for (cudaEvent_t* e : {&A.evStart, &A.evRep[0], &A.evRep[1], &A.evRev[0], &A.evRev[1]})
+        cudaCheck(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "xadj event");
+    }
+    cudaStream_t sb = A.side;
+    XWork& w0 = W[0];
     const int n = A.n;
     if (n > 0) {
-      kxPack<<<gridFor(n), kB, 0, st>>>(n, gx, 3, w.gx);
-      kxPack<<<gridFor(n), kB, 0, st>>>(n, gq, 4, w.gq);
-      kxPack<<<gridFor(n), kB, 0, st>>>(n, gv, 3, w.gv);
-      kxPack<<<gridFor(n), kB, 0, st>>>(n, gw, 3, w.gw);
+      kxPack<<<gridFor(n), kB, 0, st>>>(n, gx, 3, w0.gx);
+      kxPack<<<gridFor(n), kB, 0, st>>>(n, gq, 4, w0.gq);
+      kxPack<<<gridFor(n), kB, 0, st>>>(n, gv, 3, w0.gv);
+      kxPack<<<gridFor(n), kB, 0, st>>>(n, gw, 3, w0.gw);
     }
     cudaCheck(cudaMemsetAsync(A.small.p, 0, 8 * sizeof(double), st), "memset");
     // the last substep's ledger output feeds nothing
     const int T = (int)A.recs.size();
-    cudaCheck(cudaMemsetAsync(w.alamOut, 0, std::max(A.recs[T - 1]->nm, 1) * sizeof(D4), st), "memset");
-    cudaCheck(cudaMemsetAsync(w.aposOut, 0, std::max(A.recs[T - 1]->nm, 1) * sizeof(double), st), "memset");
+    cudaCheck(cudaMemsetAsync(w0.alamOut, 0, std::max(A.recs[T - 1]->nm, 1) * sizeof(D4), st), "memset");
+    cudaCheck(cudaMemsetAsync(w0.aposOut, 0, std::max(A.recs[T - 1]->nm, 1) * sizeof(double), st), "memset");
+    // the replay of substep t - 1 runs on the side stream beside the reverse of substep t: a replay
+    // reads only the record, and replay buffer set t % 2 serves substep t; the side stream waits
+    // until the reverse that last used a set is done before it replays into it
+    cudaCheck(cudaEventRecord(A.evStart, st), "event");
+    cudaCheck(cudaStreamWaitEvent(sb, A.evStart, 0), "event");
+    auto replayOn = [&](int t) {
+      const XRec& R = *A.recs[t];
+      replay(sb, sc, R, view(R), W[t & 1], t + 1 < T ? A.recs[t + 1].get() : nullptr, t);
+      cudaCheck(cudaEventRecord(A.evRep[t & 1], sb), "event");
+    };
+    replayOn(T - 1);
     for (int t = T - 1; t >= 0; --t) {
+      const int k = t & 1;
+      XWork& w = W[k];
+      if (t >= 1) {
+        if (t + 1 <= T - 1)
+          cudaCheck(cudaStreamWaitEvent(sb, A.evRev[k ^ 1], 0), "event");
+        replayOn(t - 1);
+      }
+      cudaCheck(cudaStreamWaitEvent(st, A.evRep[k], 0), "event");
       const XRec& R = *A.recs[t];
       const XView r = view(R);
-      replay(s, sc, R, r, w, t + 1 < T ? A.recs[t + 1].get() : nullptr, t);
       reverse(s, A, sc, R, r, w);
       if (t > 0) {
         const XRec& P = *A.recs[t - 1];
@@ -1627,8 +1681,14 @@ struct XAdjAccess {
       std::swap(w.gq, w.aq);
       std::swap(w.gv, w.av);
       std::swap(w.gw, w.aw);
+      // both sets share the adjoint buffers
+      XWork& o = W[k ^ 1];
+      o.gx = w.gx, o.gq = w.gq, o.gv = w.gv, o.gw = w.gw, o.ax = w.ax, o.aq = w.aq, o.av = w.av, o.aw = w.aw;
+      o.alamOut = w.alamOut, o.alamPrev = w.alamPrev, o.aposOut = w.aposOut, o.aposPrev = w.aposPrev;
+      cudaCheck(cudaEventRecord(A.evRev[k], st), "event");
       cudaCheck(cudaGetLastError(), "xadj backward");
     }
+    XWork& w = W[0];
     if (n > 0) {
       kxUnpack<<<gridFor(n), kB, 0, st>>>(n, w.gx, 3, dx);
       kxUnpack<<<gridFor(n), kB, 0, st>>>(n, w.gq, 4, dq);
@@ -1637,6 +1697,7 @@ struct XAdjAccess {
     }
     double h[8];
     cudaCheck(cudaMemcpyAsync(h, A.small.p, sizeof h, cudaMemcpyDeviceToHost, st), "D2H");
+    cudaCheck(cudaStreamSynchronize(sb), "xadj side stream");
     s.sync();
     dtheta[0] = h[0], dtheta[1] = h[1], dtheta[2] = h[2];
     A.err[0] = h[4], A.err[1] = h[5];
@@ -1666,14 +1727,16 @@ struct XAdjAccess {
     checkScope(s);
     cudaStream_t st = s.stream_;
     const XScene sc = scene(s, A);
-    XWork w = work(s, A);
+    XWork W[2];
+    work(s, A, W);
+    XWork& w = W[0];
     A.hashBuf.ensure(1, false, st);
     cudaCheck(cudaMemsetAsync(A.hashBuf.p, 0, sizeof(u64), st), "memset");
     w.hash = A.hashBuf.p;
     const int T = (int)A.recs.size();
     for (int t = 0; t < T; ++t) {
       const XRec& R = *A.recs[t];
-      replay(s, sc, R, view(R), w, nullptr, t);
+      replay(st, sc, R, view(R), w, nullptr, t);
     }
     u64 h = 0;
     cudaCheck(cudaMemcpyAsync(&h, A.hashBuf.p, sizeof h, cudaMemcpyDeviceToHost, st), "D2H");
