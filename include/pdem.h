@@ -176,6 +176,11 @@ int pdem_debug_set_max_contacts(pdem_handle h, int max_contacts);
  * step reports PDEM_ERR_CUDA at its next read-back and clears the bit; the substep's state is then
  * partial and the caller sets the bodies' state again. Lets a test make the wait run out. */
 int pdem_debug_set_barrier_spins(pdem_handle h, long spins);
+/* the broadphase's own stable radix sort (the Morton sort of the LBVH build) on HOST arrays of n
+ * (key, value) pairs, by the low end_bit bits of the keys (a test entry point: it allocates
+ * device memory for the call and synchronises) */
+int pdem_debug_radix_sort(const unsigned long long* keys, const int* vals, int n, int end_bit,
+                          unsigned long long* out_keys, int* out_vals);
 
 /* ---- batched form (no reference counterpart: the reference steps one scene per Simulation) ----
  * Several independent scenes share one simulation: scene s owns the bodies

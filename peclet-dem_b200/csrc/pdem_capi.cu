@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "../../include/pdem.h"
+#include "pdem_radix.cuh"
 #include "pdem_sim.cuh"
 #include "pdem_xadj_api.cuh"
 
@@ -630,6 +631,49 @@ int pdem_profile_read(pdem_handle h, double* ms, long* calls, int cap, long* lau
       *launches = S.launches_;
   });
   return n;
+}
+
+int pdem_debug_radix_sort(const unsigned long long* keys, const int* vals, int n, int end_bit,
+                          unsigned long long* out_keys, int* out_vals) {
+  if (n < 0 || end_bit < 0 || end_bit > 64 || (n > 0 && (!keys || !vals || !out_keys || !out_vals))) {
+    g_err = "debug_radix_sort: n >= 0, 0 <= end_bit <= 64 and four arrays";
+    return PDEM_ERR_INVALID;
+  }
+  if (n == 0)
+    return PDEM_OK;
+  unsigned long long *dk = nullptr, *dko = nullptr, *dkt = nullptr;
+  int *dv = nullptr, *dvo = nullptr, *dvt = nullptr, *dh = nullptr;
+  cudaError_t e = cudaSuccess;
+  const size_t kb = (size_t)n * sizeof(unsigned long long), vb = (size_t)n * sizeof(int);
+  for (auto* p : {&dk, &dko, &dkt})
+    if (e == cudaSuccess)
+      e = cudaMalloc(reinterpret_cast<void**>(p), kb);
+  for (auto* p : {&dv, &dvo, &dvt})
+    if (e == cudaSuccess)
+      e = cudaMalloc(reinterpret_cast<void**>(p), vb);
+  if (e == cudaSuccess)
+    e = cudaMalloc(reinterpret_cast<void**>(&dh), 256 * (size_t)pdem::radixBlocks(n) * sizeof(int));
+  if (e == cudaSuccess)
+    e = cudaMemcpy(dk, keys, kb, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(dv, vals, vb, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = pdem::radixSortPairs(dk, dko, dv, dvo, n, end_bit, dkt, dvt, dh, 0);
+  if (e == cudaSuccess)
+    e = cudaDeviceSynchronize();
+  if (e == cudaSuccess)
+    e = cudaMemcpy(out_keys, dko, kb, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(out_vals, dvo, vb, cudaMemcpyDeviceToHost);
+  for (void* p : {(void*)dk, (void*)dko, (void*)dkt, (void*)dv, (void*)dvo, (void*)dvt, (void*)dh})
+    if (p)
+      cudaFree(p);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    g_err = std::string("debug_radix_sort: ") + cudaGetErrorString(e);
+    return PDEM_ERR_CUDA;
+  }
+  return PDEM_OK;
 }
 
 int pdem_xa_begin(pdem_handle h, const double* x, const double* q, const double* v, const double* w, int n) {

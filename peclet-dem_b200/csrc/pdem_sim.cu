@@ -14,6 +14,7 @@
 #include "pdem_kernels.cuh"
 #include "pdem_multilevel.cuh"
 #include "pdem_persist.cuh"
+#include "pdem_radix.cuh"
 #include "pdem_shell.hpp"
 #include "pdem_sim.cuh"
 #include "pdem_sdf.cuh"
@@ -982,7 +983,14 @@ int Sim<R>::findCollisions(R margin, int cap, int2* out, R extra) {
   if (rebuild) {
     ++launches_, kMorton<R><<<gridFor(n), kBlock, 0, stream_>>>(n, bn, bb);  // into codes_ / bidx_
     KCHECK("morton");
-    sortPairs(codes_.p, codesAlt_.p, bidx_.p, bidxAlt_.p, n, codeBits);
+    // the leaf order: the broadphase's own stable radix sort of the Morton codes
+    radixK_.ensure(n, false, stream_);
+    radixV_.ensure(n, false, stream_);
+    radixH_.ensure(256 * (size_t)radixBlocks(n), false, stream_);
+    launches_ += 3 * ((codeBits + 7) / 8);
+    cudaCheck(radixSortPairs(codes_.p, codesAlt_.p, bidx_.p, bidxAlt_.p, n, codeBits, radixK_.p, radixV_.p,
+                             radixH_.p, stream_),
+              "morton sort");
   }
   // the sorted order (this build's, or the last build's on a refit-only substep) is the sort's
   // output, in the *Alt buffers

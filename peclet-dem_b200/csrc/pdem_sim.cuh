@@ -312,6 +312,8 @@ class Sim {
   // broadphase scratch
   DBuf<char> bvhBoxes_, bvhNodes_;
   DBuf<u64> codes_, codesAlt_, bounds_;
+  DBuf<u64> radixK_;            // the Morton sort's scratch (pdem_radix.cuh)
+  DBuf<int> radixV_, radixH_;
   DBuf<int> bidx_, bidxAlt_, left_, right_, parent_, flag_, qcnt_, qoff_, rowCnt_, bflag_;
   DBuf<int2> slots_;
   // manifold reduction scratch (kept for the position-impulse commit)

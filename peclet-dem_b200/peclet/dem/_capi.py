@@ -134,6 +134,7 @@ _SIGS = {
     "xa_backward": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _dbl_p]),
     "xa_info": (C.c_int, [_vp, _long_p, _dbl_p]),
     "xa_signature": (C.c_long, [_vp, _long_p, C.c_long]),
+    "debug_radix_sort": (C.c_int, [_vp, _vp, C.c_int, C.c_int, _vp, _vp]),
     "xa_branches": (C.c_int, [_vp, C.POINTER(C.c_ulonglong)]),
     # forward, adjoint and tangent-linear runs of the Hertz sphere substep (pdem_adjoint.cu)
     "hz_state_size": (C.c_long, [C.c_int, C.c_int]),
