@@ -101,9 +101,8 @@ def ref_omp_lib():
 def headline_desc(world=1):
     return {"workload": "plain_settling_4096_fp64", "particles": 4096, "substeps_per_step": SUBSTEPS,
             "dt_substep": 1e-5, "iterations": {"position": 10, "velocity": 10},
-            "state": "saved state after 800 of the configuration's 1000 outer steps (FP64 B200 step from the "
-                     "lattice start); both arms restart from it; warm-start ledger cold at the restart",
-            "l2": "flushed between timed steps (256 MiB write); the state (~4 MB) fits in L2",
+            "state": "restart at outer step 800 of 1000 (saved FP64 state), both arms; ledger cold",
+            "l2": "flushed between timed steps (256 MiB); state ~4 MB",
             "parallelism": f"replicas x{world}" if world > 1 else "single"}
 
 
@@ -363,8 +362,8 @@ def run_headline(args, rank, world, dist, dem, W):
             threads = os.cpu_count() or 1
             v, el, _ = cpu_reference_steps(sc, lib, threads, 3, args.cpu_steps)
             cpu = {"value": v, "unit": METRIC, "cores": threads, "kind": "reference",
-                   "sample": f"{args.cpu_steps} outer steps (x10 substeps) of the same restart after 3 warm-up steps, "
-                             f"{el:.1f} s; reference headers on the OpenMP Kokkos shim, float, -O3 -march={march}"}
+                   "sample": f"{args.cpu_steps}x10 substeps of the restart after 3 warm-up, {el:.1f} s; "
+                             f"reference on the OpenMP shim, float, -march={march}"}
     from peclet.dem import stats as S
     pk = S.packing_stats(x_end, np.full(n, sc.global_scale), 1.0 / sc.inv_mass, v_end, w_end,
                          1.0 / sc.inv_inertia[:, 0], sc.domain[0], sc.domain[1])
@@ -909,8 +908,7 @@ def run_ours(args):
             b = detail["batched"]
             flat.update(batched_fp64_value=b["fp64"]["value"], batched_mixed_value=b["mixed"]["value"],
                         batched_mixed_over_fp64=b["mixed_over_fp64"],
-                        mixed_err_radii=b["mixed"]["err_vs_fp64"]["max_position_error_radii"],
-                        batched_mean_velocity_sweeps=b["fp64"]["mean_sweeps_last_substep"]["velocity"])
+                        mixed_err_radii=b["mixed"]["err_vs_fp64"]["max_position_error_radii"])
         if "calibration" in detail:
             cb = detail["calibration"]
             c64 = cb["checks_64_substeps"]
@@ -951,7 +949,6 @@ def run_ours(args):
             "roofline": {k: h["roofline"][k] for k in ("bound", "kernel", "achieved", "peak", "unit", "frac",
                                                        "traffic", "peak_source")},
             "cpu_baseline": h["cpu"], "clocks": h["clocks"],
-            "sweeps_per_substep": {k: round(v, 2) for k, v in h["sweeps_per_substep"].items()},
             "device_allocations_timed": h["timed_allocs"], **{k: _compact(v) for k, v in flat.items()}}
         print(json.dumps(line))
     if dist is not None:
