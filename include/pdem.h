@@ -328,7 +328,9 @@ int pdem_hz_jvp(int precision, const pdem_hz_model* model, int steps, void* d_st
  * rollout's end state and returns the gradients with respect to its start state (rows as
  * above) and to (eN, eT, mu) of pdem_set_material_params (dtheta: 3 doubles, HOST); it replays
  * each substep from its record and reverses it, the sweeps in reverse colour and sweep order
- * over the frozen colouring. Synchronise the caller's stream before these calls; each returns
+ * over the frozen colouring. The backward uses the rollout's own substep length, material and
+ * gravity; the masses, inertia, scales, external forces and planes must stay as they were during
+ * the rollout until its backward. Synchronise the caller's stream before these calls; each returns
  * with the library's stream synchronised. pdem_xa_info: out[0] substeps recorded, out[1] bytes
  * of the record, out[2] bytes of the reverse workspace, out[3] the largest sweep count;
  * err[0] the largest deviation of a replayed substep's end positions from the recorded next

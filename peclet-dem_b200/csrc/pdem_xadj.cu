@@ -1200,7 +1200,7 @@ struct XAdj {
   std::vector<std::unique_ptr<XRec>> recs;
   bool open = false;
   int n = 0;
-  double dt = 0;
+  double dt = 0, mat[3] = {0, 0, 0}, grav[3] = {0, 0, 0};
   // workspace: two sets of replay buffers (the replay of a substep runs beside the reverse of the
   // next one, on the side stream) and one set of adjoint buffers
   DBuf<D4> rbody[2], rcont[2], rman[2], tv[2], tp[2];
@@ -1275,10 +1275,10 @@ struct XAdjAccess {
     c.gs = s.gs_;
     c.par = s.shape_.par[0];
     c.eps = 1e-4;
-    c.eN = s.eN_;
-    c.eT = s.eT_;
-    c.mu = s.mu_;
-    c.g = V3<double>{s.g_[0], s.g_[1], s.g_[2]};
+    c.eN = A.mat[0];  // the rollout's own material and gravity (recorded by its first substep)
+    c.eT = A.mat[1];
+    c.mu = A.mat[2];
+    c.g = V3<double>{A.grav[0], A.grav[1], A.grav[2]};
     c.invMass = s.invMass_.p;
     c.invI = s.invI_.p;
     c.scale = s.scale_.p;
@@ -1341,6 +1341,12 @@ struct XAdjAccess {
     if (!A.recs.empty() && dt != A.dt)
       throw std::invalid_argument("XPBD adjoint: one substep length per rollout");
     A.dt = dt;
+    // the material and gravity the rollout runs with: the backward uses these, not later settings
+    const double mat[3] = {s.eN_, s.eT_, s.mu_}, grav[3] = {s.g_[0], s.g_[1], s.g_[2]};
+    if (!A.recs.empty() && (std::memcmp(mat, A.mat, sizeof mat) || std::memcmp(grav, A.grav, sizeof grav)))
+      throw std::invalid_argument("XPBD adjoint: the material or gravity changed during the rollout");
+    std::memcpy(A.mat, mat, sizeof mat);
+    std::memcpy(A.grav, grav, sizeof grav);
     cudaStream_t st = s.stream_;
     for (int it = 0; it < substeps; ++it) {
       auto R = std::make_unique<XRec>();

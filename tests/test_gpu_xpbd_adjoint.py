@@ -139,3 +139,24 @@ def test_branch_signature_certifies_differences(gpu_api):
         hashes.append((roll.signature(), roll.branches()))
     assert np.array_equal(hashes[0][0], hashes[1][0]) and hashes[0][1] == hashes[1][1]
     assert hashes[0][1] != hashes[2][1]
+
+
+def test_backward_uses_the_rollouts_material(gpu_api):
+    """The backward differentiates the rollout that ran: a material set on the simulation after the
+    forward (before the backward) changes nothing in the gradients (beyond the rounding of the
+    reverse's atomic sums, which vary from run to run)."""
+    from peclet.dem.xpbd_adjoint import XpbdRollout
+    sc = _impacts()
+    out = []
+    for later in (None, (0.1, 0.0, 0.9)):
+        sim = P.build(gpu_api, sc, None, "fp64")
+        roll = XpbdRollout(sim)
+        start = [torch.tensor(a, dtype=torch.float64, device="cuda", requires_grad=True) for a in _start(sc)]
+        theta = torch.tensor(sc.material, dtype=torch.float64, requires_grad=True)
+        x, q, v, w = roll(*start, theta, 10)
+        if later:
+            sim.set_material_params(*later)
+        (x.sum() + v.sum()).backward()
+        out.append((theta.grad.numpy().copy(), start[2].grad.cpu().numpy()))
+    np.testing.assert_allclose(out[0][0], out[1][0], rtol=1e-12, atol=1e-15)
+    np.testing.assert_allclose(out[0][1], out[1][1], rtol=1e-12, atol=1e-12 * np.abs(out[0][1]).max())
