@@ -315,7 +315,7 @@ int pdem_hz_jvp(int precision, const pdem_hz_model* model, int steps, void* d_st
 /* ---- adjoint of the XPBD substep (added form; no reference counterpart) ----
  * The plain FP64 step (pdem_step, src/sim.hpp:97-488) differentiated over a recorded rollout:
  * one scene of spheres without point shells, planes as walls, gravity on with the coloured
- * Gauss-Seidel (PGS) velocity solve, stabilization "off" or "onesided", no periodicity, growth,
+ * Gauss-Seidel (PGS) velocity solve, stabilization "off", "onesided" or "escalate", no periodicity, growth,
  * thermostat or pair materials; every entry coloured (no Jacobi leftovers). Other set-ups are
  * refused with PDEM_ERR_INVALID at pdem_xa_begin / pdem_xa_step. Rows are DEVICE doubles:
  * positions, velocities and angular velocities n x 3, quaternions n x 4 (x, y, z, w).

@@ -28,7 +28,7 @@
 //
 // Scope (refused with std::invalid_argument otherwise): FP64, one scene, sphere shapes without
 // point shells, isotropic inverse inertia, planes as the only walls, gravity on and coloured
-// Gauss-Seidel (the PGS path), stabilization off or one-sided, no periodicity, growth,
+// Gauss-Seidel (the PGS path), stabilization off, one-sided or escalate, no periodicity, growth,
 // thermostat or pair materials, every entry coloured (no Jacobi leftovers) and no saturated
 // colour.
 #include <algorithm>
@@ -1257,8 +1257,8 @@ struct XAdjAccess {
       bad("no pair materials");
     if (!s.useGS_ || (s.g_[0] == 0.0 && s.g_[1] == 0.0 && s.g_[2] == 0.0))
       bad("the PGS path (gravity on, Gauss-Seidel velocity solve)");
-    if (s.stabMode_ != 0 && s.stabMode_ != 1)
-      bad("stabilization off or one-sided");
+    if (s.stabMode_ != 0 && s.stabMode_ != 1 && s.stabMode_ != 3)
+      bad("stabilization off, one-sided or escalate");
   }
   static void isotropic(S& s) {
     std::vector<D4> ii(s.numReal_);
@@ -1381,7 +1381,8 @@ struct XAdjAccess {
       if (R->ncolV > kMaxColours || R->ncolP > kMaxColours)
         throw std::runtime_error("XPBD adjoint: a colouring saturated its 62 colours");
       R->velSweeps = c.velSweeps;
-      R->stab = c.stabRun != 0 && s.stabMode_ == 1;
+      // the one-sided pass sweeps with its side flags, escalate with none (they stay cleared)
+      R->stab = c.stabRun != 0 && (s.stabMode_ == 1 || s.stabMode_ == 3);
       R->stabSweeps = R->stab ? c.stabSweeps : 0;
       R->posSweeps = c.posSweeps;
       const int nc = R->nc, nm = R->nm;

@@ -1,7 +1,7 @@
 """Differentiable rollout of the plain FP64 XPBD step: forward and hand-written adjoint on the B200.
 
 `XpbdRollout(sim)` wraps a configured FP64 `Simulation` (spheres without point shells, planes,
-gravity on with the Gauss-Seidel velocity solve, stabilization "off" or "onesided"; no
+gravity on with the Gauss-Seidel velocity solve, stabilization "off", "onesided" or "escalate"; no
 periodicity, growth, thermostat or pair materials). `rollout(x0, q0, v0, w0, theta, substeps)`
 runs `substeps` substeps of the production step (src/sim.hpp:97-488, `pdem_step`) from the start
 state (positions, quaternions x y z w, velocities, angular velocities) with

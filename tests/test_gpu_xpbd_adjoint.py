@@ -49,9 +49,9 @@ def _start(sc):
     return [np.asarray(a, np.float64) for a in (sc.pos, q, sc.vel, w)]
 
 
-def _gpu(gpu_api, sc, T):
+def _gpu(gpu_api, sc, T, extra=None):
     from peclet.dem.xpbd_adjoint import XpbdRollout
-    sim = P.build(gpu_api, sc, None, "fp64")
+    sim = P.build(gpu_api, sc, extra, "fp64")
     roll = XpbdRollout(sim)
     dev = torch.device("cuda")
     start = [torch.tensor(a, dtype=torch.float64, device=dev, requires_grad=True) for a in _start(sc)]
@@ -61,11 +61,13 @@ def _gpu(gpu_api, sc, T):
     L = sum((torch.tensor(w, dtype=torch.float64, device=dev) * o).sum() for w, o in zip(W, out))
     L.backward()
     grads = [t.grad.cpu().numpy() for t in start]
-    return [o.detach().cpu().numpy() for o in out], grads, theta.grad.numpy(), roll.info(), sim
+    return [o.detach().cpu().numpy() for o in out], grads, theta.grad.numpy(), roll.info(), roll
 
 
-def _dual(orc_api, sc, T, direction):
+def _dual(orc_api, sc, T, direction, extra=None):
     d = sc.apply(DO.dual_sim(orc_api, sc.n + 8))
+    if extra:
+        extra(d)
     for lane in range(3):
         DO.seed(d, DO.MATERIAL, lane, np.eye(3)[lane])
     dx, dq, dv, dw = direction
@@ -160,3 +162,20 @@ def test_backward_uses_the_rollouts_material(gpu_api):
         out.append((theta.grad.numpy().copy(), start[2].grad.cpu().numpy()))
     np.testing.assert_allclose(out[0][0], out[1][0], rtol=1e-12, atol=1e-15)
     np.testing.assert_allclose(out[0][1], out[1][1], rtol=1e-12, atol=1e-12 * np.abs(out[0][1]).max())
+
+
+def test_adjoint_with_escalate_stabilization(gpu_api, orc_api):
+    """The escalate stabilization mode (up to 256 PGS sweeps at the stabilization threshold, no
+    side flags) reversed like the one-sided pass: against the dual numbers as above."""
+    sc = _column()
+    escalate = lambda sim: sim.set_stabilization_mode("escalate")
+    rng = np.random.default_rng(19)
+    direction = [rng.normal(size=(sc.n, c)) * s for c, s in ((3, 1e-3), (4, 1e-2), (3, 0.1), (3, 10.0))]
+    end, grads, dtheta, info, roll = _gpu(gpu_api, sc, 20, escalate)
+    tans, _ = _dual(orc_api, sc, 20, direction, escalate)
+    assert info["replay_dx"] <= 1e-9, info
+    assert roll.signature()[:, 5].sum() > 0, "the stabilization pass did not run"
+    for k in range(3):
+        assert abs(dtheta[k] - tans[k]) <= RTOL * max(abs(tans[k]), 1e-6 * np.abs(tans).max()), (k, dtheta, tans)
+    dirderiv = sum(np.sum(g * d) for g, d in zip(grads, direction))
+    assert abs(dirderiv - tans[3]) <= RTOL * max(abs(tans[3]), 1e-6), (dirderiv, tans[3])
